@@ -1,0 +1,127 @@
+/* kinterp: C ABI of the B200 recursive-skeletonization solver for 2-D
+ * Laplace / Stokes boundary integral equations.
+ *
+ * Every entry point replaces one call of the reference C++ API
+ * (jpryan1/kern-interp-old; paths relative to that repository) and takes
+ * plain pointers and sizes only.  Unless a name ends in _device, buffers are
+ * host memory and the call returns after its results are in them.  The
+ * `stream` argument of ki_factor is a cudaStream_t (NULL: the library creates
+ * its own non-blocking stream); every later call on the handle is ordered on
+ * that stream.  All calls return KI_OK (0) or an error code, with the message
+ * in ki_last_error(); nothing ever aborts the process.
+ *
+ * Geometry arrays follow the reference Boundary (boundaries/boundary.h:35-51):
+ * points and normals interleaved xy (2 n_points doubles), curvatures and
+ * weights (n_points), holes as n_holes rows of (cx, cy, radius, num_nodes).
+ * A Stokes dof is 2 * point + component, as in Kernel::stokes_get
+ * (kernel/kernel.cpp:47-96).
+ */
+#ifndef KINTERP_H_
+#define KINTERP_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ki_solver_s* ki_solver_t;
+
+enum {
+  KI_OK = 0,
+  KI_ERR_ARG = 1,      /* invalid argument or handle */
+  KI_ERR_CUDA = 2,     /* CUDA runtime error (no device, launch failure, ...) */
+  KI_ERR_NUMERIC = 3,  /* singular block, no compression possible */
+  KI_ERR_STATE = 4     /* call out of order (e.g. solve before factor) */
+};
+
+enum { KI_LAPLACE = 0, KI_LAPLACE_NEUMANN = 1, KI_STOKES = 2 };
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ki_last_error(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int ki_version(void);
+
+/* Builds the quadtree and skeletonizes the boundary operator.
+ * Replaces QuadTree::initialize_tree (quadtree/quadtree.h:85-86), the U/Psi
+ * set-up of boundary_integral_solve (linear_solve.cpp:194-203) and
+ * SkelFactorization(id_tol, threads).skeletonize (skel_factorization/
+ * skel_factorization.h:25,40).  max_leaf_dofs is the reference's
+ * MAX_LEAF_DOFS (quadtree.h:10; 32 there). */
+int ki_factor(int pde, int n_points, const double* points, const double* normals,
+              const double* curvatures, const double* weights, int n_holes,
+              const double* holes, int max_leaf_dofs, double id_tol, void* stream,
+              ki_solver_t* out);
+
+/* Builds only the quadtree (host side, no GPU work): QuadTree::
+ * initialize_tree (quadtree.h:85-86) with every box's active list set as
+ * before any compression.  The handle answers the introspection calls below;
+ * solve calls on it return KI_ERR_STATE. */
+int ki_partition(int n_points, const double* points, int sol_dim, int max_leaf_dofs,
+                 ki_solver_t* out);
+
+/* Releases every device buffer of the handle. */
+void ki_destroy(ki_solver_t s);
+
+/* Dof count (n_points or 2 n_points) and border size (holes: 1 per hole for
+ * Laplace, 3 per hole for Stokes; 0 without holes). */
+int ki_num_dofs(ki_solver_t s);
+int ki_num_border(ki_solver_t s);
+
+/* linear_solve (linear_solve.h:27-29): mu = A^{-1} f with the factors; alpha
+ * receives the border unknowns (multiply_connected_solve,
+ * skel_factorization.h:60-61) and may be NULL when there are no holes. */
+int ki_solve(ki_solver_t s, const double* f, double* mu, double* alpha);
+
+/* ki_solve on device buffers, stream ordered, no host synchronisation.
+ * d_f and d_mu may be the same buffer. */
+int ki_solve_device(ki_solver_t s, const double* d_f, double* d_mu, double* d_alpha);
+
+/* y = A x with on-the-fly FP64 entries of the full operator (the dense
+ * matrix the reference test forms, kern_interp_test.cpp:54-90), bordered by
+ * [U; Psi, -I] when there are holes; device buffers of dofs + border. */
+int ki_apply_device(ki_solver_t s, const double* d_x, double* d_y);
+
+/* schur_solve's target evaluation (linear_solve.cpp:126-140): out = K_domain
+ * mu + U_forward alpha at n_targets points (interleaved xy). */
+int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets,
+                    const double* mu, const double* alpha, double* out);
+
+/* Kernel::operator() (kernel/kernel.cpp:99-111): column-major nt x ns block
+ * K(tgt, src) evaluated on the GPU. */
+int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src,
+                    double* out);
+
+/* Tree / skeleton introspection (QuadTree levels and InteractionLists,
+ * quadtree.h:14-102).  info[8] = is_leaf, compressed, |original|, |active|,
+ * |skel|, |redundant|, parent index in its level (-1 root), level;
+ * geom[3] = lower-left corner x, y and side length.  Lists may be NULL. */
+int ki_num_levels(ki_solver_t s);
+int ki_num_boxes(ki_solver_t s, int level);
+int ki_box_info(ki_solver_t s, int level, int idx, int* info, double* geom);
+int ki_box_lists(ki_solver_t s, int level, int idx, int* original, int* active,
+                 int* skel, int* redundant);
+/* Top-level skeleton (root active box); returns its size, fills out if given. */
+int ki_allskel(ki_solver_t s, int* out);
+
+/* Statistics of the last factorization: out[0] factor ms, [1] ID kernel ms,
+ * [2] ID launches, [3] ID algorithmic flops, [4] ID algorithmic bytes,
+ * [5] decouple ms, [6] top-level LU ms, [7] host ms blocked on rank
+ * downloads (timed factorizations only for [1], [5], [6]).  Returns the
+ * number of values written (at most n, at most 8). */
+int ki_stats(ki_solver_t s, double* out, int n);
+/* Launch log of a ki_factor_timed factorization: rows of 7 doubles
+ * (level, kind 0 ID / 1 decouple / 2 top LU, cluster size, boxes, max rows,
+ * max columns, ms).  Returns the row count; writes at most cap rows. */
+int ki_launch_log(ki_solver_t s, double* out, int cap);
+
+/* Enables CUDA-event timing of the ID launches for the next ki_factor calls
+ * made through ki_factor_timed. */
+int ki_factor_timed(int pde, int n_points, const double* points, const double* normals,
+                    const double* curvatures, const double* weights, int n_holes,
+                    const double* holes, int max_leaf_dofs, double id_tol, void* stream,
+                    ki_solver_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KINTERP_H_ */

@@ -1,0 +1,119 @@
+// Dense operator products with on-the-fly FP64 entries:
+//   * y = A x for the full boundary operator (and, for domains with holes,
+//     the bordered system [K U; Psi -I] of the reference's residual check,
+//     kern_interp_test.cpp:54-78), used by iterative refinement / GMRES;
+//   * target evaluation, schur_solve's K_domain mu + U_forward alpha
+//     (linear_solve.cpp:126-140, kernel.cpp:337-357, linear_solve.cpp:18-64);
+//   * explicit kernel blocks K(tgt, src) (Kernel::operator(), kernel.cpp:99-111).
+// One thread per output row; the source nodes are read in the same order by
+// all lanes of a warp, so each load is a broadcast.
+#include "ki_kernels.h"
+
+namespace kib {
+
+namespace {
+
+__global__ void apply_kernel(int pde, const Node* __restrict__ nodes, int n,
+                             const double* __restrict__ x, double* __restrict__ y, int nb,
+                             const double* __restrict__ U, const double* __restrict__ Psi) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    double s = 0.0;
+    for (int j = 0; j < n; j++) s += boundary_entry(pde, nodes, i, j) * x[j];
+    for (int b = 0; b < nb; b++) s += U[i + static_cast<long long>(n) * b] * x[n + b];
+    y[i] = s;
+  } else if (i < n + nb) {
+    const int h = i - n;
+    double s = -x[i];
+    for (int j = 0; j < n; j++) s += Psi[h + static_cast<long long>(nb) * j] * x[j];
+    y[i] = s;
+  }
+}
+
+// Border columns for one target point (initialize_U_mat, linear_solve.cpp:18-64).
+__device__ void border_u(int pde, double tx, double ty, const double* hole, int comp,
+                         double* out) {
+  const double rx = tx - hole[0], ry = ty - hole[1];
+  const double rn = sqrt(rx * rx + ry * ry);
+  if (pde == kLaplace) {
+    out[0] = log(rn);
+    return;
+  }
+  const double scale = 1.0 / (4 * 3.14159265358979323846);
+  const double inv2 = 1.0 / (rn * rn);
+  const double lg = log(1 / rn);
+  if (comp == 0) {
+    out[0] = scale * (lg + inv2 * rx * rx);
+    out[1] = scale * (inv2 * rx * ry);
+    out[2] = ry * (scale * inv2);
+  } else {
+    out[0] = scale * (inv2 * ry * rx);
+    out[1] = scale * (lg + inv2 * ry * ry);
+    out[2] = -rx * (scale * inv2);
+  }
+}
+
+__global__ void targets_kernel(int pde, const Node* __restrict__ nodes, int n, int nt,
+                               const double* __restrict__ tg, const double* __restrict__ mu,
+                               int nh, const double* __restrict__ holes,
+                               const double* __restrict__ alpha, double* __restrict__ out) {
+  const int sd = pde == kStokes ? 2 : 1;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= nt * sd) return;
+  const int t = row / sd, comp = row % sd;
+  const double tx = tg[2 * t], ty = tg[2 * t + 1];
+  double s = 0.0;
+  for (int j = 0; j < n; j++) s += forward_entry(pde, nodes, tx, ty, comp, j) * mu[j];
+  if (alpha && pde != kLaplaceNeumann) {
+    for (int h = 0; h < nh; h++) {
+      double u[3];
+      border_u(pde, tx, ty, holes + 4 * h, comp, u);
+      if (pde == kLaplace) {
+        s += u[0] * alpha[h];
+      } else {
+        s += u[0] * alpha[3 * h] + u[1] * alpha[3 * h + 1] + u[2] * alpha[3 * h + 2];
+      }
+    }
+  }
+  out[row] = s;
+}
+
+__global__ void block_kernel(int pde, const Node* __restrict__ nodes, const int* tgt, int nt,
+                             const int* src, int ns, double* out) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(nt) * ns) return;
+  const int i = static_cast<int>(e % nt), j = static_cast<int>(e / nt);
+  out[e] = boundary_entry(pde, nodes, tgt[i], src[j]);
+}
+
+}  // namespace
+
+cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const double* x,
+                                  double* y, int nb, const double* U, const double* Psi,
+                                  cudaStream_t s) {
+  const int rows = n_dofs + nb;
+  apply_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, x, y, nb, U, Psi);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
+                                const double* targets, const double* mu, int nh,
+                                const double* holes, const double* alpha, double* out,
+                                cudaStream_t s) {
+  const int rows = nt * (pde == kStokes ? 2 : 1);
+  if (rows == 0) return cudaSuccess;
+  targets_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, nt, targets, mu, nh,
+                                                     holes, alpha, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
+                                const int* src, int ns, double* out, cudaStream_t s) {
+  const long long tot = static_cast<long long>(nt) * ns;
+  if (tot == 0) return cudaSuccess;
+  block_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(pde, nodes, tgt, nt, src, ns,
+                                                                   out);
+  return cudaGetLastError();
+}
+
+}  // namespace kib

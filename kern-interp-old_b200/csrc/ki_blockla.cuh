@@ -1,0 +1,183 @@
+// CTA- and warp-level FP64 dense routines on column-major matrices, used
+// inside the per-box kernels (decouple, sweeps, diagonal solves).  They
+// restate the LAPACK/BLAS steps the reference calls through ki_Mat
+// (ki_mat.cpp:310-317 dgemm, :427-493 dgetrf/dgetrs).
+#ifndef KI_BLOCKLA_CUH_
+#define KI_BLOCKLA_CUH_
+
+#include <cuda_runtime.h>
+
+namespace kib {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// C (m x n) = C0 - op(A) op(B) over the CTA, with op(A) m x kk, op(B) kk x n.
+// C may alias C0.  ta/tb select the transposes (A stored kk x m when ta).
+__device__ inline void cta_gemm_sub(double* C, int ldc, const double* C0, int ldc0,
+                                    const double* A, int lda, bool ta, const double* B,
+                                    int ldb, bool tb, int m, int n, int kk) {
+  for (int e = threadIdx.x; e < m * n; e += blockDim.x) {
+    const int i = e % m, j = e / m;
+    double s = 0.0;
+    for (int l = 0; l < kk; l++) {
+      const double a = ta ? A[l + static_cast<long long>(lda) * i]
+                          : A[i + static_cast<long long>(lda) * l];
+      const double b = tb ? B[j + static_cast<long long>(ldb) * l]
+                          : B[l + static_cast<long long>(ldb) * j];
+      s += a * b;
+    }
+    C[i + static_cast<long long>(ldc) * j] = C0[i + static_cast<long long>(ldc0) * j] - s;
+  }
+}
+
+// In-place LU with partial pivoting (dgetf2) of an n x n matrix over the
+// CTA.  ipiv[j] = row exchanged with row j.  `red` needs 2 * 32 doubles.
+// Returns nonzero if an exactly zero pivot was met (LAPACK's info > 0).
+__device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  int* redi = reinterpret_cast<int*>(red + 32);
+  int info = 0;
+  for (int j = 0; j < n; j++) {
+    // first maximum of |a(j:n, j)|
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+      const double v = fabs(a[i + static_cast<long long>(ld) * j]);
+      if (v > bv || (v == bv && i < bp)) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = red[0];
+      int p = redi[0];
+      for (int w = 1; w < nw; w++)
+        if (red[w] > v || (red[w] == v && redi[w] < p)) {
+          v = red[w];
+          p = redi[w];
+        }
+      ipiv[j] = p;
+      redi[31] = p;
+    }
+    __syncthreads();
+    const int p = redi[31];
+    const double piv = a[p + static_cast<long long>(ld) * j];
+    if (piv != 0.0) {
+      if (p != j) {
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+          double* x = a + static_cast<long long>(ld) * c;
+          const double t = x[j];
+          x[j] = x[p];
+          x[p] = t;
+        }
+        __syncthreads();
+      }
+      const double inv = 1.0 / piv;
+      for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
+        a[i + static_cast<long long>(ld) * j] *= inv;
+    } else {
+      info = 1;
+    }
+    __syncthreads();
+    const int rem = n - j - 1;
+    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
+      const int i = j + 1 + e % rem, c = j + 1 + e / rem;
+      a[i + static_cast<long long>(ld) * c] -=
+          a[i + static_cast<long long>(ld) * j] * a[j + static_cast<long long>(ld) * c];
+    }
+    __syncthreads();
+  }
+  return info;
+}
+
+// b (length n, stride inc) <- A^{-1} b for the LU above, by one warp.
+__device__ inline void warp_lu_solve(const double* lu, int n, int ld, const int* ipiv,
+                                     double* b, int inc) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0)
+    for (int i = 0; i < n; i++) {
+      const int p = ipiv[i];
+      if (p != i) {
+        const double t = b[static_cast<long long>(inc) * i];
+        b[static_cast<long long>(inc) * i] = b[static_cast<long long>(inc) * p];
+        b[static_cast<long long>(inc) * p] = t;
+      }
+    }
+  __syncwarp();
+  for (int k = 0; k < n; k++) {  // unit lower, column sweep
+    const double v = b[static_cast<long long>(inc) * k];
+    if (v != 0.0)
+      for (int i = k + 1 + lane; i < n; i += 32)
+        b[static_cast<long long>(inc) * i] -= v * lu[i + static_cast<long long>(ld) * k];
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {  // upper, column sweep
+    const double bk = b[static_cast<long long>(inc) * k];
+    __syncwarp();
+    if (bk != 0.0) {
+      const double v = bk / lu[k + static_cast<long long>(ld) * k];
+      if (lane == 0) b[static_cast<long long>(inc) * k] = v;
+      for (int i = lane; i < k; i += 32)
+        b[static_cast<long long>(inc) * i] -= v * lu[i + static_cast<long long>(ld) * k];
+    }
+    __syncwarp();
+  }
+}
+
+// b <- A^{-T} b for the LU above (dgetrs 'T'), by one warp.
+__device__ inline void warp_lu_solve_t(const double* lu, int n, int ld, const int* ipiv,
+                                       double* b, int inc) {
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k < n; k++) {  // U^T y = b: row k of U dotted with y(0:k)
+    double s = 0.0;
+    for (int i = lane; i < k; i += 32)
+      s += lu[i + static_cast<long long>(ld) * k] * b[static_cast<long long>(inc) * i];
+    s = warp_sum_d(s);
+    if (lane == 0) {
+      const long long o = static_cast<long long>(inc) * k;
+      b[o] = (b[o] - s) / lu[k + static_cast<long long>(ld) * k];
+    }
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; k--) {  // L^T z = y (unit)
+    double s = 0.0;
+    for (int i = k + 1 + lane; i < n; i += 32)
+      s += lu[i + static_cast<long long>(ld) * k] * b[static_cast<long long>(inc) * i];
+    s = warp_sum_d(s);
+    if (lane == 0) b[static_cast<long long>(inc) * k] -= s;
+    __syncwarp();
+  }
+  if (lane == 0)
+    for (int i = n - 1; i >= 0; i--) {
+      const int p = ipiv[i];
+      if (p != i) {
+        const double t = b[static_cast<long long>(inc) * i];
+        b[static_cast<long long>(inc) * i] = b[static_cast<long long>(inc) * p];
+        b[static_cast<long long>(inc) * p] = t;
+      }
+    }
+  __syncwarp();
+}
+
+}  // namespace kib
+
+#endif  // KI_BLOCKLA_CUH_

@@ -1,0 +1,342 @@
+// C ABI of the B200 solver (declarations and reference citations in
+// include/kinterp.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/kinterp.h"
+#include "ki_solver.h"
+
+struct ki_solver_s {
+  std::unique_ptr<kib::Solver> solver;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* d_io = nullptr;  // staging for host-buffer calls
+  size_t io_bytes = 0;
+  bool tree_only = false;  // ki_partition handle: no factors on the device
+  ~ki_solver_s() {
+    solver.reset();
+    if (d_io) cudaFree(d_io);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+int from_solver(ki_solver_t s, int rc) {
+  if (rc == 0) return KI_OK;
+  return set_err(rc == -2 ? KI_ERR_CUDA : KI_ERR_NUMERIC, s->solver->error);
+}
+
+int staging(ki_solver_t s, size_t bytes) {
+  if (bytes <= s->io_bytes) return KI_OK;
+  if (s->d_io) cudaFree(s->d_io);
+  s->d_io = nullptr;
+  s->io_bytes = 0;
+  cudaError_t e = cudaMalloc(&s->d_io, bytes);
+  if (e != cudaSuccess) return set_err(KI_ERR_CUDA, cudaGetErrorString(e));
+  s->io_bytes = bytes;
+  return KI_OK;
+}
+
+int cuda_err(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return KI_OK;
+  return set_err(KI_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define KI_TRY(expr)               \
+  do {                             \
+    const int rc_ = (expr);        \
+    if (rc_ != KI_OK) return rc_;  \
+  } while (0)
+
+bool box_ref(ki_solver_t s, int level, int idx, const kib::Box** out, int* parent_idx) {
+  if (!s || !s->solver) return false;
+  const auto& lv = s->solver->tree.levels;
+  if (level < 0 || level >= static_cast<int>(lv.size())) return false;
+  if (idx < 0 || idx >= static_cast<int>(lv[level].size())) return false;
+  const int id = lv[level][idx];
+  *out = &s->solver->tree.boxes[id];
+  *parent_idx = -1;
+  const int par = (*out)->parent;
+  if (par >= 0) {
+    const auto& pl = lv[level - 1];
+    for (size_t i = 0; i < pl.size(); i++)
+      if (pl[i] == par) *parent_idx = static_cast<int>(i);
+  }
+  return true;
+}
+
+int factor_impl(int pde, int n_points, const double* points, const double* normals,
+                const double* curvatures, const double* weights, int n_holes,
+                const double* holes, int max_leaf_dofs, double id_tol, void* stream,
+                ki_solver_t* out, bool timed) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_factor: out is NULL");
+  *out = nullptr;
+  if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_factor: bad pde");
+  if (n_points <= 0 || !points || !normals || !curvatures || !weights)
+    return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+  if (n_holes < 0 || (n_holes > 0 && !holes)) return set_err(KI_ERR_ARG, "ki_factor: bad holes");
+  if (max_leaf_dofs < 1) return set_err(KI_ERR_ARG, "ki_factor: max_leaf_dofs must be >= 1");
+  if (!(id_tol > 0)) return set_err(KI_ERR_ARG, "id_tol must be greater than 0");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    return set_err(KI_ERR_CUDA, "no CUDA device available");
+  std::unique_ptr<ki_solver_s> h(new (std::nothrow) ki_solver_s());
+  if (!h) return set_err(KI_ERR_ARG, "out of host memory");
+  if (stream) {
+    h->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    KI_TRY(cuda_err(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking),
+                    "cudaStreamCreate"));
+    h->own_stream = true;
+  }
+  kib::SolverOptions opt;
+  opt.pde = pde;
+  opt.max_leaf_dofs = max_leaf_dofs;
+  opt.id_tol = id_tol;
+  h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, n_holes,
+                                  holes, h->stream));
+  h->solver->time_phases = timed;
+  const int rc = h->solver->factor();
+  if (rc) return from_solver(h.get(), rc);
+  *out = h.release();
+  return KI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ki_last_error(void) { return g_err.c_str(); }
+
+int ki_version(void) { return 100; }
+
+int ki_factor(int pde, int n_points, const double* points, const double* normals,
+              const double* curvatures, const double* weights, int n_holes,
+              const double* holes, int max_leaf_dofs, double id_tol, void* stream,
+              ki_solver_t* out) {
+  return factor_impl(pde, n_points, points, normals, curvatures, weights, n_holes, holes,
+                     max_leaf_dofs, id_tol, stream, out, false);
+}
+
+int ki_factor_timed(int pde, int n_points, const double* points, const double* normals,
+                    const double* curvatures, const double* weights, int n_holes,
+                    const double* holes, int max_leaf_dofs, double id_tol, void* stream,
+                    ki_solver_t* out) {
+  return factor_impl(pde, n_points, points, normals, curvatures, weights, n_holes, holes,
+                     max_leaf_dofs, id_tol, stream, out, true);
+}
+
+int ki_partition(int n_points, const double* points, int sol_dim, int max_leaf_dofs,
+                 ki_solver_t* out) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_partition: out is NULL");
+  *out = nullptr;
+  if (n_points <= 0 || !points)
+    return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+  if (sol_dim != 1 && sol_dim != 2) return set_err(KI_ERR_ARG, "ki_partition: sol_dim must be 1 or 2");
+  if (max_leaf_dofs < 1) return set_err(KI_ERR_ARG, "ki_partition: max_leaf_dofs must be >= 1");
+  std::unique_ptr<ki_solver_s> h(new (std::nothrow) ki_solver_s());
+  if (!h) return set_err(KI_ERR_ARG, "out of host memory");
+  kib::SolverOptions opt;
+  opt.pde = sol_dim == 2 ? KI_STOKES : KI_LAPLACE;
+  opt.max_leaf_dofs = max_leaf_dofs;
+  std::vector<double> zeros(2 * static_cast<size_t>(n_points), 0.0);
+  h->solver.reset(new kib::Solver(opt, n_points, points, zeros.data(), zeros.data(),
+                                  zeros.data(), 0, nullptr, nullptr));
+  h->solver->build_tree_only();
+  h->tree_only = true;
+  *out = h.release();
+  return KI_OK;
+}
+
+void ki_destroy(ki_solver_t s) { delete s; }
+
+int ki_num_dofs(ki_solver_t s) { return s && s->solver ? s->solver->n_dofs() : -KI_ERR_ARG; }
+
+int ki_num_border(ki_solver_t s) { return s && s->solver ? s->solver->n_border() : -KI_ERR_ARG; }
+
+int ki_solve_device(ki_solver_t s, const double* d_f, double* d_mu, double* d_alpha) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_f || !d_mu) return set_err(KI_ERR_ARG, "ki_solve_device: bad args");
+  if (s->solver->n_border() > 0 && !d_alpha)
+    return set_err(KI_ERR_ARG, "ki_solve_device: alpha required for a domain with holes");
+  return from_solver(s, s->solver->solve_device(d_f, d_mu, d_alpha));
+}
+
+int ki_solve(ki_solver_t s, const double* f, double* mu, double* alpha) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !f || !mu) return set_err(KI_ERR_ARG, "ki_solve: bad args");
+  const int N = s->solver->n_dofs(), nb = s->solver->n_border();
+  if (nb > 0 && !alpha) return set_err(KI_ERR_ARG, "ki_solve: alpha required for a domain with holes");
+  KI_TRY(staging(s, sizeof(double) * (N + nb + 1)));
+  double* d_x = s->d_io;
+  double* d_a = d_x + N;
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_x, f, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream),
+                  "copy f"));
+  KI_TRY(from_solver(s, s->solver->solve_device(d_x, d_x, nb ? d_a : nullptr)));
+  KI_TRY(cuda_err(cudaMemcpyAsync(mu, d_x, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream),
+                  "copy mu"));
+  if (nb > 0)
+    KI_TRY(cuda_err(cudaMemcpyAsync(alpha, d_a, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                    s->stream),
+                    "copy alpha"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_solve");
+}
+
+int ki_apply_device(ki_solver_t s, const double* d_x, double* d_y) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_x || !d_y) return set_err(KI_ERR_ARG, "ki_apply_device: bad args");
+  return from_solver(s, s->solver->apply_device(d_x, d_y));
+}
+
+int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets, const double* mu,
+                    const double* alpha, double* out) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || n_targets < 0 || (n_targets > 0 && (!targets || !out)) || !mu)
+    return set_err(KI_ERR_ARG, "ki_eval_targets: bad args");
+  if (n_targets == 0) return KI_OK;
+  kib::Solver& sv = *s->solver;
+  const int N = sv.n_dofs(), nb = sv.n_border(), sd = sv.sol_dim();
+  const bool use_alpha = nb > 0 && alpha;
+  const size_t need = static_cast<size_t>(N) + nb + 2 * static_cast<size_t>(n_targets) +
+                      static_cast<size_t>(sd) * n_targets;
+  KI_TRY(staging(s, sizeof(double) * need));
+  double* d_mu = s->d_io;
+  double* d_al = d_mu + N;
+  double* d_tg = d_al + nb;
+  double* d_out = d_tg + 2 * static_cast<size_t>(n_targets);
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_mu, mu, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream),
+                  "copy mu"));
+  if (use_alpha)
+    KI_TRY(cuda_err(cudaMemcpyAsync(d_al, alpha, sizeof(double) * nb, cudaMemcpyHostToDevice,
+                                    s->stream),
+                    "copy alpha"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_tg, targets, sizeof(double) * 2 * n_targets,
+                                  cudaMemcpyHostToDevice, s->stream),
+                  "copy targets"));
+  KI_TRY(cuda_err(kib::launch_eval_targets(sv.pde(), sv.d_nodes(), N, n_targets, d_tg, d_mu,
+                                           sv.n_holes(), sv.d_holes(),
+                                           use_alpha ? d_al : nullptr, d_out, s->stream),
+                  "eval targets"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(out, d_out, sizeof(double) * sd * n_targets,
+                                  cudaMemcpyDeviceToHost, s->stream),
+                  "copy out"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_eval_targets");
+}
+
+int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src, double* out) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || nt < 0 || ns < 0 || (nt * ns > 0 && (!tgt || !src || !out)))
+    return set_err(KI_ERR_ARG, "ki_kernel_block: bad args");
+  if (nt == 0 || ns == 0) return KI_OK;
+  const int N = s->solver->n_dofs();
+  for (int i = 0; i < nt; i++)
+    if (tgt[i] < 0 || tgt[i] >= N) return set_err(KI_ERR_ARG, "ki_kernel_block: tgt out of range");
+  for (int j = 0; j < ns; j++)
+    if (src[j] < 0 || src[j] >= N) return set_err(KI_ERR_ARG, "ki_kernel_block: src out of range");
+  const size_t ints = static_cast<size_t>(nt) + ns;
+  const size_t need = sizeof(double) * static_cast<size_t>(nt) * ns + sizeof(int) * ints + 64;
+  KI_TRY(staging(s, need));
+  double* d_out = s->d_io;
+  int* d_t = reinterpret_cast<int*>(d_out + static_cast<size_t>(nt) * ns);
+  int* d_s = d_t + nt;
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_t, tgt, sizeof(int) * nt, cudaMemcpyHostToDevice, s->stream), "copy"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_s, src, sizeof(int) * ns, cudaMemcpyHostToDevice, s->stream), "copy"));
+  KI_TRY(cuda_err(kib::launch_kernel_block(s->solver->pde(), s->solver->d_nodes(), d_t, nt, d_s, ns,
+                                           d_out, s->stream),
+                  "kernel block"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(out, d_out, sizeof(double) * nt * ns, cudaMemcpyDeviceToHost,
+                                  s->stream),
+                  "copy out"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_kernel_block");
+}
+
+int ki_num_levels(ki_solver_t s) {
+  if (!s || !s->solver) return -KI_ERR_ARG;
+  return static_cast<int>(s->solver->tree.levels.size());
+}
+
+int ki_num_boxes(ki_solver_t s, int level) {
+  if (!s || !s->solver || level < 0 ||
+      level >= static_cast<int>(s->solver->tree.levels.size()))
+    return -KI_ERR_ARG;
+  return static_cast<int>(s->solver->tree.levels[level].size());
+}
+
+int ki_box_info(ki_solver_t s, int level, int idx, int* info, double* geom) {
+  const kib::Box* b;
+  int par;
+  if (!box_ref(s, level, idx, &b, &par) || !info) return set_err(KI_ERR_ARG, "ki_box_info: bad box");
+  info[0] = b->leaf;
+  info[1] = b->compressed;
+  info[2] = static_cast<int>(b->original.size());
+  info[3] = static_cast<int>(b->active.size());
+  info[4] = static_cast<int>(b->skel.size());
+  info[5] = static_cast<int>(b->redundant.size());
+  info[6] = par;
+  info[7] = b->level;
+  if (geom) {
+    geom[0] = b->corner[0];
+    geom[1] = b->corner[1];
+    geom[2] = b->side;
+  }
+  return KI_OK;
+}
+
+int ki_box_lists(ki_solver_t s, int level, int idx, int* original, int* active, int* skel,
+                 int* redundant) {
+  const kib::Box* b;
+  int par;
+  if (!box_ref(s, level, idx, &b, &par)) return set_err(KI_ERR_ARG, "ki_box_lists: bad box");
+  auto cp = [](const std::vector<int>& v, int* o) {
+    if (o && !v.empty()) std::memcpy(o, v.data(), sizeof(int) * v.size());
+  };
+  cp(b->original, original);
+  cp(b->active, active);
+  cp(b->skel, skel);
+  cp(b->redundant, redundant);
+  return KI_OK;
+}
+
+int ki_allskel(ki_solver_t s, int* out) {
+  if (!s || !s->solver) return -KI_ERR_ARG;
+  const auto& v = s->solver->allskel;
+  if (out && !v.empty()) std::memcpy(out, v.data(), sizeof(int) * v.size());
+  return static_cast<int>(v.size());
+}
+
+int ki_launch_log(ki_solver_t s, double* out, int cap) {
+  if (!s || !s->solver) return -KI_ERR_ARG;
+  const auto& log = s->solver->launch_log;
+  for (int i = 0; out && i < cap && i < static_cast<int>(log.size()); i++) {
+    const auto& r = log[i];
+    const double row[7] = {double(r.level), double(r.kind), double(r.group), double(r.ntasks),
+                           double(r.m_cap), double(r.n_cap), r.ms};
+    std::memcpy(out + 7 * i, row, sizeof(row));
+  }
+  return static_cast<int>(log.size());
+}
+
+int ki_stats(ki_solver_t s, double* out, int n) {
+  if (!s || !s->solver || !out) return -KI_ERR_ARG;
+  const kib::Solver& v = *s->solver;
+  const double vals[] = {v.t_factor_ms, v.t_id_ms, static_cast<double>(v.id_launches),
+                         v.id_flops, v.id_bytes, v.t_decouple_ms, v.t_top_ms, v.t_wait_ms};
+  const int cnt = n < 8 ? n : 8;
+  for (int i = 0; i < cnt; i++) out[i] = vals[i];
+  return cnt;
+}
+
+}  // extern "C"

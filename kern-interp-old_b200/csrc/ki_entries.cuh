@@ -1,0 +1,165 @@
+// Boundary-integral matrix entries on the device.
+//
+// The double-layer entries of the reference Kernel (kern_interp/kernel/
+// kernel.cpp): Laplace (kernel.cpp:11-36, 114-150), Laplace-Neumann
+// (kernel.cpp:23-33) and the Stokes 2x2 blocks with the rank-one completion
+// (kernel.cpp:47-96), plus the proxy-circle rows used by the interpolative
+// decomposition (kernel.cpp:238-334).  Every product and sum is issued with
+// an explicit round-to-nearest intrinsic in the reference's C evaluation
+// order, so no FMA contraction happens and an entry equals the reference's
+// double-precision value bit for bit (the reference is built without FMA).
+#ifndef KI_ENTRIES_CUH_
+#define KI_ENTRIES_CUH_
+
+#include <cuda_runtime.h>
+
+namespace kib {
+
+enum Pde : int { kLaplace = 0, kLaplaceNeumann = 1, kStokes = 2 };
+
+// One boundary node: position, unit normal, quadrature weight, curvature.
+struct __align__(16) Node {
+  double x, y, nx, ny, w, k, pad0, pad1;
+};
+
+constexpr int kNumProxy = 128;        // kernel.h:10
+constexpr double kRadiusRatio = 1.5;  // kernel.h:11
+
+// Proxy directions cos/sin(2 pi q / 128) are evaluated by the host's libm
+// (so the proxy points match the reference's, kernel.cpp:244-251) and passed
+// to the kernels as a 256-entry table: cos in [0, 128), sin in [128, 256).
+
+#define KI_INV_2PI (1.0 / (2 * 3.14159265358979323846))
+#define KI_INV_PI (1.0 / (3.14159265358979323846))
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double subd(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double divd(double a, double b) { return __ddiv_rn(a, b); }
+
+// Kernel::laplace for r = t - s (not the forward/target variant).
+__device__ __forceinline__ double laplace_entry(int pde, double r1, double r2,
+                                                double sw, double sc,
+                                                double sn1, double sn2,
+                                                double tn1, double tn2) {
+  const double rr = add(mul(r1, r1), mul(r2, r2));
+  if (pde == kLaplace) {
+    if (r1 == 0. && r2 == 0.) return add(0.5, mul(mul(mul(0.5, sc), sw), KI_INV_2PI));
+    return divd(mul(mul(-sw, KI_INV_2PI), add(mul(r1, sn1), mul(r2, sn2))), rr);
+  }
+  if (r1 == 0. && r2 == 0.)
+    return add(subd(sw, 0.5), mul(mul(mul(0.5, sc), sw), KI_INV_2PI));
+  return add(sw, divd(mul(mul(sw, KI_INV_2PI), add(mul(r1, tn1), mul(r2, tn2))), rr));
+}
+
+// Boundary operator entry (tgt dof, src dof).  For Stokes a dof is
+// 2*node + component.
+__device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict__ nodes,
+                                                 int tgt, int src) {
+  if (pde != kStokes) {
+    const Node s = nodes[src];
+    const Node t = nodes[tgt];
+    return laplace_entry(pde, subd(t.x, s.x), subd(t.y, s.y), s.w, s.k, s.nx, s.ny,
+                         t.nx, t.ny);
+  }
+  const Node s = nodes[src >> 1];
+  const Node t = nodes[tgt >> 1];
+  const int tc = tgt & 1, sc = src & 1;
+  const double sn_s = sc ? s.ny : s.nx;   // sn[src % 2]
+  const double tn_t = tc ? t.ny : t.nx;   // tn[tgt % 2]
+  if (t.x == s.x && t.y == s.y) {
+    // kernel.cpp:80-85: -1/2 delta - (kappa w / 2 pi) t t^T + w n n^T
+    const int parity = (tgt + src + 1) & 1;
+    const double snA = tc ? s.nx : s.ny;  // sn[(tgt + 1) % 2]
+    const double snB = sc ? s.nx : s.ny;  // sn[(src + 1) % 2]
+    const double a = mul(-0.5, static_cast<double>(parity));
+    const double b = mul(mul(mul(mul(mul(static_cast<double>(1 - 2 * parity), 0.5), s.k), s.w),
+                             KI_INV_PI), snA);
+    return add(add(a, mul(b, snB)), mul(mul(s.w, tn_t), sn_s));
+  }
+  const double r0 = subd(t.x, s.x), r1 = subd(t.y, s.y);
+  const double rr = add(mul(r0, r0), mul(r1, r1));
+  const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
+                          mul(rr, rr));
+  const double rt = tc ? r1 : r0, rs = sc ? r1 : r0;
+  return add(mul(mul(pot, rt), rs), mul(mul(s.w, tn_t), sn_s));
+}
+
+// Proxy-block row `row` (0 <= row < 2*128 for Laplace, 4*128 for Stokes) for
+// box column dof `src` (kernel.cpp:268-334); circle centre (cx, cy), radius r.
+__device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ nodes,
+                                              const double* __restrict__ dir,
+                                              int row, int src, double cx, double cy,
+                                              double r, double pw) {
+  const double* c_proxy_cos = dir;
+  const double* c_proxy_sin = dir + kNumProxy;
+  if (pde != kStokes) {
+    const Node b = nodes[src];
+    const int q = row & (kNumProxy - 1);
+    const double px = add(cx, mul(r, c_proxy_cos[q]));
+    const double py = add(cy, mul(r, c_proxy_sin[q]));
+    const double r0 = subd(px, b.x), r1 = subd(py, b.y);
+    if (row < kNumProxy)
+      return laplace_entry(pde, r0, r1, b.w, 0.0, b.nx, b.ny, c_proxy_cos[q], c_proxy_sin[q]);
+    return laplace_entry(pde, -r0, -r1, pw, 0.0, c_proxy_cos[q], c_proxy_sin[q], b.nx, b.ny);
+  }
+  const Node s = nodes[src >> 1];
+  const int scomp = src & 1;
+  const bool second = row >= 2 * kNumProxy;
+  const int rr_ = second ? row - 2 * kNumProxy : row;
+  const int q = rr_ >> 1, comp = rr_ & 1;
+  const double tn0 = c_proxy_cos[q], tn1 = c_proxy_sin[q];
+  const double px = add(cx, mul(r, tn0));
+  const double py = add(cy, mul(r, tn1));
+  const double r0 = subd(px, s.x), r1 = subd(py, s.y);
+  const double rr = add(mul(r0, r0), mul(r1, r1));
+  const double rs = scomp ? r1 : r0;
+  const double rc = comp ? r1 : r0;
+  const double sns = scomp ? s.ny : s.nx;
+  const double tnc = comp ? tn1 : tn0;
+  if (!second) {
+    const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
+                            mul(rr, rr));
+    return add(mul(mul(pot, rc), rs), mul(mul(s.w, tnc), sns));
+  }
+  const double pot = divd(mul(mul(-pw, KI_INV_PI), add(mul(r0, tn0), mul(r1, tn1))),
+                          mul(rr, rr));
+  return add(mul(mul(pot, rc), rs), mul(mul(pw, sns), tnc));
+}
+
+// Forward (target-point) entry of Kernel::forward (kernel.cpp:337-357) with
+// target normal zero; tgt_comp is the velocity component for Stokes.
+__device__ __forceinline__ double forward_entry(int pde, const Node* __restrict__ nodes,
+                                                double tx, double ty, int tgt_comp,
+                                                int src) {
+  if (pde == kLaplace) {
+    const Node s = nodes[src];
+    return laplace_entry(kLaplace, subd(tx, s.x), subd(ty, s.y), s.w, s.k, s.nx, s.ny,
+                         0.0, 0.0);
+  }
+  if (pde == kLaplaceNeumann) {
+    const Node s = nodes[src];
+    const double r1 = subd(tx, s.x), r2 = subd(ty, s.y);
+    return mul(mul(s.w, KI_INV_2PI), log(sqrt(add(mul(r1, r1), mul(r2, r2)))));
+  }
+  const Node s = nodes[src >> 1];
+  const int sc = src & 1;
+  const double r0 = subd(tx, s.x), r1 = subd(ty, s.y);
+  if (r0 == 0.0 && r1 == 0.0) {
+    // target on a node: the diagonal formula with zero target normal
+    const int parity = (tgt_comp + src + 1) & 1;
+    const double snA = tgt_comp ? s.nx : s.ny;
+    const double snB = sc ? s.nx : s.ny;
+    const double b = mul(mul(mul(mul(mul(static_cast<double>(1 - 2 * parity), 0.5), s.k), s.w),
+                             KI_INV_PI), snA);
+    return add(mul(-0.5, static_cast<double>(parity)), mul(b, snB));
+  }
+  const double rr = add(mul(r0, r0), mul(r1, r1));
+  const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
+                          mul(rr, rr));
+  return mul(mul(pot, tgt_comp ? r1 : r0), sc ? r1 : r0);
+}
+
+}  // namespace kib
+
+#endif  // KI_ENTRIES_CUH_

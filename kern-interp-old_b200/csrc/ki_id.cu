@@ -1,0 +1,377 @@
+// Interpolative decomposition of every box of one quadtree level in one
+// launch: fused ID-matrix generation, column-pivoted Householder QR with the
+// reference's rank rule, and T = R11^{-1} R12.
+//
+// Reference semantics (paths relative to the reference repository):
+//   * ID matrix rows: Kernel::get_id_mat, kernel.cpp:153-235 (proxy circle
+//     of radius 1.5 side with 128 points; levels 1-2 use all other boxes).
+//   * Pivoting and Householder steps: LAPACK dgeqp3/dlaqp2 as called by
+//     ki_Mat::id (ki_mat.cpp:502-541): first-maximum column pivot on the
+//     partial column norms, dlarfg reflector (beta = -sign(alpha) |x|), the
+//     norm downdate with recomputation when it loses accuracy (tol3z).
+//   * Rank: first i >= 1 with |R_ii| < tol |R_00|; none => 0 (no compression).
+//   * T = R11^{-1} R12 by column back substitution (dtrtrs).
+// The factorization stops at the rank: R_ii never changes after step i and
+// T only needs R's first k rows, so steps k..n-1 of dgeqp3 are skipped.  The
+// skeleton (pivots 0..k-1, in order) is unchanged by this; the redundant
+// columns come out in their order at step k instead of dgeqp3's later pivot
+// order, which only permutes the redundant set inside the box.
+//
+// B200 layout: one box is owned by a cluster of G CTAs (G = 1 for the many
+// small boxes of deep levels, up to 8 for the few tall boxes near the root).
+// Columns are dealt round-robin to the CTAs (physical column j belongs to
+// CTA j % G), the matrix lives in HBM/L2 in column-major order, each warp
+// streams whole columns, and one cluster barrier per pivot step publishes
+// the updated columns and each CTA's best pivot candidate through
+// distributed shared memory.  Every CTA recomputes the Householder vector of
+// the pivot column itself, so no extra broadcast barrier is needed.
+#include <cooperative_groups.h>
+
+#include "ki_kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace kib {
+
+namespace {
+
+constexpr int kIdThreads = 256;
+constexpr int kIdWarps = kIdThreads / 32;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum; `red` holds kIdWarps doubles.  Ends with a barrier so
+// `red` may be reused immediately.
+__device__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = lane < kIdWarps ? red[lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) red[0] = t;
+  }
+  __syncthreads();
+  t = red[0];
+  __syncthreads();
+  return t;
+}
+
+struct Cand {
+  double val;
+  int pos;
+  int pad;
+};
+
+// Lexicographic pivot order: larger norm first, then smaller position.
+__device__ __forceinline__ bool better(double v, int p, double bv, int bp) {
+  return v > bv || (v == bv && p < bp);
+}
+
+__device__ __forceinline__ void warp_best(double& v, int& p) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    const int op = __shfl_xor_sync(0xffffffffu, p, o);
+    if (better(ov, op, v, p)) {
+      v = ov;
+      p = op;
+    }
+  }
+}
+
+__device__ __forceinline__ double lapy2(double x, double y) {
+  const double xa = fabs(x), ya = fabs(y);
+  const double w = fmax(xa, ya), z = fmin(xa, ya);
+  if (z == 0.0) return w;
+  const double q = z / w;
+  return w * sqrt(1.0 + q * q);
+}
+
+template <int G>
+__global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int task = blockIdx.x / G;
+  int g = 0;
+  if constexpr (G > 1) g = static_cast<int>(cg::this_cluster().block_rank());
+  const IdTask tk = P.tasks[task];
+  const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  double* v = reinterpret_cast<double*>(smem_raw);   // m_cap
+  double* rdiag = v + P.m_cap;                        // n_cap
+  double* vn1 = rdiag + P.n_cap;                      // n_cap
+  double* vn2 = vn1 + P.n_cap;                        // n_cap
+  double* red = vn2 + P.n_cap;                        // 32
+  double* sc = red + 32;                              // scalars
+  Cand* slot = reinterpret_cast<Cand*>(sc + 8);       // 2
+  int* pos2col = reinterpret_cast<int*>(slot + 2);    // n_cap
+  int* own = pos2col + P.n_cap;                       // n_cap
+  int* si = own + P.n_cap;                            // int scalars
+
+  double* A = P.work + tk.a_off;
+  const int* act = P.act + tk.act_off;
+  const int* rowd = P.rowdofs + tk.row_off;
+  const Node* nodes = P.nodes;
+  const int pde = P.pde;
+
+  // ---- generation of the owned columns + their initial norms
+  for (int t = warp; g + G * t < n; t += kIdWarps) {
+    const int j = g + G * t;
+    const int cd = act[j];
+    double* col = A + static_cast<long long>(j) * lda;
+    double ss = 0.0;
+    for (int r = lane; r < m; r += 32) {
+      double val;
+      if (r < I) {
+        val = boundary_entry(pde, nodes, rowd[r], cd);
+      } else if (r < 2 * I) {
+        val = boundary_entry(pde, nodes, cd, rowd[r - I]);
+      } else {
+        val = proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
+      }
+      col[r] = val;
+      ss += val * val;
+    }
+    ss = warp_sum(ss);
+    if (lane == 0) {
+      vn1[j] = sqrt(ss);
+      vn2[j] = vn1[j];
+    }
+  }
+  for (int p = threadIdx.x; p < n; p += kIdThreads) pos2col[p] = p;
+  __syncthreads();
+  if (warp == 0) {
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int p = lane; p < n; p += 32) {
+      if (p % G == g && better(vn1[p], p, bv, bp)) {
+        bv = vn1[p];
+        bp = p;
+      }
+    }
+    warp_best(bv, bp);
+    if (lane == 0) slot[0] = Cand{bv, bp, 0};
+  }
+  if constexpr (G > 1) {
+    cg::this_cluster().sync();
+  } else {
+    __syncthreads();
+  }
+
+  const double tol3z = sqrt(0.5 * 2.220446049250313e-16);
+  const int mn = min(m, n);
+  int rank = 0;
+  double thresh = 0.0;
+  for (int i = 0; i < mn; i++) {
+    // ---- pivot: best candidate over the cluster
+    if (warp == 0) {
+      double bv = -1.0;
+      int bp = 0x7fffffff;
+      if (lane < G) {
+        Cand c;
+        if constexpr (G > 1) {
+          Cand* peer = cg::this_cluster().map_shared_rank(slot, lane);
+          c = peer[i & 1];
+        } else {
+          c = slot[i & 1];
+        }
+        bv = c.val;
+        bp = c.pos;
+      }
+      warp_best(bv, bp);
+      if (lane == 0) {
+        const int pvt = bp;
+        const int tmp = pos2col[i];
+        pos2col[i] = pos2col[pvt];
+        pos2col[pvt] = tmp;
+      }
+    }
+    __syncthreads();
+    const int c = pos2col[i];
+    const double* colc = A + static_cast<long long>(c) * lda;
+    // ---- Householder reflector of the pivot column (redundantly per CTA)
+    double part = 0.0;
+    for (int r = i + 1 + threadIdx.x; r < m; r += kIdThreads) {
+      const double a = colc[r];
+      part += a * a;
+    }
+    const double xnorm = sqrt(block_sum(part, red));
+    if (threadIdx.x == 0) {
+      const double alpha = colc[i];
+      double beta = alpha, tau = 0.0, scal = 0.0;
+      if (i < m - 1 && xnorm != 0.0) {
+        beta = -copysign(lapy2(alpha, xnorm), alpha);
+        tau = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      rdiag[i] = beta;
+      sc[0] = tau;
+      sc[1] = scal;
+      if (i == 0) sc[2] = fabs(P.tol * beta);
+    }
+    __syncthreads();
+    const double tau = sc[0], scal = sc[1];
+    thresh = sc[2];
+    if (i >= 1 && fabs(rdiag[i]) < thresh) {
+      rank = i;
+      break;
+    }
+    for (int r = i + 1 + threadIdx.x; r < m; r += kIdThreads) v[r] = colc[r] * scal;
+    if (threadIdx.x == 0) v[i] = 1.0;
+    // ---- compact list of this CTA's trailing columns (positions > i)
+    if (warp == 0) {
+      int cnt = 0;
+      for (int base = i + 1; base < n; base += 32) {
+        const int p = base + lane;
+        const bool mine = p < n && (pos2col[p] % G == g);
+        const unsigned bal = __ballot_sync(0xffffffffu, mine);
+        if (mine) own[cnt + __popc(bal & ((1u << lane) - 1u))] = p;
+        cnt += __popc(bal);
+      }
+      if (lane == 0) si[0] = cnt;
+    }
+    __syncthreads();
+    const int nown = si[0];
+    // ---- apply H to the owned trailing columns, downdate their norms
+    for (int t = warp; t < nown; t += kIdWarps) {
+      const int j = pos2col[own[t]];
+      double* col = A + static_cast<long long>(j) * lda;
+      if (tau != 0.0) {
+        double w = 0.0;
+        for (int r = i + lane; r < m; r += 32) w += v[r] * col[r];
+        w = warp_sum(w);
+        const double tw = -tau * w;
+        for (int r = i + lane; r < m; r += 32) col[r] += v[r] * tw;
+      }
+      __syncwarp();
+      const double aij = col[i];
+      double nv1 = vn1[j];
+      const double nv2 = vn2[j];
+      bool recompute = false;
+      if (nv1 != 0.0) {
+        double temp = fabs(aij) / nv1;
+        temp = fmax(1.0 - temp * temp, 0.0);
+        const double q = nv1 / nv2;
+        const double temp2 = temp * (q * q);
+        if (temp2 <= tol3z) {
+          recompute = true;
+        } else {
+          nv1 *= sqrt(temp);
+        }
+      }
+      if (recompute) {
+        double ss = 0.0;
+        for (int r = i + 1 + lane; r < m; r += 32) ss += col[r] * col[r];
+        ss = warp_sum(ss);
+        nv1 = (i < m - 1) ? sqrt(ss) : 0.0;
+        if (lane == 0) vn2[j] = nv1;
+      }
+      if (lane == 0) vn1[j] = nv1;
+    }
+    __syncthreads();
+    // ---- this CTA's best candidate for step i + 1
+    if (warp == 0) {
+      double bv = -1.0;
+      int bp = 0x7fffffff;
+      for (int t = lane; t < nown; t += 32) {
+        const int p = own[t];
+        const double val = vn1[pos2col[p]];
+        if (better(val, p, bv, bp)) {
+          bv = val;
+          bp = p;
+        }
+      }
+      warp_best(bv, bp);
+      if (lane == 0) slot[(i + 1) & 1] = Cand{bv, bp, 0};
+    }
+    if constexpr (G > 1) {
+      cg::this_cluster().sync();
+    } else {
+      __syncthreads();
+    }
+  }
+
+  // No CTA may leave while a peer can still read its pivot slot.
+  if constexpr (G > 1) cg::this_cluster().sync();
+
+  // ---- outputs: rank, pivots, T = R11^{-1} R12 for the owned columns
+  if (g == 0) {
+    if (threadIdx.x == 0) P.rank[task] = rank;
+    for (int p = threadIdx.x; p < n; p += kIdThreads) P.perm[tk.perm_off + p] = pos2col[p];
+  }
+  if (rank == 0) return;
+  const int k = rank;
+  double* T = P.tout + tk.t_off;
+  for (int p = k + warp; p < n; p += kIdWarps) {
+    const int j = pos2col[p];
+    if (j % G != g) continue;
+    const double* col = A + static_cast<long long>(j) * lda;
+    double* tc = T + static_cast<long long>(p - k) * k;
+    for (int l = lane; l < k; l += 32) tc[l] = col[l];
+    __syncwarp();
+    for (int q = k - 1; q >= 0; q--) {
+      const double bq = tc[q];
+      __syncwarp();
+      if (bq != 0.0) {
+        const double xq = bq / rdiag[q];
+        const double* rq = A + static_cast<long long>(pos2col[q]) * lda;
+        if (lane == 0) tc[q] = xq;
+        for (int l = lane; l < q; l += 32) tc[l] -= xq * rq[l];
+      }
+      __syncwarp();
+    }
+  }
+}
+
+template <int G>
+cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
+  const size_t smem = id_smem_bytes(p.m_cap, p.n_cap);
+  cudaError_t e = cudaFuncSetAttribute(id_kernel<G>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G * p.ntasks);
+  cfg.blockDim = dim3(kIdThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  int na = 0;
+  if (G > 1) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    na = 1;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  return cudaLaunchKernelEx(&cfg, id_kernel<G>, p);
+}
+
+}  // namespace
+
+size_t id_smem_bytes(int m_cap, int n_cap) {
+  return sizeof(double) * (static_cast<size_t>(m_cap) + 3 * n_cap + 32 + 8) +
+         sizeof(Cand) * 2 + sizeof(int) * (2 * static_cast<size_t>(n_cap) + 8);
+}
+
+cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s) {
+  if (p.ntasks == 0) return cudaSuccess;
+  switch (group) {
+    case 1: return launch_g<1>(p, s);
+    case 2: return launch_g<2>(p, s);
+    case 4: return launch_g<4>(p, s);
+    case 8: return launch_g<8>(p, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace kib

@@ -1,0 +1,166 @@
+// Device work descriptors and kernel launchers of the B200 solver.
+#ifndef KI_KERNELS_H_
+#define KI_KERNELS_H_
+
+#include <cuda_runtime.h>
+
+#include "ki_entries.cuh"
+
+namespace kib {
+
+// ---------------------------------------------------------------- ID
+// One interpolative decomposition (Kernel::get_id_mat + ki_Mat::id,
+// kernel.cpp:153-235, ki_mat.cpp:502-541).  Rows of the ID matrix:
+//   [0, I)      K(rowdof[r], act[j])          near/outside dofs as targets
+//   [I, 2I)     K(act[j], rowdof[r - I])      the transposed block
+//   [2I, m)     proxy rows (proxy = 256 Laplace / 512 Stokes, 0 on levels 1-2)
+struct IdTask {
+  int n;          // active dofs (columns)
+  int m;          // rows = 2 I + proxy
+  int n_row;      // I
+  int proxy;      // proxy rows
+  int act_off;    // into IdParams::act
+  int row_off;    // into IdParams::rowdofs
+  int lda;        // leading dimension of A in the workspace
+  int perm_off;   // into IdParams::perm (n ints)
+  long long a_off;  // A in the workspace (doubles)
+  long long t_off;  // T output (doubles), capacity n*n/4 + 1
+  double cx, cy, rad, pw;  // proxy circle centre, radius, weight
+};
+
+struct IdParams {
+  const IdTask* tasks;
+  int ntasks;
+  int pde;
+  const Node* nodes;
+  const int* act;
+  const int* rowdofs;
+  double* work;
+  double* tout;
+  int* perm;
+  int* rank;
+  const double* proxy_dir;  // cos/sin table, 2 * kNumProxy doubles
+  double tol;
+  int m_cap, n_cap;  // maxima over the launch (shared-memory layout)
+};
+
+// Launches one ID per task with `group` CTAs (a cluster) per task.
+cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s);
+size_t id_smem_bytes(int m_cap, int n_cap);
+
+// ---------------------------------------------------------------- decouple
+// Assembly + decouple of one compressed box (skel_factorization.cpp:55-91).
+// The box's K_BN = K(act, act) - (children's accumulated Schur updates) is
+// formed in pivot order [skel; redundant]; update blocks are addressed per
+// active position: upd(a, b) = blocks[bid[a]] (bpos[a], bpos[b]) when
+// bid[a] == bid[b] >= 0.
+struct UpdBlock {
+  const double* acc;  // accumulated update matrix, size x size, ld size
+  int size;
+  int pad;
+};
+
+struct DecTask {
+  int n, k;              // active, skeleton count (r = n - k)
+  const int* act;        // n active dofs, active order
+  const int* perm;       // ID pivots: column p of the ID is active[perm[p]]
+  const int* bid;        // per active position: update block id or -1
+  const int* bpos;       // per active position: row inside that block
+  const UpdBlock* blocks;
+  const double* T;       // k x r, ld k (from the ID)
+  double* K;             // scratch n x n
+  double* Krs;           // scratch r x k (K_r_sn)
+  double* L;             // k x r, ld k
+  double* U;             // r x k, ld r
+  double* X;             // LU of X_rr, r x r, ld r
+  double* acc;           // accumulated update on the skeleton, k x k
+  int* piv;              // X_rr pivots (r)
+};
+
+struct DecParams {
+  const DecTask* tasks;
+  int ntasks;
+  int pde;
+  const Node* nodes;
+  int* status;  // set nonzero on an exactly zero pivot
+};
+
+cudaError_t launch_decouple(const DecParams& p, cudaStream_t s);
+
+// Dense assembly of the top-level skeleton matrix K(allskel, allskel) minus
+// the accumulated updates (skel_factorization.cpp:116-122), n x n, ld ld.
+cudaError_t launch_assemble_top(int pde, const Node* nodes, const int* dofs, int n,
+                                const int* bid, const int* bpos, const UpdBlock* blocks,
+                                double* out, int ld, cudaStream_t s);
+
+// ---------------------------------------------------------------- dense LU
+// In-place LU with partial pivoting of an n x n matrix (ld), pivots 0-based
+// row indices as LAPACK's (ipiv[j] = row swapped with j).
+cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s);
+// B <- A^{-1} B (n x nrhs, ldb) for the LU above.
+cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
+                           int nrhs, int ldb, cudaStream_t s);
+
+// Border blocks of the bordered top-level system S (ld >= ns + nb).
+cudaError_t launch_fill_border(double* S, int ld, int ns, int nb, const double* us,
+                               const double* ps, const double* corr, cudaStream_t s);
+
+// ---------------------------------------------------------------- sweeps
+// Per-box sweep descriptors for SkelFactorization::solve
+// (skel_factorization.cpp:341-403) and the multiply-connected variant.
+struct SweepTask {
+  int k, r;
+  const int* skel;   // k dofs
+  const int* red;    // r dofs
+  const double* T;   // k x r
+  const double* L;   // k x r
+  const double* U;   // r x k
+  const double* X;   // LU of X_rr
+  const int* piv;
+};
+
+struct SweepParams {
+  const SweepTask* tasks;
+  int ntasks;
+  double* x;
+  int ldx, nrhs;
+  int red_pos_map;      // nonzero: redundant dofs index rows of x via red_pos
+  const int* red_pos;
+  int cap;              // per-box staging: max over tasks of k + r
+};
+
+// x[red] -= T^T x[skel]; then x[skel] -= L x[red]   (or U^T when use_u)
+cudaError_t launch_sweep_up(const SweepParams& p, bool use_u, cudaStream_t s);
+// x[red] -= U x[skel]; then x[skel] -= T x[red]
+cudaError_t launch_sweep_down(const SweepParams& p, cudaStream_t s);
+// x[red] = X_rr^{-1} x[red]
+cudaError_t launch_diag_solve(const SweepParams& p, cudaStream_t s);
+
+// ---------------------------------------------------------------- misc
+// out[i] = x[idx[i]] (gather) / x[idx[i]] = in[i] (scatter), nrhs columns.
+cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int nrhs,
+                          double* out, int ldo, cudaStream_t s);
+cudaError_t launch_scatter(double* x, int ldx, const int* idx, int n, int nrhs,
+                           const double* in, int ldi, cudaStream_t s);
+// C = alpha * op(A) * op(B) + beta * C, small dense FP64 (column-major).
+cudaError_t small_gemm(bool ta, bool tb, int m, int n, int k, double alpha,
+                       const double* a, int lda, const double* b, int ldb, double beta,
+                       double* c, int ldc, cudaStream_t s);
+
+// y = K x for the full boundary operator (on-the-fly entries), plus the
+// hole border terms when U/Psi are given (nb border columns).
+cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const double* x,
+                                  double* y, int nb, const double* U, const double* Psi,
+                                  cudaStream_t s);
+// Target evaluation out = K_fwd(targets) mu (+ U_fwd alpha).
+cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
+                                const double* targets, const double* mu, int nh,
+                                const double* holes, const double* alpha, double* out,
+                                cudaStream_t s);
+// Dense kernel block K(tgt, src), column-major nt x ns.
+cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
+                                const int* src, int ns, double* out, cudaStream_t s);
+
+}  // namespace kib
+
+#endif  // KI_KERNELS_H_

@@ -1,0 +1,818 @@
+// Host orchestration of the B200 recursive-skeletonization solver.
+//
+// factor() follows SkelFactorization::skeletonize (skel_factorization.cpp:
+// 94-243) level by level from the leaves up: the host refreshes the active
+// and near dof lists of the level (quadtree.cpp:656-720) and builds one
+// device work descriptor per box, then one launch runs every box's
+// interpolative decomposition and one launch decouples every compressed box.
+// The ranks and pivots come back to the host (a few KB per level) because
+// the next level's active lists are made of this level's skeletons.  The top
+// skeleton matrix (or, with holes, the bordered system S of
+// skel_factorization.cpp:130-242) is assembled and LU-factored on the GPU.
+// solve_device() runs the level sweeps of SkelFactorization::solve and
+// multiply_connected_solve (skel_factorization.cpp:341-551) on the GPU.
+#include "ki_solver.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+namespace kib {
+
+// ------------------------------------------------------------------ memory
+Arena::~Arena() {
+  for (void* c : chunks_) cudaFree(c);
+}
+
+void* Arena::alloc(size_t bytes) {
+  bytes = (bytes + 255) & ~static_cast<size_t>(255);
+  if (bytes > left_) {
+    const size_t sz = std::max(bytes, static_cast<size_t>(64) << 20);
+    void* p = nullptr;
+    if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
+    chunks_.push_back(p);
+    cur_ = static_cast<char*>(p);
+    left_ = sz;
+    reserved_ += sz;
+  }
+  void* r = cur_;
+  cur_ += bytes;
+  left_ -= bytes;
+  return r;
+}
+
+Scratch::~Scratch() {
+  if (p) cudaFree(p);
+}
+
+cudaError_t Scratch::reserve(size_t want, cudaStream_t s) {
+  if (want <= bytes) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+  const size_t sz = want + want / 4 + 4096;
+  e = cudaMalloc(&p, sz);
+  if (e == cudaSuccess) bytes = sz;
+  return e;
+}
+
+namespace {
+
+template <class T>
+cudaError_t upload(T* dst, const std::vector<T>& src, cudaStream_t s) {
+  if (src.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, s);
+}
+
+// initialize_U_mat (linear_solve.cpp:18-64) for boundary points.
+void border_U(int pde, const std::vector<double>& pts, const std::vector<double>& holes,
+              std::vector<double>* U, int* cols) {
+  const int nh = static_cast<int>(holes.size() / 4);
+  const int np = static_cast<int>(pts.size() / 2);
+  if (pde == kLaplace) {
+    *cols = nh;
+    U->assign(static_cast<size_t>(np) * nh, 0.0);
+    for (int i = 0; i < np; i++)
+      for (int h = 0; h < nh; h++) {
+        const double rx = pts[2 * i] - holes[4 * h], ry = pts[2 * i + 1] - holes[4 * h + 1];
+        (*U)[i + static_cast<size_t>(np) * h] = std::log(std::sqrt(rx * rx + ry * ry));
+      }
+    return;
+  }
+  *cols = 3 * nh;
+  const int N = 2 * np;
+  U->assign(static_cast<size_t>(N) * 3 * nh, 0.0);
+  auto at = [&](int i, int j) -> double& { return (*U)[i + static_cast<size_t>(N) * j]; };
+  for (int q = 0; q < np; q++)
+    for (int h = 0; h < nh; h++) {
+      const int i = 2 * q;
+      const double r0 = pts[i] - holes[4 * h], r1 = pts[i + 1] - holes[4 * h + 1];
+      const double rn = std::sqrt(r0 * r0 + r1 * r1);
+      const double scale = 1.0 / (4 * M_PI);
+      at(i, 3 * h) = scale * (std::log(1 / rn) + (1.0 / std::pow(rn, 2)) * r0 * r0);
+      at(i + 1, 3 * h) = scale * ((1.0 / std::pow(rn, 2)) * r1 * r0);
+      at(i, 3 * h + 1) = scale * ((1.0 / std::pow(rn, 2)) * r0 * r1);
+      at(i + 1, 3 * h + 1) = scale * (std::log(1 / rn) + (1.0 / std::pow(rn, 2)) * r1 * r1);
+      at(i, 3 * h + 2) = r1 * (scale / std::pow(rn, 2));
+      at(i + 1, 3 * h + 2) = -r0 * (scale / std::pow(rn, 2));
+    }
+}
+
+// initialize_Psi_mat (linear_solve.cpp:67-110), stored column-major rows x N.
+void border_Psi(int pde, const std::vector<double>& pts, const std::vector<double>& w,
+                const std::vector<double>& holes, std::vector<double>* Psi) {
+  const int nh = static_cast<int>(holes.size() / 4);
+  const int np = static_cast<int>(pts.size() / 2);
+  const int rows = pde == kLaplace ? nh : 3 * nh;
+  const int N = pde == kLaplace ? np : 2 * np;
+  Psi->assign(static_cast<size_t>(rows) * N, 0.0);
+  auto at = [&](int i, int j) -> double& { return (*Psi)[i + static_cast<size_t>(rows) * j]; };
+  for (int q = 0; q < np; q++) {
+    const double x0 = pts[2 * q], x1 = pts[2 * q + 1];
+    for (int h = 0; h < nh; h++) {
+      const double rx = x0 - holes[4 * h], ry = x1 - holes[4 * h + 1];
+      if (std::sqrt(rx * rx + ry * ry) < holes[4 * h + 2] + 1e-8) {
+        if (pde == kLaplace) {
+          at(h, q) = w[q];
+        } else {
+          at(3 * h, 2 * q) = w[q];
+          at(3 * h + 1, 2 * q + 1) = w[q];
+          at(3 * h + 2, 2 * q) = w[q] * x1;
+          at(3 * h + 2, 2 * q + 1) = -w[q] * x0;
+        }
+        break;
+      }
+    }
+  }
+}
+
+int pick_group(long long m, long long n) {
+  const long long e = m * n;
+  if (e > 400000) return 8;
+  if (e > 160000) return 4;
+  if (e > 90000) return 2;
+  return 1;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ solver
+Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
+               const double* normals, const double* curvatures, const double* weights,
+               int n_holes, const double* holes, cudaStream_t stream)
+    : opt_(opt), stream_(stream) {
+  sd_ = opt.pde == kStokes ? 2 : 1;
+  n_points_ = n_points;
+  n_dofs_ = n_points * sd_;
+  pts_.assign(points, points + 2 * static_cast<size_t>(n_points));
+  nrm_.assign(normals, normals + 2 * static_cast<size_t>(n_points));
+  curv_.assign(curvatures, curvatures + n_points);
+  wts_.assign(weights, weights + n_points);
+  if (n_holes > 0) holes_.assign(holes, holes + 4 * static_cast<size_t>(n_holes));
+}
+
+Solver::~Solver() = default;
+
+int Solver::fail(const std::string& msg) {
+  error = msg;
+  return -1;
+}
+
+int Solver::cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return 0;
+  error = std::string(what) + ": " + cudaGetErrorString(e);
+  return -2;
+}
+
+#define KI_CUDA(expr)                                   \
+  do {                                                  \
+    const int rc_ = cuda_check((expr), #expr);          \
+    if (rc_) return rc_;                                \
+  } while (0)
+
+#define KI_ALLOC(ptr, type, count)                                  \
+  do {                                                              \
+    (ptr) = arena_.get<type>(count);                                \
+    if (!(ptr)) return fail("device allocation failed: " #ptr);     \
+  } while (0)
+
+std::vector<BoxBlock> Solver::blocks_of(int box) const {
+  // Accumulated updates inside the box's current dof list: its own skeleton
+  // update when compressed, else its children's lists laid end to end.
+  const Box& b = tree.boxes[box];
+  if (b.compressed) return {BoxBlock{boxdev_[box].acc, b.rank, 0}};
+  std::vector<BoxBlock> out;
+  if (b.leaf) return out;
+  int off = 0;
+  for (int q = 0; q < 4; q++) {
+    const int c = b.child[q];
+    for (const BoxBlock& x : blocks_of(c)) out.push_back(BoxBlock{x.acc, x.size, x.pos + off});
+    const Box& cb = tree.boxes[c];
+    off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
+  }
+  return out;
+}
+
+void Solver::build_block_map(const std::vector<BoxBlock>& blocks, int n, std::vector<int>* bid,
+                             std::vector<int>* bpos, std::vector<UpdBlock>* tab) const {
+  const int base = static_cast<int>(tab->size());
+  const size_t b0 = bid->size();
+  bid->resize(b0 + n, -1);
+  bpos->resize(b0 + n, 0);
+  for (size_t q = 0; q < blocks.size(); q++) {
+    tab->push_back(UpdBlock{blocks[q].acc, blocks[q].size, 0});
+    for (int t = 0; t < blocks[q].size; t++) {
+      (*bid)[b0 + blocks[q].pos + t] = static_cast<int>(q);
+      (*bpos)[b0 + blocks[q].pos + t] = t;
+    }
+  }
+  (void)base;
+}
+
+void Solver::build_tree_only() {
+  tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  for (int level = static_cast<int>(tree.levels.size()) - 1; level >= 0; level--)
+    tree.refresh_level(level, nullptr);
+  allskel = tree.boxes[0].active;
+}
+
+int Solver::factor() {
+  cudaEvent_t ev0, ev1;
+  KI_CUDA(cudaEventCreate(&ev0));
+  KI_CUDA(cudaEventCreate(&ev1));
+  KI_CUDA(cudaEventRecord(ev0, stream_));
+  t_id_ms = t_decouple_ms = t_top_ms = 0;
+  id_launches = 0;
+  id_flops = id_bytes = 0;
+
+  tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  boxdev_.assign(tree.boxes.size(), BoxDev{});
+  levels_.assign(tree.levels.size(), LevelFactors{});
+
+  // geometry, proxy directions, holes, status flag
+  {
+    std::vector<Node> nodes(n_points_);
+    for (int i = 0; i < n_points_; i++)
+      nodes[i] = Node{pts_[2 * i], pts_[2 * i + 1], nrm_[2 * i], nrm_[2 * i + 1], wts_[i],
+                      curv_[i], 0.0, 0.0};
+    KI_ALLOC(d_nodes_, Node, n_points_);
+    KI_CUDA(upload(d_nodes_, nodes, stream_));
+    std::vector<double> dir(2 * kNumProxy);
+    for (int i = 0; i < kNumProxy; i++) {
+      const double ang = 2 * M_PI * i * (1.0 / kNumProxy);
+      dir[i] = std::cos(ang);
+      dir[kNumProxy + i] = std::sin(ang);
+    }
+    KI_ALLOC(d_proxy_dir_, double, dir.size());
+    KI_CUDA(upload(d_proxy_dir_, dir, stream_));
+    if (!holes_.empty()) {
+      KI_ALLOC(d_holes_, double, holes_.size());
+      KI_CUDA(upload(d_holes_, holes_, stream_));
+    }
+    KI_ALLOC(d_status_, int, 1);
+    KI_CUDA(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_));
+  }
+  nb_ = 0;
+  if (!holes_.empty() && opt_.pde != kLaplaceNeumann) {
+    std::vector<double> U, Psi;
+    border_U(opt_.pde, pts_, holes_, &U, &nb_);
+    border_Psi(opt_.pde, pts_, wts_, holes_, &Psi);
+    KI_ALLOC(d_U_, double, U.size());
+    KI_ALLOC(d_Psi_, double, Psi.size());
+    KI_CUDA(upload(d_U_, U, stream_));
+    KI_CUDA(upload(d_Psi_, Psi, stream_));
+  }
+
+  const int L = static_cast<int>(tree.levels.size());
+  launch_log.clear();
+  t_wait_ms = 0;
+  for (int level = L - 1; level > 0; level--) {
+    const int rc = process_level(level);
+    if (rc) return rc;
+  }
+  for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
+  allskel = tree.boxes[0].active;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (time_phases) {
+    KI_CUDA(cudaEventCreate(&t0));
+    KI_CUDA(cudaEventCreate(&t1));
+    KI_CUDA(cudaEventRecord(t0, stream_));
+  }
+  int rc = factor_top();
+  if (rc) return rc;
+  if (time_phases) {
+    KI_CUDA(cudaEventRecord(t1, stream_));
+    KI_CUDA(cudaEventSynchronize(t1));
+    float ms = 0;
+    KI_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    t_top_ms = ms;
+    launch_log.push_back({0, 2, 1, 1, 0, ns_ + nb_, ms});
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+  }
+
+  int status = 0;
+  KI_CUDA(cudaMemcpyAsync(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  KI_CUDA(cudaEventRecord(ev1, stream_));
+  KI_CUDA(cudaStreamSynchronize(stream_));
+  float ms = 0;
+  KI_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+  t_factor_ms = ms;
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (status) return fail("zero pivot in an LU factorization (singular block)");
+  return 0;
+}
+
+int Solver::process_level(int level) {
+  std::vector<std::vector<int>> near(tree.boxes.size());
+  tree.refresh_level(level, &near);
+  const std::vector<int>& ids = tree.levels[level];
+  const int P = sd_ == 2 ? 4 * kNumProxy : 2 * kNumProxy;
+
+  struct Cand {
+    int box, n, m, I, g;
+    std::vector<int> rows;
+  };
+  std::vector<Cand> cand;
+  for (int id : ids) {
+    const Box& b = tree.boxes[id];
+    if (b.compressed || static_cast<int>(b.active.size()) < opt_.min_dofs_to_compress) continue;
+    Cand c;
+    c.box = id;
+    c.n = static_cast<int>(b.active.size());
+    if (level == 1 || level == 2) {
+      // kernel.cpp:164-207: every other active dof of the level (and the
+      // level-1 leaves for level 2), both directions, no proxy circle.
+      for (int o : tree.levels[level])
+        if (o != id) c.rows.insert(c.rows.end(), tree.boxes[o].active.begin(),
+                                   tree.boxes[o].active.end());
+      if (level == 2)
+        for (int o : tree.levels[1])
+          if (tree.boxes[o].leaf)
+            c.rows.insert(c.rows.end(), tree.boxes[o].original.begin(),
+                          tree.boxes[o].original.end());
+      c.I = static_cast<int>(c.rows.size());
+      c.m = 2 * c.I;
+    } else {
+      // near dofs inside the proxy circle (kernel.cpp:209-218)
+      const double cx = b.corner[0] + b.side / 2.0, cy = b.corner[1] + b.side / 2.0;
+      for (int dof : near[id]) {
+        const int pt = dof / sd_;
+        const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
+        const double dist = std::sqrt(std::pow(cx - x, 2) + std::pow(cy - y, 2));
+        if (dist < kRadiusRatio * b.side) c.rows.push_back(dof);
+      }
+      c.I = static_cast<int>(c.rows.size());
+      c.m = 2 * c.I + P;
+    }
+    if (c.m == 0) continue;
+    c.g = pick_group(c.m, c.n);
+    cand.push_back(std::move(c));
+  }
+  LevelFactors& lf = levels_[level];
+  lf.level = level;
+  if (cand.empty()) return 0;
+  std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.g < b.g; });
+
+  const int nc = static_cast<int>(cand.size());
+  std::vector<IdTask> tasks(nc);
+  std::vector<int> act, rows;
+  long long a_total = 0, t_total = 0;
+  int perm_total = 0;
+  for (int q = 0; q < nc; q++) {
+    const Cand& c = cand[q];
+    const Box& b = tree.boxes[c.box];
+    IdTask& t = tasks[q];
+    t.n = c.n;
+    t.m = c.m;
+    t.n_row = c.I;
+    t.proxy = c.m - 2 * c.I;
+    t.act_off = static_cast<int>(act.size());
+    t.row_off = static_cast<int>(rows.size());
+    t.lda = (c.m + 3) & ~3;
+    t.perm_off = perm_total;
+    t.a_off = a_total;
+    t.t_off = t_total;
+    t.cx = b.corner[0] + b.side / 2.0;
+    t.cy = b.corner[1] + b.side / 2.0;
+    t.rad = b.side * kRadiusRatio;
+    t.pw = 2.0 * M_PI * t.rad / kNumProxy;
+    act.insert(act.end(), b.active.begin(), b.active.end());
+    rows.insert(rows.end(), c.rows.begin(), c.rows.end());
+    a_total += static_cast<long long>(t.lda) * c.n;
+    t_total += static_cast<long long>(c.n) * c.n / 4 + 1;
+    perm_total += c.n;
+  }
+  int *d_act, *d_rows, *d_perm, *d_rank;
+  double* d_T;
+  IdTask* d_tasks;
+  KI_ALLOC(d_act, int, act.size());
+  KI_ALLOC(d_rows, int, rows.size());
+  KI_ALLOC(d_perm, int, perm_total);
+  KI_ALLOC(d_rank, int, nc);
+  KI_ALLOC(d_T, double, t_total);
+  KI_ALLOC(d_tasks, IdTask, nc);
+  KI_CUDA(work_.reserve(sizeof(double) * a_total, stream_));
+  KI_CUDA(upload(d_act, act, stream_));
+  KI_CUDA(upload(d_rows, rows, stream_));
+  KI_CUDA(upload(d_tasks, tasks, stream_));
+
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (time_phases) {
+    KI_CUDA(cudaEventCreate(&e0));
+    KI_CUDA(cudaEventCreate(&e1));
+  }
+  // one launch per cluster size
+  for (int q0 = 0; q0 < nc;) {
+    int q1 = q0;
+    int m_cap = 0, n_cap = 0;
+    while (q1 < nc && cand[q1].g == cand[q0].g) {
+      m_cap = std::max(m_cap, cand[q1].m);
+      n_cap = std::max(n_cap, cand[q1].n);
+      q1++;
+    }
+    if (id_smem_bytes(m_cap, n_cap) > 227 * 1024)
+      return fail("interpolative decomposition too tall for shared staging (m = " +
+                  std::to_string(m_cap) + ")");
+    IdParams p{};
+    p.tasks = d_tasks + q0;
+    p.ntasks = q1 - q0;
+    p.pde = opt_.pde;
+    p.nodes = d_nodes_;
+    p.act = d_act;
+    p.rowdofs = d_rows;
+    p.work = static_cast<double*>(work_.p);
+    p.tout = d_T;
+    p.perm = d_perm;
+    p.rank = d_rank + q0;
+    p.proxy_dir = d_proxy_dir_;
+    p.tol = opt_.id_tol;
+    p.m_cap = m_cap;
+    p.n_cap = n_cap;
+    if (time_phases) KI_CUDA(cudaEventRecord(e0, stream_));
+    KI_CUDA(launch_id(p, cand[q0].g, stream_));
+    if (time_phases) {
+      KI_CUDA(cudaEventRecord(e1, stream_));
+      KI_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      KI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      t_id_ms += ms;
+      id_launches++;
+      launch_log.push_back({level, 0, cand[q0].g, q1 - q0, m_cap, n_cap, ms});
+    }
+    q0 = q1;
+  }
+  if (time_phases) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  std::vector<int> rank(nc), perm(perm_total);
+  KI_CUDA(cudaMemcpyAsync(rank.data(), d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
+  KI_CUDA(cudaMemcpyAsync(perm.data(), d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,
+                          stream_));
+  {
+    const auto w0 = std::chrono::steady_clock::now();
+    KI_CUDA(cudaStreamSynchronize(stream_));
+    t_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0)
+                     .count();
+  }
+
+  // skeleton / redundant sets (InteractionLists::set_rs_ranges, quadtree.h:23-35)
+  std::vector<int> comp;  // candidate indices that compressed
+  for (int q = 0; q < nc; q++) {
+    const Cand& c = cand[q];
+    const IdTask& t = tasks[q];
+    const int k = rank[q];
+    // algorithmic work of the ID: entry generation + k Householder steps on
+    // the m x n matrix (dot + update over the trailing columns) + the
+    // triangular solve for T; bytes = the matrix written once and read once.
+    const double m = c.m, n = c.n;
+    const int steps = k > 0 ? k : std::min(c.m, c.n);
+    id_flops += 4.0 * m * (n * steps - 0.5 * steps * steps) + 1.0 * k * k * (n - k);
+    id_bytes += 16.0 * m * n;
+    if (k == 0) continue;
+    Box& b = tree.boxes[c.box];
+    b.compressed = true;
+    b.rank = k;
+    b.perm.assign(perm.begin() + t.perm_off, perm.begin() + t.perm_off + c.n);
+    b.skel.clear();
+    b.redundant.clear();
+    for (int i = 0; i < k; i++) b.skel.push_back(b.active[b.perm[i]]);
+    for (int i = k; i < c.n; i++) b.redundant.push_back(b.active[b.perm[i]]);
+    boxdev_[c.box].T = d_T + t.t_off;
+    comp.push_back(q);
+  }
+  if (comp.empty()) return 0;
+
+  // ---- decouple every compressed box of the level
+  const int ncomp = static_cast<int>(comp.size());
+  std::vector<DecTask> dt(ncomp);
+  std::vector<int> bid, bpos;
+  std::vector<UpdBlock> tab;
+  std::vector<long long> bid_off(ncomp), tab_off(ncomp);
+  long long scratch_total = 0;
+  std::vector<long long> k_off(ncomp), krs_off(ncomp);
+  size_t fac_total = 0, piv_total = 0;
+  for (int t = 0; t < ncomp; t++) {
+    const Cand& c = cand[comp[t]];
+    const Box& b = tree.boxes[c.box];
+    const int n = c.n, k = b.rank, r = n - k;
+    bid_off[t] = static_cast<long long>(bid.size());
+    tab_off[t] = static_cast<long long>(tab.size());
+    std::vector<BoxBlock> blocks;
+    if (!b.leaf) {
+      int off = 0;
+      for (int q = 0; q < 4; q++) {
+        const int ch = b.child[q];
+        for (const BoxBlock& x : blocks_of(ch)) blocks.push_back(BoxBlock{x.acc, x.size, x.pos + off});
+        const Box& cb = tree.boxes[ch];
+        off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
+      }
+    }
+    build_block_map(blocks, n, &bid, &bpos, &tab);
+    k_off[t] = scratch_total;
+    scratch_total += static_cast<long long>(n) * n;
+    krs_off[t] = scratch_total;
+    scratch_total += static_cast<long long>(r) * k;
+    fac_total += static_cast<size_t>(k) * r * 2 + static_cast<size_t>(r) * r +
+                 static_cast<size_t>(k) * k;
+    piv_total += r;
+  }
+  int *d_bid, *d_bpos, *d_piv;
+  UpdBlock* d_tab;
+  double* d_fac;
+  DecTask* d_dt;
+  KI_ALLOC(d_bid, int, bid.size());
+  KI_ALLOC(d_bpos, int, bpos.size());
+  KI_ALLOC(d_tab, UpdBlock, tab.size());
+  KI_ALLOC(d_fac, double, fac_total);
+  KI_ALLOC(d_piv, int, piv_total);
+  KI_ALLOC(d_dt, DecTask, ncomp);
+  KI_CUDA(scratch2_.reserve(sizeof(double) * scratch_total, stream_));
+  double* scr = static_cast<double*>(scratch2_.p);
+  size_t fo = 0, po = 0;
+  for (int t = 0; t < ncomp; t++) {
+    const Cand& c = cand[comp[t]];
+    const IdTask& it = tasks[comp[t]];
+    const Box& b = tree.boxes[c.box];
+    const int n = c.n, k = b.rank, r = n - k;
+    BoxDev& bd = boxdev_[c.box];
+    bd.L = d_fac + fo;
+    fo += static_cast<size_t>(k) * r;
+    bd.U = d_fac + fo;
+    fo += static_cast<size_t>(k) * r;
+    bd.X = d_fac + fo;
+    fo += static_cast<size_t>(r) * r;
+    bd.acc = d_fac + fo;
+    fo += static_cast<size_t>(k) * k;
+    bd.piv = d_piv + po;
+    po += r;
+    DecTask& d = dt[t];
+    d.n = n;
+    d.k = k;
+    d.act = d_act + it.act_off;
+    d.perm = d_perm + it.perm_off;
+    d.bid = d_bid + bid_off[t];
+    d.bpos = d_bpos + bid_off[t];
+    d.blocks = d_tab + tab_off[t];
+    d.T = bd.T;
+    d.K = scr + k_off[t];
+    d.Krs = scr + krs_off[t];
+    d.L = bd.L;
+    d.U = bd.U;
+    d.X = bd.X;
+    d.acc = bd.acc;
+    d.piv = bd.piv;
+  }
+  KI_CUDA(upload(d_bid, bid, stream_));
+  KI_CUDA(upload(d_bpos, bpos, stream_));
+  KI_CUDA(upload(d_tab, tab, stream_));
+  KI_CUDA(upload(d_dt, dt, stream_));
+  DecParams dp{};
+  dp.tasks = d_dt;
+  dp.ntasks = ncomp;
+  dp.pde = opt_.pde;
+  dp.nodes = d_nodes_;
+  dp.status = d_status_;
+  cudaEvent_t d0 = nullptr, d1 = nullptr;
+  if (time_phases) {
+    KI_CUDA(cudaEventCreate(&d0));
+    KI_CUDA(cudaEventCreate(&d1));
+    KI_CUDA(cudaEventRecord(d0, stream_));
+  }
+  KI_CUDA(launch_decouple(dp, stream_));
+  if (time_phases) {
+    KI_CUDA(cudaEventRecord(d1, stream_));
+    KI_CUDA(cudaEventSynchronize(d1));
+    float ms = 0;
+    KI_CUDA(cudaEventElapsedTime(&ms, d0, d1));
+    t_decouple_ms += ms;
+    int nmax = 0;
+    for (int t = 0; t < ncomp; t++) nmax = std::max(nmax, cand[comp[t]].n);
+    launch_log.push_back({level, 1, 1, ncomp, 0, nmax, ms});
+    cudaEventDestroy(d0);
+    cudaEventDestroy(d1);
+  }
+
+  // ---- sweep descriptors of the level
+  std::vector<int> sk, rd;
+  std::vector<SweepTask> st(ncomp);
+  std::vector<int> sk_off(ncomp), rd_off(ncomp);
+  int cap = 0;
+  for (int t = 0; t < ncomp; t++) {
+    const Box& b = tree.boxes[cand[comp[t]].box];
+    sk_off[t] = static_cast<int>(sk.size());
+    rd_off[t] = static_cast<int>(rd.size());
+    sk.insert(sk.end(), b.skel.begin(), b.skel.end());
+    rd.insert(rd.end(), b.redundant.begin(), b.redundant.end());
+    cap = std::max(cap, static_cast<int>(b.skel.size() + b.redundant.size()));
+    lf.boxes.push_back(cand[comp[t]].box);
+  }
+  KI_ALLOC(lf.d_skel, int, sk.size());
+  KI_ALLOC(lf.d_red, int, rd.size());
+  KI_ALLOC(lf.d_tasks, SweepTask, ncomp);
+  for (int t = 0; t < ncomp; t++) {
+    const int box = cand[comp[t]].box;
+    const Box& b = tree.boxes[box];
+    const BoxDev& bd = boxdev_[box];
+    st[t] = SweepTask{b.rank, static_cast<int>(b.redundant.size()), lf.d_skel + sk_off[t],
+                      lf.d_red + rd_off[t], bd.T, bd.L, bd.U, bd.X, bd.piv};
+  }
+  KI_CUDA(upload(lf.d_skel, sk, stream_));
+  KI_CUDA(upload(lf.d_red, rd, stream_));
+  KI_CUDA(upload(lf.d_tasks, st, stream_));
+  lf.ntasks = ncomp;
+  lf.cap = cap;
+  return 0;
+}
+
+int Solver::factor_top() {
+  // concatenated sweep tasks of every compressed box for the diagonal solves
+  {
+    std::vector<SweepTask> all;
+    int cap = 0;
+    for (LevelFactors& lf : levels_) {
+      if (!lf.ntasks) continue;
+      std::vector<SweepTask> st(lf.ntasks);
+      KI_CUDA(cudaMemcpyAsync(st.data(), lf.d_tasks, sizeof(SweepTask) * lf.ntasks,
+                              cudaMemcpyDeviceToHost, stream_));
+      KI_CUDA(cudaStreamSynchronize(stream_));
+      all.insert(all.end(), st.begin(), st.end());
+      cap = std::max(cap, lf.cap);
+    }
+    all_compressed_.ntasks = static_cast<int>(all.size());
+    all_compressed_.cap = cap;
+    KI_ALLOC(all_compressed_.d_tasks, SweepTask, all.size());
+    KI_CUDA(upload(all_compressed_.d_tasks, all, stream_));
+  }
+  ns_ = static_cast<int>(allskel.size());
+  KI_ALLOC(d_allskel_, int, ns_);
+  KI_CUDA(upload(d_allskel_, allskel, stream_));
+  std::vector<BoxBlock> blocks;
+  {
+    const Box& root = tree.boxes[0];
+    if (!root.leaf) {
+      int off = 0;
+      for (int q = 0; q < 4; q++) {
+        const int ch = root.child[q];
+        for (const BoxBlock& x : blocks_of(ch)) blocks.push_back(BoxBlock{x.acc, x.size, x.pos + off});
+        const Box& cb = tree.boxes[ch];
+        off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
+      }
+    }
+  }
+  std::vector<int> bid, bpos;
+  std::vector<UpdBlock> tab;
+  build_block_map(blocks, ns_, &bid, &bpos, &tab);
+  int *d_bid, *d_bpos;
+  UpdBlock* d_tab;
+  KI_ALLOC(d_bid, int, bid.size());
+  KI_ALLOC(d_bpos, int, bpos.size());
+  KI_ALLOC(d_tab, UpdBlock, tab.size());
+  KI_CUDA(upload(d_bid, bid, stream_));
+  KI_CUDA(upload(d_bpos, bpos, stream_));
+  KI_CUDA(upload(d_tab, tab, stream_));
+  const int ntop = ns_ + nb_;
+  KI_ALLOC(d_top_, double, static_cast<size_t>(ntop) * ntop);
+  KI_ALLOC(d_top_piv_, int, ntop);
+  KI_ALLOC(d_tmp_, double, 4 * static_cast<size_t>(n_dofs_ + ntop) + 64);
+  KI_CUDA(launch_assemble_top(opt_.pde, d_nodes_, d_allskel_, ns_, d_bid, d_bpos, d_tab, d_top_,
+                              ntop, stream_));
+  if (nb_ > 0) {
+    const int rc = factor_border();
+    if (rc) return rc;
+  }
+  if (ntop > 0) KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_));
+  return 0;
+}
+
+int Solver::factor_border() {
+  // skel_factorization.cpp:130-242: sweep U and Psi^T with the factors,
+  // D^{-1} on the redundant rows, then the bordered Schur system S.
+  const int N = n_dofs_, nb = nb_, ns = ns_;
+  std::vector<int> sorted = allskel;
+  std::sort(sorted.begin(), sorted.end());
+  allred.clear();
+  size_t si = 0;
+  for (int i = 0; i < N; i++) {
+    if (si < sorted.size() && i == sorted[si]) {
+      si++;
+    } else {
+      allred.push_back(i);
+    }
+  }
+  if (allred.empty()) return fail("No compression possible");
+  const int nr = static_cast<int>(allred.size());
+  std::vector<int> red_pos(N, -1);
+  for (int i = 0; i < nr; i++) red_pos[allred[i]] = i;
+  KI_ALLOC(d_allred_, int, nr);
+  KI_ALLOC(d_red_pos_, int, N);
+  KI_CUDA(upload(d_allred_, allred, stream_));
+  KI_CUDA(upload(d_red_pos_, red_pos, stream_));
+
+  double *modU, *modP;
+  KI_ALLOC(modU, double, static_cast<size_t>(N) * nb);
+  KI_ALLOC(modP, double, static_cast<size_t>(N) * nb);
+  KI_CUDA(cudaMemcpyAsync(modU, d_U_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice, stream_));
+  {
+    std::vector<double> Psi(static_cast<size_t>(nb) * N), PsiT(static_cast<size_t>(N) * nb);
+    KI_CUDA(cudaMemcpyAsync(Psi.data(), d_Psi_, sizeof(double) * Psi.size(),
+                            cudaMemcpyDeviceToHost, stream_));
+    KI_CUDA(cudaStreamSynchronize(stream_));
+    for (int j = 0; j < N; j++)
+      for (int i = 0; i < nb; i++) PsiT[j + static_cast<size_t>(N) * i] = Psi[i + static_cast<size_t>(nb) * j];
+    KI_CUDA(upload(modP, PsiT, stream_));
+  }
+  const int L = static_cast<int>(levels_.size());
+  for (int l = L - 1; l >= 0; l--) {
+    const LevelFactors& lf = levels_[l];
+    if (!lf.ntasks) continue;
+    SweepParams sp{lf.d_tasks, lf.ntasks, modU, N, nb, 0, nullptr, lf.cap};
+    KI_CUDA(launch_sweep_up(sp, false, stream_));
+    sp.x = modP;
+    KI_CUDA(launch_sweep_up(sp, true, stream_));
+  }
+  double *dinv, *us, *ps, *corr;
+  KI_ALLOC(d_Ured_, double, static_cast<size_t>(nr) * nb);
+  KI_ALLOC(d_Pred_, double, static_cast<size_t>(nr) * nb);
+  KI_ALLOC(dinv, double, static_cast<size_t>(nr) * nb);
+  KI_ALLOC(us, double, static_cast<size_t>(ns) * nb);
+  KI_ALLOC(ps, double, static_cast<size_t>(ns) * nb);
+  KI_ALLOC(corr, double, static_cast<size_t>(nb) * nb);
+  KI_CUDA(launch_gather(modU, N, d_allred_, nr, nb, d_Ured_, nr, stream_));
+  KI_CUDA(launch_gather(modP, N, d_allred_, nr, nb, d_Pred_, nr, stream_));
+  KI_CUDA(launch_gather(modU, N, d_allred_, nr, nb, dinv, nr, stream_));
+  KI_CUDA(launch_gather(modU, N, d_allskel_, ns, nb, us, ns, stream_));
+  KI_CUDA(launch_gather(modP, N, d_allskel_, ns, nb, ps, ns, stream_));
+  SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dinv, nr, nb, 1, d_red_pos_,
+                 all_compressed_.cap};
+  KI_CUDA(launch_diag_solve(dp, stream_));
+  KI_CUDA(small_gemm(true, false, nb, nb, nr, 1.0, d_Pred_, nr, dinv, nr, 0.0, corr, nb, stream_));
+  KI_CUDA(launch_fill_border(d_top_, ns + nb, ns, nb, us, ps, corr, stream_));
+  return 0;
+}
+
+int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha) {
+  const int N = n_dofs_;
+  double* x = d_mu;
+  if (d_b != d_mu)
+    KI_CUDA(cudaMemcpyAsync(x, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  const int L = static_cast<int>(levels_.size());
+  for (int l = L - 1; l >= 0; l--) {
+    const LevelFactors& lf = levels_[l];
+    if (!lf.ntasks) continue;
+    SweepParams sp{lf.d_tasks, lf.ntasks, x, N, 1, 0, nullptr, lf.cap};
+    KI_CUDA(launch_sweep_up(sp, false, stream_));
+  }
+  const int ns = ns_, nb = nb_;
+  if (nb == 0) {
+    SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, x, N, 1, 0, nullptr,
+                   all_compressed_.cap};
+    KI_CUDA(launch_diag_solve(dp, stream_));
+    if (ns > 0) {
+      KI_CUDA(launch_gather(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
+      KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_));
+      KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
+    }
+  } else {
+    const int nr = static_cast<int>(allred.size());
+    double* w = d_tmp_;
+    double* dw = w + nr;
+    double* M = dw + nr;
+    KI_CUDA(launch_gather(x, N, d_allred_, nr, 1, w, nr, stream_));
+    KI_CUDA(launch_gather(x, N, d_allskel_, ns, 1, M, ns, stream_));
+    KI_CUDA(cudaMemcpyAsync(dw, w, sizeof(double) * nr, cudaMemcpyDeviceToDevice, stream_));
+    SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dw, nr, 1, 1, d_red_pos_,
+                   all_compressed_.cap};
+    KI_CUDA(launch_diag_solve(dp, stream_));
+    KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, 0.0, M + ns, nb, stream_));
+    KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_));
+    if (d_alpha)
+      KI_CUDA(cudaMemcpyAsync(d_alpha, M + ns, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
+                              stream_));
+    KI_CUDA(small_gemm(false, false, nr, 1, nb, -1.0, d_Ured_, nr, M + ns, nb, 1.0, w, nr, stream_));
+    dp.x = w;
+    KI_CUDA(launch_diag_solve(dp, stream_));
+    KI_CUDA(launch_scatter(x, N, d_allred_, nr, 1, w, nr, stream_));
+    KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, M, ns, stream_));
+  }
+  for (int l = 0; l < L; l++) {
+    const LevelFactors& lf = levels_[l];
+    if (!lf.ntasks) continue;
+    SweepParams sp{lf.d_tasks, lf.ntasks, x, N, 1, 0, nullptr, lf.cap};
+    KI_CUDA(launch_sweep_down(sp, stream_));
+  }
+  return 0;
+}
+
+int Solver::apply_device(const double* d_x, double* d_y) {
+  KI_CUDA(launch_apply_operator(opt_.pde, d_nodes_, n_dofs_, d_x, d_y, nb_, d_U_, d_Psi_,
+                                stream_));
+  return 0;
+}
+
+}  // namespace kib

@@ -1,0 +1,166 @@
+// The B200 recursive-skeletonization factorization object.
+//
+// One Solver holds what the reference spreads over QuadTree (the tree and
+// every box's T, L, U, X_rr factors, quadtree.h:44-102) and
+// SkelFactorization (skeletonize/solve, skel_factorization.h:19-62): the
+// host quadtree and index lists, and device storage for the geometry, the
+// per-level factors and the top-level (bordered) skeleton LU.
+#ifndef KI_SOLVER_H_
+#define KI_SOLVER_H_
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "ki_kernels.h"
+#include "ki_tree.h"
+
+namespace kib {
+
+// Bump allocator over large cudaMalloc chunks; pointers stay valid until the
+// arena is destroyed.
+class Arena {
+ public:
+  ~Arena();
+  void* alloc(size_t bytes);
+  template <class T>
+  T* get(size_t count) { return static_cast<T*>(alloc(sizeof(T) * (count ? count : 1))); }
+  size_t reserved() const { return reserved_; }
+
+ private:
+  std::vector<void*> chunks_;
+  char* cur_ = nullptr;
+  size_t left_ = 0;
+  size_t reserved_ = 0;
+};
+
+// Reusable device scratch that only grows.
+struct Scratch {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~Scratch();
+  cudaError_t reserve(size_t want, cudaStream_t s);
+};
+
+struct SolverOptions {
+  int pde = 0;              // 0 Laplace, 1 Laplace-Neumann, 2 Stokes
+  int max_leaf_dofs = 32;   // MAX_LEAF_DOFS (quadtree.h:10)
+  double id_tol = 1e-6;
+  int min_dofs_to_compress = 16;  // MIN_DOFS_TO_COMPRESS (skel_factorization.h:11)
+};
+
+struct LevelFactors {
+  int level = 0;
+  int ntasks = 0;
+  int cap = 0;
+  SweepTask* d_tasks = nullptr;
+  int* d_skel = nullptr;
+  int* d_red = nullptr;
+  std::vector<int> boxes;  // compressed boxes of this level
+};
+
+struct BoxBlock {  // accumulated update living at positions [pos, pos + size)
+  const double* acc;
+  int size;
+  int pos;
+};
+
+class Solver {
+ public:
+  Solver(const SolverOptions& opt, int n_points, const double* points,
+         const double* normals, const double* curvatures, const double* weights,
+         int n_holes, const double* holes, cudaStream_t stream);
+  ~Solver();
+
+  // QuadTree::initialize_tree + SkelFactorization::skeletonize.
+  int factor();
+  // QuadTree::initialize_tree only, active lists as before compression.
+  void build_tree_only();
+  // linear_solve on device buffers: d_mu (dofs), d_alpha (border, may be
+  // null when there are no holes).  d_b and d_mu may be the same buffer.
+  int solve_device(const double* d_b, double* d_mu, double* d_alpha);
+  // y = A x on device (bordered when there are holes).
+  int apply_device(const double* d_x, double* d_y);
+
+  int n_dofs() const { return n_dofs_; }
+  int n_border() const { return nb_; }
+  int pde() const { return opt_.pde; }
+  int sol_dim() const { return sd_; }
+  cudaStream_t stream() const { return stream_; }
+  const Node* d_nodes() const { return d_nodes_; }
+  const double* d_holes() const { return d_holes_; }
+  int n_holes() const { return static_cast<int>(holes_.size() / 4); }
+
+  QuadTreeHost tree;
+  std::vector<int> allskel;
+  std::vector<int> allred;
+
+  // Phase times of the last factor/solve (ms, CUDA events); id_ms is the
+  // summed duration of the ID launches, id_launches their count.
+  double t_factor_ms = 0, t_id_ms = 0, t_decouple_ms = 0, t_top_ms = 0;
+  int id_launches = 0;
+  double id_flops = 0, id_bytes = 0;  // algorithmic work of the ID launches
+  bool time_phases = false;
+  // Per-launch record of the timed factorization: kind 0 ID, 1 decouple,
+  // 2 top-level assembly + LU; ms from CUDA events on the solver stream.
+  struct LaunchRecord {
+    int level, kind, group, ntasks, m_cap, n_cap;
+    double ms;
+  };
+  std::vector<LaunchRecord> launch_log;
+  double t_wait_ms = 0;  // host time blocked on the per-level rank download
+  std::string error;
+
+ private:
+  int fail(const std::string& msg);
+  int cuda_check(cudaError_t e, const char* what);
+  int process_level(int level);
+  int factor_top();
+  int factor_border();
+  std::vector<BoxBlock> blocks_of(int box) const;
+  void build_block_map(const std::vector<BoxBlock>& blocks, int n, std::vector<int>* bid,
+                       std::vector<int>* bpos, std::vector<UpdBlock>* tab) const;
+
+  SolverOptions opt_;
+  int sd_ = 1, n_points_ = 0, n_dofs_ = 0, nb_ = 0;
+  std::vector<double> pts_, nrm_, curv_, wts_, holes_;
+  cudaStream_t stream_;
+
+  Arena arena_;
+  Scratch work_, scratch2_;
+  Node* d_nodes_ = nullptr;
+  double* d_proxy_dir_ = nullptr;
+  double* d_holes_ = nullptr;
+  int* d_status_ = nullptr;
+
+  // per-box device factors (indexed by box id)
+  struct BoxDev {
+    double* T = nullptr;
+    double* L = nullptr;
+    double* U = nullptr;
+    double* X = nullptr;
+    double* acc = nullptr;
+    int* piv = nullptr;
+  };
+  std::vector<BoxDev> boxdev_;
+  std::vector<LevelFactors> levels_;
+  LevelFactors all_compressed_;
+
+  // top level
+  int ns_ = 0;
+  double* d_top_ = nullptr;  // LU of allskel_mat, or of S with holes
+  int* d_top_piv_ = nullptr;
+  int* d_allskel_ = nullptr;
+  int* d_allred_ = nullptr;
+  int* d_red_pos_ = nullptr;
+  double* d_U_ = nullptr;     // N x nb
+  double* d_Psi_ = nullptr;   // nb x N
+  double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
+  double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
+  double* d_tmp_ = nullptr;   // solve scratch
+};
+
+}  // namespace kib
+
+#endif  // KI_SOLVER_H_

@@ -1,0 +1,183 @@
+// Host quadtree: same partition rules as the reference
+// (kern_interp/quadtree/quadtree.cpp), written over an index-addressed box
+// array instead of pointer-linked nodes.
+#include "ki_tree.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace kib {
+
+int QuadTreeHost::pick_child(const Box& b, double x, double y) const {
+  // Split point and child choice of quadtree.cpp:171-185.
+  double mx = ((b.corner[6] - b.corner[0]) / 2.0) + b.corner[0];
+  double my = ((b.corner[3] - b.corner[1]) / 2.0) + b.corner[1];
+  if (x < mx) return y < my ? 0 : 1;
+  return y < my ? 3 : 2;
+}
+
+void QuadTreeHost::subdivide(int id) {
+  // quadtree.cpp:203-285: four children appended to the next level in
+  // {BL, TL, TR, BR} order, the parent's dofs handed down point by point,
+  // then any over-full child split depth first.
+  boxes[id].leaf = false;
+  double c[8];
+  std::memcpy(c, boxes[id].corner, sizeof(c));
+  const double mx = ((c[6] - c[0]) / 2.0) + c[0];
+  const double my = ((c[3] - c[1]) / 2.0) + c[1];
+  const int lvl = boxes[id].level + 1;
+  const double half = boxes[id].side / 2.0;
+  if (static_cast<int>(levels.size()) < lvl + 1) levels.emplace_back();
+  int kid[4];
+  for (int q = 0; q < 4; q++) {
+    Box ch;
+    std::memcpy(ch.corner, c, sizeof(c));
+    ch.level = lvl;
+    ch.side = half;
+    ch.parent = id;
+    kid[q] = static_cast<int>(boxes.size());
+    boxes.push_back(ch);
+    levels[lvl].push_back(kid[q]);
+  }
+  // Corner edits per child: {index, value} pairs.
+  const int edit_idx[4][4] = {{3, 4, 5, 6}, {1, 4, 6, 7}, {0, 1, 2, 7}, {0, 2, 3, 5}};
+  const double edit_val[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
+                                 {mx, my, mx, my}, {mx, mx, my, my}};
+  for (int q = 0; q < 4; q++)
+    for (int e = 0; e < 4; e++) boxes[kid[q]].corner[edit_idx[q][e]] = edit_val[q][e];
+  for (int q = 0; q < 4; q++) boxes[id].child[q] = kid[q];
+  const std::vector<int> dofs = boxes[id].original;
+  for (size_t t = 0; t < dofs.size(); t += sol_dim_) {
+    const int d = dofs[t];
+    const int p = d / sol_dim_;
+    const int q = pick_child(boxes[id], pts_[2 * p], pts_[2 * p + 1]);
+    for (int s = 0; s < sol_dim_; s++) boxes[kid[q]].original.push_back(d + s);
+  }
+  for (int q = 0; q < 4; q++)
+    if (static_cast<int>(boxes[kid[q]].original.size()) > max_leaf_) subdivide(kid[q]);
+}
+
+void QuadTreeHost::insert(int id, double x, double y, int pt) {
+  // quadtree.cpp:164-197.
+  for (int s = 0; s < sol_dim_; s++) boxes[id].original.push_back(sol_dim_ * pt + s);
+  const int ch = boxes[id].child[pick_child(boxes[id], x, y)];
+  if (ch >= 0) {
+    insert(ch, x, y, pt);
+  } else if (boxes[id].leaf &&
+             static_cast<int>(boxes[id].original.size()) > max_leaf_) {
+    subdivide(id);
+  }
+}
+
+void QuadTreeHost::descendant_neighbors(int big, int small) {
+  // quadtree.cpp:119-161, including its "y < top && y < bottom" side test.
+  const double top = boxes[big].corner[3], bottom = boxes[big].corner[1];
+  const double left = boxes[big].corner[0], right = boxes[big].corner[4];
+  for (int q = 0; q < 8; q += 2) {
+    const double x = boxes[small].corner[q], y = boxes[small].corner[q + 1];
+    const bool horiz = x > left && x < right &&
+                       (std::fabs(y - top) < 1e-14 || std::fabs(y - bottom) < 1e-14);
+    const bool vert = y < top && y < bottom &&
+                      (std::fabs(x - left) < 1e-14 || std::fabs(x - right) < 1e-14);
+    if (horiz || vert) {
+      boxes[big].nbr.push_back(small);
+      boxes[small].nbr.push_back(big);
+      break;
+    }
+  }
+  for (int q = 0; q < 4; q++)
+    if (boxes[small].child[q] >= 0) descendant_neighbors(big, boxes[small].child[q]);
+}
+
+void QuadTreeHost::neighbor_lists() {
+  // quadtree.cpp:27-69: siblings, same-level cousins whose lower-left corners
+  // lie within side*sqrt(2), then (for leaves) adjacent finer boxes.
+  for (size_t l = 0; l < levels.size(); l++) {
+    for (int a : levels[l]) {
+      const int par = boxes[a].parent;
+      if (par >= 0) {
+        for (int q = 0; q < 4; q++)
+          if (boxes[par].child[q] != a) boxes[a].nbr.push_back(boxes[par].child[q]);
+        const std::vector<int> pn = boxes[par].nbr;
+        for (int o : pn) {
+          for (int q = 0; q < 4; q++) {
+            const int cz = boxes[o].child[q];
+            if (cz < 0 || boxes[cz].level != boxes[a].level) continue;
+            const double dist =
+                std::sqrt(std::pow(boxes[a].corner[0] - boxes[cz].corner[0], 2) +
+                          std::pow(boxes[a].corner[1] - boxes[cz].corner[1], 2));
+            if (dist < boxes[a].side * std::sqrt(2) + 1e-5) boxes[a].nbr.push_back(cz);
+          }
+        }
+      }
+      if (boxes[a].leaf) {
+        for (size_t t = 0; t < boxes[a].nbr.size(); t++) {
+          const int o = boxes[a].nbr[t];
+          if (boxes[o].level != boxes[a].level) continue;
+          for (int q = 0; q < 4; q++)
+            if (boxes[o].child[q] >= 0) descendant_neighbors(a, boxes[o].child[q]);
+        }
+      }
+    }
+  }
+}
+
+void QuadTreeHost::build(const double* points, int n, int sol_dim,
+                         int max_leaf_dofs) {
+  // quadtree.cpp:72-114: root square [min - 0.01, max + 0.01]^2 over all
+  // coordinates, points inserted in order.
+  pts_.assign(points, points + 2 * static_cast<size_t>(n));
+  sol_dim_ = sol_dim;
+  max_leaf_ = max_leaf_dofs;
+  boxes.clear();
+  levels.clear();
+  min_ = max_ = pts_[0];
+  for (double v : pts_) {
+    if (v < min_) min_ = v;
+    if (v > max_) max_ = v;
+  }
+  const double lo = min_ - 0.01, hi = max_ + 0.01;
+  Box root;
+  const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
+  std::memcpy(root.corner, c, sizeof(c));
+  root.side = hi - lo;
+  boxes.push_back(root);
+  levels.push_back({0});
+  for (int p = 0; p < n; p++) insert(0, pts_[2 * p], pts_[2 * p + 1], p);
+  neighbor_lists();
+}
+
+void QuadTreeHost::refresh_box(int id) {
+  // quadtree.cpp:694-720.
+  Box& b = boxes[id];
+  b.skel.clear();
+  b.redundant.clear();
+  b.active.clear();
+  if (b.leaf) {
+    b.active = b.original;
+    return;
+  }
+  for (int q = 0; q < 4; q++) {
+    const Box& ch = boxes[b.child[q]];
+    const std::vector<int>& src = ch.compressed ? ch.skel : ch.active;
+    b.active.insert(b.active.end(), src.begin(), src.end());
+  }
+}
+
+void QuadTreeHost::refresh_level(int level, std::vector<std::vector<int>>* near) {
+  // quadtree.cpp:664-691.
+  for (int id : levels[level])
+    if (!boxes[id].compressed) refresh_box(id);
+  if (!near) return;
+  for (int id : levels[level]) {
+    std::vector<int>& nr = (*near)[id];
+    nr.clear();
+    for (int o : boxes[id].nbr) {
+      if (boxes[o].level > boxes[id].level) continue;
+      const std::vector<int>& src = boxes[o].leaf ? boxes[o].original : boxes[o].active;
+      nr.insert(nr.end(), src.begin(), src.end());
+    }
+  }
+}
+
+}  // namespace kib

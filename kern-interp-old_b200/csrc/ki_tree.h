@@ -1,0 +1,66 @@
+// Host-side adaptive quadtree for the B200 solver.
+//
+// Builds the same partition, level order and neighbour lists as the
+// reference QuadTree (kern_interp/quadtree/quadtree.cpp:27-285) and keeps the
+// per-box dof bookkeeping of remove_inactive_dofs_at_level/_box
+// (quadtree.cpp:656-720) as flat arrays that the level scheduler turns into
+// device work descriptors.  Boxes are numbered in creation order; `levels`
+// lists them in the reference's level order, which fixes the order of the
+// top-level skeleton and therefore the row/column order of its matrix.
+#ifndef KI_TREE_H_
+#define KI_TREE_H_
+
+#include <vector>
+
+namespace kib {
+
+struct Box {
+  int level = 0;
+  int parent = -1;
+  int child[4] = {-1, -1, -1, -1};  // order {BL, TL, TR, BR}
+  bool leaf = true;
+  bool compressed = false;
+  double corner[8] = {0};  // BL, TL, TR, BR corners, xy interleaved
+  double side = 0;
+  std::vector<int> nbr;       // neighbour boxes, reference order
+  std::vector<int> original;  // dofs of the points in the box
+  std::vector<int> active;    // dofs not yet eliminated below this box
+  std::vector<int> skel, redundant;
+  std::vector<int> perm;      // ID pivots (local active indices)
+  int rank = 0;
+};
+
+class QuadTreeHost {
+ public:
+  // points: interleaved xy of n points; sol_dim dofs per point.
+  void build(const double* points, int n, int sol_dim, int max_leaf_dofs);
+
+  int sol_dim() const { return sol_dim_; }
+  double min() const { return min_; }
+  double max() const { return max_; }
+  const std::vector<double>& points() const { return pts_; }
+
+  std::vector<Box> boxes;
+  std::vector<std::vector<int>> levels;
+
+  // active(b) for every not-yet-compressed box of `level`, then near(b) for
+  // every box of the level (quadtree.cpp:664-691).
+  void refresh_level(int level, std::vector<std::vector<int>>* near);
+  void refresh_box(int b);
+
+ private:
+  int pick_child(const Box& b, double x, double y) const;
+  void subdivide(int b);
+  void insert(int b, double x, double y, int pt);
+  void descendant_neighbors(int big, int small);
+  void neighbor_lists();
+
+  int sol_dim_ = 1;
+  int max_leaf_ = 32;
+  double min_ = 0, max_ = 0;
+  std::vector<double> pts_;
+};
+
+}  // namespace kib
+
+#endif  // KI_TREE_H_
