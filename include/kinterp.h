@@ -39,6 +39,8 @@ enum { KI_LAPLACE = 0, KI_LAPLACE_NEUMANN = 1, KI_STOKES = 2 };
 const char* ki_last_error(void);
 /* Library version, major * 10000 + minor * 100 + patch. */
 int ki_version(void);
+/* Number of CUDA kernels this library has launched in the process. */
+long long ki_kernel_launches(void);
 
 /* Builds the quadtree and skeletonizes the boundary operator.
  * Replaces QuadTree::initialize_tree (quadtree/quadtree.h:85-86), the U/Psi

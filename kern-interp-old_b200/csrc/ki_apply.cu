@@ -92,6 +92,7 @@ cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const 
                                   double* y, int nb, const double* U, const double* Psi,
                                   cudaStream_t s) {
   const int rows = n_dofs + nb;
+  count_launches(1);
   apply_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, x, y, nb, U, Psi);
   return cudaGetLastError();
 }
@@ -102,6 +103,7 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
                                 cudaStream_t s) {
   const int rows = nt * (pde == kStokes ? 2 : 1);
   if (rows == 0) return cudaSuccess;
+  count_launches(1);
   targets_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, nt, targets, mu, nh,
                                                      holes, alpha, out);
   return cudaGetLastError();
@@ -111,6 +113,7 @@ cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int 
                                 const int* src, int ns, double* out, cudaStream_t s) {
   const long long tot = static_cast<long long>(nt) * ns;
   if (tot == 0) return cudaSuccess;
+  count_launches(1);
   block_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(pde, nodes, tgt, nt, src, ns,
                                                                    out);
   return cudaGetLastError();

@@ -34,6 +34,86 @@ __device__ inline void cta_gemm_sub(double* C, int ldc, const double* C0, int ld
   }
 }
 
+// Tiled CTA GEMM: C (m x n) = C0 - op(A) op(B), op(A) m x kk, op(B) kk x n,
+// 64 x 64 output tiles with a 4 x 4 block per thread (256 threads), inner
+// dimension staged 16 at a time in `tile` (2 * 16 * 65 doubles).  C0 may be
+// null (taken as zero) or alias C.  Operands may live in shared or global
+// memory.  Ends with a barrier.
+constexpr int kGemmTileDoubles = 2 * 16 * 65;
+
+__device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int ldc0,
+                                      const double* A, int lda, bool ta, const double* B,
+                                      int ldb, bool tb, int m, int n, int kk, double* tile) {
+  double* sa = tile;            // [16][65]: sa[l * 65 + i] = op(A)(i0 + i, l0 + l)
+  double* sb = tile + 16 * 65;  // [16][65]: sb[l * 65 + j] = op(B)(l0 + l, j0 + j)
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int i0 = 0; i0 < m; i0 += 64) {
+    for (int j0 = 0; j0 < n; j0 += 64) {
+      double acc[4][4];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+      for (int l0 = 0; l0 < kk; l0 += 16) {
+        for (int e = threadIdx.x; e < 16 * 64; e += 256) {
+          // A: element (row i0 + q, inner l0 + l); B: (inner l0 + l, col j0 + q)
+          int q, l;
+          if (ta) {  // op(A)(i, l) = A[l + lda i]: inner index fastest in memory
+            l = e & 15;
+            q = e >> 4;
+          } else {
+            q = e & 63;
+            l = e >> 6;
+          }
+          const int gi = i0 + q, gl = l0 + l;
+          double va = 0.0;
+          if (gi < m && gl < kk)
+            va = ta ? A[gl + static_cast<long long>(lda) * gi] : A[gi + static_cast<long long>(lda) * gl];
+          sa[l * 65 + q] = va;
+          int qb, lb;
+          if (tb) {  // op(B)(l, j) = B[j + ldb l]: output index fastest
+            qb = e & 63;
+            lb = e >> 6;
+          } else {
+            lb = e & 15;
+            qb = e >> 4;
+          }
+          const int gj = j0 + qb, glb = l0 + lb;
+          double vb = 0.0;
+          if (gj < n && glb < kk)
+            vb = tb ? B[gj + static_cast<long long>(ldb) * glb] : B[glb + static_cast<long long>(ldb) * gj];
+          sb[lb * 65 + qb] = vb;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+          double av[4], bv[4];
+#pragma unroll
+          for (int a = 0; a < 4; a++) av[a] = sa[l * 65 + tx + 16 * a];
+#pragma unroll
+          for (int b = 0; b < 4; b++) bv[b] = sb[l * 65 + ty + 16 * b];
+#pragma unroll
+          for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int gi = i0 + tx + 16 * a, gj = j0 + ty + 16 * b;
+          if (gi < m && gj < n) {
+            const double c0 = C0 ? C0[gi + static_cast<long long>(ldc0) * gj] : 0.0;
+            C[gi + static_cast<long long>(ldc) * gj] = c0 - acc[a][b];
+          }
+        }
+    }
+  }
+  __syncthreads();
+}
+
 // In-place LU with partial pivoting (dgetf2) of an n x n matrix over the
 // CTA.  ipiv[j] = row exchanged with row j.  `red` needs 2 * 32 doubles.
 // Returns nonzero if an exactly zero pivot was met (LAPACK's info > 0).
@@ -99,6 +179,7 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
     }
     __syncthreads();
     const int rem = n - j - 1;
+#pragma unroll 4
     for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
       const int i = j + 1 + e % rem, c = j + 1 + e / rem;
       a[i + static_cast<long long>(ld) * c] -=

@@ -123,6 +123,8 @@ const char* ki_last_error(void) { return g_err.c_str(); }
 
 int ki_version(void) { return 100; }
 
+long long ki_kernel_launches(void) { return kib::launch_total(); }
+
 int ki_factor(int pde, int n_points, const double* points, const double* normals,
               const double* curvatures, const double* weights, int n_holes,
               const double* holes, int max_leaf_dofs, double id_tol, void* stream,

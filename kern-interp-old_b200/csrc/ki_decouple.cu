@@ -32,17 +32,23 @@ __device__ __forceinline__ double upd_lookup(const int* bid, const int* bpos,
   return blk.acc[bpos[a] + static_cast<long long>(blk.size) * bpos[b]];
 }
 
+// Boxes with n <= kSmemN keep K_BN, and then X_rr, in shared memory.
+constexpr int kSmemN = 160;
+
 __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
-  __shared__ double red[64];
+  extern __shared__ __align__(16) double dsm[];
+  double* tile = dsm;                     // kGemmTileDoubles
+  double* red = tile + kGemmTileDoubles;  // 64
+  double* kbuf = red + 64;                // n*n when staged
   const DecTask tk = P.tasks[blockIdx.x];
   const int n = tk.n, k = tk.k, r = n - k;
+  const bool staged = n <= kSmemN;
   const int* act = tk.act;
   const int* perm = tk.perm;
   const int* bid = tk.bid;
   const int* bpos = tk.bpos;
   const double* T = tk.T;
-  double* K = tk.K;
-  double* Krs = tk.Krs;
+  double* K = staged ? kbuf : tk.K;
   double* L = tk.L;
   double* U = tk.U;
   double* X = tk.X;
@@ -61,34 +67,39 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   const double* Krs_in = K + k;
   const double* Ksr = K + static_cast<long long>(n) * k;
   const double* Krr = K + k + static_cast<long long>(n) * k;
-  // K_r_sn = K_rs - T^T K_ss            (r x k)
-  cta_gemm_sub(Krs, r, Krs_in, n, T, k, true, Kss, n, false, r, k, k);
-  // K_sn_r = K_sr - K_ss T  -> L buffer  (k x r)
-  cta_gemm_sub(L, k, Ksr, n, Kss, n, false, T, k, false, k, r, k);
-  // X = K_rr - T^T K_sr                  (r x r)
-  cta_gemm_sub(X, r, Krr, n, T, k, true, Ksr, n, false, r, r, k);
-  __syncthreads();
-  // X -= K_r_sn T
-  cta_gemm_sub(X, r, X, r, Krs, r, false, T, k, false, r, r, k);
-  __syncthreads();
-  const int info = cta_lu(X, r, r, piv, red);
+  // K_r_sn = K_rs - T^T K_ss   (r x k), kept in the U buffer until the end
+  cta_gemm_tiled(U, r, Krs_in, n, T, k, true, Kss, n, false, r, k, k, tile);
+  // K_sn_r = K_sr - K_ss T     (k x r), in the L buffer
+  cta_gemm_tiled(L, k, Ksr, n, Kss, n, false, T, k, false, k, r, k, tile);
+  // X = (K_rr - T^T K_sr) - K_r_sn T
+  cta_gemm_tiled(X, r, Krr, n, T, k, true, Ksr, n, false, r, r, k, tile);
+  cta_gemm_tiled(X, r, X, r, U, r, false, T, k, false, r, r, k, tile);
+  // LU of X_rr, in shared memory when it fits (K is no longer needed)
+  double* Xw = X;
+  if (staged) {
+    Xw = kbuf;
+    for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e] = X[e];
+    __syncthreads();
+  }
+  const int info = cta_lu(Xw, r, r, piv, red);
   if (info && threadIdx.x == 0) atomicExch(P.status, 1);
-  // U = X^{-1} K_r_sn (columns), L = K_sn_r X^{-1} (rows, through X^T)
-  for (int e = threadIdx.x; e < r * k; e += kDecThreads) U[e] = Krs[e];
+  if (staged) {
+    for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e];
+  }
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // L = K_sn_r X^{-1}, row by row through X^T
+  const int warp = threadIdx.x >> 5;
   const int nw = kDecThreads / 32;
-  for (int c = warp; c < k; c += nw) warp_lu_solve(X, r, r, piv, U + static_cast<long long>(r) * c, 1);
-  for (int row = warp; row < k; row += nw) warp_lu_solve_t(X, r, r, piv, L + row, k);
+  for (int row = warp; row < k; row += nw) warp_lu_solve_t(Xw, r, r, piv, L + row, k);
   __syncthreads();
   // acc = update(s, s) + L K_r_sn
+  cta_gemm_tiled(acc, k, nullptr, 0, L, k, false, U, r, false, k, k, r, tile);
   for (int e = threadIdx.x; e < k * k; e += kDecThreads) {
     const int i = e % k, j = e / k;
-    double s = 0.0;
-    for (int l = 0; l < r; l++) s += L[i + static_cast<long long>(k) * l] * Krs[l + static_cast<long long>(r) * j];
-    acc[e] = upd_lookup(bid, bpos, tk.blocks, perm[i], perm[j]) + s;
+    acc[e] = upd_lookup(bid, bpos, tk.blocks, perm[i], perm[j]) - acc[e];
   }
-  (void)lane;
+  // U = X^{-1} K_r_sn, column by column
+  for (int c = warp; c < k; c += nw) warp_lu_solve(Xw, r, r, piv, U + static_cast<long long>(r) * c, 1);
 }
 
 __global__ void assemble_top_kernel(int pde, const Node* nodes, const int* dofs, int n,
@@ -103,9 +114,19 @@ __global__ void assemble_top_kernel(int pde, const Node* nodes, const int* dofs,
 
 }  // namespace
 
-cudaError_t launch_decouple(const DecParams& p, cudaStream_t s) {
+size_t decouple_smem_bytes(int n_max) {
+  const int ns = n_max < kSmemN ? n_max : kSmemN;
+  return sizeof(double) * (kGemmTileDoubles + 64 + static_cast<size_t>(ns) * ns);
+}
+
+cudaError_t launch_decouple(const DecParams& p, int n_max, cudaStream_t s) {
   if (p.ntasks == 0) return cudaSuccess;
-  decouple_kernel<<<p.ntasks, kDecThreads, 0, s>>>(p);
+  const size_t smem = decouple_smem_bytes(n_max);
+  cudaError_t e = cudaFuncSetAttribute(decouple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  count_launches(1);
+  decouple_kernel<<<p.ntasks, kDecThreads, smem, s>>>(p);
   return cudaGetLastError();
 }
 
@@ -116,6 +137,7 @@ cudaError_t launch_assemble_top(int pde, const Node* nodes, const int* dofs, int
   const long long total = static_cast<long long>(n) * n;
   const int threads = 256;
   const int grid = static_cast<int>((total + threads - 1) / threads);
+  count_launches(1);
   assemble_top_kernel<<<grid, threads, 0, s>>>(pde, nodes, dofs, n, bid, bpos, blocks, out,
                                                 ld);
   return cudaGetLastError();

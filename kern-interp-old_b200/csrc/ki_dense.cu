@@ -8,10 +8,19 @@
 // interchanges are applied to the other columns, U12 = L11^{-1} A12 is formed
 // per column, and the trailing matrix is updated by a tiled GEMM spread over
 // the whole GPU.
+#include <atomic>
+
 #include "ki_blockla.cuh"
 #include "ki_kernels.h"
 
 namespace kib {
+
+namespace {
+std::atomic<long long> g_launches{0};
+}  // namespace
+
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_total() { return g_launches.load(std::memory_order_relaxed); }
 
 namespace {
 
@@ -203,11 +212,42 @@ __global__ void gemm_kernel(bool ta, bool tb, int m, int n, int k, double alpha,
   *cp = alpha * s + (beta == 0.0 ? 0.0 : beta * *cp);
 }
 
+// C(i, j) = alpha * sum_l A(l, i) B(l, j) + beta C(i, j) for a long inner
+// dimension: one CTA per output entry, strided partial sums, block reduce.
+__global__ void __launch_bounds__(256) gemm_tn_long_kernel(int m, int k, double alpha,
+                                                           const double* a, int lda,
+                                                           const double* b, int ldb,
+                                                           double beta, double* c, int ldc) {
+  __shared__ double red[8];
+  const int i = blockIdx.x % m, j = blockIdx.x / m;
+  const double* ac = a + static_cast<long long>(lda) * i;
+  const double* bc = b + static_cast<long long>(ldb) * j;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int l = threadIdx.x;
+  for (; l + 768 < k; l += 1024) {
+    s0 += ac[l] * bc[l];
+    s1 += ac[l + 256] * bc[l + 256];
+    s2 += ac[l + 512] * bc[l + 512];
+    s3 += ac[l + 768] * bc[l + 768];
+  }
+  for (; l < k; l += 256) s0 += ac[l] * bc[l];
+  double t = warp_sum_d((s0 + s1) + (s2 + s3));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < 8; w++) v += red[w];
+    double* cp = c + i + static_cast<long long>(ldc) * j;
+    *cp = alpha * v + (beta == 0.0 ? 0.0 : beta * *cp);
+  }
+}
+
 }  // namespace
 
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s) {
   for (int j0 = 0; j0 < n; j0 += kNb) {
     const int w = min(kNb, n - j0);
+    count_launches(n - j0 - w > 0 ? 4 : 2);
     panel_lu_kernel<<<1, 1024, 0, s>>>(a, n, ld, j0, w, ipiv, status);
     swap_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w, ipiv);
     const int right = n - j0 - w;
@@ -224,6 +264,7 @@ cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, dou
                            int nrhs, int ldb, cudaStream_t s) {
   if (n == 0 || nrhs == 0) return cudaSuccess;
   const int per = 4;
+  count_launches(1);
   lu_solve_kernel<<<(nrhs + per - 1) / per, 32 * per, 0, s>>>(lu, n, ld, ipiv, b, nrhs, ldb);
   return cudaGetLastError();
 }
@@ -232,6 +273,7 @@ cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int n
                           double* out, int ldo, cudaStream_t s) {
   const long long tot = static_cast<long long>(n) * nrhs;
   if (tot == 0) return cudaSuccess;
+  count_launches(1);
   gather_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(x, ldx, idx, n, nrhs, out, ldo);
   return cudaGetLastError();
 }
@@ -240,6 +282,7 @@ cudaError_t launch_scatter(double* x, int ldx, const int* idx, int n, int nrhs,
                            const double* in, int ldi, cudaStream_t s) {
   const long long tot = static_cast<long long>(n) * nrhs;
   if (tot == 0) return cudaSuccess;
+  count_launches(1);
   scatter_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(x, ldx, idx, n, nrhs, in, ldi);
   return cudaGetLastError();
 }
@@ -249,6 +292,12 @@ cudaError_t small_gemm(bool ta, bool tb, int m, int n, int k, double alpha, cons
                        cudaStream_t s) {
   const long long tot = static_cast<long long>(m) * n;
   if (tot == 0) return cudaSuccess;
+  count_launches(1);
+  if (ta && !tb && k > 2048 && tot <= 65536) {
+    gemm_tn_long_kernel<<<static_cast<int>(tot), 256, 0, s>>>(m, k, alpha, a, lda, b, ldb, beta,
+                                                              c, ldc);
+    return cudaGetLastError();
+  }
   gemm_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(ta, tb, m, n, k, alpha, a, lda,
                                                                   b, ldb, beta, c, ldc);
   return cudaGetLastError();
@@ -283,6 +332,7 @@ cudaError_t launch_fill_border(double* S, int ld, int ns, int nb, const double* 
                                const double* ps, const double* corr, cudaStream_t s) {
   const int tot = ns * nb + nb * nb;
   if (tot == 0) return cudaSuccess;
+  count_launches(1);
   fill_border_kernel<<<(tot + 255) / 256, 256, 0, s>>>(S, ld, ns, nb, us, ps, corr);
   return cudaGetLastError();
 }

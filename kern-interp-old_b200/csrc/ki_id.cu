@@ -94,6 +94,45 @@ __device__ __forceinline__ double lapy2(double x, double y) {
   return w * sqrt(1.0 + q * q);
 }
 
+// Column pass helpers: four independent loads in flight per lane.
+__device__ __forceinline__ double col_dot(const double* __restrict__ col,
+                                          const double* __restrict__ v, int r0, int m) {
+  double w0 = 0.0, w1 = 0.0;
+  int r = r0;
+  for (; r + 96 < m; r += 128) {
+    const double a0 = col[r], a1 = col[r + 32], a2 = col[r + 64], a3 = col[r + 96];
+    w0 += v[r] * a0 + v[r + 64] * a2;
+    w1 += v[r + 32] * a1 + v[r + 96] * a3;
+  }
+  for (; r < m; r += 32) w0 += v[r] * col[r];
+  return w0 + w1;
+}
+
+__device__ __forceinline__ void col_axpy(double* __restrict__ col, const double* __restrict__ v,
+                                         int r0, int m, double t) {
+  int r = r0;
+  for (; r + 96 < m; r += 128) {
+    const double a0 = col[r], a1 = col[r + 32], a2 = col[r + 64], a3 = col[r + 96];
+    col[r] = a0 + v[r] * t;
+    col[r + 32] = a1 + v[r + 32] * t;
+    col[r + 64] = a2 + v[r + 64] * t;
+    col[r + 96] = a3 + v[r + 96] * t;
+  }
+  for (; r < m; r += 32) col[r] += v[r] * t;
+}
+
+__device__ __forceinline__ double col_sumsq(const double* __restrict__ col, int r0, int m) {
+  double s0 = 0.0, s1 = 0.0;
+  int r = r0;
+  for (; r + 96 < m; r += 128) {
+    const double a0 = col[r], a1 = col[r + 32], a2 = col[r + 64], a3 = col[r + 96];
+    s0 += a0 * a0 + a2 * a2;
+    s1 += a1 * a1 + a3 * a3;
+  }
+  for (; r < m; r += 32) s0 += col[r] * col[r];
+  return s0 + s1;
+}
+
 template <int G>
 __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -104,22 +143,66 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  double* v = reinterpret_cast<double*>(smem_raw);   // m_cap
-  double* rdiag = v + P.m_cap;                        // n_cap
-  double* vn1 = rdiag + P.n_cap;                      // n_cap
+  double* v = reinterpret_cast<double*>(smem_raw);   // m_cap: Householder vector
+  double* rdiag = v + P.m_cap;                        // n_cap: R_ii
+  double* vn1 = rdiag + P.n_cap;                      // n_cap: partial norms (physical)
   double* vn2 = vn1 + P.n_cap;                        // n_cap
   double* red = vn2 + P.n_cap;                        // 32
-  double* sc = red + 32;                              // scalars
-  Cand* slot = reinterpret_cast<Cand*>(sc + 8);       // 2
+  Cand* wbest = reinterpret_cast<Cand*>(red + 32);    // kIdWarps
+  Cand* slot = wbest + kIdWarps;                      // 2 (cluster exchange)
   int* pos2col = reinterpret_cast<int*>(slot + 2);    // n_cap
   int* own = pos2col + P.n_cap;                       // n_cap
-  int* si = own + P.n_cap;                            // int scalars
+  int* si = own + P.n_cap;                            // [0] own count, [1] pivot column
 
   double* A = P.work + tk.a_off;
   const int* act = P.act + tk.act_off;
   const int* rowd = P.rowdofs + tk.row_off;
   const Node* nodes = P.nodes;
   const int pde = P.pde;
+  const int mn = min(m, n);
+
+  // Warp 0: choose the pivot for step i from the candidates (own CTA's warp
+  // bests for G == 1, every CTA's slot otherwise), swap it into position i
+  // and list this CTA's columns at positions > i.
+  auto select_pivot = [&](int i, bool from_slots) {
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    if (from_slots) {
+      if (lane < G) {
+        Cand c;
+        if constexpr (G > 1) {
+          c = cg::this_cluster().map_shared_rank(slot, lane)[i & 1];
+        } else {
+          c = slot[i & 1];
+        }
+        bv = c.val;
+        bp = c.pos;
+      }
+    } else if (lane < kIdWarps) {
+      bv = wbest[lane].val;
+      bp = wbest[lane].pos;
+    }
+    warp_best(bv, bp);
+    const int pvt = bp;
+    const int ci = pos2col[i];
+    const int cp = pos2col[pvt];
+    __syncwarp();
+    if (lane == 0) {
+      pos2col[i] = cp;
+      pos2col[pvt] = ci;
+      si[1] = cp;
+    }
+    __syncwarp();
+    int cnt = 0;
+    for (int base = i + 1; base < n; base += 32) {
+      const int p = base + lane;
+      const bool mine = p < n && (pos2col[p] % G == g);
+      const unsigned bal = __ballot_sync(0xffffffffu, mine);
+      if (mine) own[cnt + __popc(bal & ((1u << lane) - 1u))] = p;
+      cnt += __popc(bal);
+    }
+    if (lane == 0) si[0] = cnt;
+  };
 
   // ---- generation of the owned columns + their initial norms
   for (int t = warp; g + G * t < n; t += kIdWarps) {
@@ -147,108 +230,94 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   }
   for (int p = threadIdx.x; p < n; p += kIdThreads) pos2col[p] = p;
   __syncthreads();
-  if (warp == 0) {
+  {
     double bv = -1.0;
     int bp = 0x7fffffff;
-    for (int p = lane; p < n; p += 32) {
-      if (p % G == g && better(vn1[p], p, bv, bp)) {
-        bv = vn1[p];
-        bp = p;
+    for (int t = warp; g + G * t < n; t += kIdWarps) {
+      const int j = g + G * t;
+      if (better(vn1[j], j, bv, bp)) {
+        bv = vn1[j];
+        bp = j;
       }
     }
-    warp_best(bv, bp);
-    if (lane == 0) slot[0] = Cand{bv, bp, 0};
+    if (lane == 0) wbest[warp] = Cand{bv, bp, 0};
   }
+  __syncthreads();
   if constexpr (G > 1) {
+    if (warp == 0) {
+      double bv = lane < kIdWarps ? wbest[lane].val : -1.0;
+      int bp = lane < kIdWarps ? wbest[lane].pos : 0x7fffffff;
+      warp_best(bv, bp);
+      if (lane == 0) slot[0] = Cand{bv, bp, 0};
+    }
     cg::this_cluster().sync();
-  } else {
-    __syncthreads();
   }
+  if (warp == 0 && mn > 0) select_pivot(0, G > 1);
+  __syncthreads();
 
   const double tol3z = sqrt(0.5 * 2.220446049250313e-16);
-  const int mn = min(m, n);
   int rank = 0;
   double thresh = 0.0;
   for (int i = 0; i < mn; i++) {
-    // ---- pivot: best candidate over the cluster
-    if (warp == 0) {
-      double bv = -1.0;
-      int bp = 0x7fffffff;
-      if (lane < G) {
-        Cand c;
-        if constexpr (G > 1) {
-          Cand* peer = cg::this_cluster().map_shared_rank(slot, lane);
-          c = peer[i & 1];
-        } else {
-          c = slot[i & 1];
-        }
-        bv = c.val;
-        bp = c.pos;
-      }
-      warp_best(bv, bp);
-      if (lane == 0) {
-        const int pvt = bp;
-        const int tmp = pos2col[i];
-        pos2col[i] = pos2col[pvt];
-        pos2col[pvt] = tmp;
-      }
-    }
-    __syncthreads();
-    const int c = pos2col[i];
+    const int c = si[1];
     const double* colc = A + static_cast<long long>(c) * lda;
-    // ---- Householder reflector of the pivot column (redundantly per CTA)
+    // ---- Householder reflector of the pivot column (redundantly per CTA);
+    // the column's rows below the diagonal are staged in v as they are read.
     double part = 0.0;
-    for (int r = i + 1 + threadIdx.x; r < m; r += kIdThreads) {
-      const double a = colc[r];
-      part += a * a;
-    }
-    const double xnorm = sqrt(block_sum(part, red));
-    if (threadIdx.x == 0) {
-      const double alpha = colc[i];
-      double beta = alpha, tau = 0.0, scal = 0.0;
-      if (i < m - 1 && xnorm != 0.0) {
-        beta = -copysign(lapy2(alpha, xnorm), alpha);
-        tau = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
+    {
+      int r = i + 1 + threadIdx.x;
+      for (; r + 3 * kIdThreads < m; r += 4 * kIdThreads) {
+        const double a0 = colc[r], a1 = colc[r + kIdThreads];
+        const double a2 = colc[r + 2 * kIdThreads], a3 = colc[r + 3 * kIdThreads];
+        v[r] = a0;
+        v[r + kIdThreads] = a1;
+        v[r + 2 * kIdThreads] = a2;
+        v[r + 3 * kIdThreads] = a3;
+        part += (a0 * a0 + a1 * a1) + (a2 * a2 + a3 * a3);
       }
-      rdiag[i] = beta;
-      sc[0] = tau;
-      sc[1] = scal;
-      if (i == 0) sc[2] = fabs(P.tol * beta);
+      for (; r < m; r += kIdThreads) {
+        const double a0 = colc[r];
+        v[r] = a0;
+        part += a0 * a0;
+      }
     }
+    part = warp_sum(part);
+    if (lane == 0) red[warp] = part;
     __syncthreads();
-    const double tau = sc[0], scal = sc[1];
-    thresh = sc[2];
-    if (i >= 1 && fabs(rdiag[i]) < thresh) {
+    double xs = 0.0;
+#pragma unroll
+    for (int w = 0; w < kIdWarps; w++) xs += red[w];
+    const double xnorm = sqrt(xs);
+    const double alpha = colc[i];
+    double beta = alpha, tau = 0.0, scal = 0.0;
+    if (i < m - 1 && xnorm != 0.0) {
+      beta = -copysign(lapy2(alpha, xnorm), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    if (i == 0) thresh = fabs(P.tol * beta);
+    if (i >= 1 && fabs(beta) < thresh) {
       rank = i;
       break;
     }
-    for (int r = i + 1 + threadIdx.x; r < m; r += kIdThreads) v[r] = colc[r] * scal;
-    if (threadIdx.x == 0) v[i] = 1.0;
-    // ---- compact list of this CTA's trailing columns (positions > i)
-    if (warp == 0) {
-      int cnt = 0;
-      for (int base = i + 1; base < n; base += 32) {
-        const int p = base + lane;
-        const bool mine = p < n && (pos2col[p] % G == g);
-        const unsigned bal = __ballot_sync(0xffffffffu, mine);
-        if (mine) own[cnt + __popc(bal & ((1u << lane) - 1u))] = p;
-        cnt += __popc(bal);
-      }
-      if (lane == 0) si[0] = cnt;
+    if (threadIdx.x == 0) {
+      rdiag[i] = beta;
+      v[i] = 1.0;
     }
+    for (int r = i + 1 + threadIdx.x; r < m; r += kIdThreads) v[r] *= scal;
     __syncthreads();
+    // ---- apply H to the owned trailing columns, downdate their norms and
+    // track this warp's best candidate for the next pivot
     const int nown = si[0];
-    // ---- apply H to the owned trailing columns, downdate their norms
+    double bv = -1.0;
+    int bp = 0x7fffffff;
     for (int t = warp; t < nown; t += kIdWarps) {
-      const int j = pos2col[own[t]];
+      const int p = own[t];
+      const int j = pos2col[p];
       double* col = A + static_cast<long long>(j) * lda;
       if (tau != 0.0) {
-        double w = 0.0;
-        for (int r = i + lane; r < m; r += 32) w += v[r] * col[r];
-        w = warp_sum(w);
-        const double tw = -tau * w;
-        for (int r = i + lane; r < m; r += 32) col[r] += v[r] * tw;
+        const double w = warp_sum(col_dot(col, v, i + lane, m));
+        col_axpy(col, v, i + lane, m, -tau * w);
       }
       __syncwarp();
       const double aij = col[i];
@@ -267,33 +336,29 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
         }
       }
       if (recompute) {
-        double ss = 0.0;
-        for (int r = i + 1 + lane; r < m; r += 32) ss += col[r] * col[r];
-        ss = warp_sum(ss);
+        const double ss = warp_sum(col_sumsq(col, i + 1 + lane, m));
         nv1 = (i < m - 1) ? sqrt(ss) : 0.0;
         if (lane == 0) vn2[j] = nv1;
       }
       if (lane == 0) vn1[j] = nv1;
-    }
-    __syncthreads();
-    // ---- this CTA's best candidate for step i + 1
-    if (warp == 0) {
-      double bv = -1.0;
-      int bp = 0x7fffffff;
-      for (int t = lane; t < nown; t += 32) {
-        const int p = own[t];
-        const double val = vn1[pos2col[p]];
-        if (better(val, p, bv, bp)) {
-          bv = val;
-          bp = p;
-        }
+      if (better(nv1, p, bv, bp)) {
+        bv = nv1;
+        bp = p;
       }
-      warp_best(bv, bp);
-      if (lane == 0) slot[(i + 1) & 1] = Cand{bv, bp, 0};
     }
-    if constexpr (G > 1) {
-      cg::this_cluster().sync();
-    } else {
+    if (lane == 0) wbest[warp] = Cand{bv, bp, 0};
+    __syncthreads();
+    if (i + 1 < mn) {
+      if constexpr (G > 1) {
+        if (warp == 0) {
+          double cv = lane < kIdWarps ? wbest[lane].val : -1.0;
+          int cpos = lane < kIdWarps ? wbest[lane].pos : 0x7fffffff;
+          warp_best(cv, cpos);
+          if (lane == 0) slot[(i + 1) & 1] = Cand{cv, cpos, 0};
+        }
+        cg::this_cluster().sync();
+      }
+      if (warp == 0) select_pivot(i + 1, G > 1);
       __syncthreads();
     }
   }
@@ -359,12 +424,13 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 }  // namespace
 
 size_t id_smem_bytes(int m_cap, int n_cap) {
-  return sizeof(double) * (static_cast<size_t>(m_cap) + 3 * n_cap + 32 + 8) +
-         sizeof(Cand) * 2 + sizeof(int) * (2 * static_cast<size_t>(n_cap) + 8);
+  return sizeof(double) * (static_cast<size_t>(m_cap) + 3 * n_cap + 32) +
+         sizeof(Cand) * (kIdWarps + 2) + sizeof(int) * (2 * static_cast<size_t>(n_cap) + 8);
 }
 
 cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s) {
   if (p.ntasks == 0) return cudaSuccess;
+  count_launches(1);
   switch (group) {
     case 1: return launch_g<1>(p, s);
     case 2: return launch_g<2>(p, s);

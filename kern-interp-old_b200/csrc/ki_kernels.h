@@ -8,6 +8,11 @@
 
 namespace kib {
 
+// Number of kernels this library has launched in the process (every launch
+// wrapper below adds its launches).
+void count_launches(int n);
+long long launch_total();
+
 // ---------------------------------------------------------------- ID
 // One interpolative decomposition (Kernel::get_id_mat + ki_Mat::id,
 // kernel.cpp:153-235, ki_mat.cpp:502-541).  Rows of the ID matrix:
@@ -68,8 +73,7 @@ struct DecTask {
   const int* bpos;       // per active position: row inside that block
   const UpdBlock* blocks;
   const double* T;       // k x r, ld k (from the ID)
-  double* K;             // scratch n x n
-  double* Krs;           // scratch r x k (K_r_sn)
+  double* K;             // scratch n x n (boxes too large for shared memory)
   double* L;             // k x r, ld k
   double* U;             // r x k, ld r
   double* X;             // LU of X_rr, r x r, ld r
@@ -85,7 +89,8 @@ struct DecParams {
   int* status;  // set nonzero on an exactly zero pivot
 };
 
-cudaError_t launch_decouple(const DecParams& p, cudaStream_t s);
+// n_max: largest box of the launch (sizes the shared-memory staging).
+cudaError_t launch_decouple(const DecParams& p, int n_max, cudaStream_t s);
 
 // Dense assembly of the top-level skeleton matrix K(allskel, allskel) minus
 // the accumulated updates (skel_factorization.cpp:116-122), n x n, ld ld.

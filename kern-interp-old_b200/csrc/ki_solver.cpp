@@ -156,6 +156,41 @@ Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
 
 Solver::~Solver() = default;
 
+int Solver::timer_begin(cudaEvent_t* e0) {
+  if (cuda_check(cudaEventCreate(e0), "cudaEventCreate")) return -2;
+  return cuda_check(cudaEventRecord(*e0, stream_), "cudaEventRecord");
+}
+
+int Solver::timer_end(cudaEvent_t e0, const LaunchRecord& rec) {
+  cudaEvent_t e1;
+  if (cuda_check(cudaEventCreate(&e1), "cudaEventCreate")) return -2;
+  if (cuda_check(cudaEventRecord(e1, stream_), "cudaEventRecord")) return -2;
+  pending_.push_back({e0, e1, rec});
+  return 0;
+}
+
+int Solver::timers_resolve() {
+  for (PendingTimer& p : pending_) {
+    float ms = 0;
+    if (cuda_check(cudaEventElapsedTime(&ms, p.e0, p.e1), "cudaEventElapsedTime")) return -2;
+    LaunchRecord r = p.rec;
+    r.ms = ms;
+    if (r.kind == 0) {
+      t_id_ms += ms;
+      id_launches++;
+    } else if (r.kind == 1) {
+      t_decouple_ms += ms;
+    } else {
+      t_top_ms += ms;
+    }
+    launch_log.push_back(r);
+    cudaEventDestroy(p.e0);
+    cudaEventDestroy(p.e1);
+  }
+  pending_.clear();
+  return 0;
+}
+
 int Solver::fail(const std::string& msg) {
   error = msg;
   return -1;
@@ -275,24 +310,11 @@ int Solver::factor() {
   }
   for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
   allskel = tree.boxes[0].active;
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
-  if (time_phases) {
-    KI_CUDA(cudaEventCreate(&t0));
-    KI_CUDA(cudaEventCreate(&t1));
-    KI_CUDA(cudaEventRecord(t0, stream_));
-  }
+  cudaEvent_t t0 = nullptr;
+  if (time_phases && timer_begin(&t0)) return -2;
   int rc = factor_top();
   if (rc) return rc;
-  if (time_phases) {
-    KI_CUDA(cudaEventRecord(t1, stream_));
-    KI_CUDA(cudaEventSynchronize(t1));
-    float ms = 0;
-    KI_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-    t_top_ms = ms;
-    launch_log.push_back({0, 2, 1, 1, 0, ns_ + nb_, ms});
-    cudaEventDestroy(t0);
-    cudaEventDestroy(t1);
-  }
+  if (time_phases && timer_end(t0, {0, 2, 1, 1, 0, ns_ + nb_, 0.0})) return -2;
 
   int status = 0;
   KI_CUDA(cudaMemcpyAsync(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
@@ -303,6 +325,7 @@ int Solver::factor() {
   t_factor_ms = ms;
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
+  if (timers_resolve()) return -2;
   if (status) return fail("zero pivot in an LU factorization (singular block)");
   return 0;
 }
@@ -401,11 +424,6 @@ int Solver::process_level(int level) {
   KI_CUDA(upload(d_rows, rows, stream_));
   KI_CUDA(upload(d_tasks, tasks, stream_));
 
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (time_phases) {
-    KI_CUDA(cudaEventCreate(&e0));
-    KI_CUDA(cudaEventCreate(&e1));
-  }
   // one launch per cluster size
   for (int q0 = 0; q0 < nc;) {
     int q1 = q0;
@@ -433,22 +451,13 @@ int Solver::process_level(int level) {
     p.tol = opt_.id_tol;
     p.m_cap = m_cap;
     p.n_cap = n_cap;
-    if (time_phases) KI_CUDA(cudaEventRecord(e0, stream_));
+    cudaEvent_t e0 = nullptr;
+    if (time_phases && timer_begin(&e0)) return -2;
     KI_CUDA(launch_id(p, cand[q0].g, stream_));
     if (time_phases) {
-      KI_CUDA(cudaEventRecord(e1, stream_));
-      KI_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      KI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      t_id_ms += ms;
-      id_launches++;
-      launch_log.push_back({level, 0, cand[q0].g, q1 - q0, m_cap, n_cap, ms});
+      if (timer_end(e0, {level, 0, cand[q0].g, q1 - q0, m_cap, n_cap, 0.0})) return -2;
     }
     q0 = q1;
-  }
-  if (time_phases) {
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
   }
   std::vector<int> rank(nc), perm(perm_total);
   KI_CUDA(cudaMemcpyAsync(rank.data(), d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
@@ -495,7 +504,8 @@ int Solver::process_level(int level) {
   std::vector<UpdBlock> tab;
   std::vector<long long> bid_off(ncomp), tab_off(ncomp);
   long long scratch_total = 0;
-  std::vector<long long> k_off(ncomp), krs_off(ncomp);
+  std::vector<long long> k_off(ncomp);
+  int n_max = 0;
   size_t fac_total = 0, piv_total = 0;
   for (int t = 0; t < ncomp; t++) {
     const Cand& c = cand[comp[t]];
@@ -515,9 +525,8 @@ int Solver::process_level(int level) {
     }
     build_block_map(blocks, n, &bid, &bpos, &tab);
     k_off[t] = scratch_total;
-    scratch_total += static_cast<long long>(n) * n;
-    krs_off[t] = scratch_total;
-    scratch_total += static_cast<long long>(r) * k;
+    if (n > 160) scratch_total += static_cast<long long>(n) * n;
+    n_max = std::max(n_max, n);
     fac_total += static_cast<size_t>(k) * r * 2 + static_cast<size_t>(r) * r +
                  static_cast<size_t>(k) * k;
     piv_total += r;
@@ -532,7 +541,7 @@ int Solver::process_level(int level) {
   KI_ALLOC(d_fac, double, fac_total);
   KI_ALLOC(d_piv, int, piv_total);
   KI_ALLOC(d_dt, DecTask, ncomp);
-  KI_CUDA(scratch2_.reserve(sizeof(double) * scratch_total, stream_));
+  KI_CUDA(scratch2_.reserve(sizeof(double) * (scratch_total + 1), stream_));
   double* scr = static_cast<double*>(scratch2_.p);
   size_t fo = 0, po = 0;
   for (int t = 0; t < ncomp; t++) {
@@ -561,7 +570,6 @@ int Solver::process_level(int level) {
     d.blocks = d_tab + tab_off[t];
     d.T = bd.T;
     d.K = scr + k_off[t];
-    d.Krs = scr + krs_off[t];
     d.L = bd.L;
     d.U = bd.U;
     d.X = bd.X;
@@ -578,25 +586,10 @@ int Solver::process_level(int level) {
   dp.pde = opt_.pde;
   dp.nodes = d_nodes_;
   dp.status = d_status_;
-  cudaEvent_t d0 = nullptr, d1 = nullptr;
-  if (time_phases) {
-    KI_CUDA(cudaEventCreate(&d0));
-    KI_CUDA(cudaEventCreate(&d1));
-    KI_CUDA(cudaEventRecord(d0, stream_));
-  }
-  KI_CUDA(launch_decouple(dp, stream_));
-  if (time_phases) {
-    KI_CUDA(cudaEventRecord(d1, stream_));
-    KI_CUDA(cudaEventSynchronize(d1));
-    float ms = 0;
-    KI_CUDA(cudaEventElapsedTime(&ms, d0, d1));
-    t_decouple_ms += ms;
-    int nmax = 0;
-    for (int t = 0; t < ncomp; t++) nmax = std::max(nmax, cand[comp[t]].n);
-    launch_log.push_back({level, 1, 1, ncomp, 0, nmax, ms});
-    cudaEventDestroy(d0);
-    cudaEventDestroy(d1);
-  }
+  cudaEvent_t d0 = nullptr;
+  if (time_phases && timer_begin(&d0)) return -2;
+  KI_CUDA(launch_decouple(dp, n_max, stream_));
+  if (time_phases && timer_end(d0, {level, 1, 1, ncomp, 0, n_max, 0.0})) return -2;
 
   // ---- sweep descriptors of the level
   std::vector<int> sk, rd;

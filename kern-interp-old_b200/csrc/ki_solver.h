@@ -113,6 +113,16 @@ class Solver {
   std::string error;
 
  private:
+  // Event pairs of the timed factorization, resolved after its final
+  // synchronisation so timing adds no extra waits.
+  struct PendingTimer {
+    cudaEvent_t e0, e1;
+    LaunchRecord rec;
+  };
+  std::vector<PendingTimer> pending_;
+  int timer_begin(cudaEvent_t* e0);
+  int timer_end(cudaEvent_t e0, const LaunchRecord& rec);
+  int timers_resolve();
   int fail(const std::string& msg);
   int cuda_check(cudaError_t e, const char* what);
   int process_level(int level);

@@ -41,6 +41,7 @@ def load():
         raise KiError("libkinterp.so not built: run kern-interp-old_b200/build.py")
     lib = C.CDLL(LIB_PATH)
     lib.ki_last_error.restype = C.c_char_p
+    lib.ki_kernel_launches.restype = C.c_longlong
     fac_args = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int, _dp, C.c_int, C.c_double,
                 C.c_void_p, C.POINTER(C.c_void_p)]
     for name in ("ki_factor", "ki_factor_timed"):
@@ -64,6 +65,11 @@ def load():
     lib.ki_launch_log.argtypes = [C.c_void_p, _dp, C.c_int]
     _lib = lib
     return lib
+
+
+def kernel_launches():
+    """Kernels launched by the library so far in this process."""
+    return int(load().ki_kernel_launches())
 
 
 def _d(a):
