@@ -122,6 +122,31 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
                     const double* holes, int max_leaf_dofs, double id_tol, void* stream,
                     ki_solver_t* out);
 
+/* Interpolative decomposition of one box that allocates no device memory,
+ * for callers that cannot call cudaMalloc (their device memory is owned by
+ * another allocator, such as a framework's caching allocator or a pool
+ * reserved up front, and a cudaMalloc/cudaFree would also synchronise the
+ * device).  No counterpart in the reference: it is the per-box step of
+ * skeletonize (Kernel::get_id_mat + ki_Mat::id) exposed on its own.
+ *
+ * Device inputs: d_nodes holds n_points records of 8 doubles (x, y, n_x,
+ * n_y, weight, curvature, 0, 0); d_active the n_active column dofs; d_rows
+ * the n_rows near dofs.  The ID matrix is [K(rows, active); K(active,
+ * rows)^T], followed, when proxy is nonzero, by the 128-point proxy-circle
+ * rows of centre (cx, cy) and the given radius (256 rows for Laplace, 512
+ * for Stokes).  Device outputs: *d_rank (0: not compressible), d_perm
+ * (n_active pivots, active positions), d_T (k x (n_active - k), ld k;
+ * capacity n_active^2 / 4 + 1 doubles).
+ * The m x n working matrix lives in one static 8 MiB device array: calls
+ * with ((m + 3) / 4 * 4) * n_active > 1048576 are rejected with KI_ERR_ARG.
+ * The first call on a device resolves that array's address (make it before
+ * any stream capture).  All calls share the array: calls that overlap on the
+ * GPU race.  Stream ordered; returns without synchronising. */
+int ki_id_noalloc(int pde, const double* d_nodes, int n_points, const int* d_active,
+                  int n_active, const int* d_rows, int n_rows, int proxy, double cx,
+                  double cy, double radius, double id_tol, int* d_rank, int* d_perm,
+                  double* d_T, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -341,4 +341,31 @@ int ki_stats(ki_solver_t s, double* out, int n) {
   return cnt;
 }
 
+int ki_id_noalloc(int pde, const double* d_nodes, int n_points, const int* d_active,
+                  int n_active, const int* d_rows, int n_rows, int proxy, double cx,
+                  double cy, double radius, double id_tol, int* d_rank, int* d_perm,
+                  double* d_T, void* stream) {
+  if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_id_noalloc: bad pde");
+  if (!d_nodes || n_points <= 0 || !d_active || n_active <= 0 || n_rows < 0 ||
+      (n_rows > 0 && !d_rows) || !d_rank || !d_perm || !d_T)
+    return set_err(KI_ERR_ARG, "ki_id_noalloc: bad arguments");
+  if (!(id_tol > 0)) return set_err(KI_ERR_ARG, "id_tol must be greater than 0");
+  const int proxy_rows = proxy ? (pde == KI_STOKES ? 4 : 2) * kib::kNumProxy : 0;
+  const long long m = 2LL * n_rows + proxy_rows;
+  if (m == 0) return set_err(KI_ERR_ARG, "ki_id_noalloc: the ID matrix has no rows");
+  const long long lda = (m + 3) / 4 * 4;
+  if (lda * n_active > kib::kNoAllocScratchDoubles)
+    return set_err(KI_ERR_ARG, "ki_id_noalloc: the " + std::to_string(m) + " x " +
+                                   std::to_string(n_active) +
+                                   " ID matrix exceeds the 8 MiB static scratch "
+                                   "(1048576 doubles, rows padded to a multiple of 4)");
+  if (kib::id_smem_bytes(static_cast<int>(m), n_active) > 227 * 1024)
+    return set_err(KI_ERR_ARG, "ki_id_noalloc: too many rows for the shared staging");
+  return cuda_err(kib::launch_id_noalloc(pde, reinterpret_cast<const kib::Node*>(d_nodes),
+                                         d_active, n_active, d_rows, n_rows, proxy_rows, cx,
+                                         cy, radius, id_tol, d_rank, d_perm, d_T,
+                                         static_cast<cudaStream_t>(stream)),
+                  "ki_id_noalloc");
+}
+
 }  // extern "C"

@@ -27,6 +27,9 @@
 // the pivot column itself, so no extra broadcast barrier is needed.
 #include <cooperative_groups.h>
 
+#include <cmath>
+#include <mutex>
+
 #include "ki_kernels.h"
 
 namespace cg = cooperative_groups;
@@ -438,6 +441,106 @@ cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s) {
     case 8: return launch_g<8>(p, s);
     default: return cudaErrorInvalidValue;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Interpolative decomposition without any device allocation.
+//
+// Some callers cannot call cudaMalloc: their device memory belongs to another
+// allocator (a framework's caching allocator or a pool reserved up front)
+// and a raw cudaMalloc/cudaFree would both bypass it and synchronise the
+// whole device.  For them the ID of one box runs with its m x n working
+// matrix in the file-scope array below, which every GPU that loads this
+// library holds (8 MiB) until the process exits.  All calls share the
+// array, the one-task descriptor and the proxy table, and each keeps the
+// previous call's contents: the working matrix is fully regenerated before
+// it is read, so nothing needs clearing, but calls that overlap on the GPU
+// (different streams, or several host threads) race on it.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+static __device__ __align__(256) IdTask g_noalloc_task[1];
+static __device__ __align__(256) double g_noalloc_dir[2 * kNumProxy];
+
+namespace {
+
+struct NoAllocSlot {
+  bool ready = false;
+  double* scratch = nullptr;
+  IdTask* task = nullptr;
+  double* dir = nullptr;
+};
+constexpr int kMaxDevices = 64;
+NoAllocSlot g_noalloc_slot[kMaxDevices];
+std::mutex g_noalloc_mu;
+
+}  // namespace
+
+// Resolves the device addresses of the static arrays for the current device
+// (host code may not pass the array names to a kernel: they are host-side
+// stand-ins) and fills the proxy table.  Runs once per device, on the first
+// call made with that device current.
+cudaError_t noalloc_setup(NoAllocSlot** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocSlot& sl = g_noalloc_slot[dev];
+  if (!sl.ready) {
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&sl.scratch), g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&sl.task), g_noalloc_task);
+    if (e != cudaSuccess) return e;
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&sl.dir), g_noalloc_dir);
+    if (e != cudaSuccess) return e;
+    double dir[2 * kNumProxy];
+    for (int i = 0; i < kNumProxy; i++) {
+      const double ang = 2 * M_PI * i * (1.0 / kNumProxy);
+      dir[i] = std::cos(ang);
+      dir[kNumProxy + i] = std::sin(ang);
+    }
+    e = cudaMemcpyToSymbol(g_noalloc_dir, dir, sizeof(dir));
+    if (e != cudaSuccess) return e;
+    sl.ready = true;
+  }
+  *out = &sl;
+  return cudaSuccess;
+}
+
+cudaError_t launch_id_noalloc(int pde, const Node* nodes, const int* act, int n,
+                              const int* rows, int n_rows, int proxy_rows, double cx,
+                              double cy, double radius, double tol, int* rank, int* perm,
+                              double* T, cudaStream_t s) {
+  NoAllocSlot* sl = nullptr;
+  cudaError_t e = noalloc_setup(&sl);
+  if (e != cudaSuccess) return e;
+  IdTask tk{};
+  tk.n = n;
+  tk.m = 2 * n_rows + proxy_rows;
+  tk.n_row = n_rows;
+  tk.proxy = proxy_rows;
+  tk.lda = (tk.m + 3) & ~3;
+  tk.cx = cx;
+  tk.cy = cy;
+  tk.rad = radius;
+  tk.pw = 2.0 * M_PI * radius / kNumProxy;
+  e = cudaMemcpyToSymbolAsync(g_noalloc_task, &tk, sizeof(IdTask), 0, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  IdParams p{};
+  p.tasks = sl->task;
+  p.ntasks = 1;
+  p.pde = pde;
+  p.nodes = nodes;
+  p.act = act;
+  p.rowdofs = rows;
+  p.work = sl->scratch;
+  p.tout = T;
+  p.perm = perm;
+  p.rank = rank;
+  p.proxy_dir = sl->dir;
+  p.tol = tol;
+  p.m_cap = tk.m;
+  p.n_cap = n;
+  return launch_id(p, 1, s);
 }
 
 }  // namespace kib

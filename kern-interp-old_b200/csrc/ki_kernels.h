@@ -53,6 +53,14 @@ struct IdParams {
 cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s);
 size_t id_smem_bytes(int m_cap, int n_cap);
 
+// One ID whose working matrix lives in a static device array (no device
+// allocation anywhere); lda * n must not exceed kNoAllocScratchDoubles.
+constexpr long long kNoAllocScratchDoubles = 1LL << 20;  // 8 MiB
+cudaError_t launch_id_noalloc(int pde, const Node* nodes, const int* act, int n,
+                              const int* rows, int n_rows, int proxy_rows, double cx,
+                              double cy, double radius, double tol, int* rank, int* perm,
+                              double* T, cudaStream_t s);
+
 // ---------------------------------------------------------------- decouple
 // Assembly + decouple of one compressed box (skel_factorization.cpp:55-91).
 // The box's K_BN = K(act, act) - (children's accumulated Schur updates) is
