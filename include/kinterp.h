@@ -41,6 +41,11 @@ const char* ki_last_error(void);
 int ki_version(void);
 /* Number of CUDA kernels this library has launched in the process. */
 long long ki_kernel_launches(void);
+/* Device and pinned host memory that destroyed handles left in the
+ * library's cache for later factorizations, in bytes; ki_release_cache()
+ * returns it to CUDA (call it with no handle alive). */
+long long ki_cached_bytes(void);
+void ki_release_cache(void);
 
 /* Builds the quadtree and skeletonizes the boundary operator.
  * Replaces QuadTree::initialize_tree (quadtree/quadtree.h:85-86), the U/Psi
@@ -107,8 +112,11 @@ int ki_allskel(ki_solver_t s, int* out);
 /* Statistics of the last factorization: out[0] factor ms, [1] ID kernel ms,
  * [2] ID launches, [3] ID algorithmic flops, [4] ID algorithmic bytes,
  * [5] decouple ms, [6] top-level LU ms, [7] host ms blocked on rank
- * downloads (timed factorizations only for [1], [5], [6]).  Returns the
- * number of values written (at most n, at most 8). */
+ * downloads, host ms spent on [8] level lists before the ID launches,
+ * [9] skeleton/decouple bookkeeping, [10] uploads, [11] the top level,
+ * [12] FP64 flops of the on-chip fold IDs (timed factorizations only for
+ * [1], [5], [6]).  Returns the number of values written (at most n, at
+ * most 13). */
 int ki_stats(ki_solver_t s, double* out, int n);
 /* Launch log of a ki_factor_timed factorization: rows of 7 doubles
  * (level, kind 0 ID / 1 decouple / 2 top LU, cluster size, boxes, max rows,

@@ -125,6 +125,10 @@ int ki_version(void) { return 100; }
 
 long long ki_kernel_launches(void) { return kib::launch_total(); }
 
+long long ki_cached_bytes(void) { return static_cast<long long>(kib::chunk_pool::cached_bytes()); }
+
+void ki_release_cache(void) { kib::chunk_pool::release_all(); }
+
 int ki_factor(int pde, int n_points, const double* points, const double* normals,
               const double* curvatures, const double* weights, int n_holes,
               const double* holes, int max_leaf_dofs, double id_tol, void* stream,
@@ -334,9 +338,12 @@ int ki_launch_log(ki_solver_t s, double* out, int cap) {
 int ki_stats(ki_solver_t s, double* out, int n) {
   if (!s || !s->solver || !out) return -KI_ERR_ARG;
   const kib::Solver& v = *s->solver;
-  const double vals[] = {v.t_factor_ms, v.t_id_ms, static_cast<double>(v.id_launches),
-                         v.id_flops, v.id_bytes, v.t_decouple_ms, v.t_top_ms, v.t_wait_ms};
-  const int cnt = n < 8 ? n : 8;
+  const double vals[] = {v.t_factor_ms,    v.t_id_ms,        static_cast<double>(v.id_launches),
+                         v.id_flops,       v.id_bytes,       v.t_decouple_ms,
+                         v.t_top_ms,       v.t_wait_ms,      v.t_host_prep_ms,
+                         v.t_host_post_ms, v.t_upload_ms,    v.t_host_top_ms,
+                         v.id_fold_flops};
+  const int cnt = n < 13 ? n : 13;
   for (int i = 0; i < cnt; i++) out[i] = vals[i];
   return cnt;
 }

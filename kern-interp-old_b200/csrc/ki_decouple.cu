@@ -33,7 +33,7 @@ __device__ __forceinline__ double upd_lookup(const int* bid, const int* bpos,
 }
 
 // Boxes with n <= kSmemN keep K_BN, and then X_rr, in shared memory.
-constexpr int kSmemN = 160;
+constexpr int kSmemN = kDecoupleSmemN;
 
 __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   extern __shared__ __align__(16) double dsm[];
@@ -112,7 +112,54 @@ __global__ void assemble_top_kernel(int pde, const Node* nodes, const int* dofs,
       boundary_entry(pde, nodes, dofs[a], dofs[b]) - upd_lookup(bid, bpos, blocks, a, b);
 }
 
+__global__ void assemble_perm_kernel(int pde, const Node* nodes, const int* act, const int* perm,
+                                     int n, const int* bid, const int* bpos,
+                                     const UpdBlock* blocks, double* K) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(n) * n) return;
+  const int a = static_cast<int>(e % n), b = static_cast<int>(e / n);
+  const int pa = perm[a], pb = perm[b];
+  K[e] = boundary_entry(pde, nodes, act[pa], act[pb]) - upd_lookup(bid, bpos, blocks, pa, pb);
+}
+
+__global__ void acc_finish_kernel(double* acc, int k, const int* perm, const int* bid,
+                                  const int* bpos, const UpdBlock* blocks) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= k * k) return;
+  const int i = e % k, j = e / k;
+  acc[e] = upd_lookup(bid, bpos, blocks, perm[i], perm[j]) - acc[e];
+}
+
 }  // namespace
+
+cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* status,
+                           cudaStream_t s) {
+  const int n = tk.n, k = tk.k, r = n - k;
+  const long long nn = static_cast<long long>(n) * n;
+  count_launches(2);
+  assemble_perm_kernel<<<static_cast<int>((nn + 255) / 256), 256, 0, s>>>(
+      pde, nodes, tk.act, tk.perm, n, tk.bid, tk.bpos, tk.blocks, tk.K);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const double* K = tk.K;
+  const double* Kss = K;
+  const double* Krs_in = K + k;
+  const double* Ksr = K + static_cast<long long>(n) * k;
+  const double* Krr = K + k + static_cast<long long>(n) * k;
+  // K_r_sn in U, K_sn_r in L, X = (K_rr - T^T K_sr) - K_r_sn T
+  if ((e = launch_gemm_sub(tk.U, r, Krs_in, n, tk.T, k, true, Kss, n, false, r, k, k, s))) return e;
+  if ((e = launch_gemm_sub(tk.L, k, Ksr, n, Kss, n, false, tk.T, k, false, k, r, k, s))) return e;
+  if ((e = launch_gemm_sub(tk.X, r, Krr, n, tk.T, k, true, Ksr, n, false, r, r, k, s))) return e;
+  if ((e = launch_gemm_sub(tk.X, r, tk.X, r, tk.U, r, false, tk.T, k, false, r, r, k, s))) return e;
+  if ((e = dense_lu(tk.X, r, r, tk.piv, status, s))) return e;
+  if ((e = dense_lu_solve_rows(tk.X, r, r, tk.piv, tk.L, k, k, s))) return e;
+  if ((e = launch_gemm_sub(tk.acc, k, nullptr, 0, tk.L, k, false, tk.U, r, false, k, k, r, s)))
+    return e;
+  acc_finish_kernel<<<(k * k + 255) / 256, 256, 0, s>>>(tk.acc, k, tk.perm, tk.bid, tk.bpos,
+                                                         tk.blocks);
+  if ((e = cudaGetLastError())) return e;
+  return dense_lu_solve(tk.X, r, r, tk.piv, tk.U, k, r, s);
+}
 
 size_t decouple_smem_bytes(int n_max) {
   const int ns = n_max < kSmemN ? n_max : kSmemN;

@@ -242,7 +242,49 @@ __global__ void __launch_bounds__(256) gemm_tn_long_kernel(int m, int k, double 
   }
 }
 
+// One 64 x 64 tile of C = C0 - op(A) op(B) per CTA.
+__global__ void __launch_bounds__(256) gemm_sub_kernel(double* C, int ldc, const double* C0,
+                                                       int ldc0, const double* A, int lda,
+                                                       bool ta, const double* B, int ldb,
+                                                       bool tb, int m, int n, int kk) {
+  __shared__ double tile[kGemmTileDoubles];
+  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  const int mt = min(64, m - i0), nt = min(64, n - j0);
+  const double* Ab = ta ? A + static_cast<long long>(lda) * i0 : A + i0;
+  const double* Bb = tb ? B + j0 : B + static_cast<long long>(ldb) * j0;
+  cta_gemm_tiled(C + i0 + static_cast<long long>(ldc) * j0, ldc,
+                 C0 ? C0 + i0 + static_cast<long long>(ldc0) * j0 : nullptr, ldc0, Ab, lda, ta, Bb,
+                 ldb, tb, mt, nt, kk, tile);
+}
+
+// Rows of B (nrows rows, row stride 1, column stride ldb) <- rows of B A^{-1},
+// i.e. each row r: solve A^T y = B(r, :)^T, one warp per row.
+__global__ void lu_solve_rows_kernel(const double* lu, int n, int ld, const int* ipiv, double* b,
+                                     int nrows, int ldb) {
+  const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (r >= nrows) return;
+  warp_lu_solve_t(lu, n, ld, ipiv, b + r, ldb);
+}
+
 }  // namespace
+
+cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, const double* A,
+                            int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,
+                            int k, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return cudaSuccess;
+  count_launches(1);
+  gemm_sub_kernel<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(C, ldc, C0, ldc0, A, lda, ta,
+                                                                      B, ldb, tb, m, n, k);
+  return cudaGetLastError();
+}
+
+cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv, double* b,
+                                int nrows, int ldb, cudaStream_t s) {
+  if (n == 0 || nrows == 0) return cudaSuccess;
+  count_launches(1);
+  lu_solve_rows_kernel<<<(nrows + 3) / 4, 128, 0, s>>>(lu, n, ld, ipiv, b, nrows, ldb);
+  return cudaGetLastError();
+}
 
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s) {
   for (int j0 = 0; j0 < n; j0 += kNb) {

@@ -136,8 +136,81 @@ __device__ __forceinline__ double col_sumsq(const double* __restrict__ col, int 
   return s0 + s1;
 }
 
+// sum over r = r0, r0 + L, ... < r1 of a[r] b[r], four loads in flight.
+__device__ __forceinline__ double strided_dot(const double* a, const double* b, int r0, int r1,
+                                              int L) {
+  double s0 = 0.0, s1 = 0.0;
+  int r = r0;
+  for (; r + 3 * L < r1; r += 4 * L) {
+    const double x0 = a[r], x1 = a[r + L], x2 = a[r + 2 * L], x3 = a[r + 3 * L];
+    const double y0 = b[r], y1 = b[r + L], y2 = b[r + 2 * L], y3 = b[r + 3 * L];
+    s0 += x0 * y0 + x2 * y2;
+    s1 += x1 * y1 + x3 * y3;
+  }
+  for (; r < r1; r += L) s0 += a[r] * b[r];
+  return s0 + s1;
+}
+
+// col[r] += v[r] t over r = r0, r0 + L, ... < r1, loads ahead of stores.
+__device__ __forceinline__ void strided_axpy(double* col, const double* v, int r0, int r1, int L,
+                                             double t) {
+  int r = r0;
+  for (; r + 3 * L < r1; r += 4 * L) {
+    const double x0 = col[r], x1 = col[r + L], x2 = col[r + 2 * L], x3 = col[r + 3 * L];
+    const double y0 = v[r], y1 = v[r + L], y2 = v[r + 2 * L], y3 = v[r + 3 * L];
+    col[r] = x0 + y0 * t;
+    col[r + L] = x1 + y1 * t;
+    col[r + 2 * L] = x2 + y2 * t;
+    col[r + 3 * L] = x3 + y3 * t;
+  }
+  for (; r < r1; r += L) col[r] += v[r] * t;
+}
+
+// T column = R11^{-1} b by one warp (dtrsm column sweep), b = R(0:k, col)
+// and the result held in registers (k <= 32 kTRegs); colq(q) is column q of
+// R in pivot order.  Returns false when k is too large for the registers.
+constexpr int kTRegs = 8;
+template <class ColFn>
+__device__ __forceinline__ bool warp_tsolve(const double* bcol, int k, const double* rdiag,
+                                            ColFn colq, double* out) {
+  if (k > 32 * kTRegs) return false;
+  const int lane = threadIdx.x & 31;
+  double b[kTRegs];
+#pragma unroll
+  for (int t = 0; t < kTRegs; t++) {
+    const int l = lane + 32 * t;
+    b[t] = l < k ? bcol[l] : 0.0;
+  }
+  for (int q = k - 1; q >= 0; q--) {
+    const int tq = q >> 5;
+    double bq = 0.0;
+#pragma unroll
+    for (int t = 0; t < kTRegs; t++)
+      if (t == tq) bq = b[t];
+    bq = __shfl_sync(0xffffffffu, bq, q & 31);
+    if (bq != 0.0) {
+      const double xq = bq / rdiag[q];
+      const double* rq = colq(q);
+#pragma unroll
+      for (int t = 0; t < kTRegs; t++) {
+        const int l = lane + 32 * t;
+        if (l == q) b[t] = xq;
+        else if (l < q) b[t] -= xq * rq[l];
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kTRegs; t++) {
+    const int l = lane + 32 * t;
+    if (l < k) out[l] = b[t];
+  }
+  return true;
+}
+
+// Streaming variant: the matrix lives in HBM/L2 (boxes too large for a
+// cluster's shared memory); G CTAs per box.
 template <int G>
-__global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
+__global__ void __launch_bounds__(kIdThreads, 1) id_kernel(IdParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int task = blockIdx.x / G;
   int g = 0;
@@ -146,7 +219,7 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  double* v = reinterpret_cast<double*>(smem_raw);   // m_cap: Householder vector
+  double* v = reinterpret_cast<double*>(smem_raw);     // m_cap: Householder vector
   double* rdiag = v + P.m_cap;                        // n_cap: R_ii
   double* vn1 = rdiag + P.n_cap;                      // n_cap: partial norms (physical)
   double* vn2 = vn1 + P.n_cap;                        // n_cap
@@ -158,6 +231,7 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   int* si = own + P.n_cap;                            // [0] own count, [1] pivot column
 
   double* A = P.work + tk.a_off;
+  auto colp = [&](int j) -> double* { return A + static_cast<long long>(j) * lda; };
   const int* act = P.act + tk.act_off;
   const int* rowd = P.rowdofs + tk.row_off;
   const Node* nodes = P.nodes;
@@ -211,7 +285,7 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   for (int t = warp; g + G * t < n; t += kIdWarps) {
     const int j = g + G * t;
     const int cd = act[j];
-    double* col = A + static_cast<long long>(j) * lda;
+    double* col = colp(j);
     double ss = 0.0;
     for (int r = lane; r < m; r += 32) {
       double val;
@@ -263,7 +337,7 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
   double thresh = 0.0;
   for (int i = 0; i < mn; i++) {
     const int c = si[1];
-    const double* colc = A + static_cast<long long>(c) * lda;
+    const double* colc = colp(c);
     // ---- Householder reflector of the pivot column (redundantly per CTA);
     // the column's rows below the diagonal are staged in v as they are read.
     double part = 0.0;
@@ -317,7 +391,7 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
     for (int t = warp; t < nown; t += kIdWarps) {
       const int p = own[t];
       const int j = pos2col[p];
-      double* col = A + static_cast<long long>(j) * lda;
+      double* col = colp(j);
       if (tau != 0.0) {
         const double w = warp_sum(col_dot(col, v, i + lane, m));
         col_axpy(col, v, i + lane, m, -tau * w);
@@ -374,14 +448,14 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
     if (threadIdx.x == 0) P.rank[task] = rank;
     for (int p = threadIdx.x; p < n; p += kIdThreads) P.perm[tk.perm_off + p] = pos2col[p];
   }
-  if (rank == 0) return;
   const int k = rank;
   double* T = P.tout + tk.t_off;
-  for (int p = k + warp; p < n; p += kIdWarps) {
+  for (int p = k + warp; k > 0 && p < n; p += kIdWarps) {
     const int j = pos2col[p];
     if (j % G != g) continue;
-    const double* col = A + static_cast<long long>(j) * lda;
+    const double* col = colp(j);
     double* tc = T + static_cast<long long>(p - k) * k;
+    if (warp_tsolve(col, k, rdiag, [&](int q) { return colp(pos2col[q]); }, tc)) continue;
     for (int l = lane; l < k; l += 32) tc[l] = col[l];
     __syncwarp();
     for (int q = k - 1; q >= 0; q--) {
@@ -389,13 +463,349 @@ __global__ void __launch_bounds__(kIdThreads) id_kernel(IdParams P) {
       __syncwarp();
       if (bq != 0.0) {
         const double xq = bq / rdiag[q];
-        const double* rq = A + static_cast<long long>(pos2col[q]) * lda;
+        const double* rq = colp(pos2col[q]);
         if (lane == 0) tc[q] = xq;
         for (int l = lane; l < q; l += 32) tc[l] -= xq * rq[l];
       }
       __syncwarp();
     }
   }
+}
+
+constexpr int kOcThreads = 512;  // on-chip variant: 16 warps per CTA
+constexpr int kOcWarps = kOcThreads / 32;
+
+// On-chip variant: the whole ID matrix sits in the shared memory of a
+// G-CTA cluster (CTA g holds the physical columns j with j % G == g) and a
+// peer's pivot column is read through distributed shared memory.  In every
+// pivot step the trailing columns are spread over all warps: each column is
+// worked by a group of L lanes (L = 256 / columns, a power of two) that walk
+// interleaved rows, so a group reads consecutive rows and every warp of the
+// CTA has independent work to hide shared-memory and FP64 latency.
+
+template <int G>
+__global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int task = blockIdx.x / G;
+  int g = 0;
+  if constexpr (G > 1) g = static_cast<int>(cg::this_cluster().block_rank());
+  const IdTask tk = P.tasks[task];
+  const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  double* cols = reinterpret_cast<double*>(smem_raw);  // owned columns
+  double* v = cols + P.col_cap;                        // m_cap
+  double* rdiag = v + P.m_cap;                          // n_cap
+  double* vn1 = rdiag + P.n_cap;                        // n_cap
+  double* vn2 = vn1 + P.n_cap;                          // n_cap
+  double* red = vn2 + P.n_cap;                          // 32
+  Cand* wbest = reinterpret_cast<Cand*>(red + 32);      // kOcWarps
+  Cand* slot = wbest + kOcWarps;                        // 2
+  int* pos2col = reinterpret_cast<int*>(slot + 2);      // n_cap
+  int* own = pos2col + P.n_cap;                         // n_cap
+  int* si = own + P.n_cap;                              // [0] own count, [1] pivot
+
+  auto colp = [&](int j) -> double* {
+    double* base = cols + static_cast<long long>(j / G) * lda;
+    if constexpr (G > 1) {
+      if (j % G != g) return cg::this_cluster().map_shared_rank(base, j % G);
+    }
+    return base;
+  };
+  const int* act = P.act + tk.act_off;
+  const int* rowd = P.rowdofs + tk.row_off;
+  const Node* nodes = P.nodes;
+  const int pde = P.pde;
+  const int mn = min(m, n);
+
+  auto select_pivot = [&](int i, bool from_slots) {
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    if (from_slots) {
+      if (lane < G) {
+        Cand c;
+        if constexpr (G > 1) {
+          c = cg::this_cluster().map_shared_rank(slot, lane)[i & 1];
+        } else {
+          c = slot[i & 1];
+        }
+        bv = c.val;
+        bp = c.pos;
+      }
+    } else if (lane < kOcWarps) {
+      bv = wbest[lane].val;
+      bp = wbest[lane].pos;
+    }
+    warp_best(bv, bp);
+    const int pvt = bp;
+    const int ci = pos2col[i];
+    const int cp = pos2col[pvt];
+    __syncwarp();
+    if (lane == 0) {
+      pos2col[i] = cp;
+      pos2col[pvt] = ci;
+      si[1] = cp;
+    }
+    __syncwarp();
+    int cnt = 0;
+    for (int base = i + 1; base < n; base += 32) {
+      const int p = base + lane;
+      const bool mine = p < n && (pos2col[p] % G == g);
+      const unsigned bal = __ballot_sync(0xffffffffu, mine);
+      if (mine) own[cnt + __popc(bal & ((1u << lane) - 1u))] = p;
+      cnt += __popc(bal);
+    }
+    if (lane == 0) si[0] = cnt;
+  };
+
+  // ---- generation of the owned columns + their initial norms (two rows per
+  // lane per iteration for instruction-level parallelism)
+  auto entry_at = [&](int r, int cd) -> double {
+    if (r < I) return boundary_entry(pde, nodes, rowd[r], cd);
+    if (r < 2 * I) return boundary_entry(pde, nodes, cd, rowd[r - I]);
+    return proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
+  };
+  for (int t = warp; g + G * t < n; t += kOcWarps) {
+    const int j = g + G * t;
+    const int cd = act[j];
+    double* col = colp(j);
+    double ss = 0.0;
+    int r = lane;
+    for (; r + 96 < m; r += 128) {
+      const double a0 = entry_at(r, cd);
+      const double a1 = entry_at(r + 32, cd);
+      const double a2 = entry_at(r + 64, cd);
+      const double a3 = entry_at(r + 96, cd);
+      col[r] = a0;
+      col[r + 32] = a1;
+      col[r + 64] = a2;
+      col[r + 96] = a3;
+      ss += (a0 * a0 + a1 * a1) + (a2 * a2 + a3 * a3);
+    }
+    for (; r < m; r += 32) {
+      const double a0 = entry_at(r, cd);
+      col[r] = a0;
+      ss += a0 * a0;
+    }
+    ss = warp_sum(ss);
+    if (lane == 0) {
+      vn1[j] = sqrt(ss);
+      vn2[j] = vn1[j];
+    }
+  }
+  for (int p = threadIdx.x; p < n; p += kOcThreads) pos2col[p] = p;
+  __syncthreads();
+  {
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int t = warp; g + G * t < n; t += kOcWarps) {
+      const int j = g + G * t;
+      if (better(vn1[j], j, bv, bp)) {
+        bv = vn1[j];
+        bp = j;
+      }
+    }
+    if (lane == 0) wbest[warp] = Cand{bv, bp, 0};
+  }
+  __syncthreads();
+  if constexpr (G > 1) {
+    if (warp == 0) {
+      double bv = lane < kOcWarps ? wbest[lane].val : -1.0;
+      int bp = lane < kOcWarps ? wbest[lane].pos : 0x7fffffff;
+      warp_best(bv, bp);
+      if (lane == 0) slot[0] = Cand{bv, bp, 0};
+    }
+    cg::this_cluster().sync();
+  }
+  if (warp == 0 && mn > 0) select_pivot(0, G > 1);
+  __syncthreads();
+
+  const double tol3z = sqrt(0.5 * 2.220446049250313e-16);
+  int rank = 0;
+  double thresh = 0.0;
+  for (int i = 0; i < mn; i++) {
+    const int c = si[1];
+    const double* colc = colp(c);
+    double part = 0.0;
+    for (int r = i + 1 + threadIdx.x; r < m; r += kOcThreads) {
+      const double a0 = colc[r];
+      v[r] = a0;
+      part += a0 * a0;
+    }
+    part = warp_sum(part);
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    double xs = 0.0;
+#pragma unroll
+    for (int w = 0; w < kOcWarps; w++) xs += red[w];
+    const double xnorm = sqrt(xs);
+    const double alpha = colc[i];
+    double beta = alpha, tau = 0.0, scal = 0.0;
+    if (i < m - 1 && xnorm != 0.0) {
+      beta = -copysign(lapy2(alpha, xnorm), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    if (i == 0) thresh = fabs(P.tol * beta);
+    if (i >= 1 && fabs(beta) < thresh) {
+      rank = i;
+      break;
+    }
+    if (threadIdx.x == 0) {
+      rdiag[i] = beta;
+      v[i] = 1.0;
+    }
+    for (int r = i + 1 + threadIdx.x; r < m; r += kOcThreads) v[r] *= scal;
+    __syncthreads();
+    const int nown = si[0];
+    // lanes per column for this step: spread the trailing columns over all
+    // warps (L = 1 .. 32, a power of two); lane s of a group walks rows
+    // i + s, i + s + L, ... so a group reads consecutive rows
+    int L = 32;
+    while (L > 1 && nown * L > kOcThreads) L >>= 1;
+    const int gl = threadIdx.x & (L - 1);         // lane within the group
+    const int gi = threadIdx.x / L;               // group index
+    const int ngroups = kOcThreads / L;
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int q0 = 0; q0 < nown; q0 += ngroups) {
+      const int q = q0 + gi;
+      const bool active = q < nown;
+      const int p = active ? own[q] : 0;
+      const int j = active ? pos2col[p] : g;
+      double* col = colp(j);
+      double w = 0.0;
+      if (active && tau != 0.0) w = strided_dot(col, v, i + gl, m, L);
+      for (int o = 1; o < L; o <<= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (active && tau != 0.0) strided_axpy(col, v, i + gl, m, L, -tau * w);
+      __syncwarp();
+      // partial-norm downdate (dlaqp2), recomputed when it lost accuracy
+      double nv1 = 0.0;
+      bool recompute = false;
+      if (active) {
+        const double aij = col[i];
+        nv1 = vn1[j];
+        const double nv2 = vn2[j];
+        if (nv1 != 0.0) {
+          double temp = fabs(aij) / nv1;
+          temp = fmax(1.0 - temp * temp, 0.0);
+          const double qq = nv1 / nv2;
+          const double temp2 = temp * (qq * qq);
+          if (temp2 <= tol3z) {
+            recompute = true;
+          } else {
+            nv1 *= sqrt(temp);
+          }
+        }
+      }
+      if (__any_sync(0xffffffffu, recompute)) {
+        double ss = 0.0;
+        if (recompute) ss = strided_dot(col, col, i + 1 + gl, m, L);
+        for (int o = 1; o < L; o <<= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+        if (recompute) {
+          nv1 = (i < m - 1) ? sqrt(ss) : 0.0;
+          if (gl == 0) vn2[j] = nv1;
+        }
+      }
+      if (active) {
+        if (gl == 0) vn1[j] = nv1;
+        if (better(nv1, p, bv, bp)) {
+          bv = nv1;
+          bp = p;
+        }
+      }
+      __syncwarp();
+    }
+    warp_best(bv, bp);
+    if (lane == 0) wbest[warp] = Cand{bv, bp, 0};
+    __syncthreads();
+    if (i + 1 < mn) {
+      if constexpr (G > 1) {
+        if (warp == 0) {
+          double cv = lane < kOcWarps ? wbest[lane].val : -1.0;
+          int cpos = lane < kOcWarps ? wbest[lane].pos : 0x7fffffff;
+          warp_best(cv, cpos);
+          if (lane == 0) slot[(i + 1) & 1] = Cand{cv, cpos, 0};
+        }
+        cg::this_cluster().sync();
+      }
+      if (warp == 0) select_pivot(i + 1, G > 1);
+      __syncthreads();
+    }
+  }
+  if constexpr (G > 1) cg::this_cluster().sync();
+
+  if (g == 0) {
+    if (threadIdx.x == 0) P.rank[task] = rank;
+    for (int p = threadIdx.x; p < n; p += kOcThreads) P.perm[tk.perm_off + p] = pos2col[p];
+  }
+  // T = R11^{-1} R12 for this CTA's redundant columns, solved in place in
+  // their first k rows (dtrsm column sweep, one barrier per row of R11)
+  const int k = rank;
+  double* T = P.tout + tk.t_off;
+  if (k > 0) {
+    if (threadIdx.x < 32) {
+      int cnt = 0;
+      for (int base = k; base < n; base += 32) {
+        const int p = base + lane;
+        const bool mine = p < n && (pos2col[p] % G == g);
+        const unsigned bal = __ballot_sync(0xffffffffu, mine);
+        if (mine) own[cnt + __popc(bal & ((1u << lane) - 1u))] = p;
+        cnt += __popc(bal);
+      }
+      if (lane == 0) si[0] = cnt;
+    }
+    __syncthreads();
+    const int nr = si[0];
+    for (int q = k - 1; q >= 0; q--) {
+      const double* rq = colp(pos2col[q]);
+      const double dq = rdiag[q];
+      for (int e = threadIdx.x; e < (q + 1) * nr; e += kOcThreads) {
+        const int l = e % (q + 1), t = e / (q + 1);
+        const int p = own[t];
+        double* col = colp(pos2col[p]);
+        const double bq = col[q];
+        if (l == q) {
+          T[q + static_cast<long long>(p - k) * k] = bq != 0.0 ? bq / dq : bq;
+        } else if (bq != 0.0) {
+          col[l] -= (bq / dq) * rq[l];
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if constexpr (G > 1) cg::this_cluster().sync();
+}
+
+template <int G>
+cudaError_t launch_onchip(const IdParams& p, cudaStream_t s) {
+  const size_t smem = id_smem_bytes(p.m_cap, p.n_cap) + sizeof(double) * p.col_cap;
+  cudaError_t e = cudaFuncSetAttribute(id_onchip_kernel<G>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  if (G > 8) {
+    e = cudaFuncSetAttribute(id_onchip_kernel<G>, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                             1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G * p.ntasks);
+  cfg.blockDim = dim3(kOcThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  int na = 0;
+  if (G > 1) {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    na = 1;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  return cudaLaunchKernelEx(&cfg, id_onchip_kernel<G>, p);
 }
 
 template <int G>
@@ -428,7 +838,7 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 
 size_t id_smem_bytes(int m_cap, int n_cap) {
   return sizeof(double) * (static_cast<size_t>(m_cap) + 3 * n_cap + 32) +
-         sizeof(Cand) * (kIdWarps + 2) + sizeof(int) * (2 * static_cast<size_t>(n_cap) + 8);
+         sizeof(Cand) * (kOcWarps + 2) + sizeof(int) * (2 * static_cast<size_t>(n_cap) + 8);
 }
 
 cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s) {
@@ -439,6 +849,11 @@ cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s) {
     case 2: return launch_g<2>(p, s);
     case 4: return launch_g<4>(p, s);
     case 8: return launch_g<8>(p, s);
+    case kOnChip + 1: return launch_onchip<1>(p, s);
+    case kOnChip + 2: return launch_onchip<2>(p, s);
+    case kOnChip + 4: return launch_onchip<4>(p, s);
+    case kOnChip + 8: return launch_onchip<8>(p, s);
+    case kOnChip + 16: return launch_onchip<16>(p, s);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -541,6 +956,44 @@ cudaError_t launch_id_noalloc(int pde, const Node* nodes, const int* act, int n,
   p.m_cap = tk.m;
   p.n_cap = n;
   return launch_id(p, 1, s);
+}
+
+int id_cluster_fits(int group, int m_cap, int n_cap, size_t col_cap) {
+  if (group < kOnChip) return 1;
+  const int G = group - kOnChip;
+  const size_t smem = id_smem_bytes(m_cap, n_cap) + sizeof(double) * col_cap;
+  if (smem > 227 * 1024) return 0;
+  if (G == 1) return 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G);
+  cfg.blockDim = dim3(kOcThreads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = G;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  cudaError_t e;
+  switch (G) {
+    case 2: e = cudaFuncSetAttribute(id_onchip_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<2>, &cfg); break;
+    case 4: e = cudaFuncSetAttribute(id_onchip_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<4>, &cfg); break;
+    case 8: e = cudaFuncSetAttribute(id_onchip_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<8>, &cfg); break;
+    case 16: e = cudaFuncSetAttribute(id_onchip_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(id_onchip_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<16>, &cfg); break;
+    default: return 0;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return clusters > 0 ? 1 : 0;
 }
 
 }  // namespace kib

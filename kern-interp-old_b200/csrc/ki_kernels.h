@@ -47,9 +47,20 @@ struct IdParams {
   const double* proxy_dir;  // cos/sin table, 2 * kNumProxy doubles
   double tol;
   int m_cap, n_cap;  // maxima over the launch (shared-memory layout)
+  long long col_cap;  // on-chip launches: doubles of columns per CTA
 };
 
-// Launches one ID per task with `group` CTAs (a cluster) per task.
+// launch_id group codes: G (1, 2, 4, 8) streams the matrix through HBM/L2
+// with G CTAs per box; kOnChip + G (G = 1 .. 16) keeps it in the shared
+// memory of a G-CTA cluster.
+constexpr int kOnChip = 100;
+// Column stride of an on-chip ID matrix with m rows: odd, so that lane
+// groups reading different columns spread over the shared-memory banks.
+inline int onchip_lda(int m) { return m | 1; }
+// Nonzero if an on-chip launch of this size can be scheduled on the device.
+int id_cluster_fits(int group, int m_cap, int n_cap, size_t col_cap);
+
+// Launches one ID per task with a cluster of CTAs per task (group codes above).
 cudaError_t launch_id(const IdParams& p, int group, cudaStream_t s);
 size_t id_smem_bytes(int m_cap, int n_cap);
 
@@ -98,7 +109,13 @@ struct DecParams {
 };
 
 // n_max: largest box of the launch (sizes the shared-memory staging).
+// Boxes with n > kDecoupleSmemN must go through decouple_large instead.
+constexpr int kDecoupleSmemN = 160;
 cudaError_t launch_decouple(const DecParams& p, int n_max, cudaStream_t s);
+// The same decoupling for one large box as a sequence of GPU-wide kernels
+// (tk is the host copy of the box's descriptor; tk.K must hold n x n).
+cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* status,
+                           cudaStream_t s);
 
 // Dense assembly of the top-level skeleton matrix K(allskel, allskel) minus
 // the accumulated updates (skel_factorization.cpp:116-122), n x n, ld ld.
@@ -110,6 +127,13 @@ cudaError_t launch_assemble_top(int pde, const Node* nodes, const int* dofs, int
 // In-place LU with partial pivoting of an n x n matrix (ld), pivots 0-based
 // row indices as LAPACK's (ipiv[j] = row swapped with j).
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s);
+// Multi-CTA tiled C = C0 - op(A) op(B) (64 x 64 tiles); C0 may be null.
+cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, const double* A,
+                            int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,
+                            int k, cudaStream_t s);
+// Each of the nrows rows of B (column stride ldb) <- row * A^{-1}.
+cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv, double* b,
+                                int nrows, int ldb, cudaStream_t s);
 // B <- A^{-1} B (n x nrhs, ldb) for the LU above.
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
                            int nrhs, int ldb, cudaStream_t s);

@@ -17,21 +17,76 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace kib {
 
 // ------------------------------------------------------------------ memory
+namespace chunk_pool {
+namespace {
+std::mutex g_mu;
+std::multimap<size_t, void*> g_free[2];  // [0] device, [1] pinned host
+size_t g_cached = 0;
+}  // namespace
+
+void* get(size_t bytes, bool pinned, size_t* got) {
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto& fl = g_free[pinned ? 1 : 0];
+    auto it = fl.lower_bound(bytes);
+    if (it != fl.end() && it->first <= 4 * bytes + (64u << 20)) {
+      void* p = it->second;
+      *got = it->first;
+      g_cached -= it->first;
+      fl.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  const cudaError_t e = pinned ? cudaHostAlloc(&p, bytes, cudaHostAllocDefault)
+                               : cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  *got = bytes;
+  return p;
+}
+
+void put(void* p, size_t bytes, bool pinned) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  g_free[pinned ? 1 : 0].emplace(bytes, p);
+  g_cached += bytes;
+}
+
+void release_all() {
+  std::lock_guard<std::mutex> lock(g_mu);
+  for (auto& kv : g_free[0]) cudaFree(kv.second);
+  for (auto& kv : g_free[1]) cudaFreeHost(kv.second);
+  g_free[0].clear();
+  g_free[1].clear();
+  g_cached = 0;
+}
+
+size_t cached_bytes() {
+  std::lock_guard<std::mutex> lock(g_mu);
+  return g_cached;
+}
+}  // namespace chunk_pool
+
 Arena::~Arena() {
-  for (void* c : chunks_) cudaFree(c);
+  for (auto& c : chunks_) chunk_pool::put(c.first, c.second, pinned_);
 }
 
 void* Arena::alloc(size_t bytes) {
   bytes = (bytes + 255) & ~static_cast<size_t>(255);
   if (bytes > left_) {
-    const size_t sz = std::max(bytes, static_cast<size_t>(64) << 20);
-    void* p = nullptr;
-    if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
-    chunks_.push_back(p);
+    const size_t want = std::max(bytes, static_cast<size_t>(pinned_ ? 16 : 64) << 20);
+    size_t sz = 0;
+    void* p = chunk_pool::get(want, pinned_, &sz);
+    if (!p) return nullptr;
+    chunks_.push_back({p, sz});
     cur_ = static_cast<char*>(p);
     left_ = sz;
     reserved_ += sz;
@@ -43,29 +98,33 @@ void* Arena::alloc(size_t bytes) {
 }
 
 Scratch::~Scratch() {
-  if (p) cudaFree(p);
+  if (p) chunk_pool::put(p, bytes, false);
 }
 
 cudaError_t Scratch::reserve(size_t want, cudaStream_t s) {
   if (want <= bytes) return cudaSuccess;
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  if (p) cudaFree(p);
+  if (p) chunk_pool::put(p, bytes, false);
   p = nullptr;
   bytes = 0;
-  const size_t sz = want + want / 4 + 4096;
-  e = cudaMalloc(&p, sz);
-  if (e == cudaSuccess) bytes = sz;
-  return e;
+  size_t got = 0;
+  p = chunk_pool::get(want + want / 4 + 4096, false, &got);
+  if (!p) return cudaErrorMemoryAllocation;
+  bytes = got;
+  return cudaSuccess;
 }
 
 namespace {
 
-template <class T>
-cudaError_t upload(T* dst, const std::vector<T>& src, cudaStream_t s) {
-  if (src.empty()) return cudaSuccess;
-  return cudaMemcpyAsync(dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, s);
+double g_upload_ms = 0;  // accumulated by upload() (single host thread per solver)
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+
 
 // initialize_U_mat (linear_solve.cpp:18-64) for boundary points.
 void border_U(int pde, const std::vector<double>& pts, const std::vector<double>& holes,
@@ -129,7 +188,8 @@ void border_Psi(int pde, const std::vector<double>& pts, const std::vector<doubl
   }
 }
 
-int pick_group(long long m, long long n) {
+// Streaming launches: CTAs per box by matrix size.
+int pick_stream_group(long long m, long long n) {
   const long long e = m * n;
   if (e > 400000) return 8;
   if (e > 160000) return 4;
@@ -137,9 +197,36 @@ int pick_group(long long m, long long n) {
   return 1;
 }
 
+// Smallest cluster whose shared memory holds the whole m x n matrix (group
+// code kOnChip + G), else a streaming launch.  onchip_ok[G] says whether a
+// G-CTA cluster with full shared memory can be scheduled on this device.
+int pick_group(int m, int n, const bool* onchip_ok) {
+  const long long lda = onchip_lda(m);
+  for (int G = 1; G <= 16; G *= 2) {
+    if (!onchip_ok[G]) continue;
+    const long long cols = (n + G - 1) / G * lda;
+    if (id_smem_bytes(m, n) + sizeof(double) * cols <= 227 * 1024) return kOnChip + G;
+  }
+  return pick_stream_group(m, n);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ solver
+template <class T>
+int Solver::upload(T* dst, const std::vector<T>& src, cudaStream_t s) {
+  if (src.empty()) return 0;
+  const double t0 = now_ms();
+  const size_t bytes = sizeof(T) * src.size();
+  void* st = stage_.alloc(bytes);
+  if (!st) return fail("pinned staging allocation failed");
+  std::memcpy(st, src.data(), bytes);
+  const int rc = cuda_check(cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, s),
+                            "cudaMemcpyAsync (upload)");
+  g_upload_ms += now_ms() - t0;
+  return rc;
+}
+
 Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
                const double* normals, const double* curvatures, const double* weights,
                int n_holes, const double* holes, cudaStream_t stream)
@@ -154,17 +241,24 @@ Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
   if (n_holes > 0) holes_.assign(holes, holes + 4 * static_cast<size_t>(n_holes));
 }
 
-Solver::~Solver() = default;
-
-int Solver::timer_begin(cudaEvent_t* e0) {
-  if (cuda_check(cudaEventCreate(e0), "cudaEventCreate")) return -2;
-  return cuda_check(cudaEventRecord(*e0, stream_), "cudaEventRecord");
+Solver::~Solver() {
+  // chunks go back to the pool only once no queued work can touch them
+  cudaStreamSynchronize(stream_);
+  if (dstream_) cudaStreamSynchronize(dstream_);
+  if (ev_id_) cudaEventDestroy(ev_id_);
+  if (ev_dec_) cudaEventDestroy(ev_dec_);
+  if (dstream_) cudaStreamDestroy(dstream_);
 }
 
-int Solver::timer_end(cudaEvent_t e0, const LaunchRecord& rec) {
+int Solver::timer_begin(cudaEvent_t* e0, cudaStream_t s) {
+  if (cuda_check(cudaEventCreate(e0), "cudaEventCreate")) return -2;
+  return cuda_check(cudaEventRecord(*e0, s ? s : stream_), "cudaEventRecord");
+}
+
+int Solver::timer_end(cudaEvent_t e0, const LaunchRecord& rec, cudaStream_t s) {
   cudaEvent_t e1;
   if (cuda_check(cudaEventCreate(&e1), "cudaEventCreate")) return -2;
-  if (cuda_check(cudaEventRecord(e1, stream_), "cudaEventRecord")) return -2;
+  if (cuda_check(cudaEventRecord(e1, s ? s : stream_), "cudaEventRecord")) return -2;
   pending_.push_back({e0, e1, rec});
   return 0;
 }
@@ -180,7 +274,7 @@ int Solver::timers_resolve() {
       id_launches++;
     } else if (r.kind == 1) {
       t_decouple_ms += ms;
-    } else {
+    } else if (r.kind == 2) {
       t_top_ms += ms;
     }
     launch_log.push_back(r);
@@ -206,6 +300,12 @@ int Solver::cuda_check(cudaError_t e, const char* what) {
   do {                                                  \
     const int rc_ = cuda_check((expr), #expr);          \
     if (rc_) return rc_;                                \
+  } while (0)
+
+#define KI_UPLOAD(...)                     \
+  do {                                     \
+    const int urc_ = upload(__VA_ARGS__);  \
+    if (urc_) return urc_;                 \
   } while (0)
 
 #define KI_ALLOC(ptr, type, count)                                  \
@@ -261,8 +361,15 @@ int Solver::factor() {
   KI_CUDA(cudaEventRecord(ev0, stream_));
   t_id_ms = t_decouple_ms = t_top_ms = 0;
   id_launches = 0;
-  id_flops = id_bytes = 0;
+  id_flops = id_bytes = id_fold_flops = 0;
 
+  if (!dstream_) {
+    KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
+    KI_CUDA(cudaEventCreateWithFlags(&ev_id_, cudaEventDisableTiming));
+    KI_CUDA(cudaEventCreateWithFlags(&ev_dec_, cudaEventDisableTiming));
+  }
+  for (int G = 1; G <= 16; G *= 2)
+    onchip_ok_[G] = id_cluster_fits(kOnChip + G, 4096, 256, (227 * 1024 - id_smem_bytes(4096, 256)) / 8) != 0;
   tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
   boxdev_.assign(tree.boxes.size(), BoxDev{});
   levels_.assign(tree.levels.size(), LevelFactors{});
@@ -274,7 +381,7 @@ int Solver::factor() {
       nodes[i] = Node{pts_[2 * i], pts_[2 * i + 1], nrm_[2 * i], nrm_[2 * i + 1], wts_[i],
                       curv_[i], 0.0, 0.0};
     KI_ALLOC(d_nodes_, Node, n_points_);
-    KI_CUDA(upload(d_nodes_, nodes, stream_));
+    KI_UPLOAD(d_nodes_, nodes, stream_);
     std::vector<double> dir(2 * kNumProxy);
     for (int i = 0; i < kNumProxy; i++) {
       const double ang = 2 * M_PI * i * (1.0 / kNumProxy);
@@ -282,10 +389,10 @@ int Solver::factor() {
       dir[kNumProxy + i] = std::sin(ang);
     }
     KI_ALLOC(d_proxy_dir_, double, dir.size());
-    KI_CUDA(upload(d_proxy_dir_, dir, stream_));
+    KI_UPLOAD(d_proxy_dir_, dir, stream_);
     if (!holes_.empty()) {
       KI_ALLOC(d_holes_, double, holes_.size());
-      KI_CUDA(upload(d_holes_, holes_, stream_));
+      KI_UPLOAD(d_holes_, holes_, stream_);
     }
     KI_ALLOC(d_status_, int, 1);
     KI_CUDA(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_));
@@ -295,24 +402,33 @@ int Solver::factor() {
     std::vector<double> U, Psi;
     border_U(opt_.pde, pts_, holes_, &U, &nb_);
     border_Psi(opt_.pde, pts_, wts_, holes_, &Psi);
+    const size_t rows = Psi.size() / n_dofs_;
+    h_PsiT_.assign(Psi.size(), 0.0);
+    for (int j = 0; j < n_dofs_; j++)
+      for (size_t i = 0; i < rows; i++) h_PsiT_[j + static_cast<size_t>(n_dofs_) * i] = Psi[i + rows * j];
     KI_ALLOC(d_U_, double, U.size());
     KI_ALLOC(d_Psi_, double, Psi.size());
-    KI_CUDA(upload(d_U_, U, stream_));
-    KI_CUDA(upload(d_Psi_, Psi, stream_));
+    KI_UPLOAD(d_U_, U, stream_);
+    KI_UPLOAD(d_Psi_, Psi, stream_);
   }
 
   const int L = static_cast<int>(tree.levels.size());
   launch_log.clear();
-  t_wait_ms = 0;
+  t_wait_ms = t_host_prep_ms = t_host_post_ms = t_upload_ms = t_host_top_ms = 0;
+  g_upload_ms = 0;
   for (int level = L - 1; level > 0; level--) {
     const int rc = process_level(level);
     if (rc) return rc;
   }
   for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
   allskel = tree.boxes[0].active;
+  KI_CUDA(cudaEventRecord(ev_dec_, dstream_));
+  KI_CUDA(cudaStreamWaitEvent(stream_, ev_dec_, 0));
   cudaEvent_t t0 = nullptr;
   if (time_phases && timer_begin(&t0)) return -2;
+  const double ht = now_ms();
   int rc = factor_top();
+  t_host_top_ms = now_ms() - ht;
   if (rc) return rc;
   if (time_phases && timer_end(t0, {0, 2, 1, 1, 0, ns_ + nb_, 0.0})) return -2;
 
@@ -326,11 +442,13 @@ int Solver::factor() {
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   if (timers_resolve()) return -2;
+  t_upload_ms = g_upload_ms;
   if (status) return fail("zero pivot in an LU factorization (singular block)");
   return 0;
 }
 
 int Solver::process_level(int level) {
+  const double h0 = now_ms();
   std::vector<std::vector<int>> near(tree.boxes.size());
   tree.refresh_level(level, &near);
   const std::vector<int>& ids = tree.levels[level];
@@ -373,7 +491,7 @@ int Solver::process_level(int level) {
       c.m = 2 * c.I + P;
     }
     if (c.m == 0) continue;
-    c.g = pick_group(c.m, c.n);
+    c.g = pick_group(c.m, c.n, onchip_ok_);
     cand.push_back(std::move(c));
   }
   LevelFactors& lf = levels_[level];
@@ -396,7 +514,7 @@ int Solver::process_level(int level) {
     t.proxy = c.m - 2 * c.I;
     t.act_off = static_cast<int>(act.size());
     t.row_off = static_cast<int>(rows.size());
-    t.lda = (c.m + 3) & ~3;
+    t.lda = c.g >= kOnChip ? onchip_lda(c.m) : (c.m + 3) & ~3;
     t.perm_off = perm_total;
     t.a_off = a_total;
     t.t_off = t_total;
@@ -406,10 +524,11 @@ int Solver::process_level(int level) {
     t.pw = 2.0 * M_PI * t.rad / kNumProxy;
     act.insert(act.end(), b.active.begin(), b.active.end());
     rows.insert(rows.end(), c.rows.begin(), c.rows.end());
-    a_total += static_cast<long long>(t.lda) * c.n;
+    if (c.g < kOnChip) a_total += static_cast<long long>(t.lda) * c.n;  // on-chip: none
     t_total += static_cast<long long>(c.n) * c.n / 4 + 1;
     perm_total += c.n;
   }
+  t_host_prep_ms += now_ms() - h0;
   int *d_act, *d_rows, *d_perm, *d_rank;
   double* d_T;
   IdTask* d_tasks;
@@ -420,20 +539,31 @@ int Solver::process_level(int level) {
   KI_ALLOC(d_T, double, t_total);
   KI_ALLOC(d_tasks, IdTask, nc);
   KI_CUDA(work_.reserve(sizeof(double) * a_total, stream_));
-  KI_CUDA(upload(d_act, act, stream_));
-  KI_CUDA(upload(d_rows, rows, stream_));
-  KI_CUDA(upload(d_tasks, tasks, stream_));
+  KI_UPLOAD(d_act, act, stream_);
+  KI_UPLOAD(d_rows, rows, stream_);
+  KI_UPLOAD(d_tasks, tasks, stream_);
 
-  // one launch per cluster size
+  // one launch per cluster size (split further so that the launch's
+  // shared-memory layout, sized by its largest rows / columns / column
+  // storage, still fits)
   for (int q0 = 0; q0 < nc;) {
     int q1 = q0;
     int m_cap = 0, n_cap = 0;
-    while (q1 < nc && cand[q1].g == cand[q0].g) {
-      m_cap = std::max(m_cap, cand[q1].m);
-      n_cap = std::max(n_cap, cand[q1].n);
+    long long col_cap = 0;
+    const int g0 = cand[q0].g;
+    const int G = g0 >= kOnChip ? g0 - kOnChip : 0;
+    while (q1 < nc && cand[q1].g == g0) {
+      const int mm = std::max(m_cap, cand[q1].m), nn = std::max(n_cap, cand[q1].n);
+      long long cc = col_cap;
+      if (G) cc = std::max(cc, static_cast<long long>((cand[q1].n + G - 1) / G) *
+                                   onchip_lda(cand[q1].m));
+      if (q1 > q0 && id_smem_bytes(mm, nn) + sizeof(double) * cc > 227 * 1024) break;
+      m_cap = mm;
+      n_cap = nn;
+      col_cap = cc;
       q1++;
     }
-    if (id_smem_bytes(m_cap, n_cap) > 227 * 1024)
+    if (id_smem_bytes(m_cap, n_cap) + sizeof(double) * col_cap > 227 * 1024)
       return fail("interpolative decomposition too tall for shared staging (m = " +
                   std::to_string(m_cap) + ")");
     IdParams p{};
@@ -451,6 +581,7 @@ int Solver::process_level(int level) {
     p.tol = opt_.id_tol;
     p.m_cap = m_cap;
     p.n_cap = n_cap;
+    p.col_cap = col_cap;
     cudaEvent_t e0 = nullptr;
     if (time_phases && timer_begin(&e0)) return -2;
     KI_CUDA(launch_id(p, cand[q0].g, stream_));
@@ -471,6 +602,7 @@ int Solver::process_level(int level) {
   }
 
   // skeleton / redundant sets (InteractionLists::set_rs_ranges, quadtree.h:23-35)
+  const double h1 = now_ms();
   std::vector<int> comp;  // candidate indices that compressed
   for (int q = 0; q < nc; q++) {
     const Cand& c = cand[q];
@@ -481,8 +613,14 @@ int Solver::process_level(int level) {
     // triangular solve for T; bytes = the matrix written once and read once.
     const double m = c.m, n = c.n;
     const int steps = k > 0 ? k : std::min(c.m, c.n);
-    id_flops += 4.0 * m * (n * steps - 0.5 * steps * steps) + 1.0 * k * k * (n - k);
-    id_bytes += 16.0 * m * n;
+    const double qr = 4.0 * m * (n * steps - 0.5 * steps * steps) + 1.0 * k * k * (n - k);
+    if (c.g < kOnChip) {
+      // matrix streamed through HBM/L2: written once, read once
+      id_flops += qr;
+      id_bytes += 16.0 * m * n;
+    } else {
+      id_fold_flops += qr;  // on-chip: FP64 work only
+    }
     if (k == 0) continue;
     Box& b = tree.boxes[c.box];
     b.compressed = true;
@@ -525,8 +663,11 @@ int Solver::process_level(int level) {
     }
     build_block_map(blocks, n, &bid, &bpos, &tab);
     k_off[t] = scratch_total;
-    if (n > 160) scratch_total += static_cast<long long>(n) * n;
-    n_max = std::max(n_max, n);
+    if (n > kDecoupleSmemN) {
+      scratch_total += static_cast<long long>(n) * n;
+    } else {
+      n_max = std::max(n_max, n);
+    }
     fac_total += static_cast<size_t>(k) * r * 2 + static_cast<size_t>(r) * r +
                  static_cast<size_t>(k) * k;
     piv_total += r;
@@ -541,7 +682,7 @@ int Solver::process_level(int level) {
   KI_ALLOC(d_fac, double, fac_total);
   KI_ALLOC(d_piv, int, piv_total);
   KI_ALLOC(d_dt, DecTask, ncomp);
-  KI_CUDA(scratch2_.reserve(sizeof(double) * (scratch_total + 1), stream_));
+  KI_CUDA(scratch2_.reserve(sizeof(double) * (scratch_total + 1), dstream_));
   double* scr = static_cast<double*>(scratch2_.p);
   size_t fo = 0, po = 0;
   for (int t = 0; t < ncomp; t++) {
@@ -576,20 +717,34 @@ int Solver::process_level(int level) {
     d.acc = bd.acc;
     d.piv = bd.piv;
   }
-  KI_CUDA(upload(d_bid, bid, stream_));
-  KI_CUDA(upload(d_bpos, bpos, stream_));
-  KI_CUDA(upload(d_tab, tab, stream_));
-  KI_CUDA(upload(d_dt, dt, stream_));
+  // small boxes first in one batched launch, then each large box
+  std::vector<DecTask> small, large;
+  for (const DecTask& d : dt) (d.n > kDecoupleSmemN ? large : small).push_back(d);
+  KI_CUDA(cudaEventRecord(ev_id_, stream_));
+  KI_CUDA(cudaStreamWaitEvent(dstream_, ev_id_, 0));
+  KI_UPLOAD(d_bid, bid, dstream_);
+  KI_UPLOAD(d_bpos, bpos, dstream_);
+  KI_UPLOAD(d_tab, tab, dstream_);
+  KI_UPLOAD(d_dt, small, dstream_);
   DecParams dp{};
   dp.tasks = d_dt;
-  dp.ntasks = ncomp;
+  dp.ntasks = static_cast<int>(small.size());
   dp.pde = opt_.pde;
   dp.nodes = d_nodes_;
   dp.status = d_status_;
   cudaEvent_t d0 = nullptr;
-  if (time_phases && timer_begin(&d0)) return -2;
-  KI_CUDA(launch_decouple(dp, n_max, stream_));
-  if (time_phases && timer_end(d0, {level, 1, 1, ncomp, 0, n_max, 0.0})) return -2;
+  t_host_post_ms += now_ms() - h1;
+  if (time_phases && timer_begin(&d0, dstream_)) return -2;
+  KI_CUDA(launch_decouple(dp, n_max, dstream_));
+  int n_large = 0;
+  for (const DecTask& d : large) {
+    KI_CUDA(decouple_large(d, opt_.pde, d_nodes_, d_status_, dstream_));
+    n_large = std::max(n_large, d.n);
+  }
+  if (time_phases &&
+      timer_end(d0, {level, 1, static_cast<int>(large.size()), ncomp, n_large, n_max, 0.0},
+                dstream_))
+    return -2;
 
   // ---- sweep descriptors of the level
   std::vector<int> sk, rd;
@@ -615,9 +770,10 @@ int Solver::process_level(int level) {
     st[t] = SweepTask{b.rank, static_cast<int>(b.redundant.size()), lf.d_skel + sk_off[t],
                       lf.d_red + rd_off[t], bd.T, bd.L, bd.U, bd.X, bd.piv};
   }
-  KI_CUDA(upload(lf.d_skel, sk, stream_));
-  KI_CUDA(upload(lf.d_red, rd, stream_));
-  KI_CUDA(upload(lf.d_tasks, st, stream_));
+  KI_UPLOAD(lf.d_skel, sk, dstream_);
+  KI_UPLOAD(lf.d_red, rd, dstream_);
+  KI_UPLOAD(lf.d_tasks, st, dstream_);
+  lf.h_tasks = st;
   lf.ntasks = ncomp;
   lf.cap = cap;
   return 0;
@@ -630,21 +786,17 @@ int Solver::factor_top() {
     int cap = 0;
     for (LevelFactors& lf : levels_) {
       if (!lf.ntasks) continue;
-      std::vector<SweepTask> st(lf.ntasks);
-      KI_CUDA(cudaMemcpyAsync(st.data(), lf.d_tasks, sizeof(SweepTask) * lf.ntasks,
-                              cudaMemcpyDeviceToHost, stream_));
-      KI_CUDA(cudaStreamSynchronize(stream_));
-      all.insert(all.end(), st.begin(), st.end());
+      all.insert(all.end(), lf.h_tasks.begin(), lf.h_tasks.end());
       cap = std::max(cap, lf.cap);
     }
     all_compressed_.ntasks = static_cast<int>(all.size());
     all_compressed_.cap = cap;
     KI_ALLOC(all_compressed_.d_tasks, SweepTask, all.size());
-    KI_CUDA(upload(all_compressed_.d_tasks, all, stream_));
+    KI_UPLOAD(all_compressed_.d_tasks, all, stream_);
   }
   ns_ = static_cast<int>(allskel.size());
   KI_ALLOC(d_allskel_, int, ns_);
-  KI_CUDA(upload(d_allskel_, allskel, stream_));
+  KI_UPLOAD(d_allskel_, allskel, stream_);
   std::vector<BoxBlock> blocks;
   {
     const Box& root = tree.boxes[0];
@@ -666,9 +818,9 @@ int Solver::factor_top() {
   KI_ALLOC(d_bid, int, bid.size());
   KI_ALLOC(d_bpos, int, bpos.size());
   KI_ALLOC(d_tab, UpdBlock, tab.size());
-  KI_CUDA(upload(d_bid, bid, stream_));
-  KI_CUDA(upload(d_bpos, bpos, stream_));
-  KI_CUDA(upload(d_tab, tab, stream_));
+  KI_UPLOAD(d_bid, bid, stream_);
+  KI_UPLOAD(d_bpos, bpos, stream_);
+  KI_UPLOAD(d_tab, tab, stream_);
   const int ntop = ns_ + nb_;
   KI_ALLOC(d_top_, double, static_cast<size_t>(ntop) * ntop);
   KI_ALLOC(d_top_piv_, int, ntop);
@@ -679,7 +831,10 @@ int Solver::factor_top() {
     const int rc = factor_border();
     if (rc) return rc;
   }
+  cudaEvent_t l0 = nullptr;
+  if (time_phases && timer_begin(&l0)) return -2;
   if (ntop > 0) KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_));
+  if (time_phases && timer_end(l0, {0, 4, 1, 1, 0, ntop, 0.0})) return -2;
   return 0;
 }
 
@@ -704,23 +859,17 @@ int Solver::factor_border() {
   for (int i = 0; i < nr; i++) red_pos[allred[i]] = i;
   KI_ALLOC(d_allred_, int, nr);
   KI_ALLOC(d_red_pos_, int, N);
-  KI_CUDA(upload(d_allred_, allred, stream_));
-  KI_CUDA(upload(d_red_pos_, red_pos, stream_));
+  KI_UPLOAD(d_allred_, allred, stream_);
+  KI_UPLOAD(d_red_pos_, red_pos, stream_);
 
   double *modU, *modP;
   KI_ALLOC(modU, double, static_cast<size_t>(N) * nb);
   KI_ALLOC(modP, double, static_cast<size_t>(N) * nb);
   KI_CUDA(cudaMemcpyAsync(modU, d_U_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice, stream_));
-  {
-    std::vector<double> Psi(static_cast<size_t>(nb) * N), PsiT(static_cast<size_t>(N) * nb);
-    KI_CUDA(cudaMemcpyAsync(Psi.data(), d_Psi_, sizeof(double) * Psi.size(),
-                            cudaMemcpyDeviceToHost, stream_));
-    KI_CUDA(cudaStreamSynchronize(stream_));
-    for (int j = 0; j < N; j++)
-      for (int i = 0; i < nb; i++) PsiT[j + static_cast<size_t>(N) * i] = Psi[i + static_cast<size_t>(nb) * j];
-    KI_CUDA(upload(modP, PsiT, stream_));
-  }
+  KI_UPLOAD(modP, h_PsiT_, stream_);
   const int L = static_cast<int>(levels_.size());
+  cudaEvent_t b0 = nullptr;
+  if (time_phases && timer_begin(&b0)) return -2;
   for (int l = L - 1; l >= 0; l--) {
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
@@ -729,6 +878,7 @@ int Solver::factor_border() {
     sp.x = modP;
     KI_CUDA(launch_sweep_up(sp, true, stream_));
   }
+  if (time_phases && timer_end(b0, {0, 3, 1, nb, 0, N, 0.0})) return -2;
   double *dinv, *us, *ps, *corr;
   KI_ALLOC(d_Ured_, double, static_cast<size_t>(nr) * nb);
   KI_ALLOC(d_Pred_, double, static_cast<size_t>(nr) * nb);

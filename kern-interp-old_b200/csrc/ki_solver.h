@@ -18,10 +18,23 @@
 
 namespace kib {
 
-// Bump allocator over large cudaMalloc chunks; pointers stay valid until the
-// arena is destroyed.
+// Process-wide cache of device chunks and pinned host chunks.  A solver
+// takes chunks while it factors and hands them back when it is destroyed
+// (after its streams are idle), so repeated factorizations neither call
+// cudaMalloc/cudaHostAlloc again nor pay cudaFree's device synchronisation.
+// Cached memory is kept until ki_release_cache() or process exit.
+namespace chunk_pool {
+void* get(size_t bytes, bool pinned, size_t* got);
+void put(void* p, size_t bytes, bool pinned);
+void release_all();
+size_t cached_bytes();
+}  // namespace chunk_pool
+
+// Bump allocator over pooled chunks (device memory, or pinned host memory
+// for upload staging); pointers stay valid until the arena is destroyed.
 class Arena {
  public:
+  explicit Arena(bool pinned = false) : pinned_(pinned) {}
   ~Arena();
   void* alloc(size_t bytes);
   template <class T>
@@ -29,7 +42,8 @@ class Arena {
   size_t reserved() const { return reserved_; }
 
  private:
-  std::vector<void*> chunks_;
+  bool pinned_;
+  std::vector<std::pair<void*, size_t>> chunks_;
   char* cur_ = nullptr;
   size_t left_ = 0;
   size_t reserved_ = 0;
@@ -55,6 +69,7 @@ struct LevelFactors {
   int ntasks = 0;
   int cap = 0;
   SweepTask* d_tasks = nullptr;
+  std::vector<SweepTask> h_tasks;  // host copy of d_tasks
   int* d_skel = nullptr;
   int* d_red = nullptr;
   std::vector<int> boxes;  // compressed boxes of this level
@@ -100,7 +115,8 @@ class Solver {
   // summed duration of the ID launches, id_launches their count.
   double t_factor_ms = 0, t_id_ms = 0, t_decouple_ms = 0, t_top_ms = 0;
   int id_launches = 0;
-  double id_flops = 0, id_bytes = 0;  // algorithmic work of the ID launches
+  double id_flops = 0, id_bytes = 0;  // algorithmic work of the streamed ID launches
+  double id_fold_flops = 0;           // FP64 work of the on-chip fold ID launches
   bool time_phases = false;
   // Per-launch record of the timed factorization: kind 0 ID, 1 decouple,
   // 2 top-level assembly + LU; ms from CUDA events on the solver stream.
@@ -110,6 +126,9 @@ class Solver {
   };
   std::vector<LaunchRecord> launch_log;
   double t_wait_ms = 0;  // host time blocked on the per-level rank download
+  // host-side phases (steady clock): level list building before the ID
+  // launch, skeleton/decouple bookkeeping after it, uploads, top level
+  double t_host_prep_ms = 0, t_host_post_ms = 0, t_upload_ms = 0, t_host_top_ms = 0;
   std::string error;
 
  private:
@@ -120,8 +139,8 @@ class Solver {
     LaunchRecord rec;
   };
   std::vector<PendingTimer> pending_;
-  int timer_begin(cudaEvent_t* e0);
-  int timer_end(cudaEvent_t e0, const LaunchRecord& rec);
+  int timer_begin(cudaEvent_t* e0, cudaStream_t s = nullptr);
+  int timer_end(cudaEvent_t e0, const LaunchRecord& rec, cudaStream_t s = nullptr);
   int timers_resolve();
   int fail(const std::string& msg);
   int cuda_check(cudaError_t e, const char* what);
@@ -136,8 +155,16 @@ class Solver {
   int sd_ = 1, n_points_ = 0, n_dofs_ = 0, nb_ = 0;
   std::vector<double> pts_, nrm_, curv_, wts_, holes_;
   cudaStream_t stream_;
+  // Decoupling of level l runs on dstream_ while the host prepares, and the
+  // GPU runs, the interpolative decompositions of level l - 1.
+  cudaStream_t dstream_ = nullptr;
+  cudaEvent_t ev_id_ = nullptr, ev_dec_ = nullptr;
 
+  bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
+  Arena stage_{true};  // pinned staging of every host-to-device upload
+  template <class T>
+  int upload(T* dst, const std::vector<T>& src, cudaStream_t s);
   Scratch work_, scratch2_;
   Node* d_nodes_ = nullptr;
   double* d_proxy_dir_ = nullptr;
@@ -166,6 +193,7 @@ class Solver {
   int* d_red_pos_ = nullptr;
   double* d_U_ = nullptr;     // N x nb
   double* d_Psi_ = nullptr;   // nb x N
+  std::vector<double> h_PsiT_;  // Psi^T (N x nb), host
   double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
   double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
   double* d_tmp_ = nullptr;   // solve scratch

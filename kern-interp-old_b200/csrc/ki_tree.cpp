@@ -3,6 +3,7 @@
 // array instead of pointer-linked nodes.
 #include "ki_tree.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -46,7 +47,8 @@ void QuadTreeHost::subdivide(int id) {
   for (int q = 0; q < 4; q++)
     for (int e = 0; e < 4; e++) boxes[kid[q]].corner[edit_idx[q][e]] = edit_val[q][e];
   for (int q = 0; q < 4; q++) boxes[id].child[q] = kid[q];
-  const std::vector<int> dofs = boxes[id].original;
+  const std::vector<int>& dofs = boxes[id].original;
+  for (int q = 0; q < 4; q++) boxes[kid[q]].original.reserve(dofs.size() / 2);
   for (size_t t = 0; t < dofs.size(); t += sol_dim_) {
     const int d = dofs[t];
     const int p = d / sol_dim_;
@@ -58,14 +60,18 @@ void QuadTreeHost::subdivide(int id) {
 }
 
 void QuadTreeHost::insert(int id, double x, double y, int pt) {
-  // quadtree.cpp:164-197.
-  for (int s = 0; s < sol_dim_; s++) boxes[id].original.push_back(sol_dim_ * pt + s);
-  const int ch = boxes[id].child[pick_child(boxes[id], x, y)];
-  if (ch >= 0) {
-    insert(ch, x, y, pt);
-  } else if (boxes[id].leaf &&
-             static_cast<int>(boxes[id].original.size()) > max_leaf_) {
-    subdivide(id);
+  // quadtree.cpp:164-197: the point's dofs join every box on its path; the
+  // leaf it reaches splits once it holds more than max_leaf dofs.
+  for (;;) {
+    Box& b = boxes[id];
+    for (int s = 0; s < sol_dim_; s++) b.original.push_back(sol_dim_ * pt + s);
+    const int ch = b.child[pick_child(b, x, y)];
+    if (ch >= 0) {
+      id = ch;
+      continue;
+    }
+    if (b.leaf && static_cast<int>(b.original.size()) > max_leaf_) subdivide(id);
+    return;
   }
 }
 
@@ -98,7 +104,7 @@ void QuadTreeHost::neighbor_lists() {
       if (par >= 0) {
         for (int q = 0; q < 4; q++)
           if (boxes[par].child[q] != a) boxes[a].nbr.push_back(boxes[par].child[q]);
-        const std::vector<int> pn = boxes[par].nbr;
+        const std::vector<int>& pn = boxes[par].nbr;  // not modified below
         for (int o : pn) {
           for (int q = 0; q < 4; q++) {
             const int cz = boxes[o].child[q];
@@ -131,6 +137,7 @@ void QuadTreeHost::build(const double* points, int n, int sol_dim,
   max_leaf_ = max_leaf_dofs;
   boxes.clear();
   levels.clear();
+  boxes.reserve(8 * (static_cast<size_t>(n) * sol_dim / std::max(1, max_leaf_dofs)) + 64);
   min_ = max_ = pts_[0];
   for (double v : pts_) {
     if (v < min_) min_ = v;

@@ -201,12 +201,15 @@ class Solver(_Tree):
         return out
 
     def stats(self):
-        out = np.zeros(8)
-        self.lib.ki_stats(self.h, _d(out), 8)
+        out = np.zeros(13)
+        self.lib.ki_stats(self.h, _d(out), 13)
         return {"factor_ms": float(out[0]), "id_ms": float(out[1]),
                 "id_launches": int(out[2]), "id_flops": float(out[3]),
                 "id_bytes": float(out[4]), "decouple_ms": float(out[5]),
-                "top_ms": float(out[6]), "wait_ms": float(out[7])}
+                "top_ms": float(out[6]), "wait_ms": float(out[7]),
+                "host_prep_ms": float(out[8]), "host_post_ms": float(out[9]),
+                "upload_ms": float(out[10]), "host_top_ms": float(out[11]),
+                "id_fold_flops": float(out[12])}
 
     def launch_log(self):
         n = self.lib.ki_launch_log(self.h, None, 0)
