@@ -62,14 +62,40 @@ def peaks():
 
 
 def traffic_from_profile(workload):
-    """DRAM bytes per ID launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "id_kernel_traffic.json")
+    """DRAM bytes per ID launch (read + write, averaged over the ID launches of
+    one factorization) from the committed ncu summary of this workload."""
+    import re
+    path = os.path.join(ROOT, "profiles", "id_kernel_%s.txt" % workload)
     try:
         with open(path) as f:
-            d = json.load(f)
-        return d.get(workload, {}).get("dram_bytes_per_launch")
-    except Exception:
+            m = re.search(r"^dram_bytes_per_id_launch:\s*([0-9.eE+]+)", f.read(), re.M)
+        return float(m.group(1)) if m else None
+    except OSError:
         return None
+
+
+def fp64_peak_tflops(dev):
+    """FP64 compute roof measured on this GPU: cuBLAS DGEMM 4096^3 (2 n^3
+    flops), best of 5, CUDA events.  The B200's FP64 FMA pipe and its FP64
+    tensor path have the same nominal rate; tcgen05 has no FP64 kind."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, device=dev, dtype=torch.float64)
+    b = torch.randn(n, n, device=dev, dtype=torch.float64)
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = float("inf")
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
 class Clocks:
@@ -225,7 +251,7 @@ def main():
     clocks = Clocks(local)
     launches0 = kinterp.kernel_launches()
     total_ms = 0.0
-    id_ms = id_bytes = id_launch = 0.0
+    id_ms = id_flops = id_bytes = id_launch = 0.0
     factor_ms = []
     kinds = {}
     for _ in range(args.steps):
@@ -241,6 +267,7 @@ def main():
         st = s.stats()
         factor_ms.append(st["factor_ms"])
         id_ms += st["id_ms"]
+        id_flops += st["id_flops"]
         id_bytes += st["id_bytes"]
         id_launch += st["id_launches"]
         for row in s.launch_log():
@@ -287,8 +314,9 @@ def main():
         u = s.eval_targets(pr.targets, mu_h, al_h)
         analytic = float(np.linalg.norm(u - pr.exact) / np.linalg.norm(pr.exact))
         s.close()
-        peak, peak_kind = peaks()
-        achieved = (id_bytes / (id_ms * 1e-3)) / 1e9 if id_ms > 0 else None
+        hbm_peak, hbm_kind = peaks()
+        fp64_peak = fp64_peak_tflops(dev)
+        achieved = (id_flops / (id_ms * 1e-3)) / 1e12 if id_ms > 0 else None
         traffic = traffic_from_profile(args.workload)
         h2d = 8 * (6 * pr.n_points + units)
         d2h = 8 * (units + nb)
@@ -308,12 +336,20 @@ def main():
             "phase_ms_per_step": {"id": kinds.get(0, 0.0) / args.steps,
                                   "decouple": kinds.get(1, 0.0) / args.steps,
                                   "top": kinds.get(2, 0.0) / args.steps},
-            "roofline": {"kernel": "id_kernel (ID-matrix generation + pivoted QR)",
-                         "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                         "peak_source": peak_kind,
-                         "algorithmic_bytes_per_launch": id_bytes / max(id_launch, 1),
+            "roofline": {"kernel": "ID kernels (id_onchip_kernel / id_kernel: entry generation, "
+                                   "pivoted QR, T)",
+                         "bound": "tensor", "pipe": "fp64 (no tcgen05 FP64 kind; FP64 FMA)",
+                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": (achieved / fp64_peak) if achieved else None,
+                         "peak_source": "measured live on this GPU: cuBLAS DGEMM 4096^3 "
+                                        "(no FP64 figure in MEASURED_PEAKS.json)",
+                         "flops_per_launch": id_flops / max(id_launch, 1),
+                         "algorithmic_hbm_bytes_per_launch": id_bytes / max(id_launch, 1),
+                         "hbm_frac_of_measured": ((id_bytes / (id_ms * 1e-3)) / 1e9 / hbm_peak)
+                         if id_ms > 0 else None,
+                         "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_kind,
                          "launches_per_step": id_launch / args.steps,
+                         "ms_per_step": id_ms / args.steps,
                          "traffic": traffic},
             "e2e": {"value": world * units * args.steps / (e2e_max * 1e-3),
                     "unit": "unknowns/s", "h2d_bytes_per_step": h2d,

@@ -87,10 +87,60 @@ int ki_solve_device(ki_solver_t s, const double* d_f, double* d_mu, double* d_al
  * [U; Psi, -I] when there are holes; device buffers of dofs + border. */
 int ki_apply_device(ki_solver_t s, const double* d_x, double* d_y);
 
+/* The bordered solve with a nonzero border right-hand side g (nb values,
+ * NULL = zero): [A U; Psi -I][mu; alpha] = [f; g].  The reference solves
+ * only g = 0 (skel_factorization.cpp:406-551); the refinement needs the
+ * general form to precondition residuals. */
+int ki_solve_bordered_device(ki_solver_t s, const double* d_f, const double* d_g, double* d_mu,
+                             double* d_alpha);
+
+/* FP64 refinement (no counterpart in the reference, whose linear_solve is
+ * the direct solve only, linear_solve.cpp:113-124): right-preconditioned
+ * GMRES on the operator of ki_apply_device with this factorization as the
+ * preconditioner, stopping when the true relative residual
+ * ||[f; 0] - A [mu; alpha]|| / ||f|| <= rel_tol or after max_iters
+ * preconditioned products (each = one solve + one operator product).
+ * iters and rel_res (may be NULL) report the products used and the final
+ * true residual.  Use with a factorization at a looser id_tol (or the
+ * reduced-precision one of ki_factor_ex) to reach FP64 accuracy. */
+int ki_solve_refined_device(ki_solver_t s, const double* d_f, double* d_mu, double* d_alpha,
+                            double rel_tol, int max_iters, int* iters, double* rel_res);
+/* Same with host buffers (copies inside the call; returns when mu and alpha
+ * are in host memory). */
+int ki_solve_refined(ki_solver_t s, const double* f, double* mu, double* alpha, double rel_tol,
+                     int max_iters, int* iters, double* rel_res);
+/* The refinement's operator product: same y as ki_apply_device up to FP64
+ * rounding (fused and reassociated, not bit-identical to the entries). */
+int ki_matvec_device(ki_solver_t s, const double* d_x, double* d_y);
+
+/* x = A^-T b with the factorization (no reference counterpart: the
+ * reference solves only with A, skel_factorization.cpp:341-403).  Simply
+ * connected domains only.  d_b and d_x may be the same buffer. */
+int ki_solve_transpose_device(ki_solver_t s, const double* d_b, double* d_x);
+
+/* Differentiable target potential u = K_t A^-1 f (Laplace double layer,
+ * simply connected; the target map of linear_solve.cpp:126-140), as the
+ * forward/backward pair of an autograd function.  Forward: d_mu = A^-1 d_f
+ * (kept by the caller for the backward) and d_u = K_t d_mu at n_targets
+ * points (interleaved xy).  Backward: given d_grad_u = dJ/du, writes
+ * dJ/df = A^-T K_t^T grad_u (n dofs) and dJ/d(points) (2n), dJ/d(normals)
+ * (2n), dJ/d(weights) (n), dJ/d(curvatures) (n), the node geometry held
+ * by the handle; chain them to any shape parameters on the caller's side.
+ * No reference counterpart (the reference has no derivatives). */
+int ki_adjoint_forward(ki_solver_t s, const double* d_f, int n_targets, const double* d_targets,
+                       double* d_mu, double* d_u);
+int ki_adjoint_backward(ki_solver_t s, int n_targets, const double* d_targets, const double* d_mu,
+                        const double* d_grad_u, double* d_grad_f, double* d_grad_points,
+                        double* d_grad_normals, double* d_grad_weights,
+                        double* d_grad_curvatures);
+
 /* schur_solve's target evaluation (linear_solve.cpp:126-140): out = K_domain
  * mu + U_forward alpha at n_targets points (interleaved xy). */
 int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets,
                     const double* mu, const double* alpha, double* out);
+/* Same on device buffers (targets, mu, alpha, out), stream-ordered. */
+int ki_eval_targets_device(ki_solver_t s, int n_targets, const double* d_targets,
+                           const double* d_mu, const double* d_alpha, double* d_out);
 
 /* Kernel::operator() (kernel/kernel.cpp:99-111): column-major nt x ns block
  * K(tgt, src) evaluated on the GPU. */
@@ -110,11 +160,13 @@ int ki_box_lists(ki_solver_t s, int level, int idx, int* original, int* active,
 int ki_allskel(ki_solver_t s, int* out);
 
 /* Statistics of the last factorization: out[0] factor ms, [1] ID kernel ms,
- * [2] ID launches, [3] ID algorithmic flops, [4] ID algorithmic bytes,
+ * [2] ID launches, [3] ID algorithmic FP64 flops (entry generation,
+ * Householder steps taken, T solve), [4] ID algorithmic HBM bytes (inputs,
+ * outputs, and the working matrix of launches that stream it),
  * [5] decouple ms, [6] top-level LU ms, [7] host ms blocked on rank
  * downloads, host ms spent on [8] level lists before the ID launches,
  * [9] skeleton/decouple bookkeeping, [10] uploads, [11] the top level,
- * [12] FP64 flops of the on-chip fold IDs (timed factorizations only for
+ * [12] the part of [3] done by on-chip launches (timed factorizations only for
  * [1], [5], [6]).  Returns the number of values written (at most n, at
  * most 13). */
 int ki_stats(ki_solver_t s, double* out, int n);
@@ -122,6 +174,14 @@ int ki_stats(ki_solver_t s, double* out, int n);
  * (level, kind 0 ID / 1 decouple / 2 top LU, cluster size, boxes, max rows,
  * max columns, ms).  Returns the row count; writes at most cap rows. */
 int ki_launch_log(ki_solver_t s, double* out, int cap);
+/* Timeline of a ki_factor_timed factorization: rows of 4 doubles
+ * (what, level, start ms, end ms) after the factorization began: `what` <
+ * 100 is a launch kind of ki_launch_log timed on the GPU clock; `what` =
+ * 100 + code is a host mark (0 tree built, 1 level lists ready and ID
+ * launched, 2 ranks received, 3 decouple launched, 4 top level started,
+ * 5 top level launched, 6 synchronised) on the host clock.  Returns the row
+ * count; writes at most cap rows. */
+int ki_timeline(ki_solver_t s, double* out, int cap);
 
 /* Enables CUDA-event timing of the ID launches for the next ki_factor calls
  * made through ki_factor_timed. */
@@ -129,6 +189,26 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
                     const double* curvatures, const double* weights, int n_holes,
                     const double* holes, int max_leaf_dofs, double id_tol, void* stream,
                     ki_solver_t* out);
+
+/* Many independent problems factored together (no reference counterpart:
+ * the reference factors one boundary per QuadTree).  Problem p has
+ * n_points[p] nodes; the geometry arrays are the problems' arrays laid end
+ * to end (points/normals interleaved xy), and so are the dofs of every
+ * later call (ki_solve, ki_solve_device, ki_solve_refined[_device]): the
+ * handle holds one quadtree per problem, and every level of every tree is
+ * processed by the same launches.  Each problem gets exactly the partition,
+ * skeletons and factors it would get alone.  Simply connected domains only
+ * (no holes); n_problems >= 1. */
+int ki_factor_batch(int pde, int n_problems, const int* n_points, const double* points,
+                    const double* normals, const double* curvatures, const double* weights,
+                    int max_leaf_dofs, double id_tol, void* stream, ki_solver_t* out);
+/* The partition of a batch only (host; like ki_partition per problem). */
+int ki_partition_batch(int n_problems, const int* n_points, const double* points, int sol_dim,
+                       int max_leaf_dofs, ki_solver_t* out);
+/* Number of problems in the handle (1 for ki_factor). */
+int ki_num_problems(ki_solver_t s);
+/* Problem index of box idx of level `level` (negative on error). */
+int ki_box_tree(ki_solver_t s, int level, int idx);
 
 /* Interpolative decomposition of one box that allocates no device memory,
  * for callers that cannot call cudaMalloc (their device memory is owned by

@@ -13,13 +13,32 @@ namespace kib {
 
 namespace {
 
+// Segment (problem) of a node: seg[p] <= node < seg[p + 1].
+__device__ __forceinline__ int apply_segment(const int* __restrict__ seg, int nseg, int node) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg[mid] <= node) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 __global__ void apply_kernel(int pde, const Node* __restrict__ nodes, int n,
+                             const int* __restrict__ seg, int nseg,
                              const double* __restrict__ x, double* __restrict__ y, int nb,
                              const double* __restrict__ U, const double* __restrict__ Psi) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
+    // a forest's operator is block diagonal: sources of the row's problem
+    const int sd = pde == kStokes ? 2 : 1;
+    int j0 = 0, j1 = n;
+    if (seg) {
+      const int p = apply_segment(seg, nseg, i / sd);
+      j0 = seg[p] * sd;
+      j1 = seg[p + 1] * sd;
+    }
     double s = 0.0;
-    for (int j = 0; j < n; j++) s += boundary_entry(pde, nodes, i, j) * x[j];
+    for (int j = j0; j < j1; j++) s += boundary_entry(pde, nodes, i, j) * x[j];
     for (int b = 0; b < nb; b++) s += U[i + static_cast<long long>(n) * b] * x[n + b];
     y[i] = s;
   } else if (i < n + nb) {
@@ -53,17 +72,30 @@ __device__ void border_u(int pde, double tx, double ty, const double* hole, int 
   }
 }
 
-__global__ void targets_kernel(int pde, const Node* __restrict__ nodes, int n, int nt,
-                               const double* __restrict__ tg, const double* __restrict__ mu,
-                               int nh, const double* __restrict__ holes,
-                               const double* __restrict__ alpha, double* __restrict__ out) {
+// One CTA per target row: the threads stride over the source dofs and the
+// partial sums are reduced in a fixed order (each entry is the exact
+// forward entry; only the summation order differs from a serial sum).
+constexpr int kTgtThreads = 256;
+__global__ void __launch_bounds__(kTgtThreads)
+    targets_kernel(int pde, const Node* __restrict__ nodes, int n, int nt,
+                   const double* __restrict__ tg, const double* __restrict__ mu, int nh,
+                   const double* __restrict__ holes, const double* __restrict__ alpha,
+                   double* __restrict__ out) {
+  __shared__ double red[kTgtThreads / 32];
   const int sd = pde == kStokes ? 2 : 1;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= nt * sd) return;
+  const int row = blockIdx.x;
   const int t = row / sd, comp = row % sd;
   const double tx = tg[2 * t], ty = tg[2 * t + 1];
   double s = 0.0;
-  for (int j = 0; j < n; j++) s += forward_entry(pde, nodes, tx, ty, comp, j) * mu[j];
+  for (int j = threadIdx.x; j < n; j += kTgtThreads)
+    s += forward_entry(pde, nodes, tx, ty, comp, j) * mu[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  s = 0.0;
+  for (int w = 0; w < kTgtThreads / 32; w++) s += red[w];
   if (alpha && pde != kLaplaceNeumann) {
     for (int h = 0; h < nh; h++) {
       double u[3];
@@ -88,12 +120,13 @@ __global__ void block_kernel(int pde, const Node* __restrict__ nodes, const int*
 
 }  // namespace
 
-cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const double* x,
-                                  double* y, int nb, const double* U, const double* Psi,
-                                  cudaStream_t s) {
+cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const int* seg,
+                                  int nseg, const double* x, double* y, int nb, const double* U,
+                                  const double* Psi, cudaStream_t s) {
   const int rows = n_dofs + nb;
   count_launches(1);
-  apply_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, x, y, nb, U, Psi);
+  apply_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, seg, nseg, x, y, nb, U,
+                                                  Psi);
   return cudaGetLastError();
 }
 
@@ -104,8 +137,8 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
   const int rows = nt * (pde == kStokes ? 2 : 1);
   if (rows == 0) return cudaSuccess;
   count_launches(1);
-  targets_kernel<<<(rows + 127) / 128, 128, 0, s>>>(pde, nodes, n_dofs, nt, targets, mu, nh,
-                                                     holes, alpha, out);
+  targets_kernel<<<rows, kTgtThreads, 0, s>>>(pde, nodes, n_dofs, nt, targets, mu, nh, holes,
+                                               alpha, out);
   return cudaGetLastError();
 }
 

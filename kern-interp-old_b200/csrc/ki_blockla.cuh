@@ -259,6 +259,77 @@ __device__ inline void warp_lu_solve_t(const double* lu, int n, int ld, const in
   __syncwarp();
 }
 
+// x <- A^{-1} x for the LU above, x in shared memory (n values), by the
+// whole CTA (blockDim >= 32): row interchanges, then blocked forward (unit
+// L) and backward (U) substitution in 32-row blocks; warp 0 solves each
+// diagonal block from registers, then every thread updates its rows with
+// the block's 32 values.  Ends with a barrier.
+__device__ inline void cta_lu_solve(const double* __restrict__ lu, int n, int ld,
+                                    const int* __restrict__ ipiv, double* x) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; i++) {
+      const int p = ipiv[i];
+      if (p != i) {
+        const double t = x[i];
+        x[i] = x[p];
+        x[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int kb = 0; kb < n; kb += 32) {  // L y = P b
+    const int nbk = min(32, n - kb);
+    if (warp == 0) {
+      double Lr[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+        Lr[k] = (lane < nbk && k < lane) ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)] : 0.0;
+      double xv = lane < nbk ? x[kb + lane] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        const double xk = __shfl_sync(0xffffffffu, xv, k);
+        xv -= Lr[k] * xk;  // Lr[k] = 0 unless k < lane
+      }
+      if (lane < nbk) x[kb + lane] = xv;
+    }
+    __syncthreads();
+    for (int i = kb + nbk + threadIdx.x; i < n; i += blockDim.x) {
+      double s = 0.0;
+      for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(ld) * (kb + k)] * x[kb + k];
+      x[i] -= s;
+    }
+    __syncthreads();
+  }
+  for (int kb = ((n - 1) / 32) * 32; kb >= 0; kb -= 32) {  // U x = y
+    const int nbk = min(32, n - kb);
+    if (warp == 0) {
+      double Ur[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+        Ur[k] = (lane < nbk && k < nbk && k >= lane)
+                    ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)]
+                    : 0.0;
+      double xv = lane < nbk ? x[kb + lane] : 0.0;
+#pragma unroll
+      for (int k = 31; k >= 0; k--) {
+        if (k < nbk) {
+          if (lane == k) xv /= Ur[k];
+          const double xk = __shfl_sync(0xffffffffu, xv, k);
+          if (lane < k) xv -= Ur[k] * xk;
+        }
+      }
+      if (lane < nbk) x[kb + lane] = xv;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kb; i += blockDim.x) {
+      double s = 0.0;
+      for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(ld) * (kb + k)] * x[kb + k];
+      x[i] -= s;
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace kib
 
 #endif  // KI_BLOCKLA_CUH_

@@ -81,7 +81,7 @@ bool box_ref(ki_solver_t s, int level, int idx, const kib::Box** out, int* paren
 int factor_impl(int pde, int n_points, const double* points, const double* normals,
                 const double* curvatures, const double* weights, int n_holes,
                 const double* holes, int max_leaf_dofs, double id_tol, void* stream,
-                ki_solver_t* out, bool timed) {
+                ki_solver_t* out, bool timed, const std::vector<int>* starts = nullptr) {
   if (!out) return set_err(KI_ERR_ARG, "ki_factor: out is NULL");
   *out = nullptr;
   if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_factor: bad pde");
@@ -109,6 +109,7 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
   h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, n_holes,
                                   holes, h->stream));
   h->solver->time_phases = timed;
+  if (starts) h->solver->set_forest(*starts);
   const int rc = h->solver->factor();
   if (rc) return from_solver(h.get(), rc);
   *out = h.release();
@@ -145,6 +146,34 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
                      max_leaf_dofs, id_tol, stream, out, true);
 }
 
+int ki_factor_batch(int pde, int n_problems, const int* n_points, const double* points,
+                    const double* normals, const double* curvatures, const double* weights,
+                    int max_leaf_dofs, double id_tol, void* stream, ki_solver_t* out) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_factor_batch: out is NULL");
+  *out = nullptr;
+  if (n_problems < 1 || !n_points) return set_err(KI_ERR_ARG, "ki_factor_batch: no problems");
+  std::vector<int> starts(1, 0);
+  long long total = 0;
+  for (int p = 0; p < n_problems; p++) {
+    if (n_points[p] <= 0)
+      return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+    total += n_points[p];
+    if (total > (1LL << 30)) return set_err(KI_ERR_ARG, "ki_factor_batch: too many points");
+    starts.push_back(static_cast<int>(total));
+  }
+  return factor_impl(pde, static_cast<int>(total), points, normals, curvatures, weights, 0,
+                     nullptr, max_leaf_dofs, id_tol, stream, out, false, &starts);
+}
+
+int ki_num_problems(ki_solver_t s) { return s && s->solver ? s->solver->n_trees() : -KI_ERR_ARG; }
+
+int ki_box_tree(ki_solver_t s, int level, int idx) {
+  const kib::Box* b;
+  int par;
+  if (!box_ref(s, level, idx, &b, &par)) return -set_err(KI_ERR_ARG, "ki_box_tree: bad box");
+  return b->tree;
+}
+
 int ki_partition(int n_points, const double* points, int sol_dim, int max_leaf_dofs,
                  ki_solver_t* out) {
   if (!out) return set_err(KI_ERR_ARG, "ki_partition: out is NULL");
@@ -161,6 +190,40 @@ int ki_partition(int n_points, const double* points, int sol_dim, int max_leaf_d
   std::vector<double> zeros(2 * static_cast<size_t>(n_points), 0.0);
   h->solver.reset(new kib::Solver(opt, n_points, points, zeros.data(), zeros.data(),
                                   zeros.data(), 0, nullptr, nullptr));
+  h->solver->build_tree_only();
+  h->tree_only = true;
+  *out = h.release();
+  return KI_OK;
+}
+
+int ki_partition_batch(int n_problems, const int* n_points, const double* points, int sol_dim,
+                       int max_leaf_dofs, ki_solver_t* out) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_partition_batch: out is NULL");
+  *out = nullptr;
+  if (n_problems < 1 || !n_points || !points)
+    return set_err(KI_ERR_ARG, "ki_partition_batch: no problems");
+  if (sol_dim != 1 && sol_dim != 2)
+    return set_err(KI_ERR_ARG, "ki_partition_batch: sol_dim must be 1 or 2");
+  if (max_leaf_dofs < 1) return set_err(KI_ERR_ARG, "ki_partition_batch: max_leaf_dofs must be >= 1");
+  std::vector<int> starts(1, 0);
+  long long total = 0;
+  for (int p = 0; p < n_problems; p++) {
+    if (n_points[p] <= 0)
+      return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+    total += n_points[p];
+    if (total > (1LL << 30)) return set_err(KI_ERR_ARG, "ki_partition_batch: too many points");
+    starts.push_back(static_cast<int>(total));
+  }
+  std::unique_ptr<ki_solver_s> h(new (std::nothrow) ki_solver_s());
+  if (!h) return set_err(KI_ERR_ARG, "out of host memory");
+  kib::SolverOptions opt;
+  opt.pde = sol_dim == 2 ? KI_STOKES : KI_LAPLACE;
+  opt.max_leaf_dofs = max_leaf_dofs;
+  const int n = static_cast<int>(total);
+  std::vector<double> zeros(2 * static_cast<size_t>(n), 0.0);
+  h->solver.reset(new kib::Solver(opt, n, points, zeros.data(), zeros.data(), zeros.data(), 0,
+                                  nullptr, nullptr));
+  h->solver->set_forest(starts);
   h->solver->build_tree_only();
   h->tree_only = true;
   *out = h.release();
@@ -201,6 +264,111 @@ int ki_solve(ki_solver_t s, const double* f, double* mu, double* alpha) {
   return cuda_err(cudaStreamSynchronize(s->stream), "ki_solve");
 }
 
+int ki_solve_bordered_device(ki_solver_t s, const double* d_f, const double* d_g, double* d_mu,
+                             double* d_alpha) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_f || !d_mu) return set_err(KI_ERR_ARG, "ki_solve_bordered_device: bad args");
+  if (s->solver->n_border() > 0 && !d_alpha)
+    return set_err(KI_ERR_ARG, "ki_solve_bordered_device: alpha required for a domain with holes");
+  return from_solver(s, s->solver->solve_device(d_f, d_mu, d_alpha,
+                                                s->solver->n_border() ? d_g : nullptr));
+}
+
+int ki_solve_refined_device(ki_solver_t s, const double* d_f, double* d_mu, double* d_alpha,
+                            double rel_tol, int max_iters, int* iters, double* rel_res) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_f || !d_mu || !(rel_tol >= 0.0) || max_iters < 1)
+    return set_err(KI_ERR_ARG, "ki_solve_refined_device: bad args");
+  if (s->solver->n_border() > 0 && !d_alpha)
+    return set_err(KI_ERR_ARG, "ki_solve_refined_device: alpha required for a domain with holes");
+  return from_solver(s, s->solver->solve_refined(d_f, d_mu, d_alpha, rel_tol, max_iters, iters,
+                                                 rel_res));
+}
+
+int ki_solve_refined(ki_solver_t s, const double* f, double* mu, double* alpha, double rel_tol,
+                     int max_iters, int* iters, double* rel_res) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !f || !mu || !(rel_tol >= 0.0) || max_iters < 1)
+    return set_err(KI_ERR_ARG, "ki_solve_refined: bad args");
+  const int N = s->solver->n_dofs(), nb = s->solver->n_border();
+  if (nb > 0 && !alpha)
+    return set_err(KI_ERR_ARG, "ki_solve_refined: alpha required for a domain with holes");
+  KI_TRY(staging(s, sizeof(double) * (2 * static_cast<size_t>(N) + nb + 1)));
+  double* d_f = s->d_io;
+  double* d_x = d_f + N;
+  double* d_a = d_x + N;
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_f, f, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream),
+                  "copy f"));
+  KI_TRY(from_solver(s, s->solver->solve_refined(d_f, d_x, nb ? d_a : nullptr, rel_tol,
+                                                 max_iters, iters, rel_res)));
+  KI_TRY(cuda_err(cudaMemcpyAsync(mu, d_x, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream),
+                  "copy mu"));
+  if (nb > 0)
+    KI_TRY(cuda_err(cudaMemcpyAsync(alpha, d_a, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                    s->stream),
+                    "copy alpha"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_solve_refined");
+}
+
+int ki_matvec_device(ki_solver_t s, const double* d_x, double* d_y) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_x || !d_y) return set_err(KI_ERR_ARG, "ki_matvec_device: bad args");
+  return from_solver(s, s->solver->matvec_device(d_x, d_y));
+}
+
+int ki_solve_transpose_device(ki_solver_t s, const double* d_b, double* d_x) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_b || !d_x) return set_err(KI_ERR_ARG, "ki_solve_transpose_device: bad args");
+  if (s->solver->n_border() > 0)
+    return set_err(KI_ERR_ARG, "ki_solve_transpose_device: domains with holes are not supported");
+  return from_solver(s, s->solver->solve_transpose_device(d_b, d_x));
+}
+
+int ki_eval_targets_device(ki_solver_t s, int n_targets, const double* d_targets,
+                           const double* d_mu, const double* d_alpha, double* d_out) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || n_targets < 0 || (n_targets > 0 && (!d_targets || !d_out)) || !d_mu)
+    return set_err(KI_ERR_ARG, "ki_eval_targets_device: bad args");
+  if (n_targets == 0) return KI_OK;
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, "ki_eval_targets_device: not available for a batch of problems");
+  kib::Solver& sv = *s->solver;
+  const bool use_alpha = sv.n_border() > 0 && d_alpha;
+  return cuda_err(kib::launch_eval_targets(sv.pde(), sv.d_nodes(), sv.n_dofs(), n_targets,
+                                           d_targets, d_mu, sv.n_holes(), sv.d_holes(),
+                                           use_alpha ? d_alpha : nullptr, d_out, s->stream),
+                  "ki_eval_targets_device");
+}
+
+int ki_adjoint_forward(ki_solver_t s, const double* d_f, int n_targets, const double* d_targets,
+                       double* d_mu, double* d_u) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_f || !d_mu || n_targets < 0 || (n_targets > 0 && (!d_targets || !d_u)))
+    return set_err(KI_ERR_ARG, "ki_adjoint_forward: bad args");
+  if (s->solver->pde() != KI_LAPLACE || s->solver->n_border() > 0)
+    return set_err(KI_ERR_ARG,
+                   "ki_adjoint_forward: only the Laplace double layer on a simply connected domain");
+  KI_TRY(from_solver(s, s->solver->solve_device(d_f, d_mu, nullptr)));
+  return ki_eval_targets_device(s, n_targets, d_targets, d_mu, nullptr, d_u);
+}
+
+int ki_adjoint_backward(ki_solver_t s, int n_targets, const double* d_targets, const double* d_mu,
+                        const double* d_grad_u, double* d_grad_f, double* d_grad_points,
+                        double* d_grad_normals, double* d_grad_weights,
+                        double* d_grad_curvatures) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || n_targets < 0 || (n_targets > 0 && (!d_targets || !d_grad_u)) ||
+      !d_mu || !d_grad_f || !d_grad_points || !d_grad_normals || !d_grad_weights ||
+      !d_grad_curvatures)
+    return set_err(KI_ERR_ARG, "ki_adjoint_backward: bad args");
+  if (s->solver->pde() != KI_LAPLACE || s->solver->n_border() > 0)
+    return set_err(KI_ERR_ARG,
+                   "ki_adjoint_backward: only the Laplace double layer on a simply connected domain");
+  return from_solver(s, s->solver->adjoint_backward(n_targets, d_targets, d_mu, d_grad_u,
+                                                    d_grad_f, d_grad_points, d_grad_normals,
+                                                    d_grad_weights, d_grad_curvatures));
+}
+
 int ki_apply_device(ki_solver_t s, const double* d_x, double* d_y) {
   if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
   if (!s || !s->solver || !d_x || !d_y) return set_err(KI_ERR_ARG, "ki_apply_device: bad args");
@@ -213,6 +381,8 @@ int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets, const d
   if (!s || !s->solver || n_targets < 0 || (n_targets > 0 && (!targets || !out)) || !mu)
     return set_err(KI_ERR_ARG, "ki_eval_targets: bad args");
   if (n_targets == 0) return KI_OK;
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, "ki_eval_targets: not available for a batch of problems");
   kib::Solver& sv = *s->solver;
   const int N = sv.n_dofs(), nb = sv.n_border(), sd = sv.sol_dim();
   const bool use_alpha = nb > 0 && alpha;
@@ -335,6 +505,29 @@ int ki_launch_log(ki_solver_t s, double* out, int cap) {
   return static_cast<int>(log.size());
 }
 
+int ki_timeline(ki_solver_t s, double* out, int cap) {
+  if (!s || !s->solver) return -KI_ERR_ARG;
+  const auto& log = s->solver->launch_log;
+  const auto& hm = s->solver->host_marks;
+  const int total = static_cast<int>(log.size() + hm.size());
+  int i = 0;
+  for (const auto& r : log) {
+    if (out && i < cap) {
+      const double row[4] = {double(r.kind), double(r.level), r.t0, r.t1};
+      std::memcpy(out + 4 * i, row, sizeof(row));
+    }
+    i++;
+  }
+  for (const auto& m : hm) {
+    if (out && i < cap) {
+      const double row[4] = {100.0 + m.code, double(m.level), m.ms, m.ms};
+      std::memcpy(out + 4 * i, row, sizeof(row));
+    }
+    i++;
+  }
+  return total;
+}
+
 int ki_stats(ki_solver_t s, double* out, int n) {
   if (!s || !s->solver || !out) return -KI_ERR_ARG;
   const kib::Solver& v = *s->solver;
@@ -342,7 +535,7 @@ int ki_stats(ki_solver_t s, double* out, int n) {
                          v.id_flops,       v.id_bytes,       v.t_decouple_ms,
                          v.t_top_ms,       v.t_wait_ms,      v.t_host_prep_ms,
                          v.t_host_post_ms, v.t_upload_ms,    v.t_host_top_ms,
-                         v.id_fold_flops};
+                         v.id_onchip_flops};
   const int cnt = n < 13 ? n : 13;
   for (int i = 0; i < cnt; i++) out[i] = vals[i];
   return cnt;

@@ -99,6 +99,95 @@ __global__ void __launch_bounds__(1024) panel_lu_kernel(double* a, int n, int ld
   }
 }
 
+// The same panel factorization with the panel staged in shared memory
+// (rows n - j0, w columns, leading dimension ldp): the column steps touch
+// only on-chip data, and the panel is written back once.
+__global__ void __launch_bounds__(1024) panel_lu_smem_kernel(double* a, int n, int ld, int j0,
+                                                             int w, int* ipiv, int* status) {
+  extern __shared__ double P[];
+  __shared__ double red[32];
+  __shared__ int redi[32];
+  __shared__ int sp;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  const int rows = n - j0, ldp = rows | 1;
+  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
+    const int i = e % rows, c = e / rows;
+    P[i + ldp * c] = a[j0 + i + static_cast<long long>(ld) * (j0 + c)];
+  }
+  __syncthreads();
+  for (int jj = 0; jj < w; jj++) {
+    const double* col = P + ldp * jj;
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int i = jj + threadIdx.x; i < rows; i += blockDim.x) {
+      const double v = fabs(col[i]);
+      if (v > bv || (v == bv && i < bp)) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double v = lane < nw ? red[lane] : -1.0;
+      int q = lane < nw ? redi[lane] : 0x7fffffff;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oq = __shfl_xor_sync(0xffffffffu, q, o);
+        if (ov > v || (ov == v && oq < q)) {
+          v = ov;
+          q = oq;
+        }
+      }
+      if (lane == 0) {
+        sp = q;
+        ipiv[j0 + jj] = j0 + q;
+      }
+    }
+    __syncthreads();
+    const int p = sp;
+    if (p != jj && threadIdx.x < w) {
+      double* x = P + ldp * threadIdx.x;
+      const double t = x[jj];
+      x[jj] = x[p];
+      x[p] = t;
+    }
+    __syncthreads();
+    const double piv = col[jj];
+    if (piv == 0.0) {
+      if (threadIdx.x == 0) atomicExch(status, 1);
+    } else {
+      const double inv = 1.0 / piv;
+      for (int i = jj + 1 + threadIdx.x; i < rows; i += blockDim.x) P[i + ldp * jj] *= inv;
+    }
+    __syncthreads();
+    const int r = rows - jj - 1, cols = w - jj - 1;
+    for (int e = threadIdx.x; e < r * cols; e += blockDim.x) {
+      const int i = jj + 1 + e % r, c = jj + 1 + e / r;
+      P[i + ldp * c] -= P[i + ldp * jj] * P[jj + ldp * c];
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < rows * w; e += blockDim.x) {
+    const int i = e % rows, c = e / rows;
+    a[j0 + i + static_cast<long long>(ld) * (j0 + c)] = P[i + ldp * c];
+  }
+}
+
 // Row interchanges of panel j0 applied to every column outside the panel.
 __global__ void swap_kernel(double* a, int n, int ld, int j0, int w, const int* ipiv) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,6 +259,19 @@ __global__ void __launch_bounds__(256) trailing_kernel(double* a, int n, int ld,
       const int gi = r0 + tx + 16 * q, gc = c0 + ty + 16 * t;
       if (gi < n && gc < n) a[gi + static_cast<long long>(ld) * gc] -= acc[q][t];
     }
+}
+
+// B <- A^{-1} B, one CTA per right-hand side, the vector in shared memory.
+constexpr int kSolveThreads = 512;
+__global__ void __launch_bounds__(kSolveThreads)
+    lu_solve_cta_kernel(const double* __restrict__ lu, int n, int ld, const int* __restrict__ ipiv,
+                        double* b, int ldb) {
+  extern __shared__ double x[];
+  double* bc = b + static_cast<long long>(ldb) * blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[i];
+  __syncthreads();
+  cta_lu_solve(lu, n, ld, ipiv, x);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) bc[i] = x[i];
 }
 
 // B <- A^{-1} B with one warp per right-hand side.
@@ -286,11 +388,24 @@ cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv
   return cudaGetLastError();
 }
 
+namespace {
+constexpr size_t kPanelSmemMax = 200 * 1024;
+constexpr size_t kSolveSmemMax = 200 * 1024;
+}  // namespace
+
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s) {
   for (int j0 = 0; j0 < n; j0 += kNb) {
     const int w = min(kNb, n - j0);
     count_launches(n - j0 - w > 0 ? 4 : 2);
-    panel_lu_kernel<<<1, 1024, 0, s>>>(a, n, ld, j0, w, ipiv, status);
+    const size_t psmem = sizeof(double) * static_cast<size_t>((n - j0) | 1) * w;
+    if (psmem <= kPanelSmemMax) {
+      const cudaError_t e = cudaFuncSetAttribute(
+          panel_lu_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
+      if (e != cudaSuccess) return e;
+      panel_lu_smem_kernel<<<1, 1024, psmem, s>>>(a, n, ld, j0, w, ipiv, status);
+    } else {
+      panel_lu_kernel<<<1, 1024, 0, s>>>(a, n, ld, j0, w, ipiv, status);
+    }
     swap_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w, ipiv);
     const int right = n - j0 - w;
     if (right > 0) {
@@ -305,8 +420,16 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
                            int nrhs, int ldb, cudaStream_t s) {
   if (n == 0 || nrhs == 0) return cudaSuccess;
-  const int per = 4;
   count_launches(1);
+  const size_t smem = sizeof(double) * static_cast<size_t>(n);
+  if (n >= 64 && smem <= kSolveSmemMax) {
+    const cudaError_t e = cudaFuncSetAttribute(
+        lu_solve_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmemMax);
+    if (e != cudaSuccess) return e;
+    lu_solve_cta_kernel<<<nrhs, kSolveThreads, smem, s>>>(lu, n, ld, ipiv, b, ldb);
+    return cudaGetLastError();
+  }
+  const int per = 4;
   lu_solve_kernel<<<(nrhs + per - 1) / per, 32 * per, 0, s>>>(lu, n, ld, ipiv, b, nrhs, ldb);
   return cudaGetLastError();
 }

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "ki_entries.cuh"
 
 namespace kib {
@@ -123,6 +125,26 @@ cudaError_t launch_assemble_top(int pde, const Node* nodes, const int* dofs, int
                                 const int* bid, const int* bpos, const UpdBlock* blocks,
                                 double* out, int ld, cudaStream_t s);
 
+// ---------------------------------------------------------------- forest
+// Per-tree top-level system of a forest: the tree's root skeleton dofs, the
+// update-block lookup of its children, and its n x n matrix / pivots.
+struct TopTask {
+  int n;
+  int pad;
+  const int* dofs;
+  const int* bid;
+  const int* bpos;
+  const UpdBlock* blocks;
+  double* a;
+  int* piv;
+};
+// Assemble and LU-factor every tree's top matrix (one CTA per tree).
+cudaError_t launch_forest_top(int pde, const Node* nodes, const TopTask* tasks, int ntasks,
+                              int n_max, int* status, cudaStream_t s);
+// x[dofs_t] <- A_t^{-1} x[dofs_t] for every tree t (one CTA per tree).
+cudaError_t launch_forest_top_solve(const TopTask* tasks, int ntasks, int n_max, double* x,
+                                    cudaStream_t s);
+
 // ---------------------------------------------------------------- dense LU
 // In-place LU with partial pivoting of an n x n matrix (ld), pivots 0-based
 // row indices as LAPACK's (ipiv[j] = row swapped with j).
@@ -172,6 +194,12 @@ cudaError_t launch_sweep_up(const SweepParams& p, bool use_u, cudaStream_t s);
 cudaError_t launch_sweep_down(const SweepParams& p, cudaStream_t s);
 // x[red] = X_rr^{-1} x[red]
 cudaError_t launch_diag_solve(const SweepParams& p, cudaStream_t s);
+// Transposed solve pieces (A^-T = Up^T Diag^T Top^T Down^T): the transposed
+// down step x_r -= T^T x_s, x_s -= U^T x_r is launch_sweep_up(use_u = true);
+// the transposed up step is x_r -= L^T x_s, x_s -= T x_r; the transposed
+// diagonal solve is X_rr^-T.
+cudaError_t launch_transposed_up(const SweepParams& p, cudaStream_t s);
+cudaError_t launch_diag_solve_t(const SweepParams& p, cudaStream_t s);
 
 // ---------------------------------------------------------------- misc
 // out[i] = x[idx[i]] (gather) / x[idx[i]] = in[i] (scatter), nrhs columns.
@@ -185,10 +213,11 @@ cudaError_t small_gemm(bool ta, bool tb, int m, int n, int k, double alpha,
                        double* c, int ldc, cudaStream_t s);
 
 // y = K x for the full boundary operator (on-the-fly entries), plus the
-// hole border terms when U/Psi are given (nb border columns).
-cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const double* x,
-                                  double* y, int nb, const double* U, const double* Psi,
-                                  cudaStream_t s);
+// hole border terms when U/Psi are given (nb border columns).  seg (node
+// offsets of nseg problems, may be null) makes it block diagonal.
+cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const int* seg,
+                                  int nseg, const double* x, double* y, int nb, const double* U,
+                                  const double* Psi, cudaStream_t s);
 // Target evaluation out = K_fwd(targets) mu (+ U_fwd alpha).
 cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
                                 const double* targets, const double* mu, int nh,
@@ -197,6 +226,56 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
 // Dense kernel block K(tgt, src), column-major nt x ns.
 cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
                                 const int* src, int ns, double* out, cudaStream_t s);
+
+// ---------------------------------------------------------------- Krylov
+// Fast FP64 operator product y = A x (fused, reassociated: accurate to FP64
+// rounding, not bit-identical to the entry kernels), bordered by U / Psi
+// when nb > 0.  `part` needs fast_matvec_scratch_doubles(n_dofs, splits).
+constexpr int kMaxMatvecSplits = 64;
+constexpr int kMaxKrylov = 64;  // vectors per multi-dot
+// One CTA of the operator product: targets [t0, t1) (nodes) against sources
+// [s0, s1) of the same segment (problem); partial `split`; the first target
+// tile of a (segment, split) also sums the rank-one coefficient into slot
+// rank1_slot.
+struct MvTile {
+  int t0, t1, s0, s1, split, rank1_slot, first, pad;
+};
+int matvec_splits(int n_nodes, int num_sms);
+// seg: node offsets of the segments (size nseg + 1); one segment = one
+// problem, so a forest's operator is block diagonal.
+void matvec_tiles(const std::vector<int>& seg, int splits, std::vector<MvTile>* tiles);
+size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg);
+cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, int ntiles,
+                               const int* seg, int nseg, int n_dofs, int splits, const double* x,
+                               double* y, int nb, const double* U, const double* Psi,
+                               double* part, cudaStream_t s);
+// out[j] = V_j . w for j < k (V column j at V + ldv j); part needs
+// k * multi_dot_blocks(n) doubles.  Fixed reduction order.
+int multi_dot_blocks(int n);
+cudaError_t launch_multi_dot(const double* V, long long ldv, int k, const double* w, int n,
+                             double* part, double* out, cudaStream_t s);
+// w += sign * V h
+cudaError_t launch_multi_axpy(double* w, const double* V, long long ldv, int k, const double* h,
+                              int n, double sign, cudaStream_t s);
+// ---------------------------------------------------------------- adjoint
+// Laplace double-layer adjoint contractions (see ki_adjoint.cu).  work needs
+// adjoint_work_doubles(n).  Phase 1: g_mu = K_t^T grad_u and the target
+// term; phase 2 (after lam = A^-T g_mu): node gradients of J.
+size_t adjoint_work_doubles(int n);
+cudaError_t launch_adjoint_laplace(const Node* nodes, int n, const double* mu, int nt,
+                                   const double* targets, const double* grad_u, double* g_mu,
+                                   double* work, cudaStream_t s);
+cudaError_t launch_adjoint_laplace_finish(const Node* nodes, int n, const double* mu,
+                                          const double* lam, double* work, double* g_pts,
+                                          double* g_nrm, double* g_w, double* g_k,
+                                          cudaStream_t s);
+
+cudaError_t launch_scale_copy(double* dst, const double* src, int n, double a, cudaStream_t s);
+// out[p] = squared norm of segment p of v (dofs seg[p] sd .. seg[p + 1] sd)
+cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int sd, double* out,
+                                 cudaStream_t s);
+// r = b - ax
+cudaError_t launch_sub(double* r, const double* b, const double* ax, int n, cudaStream_t s);
 
 }  // namespace kib
 

@@ -1,0 +1,363 @@
+// FP64 kernels of the iterative-refinement / GMRES solve:
+//   * a fast dense operator product y = A x with entries formed on the fly
+//     (the boundary operator of kernel.cpp:11-96, bordered by the hole
+//     columns U and rows Psi when the domain has holes, as in the residual
+//     check of kern_interp_test.cpp:54-78).  Unlike apply_kernel it is free
+//     to fuse and reassociate: it is the refinement residual, accurate to
+//     FP64 rounding, not the bit-exact entry path of the factorization;
+//   * the few vector operations GMRES needs (several dot products in one
+//     pass, several axpys in one pass, scaling), all with a fixed reduction
+//     order so a solve is reproducible.
+//
+// Operator product layout: one thread per target node, 256 targets per CTA,
+// sources staged 256 at a time in shared memory as structure-of-arrays with
+// the density folded in; the source range is split over gridDim.y so the
+// grid covers every SM, and the splits' partial sums are added in order by
+// a second kernel (no atomics).
+#include <algorithm>
+#include <vector>
+
+#include "ki_kernels.h"
+
+namespace kib {
+
+namespace {
+
+constexpr int kMvThreads = 256;
+
+// Per-source values staged in shared memory.
+//   Laplace:          a = -(w / 2 pi) x (n_x, n_y)
+//   Laplace-Neumann:  a = (w / 2 pi) x (1, 1)      (target normal applied later)
+//   Stokes:           a = (w / pi) (n_x, n_y), density (x0, x1)
+template <int PDE>
+__global__ void __launch_bounds__(kMvThreads)
+    mv_partial_kernel(const Node* __restrict__ nodes, const MvTile* __restrict__ tiles,
+                      long long part_stride, const double* __restrict__ x,
+                      double* __restrict__ part, double* __restrict__ part_rank1) {
+  __shared__ double sx[kMvThreads], sy[kMvThreads], sa0[kMvThreads], sa1[kMvThreads];
+  __shared__ double sd0[kMvThreads], sd1[kMvThreads];
+  __shared__ double red[kMvThreads / 32];
+  const MvTile tile = tiles[blockIdx.x];
+  const int t = tile.t0 + threadIdx.x;
+  const int s0 = tile.s0, s1 = tile.s1;
+  const bool live = t < tile.t1;
+  double tx = 0, ty = 0, tnx = 0, tny = 0;
+  if (live) {
+    const Node nt = nodes[t];
+    tx = nt.x;
+    ty = nt.y;
+    tnx = nt.nx;
+    tny = nt.ny;
+  }
+  double y0 = 0.0, y1 = 0.0, r1 = 0.0;
+  for (int base = s0; base < s1; base += kMvThreads) {
+    const int j = base + threadIdx.x;
+    __syncthreads();
+    if (j < s1) {
+      const Node s = nodes[j];
+      sx[threadIdx.x] = s.x;
+      sy[threadIdx.x] = s.y;
+      if (PDE == kLaplace) {
+        const double c = -s.w * KI_INV_2PI * x[j];
+        sa0[threadIdx.x] = c * s.nx;
+        sa1[threadIdx.x] = c * s.ny;
+      } else if (PDE == kLaplaceNeumann) {
+        sa0[threadIdx.x] = s.w * KI_INV_2PI * x[j];
+        // rank-one part: sum_j w_j x_j (the "+ w_s" of every entry)
+        if (tile.first) r1 += s.w * x[j];
+      } else {
+        const double c = s.w * KI_INV_PI;
+        sa0[threadIdx.x] = c * s.nx;
+        sa1[threadIdx.x] = c * s.ny;
+        const double d0 = x[2 * j], d1 = x[2 * j + 1];
+        sd0[threadIdx.x] = d0;
+        sd1[threadIdx.x] = d1;
+        // rank-one part: sum_j w_j (n_j . x_j), applied as tn_t * sum
+        if (tile.first) r1 += s.w * (s.nx * d0 + s.ny * d1);
+      }
+    } else {
+      // padding: a source far away with zero strength
+      sx[threadIdx.x] = 1e30;
+      sy[threadIdx.x] = 1e30;
+      sa0[threadIdx.x] = 0.0;
+      sa1[threadIdx.x] = 0.0;
+      sd0[threadIdx.x] = 0.0;
+      sd1[threadIdx.x] = 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int q = 0; q < kMvThreads; q++) {
+      const double r0 = tx - sx[q], rr1 = ty - sy[q];
+      const double rr = r0 * r0 + rr1 * rr1;
+      if (PDE == kLaplace) {
+        const double num = r0 * sa0[q] + rr1 * sa1[q];
+        y0 += rr > 0.0 ? num / rr : 0.0;
+      } else if (PDE == kLaplaceNeumann) {
+        const double num = (r0 * tnx + rr1 * tny) * sa0[q];
+        y0 += rr > 0.0 ? num / rr : 0.0;
+      } else {
+        const double rn = r0 * sa0[q] + rr1 * sa1[q];
+        const double rx = r0 * sd0[q] + rr1 * sd1[q];
+        const double pq = rr > 0.0 ? (rn * rx) / (rr * rr) : 0.0;
+        y0 += pq * r0;
+        y1 += pq * rr1;
+      }
+    }
+  }
+  if (live) {
+    if (PDE == kStokes) {
+      part[part_stride * tile.split + 2 * t] = y0;
+      part[part_stride * tile.split + 2 * t + 1] = y1;
+    } else {
+      part[part_stride * tile.split + t] = y0;
+    }
+  }
+  if (PDE != kLaplace && tile.first) {
+    // fixed-order block sum of the rank-one coefficient of this split
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      for (int w = 0; w < kMvThreads / 32; w++) v += red[w];
+      part_rank1[tile.rank1_slot] = v;
+    }
+  }
+}
+
+// y_i = sum of the splits' partials + diagonal correction + rank-one term +
+// U x_border; the border rows are done by mv_border_rows_kernel.
+__device__ __forceinline__ int segment_of(const int* __restrict__ seg, int nseg, int node) {
+  int lo = 0, hi = nseg - 1;  // seg[lo] <= node < seg[hi + 1]
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg[mid] <= node) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void mv_finish_kernel(int pde, const Node* __restrict__ nodes, int n_dofs,
+                                 int splits, const double* __restrict__ part,
+                                 const double* __restrict__ part_rank1,
+                                 const int* __restrict__ seg, int nseg,
+                                 const double* __restrict__ x, double* __restrict__ y, int nb,
+                                 const double* __restrict__ U) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_dofs) return;
+  double s = 0.0;
+  for (int p = 0; p < splits; p++) s += part[static_cast<long long>(p) * n_dofs + i];
+  double g = 0.0;
+  if (pde != kLaplace) {
+    const int q = segment_of(seg, nseg, pde == kStokes ? i >> 1 : i);
+    for (int p = 0; p < splits; p++) g += part_rank1[static_cast<long long>(q) * splits + p];
+  }
+  if (pde == kLaplace) {
+    const Node nd = nodes[i];
+    s += (0.5 + 0.5 * nd.k * nd.w * KI_INV_2PI) * x[i];
+  } else if (pde == kLaplaceNeumann) {
+    const Node nd = nodes[i];
+    s += g + (-0.5 + 0.5 * nd.k * nd.w * KI_INV_2PI) * x[i];
+  } else {
+    const Node nd = nodes[i >> 1];
+    const int c = i & 1;
+    const double tn = c ? nd.ny : nd.nx;
+    // -1/2 x - (kappa w / 2 pi) t (t . x), t = (-n_y, n_x), and tn_c * g
+    const double tc = c ? nd.nx : -nd.ny;
+    const double tdotx = -nd.ny * x[i & ~1] + nd.nx * x[i | 1];
+    s += -0.5 * x[i] - nd.k * nd.w * KI_INV_2PI * tc * tdotx + tn * g;
+  }
+  for (int b = 0; b < nb; b++) s += U[i + static_cast<long long>(n_dofs) * b] * x[n_dofs + b];
+  y[i] = s;
+}
+
+// Border rows: y_{N+h} = Psi(h, :) x(0:N) - x_{N+h}, one CTA per row.
+__global__ void mv_border_rows_kernel(int n_dofs, int nb, const double* __restrict__ Psi,
+                                      const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double red[32];
+  const int h = blockIdx.x;
+  double s = 0.0;
+  for (int j = threadIdx.x; j < n_dofs; j += blockDim.x)
+    s += Psi[h + static_cast<long long>(nb) * j] * x[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); w++) v += red[w];
+    y[n_dofs + h] = v - x[n_dofs + h];
+  }
+}
+
+// ---- vector kernels (n up to a few million; k <= kMaxKrylov vectors)
+
+constexpr int kVecThreads = 256;
+
+// part[j * gridDim.x + b] = sum over this CTA's slice of V_j . w
+__global__ void multi_dot_kernel(const double* __restrict__ V, long long ldv, int k,
+                                 const double* __restrict__ w, int n, double* __restrict__ part) {
+  __shared__ double red[kVecThreads / 32][kMaxKrylov + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int j = 0; j < k; j++) {
+    const double* v = V + ldv * j;
+    double s = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += kVecThreads) s += v[i] * w[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp][j] = s;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < k; j += kVecThreads) {
+    double v = 0.0;
+    for (int q = 0; q < kVecThreads / 32; q++) v += red[q][j];
+    part[static_cast<long long>(j) * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+__global__ void multi_dot_finish_kernel(const double* __restrict__ part, int nblk, int k,
+                                        double* __restrict__ out) {
+  const int j = threadIdx.x;
+  if (j >= k) return;
+  double v = 0.0;
+  for (int b = 0; b < nblk; b++) v += part[static_cast<long long>(j) * nblk + b];
+  out[j] = v;
+}
+
+// w -= V h (h on the device, k entries)
+__global__ void multi_axpy_kernel(double* __restrict__ w, const double* __restrict__ V,
+                                  long long ldv, int k, const double* __restrict__ h, int n,
+                                  double sign) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int j = 0; j < k; j++) s += V[ldv * j + i] * h[j];
+  w[i] += sign * s;
+}
+
+__global__ void scale_copy_kernel(double* __restrict__ dst, const double* __restrict__ src,
+                                  int n, double a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = a * src[i];
+}
+
+__global__ void sub_kernel(double* __restrict__ r, const double* __restrict__ b,
+                           const double* __restrict__ ax, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = b[i] - ax[i];
+}
+
+// out[p] = sum of v^2 over dofs [seg[p] * sd, seg[p + 1] * sd), one CTA per
+// segment, fixed order.
+__global__ void segment_sumsq_kernel(const double* __restrict__ v, const int* __restrict__ seg,
+                                     int sd, double* __restrict__ out) {
+  __shared__ double red[32];
+  const long long a = static_cast<long long>(seg[blockIdx.x]) * sd;
+  const long long b = static_cast<long long>(seg[blockIdx.x + 1]) * sd;
+  double s = 0.0;
+  for (long long i = a + threadIdx.x; i < b; i += blockDim.x) s += v[i] * v[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); w++) t += red[w];
+    out[blockIdx.x] = t;
+  }
+}
+
+}  // namespace
+
+int matvec_splits(int n_nodes, int num_sms) {
+  const int tblocks = (n_nodes + kMvThreads - 1) / kMvThreads;
+  const int want = (4 * num_sms + tblocks - 1) / tblocks;  // about 4 CTAs per SM
+  const int max_split = (n_nodes + kMvThreads - 1) / kMvThreads;  // >= 256 sources each
+  return std::max(1, std::min(want, std::min(max_split, kMaxMatvecSplits)));
+}
+
+void matvec_tiles(const std::vector<int>& seg, int splits, std::vector<MvTile>* tiles) {
+  // per segment: target tiles of 256 nodes x source chunks; every (target,
+  // split) pair gets a tile, so each partial is written exactly once
+  tiles->clear();
+  const int nseg = static_cast<int>(seg.size()) - 1;
+  for (int p = 0; p < nseg; p++) {
+    const int a = seg[p], b = seg[p + 1];
+    const int chunk = ((b - a + splits - 1) / splits + kMvThreads - 1) / kMvThreads * kMvThreads;
+    for (int q = 0; q < splits; q++) {
+      const int s0 = std::min(b, a + q * chunk), s1 = std::min(b, s0 + chunk);
+      for (int t0 = a; t0 < b; t0 += kMvThreads)
+        tiles->push_back(MvTile{t0, std::min(b, t0 + kMvThreads), s0, s1, q, p * splits + q,
+                                t0 == a ? 1 : 0, 0});
+    }
+  }
+}
+
+cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, int ntiles,
+                               const int* seg, int nseg, int n_dofs, int splits, const double* x,
+                               double* y, int nb, const double* U, const double* Psi,
+                               double* part, cudaStream_t s) {
+  if (splits < 1 || splits > kMaxMatvecSplits) return cudaErrorInvalidValue;
+  double* part_rank1 = part + static_cast<long long>(splits) * n_dofs;
+  count_launches(nb ? 3 : 2);
+  if (pde == kLaplace)
+    mv_partial_kernel<kLaplace><<<ntiles, kMvThreads, 0, s>>>(nodes, tiles, n_dofs, x, part,
+                                                               part_rank1);
+  else if (pde == kLaplaceNeumann)
+    mv_partial_kernel<kLaplaceNeumann><<<ntiles, kMvThreads, 0, s>>>(nodes, tiles, n_dofs, x,
+                                                                      part, part_rank1);
+  else
+    mv_partial_kernel<kStokes><<<ntiles, kMvThreads, 0, s>>>(nodes, tiles, n_dofs, x, part,
+                                                              part_rank1);
+  mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
+                                                        part_rank1, seg, nseg, x, y, nb, U);
+  if (nb) mv_border_rows_kernel<<<nb, 256, 0, s>>>(n_dofs, nb, Psi, x, y);
+  return cudaGetLastError();
+}
+
+size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg) {
+  return static_cast<size_t>(splits) * n_dofs + static_cast<size_t>(splits) * nseg;
+}
+
+int multi_dot_blocks(int n) { return std::max(1, std::min(296, (n + 1023) / 1024)); }
+
+cudaError_t launch_multi_dot(const double* V, long long ldv, int k, const double* w, int n,
+                             double* part, double* out, cudaStream_t s) {
+  if (k < 1 || k > kMaxKrylov) return cudaErrorInvalidValue;
+  const int nblk = multi_dot_blocks(n);
+  count_launches(2);
+  multi_dot_kernel<<<nblk, kVecThreads, 0, s>>>(V, ldv, k, w, n, part);
+  multi_dot_finish_kernel<<<1, 64, 0, s>>>(part, nblk, k, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_multi_axpy(double* w, const double* V, long long ldv, int k, const double* h,
+                              int n, double sign, cudaStream_t s) {
+  if (k < 1) return cudaSuccess;
+  count_launches(1);
+  multi_axpy_kernel<<<(n + 255) / 256, 256, 0, s>>>(w, V, ldv, k, h, n, sign);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_copy(double* dst, const double* src, int n, double a, cudaStream_t s) {
+  count_launches(1);
+  scale_copy_kernel<<<(n + 255) / 256, 256, 0, s>>>(dst, src, n, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int sd, double* out,
+                                 cudaStream_t s) {
+  count_launches(1);
+  segment_sumsq_kernel<<<nseg, 256, 0, s>>>(v, seg, sd, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sub(double* r, const double* b, const double* ax, int n, cudaStream_t s) {
+  count_launches(1);
+  sub_kernel<<<(n + 255) / 256, 256, 0, s>>>(r, b, ax, n);
+  return cudaGetLastError();
+}
+
+}  // namespace kib

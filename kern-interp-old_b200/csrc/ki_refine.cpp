@@ -1,0 +1,229 @@
+// FP64 refinement of a (possibly low-accuracy) factorization: right-
+// preconditioned GMRES on the bordered boundary operator
+//
+//     [ A  U ] [mu   ]   [f]
+//     [Psi -I] [alpha] = [0]        (kern_interp_test.cpp:54-78 form; no
+//                                    border when the domain has no holes)
+//
+// with the factorization's solve as the preconditioner M^-1 and the
+// operator applied by the fast on-the-fly FP64 product.  The preconditioned
+// directions Z_j = M^-1 V_j are kept (flexible-GMRES storage), so the
+// correction is X += Z y without a further solve.  Orthogonalisation is
+// classical Gram-Schmidt applied twice; the Hessenberg least-squares problem
+// is tiny and solved on the host with Givens rotations.  The reference has no
+// iterative solver; its direct solve is the X_0 = M^-1 b first step here.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ki_solver.h"
+
+namespace kib {
+
+int Solver::mv_setup() {
+  if (d_mv_tiles_) return 0;
+  if (!num_sms_) {
+    int dev = 0;
+    KI_CUDA(cudaGetDevice(&dev));
+    KI_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  }
+  seg_ = starts_.size() > 1 ? starts_ : std::vector<int>{0, n_points_};
+  const int nseg = static_cast<int>(seg_.size()) - 1;
+  // splits sized for the average problem: about 4 CTAs per SM over the job
+  mv_splits_ = matvec_splits(std::max(1, n_points_ / nseg), num_sms_);
+  mv_splits_ = std::max(1, std::min(mv_splits_, (4 * num_sms_ * 256 + n_points_ - 1) /
+                                                   std::max(1, n_points_)));
+  std::vector<MvTile> tiles;
+  matvec_tiles(seg_, mv_splits_, &tiles);
+  n_mv_tiles_ = static_cast<int>(tiles.size());
+  KI_ALLOC(d_mv_tiles_, MvTile, tiles.size());
+  KI_ALLOC(d_seg_, int, seg_.size());
+  KI_UPLOAD(d_mv_tiles_, tiles, stream_);
+  KI_UPLOAD(d_seg_, seg_, stream_);
+  return 0;
+}
+
+int Solver::matvec_device(const double* d_x, double* d_y) {
+  if (mv_setup()) return -2;
+  const int nseg = static_cast<int>(seg_.size()) - 1;
+  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg);
+  // the product's partials live at the start of kry_; solve_refined places
+  // its vectors after them
+  if (kry_.bytes < sizeof(double) * need) KI_CUDA(kry_.reserve(sizeof(double) * need, stream_));
+  KI_CUDA(launch_fast_matvec(opt_.pde, d_nodes_, d_mv_tiles_, n_mv_tiles_, d_seg_, nseg, n_dofs_,
+                             mv_splits_, d_x, d_y, nb_, d_U_, d_Psi_, static_cast<double*>(kry_.p),
+                             stream_));
+  return 0;
+}
+
+int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, double rel_tol,
+                          int max_iters, int* iters_out, double* rel_res_out) {
+  const int N = n_dofs_, nb = nb_, n = N + nb;
+  const int m = std::max(1, std::min(max_iters, kMaxKrylov - 2));  // restart length
+  if (mv_setup()) return -2;
+  const int nseg = static_cast<int>(seg_.size()) - 1;
+  const size_t mv = (fast_matvec_scratch_doubles(N, mv_splits_, nseg) + 31) / 32 * 32;
+  const size_t ldv = (static_cast<size_t>(n) + 31) / 32 * 32;
+  const size_t dotp = static_cast<size_t>(kMaxKrylov) * multi_dot_blocks(n);
+  // [mv partials][V: (m+1) ldv][Z: m ldv][B][X][W][dot partials][h: 3 kMaxKrylov]
+  // [segment norms: nseg]
+  const size_t total =
+      mv + (2 * static_cast<size_t>(m) + 4) * ldv + dotp + 3 * kMaxKrylov + nseg + 1;
+  KI_CUDA(kry_.reserve(sizeof(double) * total, stream_));
+  double* base = static_cast<double*>(kry_.p);
+  double* V = base + mv;
+  double* Z = V + (m + 1) * ldv;
+  double* B = Z + m * ldv;
+  double* X = B + ldv;
+  double* W = X + ldv;
+  double* part = W + ldv;
+  double* dh = part + dotp;  // [0, k) first pass, [kMax, kMax + k) second, [2 kMax] norm
+  double* dseg = dh + 3 * kMaxKrylov;
+  if (!h_kry_) {
+    h_kry_ = stage_.get<double>(3 * kMaxKrylov + nseg + 1);
+    if (!h_kry_) return fail("pinned allocation failed: refinement coefficients");
+  }
+  double* hh = h_kry_;
+  double* hseg = hh + 3 * kMaxKrylov;
+  // largest per-problem relative residual of v (forest: every problem must
+  // meet the tolerance on its own)
+  std::vector<double> bseg;
+  auto seg_norms = [&](const double* v, std::vector<double>* out) -> int {
+    KI_CUDA(launch_segment_sumsq(v, d_seg_, nseg, sd_, dseg, stream_));
+    KI_CUDA(cudaMemcpyAsync(hseg, dseg, sizeof(double) * nseg, cudaMemcpyDeviceToHost, stream_));
+    KI_CUDA(cudaStreamSynchronize(stream_));
+    out->assign(nseg, 0.0);
+    for (int p = 0; p < nseg; p++) (*out)[p] = std::sqrt(hseg[p]);
+    return 0;
+  };
+
+  // B = [f; 0], X = 0
+  KI_CUDA(cudaMemcpyAsync(B, d_f, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  if (nb) KI_CUDA(cudaMemsetAsync(B + N, 0, sizeof(double) * nb, stream_));
+  KI_CUDA(cudaMemsetAsync(X, 0, sizeof(double) * n, stream_));
+
+  auto norm2 = [&](const double* v, double* out) -> int {
+    KI_CUDA(launch_multi_dot(v, 0, 1, v, n, part, dh + 2 * kMaxKrylov, stream_));
+    KI_CUDA(cudaMemcpyAsync(hh + 2 * kMaxKrylov, dh + 2 * kMaxKrylov, sizeof(double),
+                            cudaMemcpyDeviceToHost, stream_));
+    KI_CUDA(cudaStreamSynchronize(stream_));
+    *out = std::sqrt(hh[2 * kMaxKrylov]);
+    return 0;
+  };
+
+  double bnorm = 0;
+  if (norm2(B, &bnorm)) return -2;
+  // a forest stops on the global residual only once it is below every
+  // problem's own share: ||r|| <= tol min_p ||b_p|| bounds each ||r_p||
+  double tol_eff = rel_tol;
+  if (nseg > 1) {
+    if (seg_norms(B, &bseg)) return -2;
+    double bmin = bnorm;
+    for (double v : bseg)
+      if (v > 0.0) bmin = std::min(bmin, v);
+    tol_eff = rel_tol * bmin / bnorm;
+  }
+  int iters = 0;
+  double rel = 0.0;
+  if (bnorm == 0.0) {
+    KI_CUDA(cudaMemsetAsync(d_mu, 0, sizeof(double) * N, stream_));
+    if (nb && d_alpha) KI_CUDA(cudaMemsetAsync(d_alpha, 0, sizeof(double) * nb, stream_));
+    if (iters_out) *iters_out = 0;
+    if (rel_res_out) *rel_res_out = 0.0;
+    return 0;
+  }
+  bool first = true;
+  for (;;) {
+    // r = B - A X (the first cycle starts from X = 0, r = B)
+    double beta = bnorm;
+    if (first) {
+      KI_CUDA(cudaMemcpyAsync(V, B, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
+    } else {
+      if (matvec_device(X, W)) return -2;
+      KI_CUDA(launch_sub(V, B, W, n, stream_));
+      if (norm2(V, &beta)) return -2;
+    }
+    rel = beta / bnorm;
+    if (nseg > 1 && !first) {
+      std::vector<double> rs;
+      if (seg_norms(V, &rs)) return -2;
+      double worst = 0.0;
+      for (int p = 0; p < nseg; p++)
+        if (bseg[p] > 0.0) worst = std::max(worst, rs[p] / bseg[p]);
+      rel = worst;
+    }
+    if ((nseg > 1 ? rel <= rel_tol : rel <= tol_eff) || iters >= max_iters || beta == 0.0) break;
+    first = false;
+    KI_CUDA(launch_scale_copy(V, V, n, 1.0 / beta, stream_));
+
+    // Arnoldi with Givens rotations; H column-major (m+1) x m on the host
+    std::vector<double> H(static_cast<size_t>(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1, 0.0);
+    g[0] = beta;
+    int k = 0;
+    for (; k < m && iters < max_iters; k++) {
+      double* vk = V + k * ldv;
+      double* zk = Z + k * ldv;
+      if (solve_device(vk, zk, nb ? zk + N : nullptr, nb ? vk + N : nullptr)) return -2;
+      if (matvec_device(zk, W)) return -2;
+      iters++;
+      // two passes of classical Gram-Schmidt against V_0..V_k
+      KI_CUDA(launch_multi_dot(V, static_cast<long long>(ldv), k + 1, W, n, part, dh, stream_));
+      KI_CUDA(launch_multi_axpy(W, V, static_cast<long long>(ldv), k + 1, dh, n, -1.0, stream_));
+      KI_CUDA(launch_multi_dot(V, static_cast<long long>(ldv), k + 1, W, n, part, dh + kMaxKrylov,
+                               stream_));
+      KI_CUDA(launch_multi_axpy(W, V, static_cast<long long>(ldv), k + 1, dh + kMaxKrylov, n,
+                                -1.0, stream_));
+      KI_CUDA(launch_multi_dot(W, 0, 1, W, n, part, dh + 2 * kMaxKrylov, stream_));
+      KI_CUDA(cudaMemcpyAsync(hh, dh, sizeof(double) * 3 * kMaxKrylov, cudaMemcpyDeviceToHost,
+                              stream_));
+      KI_CUDA(cudaStreamSynchronize(stream_));
+      double* hk = &H[static_cast<size_t>(k) * (m + 1)];
+      for (int i = 0; i <= k; i++) hk[i] = hh[i] + hh[kMaxKrylov + i];
+      const double hnext = std::sqrt(hh[2 * kMaxKrylov]);
+      hk[k + 1] = hnext;
+      if (hnext > 0.0) KI_CUDA(launch_scale_copy(V + (k + 1) * ldv, W, n, 1.0 / hnext, stream_));
+      for (int i = 0; i < k; i++) {  // apply the earlier rotations
+        const double a = hk[i], b = hk[i + 1];
+        hk[i] = cs[i] * a + sn[i] * b;
+        hk[i + 1] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = hk[k], b = hk[k + 1];
+      const double r = std::hypot(a, b);
+      cs[k] = r > 0 ? a / r : 1.0;
+      sn[k] = r > 0 ? b / r : 0.0;
+      hk[k] = r;
+      hk[k + 1] = 0.0;
+      g[k + 1] = -sn[k] * g[k];
+      g[k] = cs[k] * g[k];
+      if (std::fabs(g[k + 1]) <= tol_eff * bnorm || hnext == 0.0) {
+        k++;
+        break;
+      }
+    }
+    // y = R^-1 g (upper triangular k x k), X += Z y
+    std::vector<double> y(k, 0.0);
+    for (int i = k - 1; i >= 0; i--) {
+      double s = g[i];
+      for (int j = i + 1; j < k; j++) s -= H[static_cast<size_t>(j) * (m + 1) + i] * y[j];
+      const double d = H[static_cast<size_t>(i) * (m + 1) + i];
+      y[i] = d != 0.0 ? s / d : 0.0;
+    }
+    if (k > 0) {
+      for (int i = 0; i < k; i++) hh[i] = y[i];
+      KI_CUDA(cudaMemcpyAsync(dh, hh, sizeof(double) * k, cudaMemcpyHostToDevice, stream_));
+      KI_CUDA(launch_multi_axpy(X, Z, static_cast<long long>(ldv), k, dh, n, 1.0, stream_));
+      // the host buffer is reused by the next cycle's download: keep the
+      // upload ordered before it
+      KI_CUDA(cudaStreamSynchronize(stream_));
+    }
+  }
+  KI_CUDA(cudaMemcpyAsync(d_mu, X, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  if (nb && d_alpha)
+    KI_CUDA(cudaMemcpyAsync(d_alpha, X + N, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
+                            stream_));
+  if (iters_out) *iters_out = iters;
+  if (rel_res_out) *rel_res_out = rel;
+  return 0;
+}
+
+}  // namespace kib

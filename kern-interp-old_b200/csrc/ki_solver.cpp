@@ -227,6 +227,11 @@ int Solver::upload(T* dst, const std::vector<T>& src, cudaStream_t s) {
   return rc;
 }
 
+// members in other files upload these types
+template int Solver::upload<int>(int*, const std::vector<int>&, cudaStream_t);
+template int Solver::upload<double>(double*, const std::vector<double>&, cudaStream_t);
+template int Solver::upload<MvTile>(MvTile*, const std::vector<MvTile>&, cudaStream_t);
+
 Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
                const double* normals, const double* curvatures, const double* weights,
                int n_holes, const double* holes, cudaStream_t stream)
@@ -263,12 +268,22 @@ int Solver::timer_end(cudaEvent_t e0, const LaunchRecord& rec, cudaStream_t s) {
   return 0;
 }
 
+void Solver::mark(int code, int level) {
+  if (time_phases) host_marks.push_back(HostMark{code, level, now_ms() - host_start_});
+}
+
 int Solver::timers_resolve() {
   for (PendingTimer& p : pending_) {
-    float ms = 0;
+    float ms = 0, a = 0, b = 0;
     if (cuda_check(cudaEventElapsedTime(&ms, p.e0, p.e1), "cudaEventElapsedTime")) return -2;
     LaunchRecord r = p.rec;
     r.ms = ms;
+    if (ev_start_) {
+      if (cuda_check(cudaEventElapsedTime(&a, ev_start_, p.e0), "cudaEventElapsedTime")) return -2;
+      if (cuda_check(cudaEventElapsedTime(&b, ev_start_, p.e1), "cudaEventElapsedTime")) return -2;
+      r.t0 = a;
+      r.t1 = b;
+    }
     if (r.kind == 0) {
       t_id_ms += ms;
       id_launches++;
@@ -295,24 +310,6 @@ int Solver::cuda_check(cudaError_t e, const char* what) {
   error = std::string(what) + ": " + cudaGetErrorString(e);
   return -2;
 }
-
-#define KI_CUDA(expr)                                   \
-  do {                                                  \
-    const int rc_ = cuda_check((expr), #expr);          \
-    if (rc_) return rc_;                                \
-  } while (0)
-
-#define KI_UPLOAD(...)                     \
-  do {                                     \
-    const int urc_ = upload(__VA_ARGS__);  \
-    if (urc_) return urc_;                 \
-  } while (0)
-
-#define KI_ALLOC(ptr, type, count)                                  \
-  do {                                                              \
-    (ptr) = arena_.get<type>(count);                                \
-    if (!(ptr)) return fail("device allocation failed: " #ptr);     \
-  } while (0)
 
 std::vector<BoxBlock> Solver::blocks_of(int box) const {
   // Accumulated updates inside the box's current dof list: its own skeleton
@@ -348,10 +345,15 @@ void Solver::build_block_map(const std::vector<BoxBlock>& blocks, int n, std::ve
 }
 
 void Solver::build_tree_only() {
-  tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  if (starts_.size() > 1)
+    tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
+  else
+    tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
   for (int level = static_cast<int>(tree.levels.size()) - 1; level >= 0; level--)
     tree.refresh_level(level, nullptr);
-  allskel = tree.boxes[0].active;
+  allskel.clear();
+  for (int r : tree.roots)
+    allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
 }
 
 int Solver::factor() {
@@ -359,9 +361,12 @@ int Solver::factor() {
   KI_CUDA(cudaEventCreate(&ev0));
   KI_CUDA(cudaEventCreate(&ev1));
   KI_CUDA(cudaEventRecord(ev0, stream_));
+  host_start_ = now_ms();
+  ev_start_ = ev0;
+  host_marks.clear();
   t_id_ms = t_decouple_ms = t_top_ms = 0;
   id_launches = 0;
-  id_flops = id_bytes = id_fold_flops = 0;
+  id_flops = id_bytes = id_onchip_flops = 0;
 
   if (!dstream_) {
     KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
@@ -370,9 +375,15 @@ int Solver::factor() {
   }
   for (int G = 1; G <= 16; G *= 2)
     onchip_ok_[G] = id_cluster_fits(kOnChip + G, 4096, 256, (227 * 1024 - id_smem_bytes(4096, 256)) / 8) != 0;
-  tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  if (starts_.size() > 1) {
+    if (!holes_.empty()) return fail("a forest of problems cannot have holes");
+    tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
+  } else {
+    tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  }
   boxdev_.assign(tree.boxes.size(), BoxDev{});
   levels_.assign(tree.levels.size(), LevelFactors{});
+  mark(0, 0);
 
   // geometry, proxy directions, holes, status flag
   {
@@ -421,14 +432,18 @@ int Solver::factor() {
     if (rc) return rc;
   }
   for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
-  allskel = tree.boxes[0].active;
+  allskel.clear();
+  for (int r : tree.roots)
+    allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
   KI_CUDA(cudaEventRecord(ev_dec_, dstream_));
   KI_CUDA(cudaStreamWaitEvent(stream_, ev_dec_, 0));
   cudaEvent_t t0 = nullptr;
   if (time_phases && timer_begin(&t0)) return -2;
   const double ht = now_ms();
-  int rc = factor_top();
+  mark(4, 0);
+  int rc = tree.roots.size() > 1 ? factor_top_forest() : factor_top();
   t_host_top_ms = now_ms() - ht;
+  mark(5, 0);
   if (rc) return rc;
   if (time_phases && timer_end(t0, {0, 2, 1, 1, 0, ns_ + nb_, 0.0})) return -2;
 
@@ -436,12 +451,15 @@ int Solver::factor() {
   KI_CUDA(cudaMemcpyAsync(&status, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
   KI_CUDA(cudaEventRecord(ev1, stream_));
   KI_CUDA(cudaStreamSynchronize(stream_));
+  mark(6, 0);
   float ms = 0;
   KI_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
   t_factor_ms = ms;
+  const int trc = timers_resolve();
+  ev_start_ = nullptr;
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  if (timers_resolve()) return -2;
+  if (trc) return -2;
   t_upload_ms = g_upload_ms;
   if (status) return fail("zero pivot in an LU factorization (singular block)");
   return 0;
@@ -468,12 +486,13 @@ int Solver::process_level(int level) {
     if (level == 1 || level == 2) {
       // kernel.cpp:164-207: every other active dof of the level (and the
       // level-1 leaves for level 2), both directions, no proxy circle.
+      // (a forest restricts both to the box's own tree)
       for (int o : tree.levels[level])
-        if (o != id) c.rows.insert(c.rows.end(), tree.boxes[o].active.begin(),
-                                   tree.boxes[o].active.end());
+        if (o != id && tree.boxes[o].tree == b.tree)
+          c.rows.insert(c.rows.end(), tree.boxes[o].active.begin(), tree.boxes[o].active.end());
       if (level == 2)
         for (int o : tree.levels[1])
-          if (tree.boxes[o].leaf)
+          if (tree.boxes[o].leaf && tree.boxes[o].tree == b.tree)
             c.rows.insert(c.rows.end(), tree.boxes[o].original.begin(),
                           tree.boxes[o].original.end());
       c.I = static_cast<int>(c.rows.size());
@@ -529,6 +548,7 @@ int Solver::process_level(int level) {
     perm_total += c.n;
   }
   t_host_prep_ms += now_ms() - h0;
+  mark(1, level);
   int *d_act, *d_rows, *d_perm, *d_rank;
   double* d_T;
   IdTask* d_tasks;
@@ -603,24 +623,28 @@ int Solver::process_level(int level) {
 
   // skeleton / redundant sets (InteractionLists::set_rs_ranges, quadtree.h:23-35)
   const double h1 = now_ms();
+  mark(2, level);
   std::vector<int> comp;  // candidate indices that compressed
   for (int q = 0; q < nc; q++) {
     const Cand& c = cand[q];
     const IdTask& t = tasks[q];
     const int k = rank[q];
-    // algorithmic work of the ID: entry generation + k Householder steps on
-    // the m x n matrix (dot + update over the trailing columns) + the
-    // triangular solve for T; bytes = the matrix written once and read once.
+    // Algorithmic work of the ID, counted from the actual sizes and rank:
+    // FP64 flops = entry generation (20 per entry) + the Householder steps
+    // actually taken (column dots + rank-one updates over the shrinking
+    // trailing block) + the triangular solve for T; HBM bytes = the dof
+    // lists and node records read, perm and T written, plus, for the
+    // streamed launches, the working matrix written once and read once.
     const double m = c.m, n = c.n;
     const int steps = k > 0 ? k : std::min(c.m, c.n);
-    const double qr = 4.0 * m * (n * steps - 0.5 * steps * steps) + 1.0 * k * k * (n - k);
-    if (c.g < kOnChip) {
-      // matrix streamed through HBM/L2: written once, read once
-      id_flops += qr;
-      id_bytes += 16.0 * m * n;
-    } else {
-      id_fold_flops += qr;  // on-chip: FP64 work only
-    }
+    double qr = 20.0 * m * n + 1.0 * k * k * (n - k);
+    for (int j = 0; j < steps; j++) qr += 4.0 * (m - j) * (n - j - 1) + 3.0 * (m - j);
+    const double sd = sd_;  // dofs per node record
+    double bytes = 4.0 * (c.I + 2 * n) + 64.0 * (c.I + c.n) / sd + 8.0 * k * (n - k);
+    if (c.g < kOnChip) bytes += 16.0 * m * n;
+    id_flops += qr;
+    id_bytes += bytes;
+    if (c.g >= kOnChip) id_onchip_flops += qr;
     if (k == 0) continue;
     Box& b = tree.boxes[c.box];
     b.compressed = true;
@@ -734,6 +758,7 @@ int Solver::process_level(int level) {
   dp.status = d_status_;
   cudaEvent_t d0 = nullptr;
   t_host_post_ms += now_ms() - h1;
+  mark(3, level);
   if (time_phases && timer_begin(&d0, dstream_)) return -2;
   KI_CUDA(launch_decouple(dp, n_max, dstream_));
   int n_large = 0;
@@ -779,21 +804,95 @@ int Solver::process_level(int level) {
   return 0;
 }
 
-int Solver::factor_top() {
+int Solver::build_all_compressed() {
   // concatenated sweep tasks of every compressed box for the diagonal solves
-  {
-    std::vector<SweepTask> all;
-    int cap = 0;
-    for (LevelFactors& lf : levels_) {
-      if (!lf.ntasks) continue;
-      all.insert(all.end(), lf.h_tasks.begin(), lf.h_tasks.end());
-      cap = std::max(cap, lf.cap);
-    }
-    all_compressed_.ntasks = static_cast<int>(all.size());
-    all_compressed_.cap = cap;
-    KI_ALLOC(all_compressed_.d_tasks, SweepTask, all.size());
-    KI_UPLOAD(all_compressed_.d_tasks, all, stream_);
+  std::vector<SweepTask> all;
+  int cap = 0;
+  for (LevelFactors& lf : levels_) {
+    if (!lf.ntasks) continue;
+    all.insert(all.end(), lf.h_tasks.begin(), lf.h_tasks.end());
+    cap = std::max(cap, lf.cap);
   }
+  all_compressed_.ntasks = static_cast<int>(all.size());
+  all_compressed_.cap = cap;
+  KI_ALLOC(all_compressed_.d_tasks, SweepTask, all.size());
+  KI_UPLOAD(all_compressed_.d_tasks, all, stream_);
+  return 0;
+}
+
+int Solver::factor_top_forest() {
+  // skel_factorization.cpp:116-128 for every tree: its root's active dofs,
+  // the accumulated updates of the root's children, one LU per tree.
+  if (build_all_compressed()) return -2;
+  const int P = static_cast<int>(tree.roots.size());
+  std::vector<int> dofs, bid, bpos;
+  std::vector<UpdBlock> tab;
+  std::vector<size_t> d_off(P), b_off(P), t_off(P), a_off(P), p_off(P);
+  size_t a_total = 0, p_total = 0;
+  forest_nmax_ = 0;
+  for (int p = 0; p < P; p++) {
+    const Box& root = tree.boxes[tree.roots[p]];
+    const int n = static_cast<int>(root.active.size());
+    std::vector<BoxBlock> blocks;
+    if (!root.leaf) {
+      int off = 0;
+      for (int q = 0; q < 4; q++) {
+        const int ch = root.child[q];
+        for (const BoxBlock& x : blocks_of(ch)) blocks.push_back(BoxBlock{x.acc, x.size, x.pos + off});
+        const Box& cb = tree.boxes[ch];
+        off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
+      }
+    }
+    std::vector<int> tb, tp;
+    std::vector<UpdBlock> tt;
+    build_block_map(blocks, n, &tb, &tp, &tt);
+    d_off[p] = dofs.size();
+    b_off[p] = bid.size();
+    t_off[p] = tab.size();
+    a_off[p] = a_total;
+    p_off[p] = p_total;
+    dofs.insert(dofs.end(), root.active.begin(), root.active.end());
+    bid.insert(bid.end(), tb.begin(), tb.end());
+    bpos.insert(bpos.end(), tp.begin(), tp.end());
+    tab.insert(tab.end(), tt.begin(), tt.end());
+    a_total += static_cast<size_t>(n) * n;
+    p_total += n;
+    forest_nmax_ = std::max(forest_nmax_, n);
+  }
+  if (static_cast<size_t>(forest_nmax_) * sizeof(double) > 200 * 1024)
+    return fail("a forest tree's top skeleton is too large for the batched top solve");
+  int *d_dofs, *d_bid, *d_bpos, *d_piv;
+  UpdBlock* d_tab;
+  double* d_a;
+  KI_ALLOC(d_dofs, int, dofs.size());
+  KI_ALLOC(d_bid, int, bid.size());
+  KI_ALLOC(d_bpos, int, bpos.size());
+  KI_ALLOC(d_tab, UpdBlock, tab.size());
+  KI_ALLOC(d_a, double, a_total);
+  KI_ALLOC(d_piv, int, p_total);
+  KI_ALLOC(d_forest_, TopTask, P);
+  std::vector<TopTask> tasks(P);
+  for (int p = 0; p < P; p++) {
+    const int n = static_cast<int>(tree.boxes[tree.roots[p]].active.size());
+    tasks[p] = TopTask{n, 0, d_dofs + d_off[p], d_bid + b_off[p], d_bpos + b_off[p],
+                       d_tab + t_off[p], d_a + a_off[p], d_piv + p_off[p]};
+  }
+  KI_UPLOAD(d_dofs, dofs, stream_);
+  KI_UPLOAD(d_bid, bid, stream_);
+  KI_UPLOAD(d_bpos, bpos, stream_);
+  KI_UPLOAD(d_tab, tab, stream_);
+  KI_UPLOAD(d_forest_, tasks, stream_);
+  ns_ = static_cast<int>(allskel.size());
+  KI_ALLOC(d_tmp_, double, 4 * static_cast<size_t>(n_dofs_) + 64);
+  cudaEvent_t l0 = nullptr;
+  if (time_phases && timer_begin(&l0)) return -2;
+  KI_CUDA(launch_forest_top(opt_.pde, d_nodes_, d_forest_, P, forest_nmax_, d_status_, stream_));
+  if (time_phases && timer_end(l0, {0, 4, 1, P, 0, forest_nmax_, 0.0})) return -2;
+  return 0;
+}
+
+int Solver::factor_top() {
+  if (build_all_compressed()) return -2;
   ns_ = static_cast<int>(allskel.size());
   KI_ALLOC(d_allskel_, int, ns_);
   KI_UPLOAD(d_allskel_, allskel, stream_);
@@ -899,7 +998,7 @@ int Solver::factor_border() {
   return 0;
 }
 
-int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha) {
+int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const double* d_g) {
   const int N = n_dofs_;
   double* x = d_mu;
   if (d_b != d_mu)
@@ -912,7 +1011,12 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha) {
     KI_CUDA(launch_sweep_up(sp, false, stream_));
   }
   const int ns = ns_, nb = nb_;
-  if (nb == 0) {
+  if (d_forest_) {
+    SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, x, N, 1, 0, nullptr,
+                   all_compressed_.cap};
+    KI_CUDA(launch_diag_solve(dp, stream_));
+    KI_CUDA(launch_forest_top_solve(d_forest_, n_trees(), forest_nmax_, x, stream_));
+  } else if (nb == 0) {
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, x, N, 1, 0, nullptr,
                    all_compressed_.cap};
     KI_CUDA(launch_diag_solve(dp, stream_));
@@ -932,7 +1036,11 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha) {
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dw, nr, 1, 1, d_red_pos_,
                    all_compressed_.cap};
     KI_CUDA(launch_diag_solve(dp, stream_));
-    KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, 0.0, M + ns, nb, stream_));
+    // border rows of the reduced system: g - Psi~_r D^-1 w_r
+    if (d_g)
+      KI_CUDA(cudaMemcpyAsync(M + ns, d_g, sizeof(double) * nb, cudaMemcpyDeviceToDevice, stream_));
+    KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, d_g ? 1.0 : 0.0, M + ns,
+                       nb, stream_));
     KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_));
     if (d_alpha)
       KI_CUDA(cudaMemcpyAsync(d_alpha, M + ns, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
@@ -953,7 +1061,10 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha) {
 }
 
 int Solver::apply_device(const double* d_x, double* d_y) {
-  KI_CUDA(launch_apply_operator(opt_.pde, d_nodes_, n_dofs_, d_x, d_y, nb_, d_U_, d_Psi_,
+  const bool forest = starts_.size() > 2;
+  if (forest && mv_setup()) return -2;
+  KI_CUDA(launch_apply_operator(opt_.pde, d_nodes_, n_dofs_, forest ? d_seg_ : nullptr,
+                                static_cast<int>(seg_.size()) - 1, d_x, d_y, nb_, d_U_, d_Psi_,
                                 stream_));
   return 0;
 }

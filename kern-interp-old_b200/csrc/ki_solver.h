@@ -88,13 +88,42 @@ class Solver {
          int n_holes, const double* holes, cudaStream_t stream);
   ~Solver();
 
+  // Many independent problems in one factorization (a forest): problem p
+  // owns points [starts[p], starts[p + 1]); its dofs are numbered after the
+  // previous problems'.  Call before factor(); no holes.
+  void set_forest(const std::vector<int>& starts) { starts_ = starts; }
+  int n_trees() const { return starts_.size() > 1 ? static_cast<int>(starts_.size()) - 1 : 1; }
+  const std::vector<int>& starts() const { return starts_; }
+
   // QuadTree::initialize_tree + SkelFactorization::skeletonize.
   int factor();
   // QuadTree::initialize_tree only, active lists as before compression.
   void build_tree_only();
   // linear_solve on device buffers: d_mu (dofs), d_alpha (border, may be
   // null when there are no holes).  d_b and d_mu may be the same buffer.
-  int solve_device(const double* d_b, double* d_mu, double* d_alpha);
+  // d_g (nb values, may be null = zero) is the right-hand side of the
+  // border rows [Psi -I][mu; alpha] = g; the reference always has g = 0.
+  int solve_device(const double* d_b, double* d_mu, double* d_alpha,
+                   const double* d_g = nullptr);
+  // FP64 GMRES on the (bordered) boundary operator, right-preconditioned by
+  // this factorization, entries of A formed on the fly: stops when
+  // ||[f; 0] - A [mu; alpha]|| <= rel_tol ||f|| (true residual) or after
+  // max_iters preconditioned products.  iters / rel_res report the work and
+  // the final true residual.
+  int solve_refined(const double* d_f, double* d_mu, double* d_alpha, double rel_tol,
+                    int max_iters, int* iters, double* rel_res);
+  // Fast FP64 product y = A x (bordered), the refinement's residual operator.
+  int matvec_device(const double* d_x, double* d_y);
+  // x = A^-T b with the same factorization (simply connected domains):
+  // the sweeps of solve_device transposed and run in reverse order.
+  int solve_transpose_device(const double* d_b, double* d_x);
+  // Backward pass of u = K_t A^-1 f (Laplace, no holes): given mu = A^-1 f
+  // and grad_u at n_targets points, writes grad_f = A^-T K_t^T grad_u and
+  // the gradients with respect to the node positions (2 per node), normals
+  // (2 per node), weights and curvatures.
+  int adjoint_backward(int n_targets, const double* d_targets, const double* d_mu,
+                       const double* d_grad_u, double* d_grad_f, double* d_grad_points,
+                       double* d_grad_normals, double* d_grad_weights, double* d_grad_curv);
   // y = A x on device (bordered when there are holes).
   int apply_device(const double* d_x, double* d_y);
 
@@ -115,16 +144,26 @@ class Solver {
   // summed duration of the ID launches, id_launches their count.
   double t_factor_ms = 0, t_id_ms = 0, t_decouple_ms = 0, t_top_ms = 0;
   int id_launches = 0;
-  double id_flops = 0, id_bytes = 0;  // algorithmic work of the streamed ID launches
-  double id_fold_flops = 0;           // FP64 work of the on-chip fold ID launches
+  double id_flops = 0, id_bytes = 0;  // algorithmic FP64 flops / HBM bytes of all ID launches
+  double id_onchip_flops = 0;         // the part of id_flops done by on-chip launches
   bool time_phases = false;
   // Per-launch record of the timed factorization: kind 0 ID, 1 decouple,
   // 2 top-level assembly + LU; ms from CUDA events on the solver stream.
   struct LaunchRecord {
     int level, kind, group, ntasks, m_cap, n_cap;
     double ms;
+    double t0 = 0, t1 = 0;  // start / end, ms after the factorization began (GPU clock)
   };
   std::vector<LaunchRecord> launch_log;
+  // Host side of the timed factorization: code (0 tree built, 1 level lists
+  // ready / ID launched, 2 ranks received, 3 decouple launched, 4 top level
+  // started, 5 top level launched, 6 factorization synchronised), level,
+  // ms after the factorization began (host clock).
+  struct HostMark {
+    int code, level;
+    double ms;
+  };
+  std::vector<HostMark> host_marks;
   double t_wait_ms = 0;  // host time blocked on the per-level rank download
   // host-side phases (steady clock): level list building before the ID
   // launch, skeleton/decouple bookkeeping after it, uploads, top level
@@ -139,13 +178,18 @@ class Solver {
     LaunchRecord rec;
   };
   std::vector<PendingTimer> pending_;
+  cudaEvent_t ev_start_ = nullptr;  // GPU time origin of the timed factorization
+  double host_start_ = 0;           // host time origin
+  void mark(int code, int level);
   int timer_begin(cudaEvent_t* e0, cudaStream_t s = nullptr);
   int timer_end(cudaEvent_t e0, const LaunchRecord& rec, cudaStream_t s = nullptr);
   int timers_resolve();
   int fail(const std::string& msg);
   int cuda_check(cudaError_t e, const char* what);
   int process_level(int level);
+  int build_all_compressed();
   int factor_top();
+  int factor_top_forest();
   int factor_border();
   std::vector<BoxBlock> blocks_of(int box) const;
   void build_block_map(const std::vector<BoxBlock>& blocks, int n, std::vector<int>* bid,
@@ -184,6 +228,11 @@ class Solver {
   std::vector<LevelFactors> levels_;
   LevelFactors all_compressed_;
 
+  // forest
+  std::vector<int> starts_;       // point offsets of the problems (empty: one problem)
+  TopTask* d_forest_ = nullptr;   // per-tree top systems
+  int forest_nmax_ = 0;
+
   // top level
   int ns_ = 0;
   double* d_top_ = nullptr;  // LU of allskel_mat, or of S with holes
@@ -197,8 +246,39 @@ class Solver {
   double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
   double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
   double* d_tmp_ = nullptr;   // solve scratch
+  // refinement workspace: Krylov basis V, preconditioned basis Z, vectors,
+  // operator-product and dot-product partials
+  Scratch kry_;
+  Scratch adj_;  // adjoint contraction partials
+  int mv_setup();  // tile table of the operator product (once)
+  MvTile* d_mv_tiles_ = nullptr;
+  int n_mv_tiles_ = 0, mv_splits_ = 0;
+  int* d_seg_ = nullptr;  // node offsets of the problems
+  std::vector<int> seg_;
+  double* h_kry_ = nullptr;  // pinned host copy of the Arnoldi coefficients
+  int num_sms_ = 0;
 };
 
 }  // namespace kib
+
+// Error propagation inside Solver members: a failing CUDA call or allocation
+// records the message in `error` and returns a nonzero status.
+#define KI_CUDA(expr)                                   \
+  do {                                                  \
+    const int rc_ = cuda_check((expr), #expr);          \
+    if (rc_) return rc_;                                \
+  } while (0)
+
+#define KI_UPLOAD(...)                     \
+  do {                                     \
+    const int urc_ = upload(__VA_ARGS__);  \
+    if (urc_) return urc_;                 \
+  } while (0)
+
+#define KI_ALLOC(ptr, type, count)                                  \
+  do {                                                              \
+    (ptr) = arena_.get<type>(count);                                \
+    if (!(ptr)) return fail("device allocation failed: " #ptr);     \
+  } while (0)
 
 #endif  // KI_SOLVER_H_

@@ -33,6 +33,7 @@ void QuadTreeHost::subdivide(int id) {
   for (int q = 0; q < 4; q++) {
     Box ch;
     std::memcpy(ch.corner, c, sizeof(c));
+    ch.tree = boxes[id].tree;
     ch.level = lvl;
     ch.side = half;
     ch.parent = id;
@@ -130,27 +131,45 @@ void QuadTreeHost::neighbor_lists() {
 
 void QuadTreeHost::build(const double* points, int n, int sol_dim,
                          int max_leaf_dofs) {
-  // quadtree.cpp:72-114: root square [min - 0.01, max + 0.01]^2 over all
-  // coordinates, points inserted in order.
+  build_forest(points, n, sol_dim, max_leaf_dofs, {0, n});
+}
+
+void QuadTreeHost::build_forest(const double* points, int n, int sol_dim, int max_leaf_dofs,
+                                const std::vector<int>& starts) {
+  // quadtree.cpp:72-114 per tree: root square [min - 0.01, max + 0.01]^2
+  // over all of the tree's coordinates, its points inserted in order.
   pts_.assign(points, points + 2 * static_cast<size_t>(n));
   sol_dim_ = sol_dim;
   max_leaf_ = max_leaf_dofs;
   boxes.clear();
   levels.clear();
-  boxes.reserve(8 * (static_cast<size_t>(n) * sol_dim / std::max(1, max_leaf_dofs)) + 64);
-  min_ = max_ = pts_[0];
-  for (double v : pts_) {
-    if (v < min_) min_ = v;
-    if (v > max_) max_ = v;
+  roots.clear();
+  boxes.reserve(8 * (static_cast<size_t>(n) * sol_dim / std::max(1, max_leaf_dofs)) +
+                64 * starts.size());
+  levels.emplace_back();
+  for (size_t p = 0; p + 1 < starts.size(); p++) {
+    const int p0 = starts[p], p1 = starts[p + 1];
+    double lo_v = pts_[2 * static_cast<size_t>(p0)], hi_v = lo_v;
+    for (size_t i = 2 * static_cast<size_t>(p0); i < 2 * static_cast<size_t>(p1); i++) {
+      if (pts_[i] < lo_v) lo_v = pts_[i];
+      if (pts_[i] > hi_v) hi_v = pts_[i];
+    }
+    if (p == 0) {
+      min_ = lo_v;
+      max_ = hi_v;
+    }
+    const double lo = lo_v - 0.01, hi = hi_v + 0.01;
+    Box root;
+    root.tree = static_cast<int>(p);
+    const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
+    std::memcpy(root.corner, c, sizeof(c));
+    root.side = hi - lo;
+    const int id = static_cast<int>(boxes.size());
+    boxes.push_back(root);
+    levels[0].push_back(id);
+    roots.push_back(id);
+    for (int q = p0; q < p1; q++) insert(id, pts_[2 * q], pts_[2 * q + 1], q);
   }
-  const double lo = min_ - 0.01, hi = max_ + 0.01;
-  Box root;
-  const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
-  std::memcpy(root.corner, c, sizeof(c));
-  root.side = hi - lo;
-  boxes.push_back(root);
-  levels.push_back({0});
-  for (int p = 0; p < n; p++) insert(0, pts_[2 * p], pts_[2 * p + 1], p);
   neighbor_lists();
 }
 

@@ -15,6 +15,7 @@
 namespace kib {
 
 struct Box {
+  int tree = 0;  // which problem of a forest the box belongs to
   int level = 0;
   int parent = -1;
   int child[4] = {-1, -1, -1, -1};  // order {BL, TL, TR, BR}
@@ -34,6 +35,13 @@ class QuadTreeHost {
  public:
   // points: interleaved xy of n points; sol_dim dofs per point.
   void build(const double* points, int n, int sol_dim, int max_leaf_dofs);
+  // A forest of independent problems: problem p owns points
+  // [starts[p], starts[p + 1]) and gets its own root (its own bounding
+  // square, quadtree.cpp:83-105); level l lists every tree's level-l boxes,
+  // tree by tree.  Boxes of different trees are never neighbours.
+  void build_forest(const double* points, int n, int sol_dim, int max_leaf_dofs,
+                    const std::vector<int>& starts);
+  std::vector<int> roots;  // root box of each tree
 
   int sol_dim() const { return sol_dim_; }
   double min() const { return min_; }

@@ -48,6 +48,12 @@ def load():
         getattr(lib, name).argtypes = fac_args
         getattr(lib, name).restype = C.c_int
     lib.ki_partition.argtypes = [C.c_int, _dp, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    lib.ki_partition_batch.argtypes = [C.c_int, _ip, _dp, C.c_int, C.c_int,
+                                       C.POINTER(C.c_void_p)]
+    lib.ki_factor_batch.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp, C.c_int,
+                                    C.c_double, C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.ki_num_problems.argtypes = [C.c_void_p]
+    lib.ki_box_tree.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.ki_destroy.argtypes = [C.c_void_p]
     lib.ki_destroy.restype = None
     for name in ("ki_num_dofs", "ki_num_border", "ki_num_levels"):
@@ -56,6 +62,16 @@ def load():
     lib.ki_solve.argtypes = [C.c_void_p, _dp, _dp, _dp]
     lib.ki_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ki_apply_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ki_solve_bordered_device.argtypes = [C.c_void_p] + [C.c_void_p] * 4
+    lib.ki_solve_transpose_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ki_eval_targets_device.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 4
+    lib.ki_adjoint_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
+    lib.ki_adjoint_backward.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8
+    lib.ki_matvec_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ki_solve_refined.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_int, _ip, _dp]
+    lib.ki_solve_refined_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_double, C.c_int, _ip, _dp]
     lib.ki_eval_targets.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
     lib.ki_kernel_block.argtypes = [C.c_void_p, C.c_int, _ip, C.c_int, _ip, _dp]
     lib.ki_box_info.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _dp]
@@ -63,6 +79,7 @@ def load():
     lib.ki_allskel.argtypes = [C.c_void_p, _ip]
     lib.ki_stats.argtypes = [C.c_void_p, _dp, C.c_int]
     lib.ki_launch_log.argtypes = [C.c_void_p, _dp, C.c_int]
+    lib.ki_timeline.argtypes = [C.c_void_p, _dp, C.c_int]
     _lib = lib
     return lib
 
@@ -109,7 +126,7 @@ class _Tree:
                 "parent": int(info[6]), "level": int(info[7]),
                 "corner": (geom[0], geom[1]), "side": geom[2],
                 "original": lists[0], "active": lists[1], "skel": lists[2],
-                "redundant": lists[3]}
+                "redundant": lists[3], "tree": int(self.lib.ki_box_tree(self.h, level, idx))}
 
     def all_nodes(self):
         return [[self.node(l, i) for i in range(self.nodes(l))]
@@ -177,6 +194,62 @@ class Solver(_Tree):
         _check(self.lib.ki_apply_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)),
                "ki_apply_device")
 
+    def solve_bordered_device(self, f_ptr, g_ptr, mu_ptr, alpha_ptr):
+        _check(self.lib.ki_solve_bordered_device(self.h, C.c_void_p(f_ptr),
+                                                 C.c_void_p(g_ptr) if g_ptr else None,
+                                                 C.c_void_p(mu_ptr),
+                                                 C.c_void_p(alpha_ptr) if alpha_ptr else None),
+               "ki_solve_bordered_device")
+
+    def solve_transpose_device(self, b_ptr, x_ptr):
+        _check(self.lib.ki_solve_transpose_device(self.h, C.c_void_p(b_ptr), C.c_void_p(x_ptr)),
+               "ki_solve_transpose_device")
+
+    def eval_targets_device(self, n_targets, tg_ptr, mu_ptr, alpha_ptr, out_ptr):
+        _check(self.lib.ki_eval_targets_device(self.h, n_targets, C.c_void_p(tg_ptr),
+                                               C.c_void_p(mu_ptr),
+                                               C.c_void_p(alpha_ptr) if alpha_ptr else None,
+                                               C.c_void_p(out_ptr)), "ki_eval_targets_device")
+
+    def adjoint_forward(self, f_ptr, n_targets, tg_ptr, mu_ptr, u_ptr):
+        _check(self.lib.ki_adjoint_forward(self.h, C.c_void_p(f_ptr), n_targets,
+                                           C.c_void_p(tg_ptr), C.c_void_p(mu_ptr),
+                                           C.c_void_p(u_ptr)), "ki_adjoint_forward")
+
+    def adjoint_backward(self, n_targets, tg_ptr, mu_ptr, gu_ptr, gf_ptr, gp_ptr, gn_ptr, gw_ptr,
+                         gk_ptr):
+        _check(self.lib.ki_adjoint_backward(self.h, n_targets, C.c_void_p(tg_ptr),
+                                            C.c_void_p(mu_ptr), C.c_void_p(gu_ptr),
+                                            C.c_void_p(gf_ptr), C.c_void_p(gp_ptr),
+                                            C.c_void_p(gn_ptr), C.c_void_p(gw_ptr),
+                                            C.c_void_p(gk_ptr)), "ki_adjoint_backward")
+
+    def matvec_device(self, x_ptr, y_ptr):
+        _check(self.lib.ki_matvec_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)),
+               "ki_matvec_device")
+
+    def solve_refined(self, f, rel_tol=1e-12, max_iters=20):
+        """FP64 GMRES refinement preconditioned by this factorization.
+        Returns (mu, alpha, iterations, final true relative residual)."""
+        f = _f64(f)
+        mu = np.zeros(self.n_dofs)
+        alpha = np.zeros(max(1, self.n_border))
+        it = np.zeros(1, dtype=np.int32)
+        rr = np.zeros(1)
+        _check(self.lib.ki_solve_refined(self.h, _d(f), _d(mu),
+                                         _d(alpha) if self.n_border else None, rel_tol,
+                                         max_iters, _i(it), _d(rr)), "ki_solve_refined")
+        return mu, alpha[:self.n_border].copy(), int(it[0]), float(rr[0])
+
+    def solve_refined_device(self, f_ptr, mu_ptr, alpha_ptr=None, rel_tol=1e-12, max_iters=20):
+        it = np.zeros(1, dtype=np.int32)
+        rr = np.zeros(1)
+        _check(self.lib.ki_solve_refined_device(self.h, C.c_void_p(f_ptr), C.c_void_p(mu_ptr),
+                                                C.c_void_p(alpha_ptr) if alpha_ptr else None,
+                                                rel_tol, max_iters, _i(it), _d(rr)),
+               "ki_solve_refined_device")
+        return int(it[0]), float(rr[0])
+
     def eval_targets(self, targets, mu, alpha=None):
         targets = _f64(targets)
         nt = targets.size // 2
@@ -209,10 +282,98 @@ class Solver(_Tree):
                 "top_ms": float(out[6]), "wait_ms": float(out[7]),
                 "host_prep_ms": float(out[8]), "host_post_ms": float(out[9]),
                 "upload_ms": float(out[10]), "host_top_ms": float(out[11]),
-                "id_fold_flops": float(out[12])}
+                "id_onchip_flops": float(out[12])}
+
+    def timeline(self):
+        n = self.lib.ki_timeline(self.h, None, 0)
+        out = np.zeros(4 * max(n, 1))
+        self.lib.ki_timeline(self.h, _d(out), n)
+        return out[:4 * n].reshape(n, 4)
 
     def launch_log(self):
         n = self.lib.ki_launch_log(self.h, None, 0)
         out = np.zeros(7 * max(n, 1))
         self.lib.ki_launch_log(self.h, _d(out), n)
         return out[:7 * n].reshape(n, 7)
+
+
+def _concat(problems):
+    n = np.array([p.n_points for p in problems], dtype=np.int32)
+    cat = lambda name: np.ascontiguousarray(np.concatenate([getattr(p, name) for p in problems]),
+                                            dtype=np.float64)
+    return n, cat("points"), cat("normals"), cat("curvatures"), cat("weights")
+
+
+class BatchPartition(_Tree):
+    """The host partition of many problems (one quadtree each)."""
+
+    def __init__(self, problems, max_leaf_dofs=None):
+        self.lib = load()
+        pr0 = problems[0]
+        leaf = pr0.max_leaf_dofs if max_leaf_dofs is None else max_leaf_dofs
+        self._n, pts, _, _, _ = _concat(problems)
+        self._keep = [pts]
+        h = C.c_void_p()
+        _check(self.lib.ki_partition_batch(len(problems), _i(self._n), _d(pts), pr0.sol_dim, leaf,
+                                           C.byref(h)), "ki_partition_batch")
+        self.h = h
+
+
+class BatchSolver(_Tree):
+    """Many independent problems factored together (ki_factor_batch): dofs
+    of problem p follow those of problems 0..p-1."""
+
+    def __init__(self, problems, id_tol=None, max_leaf_dofs=None, stream=None):
+        self.lib = load()
+        pr0 = problems[0]
+        self.problems = problems
+        self._n, pts, nrm, kap, w = _concat(problems)
+        self._keep = [pts, nrm, kap, w]
+        tol = pr0.id_tol if id_tol is None else id_tol
+        leaf = pr0.max_leaf_dofs if max_leaf_dofs is None else max_leaf_dofs
+        h = C.c_void_p()
+        _check(self.lib.ki_factor_batch(pr0.pde, len(problems), _i(self._n), _d(pts), _d(nrm),
+                                        _d(kap), _d(w), leaf, tol,
+                                        C.c_void_p(stream) if stream else None, C.byref(h)),
+               "ki_factor_batch")
+        self.h = h
+        self.n_dofs = self.lib.ki_num_dofs(h)
+        sd = pr0.sol_dim
+        self.offsets = np.concatenate([[0], np.cumsum(self._n * sd)]).astype(np.int64)
+
+    def split(self, x):
+        return [x[self.offsets[p]:self.offsets[p + 1]] for p in range(len(self.problems))]
+
+    def solve(self, f=None):
+        f = _f64(np.concatenate([p.f for p in self.problems]) if f is None else f)
+        mu = np.zeros(self.n_dofs)
+        _check(self.lib.ki_solve(self.h, _d(f), _d(mu), None), "ki_solve")
+        return mu
+
+    def solve_device(self, f_ptr, mu_ptr):
+        _check(self.lib.ki_solve_device(self.h, C.c_void_p(f_ptr), C.c_void_p(mu_ptr), None),
+               "ki_solve_device")
+
+    def solve_refined(self, f=None, rel_tol=1e-12, max_iters=20):
+        f = _f64(np.concatenate([p.f for p in self.problems]) if f is None else f)
+        mu = np.zeros(self.n_dofs)
+        it = np.zeros(1, dtype=np.int32)
+        rr = np.zeros(1)
+        _check(self.lib.ki_solve_refined(self.h, _d(f), _d(mu), None, rel_tol, max_iters,
+                                         _i(it), _d(rr)), "ki_solve_refined")
+        return mu, int(it[0]), float(rr[0])
+
+    def solve_refined_device(self, f_ptr, mu_ptr, rel_tol=1e-12, max_iters=20):
+        it = np.zeros(1, dtype=np.int32)
+        rr = np.zeros(1)
+        _check(self.lib.ki_solve_refined_device(self.h, C.c_void_p(f_ptr), C.c_void_p(mu_ptr),
+                                                None, rel_tol, max_iters, _i(it), _d(rr)),
+               "ki_solve_refined_device")
+        return int(it[0]), float(rr[0])
+
+    def apply_device(self, x_ptr, y_ptr):
+        _check(self.lib.ki_apply_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)),
+               "ki_apply_device")
+
+    def stats(self):
+        return Solver.stats(self)

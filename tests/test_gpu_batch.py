@@ -1,0 +1,83 @@
+"""GPU batch of independent problems (ki_factor_batch): one forest
+factorization must give every problem the ranks, skeletons and solution it
+gets alone, and the batch refinement must bring every problem to FP64
+accuracy.
+
+Bars: ranks and skeleton sets identical to the single-problem factorization
+(integers); direct-solve mu within 1e-12 relative of the single-problem
+solve (the top-level LU of a batch runs in a different kernel, so only the
+last bits differ); refined per-problem residual <= 1e-12 and mu within 1e-10
+of the FP64 oracle at id_tol 1e-13."""
+import numpy as np
+import pytest
+
+import helpers as H
+import ki_geometry as G
+import kinterp
+import kioracle as K
+
+pytestmark = pytest.mark.gpu
+
+
+def _boxes(s):
+    out = {}
+    for l in range(s.levels()):
+        for i in range(s.nodes(l)):
+            b = s.node(l, i)
+            out.setdefault(b["tree"], []).append(b)
+    return out
+
+
+def test_batch_matches_single_factorizations():
+    probs = G.random_star_cases(count=12, seed=21, nmin=512, nmax=4096)
+    bs = kinterp.BatchSolver(probs, id_tol=1e-10)
+    trees = _boxes(bs)
+    mu_all = bs.split(bs.solve())
+    off = 0
+    for p, pr in enumerate(probs):
+        s = kinterp.Solver(pr, id_tol=1e-10)
+        single = [s.node(l, i) for l in range(s.levels()) for i in range(s.nodes(l))]
+        assert len(single) == len(trees[p])
+        for a, b in zip(single, trees[p]):
+            assert a["compressed"] == b["compressed"]
+            assert len(a["skel"]) == len(b["skel"])
+            assert np.array_equal(np.sort(a["skel"] + off), np.sort(b["skel"]))
+        mu, _ = s.solve(pr.f)
+        assert H.rel(mu_all[p], mu) < 1e-12
+        off += pr.n_dofs
+        s.close()
+    bs.close()
+
+
+def test_batch_refined_mixed():
+    probs = G.random_star_cases(count=16, seed=22, nmin=512, nmax=8192)
+    bs = kinterp.BatchSolver(probs, id_tol=1e-6)
+    mu, it, rr = bs.solve_refined(rel_tol=1e-12, max_iters=20)
+    assert rr <= 1e-12, (it, rr)
+    parts = bs.split(mu)
+    for p in (0, 5, 11):
+        o = K.PortSolver(probs[p], id_tol=1e-13, threads=8)
+        mt, _ = o.solve(probs[p].f)
+        o.close()
+        assert H.rel(parts[p], mt) < 1e-10
+
+
+def test_batch_exact_operator_is_block_diagonal():
+    import torch
+    probs = G.random_star_cases(count=3, seed=23, nmin=300, nmax=900)
+    bs = kinterp.BatchSolver(probs, id_tol=1e-6)
+    x = np.random.default_rng(1).standard_normal(bs.n_dofs)
+    xd = torch.tensor(x, device="cuda")
+    y = torch.empty_like(xd)
+    bs.apply_device(xd.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    ys = bs.split(y.cpu().numpy())
+    xs = bs.split(x)
+    for p, pr in enumerate(probs):
+        s = kinterp.Solver(pr, id_tol=1e-6)
+        xp = torch.tensor(xs[p], device="cuda")
+        yp = torch.empty_like(xp)
+        s.apply_device(xp.data_ptr(), yp.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(yp.cpu().numpy(), ys[p])
+        s.close()

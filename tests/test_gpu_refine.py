@@ -1,0 +1,122 @@
+"""GPU refinement path: the fast FP64 operator product, the preconditioner
+with a border right-hand side, and GMRES refinement of a loose
+factorization to FP64 accuracy, against the FP64 oracle and dense solves.
+
+Bars: the fast product equals the entry-exact product to 1e-13 relative
+(FP64 rounding of a reassociated sum); the refined solution of a factorization
+at id_tol 1e-6 has true relative residual <= 1e-12 and is within 1e-10
+relative of the FP64 oracle's solution at id_tol 1e-10."""
+import numpy as np
+import pytest
+
+import helpers as H
+import ki_geometry as G
+import kinterp
+import kioracle as K
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _oracle_built():
+    H.ensure_oracle()
+
+
+def _problems():
+    return {
+        "ellipse_laplace_1024": G.ellipse_case(),
+        "stokes_holes_4096": G.stokes_holes_case(n_total=4096),
+        "fourier_star_laplace_2048": G.fourier_star_case(n=2048),
+    }
+
+
+def _dev(a):
+    import torch
+    return torch.tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+@pytest.mark.parametrize("name", list(_problems()))
+def test_fast_matvec_matches_entry_exact_product(name):
+    import torch
+    pr = _problems()[name]
+    s = kinterp.Solver(pr, id_tol=1e-6)
+    rng = np.random.default_rng(7)
+    x = _dev(rng.standard_normal(s.n_dofs + s.n_border))
+    y0 = torch.empty_like(x)
+    y1 = torch.empty_like(x)
+    s.apply_device(x.data_ptr(), y0.data_ptr())
+    s.matvec_device(x.data_ptr(), y1.data_ptr())
+    torch.cuda.synchronize()
+    a, b = y0.cpu().numpy(), y1.cpu().numpy()
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-13
+
+
+def test_fast_matvec_laplace_neumann():
+    import torch
+    pr = G.ellipse_case(n=1024)
+    pr.pde = G.LAPLACE_NEUMANN
+    s = kinterp.Solver(pr, id_tol=1e-6)
+    x = _dev(np.random.default_rng(3).standard_normal(s.n_dofs))
+    y0 = torch.empty_like(x)
+    y1 = torch.empty_like(x)
+    s.apply_device(x.data_ptr(), y0.data_ptr())
+    s.matvec_device(x.data_ptr(), y1.data_ptr())
+    torch.cuda.synchronize()
+    a, b = y0.cpu().numpy(), y1.cpu().numpy()
+    assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-13
+
+
+def test_preconditioner_border_rhs():
+    """The bordered solve with a nonzero border right-hand side g inverts the
+    bordered operator: A M^-1 [f; g] = [f; g] to the factorization's accuracy."""
+    import torch
+    pr = G.stokes_holes_case(n_total=4096)
+    s = kinterp.Solver(pr, id_tol=1e-10)
+    rng = np.random.default_rng(11)
+    N, nb = s.n_dofs, s.n_border
+    f = rng.standard_normal(N)
+    g = rng.standard_normal(nb)
+    fd, gd = _dev(f), _dev(g)
+    x = torch.zeros(N + nb, dtype=torch.float64, device="cuda")
+    s.solve_bordered_device(fd.data_ptr(), gd.data_ptr(), x.data_ptr(), x.data_ptr() + 8 * N)
+    y = torch.empty_like(x)
+    s.apply_device(x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    r = y.cpu().numpy() - np.concatenate([f, g])
+    assert np.linalg.norm(r) / np.linalg.norm(np.concatenate([f, g])) < 1e-8
+
+
+@pytest.mark.parametrize("name", list(_problems()))
+def test_refined_loose_factor_reaches_fp64(name):
+    """The FP64 oracle at id_tol 1e-10 carries its own ~1e-10 error (it is a
+    1e-10 factorization); the converged reference here is the same oracle
+    at id_tol 1e-13.  The refined GPU solution must be within 1e-10 of it,
+    and no farther from the 1e-10 oracle than that oracle's own error allows."""
+    pr = _problems()[name]
+    s = kinterp.Solver(pr, id_tol=1e-6)
+    mu, alpha, it, rr = s.solve_refined(pr.f, rel_tol=1e-12, max_iters=30)
+    assert rr <= 1e-12, (it, rr)
+    assert it <= 10
+    o = K.PortSolver(pr, threads=8)
+    mo, ao = o.solve(pr.f)
+    o.close()
+    o = K.PortSolver(pr, id_tol=1e-13, threads=8)
+    mt, at = o.solve(pr.f)
+    o.close()
+    assert H.rel(mu, mt) < 1e-10
+    if len(alpha):
+        assert np.abs(alpha - at).max() < 1e-10 * max(1.0, np.abs(mt).max())
+    own = H.rel(mo, mt)
+    assert H.rel(mu, mo) < max(1e-10, 2.0 * own)
+
+
+def test_refined_matches_dense_solve():
+    """Small Laplace problem: dense FP64 matrix from the exact entries,
+    numpy solve; the refined GPU solution agrees to 1e-12."""
+    pr = G.ellipse_case(n=1024)
+    s = kinterp.Solver(pr, id_tol=1e-6)
+    idx = np.arange(s.n_dofs, dtype=np.int32)
+    A = s.kernel_block(idx, idx)
+    mu_dense = np.linalg.solve(A, pr.f)
+    mu, _, it, rr = s.solve_refined(pr.f, rel_tol=1e-13, max_iters=30)
+    assert H.rel(mu, mu_dense) < 1e-12
