@@ -2,23 +2,38 @@
 """Factor + solve throughput of the B200 recursive-skeletonization solver.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload star16k|stokes65k|ellipse1k]
+                    [--workload star16k|stokes65k|ellipse1k|batch256]
+                    [--no-cpu-baseline] [--no-adjoint]
 
-One step = QuadTree build + skeletonize + solve of one boundary integral
-problem (the reference's SkelFactorization::skeletonize + linear_solve,
-skel_factorization.cpp:94-403).  The default workload is the Laplace star
-r = 1 + 0.3 cos 5t with N = 16384 nodes, 64-point leaves and ID tolerance
-1e-10 (FP64).  The metric is unknowns / (factor + solve time).
+One step = QuadTree build + skeletonize + solve of the workload (the
+reference's SkelFactorization::skeletonize + linear_solve,
+skel_factorization.cpp:94-403) to 1e-10 relative error.  The metric is
+unknowns / (factor + solve time), for two methods on the same GPU:
 
-`value` times ki_factor (geometry from host memory: the quadtree is built on
-the host) + ki_solve_device with the right-hand side resident in HBM; `e2e`
-times the public host-buffer path ki_factor + ki_solve with pinned inputs
-and the solution copied back.  Both are CUDA-event times on the stream the
-library launches on, L2 flushed (256 MiB write) between steps.  With N > 1
-GPUs (torchrun) every rank factors its own replica of the problem (one
-problem does not shard); the time is the max over ranks.
-`--impl reference` times the reference solver compiled from its own sources
-(oracle/_ref) on the host cores for the same workload.
+  * mixed + refine (`value`): the factorization at ID tolerance 1e-6 used as
+    the preconditioner of FP64 GMRES on the operator with on-the-fly FP64
+    entries, stopped at true relative residual 1e-12 (ki_factor +
+    ki_solve_refined_device);
+  * FP64 (`fp64`): the reference method, factorization at ID tolerance
+    1e-10 and one direct solve (ki_factor + ki_solve_device).
+
+The default workload is the Laplace star r = 1 + 0.3 cos 5t, N = 16384 nodes,
+64-point leaves; `stokes65k` is the Stokes disk with 8 holes (65,536 dofs);
+`batch256` is 256 random stars of 512-8192 nodes factored together
+(ki_factor_batch).  Errors are reported against the FP64 oracle (the
+reference algorithm restated on the CPU) at ID tolerance 1e-10 and, as the
+converged reference, at 1e-13.
+
+Timing: CUDA events on the stream the library launches on, the right-hand
+side resident in HBM, the L2 flushed (256 MiB write) before every step;
+`e2e` is the mixed method through the host-buffer API (pinned geometry and
+data in, solution out) in the same way.  With N > 1 GPUs (torchrun) every
+rank solves its own replica (one problem does not shard): weak scaling, time
+= max over ranks.  Unless --no-adjoint, the default workload also times the
+adjoint of the target-potential objective on the 8192-node Fourier star
+(forward solve + targets, backward transposed solve + kernel-derivative
+contractions).  `--impl reference` times the reference solver compiled from
+its own sources (oracle/_ref) on the host cores for the same workload.
 """
 from __future__ import annotations
 
@@ -40,15 +55,21 @@ import numpy as np  # noqa: E402
 import ki_geometry as G  # noqa: E402
 
 METRIC = "factor+solve unknowns/s at 1e-10 rel err"
+MIXED_TOL = 1e-6      # ID tolerance of the preconditioning factorization
+REFINE_TOL = 1e-12    # true relative residual at which GMRES stops
+FP64_TOL = 1e-10
+
 WORKLOADS = {
     "star16k": (lambda: G.star_case(),
-                "Laplace double layer, star r=1+0.3cos5t, N=16384 nodes, leaf 64 pts, "
-                "id_tol 1e-10, FP64"),
+                "Laplace double layer, star r=1+0.3cos5t, N=16384 nodes, leaf 64 pts"),
     "stokes65k": (lambda: G.stokes_holes_case(),
                   "Stokes double layer, unit disk with 8 holes, 32768 nodes (65536 dofs), "
-                  "leaf 64 pts, id_tol 1e-10, FP64, multiply-connected"),
+                  "leaf 64 pts, multiply-connected"),
     "ellipse1k": (lambda: G.ellipse_case(),
-                  "Laplace double layer, ellipse (1.0,0.6), N=1024, leaf 64 pts, id_tol 1e-10, FP64"),
+                  "Laplace double layer, ellipse (1.0,0.6), N=1024, leaf 64 pts"),
+    "batch256": (lambda: G.random_star_cases(256, seed=4),
+                 "256 Laplace random stars r=1+sum a_k cos(k t+phi_k), N log-uniform in "
+                 "[512, 8192] (796,517 dofs in all), leaf 64 pts, one batched factorization"),
 }
 
 
@@ -144,59 +165,105 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def run_reference(args, pr, units):
-    """Reference arm: the reference solver built from its own sources."""
+# ------------------------------------------------------------------ CPU arms
+def _ref_solver():
     import kioracle as K
     kind = "reference" if K.ref_available() else "port"
+    return kind, (K.RefSolver if kind == "reference" else K.PortSolver)
+
+
+def _cpu_problems(workload, probs, per_step):
+    """The problems one CPU step solves: the whole workload, or for the
+    batch a bounded rotating sample of it."""
+    if workload != "batch256":
+        return lambda step: probs
+    return lambda step: [probs[(step * per_step + i) % len(probs)] for i in range(per_step)]
+
+
+def run_reference(args, probs):
+    """Reference arm: the reference solver built from its own sources."""
+    kind, Solver = _ref_solver()
     cores = os.cpu_count() or 1
-    Solver = K.RefSolver if kind == "reference" else K.PortSolver
+    pick = _cpu_problems(args.workload, probs, 16)
 
-    def step():
-        t0 = time.perf_counter()
-        s = Solver(pr, threads=cores)
-        mu, alpha = s.solve(pr.f)
-        dt = time.perf_counter() - t0
-        s.close()
-        return dt
+    def step(i):
+        t = 0.0
+        u = 0
+        for pr in pick(i):
+            t0 = time.perf_counter()
+            s = Solver(pr, id_tol=FP64_TOL, threads=cores)
+            s.solve(pr.f)
+            t += time.perf_counter() - t0
+            s.close()
+            u += pr.n_dofs
+        return t, u
 
-    for _ in range(args.warmup):
-        step()
-    times = [step() for _ in range(args.steps)]
-    total = sum(times)
-    value = units * args.steps / total
+    for i in range(args.warmup):
+        step(i)
+    tot_t, tot_u = 0.0, 0
+    for i in range(args.steps):
+        t, u = step(args.warmup + i)
+        tot_t += t
+        tot_u += u
+    value = tot_u / tot_t
+    sample = ("%d steps, each a full FP64 factor+solve (id_tol 1e-10) of %s (OpenBLAS 0.3.15, "
+              "1 BLAS thread, %d OpenMP box threads)"
+              % (args.steps, "16 of the 256 problems" if args.workload == "batch256"
+                 else "the workload", cores))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "unknowns/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload][1], "n_dofs": units,
+            "config": {"workload": WORKLOADS[args.workload][1], "method": "FP64 direct",
                        "parallelism": "host threads", "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": "unknowns/s", "cores": cores,
-                             "kind": kind,
-                             "sample": "%d full factor+solve runs of the workload "
-                                       "(OpenBLAS 0.3.15, 1 BLAS thread, %d OpenMP box "
-                                       "threads)" % (args.steps, cores)},
+                             "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "unknowns/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(pr, units, budget_s=12.0):
-    import kioracle as K
-    kind = "reference" if K.ref_available() else "port"
-    Solver = K.RefSolver if kind == "reference" else K.PortSolver
+def cpu_baseline(workload, probs, budget_s=12.0):
+    kind, Solver = _ref_solver()
     cores = os.cpu_count() or 1
-    n, t = 0, 0.0
+    pick = _cpu_problems(workload, probs, 16)
+    n, t, u = 0, 0.0, 0
     while t < budget_s and n < 40:
-        t0 = time.perf_counter()
-        s = Solver(pr, threads=cores)
-        s.solve(pr.f)
-        t += time.perf_counter() - t0
-        s.close()
+        for pr in pick(n):
+            t0 = time.perf_counter()
+            s = Solver(pr, id_tol=FP64_TOL, threads=cores)
+            s.solve(pr.f)
+            t += time.perf_counter() - t0
+            s.close()
+            u += pr.n_dofs
         n += 1
-    return {"value": units * n / t, "unit": "unknowns/s", "cores": cores, "kind": kind,
-            "sample": "%d full factor+solve runs of the same workload (%.1f s)" % (n, t)}
+    what = "16-problem samples of the batch" if workload == "batch256" else "full factor+solve runs"
+    return {"value": u / t, "unit": "unknowns/s", "cores": cores, "kind": kind,
+            "sample": "%d %s, FP64 id_tol 1e-10 (%.1f s)" % (n, what, t)}
 
 
+def oracle_solutions(probs, idx):
+    """FP64 oracle (CPU restatement) at id_tol 1e-10 and 1e-13 for the
+    problems idx: (mu_1e10, mu_1e13) lists."""
+    import kioracle as K
+    cores = os.cpu_count() or 1
+    a, b = [], []
+    for i in idx:
+        pr = probs[i]
+        o = K.PortSolver(pr, id_tol=FP64_TOL, threads=cores)
+        a.append(o.solve(pr.f)[0])
+        o.close()
+        o = K.PortSolver(pr, id_tol=1e-13, threads=cores)
+        b.append(o.solve(pr.f)[0])
+        o.close()
+    return a, b
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,18 +272,21 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="star16k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    pr = WORKLOADS[args.workload][0]()
-    units = pr.n_dofs
+    built = WORKLOADS[args.workload][0]()
+    batch = args.workload == "batch256"
+    probs = built if batch else [built]
+    units = sum(p.n_dofs for p in probs)
 
     if args.impl == "reference":
         if rank == 0:
-            run_reference(args, pr, units)
+            run_reference(args, probs)
         return
 
     import torch
@@ -233,136 +303,255 @@ def main():
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    f_dev = torch.tensor(pr.f, device=dev, dtype=torch.float64)
+    f_host = np.concatenate([p.f for p in probs])
+    f_dev = torch.tensor(f_host, device=dev, dtype=torch.float64)
     mu_dev = torch.empty_like(f_dev)
-    nb = 3 * pr.holes.shape[0] if pr.pde == G.STOKES else pr.holes.shape[0]
+    pr0 = probs[0]
+    nb = 0 if batch else (3 * pr0.holes.shape[0] if pr0.pde == G.STOKES else pr0.holes.shape[0])
     al_dev = torch.empty(max(nb, 1), device=dev, dtype=torch.float64)
 
-    def device_step(timed):
-        s = kinterp.Solver(pr, stream=sh, timed=timed)
-        s.solve_device(f_dev.data_ptr(), mu_dev.data_ptr(), al_dev.data_ptr() if nb else None)
+    def factor(tol, timed=False):
+        if batch:
+            return kinterp.BatchSolver(probs, id_tol=tol, stream=sh)
+        return kinterp.Solver(pr0, id_tol=tol, stream=sh, timed=timed)
+
+    def mixed_step(timed):
+        s = factor(MIXED_TOL, timed)
+        if batch:
+            it, rr = s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
+                                            rel_tol=REFINE_TOL, max_iters=20)
+        else:
+            it, rr = s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
+                                            al_dev.data_ptr() if nb else None,
+                                            rel_tol=REFINE_TOL, max_iters=20)
+        return s, it, rr
+
+    def fp64_step(timed):
+        s = factor(FP64_TOL, timed)
+        if batch:
+            s.solve_device(f_dev.data_ptr(), mu_dev.data_ptr())
+        else:
+            s.solve_device(f_dev.data_ptr(), mu_dev.data_ptr(), al_dev.data_ptr() if nb else None)
         return s
 
+    def timed_loop(step_fn):
+        """K steps, each: flush L2, events around one step on the library's
+        stream.  Returns the total ms."""
+        total = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_fn()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total
+
+    # warm-up of both methods
     for _ in range(args.warmup):
-        device_step(False).close()
+        mixed_step(False)[0].close()
+        fp64_step(False).close()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
+
+    # ---- mixed + refine (the value)
     clocks = Clocks(local)
     launches0 = kinterp.kernel_launches()
-    total_ms = 0.0
-    id_ms = id_flops = id_bytes = id_launch = 0.0
-    factor_ms = []
-    kinds = {}
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s = device_step(True)
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        st = s.stats()
-        factor_ms.append(st["factor_ms"])
-        id_ms += st["id_ms"]
-        id_flops += st["id_flops"]
-        id_bytes += st["id_bytes"]
-        id_launch += st["id_launches"]
-        for row in s.launch_log():
-            kinds[int(row[1])] = kinds.get(int(row[1]), 0.0) + row[6]
+    keys = ("id_ms", "id_flops", "id_bytes", "id_launches", "factor_ms", "decouple_ms", "top_ms")
+    st_acc = {k: 0.0 for k in keys}
+    iters, rres = [], []
+
+    def mixed_timed():
+        s, it, rr = mixed_step(not batch)
+        if not batch:
+            st = s.stats()
+            for k in keys:
+                st_acc[k] += st[k]
+        iters.append(it)
+        rres.append(rr)
         s.close()
-    torch.cuda.synchronize()
+
+    t_mixed = timed_loop(mixed_timed)
     launches = kinterp.kernel_launches() - launches0
     clk = clocks.stop()
+    mu_mixed = mu_dev.cpu().numpy()
+    al_mixed = al_dev.cpu().numpy()[:nb]
 
-    # e2e: public host-buffer API, pinned inputs, result read back every step
+    # ---- FP64 direct (the reference method on the GPU)
+    f64_factor = []
+
+    def fp64_timed():
+        s = fp64_step(not batch)
+        if not batch:
+            f64_factor.append(s.stats()["factor_ms"])
+        s.close()
+
+    t_fp64 = timed_loop(fp64_timed)
+    mu_fp64 = mu_dev.cpu().numpy()
+
+    # ---- e2e: public host-buffer API, pinned inputs, solution read back
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
     import copy
-    pe = copy.copy(pr)
-    pe.points, pe.normals = pin(pr.points), pin(pr.normals)
-    pe.curvatures, pe.weights, pe.f = pin(pr.curvatures), pin(pr.weights), pin(pr.f)
-    e2e_ms = 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s = kinterp.Solver(pe, stream=sh)
-        mu_h, al_h = s.solve(pe.f)
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
+    pp = []
+    for p in probs:
+        q = copy.copy(p)
+        q.points, q.normals = pin(p.points), pin(p.normals)
+        q.curvatures, q.weights = pin(p.curvatures), pin(p.weights)
+        pp.append(q)
+    f_pin = pin(f_host)
+
+    def e2e_step():
+        if batch:
+            s = kinterp.BatchSolver(pp, id_tol=MIXED_TOL, stream=sh)
+        else:
+            s = kinterp.Solver(pp[0], id_tol=MIXED_TOL, stream=sh)
+        s.solve_refined(f_pin, rel_tol=REFINE_TOL, max_iters=20)
         s.close()
 
-    t_max = total_ms
-    e2e_max = e2e_ms
+    t_e2e = timed_loop(e2e_step)
+
+    t_max = [t_mixed, t_fp64, t_e2e]
     if dist:
-        t = torch.tensor([total_ms, e2e_ms], device=dev, dtype=torch.float64)
+        t = torch.tensor(t_max, device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max, e2e_max = float(t[0]), float(t[1])
+        t_max = [float(x) for x in t]
+    t_mixed, t_fp64, t_e2e = t_max
 
     if rank == 0:
-        # parity of the timed path against the FP64 oracle, and the analytic error
-        import kioracle as K
-        o = K.PortSolver(pr, threads=os.cpu_count() or 1)
-        mo, ao = o.solve(pr.f)
-        rel_oracle = float(np.linalg.norm(mu_h - mo) / np.linalg.norm(mo))
-        s = kinterp.Solver(pr)
-        u = s.eval_targets(pr.targets, mu_h, al_h)
-        analytic = float(np.linalg.norm(u - pr.exact) / np.linalg.norm(pr.exact))
-        s.close()
+        # accuracy against the FP64 oracle (at the reference's 1e-10 and,
+        # as the converged solution, at 1e-13)
+        idx = [0, 100, 200] if batch else [0]
+        o10, o13 = oracle_solutions(probs, idx)
+        offs = np.concatenate([[0], np.cumsum([p.n_dofs for p in probs])])
+        err = lambda mu, ref: max(rel(mu[offs[i]:offs[i + 1]], r) for i, r in zip(idx, ref))
+        analytic = None
+        if not batch:
+            s = kinterp.Solver(pr0)
+            u = s.eval_targets(pr0.targets, mu_mixed, al_mixed)
+            analytic = rel(u, pr0.exact)
+            s.close()
+        peak64 = fp64_peak_tflops(dev)
         hbm_peak, hbm_kind = peaks()
-        fp64_peak = fp64_peak_tflops(dev)
-        achieved = (id_flops / (id_ms * 1e-3)) / 1e12 if id_ms > 0 else None
-        traffic = traffic_from_profile(args.workload)
-        h2d = 8 * (6 * pr.n_points + units)
+        id_ms = st_acc["id_ms"]
+        achieved = (st_acc["id_flops"] / (id_ms * 1e-3)) / 1e12 if id_ms > 0 else None
+        nlaunch = max(st_acc["id_launches"], 1)
+        h2d = sum(8 * (6 * p.n_points) for p in probs) + 8 * units
         d2h = 8 * (units + nb)
-        value = world * units * args.steps / (t_max * 1e-3)
+        value = world * units * args.steps / (t_mixed * 1e-3)
+        fp64_value = world * units * args.steps / (t_fp64 * 1e-3)
         line = {
             "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload][1], "n_dofs": units,
-                       "leaf_dofs": pr.max_leaf_dofs, "id_tol": pr.id_tol,
+                       "method": "mixed+refine: factor at id_tol %g, FP64 GMRES with on-the-fly "
+                                 "FP64 operator to true rel. residual %g" % (MIXED_TOL, REFINE_TOL),
+                       "leaf_dofs": pr0.max_leaf_dofs,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "flushed between steps (256 MiB device write)"},
-            "factor_ms": float(np.mean(factor_ms)),
-            "solve_ms": t_max / args.steps - float(np.mean(factor_ms)),
-            "rel_err_vs_fp64_oracle": rel_oracle, "analytic_rel_err": analytic,
-            "phase_ms_per_step": {"id": kinds.get(0, 0.0) / args.steps,
-                                  "decouple": kinds.get(1, 0.0) / args.steps,
-                                  "top": kinds.get(2, 0.0) / args.steps},
-            "roofline": {"kernel": "ID kernels (id_onchip_kernel / id_kernel: entry generation, "
-                                   "pivoted QR, T)",
-                         "bound": "tensor", "pipe": "fp64 (no tcgen05 FP64 kind; FP64 FMA)",
-                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": (achieved / fp64_peak) if achieved else None,
-                         "peak_source": "measured live on this GPU: cuBLAS DGEMM 4096^3 "
-                                        "(no FP64 figure in MEASURED_PEAKS.json)",
-                         "flops_per_launch": id_flops / max(id_launch, 1),
-                         "algorithmic_hbm_bytes_per_launch": id_bytes / max(id_launch, 1),
-                         "hbm_frac_of_measured": ((id_bytes / (id_ms * 1e-3)) / 1e9 / hbm_peak)
-                         if id_ms > 0 else None,
-                         "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_kind,
-                         "launches_per_step": id_launch / args.steps,
-                         "ms_per_step": id_ms / args.steps,
-                         "traffic": traffic},
-            "e2e": {"value": world * units * args.steps / (e2e_max * 1e-3),
+            "gmres_iters": float(np.mean(iters)), "true_rel_residual": float(max(rres)),
+            "rel_err_vs_fp64_oracle": err(mu_mixed, o10),
+            "rel_err_vs_converged_oracle": err(mu_mixed, o13),
+            "fp64_oracle_own_err": max(rel(a, b) for a, b in zip(o10, o13)),
+            "analytic_rel_err": analytic,
+            "factor_ms": None if batch else st_acc["factor_ms"] / args.steps,
+            "phase_ms_per_step": None if batch else {
+                "id": id_ms / args.steps, "decouple": st_acc["decouple_ms"] / args.steps,
+                "top": st_acc["top_ms"] / args.steps},
+            "fp64": {"value": fp64_value, "ms_per_step": t_fp64 / args.steps,
+                     "factor_ms": float(np.mean(f64_factor)) if f64_factor else None,
+                     "id_tol": FP64_TOL,
+                     "rel_err_vs_fp64_oracle": err(mu_fp64, o10),
+                     "rel_err_vs_converged_oracle": err(mu_fp64, o13)},
+            "speedup_mixed_vs_fp64": value / fp64_value,
+            "roofline": None if not id_ms else {
+                "kernel": "ID kernels (id_onchip_kernel / id_kernel: entry generation, "
+                          "pivoted QR, T) of the mixed factorization",
+                "bound": "tensor", "pipe": "fp64 (no tcgen05 FP64 kind; FP64 FMA)",
+                "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
+                "frac": (achieved / peak64) if achieved else None,
+                "peak_source": "measured live on this GPU: cuBLAS DGEMM 4096^3 "
+                               "(no FP64 figure in MEASURED_PEAKS.json)",
+                "flops_per_launch": st_acc["id_flops"] / nlaunch,
+                "algorithmic_hbm_bytes_per_launch": st_acc["id_bytes"] / nlaunch,
+                "hbm_frac_of_measured": (st_acc["id_bytes"] / (id_ms * 1e-3)) / 1e9 / hbm_peak,
+                "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_kind,
+                "launches_per_step": st_acc["id_launches"] / args.steps,
+                "ms_per_step": id_ms / args.steps,
+                "traffic": traffic_from_profile(args.workload)},
+            "e2e": {"value": world * units * args.steps / (t_e2e * 1e-3),
                     "unit": "unknowns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "clocks": clk,
         }
+        if args.workload == "star16k" and not args.no_adjoint:
+            line["adjoint"] = adjoint_bench(dev, stream)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(pr, units)
+            line["cpu_baseline"] = cpu_baseline(args.workload, probs)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def adjoint_bench(dev, stream, reps=5):
+    """Adjoint of J = sum_t (u_t - u*_t)^2 on the 8192-node Fourier star (32
+    shape coefficients, 64 targets): forward (geometry, factor at 1e-10,
+    solve, targets) + backward (transposed solve, kernel-derivative
+    contractions, chain rule to the coefficients), CUDA events on the
+    caller's stream (device-wide synchronisation around each run); gradient
+    checked against central differences (h = 1e-6) in two coefficients."""
+    import torch
+    import ki_autograd as KA
+    pr = G.fourier_star_case(n=8192)
+    coef, u_star = pr.extra["coef"], pr.extra["u_star"]
+    tg = torch.tensor(pr.targets, dtype=torch.float64, device=dev)
+    us = torch.tensor(u_star, dtype=torch.float64, device=dev)
+    f = torch.tensor(pr.f, dtype=torch.float64, device=dev)
+
+    def objective(c_np):
+        c = torch.tensor(c_np, dtype=torch.float64, device=dev)
+        pts, nrm, kap, w = KA.fourier_star_geometry(c, pr.n_points)
+        u = KA.target_potential(pts, nrm, kap, w, f, tg, pr.leaf_points, FP64_TOL)
+        return float(((u - us) ** 2).sum())
+
+    times, fwd = [], []
+    g = None
+    for i in range(reps + 2):
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        c = torch.tensor(coef, dtype=torch.float64, device=dev, requires_grad=True)
+        pts, nrm, kap, w = KA.fourier_star_geometry(c, pr.n_points)
+        u = KA.target_potential(pts, nrm, kap, w, f, tg, pr.leaf_points, FP64_TOL)
+        J = ((u - us) ** 2).sum()
+        e1.record(stream)
+        J.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        if i >= 2:
+            times.append(e0.elapsed_time(e2))
+            fwd.append(e0.elapsed_time(e1))
+        g = c.grad.cpu().numpy()
+    h = 1e-6
+    fd_err = 0.0
+    for q in (0, 17):
+        cp, cm = coef.copy(), coef.copy()
+        cp[q] += h
+        cm[q] -= h
+        fd = (objective(cp) - objective(cm)) / (2 * h)
+        fd_err = max(fd_err, abs(fd - g[q]) / np.abs(g).max())
+    return {"workload": "Laplace Fourier star, 32 shape coefficients, N=8192, leaf 64 pts, "
+                        "64 targets, id_tol 1e-10",
+            "ms": float(np.median(times)), "forward_ms": float(np.median(fwd)),
+            "backward_ms": float(np.median(times) - np.median(fwd)),
+            "grad_vs_central_fd_rel": fd_err}
 
 
 if __name__ == "__main__":

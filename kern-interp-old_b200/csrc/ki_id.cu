@@ -493,17 +493,18 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
   const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  double* cols = reinterpret_cast<double*>(smem_raw);  // owned columns
-  double* v = cols + P.col_cap;                        // m_cap
-  double* rdiag = v + P.m_cap;                          // n_cap
-  double* vn1 = rdiag + P.n_cap;                        // n_cap
-  double* vn2 = vn1 + P.n_cap;                          // n_cap
-  double* red = vn2 + P.n_cap;                          // 32
-  Cand* wbest = reinterpret_cast<Cand*>(red + 32);      // kOcWarps
-  Cand* slot = wbest + kOcWarps;                        // 2
-  int* pos2col = reinterpret_cast<int*>(slot + 2);      // n_cap
-  int* own = pos2col + P.n_cap;                         // n_cap
-  int* si = own + P.n_cap;                              // [0] own count, [1] pivot
+  // layout of this task (every CTA of the cluster has the same task)
+  double* cols = reinterpret_cast<double*>(smem_raw);   // owned columns
+  double* v = cols + static_cast<long long>((n + G - 1) / G) * lda;  // m
+  double* rdiag = v + m;                                 // n
+  double* vn1 = rdiag + n;                               // n
+  double* vn2 = vn1 + n;                                 // n
+  double* red = vn2 + n;                                 // 32
+  Cand* wbest = reinterpret_cast<Cand*>(red + 32);       // kOcWarps
+  Cand* slot = wbest + kOcWarps;                         // 2
+  int* pos2col = reinterpret_cast<int*>(slot + 2);       // n
+  int* own = pos2col + n;                                // n
+  int* si = own + n;                                     // [0] own count, [1] pivot
 
   auto colp = [&](int j) -> double* {
     double* base = cols + static_cast<long long>(j / G) * lda;
@@ -779,7 +780,8 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
 
 template <int G>
 cudaError_t launch_onchip(const IdParams& p, cudaStream_t s) {
-  const size_t smem = id_smem_bytes(p.m_cap, p.n_cap) + sizeof(double) * p.col_cap;
+  const size_t smem = static_cast<size_t>(p.onchip_smem);
+  if (smem == 0 || smem > 227 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(id_onchip_kernel<G>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
@@ -835,6 +837,11 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 }
 
 }  // namespace
+
+size_t id_onchip_smem_bytes(int m, int n, int G) {
+  return id_smem_bytes(m, n) +
+         sizeof(double) * static_cast<size_t>((n + G - 1) / G) * onchip_lda(m);
+}
 
 size_t id_smem_bytes(int m_cap, int n_cap) {
   return sizeof(double) * (static_cast<size_t>(m_cap) + 3 * n_cap + 32) +

@@ -48,9 +48,14 @@ struct IdParams {
   int* rank;
   const double* proxy_dir;  // cos/sin table, 2 * kNumProxy doubles
   double tol;
-  int m_cap, n_cap;  // maxima over the launch (shared-memory layout)
-  long long col_cap;  // on-chip launches: doubles of columns per CTA
+  int m_cap, n_cap;  // streaming launches: maxima over the launch (shared-memory layout)
+  long long col_cap;  // unused by the kernels (kept for the host's bookkeeping)
+  long long onchip_smem;  // on-chip launches: dynamic shared memory per CTA, the
+                          // largest id_onchip_smem_bytes over the launch's tasks
 };
+// Shared memory of one on-chip CTA for an m x n box in a G-CTA cluster (the
+// layout is per task, so boxes of different sizes share a launch).
+size_t id_onchip_smem_bytes(int m, int n, int G);
 
 // launch_id group codes: G (1, 2, 4, 8) streams the matrix through HBM/L2
 // with G CTAs per box; kOnChip + G (G = 1 .. 16) keeps it in the shared
@@ -223,6 +228,10 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
                                 const double* targets, const double* mu, int nh,
                                 const double* holes, const double* alpha, double* out,
                                 cudaStream_t s);
+// Hole border of a multiply-connected domain: U (dofs x nb), Psi (nb x
+// dofs) and PsiT = Psi^T (initialize_U_mat / initialize_Psi_mat).
+cudaError_t launch_border_fill(int pde, const Node* nodes, int np, const double* holes, int nh,
+                               double* U, double* Psi, double* PsiT, cudaStream_t s);
 // Dense kernel block K(tgt, src), column-major nt x ns.
 cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
                                 const int* src, int ns, double* out, cudaStream_t s);

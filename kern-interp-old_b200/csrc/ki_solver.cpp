@@ -13,6 +13,8 @@
 // multiply_connected_solve (skel_factorization.cpp:341-551) on the GPU.
 #include "ki_solver.h"
 
+#include "ki_pool.h"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -122,70 +124,6 @@ double g_upload_ms = 0;  // accumulated by upload() (single host thread per solv
 double now_ms() {
   return std::chrono::duration<double, std::milli>(
              std::chrono::steady_clock::now().time_since_epoch()).count();
-}
-
-
-
-// initialize_U_mat (linear_solve.cpp:18-64) for boundary points.
-void border_U(int pde, const std::vector<double>& pts, const std::vector<double>& holes,
-              std::vector<double>* U, int* cols) {
-  const int nh = static_cast<int>(holes.size() / 4);
-  const int np = static_cast<int>(pts.size() / 2);
-  if (pde == kLaplace) {
-    *cols = nh;
-    U->assign(static_cast<size_t>(np) * nh, 0.0);
-    for (int i = 0; i < np; i++)
-      for (int h = 0; h < nh; h++) {
-        const double rx = pts[2 * i] - holes[4 * h], ry = pts[2 * i + 1] - holes[4 * h + 1];
-        (*U)[i + static_cast<size_t>(np) * h] = std::log(std::sqrt(rx * rx + ry * ry));
-      }
-    return;
-  }
-  *cols = 3 * nh;
-  const int N = 2 * np;
-  U->assign(static_cast<size_t>(N) * 3 * nh, 0.0);
-  auto at = [&](int i, int j) -> double& { return (*U)[i + static_cast<size_t>(N) * j]; };
-  for (int q = 0; q < np; q++)
-    for (int h = 0; h < nh; h++) {
-      const int i = 2 * q;
-      const double r0 = pts[i] - holes[4 * h], r1 = pts[i + 1] - holes[4 * h + 1];
-      const double rn = std::sqrt(r0 * r0 + r1 * r1);
-      const double scale = 1.0 / (4 * M_PI);
-      at(i, 3 * h) = scale * (std::log(1 / rn) + (1.0 / std::pow(rn, 2)) * r0 * r0);
-      at(i + 1, 3 * h) = scale * ((1.0 / std::pow(rn, 2)) * r1 * r0);
-      at(i, 3 * h + 1) = scale * ((1.0 / std::pow(rn, 2)) * r0 * r1);
-      at(i + 1, 3 * h + 1) = scale * (std::log(1 / rn) + (1.0 / std::pow(rn, 2)) * r1 * r1);
-      at(i, 3 * h + 2) = r1 * (scale / std::pow(rn, 2));
-      at(i + 1, 3 * h + 2) = -r0 * (scale / std::pow(rn, 2));
-    }
-}
-
-// initialize_Psi_mat (linear_solve.cpp:67-110), stored column-major rows x N.
-void border_Psi(int pde, const std::vector<double>& pts, const std::vector<double>& w,
-                const std::vector<double>& holes, std::vector<double>* Psi) {
-  const int nh = static_cast<int>(holes.size() / 4);
-  const int np = static_cast<int>(pts.size() / 2);
-  const int rows = pde == kLaplace ? nh : 3 * nh;
-  const int N = pde == kLaplace ? np : 2 * np;
-  Psi->assign(static_cast<size_t>(rows) * N, 0.0);
-  auto at = [&](int i, int j) -> double& { return (*Psi)[i + static_cast<size_t>(rows) * j]; };
-  for (int q = 0; q < np; q++) {
-    const double x0 = pts[2 * q], x1 = pts[2 * q + 1];
-    for (int h = 0; h < nh; h++) {
-      const double rx = x0 - holes[4 * h], ry = x1 - holes[4 * h + 1];
-      if (std::sqrt(rx * rx + ry * ry) < holes[4 * h + 2] + 1e-8) {
-        if (pde == kLaplace) {
-          at(h, q) = w[q];
-        } else {
-          at(3 * h, 2 * q) = w[q];
-          at(3 * h + 1, 2 * q + 1) = w[q];
-          at(3 * h + 2, 2 * q) = w[q] * x1;
-          at(3 * h + 2, 2 * q + 1) = -w[q] * x0;
-        }
-        break;
-      }
-    }
-  }
 }
 
 // Streaming launches: CTAs per box by matrix size.
@@ -410,17 +348,14 @@ int Solver::factor() {
   }
   nb_ = 0;
   if (!holes_.empty() && opt_.pde != kLaplaceNeumann) {
-    std::vector<double> U, Psi;
-    border_U(opt_.pde, pts_, holes_, &U, &nb_);
-    border_Psi(opt_.pde, pts_, wts_, holes_, &Psi);
-    const size_t rows = Psi.size() / n_dofs_;
-    h_PsiT_.assign(Psi.size(), 0.0);
-    for (int j = 0; j < n_dofs_; j++)
-      for (size_t i = 0; i < rows; i++) h_PsiT_[j + static_cast<size_t>(n_dofs_) * i] = Psi[i + rows * j];
-    KI_ALLOC(d_U_, double, U.size());
-    KI_ALLOC(d_Psi_, double, Psi.size());
-    KI_UPLOAD(d_U_, U, stream_);
-    KI_UPLOAD(d_Psi_, Psi, stream_);
+    const int nh = static_cast<int>(holes_.size() / 4);
+    nb_ = opt_.pde == kStokes ? 3 * nh : nh;
+    const size_t cnt = static_cast<size_t>(n_dofs_) * nb_;
+    KI_ALLOC(d_U_, double, cnt);
+    KI_ALLOC(d_Psi_, double, cnt);
+    KI_ALLOC(d_PsiT_, double, cnt);
+    KI_CUDA(launch_border_fill(opt_.pde, d_nodes_, n_points_, d_holes_, nh, d_U_, d_Psi_, d_PsiT_,
+                               stream_));
   }
 
   const int L = static_cast<int>(tree.levels.size());
@@ -467,52 +402,69 @@ int Solver::factor() {
 
 int Solver::process_level(int level) {
   const double h0 = now_ms();
-  std::vector<std::vector<int>> near(tree.boxes.size());
-  tree.refresh_level(level, &near);
   const std::vector<int>& ids = tree.levels[level];
+  const int nids = static_cast<int>(ids.size());
+  // active lists of the level (quadtree.cpp:694-720), independent per box
+  parallel_for(nids, 32, [&](int a, int e) {
+    for (int q = a; q < e; q++)
+      if (!tree.boxes[ids[q]].compressed) tree.refresh_box(ids[q]);
+  });
   const int P = sd_ == 2 ? 4 * kNumProxy : 2 * kNumProxy;
 
   struct Cand {
-    int box, n, m, I, g;
+    int box = -1, n = 0, m = 0, I = 0, g = 0;
     std::vector<int> rows;
   };
-  std::vector<Cand> cand;
-  for (int id : ids) {
-    const Box& b = tree.boxes[id];
-    if (b.compressed || static_cast<int>(b.active.size()) < opt_.min_dofs_to_compress) continue;
-    Cand c;
-    c.box = id;
-    c.n = static_cast<int>(b.active.size());
-    if (level == 1 || level == 2) {
-      // kernel.cpp:164-207: every other active dof of the level (and the
-      // level-1 leaves for level 2), both directions, no proxy circle.
-      // (a forest restricts both to the box's own tree)
-      for (int o : tree.levels[level])
-        if (o != id && tree.boxes[o].tree == b.tree)
-          c.rows.insert(c.rows.end(), tree.boxes[o].active.begin(), tree.boxes[o].active.end());
-      if (level == 2)
-        for (int o : tree.levels[1])
-          if (tree.boxes[o].leaf && tree.boxes[o].tree == b.tree)
-            c.rows.insert(c.rows.end(), tree.boxes[o].original.begin(),
-                          tree.boxes[o].original.end());
-      c.I = static_cast<int>(c.rows.size());
-      c.m = 2 * c.I;
-    } else {
-      // near dofs inside the proxy circle (kernel.cpp:209-218)
-      const double cx = b.corner[0] + b.side / 2.0, cy = b.corner[1] + b.side / 2.0;
-      for (int dof : near[id]) {
-        const int pt = dof / sd_;
-        const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
-        const double dist = std::sqrt(std::pow(cx - x, 2) + std::pow(cy - y, 2));
-        if (dist < kRadiusRatio * b.side) c.rows.push_back(dof);
+  std::vector<Cand> all(nids);
+  std::vector<char> keep(nids, 0);
+  parallel_for(nids, 8, [&](int a, int e) {
+    for (int q = a; q < e; q++) {
+      const int id = ids[q];
+      const Box& b = tree.boxes[id];
+      if (b.compressed || static_cast<int>(b.active.size()) < opt_.min_dofs_to_compress) continue;
+      Cand& c = all[q];
+      c.box = id;
+      c.n = static_cast<int>(b.active.size());
+      if (level == 1 || level == 2) {
+        // kernel.cpp:164-207: every other active dof of the level (and the
+        // level-1 leaves for level 2), both directions, no proxy circle.
+        // (a forest restricts both to the box's own tree)
+        for (int o : tree.levels[level])
+          if (o != id && tree.boxes[o].tree == b.tree)
+            c.rows.insert(c.rows.end(), tree.boxes[o].active.begin(), tree.boxes[o].active.end());
+        if (level == 2)
+          for (int o : tree.levels[1])
+            if (tree.boxes[o].leaf && tree.boxes[o].tree == b.tree)
+              c.rows.insert(c.rows.end(), tree.boxes[o].original.begin(),
+                            tree.boxes[o].original.end());
+        c.I = static_cast<int>(c.rows.size());
+        c.m = 2 * c.I;
+      } else {
+        // the near dofs (neighbours at this level or coarser: leaves give
+        // their original dofs, others their active ones, quadtree.cpp:
+        // 664-691) that lie inside the proxy circle (kernel.cpp:209-218)
+        const double cx = b.corner[0] + b.side / 2.0, cy = b.corner[1] + b.side / 2.0;
+        for (int o : b.nbr) {
+          const Box& ob = tree.boxes[o];
+          if (ob.level > b.level) continue;
+          for (int dof : ob.leaf ? ob.original : ob.active) {
+            const int pt = dof / sd_;
+            const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
+            const double dist = std::sqrt(std::pow(cx - x, 2) + std::pow(cy - y, 2));
+            if (dist < kRadiusRatio * b.side) c.rows.push_back(dof);
+          }
+        }
+        c.I = static_cast<int>(c.rows.size());
+        c.m = 2 * c.I + P;
       }
-      c.I = static_cast<int>(c.rows.size());
-      c.m = 2 * c.I + P;
+      if (c.m == 0) continue;
+      c.g = pick_group(c.m, c.n, onchip_ok_);
+      keep[q] = 1;
     }
-    if (c.m == 0) continue;
-    c.g = pick_group(c.m, c.n, onchip_ok_);
-    cand.push_back(std::move(c));
-  }
+  });
+  std::vector<Cand> cand;
+  for (int q = 0; q < nids; q++)
+    if (keep[q]) cand.push_back(std::move(all[q]));
   LevelFactors& lf = levels_[level];
   lf.level = level;
   if (cand.empty()) return 0;
@@ -569,21 +521,22 @@ int Solver::process_level(int level) {
   for (int q0 = 0; q0 < nc;) {
     int q1 = q0;
     int m_cap = 0, n_cap = 0;
-    long long col_cap = 0;
+    long long onchip = 0;
     const int g0 = cand[q0].g;
     const int G = g0 >= kOnChip ? g0 - kOnChip : 0;
     while (q1 < nc && cand[q1].g == g0) {
       const int mm = std::max(m_cap, cand[q1].m), nn = std::max(n_cap, cand[q1].n);
-      long long cc = col_cap;
-      if (G) cc = std::max(cc, static_cast<long long>((cand[q1].n + G - 1) / G) *
-                                   onchip_lda(cand[q1].m));
-      if (q1 > q0 && id_smem_bytes(mm, nn) + sizeof(double) * cc > 227 * 1024) break;
+      if (G) {
+        // per-task layout: the launch needs the largest single task's share
+        onchip = std::max<long long>(onchip, id_onchip_smem_bytes(cand[q1].m, cand[q1].n, G));
+      } else if (q1 > q0 && id_smem_bytes(mm, nn) > 227 * 1024) {
+        break;
+      }
       m_cap = mm;
       n_cap = nn;
-      col_cap = cc;
       q1++;
     }
-    if (id_smem_bytes(m_cap, n_cap) + sizeof(double) * col_cap > 227 * 1024)
+    if ((G ? static_cast<size_t>(onchip) : id_smem_bytes(m_cap, n_cap)) > 227 * 1024)
       return fail("interpolative decomposition too tall for shared staging (m = " +
                   std::to_string(m_cap) + ")");
     IdParams p{};
@@ -601,7 +554,7 @@ int Solver::process_level(int level) {
     p.tol = opt_.id_tol;
     p.m_cap = m_cap;
     p.n_cap = n_cap;
-    p.col_cap = col_cap;
+    p.onchip_smem = onchip;
     cudaEvent_t e0 = nullptr;
     if (time_phases && timer_begin(&e0)) return -2;
     KI_CUDA(launch_id(p, cand[q0].g, stream_));
@@ -965,7 +918,8 @@ int Solver::factor_border() {
   KI_ALLOC(modU, double, static_cast<size_t>(N) * nb);
   KI_ALLOC(modP, double, static_cast<size_t>(N) * nb);
   KI_CUDA(cudaMemcpyAsync(modU, d_U_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice, stream_));
-  KI_UPLOAD(modP, h_PsiT_, stream_);
+  KI_CUDA(cudaMemcpyAsync(modP, d_PsiT_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
+                          stream_));
   const int L = static_cast<int>(levels_.size());
   cudaEvent_t b0 = nullptr;
   if (time_phases && timer_begin(&b0)) return -2;

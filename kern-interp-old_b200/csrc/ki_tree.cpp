@@ -3,6 +3,8 @@
 // array instead of pointer-linked nodes.
 #include "ki_tree.h"
 
+#include "ki_pool.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -62,17 +64,43 @@ void QuadTreeHost::subdivide(int id) {
 
 void QuadTreeHost::insert(int id, double x, double y, int pt) {
   // quadtree.cpp:164-197: the point's dofs join every box on its path; the
-  // leaf it reaches splits once it holds more than max_leaf dofs.
+  // leaf it reaches splits once it holds more than max_leaf dofs.  Here
+  // only the leaf's list grows; the lists of boxes that were already split
+  // are completed once at the end (fill_internal_lists), which gives the
+  // same lists because points arrive in index order.
   for (;;) {
     Box& b = boxes[id];
-    for (int s = 0; s < sol_dim_; s++) b.original.push_back(sol_dim_ * pt + s);
     const int ch = b.child[pick_child(b, x, y)];
     if (ch >= 0) {
       id = ch;
       continue;
     }
+    for (int s = 0; s < sol_dim_; s++) b.original.push_back(sol_dim_ * pt + s);
     if (b.leaf && static_cast<int>(b.original.size()) > max_leaf_) subdivide(id);
     return;
+  }
+}
+
+void QuadTreeHost::fill_internal_lists() {
+  // Every internal box holds the dofs of all points in it in insertion
+  // (= index) order: the merge of its children's sorted lists, built from
+  // the deepest level up.
+  std::vector<int> tmp;
+  for (int l = static_cast<int>(levels.size()) - 1; l >= 0; l--) {
+    for (int id : levels[l]) {
+      Box& b = boxes[id];
+      if (b.leaf) continue;
+      const std::vector<int>& c0 = boxes[b.child[0]].original;
+      const std::vector<int>& c1 = boxes[b.child[1]].original;
+      const std::vector<int>& c2 = boxes[b.child[2]].original;
+      const std::vector<int>& c3 = boxes[b.child[3]].original;
+      tmp.resize(c0.size() + c1.size());
+      std::merge(c0.begin(), c0.end(), c1.begin(), c1.end(), tmp.begin());
+      std::vector<int> t2(c2.size() + c3.size());
+      std::merge(c2.begin(), c2.end(), c3.begin(), c3.end(), t2.begin());
+      b.original.resize(tmp.size() + t2.size());
+      std::merge(tmp.begin(), tmp.end(), t2.begin(), t2.end(), b.original.begin());
+    }
   }
 }
 
@@ -134,43 +162,88 @@ void QuadTreeHost::build(const double* points, int n, int sol_dim,
   build_forest(points, n, sol_dim, max_leaf_dofs, {0, n});
 }
 
-void QuadTreeHost::build_forest(const double* points, int n, int sol_dim, int max_leaf_dofs,
-                                const std::vector<int>& starts) {
-  // quadtree.cpp:72-114 per tree: root square [min - 0.01, max + 0.01]^2
-  // over all of the tree's coordinates, its points inserted in order.
-  pts_.assign(points, points + 2 * static_cast<size_t>(n));
-  sol_dim_ = sol_dim;
-  max_leaf_ = max_leaf_dofs;
+void QuadTreeHost::build_one(int p0, int p1, int tree_id) {
+  // quadtree.cpp:72-114: root square [min - 0.01, max + 0.01]^2 over all
+  // of the tree's coordinates, its points inserted in order, then the
+  // neighbour lists.
+  double lo_v = pts_[2 * static_cast<size_t>(p0)], hi_v = lo_v;
+  for (size_t i = 2 * static_cast<size_t>(p0); i < 2 * static_cast<size_t>(p1); i++) {
+    if (pts_[i] < lo_v) lo_v = pts_[i];
+    if (pts_[i] > hi_v) hi_v = pts_[i];
+  }
+  min_ = lo_v;
+  max_ = hi_v;
+  const double lo = lo_v - 0.01, hi = hi_v + 0.01;
   boxes.clear();
   levels.clear();
-  roots.clear();
-  boxes.reserve(8 * (static_cast<size_t>(n) * sol_dim / std::max(1, max_leaf_dofs)) +
-                64 * starts.size());
-  levels.emplace_back();
-  for (size_t p = 0; p + 1 < starts.size(); p++) {
-    const int p0 = starts[p], p1 = starts[p + 1];
-    double lo_v = pts_[2 * static_cast<size_t>(p0)], hi_v = lo_v;
-    for (size_t i = 2 * static_cast<size_t>(p0); i < 2 * static_cast<size_t>(p1); i++) {
-      if (pts_[i] < lo_v) lo_v = pts_[i];
-      if (pts_[i] > hi_v) hi_v = pts_[i];
-    }
-    if (p == 0) {
-      min_ = lo_v;
-      max_ = hi_v;
-    }
-    const double lo = lo_v - 0.01, hi = hi_v + 0.01;
-    Box root;
-    root.tree = static_cast<int>(p);
-    const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
-    std::memcpy(root.corner, c, sizeof(c));
-    root.side = hi - lo;
-    const int id = static_cast<int>(boxes.size());
-    boxes.push_back(root);
-    levels[0].push_back(id);
-    roots.push_back(id);
-    for (int q = p0; q < p1; q++) insert(id, pts_[2 * q], pts_[2 * q + 1], q);
-  }
+  boxes.reserve(4 * (static_cast<size_t>(p1 - p0) * sol_dim_ / std::max(1, max_leaf_)) + 16);
+  Box root;
+  root.tree = tree_id;
+  const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
+  std::memcpy(root.corner, c, sizeof(c));
+  root.side = hi - lo;
+  boxes.push_back(root);
+  levels.push_back({0});
+  for (int q = p0; q < p1; q++) insert(0, pts_[2 * q], pts_[2 * q + 1], q);
+  fill_internal_lists();
   neighbor_lists();
+}
+
+void QuadTreeHost::build_forest(const double* points, int n, int sol_dim, int max_leaf_dofs,
+                                const std::vector<int>& starts) {
+  pts_ = points;
+  sol_dim_ = sol_dim;
+  max_leaf_ = max_leaf_dofs;
+  const int P = static_cast<int>(starts.size()) - 1;
+  roots.clear();
+  if (P == 1) {
+    build_one(starts[0], starts[1], 0);
+    roots.push_back(0);
+    pts_ = nullptr;
+    return;
+  }
+  // trees are independent: build them in parallel, then lay them end to
+  // end (tree p's boxes after tree p - 1's, level lists concatenated in
+  // tree order), shifting box ids
+  std::vector<QuadTreeHost> part(P);
+  parallel_for(P, 1, [&](int a, int e) {
+    for (int p = a; p < e; p++) {
+      part[p].pts_ = points;
+      part[p].sol_dim_ = sol_dim;
+      part[p].max_leaf_ = max_leaf_dofs;
+      part[p].build_one(starts[p], starts[p + 1], p);
+    }
+  }, 2);
+  std::vector<int> off(P + 1, 0);
+  size_t depth = 0;
+  for (int p = 0; p < P; p++) {
+    off[p + 1] = off[p] + static_cast<int>(part[p].boxes.size());
+    depth = std::max(depth, part[p].levels.size());
+  }
+  boxes.clear();
+  boxes.resize(off[P]);
+  levels.assign(depth, {});
+  parallel_for(P, 1, [&](int a, int e) {
+    for (int p = a; p < e; p++) {
+      const int o = off[p];
+      for (size_t i = 0; i < part[p].boxes.size(); i++) {
+        Box& b = boxes[o + i];
+        b = std::move(part[p].boxes[i]);
+        if (b.parent >= 0) b.parent += o;
+        for (int& c : b.child)
+          if (c >= 0) c += o;
+        for (int& x : b.nbr) x += o;
+      }
+    }
+  }, 2);
+  for (size_t l = 0; l < depth; l++)
+    for (int p = 0; p < P; p++)
+      if (l < part[p].levels.size())
+        for (int id : part[p].levels[l]) levels[l].push_back(id + off[p]);
+  for (int p = 0; p < P; p++) roots.push_back(off[p]);
+  min_ = part[0].min_;
+  max_ = part[0].max_;
+  pts_ = nullptr;
 }
 
 void QuadTreeHost::refresh_box(int id) {

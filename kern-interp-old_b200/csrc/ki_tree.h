@@ -46,7 +46,7 @@ class QuadTreeHost {
   int sol_dim() const { return sol_dim_; }
   double min() const { return min_; }
   double max() const { return max_; }
-  const std::vector<double>& points() const { return pts_; }
+  const double* points() const { return pts_; }
 
   std::vector<Box> boxes;
   std::vector<std::vector<int>> levels;
@@ -60,13 +60,15 @@ class QuadTreeHost {
   int pick_child(const Box& b, double x, double y) const;
   void subdivide(int b);
   void insert(int b, double x, double y, int pt);
+  void fill_internal_lists();
   void descendant_neighbors(int big, int small);
   void neighbor_lists();
 
   int sol_dim_ = 1;
   int max_leaf_ = 32;
   double min_ = 0, max_ = 0;
-  std::vector<double> pts_;
+  const double* pts_ = nullptr;  // caller's points, valid during the build
+  void build_one(int p0, int p1, int tree_id);  // one tree into boxes/levels
 };
 
 }  // namespace kib
