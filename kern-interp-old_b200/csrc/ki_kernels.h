@@ -283,6 +283,8 @@ cudaError_t launch_scale_copy(double* dst, const double* src, int n, double a, c
 // out[p] = squared norm of segment p of v (dofs seg[p] sd .. seg[p + 1] sd)
 cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int sd, double* out,
                                  cudaStream_t s);
+// x += y
+cudaError_t launch_add(double* x, const double* y, int n, cudaStream_t s);
 // r = b - ax
 cudaError_t launch_sub(double* r, const double* b, const double* ax, int n, cudaStream_t s);
 

@@ -25,6 +25,22 @@ namespace {
 
 constexpr int kMvThreads = 256;
 
+// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
+// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
+// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
+// relative error, so the result is accurate to FP64 rounding.  x = 0 or
+// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
+// only pass far-away padding (whose numerators are zero) beyond it.
+__device__ __forceinline__ double nr_rcp(double x) {
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
+  double y = static_cast<double>(yf);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
 // Per-source values staged in shared memory.
 //   Laplace:          a = -(w / 2 pi) x (n_x, n_y)
 //   Laplace-Neumann:  a = (w / 2 pi) x (1, 1)      (target normal applied later)
@@ -76,9 +92,10 @@ __global__ void __launch_bounds__(kMvThreads)
         if (tile.first) r1 += s.w * (s.nx * d0 + s.ny * d1);
       }
     } else {
-      // padding: a source far away with zero strength
-      sx[threadIdx.x] = 1e30;
-      sy[threadIdx.x] = 1e30;
+      // padding: a source far away with zero strength (|r|^2 stays within
+      // the FP32 range of the reciprocal estimate; its numerators are zero)
+      sx[threadIdx.x] = 1e15;
+      sy[threadIdx.x] = 1e15;
       sa0[threadIdx.x] = 0.0;
       sa1[threadIdx.x] = 0.0;
       sd0[threadIdx.x] = 0.0;
@@ -89,16 +106,15 @@ __global__ void __launch_bounds__(kMvThreads)
     for (int q = 0; q < kMvThreads; q++) {
       const double r0 = tx - sx[q], rr1 = ty - sy[q];
       const double rr = r0 * r0 + rr1 * rr1;
+      const double inv = rr > 0.0 ? nr_rcp(rr) : 0.0;
       if (PDE == kLaplace) {
-        const double num = r0 * sa0[q] + rr1 * sa1[q];
-        y0 += rr > 0.0 ? num / rr : 0.0;
+        y0 += (r0 * sa0[q] + rr1 * sa1[q]) * inv;
       } else if (PDE == kLaplaceNeumann) {
-        const double num = (r0 * tnx + rr1 * tny) * sa0[q];
-        y0 += rr > 0.0 ? num / rr : 0.0;
+        y0 += ((r0 * tnx + rr1 * tny) * sa0[q]) * inv;
       } else {
         const double rn = r0 * sa0[q] + rr1 * sa1[q];
         const double rx = r0 * sd0[q] + rr1 * sd1[q];
-        const double pq = rr > 0.0 ? (rn * rx) / (rr * rr) : 0.0;
+        const double pq = (rn * rx) * (inv * inv);
         y0 += pq * r0;
         y1 += pq * rr1;
       }
@@ -243,6 +259,11 @@ __global__ void scale_copy_kernel(double* __restrict__ dst, const double* __rest
   if (i < n) dst[i] = a * src[i];
 }
 
+__global__ void add_kernel(double* __restrict__ x, const double* __restrict__ y, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += y[i];
+}
+
 __global__ void sub_kernel(double* __restrict__ r, const double* __restrict__ b,
                            const double* __restrict__ ax, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -351,6 +372,12 @@ cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int 
                                  cudaStream_t s) {
   count_launches(1);
   segment_sumsq_kernel<<<nseg, 256, 0, s>>>(v, seg, sd, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add(double* x, const double* y, int n, cudaStream_t s) {
+  count_launches(1);
+  add_kernel<<<(n + 255) / 256, 256, 0, s>>>(x, y, n);
   return cudaGetLastError();
 }
 

@@ -1,12 +1,16 @@
-// FP64 refinement of a (possibly low-accuracy) factorization: right-
-// preconditioned GMRES on the bordered boundary operator
+// FP64 refinement of a (possibly low-accuracy) factorization on the
+// bordered boundary operator
 //
 //     [ A  U ] [mu   ]   [f]
 //     [Psi -I] [alpha] = [0]        (kern_interp_test.cpp:54-78 form; no
 //                                    border when the domain has no holes)
 //
 // with the factorization's solve as the preconditioner M^-1 and the
-// operator applied by the fast on-the-fly FP64 product.  The preconditioned
+// operator applied by the fast on-the-fly FP64 product.  Stationary
+// refinement X += M^-1 (B - A X) runs first (the usual case: each step gains
+// the factorization's accuracy); if it stalls, right-preconditioned GMRES
+// continues from the current iterate.  The preconditioner application is a
+// CUDA graph of the whole solve, captured once.  In GMRES the preconditioned
 // directions Z_j = M^-1 V_j are kept (flexible-GMRES storage), so the
 // correction is X += Z y without a further solve.  Orthogonalisation is
 // classical Gram-Schmidt applied twice; the Hessenberg least-squares problem
@@ -40,6 +44,41 @@ int Solver::mv_setup() {
   KI_ALLOC(d_seg_, int, seg_.size());
   KI_UPLOAD(d_mv_tiles_, tiles, stream_);
   KI_UPLOAD(d_seg_, seg_, stream_);
+  return 0;
+}
+
+int Solver::solve_graph(const double* d_b, double* d_mu, double* d_alpha, const double* d_g) {
+  const int N = n_dofs_, nb = nb_;
+  if (!solve_exec_) {
+    KI_ALLOC(g_x_, double, static_cast<size_t>(N) + 2 * nb);
+    double* ga = g_x_ + N;
+    double* gg = ga + nb;
+    cudaGraph_t graph = nullptr;
+    KI_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
+    const int rc = solve_device(g_x_, g_x_, nb ? ga : nullptr, nb ? gg : nullptr);
+    const cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    KI_CUDA(e);
+    const cudaError_t ei = cudaGraphInstantiate(&solve_exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    KI_CUDA(ei);
+  }
+  KI_CUDA(cudaMemcpyAsync(g_x_, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  if (nb) {
+    if (d_g)
+      KI_CUDA(cudaMemcpyAsync(g_x_ + N + nb, d_g, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
+                              stream_));
+    else
+      KI_CUDA(cudaMemsetAsync(g_x_ + N + nb, 0, sizeof(double) * nb, stream_));
+  }
+  KI_CUDA(cudaGraphLaunch(solve_exec_, stream_));
+  KI_CUDA(cudaMemcpyAsync(d_mu, g_x_, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  if (nb && d_alpha)
+    KI_CUDA(cudaMemcpyAsync(d_alpha, g_x_ + N, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
+                            stream_));
   return 0;
 }
 
@@ -132,28 +171,55 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
     if (rel_res_out) *rel_res_out = 0.0;
     return 0;
   }
-  bool first = true;
-  for (;;) {
-    // r = B - A X (the first cycle starts from X = 0, r = B)
-    double beta = bnorm;
-    if (first) {
-      KI_CUDA(cudaMemcpyAsync(V, B, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream_));
-    } else {
-      if (matvec_device(X, W)) return -2;
-      KI_CUDA(launch_sub(V, B, W, n, stream_));
-      if (norm2(V, &beta)) return -2;
-    }
-    rel = beta / bnorm;
-    if (nseg > 1 && !first) {
+  // relative residual of r = V (per problem for a forest), and ||r||
+  auto residual = [&](double* beta, double* relr) -> int {
+    if (norm2(V, beta)) return -2;
+    *relr = *beta / bnorm;
+    if (nseg > 1) {
       std::vector<double> rs;
       if (seg_norms(V, &rs)) return -2;
       double worst = 0.0;
       for (int p = 0; p < nseg; p++)
         if (bseg[p] > 0.0) worst = std::max(worst, rs[p] / bseg[p]);
-      rel = worst;
+      *relr = worst;
     }
-    if ((nseg > 1 ? rel <= rel_tol : rel <= tol_eff) || iters >= max_iters || beta == 0.0) break;
-    first = false;
+    return 0;
+  };
+
+  // Stationary refinement first: X = M^-1 B, then X += M^-1 (B - A X) while
+  // each step shrinks the residual at least tenfold (one solve and one
+  // operator product per step, no inner products).  If it stalls, GMRES
+  // continues from the current X and residual.
+  double beta = 0.0;
+  bool done = false;
+  {
+    if (solve_graph(B, X, nb ? X + N : nullptr, nb ? B + N : nullptr)) return -2;
+    iters++;
+    double prev = 1.0;
+    for (;;) {
+      if (matvec_device(X, W)) return -2;
+      KI_CUDA(launch_sub(V, B, W, n, stream_));
+      if (residual(&beta, &rel)) return -2;
+      if (rel <= rel_tol || iters >= max_iters || beta == 0.0) {
+        done = true;
+        break;
+      }
+      if (rel > 0.1 * prev) break;
+      prev = rel;
+      if (solve_graph(V, W, nb ? W + N : nullptr, nb ? V + N : nullptr)) return -2;
+      KI_CUDA(launch_add(X, W, n, stream_));
+      iters++;
+    }
+  }
+  bool have_r = true;  // V holds B - A X with norm beta
+  for (; !done;) {
+    if (!have_r) {
+      if (matvec_device(X, W)) return -2;
+      KI_CUDA(launch_sub(V, B, W, n, stream_));
+      if (residual(&beta, &rel)) return -2;
+    }
+    have_r = false;
+    if (rel <= rel_tol || iters >= max_iters || beta == 0.0) break;
     KI_CUDA(launch_scale_copy(V, V, n, 1.0 / beta, stream_));
 
     // Arnoldi with Givens rotations; H column-major (m+1) x m on the host
@@ -163,7 +229,7 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
     for (; k < m && iters < max_iters; k++) {
       double* vk = V + k * ldv;
       double* zk = Z + k * ldv;
-      if (solve_device(vk, zk, nb ? zk + N : nullptr, nb ? vk + N : nullptr)) return -2;
+      if (solve_graph(vk, zk, nb ? zk + N : nullptr, nb ? vk + N : nullptr)) return -2;
       if (matvec_device(zk, W)) return -2;
       iters++;
       // two passes of classical Gram-Schmidt against V_0..V_k

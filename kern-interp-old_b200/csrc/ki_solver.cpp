@@ -187,6 +187,7 @@ Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
 Solver::~Solver() {
   // chunks go back to the pool only once no queued work can touch them
   cudaStreamSynchronize(stream_);
+  if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   if (dstream_) cudaStreamSynchronize(dstream_);
   if (ev_id_) cudaEventDestroy(ev_id_);
   if (ev_dec_) cudaEventDestroy(ev_dec_);

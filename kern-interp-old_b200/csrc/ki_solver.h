@@ -251,6 +251,12 @@ class Solver {
   Scratch kry_;
   Scratch adj_;  // adjoint contraction partials
   int mv_setup();  // tile table of the operator product (once)
+  // The solve as a CUDA graph on fixed buffers (captured at the first call,
+  // replayed for every preconditioner application of the refinement):
+  // copies in, one graph launch, copies out.
+  int solve_graph(const double* d_b, double* d_mu, double* d_alpha, const double* d_g);
+  cudaGraphExec_t solve_exec_ = nullptr;
+  double* g_x_ = nullptr;  // graph buffers: dofs, then border alpha, then border g
   MvTile* d_mv_tiles_ = nullptr;
   int n_mv_tiles_ = 0, mv_splits_ = 0;
   int* d_seg_ = nullptr;  // node offsets of the problems

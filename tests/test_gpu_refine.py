@@ -120,3 +120,17 @@ def test_refined_matches_dense_solve():
     mu_dense = np.linalg.solve(A, pr.f)
     mu, _, it, rr = s.solve_refined(pr.f, rel_tol=1e-13, max_iters=30)
     assert H.rel(mu, mu_dense) < 1e-12
+
+
+@pytest.mark.parametrize("tol", [1e-2, 1e-3])
+def test_refine_from_very_loose_factorization(tol):
+    """A factorization too loose for stationary refinement to converge fast
+    hands over to GMRES, which still reaches the FP64 residual."""
+    pr = G.star_case(n=4096)
+    s = kinterp.Solver(pr, id_tol=tol)
+    mu, _, it, rr = s.solve_refined(pr.f, rel_tol=1e-12, max_iters=60)
+    assert rr <= 1e-12, (it, rr)
+    o = K.PortSolver(pr, id_tol=1e-13, threads=8)
+    mt, _ = o.solve(pr.f)
+    o.close()
+    assert H.rel(mu, mt) < 1e-10
