@@ -10,9 +10,10 @@ reference's SkelFactorization::skeletonize + linear_solve,
 skel_factorization.cpp:94-403) to 1e-10 relative error.  The metric is
 unknowns / (factor + solve time), for two methods on the same GPU:
 
-  * mixed + refine (`value`): the factorization at ID tolerance 1e-6 used as
-    the preconditioner of FP64 GMRES on the operator with on-the-fly FP64
-    entries, stopped at true relative residual 1e-12 (ki_factor +
+  * mixed + refine (`value`): the factorization at ID tolerance 1e-6 in
+    preconditioner mode (tall ID matrices reduced by a sparse row sketch)
+    used by FP64 refinement / GMRES on the operator with on-the-fly FP64
+    entries, stopped at true relative residual 1e-12 (ki_factor_ex +
     ki_solve_refined_device);
   * FP64 (`fp64`): the reference method, factorization at ID tolerance
     1e-10 and one direct solve (ki_factor + ki_solve_device).
@@ -56,6 +57,7 @@ import ki_geometry as G  # noqa: E402
 
 METRIC = "factor+solve unknowns/s at 1e-10 rel err"
 MIXED_TOL = 1e-6      # ID tolerance of the preconditioning factorization
+MIXED_MODE = 1        # KI_MODE_PRECONDITIONER: sketched IDs for tall boxes
 REFINE_TOL = 1e-12    # true relative residual at which GMRES stops
 FP64_TOL = 1e-10
 
@@ -310,13 +312,13 @@ def main():
     nb = 0 if batch else (3 * pr0.holes.shape[0] if pr0.pde == G.STOKES else pr0.holes.shape[0])
     al_dev = torch.empty(max(nb, 1), device=dev, dtype=torch.float64)
 
-    def factor(tol, timed=False):
+    def factor(tol, timed=False, mode=0):
         if batch:
-            return kinterp.BatchSolver(probs, id_tol=tol, stream=sh)
-        return kinterp.Solver(pr0, id_tol=tol, stream=sh, timed=timed)
+            return kinterp.BatchSolver(probs, id_tol=tol, stream=sh, mode=mode)
+        return kinterp.Solver(pr0, id_tol=tol, stream=sh, timed=timed, mode=mode)
 
     def mixed_step(timed):
-        s = factor(MIXED_TOL, timed)
+        s = factor(MIXED_TOL, timed, MIXED_MODE)
         if batch:
             it, rr = s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
                                             rel_tol=REFINE_TOL, max_iters=20)
@@ -406,9 +408,9 @@ def main():
 
     def e2e_step():
         if batch:
-            s = kinterp.BatchSolver(pp, id_tol=MIXED_TOL, stream=sh)
+            s = kinterp.BatchSolver(pp, id_tol=MIXED_TOL, stream=sh, mode=MIXED_MODE)
         else:
-            s = kinterp.Solver(pp[0], id_tol=MIXED_TOL, stream=sh)
+            s = kinterp.Solver(pp[0], id_tol=MIXED_TOL, stream=sh, mode=MIXED_MODE)
         s.solve_refined(f_pin, rel_tol=REFINE_TOL, max_iters=20)
         s.close()
 
@@ -449,8 +451,9 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOADS[args.workload][1], "n_dofs": units,
-                       "method": "mixed+refine: factor at id_tol %g, FP64 GMRES with on-the-fly "
-                                 "FP64 operator to true rel. residual %g" % (MIXED_TOL, REFINE_TOL),
+                       "method": "mixed+refine: factor at id_tol %g in preconditioner mode "
+                                 "(sketched IDs), FP64 refinement/GMRES with on-the-fly FP64 "
+                                 "operator to true rel. residual %g" % (MIXED_TOL, REFINE_TOL),
                        "leaf_dofs": pr0.max_leaf_dofs,
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "flushed between steps (256 MiB device write)"},

@@ -35,6 +35,13 @@ enum {
 
 enum { KI_LAPLACE = 0, KI_LAPLACE_NEUMANN = 1, KI_STOKES = 2 };
 
+/* Factorization modes.  KI_MODE_REFERENCE: the reference's method exactly
+ * (same partition, ranks and skeletons).  KI_MODE_PRECONDITIONER: for a
+ * factorization used by ki_solve_refined: boxes whose ID matrix is much
+ * taller than wide are decomposed through a sparse random row sketch
+ * (cheaper, different skeletons, same accuracy class). */
+enum { KI_MODE_REFERENCE = 0, KI_MODE_PRECONDITIONER = 1 };
+
 /* Message of the last failing call on this thread ("" if none). */
 const char* ki_last_error(void);
 /* Library version, major * 10000 + minor * 100 + patch. */
@@ -190,6 +197,13 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
                     const double* holes, int max_leaf_dofs, double id_tol, void* stream,
                     ki_solver_t* out);
 
+/* ki_factor with a mode (KI_MODE_*) and phase timing (timed != 0, as
+ * ki_factor_timed). */
+int ki_factor_ex(int pde, int n_points, const double* points, const double* normals,
+                 const double* curvatures, const double* weights, int n_holes,
+                 const double* holes, int max_leaf_dofs, double id_tol, int mode, int timed,
+                 void* stream, ki_solver_t* out);
+
 /* Many independent problems factored together (no reference counterpart:
  * the reference factors one boundary per QuadTree).  Problem p has
  * n_points[p] nodes; the geometry arrays are the problems' arrays laid end
@@ -201,7 +215,7 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
  * (no holes); n_problems >= 1. */
 int ki_factor_batch(int pde, int n_problems, const int* n_points, const double* points,
                     const double* normals, const double* curvatures, const double* weights,
-                    int max_leaf_dofs, double id_tol, void* stream, ki_solver_t* out);
+                    int max_leaf_dofs, double id_tol, int mode, void* stream, ki_solver_t* out);
 /* The partition of a batch only (host; like ki_partition per problem). */
 int ki_partition_batch(int n_problems, const int* n_points, const double* points, int sol_dim,
                        int max_leaf_dofs, ki_solver_t* out);

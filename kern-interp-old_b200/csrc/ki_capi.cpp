@@ -81,7 +81,8 @@ bool box_ref(ki_solver_t s, int level, int idx, const kib::Box** out, int* paren
 int factor_impl(int pde, int n_points, const double* points, const double* normals,
                 const double* curvatures, const double* weights, int n_holes,
                 const double* holes, int max_leaf_dofs, double id_tol, void* stream,
-                ki_solver_t* out, bool timed, const std::vector<int>* starts = nullptr) {
+                ki_solver_t* out, bool timed, const std::vector<int>* starts = nullptr,
+                int mode = KI_MODE_REFERENCE) {
   if (!out) return set_err(KI_ERR_ARG, "ki_factor: out is NULL");
   *out = nullptr;
   if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_factor: bad pde");
@@ -90,6 +91,8 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
   if (n_holes < 0 || (n_holes > 0 && !holes)) return set_err(KI_ERR_ARG, "ki_factor: bad holes");
   if (max_leaf_dofs < 1) return set_err(KI_ERR_ARG, "ki_factor: max_leaf_dofs must be >= 1");
   if (!(id_tol > 0)) return set_err(KI_ERR_ARG, "id_tol must be greater than 0");
+  if (mode != KI_MODE_REFERENCE && mode != KI_MODE_PRECONDITIONER)
+    return set_err(KI_ERR_ARG, "ki_factor: bad mode");
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
     return set_err(KI_ERR_CUDA, "no CUDA device available");
@@ -106,6 +109,7 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
   opt.pde = pde;
   opt.max_leaf_dofs = max_leaf_dofs;
   opt.id_tol = id_tol;
+  opt.sketch_id = mode == KI_MODE_PRECONDITIONER;
   h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, n_holes,
                                   holes, h->stream));
   h->solver->time_phases = timed;
@@ -146,9 +150,17 @@ int ki_factor_timed(int pde, int n_points, const double* points, const double* n
                      max_leaf_dofs, id_tol, stream, out, true);
 }
 
+int ki_factor_ex(int pde, int n_points, const double* points, const double* normals,
+                 const double* curvatures, const double* weights, int n_holes,
+                 const double* holes, int max_leaf_dofs, double id_tol, int mode, int timed,
+                 void* stream, ki_solver_t* out) {
+  return factor_impl(pde, n_points, points, normals, curvatures, weights, n_holes, holes,
+                     max_leaf_dofs, id_tol, stream, out, timed != 0, nullptr, mode);
+}
+
 int ki_factor_batch(int pde, int n_problems, const int* n_points, const double* points,
                     const double* normals, const double* curvatures, const double* weights,
-                    int max_leaf_dofs, double id_tol, void* stream, ki_solver_t* out) {
+                    int max_leaf_dofs, double id_tol, int mode, void* stream, ki_solver_t* out) {
   if (!out) return set_err(KI_ERR_ARG, "ki_factor_batch: out is NULL");
   *out = nullptr;
   if (n_problems < 1 || !n_points) return set_err(KI_ERR_ARG, "ki_factor_batch: no problems");
@@ -162,7 +174,7 @@ int ki_factor_batch(int pde, int n_problems, const int* n_points, const double* 
     starts.push_back(static_cast<int>(total));
   }
   return factor_impl(pde, static_cast<int>(total), points, normals, curvatures, weights, 0,
-                     nullptr, max_leaf_dofs, id_tol, stream, out, false, &starts);
+                     nullptr, max_leaf_dofs, id_tol, stream, out, false, &starts, mode);
 }
 
 int ki_num_problems(ki_solver_t s) { return s && s->solver ? s->solver->n_trees() : -KI_ERR_ARG; }

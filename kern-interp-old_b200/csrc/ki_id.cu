@@ -47,6 +47,18 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// 32-bit integer hash (the "lowbias32" finalizer published by C. Wellons):
+// the sketch takes its row choice from the low bits and its sign from the
+// top bit.
+__device__ __forceinline__ unsigned sketch_hash(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
 // Block-wide sum; `red` holds kIdWarps doubles.  Ends with a barrier so
 // `red` may be reused immediately.
 __device__ double block_sum(double v, double* red) {
@@ -490,12 +502,16 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
   int g = 0;
   if constexpr (G > 1) g = static_cast<int>(cg::this_cluster().block_rank());
   const IdTask tk = P.tasks[task];
-  const int n = tk.n, m = tk.m, lda = tk.lda, I = tk.n_row;
+  // sketched box: the working matrix is the sk x n sketch S A
+  const bool sketch = tk.sk > 0;
+  const int n = tk.n, m = sketch ? tk.sk : tk.m, lda = tk.lda, I = tk.n_row;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   // layout of this task (every CTA of the cluster has the same task)
   double* cols = reinterpret_cast<double*>(smem_raw);   // owned columns
-  double* v = cols + static_cast<long long>((n + G - 1) / G) * lda;  // m
+  double* tile = cols + static_cast<long long>((n + G - 1) / G) * lda;  // sketch: rows of A
+  const int nloc = (n - g + G - 1) / G;  // columns j = g + G t owned by this CTA
+  double* v = tile + (sketch ? static_cast<long long>(kSketchTile + 1) * nloc : 0);  // m
   double* rdiag = v + m;                                 // n
   double* vn1 = rdiag + n;                               // n
   double* vn2 = vn1 + n;                                 // n
@@ -566,6 +582,48 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
     if (r < 2 * I) return boundary_entry(pde, nodes, cd, rowd[r - I]);
     return proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
   };
+  if (sketch) {
+    // Y = S A for this CTA's columns, accumulated kSketchTile rows of A at a
+    // time: the rows are generated into `tile`, then work item (column,
+    // block b) adds each row, signed, into its hashed row of block b; items
+    // own disjoint entries of Y and add the rows in order, so the result is
+    // deterministic.  Columns never mix, so the CTAs of a cluster need no
+    // exchange here.
+    const int mA = tk.m, blk = m / kSketchBlocks;
+    for (long long e = threadIdx.x; e < static_cast<long long>(lda) * nloc; e += kOcThreads)
+      cols[e] = 0.0;
+    for (int r0 = 0; r0 < mA; r0 += kSketchTile) {
+      const int rows = min(kSketchTile, mA - r0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < rows * nloc; e += kOcThreads) {
+        const int rr = e % rows, t = e / rows;
+        tile[rr + (kSketchTile + 1) * t] = entry_at(r0 + rr, act[g + G * t]);
+      }
+      __syncthreads();
+      for (int it = threadIdx.x; it < nloc * kSketchBlocks; it += kOcThreads) {
+        const int t = it % nloc, b = it / nloc;
+        double* ycol = cols + static_cast<long long>(lda) * t + b * blk;
+        const double* tcol = tile + (kSketchTile + 1) * t;
+        for (int rr = 0; rr < rows; rr++) {
+          const unsigned h = sketch_hash(static_cast<unsigned>(r0 + rr) * kSketchBlocks + b);
+          const double a = tcol[rr];
+          ycol[h % blk] += (h & 0x80000000u) ? -a : a;
+        }
+      }
+    }
+    __syncthreads();
+    for (int t = warp; t < nloc; t += kOcWarps) {
+      const double* col = cols + static_cast<long long>(lda) * t;
+      double ss = 0.0;
+      for (int r = lane; r < m; r += 32) ss += col[r] * col[r];
+      ss = warp_sum(ss);
+      if (lane == 0) {
+        const int j = g + G * t;
+        vn1[j] = sqrt(ss);
+        vn2[j] = vn1[j];
+      }
+    }
+  } else {
   for (int t = warp; g + G * t < n; t += kOcWarps) {
     const int j = g + G * t;
     const int cd = act[j];
@@ -593,6 +651,7 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
       vn1[j] = sqrt(ss);
       vn2[j] = vn1[j];
     }
+  }
   }
   for (int p = threadIdx.x; p < n; p += kOcThreads) pos2col[p] = p;
   __syncthreads();
@@ -837,6 +896,12 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 }
 
 }  // namespace
+
+size_t id_sketch_smem_bytes(int sk, int n, int G) {
+  const size_t nloc = static_cast<size_t>((n + G - 1) / G);
+  return id_smem_bytes(sk, n) +
+         sizeof(double) * (nloc * onchip_lda(sk) + static_cast<size_t>(kSketchTile + 1) * nloc);
+}
 
 size_t id_onchip_smem_bytes(int m, int n, int G) {
   return id_smem_bytes(m, n) +

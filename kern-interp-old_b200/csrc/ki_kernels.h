@@ -33,7 +33,17 @@ struct IdTask {
   long long a_off;  // A in the workspace (doubles)
   long long t_off;  // T output (doubles), capacity n*n/4 + 1
   double cx, cy, rad, pw;  // proxy circle centre, radius, weight
+  int sk;         // > 0: on-chip CTA factors the sk x n row sketch S A instead of A
+  int pad;
 };
+
+// Row sketch of an ID matrix (on-chip, one CTA): S has kSketchBlocks blocks
+// of sk / kSketchBlocks rows, and every row of A is added with a hashed sign
+// into one hashed row of each block (a sparse sign embedding).
+constexpr int kSketchBlocks = 8;
+constexpr int kSketchTile = 32;  // rows of A generated per pass
+// Sketch rows for an m x n matrix: n + 16 rounded up to the block count.
+inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlocks * kSketchBlocks; }
 
 struct IdParams {
   const IdTask* tasks;
@@ -56,6 +66,8 @@ struct IdParams {
 // Shared memory of one on-chip CTA for an m x n box in a G-CTA cluster (the
 // layout is per task, so boxes of different sizes share a launch).
 size_t id_onchip_smem_bytes(int m, int n, int G);
+// ... and for a sketched box (sk sketch rows) in a G-CTA cluster.
+size_t id_sketch_smem_bytes(int sk, int n, int G);
 
 // launch_id group codes: G (1, 2, 4, 8) streams the matrix through HBM/L2
 // with G CTAs per box; kOnChip + G (G = 1 .. 16) keeps it in the shared

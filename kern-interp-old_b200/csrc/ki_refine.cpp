@@ -18,6 +18,7 @@
 // iterative solver; its direct solve is the X_0 = M^-1 b first step here.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "ki_solver.h"
@@ -49,6 +50,13 @@ int Solver::mv_setup() {
 
 int Solver::solve_graph(const double* d_b, double* d_mu, double* d_alpha, const double* d_g) {
   const int N = n_dofs_, nb = nb_;
+  // KI_SOLVE_GRAPH=0 launches the same kernels one by one instead (for tools
+  // that cannot follow stream capture, e.g. kernel profilers)
+  static const bool use_graph = [] {
+    const char* e = std::getenv("KI_SOLVE_GRAPH");
+    return !(e && e[0] == '0');
+  }();
+  if (!use_graph) return solve_device(d_b, d_mu, d_alpha, d_g);
   if (!solve_exec_) {
     KI_ALLOC(g_x_, double, static_cast<size_t>(N) + 2 * nb);
     double* ga = g_x_ + N;

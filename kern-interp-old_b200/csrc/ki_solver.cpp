@@ -413,7 +413,7 @@ int Solver::process_level(int level) {
   const int P = sd_ == 2 ? 4 * kNumProxy : 2 * kNumProxy;
 
   struct Cand {
-    int box = -1, n = 0, m = 0, I = 0, g = 0;
+    int box = -1, n = 0, m = 0, I = 0, g = 0, sk = 0;
     std::vector<int> rows;
   };
   std::vector<Cand> all(nids);
@@ -460,6 +460,17 @@ int Solver::process_level(int level) {
       }
       if (c.m == 0) continue;
       c.g = pick_group(c.m, c.n, onchip_ok_);
+      if (opt_.sketch_id) {
+        // the smallest cluster whose shared memory holds the sketch
+        const int l = sketch_rows(c.n);
+        if (c.m > l + 64)
+          for (int G = 1; G <= 16; G *= 2)
+            if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= 227 * 1024) {
+              c.sk = l;
+              c.g = kOnChip + G;
+              break;
+            }
+      }
       keep[q] = 1;
     }
   });
@@ -486,7 +497,9 @@ int Solver::process_level(int level) {
     t.proxy = c.m - 2 * c.I;
     t.act_off = static_cast<int>(act.size());
     t.row_off = static_cast<int>(rows.size());
-    t.lda = c.g >= kOnChip ? onchip_lda(c.m) : (c.m + 3) & ~3;
+    t.lda = c.sk ? onchip_lda(c.sk) : c.g >= kOnChip ? onchip_lda(c.m) : (c.m + 3) & ~3;
+    t.sk = c.sk;
+    t.pad = 0;
     t.perm_off = perm_total;
     t.a_off = a_total;
     t.t_off = t_total;
@@ -529,7 +542,9 @@ int Solver::process_level(int level) {
       const int mm = std::max(m_cap, cand[q1].m), nn = std::max(n_cap, cand[q1].n);
       if (G) {
         // per-task layout: the launch needs the largest single task's share
-        onchip = std::max<long long>(onchip, id_onchip_smem_bytes(cand[q1].m, cand[q1].n, G));
+        onchip = std::max<long long>(
+            onchip, cand[q1].sk ? id_sketch_smem_bytes(cand[q1].sk, cand[q1].n, G)
+                                : id_onchip_smem_bytes(cand[q1].m, cand[q1].n, G));
       } else if (q1 > q0 && id_smem_bytes(mm, nn) > 227 * 1024) {
         break;
       }
@@ -589,13 +604,16 @@ int Solver::process_level(int level) {
     // trailing block) + the triangular solve for T; HBM bytes = the dof
     // lists and node records read, perm and T written, plus, for the
     // streamed launches, the working matrix written once and read once.
-    const double m = c.m, n = c.n;
-    const int steps = k > 0 ? k : std::min(c.m, c.n);
-    double qr = 20.0 * m * n + 1.0 * k * k * (n - k);
+    // (a sketched box: generation + kSketchBlocks signed adds per entry, the
+    // QR on the sk rows of the sketch)
+    const double n = c.n, m = c.sk ? c.sk : c.m;
+    const int steps = k > 0 ? k : std::min(static_cast<int>(m), c.n);
+    double qr = 20.0 * c.m * n + 1.0 * k * k * (n - k);
+    if (c.sk) qr += 1.0 * kSketchBlocks * c.m * n;
     for (int j = 0; j < steps; j++) qr += 4.0 * (m - j) * (n - j - 1) + 3.0 * (m - j);
     const double sd = sd_;  // dofs per node record
     double bytes = 4.0 * (c.I + 2 * n) + 64.0 * (c.I + c.n) / sd + 8.0 * k * (n - k);
-    if (c.g < kOnChip) bytes += 16.0 * m * n;
+    if (c.g < kOnChip) bytes += 16.0 * c.m * n;
     id_flops += qr;
     id_bytes += bytes;
     if (c.g >= kOnChip) id_onchip_flops += qr;

@@ -62,6 +62,11 @@ struct SolverOptions {
   int max_leaf_dofs = 32;   // MAX_LEAF_DOFS (quadtree.h:10)
   double id_tol = 1e-6;
   int min_dofs_to_compress = 16;  // MIN_DOFS_TO_COMPRESS (skel_factorization.h:11)
+  // Preconditioner mode: boxes whose ID matrix is much taller than wide are
+  // decomposed through a sparse row sketch (different skeletons from the
+  // reference, same accuracy class); for factorizations used with the
+  // refinement, never for reference-identical results.
+  bool sketch_id = false;
 };
 
 struct LevelFactors {

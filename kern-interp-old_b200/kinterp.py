@@ -51,7 +51,8 @@ def load():
     lib.ki_partition_batch.argtypes = [C.c_int, _ip, _dp, C.c_int, C.c_int,
                                        C.POINTER(C.c_void_p)]
     lib.ki_factor_batch.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp, C.c_int,
-                                    C.c_double, C.c_void_p, C.POINTER(C.c_void_p)]
+                                    C.c_double, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]
+    lib.ki_factor_ex.argtypes = fac_args[:10] + [C.c_int, C.c_int] + fac_args[10:]
     lib.ki_num_problems.argtypes = [C.c_void_p]
     lib.ki_box_tree.argtypes = [C.c_void_p, C.c_int, C.c_int]
     lib.ki_destroy.argtypes = [C.c_void_p]
@@ -159,7 +160,10 @@ class Partition(_Tree):
 class Solver(_Tree):
     """A factorization on the GPU (QuadTree + SkelFactorization)."""
 
-    def __init__(self, problem, id_tol=None, max_leaf_dofs=None, stream=None, timed=False):
+    def __init__(self, problem, id_tol=None, max_leaf_dofs=None, stream=None, timed=False,
+                 mode=0):
+        """mode 0 (KI_MODE_REFERENCE): the reference's factorization; mode 1
+        (KI_MODE_PRECONDITIONER): for use with solve_refined."""
         self.lib = load()
         pr = problem
         self.problem = pr
@@ -169,10 +173,11 @@ class Solver(_Tree):
         tol = pr.id_tol if id_tol is None else id_tol
         leaf = pr.max_leaf_dofs if max_leaf_dofs is None else max_leaf_dofs
         h = C.c_void_p()
-        fn = self.lib.ki_factor_timed if timed else self.lib.ki_factor
-        _check(fn(pr.pde, pr.n_points, _d(pts), _d(nrm), _d(kap), _d(w),
-                  pr.holes.shape[0], _d(holes) if holes.size else None, leaf, tol,
-                  C.c_void_p(stream) if stream else None, C.byref(h)), "ki_factor")
+        _check(self.lib.ki_factor_ex(pr.pde, pr.n_points, _d(pts), _d(nrm), _d(kap), _d(w),
+                                     pr.holes.shape[0], _d(holes) if holes.size else None, leaf,
+                                     tol, mode, 1 if timed else 0,
+                                     C.c_void_p(stream) if stream else None, C.byref(h)),
+               "ki_factor")
         self.h = h
         self.n_dofs = self.lib.ki_num_dofs(h)
         self.n_border = self.lib.ki_num_border(h)
@@ -323,7 +328,7 @@ class BatchSolver(_Tree):
     """Many independent problems factored together (ki_factor_batch): dofs
     of problem p follow those of problems 0..p-1."""
 
-    def __init__(self, problems, id_tol=None, max_leaf_dofs=None, stream=None):
+    def __init__(self, problems, id_tol=None, max_leaf_dofs=None, stream=None, mode=0):
         self.lib = load()
         pr0 = problems[0]
         self.problems = problems
@@ -333,7 +338,7 @@ class BatchSolver(_Tree):
         leaf = pr0.max_leaf_dofs if max_leaf_dofs is None else max_leaf_dofs
         h = C.c_void_p()
         _check(self.lib.ki_factor_batch(pr0.pde, len(problems), _i(self._n), _d(pts), _d(nrm),
-                                        _d(kap), _d(w), leaf, tol,
+                                        _d(kap), _d(w), leaf, tol, mode,
                                         C.c_void_p(stream) if stream else None, C.byref(h)),
                "ki_factor_batch")
         self.h = h

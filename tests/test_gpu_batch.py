@@ -49,9 +49,10 @@ def test_batch_matches_single_factorizations():
     bs.close()
 
 
-def test_batch_refined_mixed():
+@pytest.mark.parametrize("mode", [0, 1], ids=["reference_ids", "sketched_ids"])
+def test_batch_refined_mixed(mode):
     probs = G.random_star_cases(count=16, seed=22, nmin=512, nmax=8192)
-    bs = kinterp.BatchSolver(probs, id_tol=1e-6)
+    bs = kinterp.BatchSolver(probs, id_tol=1e-6, mode=mode)
     mu, it, rr = bs.solve_refined(rel_tol=1e-12, max_iters=20)
     assert rr <= 1e-12, (it, rr)
     parts = bs.split(mu)

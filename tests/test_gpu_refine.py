@@ -86,14 +86,15 @@ def test_preconditioner_border_rhs():
     assert np.linalg.norm(r) / np.linalg.norm(np.concatenate([f, g])) < 1e-8
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["reference_ids", "sketched_ids"])
 @pytest.mark.parametrize("name", list(_problems()))
-def test_refined_loose_factor_reaches_fp64(name):
+def test_refined_loose_factor_reaches_fp64(name, mode):
     """The FP64 oracle at id_tol 1e-10 carries its own ~1e-10 error (it is a
     1e-10 factorization); the converged reference here is the same oracle
     at id_tol 1e-13.  The refined GPU solution must be within 1e-10 of it,
     and no farther from the 1e-10 oracle than that oracle's own error allows."""
     pr = _problems()[name]
-    s = kinterp.Solver(pr, id_tol=1e-6)
+    s = kinterp.Solver(pr, id_tol=1e-6, mode=mode)
     mu, alpha, it, rr = s.solve_refined(pr.f, rel_tol=1e-12, max_iters=30)
     assert rr <= 1e-12, (it, rr)
     assert it <= 10
