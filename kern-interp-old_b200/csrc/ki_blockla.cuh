@@ -34,16 +34,18 @@ __device__ inline void cta_gemm_sub(double* C, int ldc, const double* C0, int ld
   }
 }
 
-// Tiled CTA GEMM: C (m x n) = C0 - op(A) op(B), op(A) m x kk, op(B) kk x n,
-// 64 x 64 output tiles with a 4 x 4 block per thread (256 threads), inner
-// dimension staged 16 at a time in `tile` (2 * 16 * 65 doubles).  C0 may be
-// null (taken as zero) or alias C.  Operands may live in shared or global
-// memory.  Ends with a barrier.
+// Tiled CTA GEMM: C (m x n) = C0 + alpha op(A) op(B) (alpha = -1 unless
+// given), op(A) m x kk, op(B) kk x n, 64 x 64 output tiles with a 4 x 4 block
+// per thread (256 threads), inner dimension staged 16 at a time in `tile`
+// (2 * 16 * 65 doubles).  C0 may be null (taken as zero) or alias C; C must
+// not alias A or B.  Operands may live in shared or global memory.  Ends
+// with a barrier.
 constexpr int kGemmTileDoubles = 2 * 16 * 65;
 
 __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int ldc0,
                                       const double* A, int lda, bool ta, const double* B,
-                                      int ldb, bool tb, int m, int n, int kk, double* tile) {
+                                      int ldb, bool tb, int m, int n, int kk, double* tile,
+                                      double alpha = -1.0) {
   double* sa = tile;            // [16][65]: sa[l * 65 + i] = op(A)(i0 + i, l0 + l)
   double* sb = tile + 16 * 65;  // [16][65]: sb[l * 65 + j] = op(B)(l0 + l, j0 + j)
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -106,7 +108,7 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
           const int gi = i0 + tx + 16 * a, gj = j0 + ty + 16 * b;
           if (gi < m && gj < n) {
             const double c0 = C0 ? C0[gi + static_cast<long long>(ldc0) * gj] : 0.0;
-            C[gi + static_cast<long long>(ldc) * gj] = c0 - acc[a][b];
+            C[gi + static_cast<long long>(ldc) * gj] = c0 + alpha * acc[a][b];
           }
         }
     }
@@ -185,6 +187,104 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
       a[i + static_cast<long long>(ld) * c] -=
           a[i + static_cast<long long>(ld) * j] * a[j + static_cast<long long>(ld) * c];
     }
+    __syncthreads();
+  }
+  return info;
+}
+
+// In-place inverse of the n x n matrix a (leading dimension ld) by
+// Gauss-Jordan elimination with partial pivoting over the CTA: at step j the
+// first-maximum |a(i, j)|, i >= j, is swapped into row j (ipiv[j] records
+// it), row j is scaled by the pivot's reciprocal and column j eliminated
+// from every other row; the row interchanges are undone as column
+// interchanges in reverse order at the end.  `col` needs n doubles, `red`
+// 64.  Returns nonzero if an exactly zero pivot was met.
+__device__ inline int cta_gj_invert(double* a, int n, int ld, int* ipiv, double* col,
+                                    double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  int* redi = reinterpret_cast<int*>(red + 32);
+  int info = 0;
+  for (int j = 0; j < n; j++) {
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+      const double v = fabs(a[i + static_cast<long long>(ld) * j]);
+      if (v > bv || (v == bv && i < bp)) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = red[0];
+      int p = redi[0];
+      for (int w = 1; w < nw; w++)
+        if (red[w] > v || (red[w] == v && redi[w] < p)) {
+          v = red[w];
+          p = redi[w];
+        }
+      ipiv[j] = p;
+      redi[31] = p;
+    }
+    __syncthreads();
+    const int p = redi[31];
+    if (p != j)
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        double* x = a + static_cast<long long>(ld) * c;
+        const double t = x[j];
+        x[j] = x[p];
+        x[p] = t;
+      }
+    __syncthreads();
+    const double piv = a[j + static_cast<long long>(ld) * j];
+    if (piv == 0.0) {
+      info = 1;
+      continue;
+    }
+    const double inv = 1.0 / piv;
+    // keep column j (the multipliers), scale row j
+    for (int i = threadIdx.x; i < n; i += blockDim.x) col[i] = a[i + static_cast<long long>(ld) * j];
+    __syncthreads();
+    for (int c = threadIdx.x; c < n; c += blockDim.x)
+      a[j + static_cast<long long>(ld) * c] = c == j ? inv : a[j + static_cast<long long>(ld) * c] * inv;
+    __syncthreads();
+    // eliminate column j from the other rows
+    for (long long e = threadIdx.x; e < static_cast<long long>(n) * n; e += blockDim.x) {
+      const int i = static_cast<int>(e % n), c = static_cast<int>(e / n);
+      if (i == j) continue;
+      const double f = col[i];
+      if (c == j)
+        a[i + static_cast<long long>(ld) * c] = -f * inv;
+      else if (f != 0.0)
+        a[i + static_cast<long long>(ld) * c] -= f * a[j + static_cast<long long>(ld) * c];
+    }
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, last first
+  for (int j = n - 1; j >= 0; j--) {
+    const int p = ipiv[j];
+    if (p != j)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double* cj = a + static_cast<long long>(ld) * j;
+        double* cp = a + static_cast<long long>(ld) * p;
+        const double t = cj[i];
+        cj[i] = cp[i];
+        cp[i] = t;
+      }
     __syncthreads();
   }
   return info;

@@ -8,8 +8,9 @@
 //   K_r_sn   = K_rs - T^T K_ss
 //   X_rr     = (K_rr - T^T K_sr) - K_r_sn T
 //   K_sn_r   = K_sr - K_ss T
-//   X_rr     = P L U                        (partial pivoting)
-//   U        = X_rr^{-1} K_r_sn,  L = K_sn_r X_rr^{-1}
+//   X_rr^-1  by Gauss-Jordan elimination with partial pivoting (kept: the
+//            solve sweeps multiply by it instead of solving with LU factors)
+//   U        = X_rr^{-1} K_r_sn,  L = K_sn_r X_rr^{-1}   (GEMMs)
 //   acc      = update(s, s) + L K_r_sn      (what the ancestors subtract)
 // The reference re-searches every compressed descendant's skeleton inside
 // the parent's index list (skel_factorization.cpp:246-294); here each box
@@ -41,14 +42,13 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   double* red = tile + kGemmTileDoubles;  // 64
   double* kbuf = red + 64;                // n*n when staged
   const DecTask tk = P.tasks[blockIdx.x];
-  const int n = tk.n, k = tk.k, r = n - k;
-  const bool staged = n <= kSmemN;
-  const int* act = tk.act;
+  const int n = tk.n, k = tk.k, r = n - k;  // n <= kSmemN: the host sends larger boxes
+  const int* act = tk.act;                  // through decouple_large
   const int* perm = tk.perm;
   const int* bid = tk.bid;
   const int* bpos = tk.bpos;
   const double* T = tk.T;
-  double* K = staged ? kbuf : tk.K;
+  double* K = kbuf;
   double* L = tk.L;
   double* U = tk.U;
   double* X = tk.X;
@@ -67,39 +67,36 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   const double* Krs_in = K + k;
   const double* Ksr = K + static_cast<long long>(n) * k;
   const double* Krr = K + k + static_cast<long long>(n) * k;
-  // K_r_sn = K_rs - T^T K_ss   (r x k), kept in the U buffer until the end
+  // K_r_sn = K_rs - T^T K_ss   (r x k), in the U buffer for now
   cta_gemm_tiled(U, r, Krs_in, n, T, k, true, Kss, n, false, r, k, k, tile);
-  // K_sn_r = K_sr - K_ss T     (k x r), in the L buffer
+  // K_sn_r = K_sr - K_ss T     (k x r), in the L buffer for now
   cta_gemm_tiled(L, k, Ksr, n, Kss, n, false, T, k, false, k, r, k, tile);
   // X = (K_rr - T^T K_sr) - K_r_sn T
   cta_gemm_tiled(X, r, Krr, n, T, k, true, Ksr, n, false, r, r, k, tile);
   cta_gemm_tiled(X, r, X, r, U, r, false, T, k, false, r, r, k, tile);
-  // LU of X_rr, in shared memory when it fits (K is no longer needed)
-  double* Xw = X;
-  if (staged) {
-    Xw = kbuf;
-    for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e] = X[e];
-    __syncthreads();
+  // K is done with: stage X, K_r_sn and K_sn_r in its place (r^2 + 2 k r
+  // <= n^2) and invert X there (Gauss-Jordan, partial pivoting)
+  double* Xw = kbuf;
+  double* Krsn = Xw + r * r;    // r x k
+  double* Ksnr = Krsn + r * k;  // k x r
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e] = X[e];
+  for (int e = threadIdx.x; e < r * k; e += kDecThreads) {
+    Krsn[e] = U[e];
+    Ksnr[e] = L[e];
   }
-  const int info = cta_lu(Xw, r, r, piv, red);
+  __syncthreads();
+  const int info = cta_gj_invert(Xw, r, r, piv, tile, red);
   if (info && threadIdx.x == 0) atomicExch(P.status, 1);
-  if (staged) {
-    for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e];
-  }
-  __syncthreads();
-  // L = K_sn_r X^{-1}, row by row through X^T
-  const int warp = threadIdx.x >> 5;
-  const int nw = kDecThreads / 32;
-  for (int row = warp; row < k; row += nw) warp_lu_solve_t(Xw, r, r, piv, L + row, k);
-  __syncthreads();
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e];
+  // U = X^{-1} K_r_sn,  L = K_sn_r X^{-1}
+  cta_gemm_tiled(U, r, nullptr, 0, Xw, r, false, Krsn, r, false, r, k, r, tile, 1.0);
+  cta_gemm_tiled(L, k, nullptr, 0, Ksnr, k, false, Xw, r, false, k, r, r, tile, 1.0);
   // acc = update(s, s) + L K_r_sn
-  cta_gemm_tiled(acc, k, nullptr, 0, L, k, false, U, r, false, k, k, r, tile);
+  cta_gemm_tiled(acc, k, nullptr, 0, L, k, false, Krsn, r, false, k, k, r, tile, 1.0);
   for (int e = threadIdx.x; e < k * k; e += kDecThreads) {
     const int i = e % k, j = e / k;
-    acc[e] = upd_lookup(bid, bpos, tk.blocks, perm[i], perm[j]) - acc[e];
+    acc[e] += upd_lookup(bid, bpos, tk.blocks, perm[i], perm[j]);
   }
-  // U = X^{-1} K_r_sn, column by column
-  for (int c = warp; c < k; c += nw) warp_lu_solve(Xw, r, r, piv, U + static_cast<long long>(r) * c, 1);
 }
 
 __global__ void assemble_top_kernel(int pde, const Node* nodes, const int* dofs, int n,
@@ -120,6 +117,11 @@ __global__ void assemble_perm_kernel(int pde, const Node* nodes, const int* act,
   const int a = static_cast<int>(e % n), b = static_cast<int>(e / n);
   const int pa = perm[a], pb = perm[b];
   K[e] = boundary_entry(pde, nodes, act[pa], act[pb]) - upd_lookup(bid, bpos, blocks, pa, pb);
+}
+
+__global__ void identity_kernel(double* y, int r) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < r * r) y[e] = (e % r == e / r) ? 1.0 : 0.0;
 }
 
 __global__ void acc_finish_kernel(double* acc, int k, const int* perm, const int* bid,
@@ -151,14 +153,30 @@ cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* s
   if ((e = launch_gemm_sub(tk.L, k, Ksr, n, Kss, n, false, tk.T, k, false, k, r, k, s))) return e;
   if ((e = launch_gemm_sub(tk.X, r, Krr, n, tk.T, k, true, Ksr, n, false, r, r, k, s))) return e;
   if ((e = launch_gemm_sub(tk.X, r, tk.X, r, tk.U, r, false, tk.T, k, false, r, r, k, s))) return e;
+  // X^{-1}: LU, then the solve of X Y = I (one CTA per column), into X
+  // through the K scratch (K is no longer needed); K_r_sn and K_sn_r are
+  // kept behind it (r^2 + 2 k r <= n^2)
+  double* Y = tk.K;
+  double* Krsn = Y + static_cast<long long>(r) * r;
+  double* Ksnr = Krsn + static_cast<long long>(r) * k;
+  if ((e = cudaMemcpyAsync(Krsn, tk.U, sizeof(double) * r * k, cudaMemcpyDeviceToDevice, s)))
+    return e;
+  if ((e = cudaMemcpyAsync(Ksnr, tk.L, sizeof(double) * r * k, cudaMemcpyDeviceToDevice, s)))
+    return e;
   if ((e = dense_lu(tk.X, r, r, tk.piv, status, s))) return e;
-  if ((e = dense_lu_solve_rows(tk.X, r, r, tk.piv, tk.L, k, k, s))) return e;
-  if ((e = launch_gemm_sub(tk.acc, k, nullptr, 0, tk.L, k, false, tk.U, r, false, k, k, r, s)))
+  count_launches(1);
+  identity_kernel<<<(r * r + 255) / 256, 256, 0, s>>>(Y, r);
+  if ((e = cudaGetLastError())) return e;
+  if ((e = dense_lu_solve(tk.X, r, r, tk.piv, Y, r, r, s))) return e;
+  if ((e = cudaMemcpyAsync(tk.X, Y, sizeof(double) * r * r, cudaMemcpyDeviceToDevice, s))) return e;
+  // U = X^{-1} K_r_sn, L = K_sn_r X^{-1}, acc = update + L K_r_sn
+  if ((e = small_gemm(false, false, r, k, r, 1.0, tk.X, r, Krsn, r, 0.0, tk.U, r, s))) return e;
+  if ((e = small_gemm(false, false, k, r, r, 1.0, Ksnr, k, tk.X, r, 0.0, tk.L, k, s))) return e;
+  if ((e = launch_gemm_sub(tk.acc, k, nullptr, 0, tk.L, k, false, Krsn, r, false, k, k, r, s)))
     return e;
   acc_finish_kernel<<<(k * k + 255) / 256, 256, 0, s>>>(tk.acc, k, tk.perm, tk.bid, tk.bpos,
                                                          tk.blocks);
-  if ((e = cudaGetLastError())) return e;
-  return dense_lu_solve(tk.X, r, r, tk.piv, tk.U, k, r, s);
+  return cudaGetLastError();
 }
 
 size_t decouple_smem_bytes(int n_max) {

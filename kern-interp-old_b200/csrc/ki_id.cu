@@ -511,7 +511,9 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
   double* cols = reinterpret_cast<double*>(smem_raw);   // owned columns
   double* tile = cols + static_cast<long long>((n + G - 1) / G) * lda;  // sketch: rows of A
   const int nloc = (n - g + G - 1) / G;  // columns j = g + G t owned by this CTA
-  double* v = tile + (sketch ? static_cast<long long>(kSketchTile + 1) * nloc : 0);  // m
+  // (the layout must be the same in every CTA of the cluster, whose peers
+  // read `slot` at the local offset: size the tile for the largest share)
+  double* v = tile + (sketch ? static_cast<long long>(kSketchTile + 1) * ((n + G - 1) / G) : 0);  // m
   double* rdiag = v + m;                                 // n
   double* vn1 = rdiag + n;                               // n
   double* vn2 = vn1 + n;                                 // n

@@ -114,9 +114,9 @@ struct DecTask {
   double* K;             // scratch n x n (boxes too large for shared memory)
   double* L;             // k x r, ld k
   double* U;             // r x k, ld r
-  double* X;             // LU of X_rr, r x r, ld r
+  double* X;             // X_rr^{-1}, r x r, ld r (written by the decoupling)
   double* acc;           // accumulated update on the skeleton, k x k
-  int* piv;              // X_rr pivots (r)
+  int* piv;              // r ints of scratch (pivots of the inversion)
 };
 
 struct DecParams {
@@ -191,8 +191,8 @@ struct SweepTask {
   const double* T;   // k x r
   const double* L;   // k x r
   const double* U;   // r x k
-  const double* X;   // LU of X_rr
-  const int* piv;
+  const double* X;   // X_rr^{-1} (r x r)
+  const int* piv;    // unused by the sweeps (kept with the factors)
 };
 
 struct SweepParams {

@@ -5,7 +5,8 @@
 // up to 32 right-hand sides staged in shared memory:
 //   up:    x[r] -= T^T x[s];  x[s] -= L x[r]      (apply_sweep_matrix :301-318)
 //          (x[s] -= U^T x[r] when sweeping Psi^T, skel_factorization.cpp:253-270)
-//   diag:  x[r] = X_rr^{-1} x[r]                  (apply_diag_inv_matrix :331-338)
+//   diag:  x[r] = X_rr^{-1} x[r]                  (apply_diag_inv_matrix :331-338;
+//          the factorization keeps X_rr^{-1} itself, so this is a product)
 //   down:  x[r] -= U x[s];    x[s] -= T x[r]
 // Staged vectors are stored dof-major (row * nc + rhs) so the threads that
 // share a matrix entry read consecutive shared-memory words.
@@ -28,7 +29,6 @@ inline int rhs_chunk(int nrhs, int cap) {
   const int fit = static_cast<int>(kSweepSmemBudget / (sizeof(double) * (cap > 0 ? cap : 1)));
   return std::max(1, std::min(std::min(nrhs, kRhsChunkMax), fit));
 }
-constexpr int kDiagWarps = 4;
 
 __device__ __forceinline__ int row_of(const SweepParams& P, int dof) {
   return P.red_pos_map ? P.red_pos[dof] : dof;
@@ -108,116 +108,49 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
   }
 }
 
-// X_rr^{-1} on a box's redundant entries of up to `chunk` right-hand sides
-// at once, one CTA per box, the entries staged dof-major in shared memory:
-// pivots, then blocked unit-L and U substitution in 32-row blocks (warps
-// take the right-hand sides of a diagonal block, all threads the updates
-// below / above it).  The LU factors are read with coalesced column loads.
-constexpr int kDiagCtaThreads = 256;
-__global__ void __launch_bounds__(kDiagCtaThreads) diag_cta_kernel(SweepParams P, int chunk) {
-  extern __shared__ double xs[];
+// x_r <- X_rr^{-1} x_r (TRANS: X_rr^{-T} x_r) on every box's redundant entries,
+// one CTA per box, up to `chunk` right-hand sides per pass staged dof-major
+// in shared memory; the decoupling stored X_rr^{-1} itself, so this is a
+// small matrix product (coalesced column reads) with no sequential steps.
+constexpr int kDiagThreads = 256;
+template <bool TRANS>
+__global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, int chunk) {
+  extern __shared__ double sm[];
   const SweepTask tk = P.tasks[blockIdx.x];
   const int r = tk.r;
-  const double* lu = tk.X;
+  const double* Xi = tk.X;
   const int* R = tk.red;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int nw = kDiagCtaThreads / 32;
   for (int c0 = 0; c0 < P.nrhs; c0 += chunk) {
     const int nc = min(chunk, P.nrhs - c0);
-    for (int t = threadIdx.x; t < r * nc; t += kDiagCtaThreads) {
+    double* xs = sm;
+    double* ys = sm + static_cast<long long>(r) * nc;
+    for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int j = t / nc, c = t - j * nc;
       xs[t] = P.x[row_of(P, R[j]) + static_cast<long long>(P.ldx) * (c0 + c)];
     }
     __syncthreads();
-    if (threadIdx.x < nc)
-      for (int i = 0; i < r; i++) {
-        const int p = tk.piv[i];
-        if (p != i) {
-          const double t = xs[i * nc + threadIdx.x];
-          xs[i * nc + threadIdx.x] = xs[p * nc + threadIdx.x];
-          xs[p * nc + threadIdx.x] = t;
-        }
+    for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
+      const int i = t % r, c = t / r;  // consecutive threads: consecutive rows i
+      double s0 = 0.0, s1 = 0.0;
+      int j = 0;
+      for (; j + 1 < r; j += 2) {
+        const double a0 = TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
+        const double a1 = TRANS ? Xi[j + 1 + static_cast<long long>(r) * i]
+                                : Xi[i + static_cast<long long>(r) * (j + 1)];
+        s0 += a0 * xs[j * nc + c];
+        s1 += a1 * xs[(j + 1) * nc + c];
       }
+      if (j < r)
+        s0 += (TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j]) *
+              xs[j * nc + c];
+      ys[i * nc + c] = s0 + s1;
+    }
     __syncthreads();
-    for (int kb = 0; kb < r; kb += 32) {  // unit L
-      const int nbk = min(32, r - kb);
-      double Lr[32];
-#pragma unroll
-      for (int k = 0; k < 32; k++)
-        Lr[k] = (lane < nbk && k < lane) ? lu[kb + lane + static_cast<long long>(r) * (kb + k)] : 0.0;
-      for (int c = warp; c < nc; c += nw) {
-        double xv = lane < nbk ? xs[(kb + lane) * nc + c] : 0.0;
-#pragma unroll
-        for (int k = 0; k < 32; k++) xv -= Lr[k] * __shfl_sync(0xffffffffu, xv, k);
-        if (lane < nbk) xs[(kb + lane) * nc + c] = xv;
-      }
-      __syncthreads();
-      const int below = r - kb - nbk;
-      for (int t = threadIdx.x; t < below * nc; t += kDiagCtaThreads) {
-        const int i = kb + nbk + t / nc, c = t % nc;
-        double s = 0.0;
-        for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(r) * (kb + k)] * xs[(kb + k) * nc + c];
-        xs[i * nc + c] -= s;
-      }
-      __syncthreads();
-    }
-    for (int kb = ((r - 1) / 32) * 32; kb >= 0; kb -= 32) {  // U
-      const int nbk = min(32, r - kb);
-      double Ur[32];
-#pragma unroll
-      for (int k = 0; k < 32; k++)
-        Ur[k] = (lane < nbk && k < nbk && k >= lane)
-                    ? lu[kb + lane + static_cast<long long>(r) * (kb + k)]
-                    : 0.0;
-      for (int c = warp; c < nc; c += nw) {
-        double xv = lane < nbk ? xs[(kb + lane) * nc + c] : 0.0;
-#pragma unroll
-        for (int k = 31; k >= 0; k--) {
-          if (k < nbk) {
-            if (lane == k) xv /= Ur[k];
-            const double xk = __shfl_sync(0xffffffffu, xv, k);
-            if (lane < k) xv -= Ur[k] * xk;
-          }
-        }
-        if (lane < nbk) xs[(kb + lane) * nc + c] = xv;
-      }
-      __syncthreads();
-      for (int t = threadIdx.x; t < kb * nc; t += kDiagCtaThreads) {
-        const int i = t / nc, c = t % nc;
-        double s = 0.0;
-        for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(r) * (kb + k)] * xs[(kb + k) * nc + c];
-        xs[i * nc + c] -= s;
-      }
-      __syncthreads();
-    }
-    for (int t = threadIdx.x; t < r * nc; t += kDiagCtaThreads) {
+    for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int j = t / nc, c = t - j * nc;
-      P.x[row_of(P, R[j]) + static_cast<long long>(P.ldx) * (c0 + c)] = xs[t];
+      P.x[row_of(P, R[j]) + static_cast<long long>(P.ldx) * (c0 + c)] = ys[t];
     }
     __syncthreads();
-  }
-}
-
-template <bool TRANS>
-__global__ void __launch_bounds__(32 * kDiagWarps) diag_kernel(SweepParams P, int cap) {
-  extern __shared__ double sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int b = blockIdx.x * kDiagWarps + warp;
-  if (b >= P.ntasks) return;
-  const SweepTask tk = P.tasks[b];
-  const int r = tk.r;
-  double* xr = sm + static_cast<long long>(warp) * cap;
-  const int* R = tk.red;
-  for (int c = 0; c < P.nrhs; c++) {
-    double* x = P.x + static_cast<long long>(P.ldx) * c;
-    for (int j = lane; j < r; j += 32) xr[j] = x[row_of(P, R[j])];
-    __syncwarp();
-    if (TRANS)
-      warp_lu_solve_t(tk.X, r, r, tk.piv, xr, 1);
-    else
-      warp_lu_solve(tk.X, r, r, tk.piv, xr, 1);
-    for (int j = lane; j < r; j += 32) x[row_of(P, R[j])] = xr[j];
-    __syncwarp();
   }
 }
 
@@ -257,30 +190,19 @@ namespace {
 template <bool TRANS>
 cudaError_t launch_diag(const SweepParams& p, cudaStream_t s) {
   if (p.ntasks == 0 || p.nrhs == 0) return cudaSuccess;
-  const int cap = p.cap;
-  const size_t smem = sizeof(double) * static_cast<size_t>(cap) * kDiagWarps;
-  cudaError_t e = cudaFuncSetAttribute(diag_kernel<TRANS>,
+  const int nc = rhs_chunk(p.nrhs, 2 * (p.cap > 0 ? p.cap : 1));
+  const size_t smem = 2 * sizeof(double) * static_cast<size_t>(p.cap > 0 ? p.cap : 1) * nc;
+  cudaError_t e = cudaFuncSetAttribute(diag_inv_kernel<TRANS>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   count_launches(1);
-  diag_kernel<TRANS><<<(p.ntasks + kDiagWarps - 1) / kDiagWarps, 32 * kDiagWarps, smem, s>>>(
-      p, cap);
+  diag_inv_kernel<TRANS><<<p.ntasks, kDiagThreads, smem, s>>>(p, nc);
   return cudaGetLastError();
 }
 }  // namespace
 
-cudaError_t launch_diag_solve(const SweepParams& p, cudaStream_t s) {
-  if (p.ntasks == 0 || p.nrhs == 0) return cudaSuccess;
-  const int nc = rhs_chunk(p.nrhs, p.cap);
-  const size_t smem = sizeof(double) * static_cast<size_t>(p.cap > 0 ? p.cap : 1) * nc;
-  cudaError_t e = cudaFuncSetAttribute(diag_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
-  if (e != cudaSuccess) return e;
-  count_launches(1);
-  diag_cta_kernel<<<p.ntasks, kDiagCtaThreads, smem, s>>>(p, nc);
-  return cudaGetLastError();
-}
+cudaError_t launch_diag_solve(const SweepParams& p, cudaStream_t s) { return launch_diag<false>(p, s); }
 
 cudaError_t launch_diag_solve_t(const SweepParams& p, cudaStream_t s) { return launch_diag<true>(p, s); }
 

@@ -135,3 +135,17 @@ def test_refine_from_very_loose_factorization(tol):
     mt, _ = o.solve(pr.f)
     o.close()
     assert H.rel(mu, mt) < 1e-10
+
+
+def test_sketched_ids_in_clusters_reach_fp64():
+    """Preconditioner mode on a problem whose top-level boxes need
+    multi-CTA clusters for their sketches (wide boxes at levels 1-2)."""
+    pr = G.stokes_holes_case(n_total=16384)
+    s = kinterp.Solver(pr, id_tol=1e-6, mode=1)
+    mu, alpha, it, rr = s.solve_refined(pr.f, rel_tol=1e-12, max_iters=30)
+    assert rr <= 1e-12, (it, rr)
+    assert it <= 10
+    o = K.PortSolver(pr, id_tol=1e-13, threads=8)
+    mt, at = o.solve(pr.f)
+    o.close()
+    assert H.rel(mu, mt) < 1e-10
