@@ -75,12 +75,12 @@ __device__ void border_u(int pde, double tx, double ty, const double* hole, int 
 // The hole border of a multiply-connected domain (initialize_U_mat and
 // initialize_Psi_mat, linear_solve.cpp:18-110), one thread per node: U
 // (dofs x nb, column-major) holds each hole's log / Stokeslet + rotlet
-// columns at the node, Psi (nb x dofs) and its transpose PsiT (dofs x nb)
-// the quadrature weights (and w (y, -x) for Stokes rotation) of the nodes on
-// each hole.  All three must be zero on entry.
+// columns at the node (and Urow the same dof-major), Psi (nb x dofs) the
+// quadrature weights (and w (y, -x) for Stokes rotation) of the nodes on
+// each hole.  Psi must be zero on entry.
 __global__ void border_fill_kernel(int pde, const Node* __restrict__ nodes, int np,
                                    const double* __restrict__ holes, int nh, double* U,
-                                   double* Psi, double* PsiT) {
+                                   double* Psi, double* Urow) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= np) return;
   const Node nd = nodes[q];
@@ -91,21 +91,22 @@ __global__ void border_fill_kernel(int pde, const Node* __restrict__ nodes, int 
       double u[3];
       border_u(pde, nd.x, nd.y, holes + 4 * h, 0, u);
       U[q + N * h] = u[0];
+      Urow[static_cast<long long>(q) * rows + h] = u[0];
     } else {
       for (int c = 0; c < 2; c++) {
         double u[3];
         border_u(pde, nd.x, nd.y, holes + 4 * h, c, u);
-        for (int j = 0; j < 3; j++) U[2 * q + c + N * (3 * h + j)] = u[j];
+        for (int j = 0; j < 3; j++) {
+          U[2 * q + c + N * (3 * h + j)] = u[j];
+          Urow[(2LL * q + c) * rows + 3 * h + j] = u[j];
+        }
       }
     }
   }
   for (int h = 0; h < nh; h++) {
     const double rx = nd.x - holes[4 * h], ry = nd.y - holes[4 * h + 1];
     if (sqrt(rx * rx + ry * ry) < holes[4 * h + 2] + 1e-8) {
-      auto put = [&](int i, long long j, double v) {
-        Psi[i + rows * j] = v;
-        PsiT[j + N * i] = v;
-      };
+      auto put = [&](int i, long long j, double v) { Psi[i + rows * j] = v; };
       if (pde == kLaplace) {
         put(h, q, nd.w);
       } else {
@@ -190,15 +191,13 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
 }
 
 cudaError_t launch_border_fill(int pde, const Node* nodes, int np, const double* holes, int nh,
-                               double* U, double* Psi, double* PsiT, cudaStream_t s) {
+                               double* U, double* Psi, double* Urow, cudaStream_t s) {
   const long long N = pde == kStokes ? 2LL * np : np;
   const long long nb = pde == kStokes ? 3LL * nh : nh;
-  cudaError_t e = cudaMemsetAsync(U, 0, sizeof(double) * N * nb, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(Psi, 0, sizeof(double) * N * nb, s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(PsiT, 0, sizeof(double) * N * nb, s);
+  const cudaError_t e = cudaMemsetAsync(Psi, 0, sizeof(double) * N * nb, s);
   if (e != cudaSuccess) return e;
   count_launches(1);
-  border_fill_kernel<<<(np + 255) / 256, 256, 0, s>>>(pde, nodes, np, holes, nh, U, Psi, PsiT);
+  border_fill_kernel<<<(np + 255) / 256, 256, 0, s>>>(pde, nodes, np, holes, nh, U, Psi, Urow);
   return cudaGetLastError();
 }
 

@@ -180,12 +180,14 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
       info = 1;
     }
     __syncthreads();
-    const int rem = n - j - 1;
-#pragma unroll 4
-    for (int e = threadIdx.x; e < rem * rem; e += blockDim.x) {
-      const int i = j + 1 + e % rem, c = j + 1 + e / rem;
-      a[i + static_cast<long long>(ld) * c] -=
-          a[i + static_cast<long long>(ld) * j] * a[j + static_cast<long long>(ld) * c];
+    // rank-one update of the trailing block: warps take columns, lanes rows
+    for (int c = j + 1 + warp; c < n; c += nw) {
+      double* ac = a + static_cast<long long>(ld) * c;
+      const double ajc = ac[j];
+      if (ajc != 0.0) {
+        const double* aj = a + static_cast<long long>(ld) * j;
+        for (int i = j + 1 + lane; i < n; i += 32) ac[i] -= aj[i] * ajc;
+      }
     }
     __syncthreads();
   }
@@ -262,15 +264,19 @@ __device__ inline int cta_gj_invert(double* a, int n, int ld, int* ipiv, double*
     for (int c = threadIdx.x; c < n; c += blockDim.x)
       a[j + static_cast<long long>(ld) * c] = c == j ? inv : a[j + static_cast<long long>(ld) * c] * inv;
     __syncthreads();
-    // eliminate column j from the other rows
-    for (long long e = threadIdx.x; e < static_cast<long long>(n) * n; e += blockDim.x) {
-      const int i = static_cast<int>(e % n), c = static_cast<int>(e / n);
-      if (i == j) continue;
-      const double f = col[i];
-      if (c == j)
-        a[i + static_cast<long long>(ld) * c] = -f * inv;
-      else if (f != 0.0)
-        a[i + static_cast<long long>(ld) * c] -= f * a[j + static_cast<long long>(ld) * c];
+    // eliminate column j from the other rows: warps take columns, lanes
+    // walk the rows (no index division in the inner loop)
+    for (int c = warp; c < n; c += nw) {
+      double* ac = a + static_cast<long long>(ld) * c;
+      if (c == j) {
+        for (int i = lane; i < n; i += 32)
+          if (i != j) ac[i] = -col[i] * inv;
+      } else {
+        const double rj = ac[j];
+        if (rj != 0.0)
+          for (int i = lane; i < n; i += 32)
+            if (i != j) ac[i] -= col[i] * rj;
+      }
     }
     __syncthreads();
   }

@@ -89,11 +89,15 @@ __global__ void __launch_bounds__(1024) panel_lu_kernel(double* a, int n, int ld
       atomicExch(status, 1);
     }
     __syncthreads();
-    const int rows = n - j - 1, cols = w - jj - 1;
-    for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
-      const int i = j + 1 + e % rows, c = j + 1 + e / rows;
-      a[i + static_cast<long long>(ld) * c] -=
-          a[i + static_cast<long long>(ld) * j] * a[j + static_cast<long long>(ld) * c];
+    // rank-one update of the panel's remaining columns: a warp per column,
+    // lanes over the rows
+    for (int c = j0 + jj + 1 + warp; c < j0 + w; c += nw) {
+      double* ac = a + static_cast<long long>(ld) * c;
+      const double ajc = ac[j];
+      if (ajc != 0.0) {
+        const double* aj = a + static_cast<long long>(ld) * j;
+        for (int i = j + 1 + lane; i < n; i += 32) ac[i] -= aj[i] * ajc;
+      }
     }
     __syncthreads();
   }
@@ -175,10 +179,15 @@ __global__ void __launch_bounds__(1024) panel_lu_smem_kernel(double* a, int n, i
       for (int i = jj + 1 + threadIdx.x; i < rows; i += blockDim.x) P[i + ldp * jj] *= inv;
     }
     __syncthreads();
-    const int r = rows - jj - 1, cols = w - jj - 1;
-    for (int e = threadIdx.x; e < r * cols; e += blockDim.x) {
-      const int i = jj + 1 + e % r, c = jj + 1 + e / r;
-      P[i + ldp * c] -= P[i + ldp * jj] * P[jj + ldp * c];
+    // rank-one update of the panel's remaining columns: a warp per column,
+    // lanes over the rows
+    for (int c = jj + 1 + warp; c < w; c += nw) {
+      double* pc = P + ldp * c;
+      const double pjc = pc[jj];
+      if (pjc != 0.0) {
+        const double* pj = P + ldp * jj;
+        for (int i = jj + 1 + lane; i < rows; i += 32) pc[i] -= pj[i] * pjc;
+      }
     }
     __syncthreads();
   }
@@ -288,6 +297,14 @@ __global__ void gather_kernel(const double* x, int ldx, const int* idx, int n, i
   if (e >= static_cast<long long>(n) * nrhs) return;
   const int i = static_cast<int>(e % n), c = static_cast<int>(e / n);
   out[i + static_cast<long long>(ldo) * c] = x[idx[i] + static_cast<long long>(ldx) * c];
+}
+
+__global__ void gather_rows_kernel(const double* x, int ldd, const int* idx, int n, int nrhs,
+                                   double* out, int ldo) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(n) * nrhs) return;
+  const int c = static_cast<int>(e % nrhs), i = static_cast<int>(e / nrhs);
+  out[i + static_cast<long long>(ldo) * c] = x[static_cast<long long>(idx[i]) * ldd + c];
 }
 
 __global__ void scatter_kernel(double* x, int ldx, const int* idx, int n, int nrhs,
@@ -440,6 +457,16 @@ cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int n
   if (tot == 0) return cudaSuccess;
   count_launches(1);
   gather_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(x, ldx, idx, n, nrhs, out, ldo);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_rows(const double* x, int ldd, const int* idx, int n, int nrhs,
+                               double* out, int ldo, cudaStream_t s) {
+  const long long tot = static_cast<long long>(n) * nrhs;
+  if (tot == 0) return cudaSuccess;
+  count_launches(1);
+  gather_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(x, ldd, idx, n, nrhs, out,
+                                                                          ldo);
   return cudaGetLastError();
 }
 

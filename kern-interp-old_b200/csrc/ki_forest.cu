@@ -19,10 +19,9 @@ __device__ __forceinline__ double top_upd(const TopTask& t, int a, int b) {
 __global__ void forest_assemble_kernel(int pde, const Node* __restrict__ nodes,
                                        const TopTask* __restrict__ tasks) {
   const TopTask t = tasks[blockIdx.y];
-  const long long nn = static_cast<long long>(t.n) * t.n;
-  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < nn;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int a = static_cast<int>(e % t.n), b = static_cast<int>(e / t.n);
+  const int nn = t.n * t.n;  // top skeletons are far below 46341 dofs
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += gridDim.x * blockDim.x) {
+    const int a = e % t.n, b = e / t.n;
     t.a[e] = boundary_entry(pde, nodes, t.dofs[a], t.dofs[b]) - top_upd(t, a, b);
   }
 }

@@ -802,7 +802,7 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
     for (int p = threadIdx.x; p < n; p += kOcThreads) P.perm[tk.perm_off + p] = pos2col[p];
   }
   // T = R11^{-1} R12 for this CTA's redundant columns, solved in place in
-  // their first k rows (dtrsm column sweep, one barrier per row of R11)
+  // their first k rows (dtrsm column sweep)
   const int k = rank;
   double* T = P.tout + tk.t_off;
   if (k > 0) {
@@ -818,23 +818,25 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
       if (lane == 0) si[0] = cnt;
     }
     __syncthreads();
+    // one warp per redundant column: the column's back substitution runs
+    // in its warp with no CTA barrier (columns are independent)
     const int nr = si[0];
-    for (int q = k - 1; q >= 0; q--) {
-      const double* rq = colp(pos2col[q]);
-      const double dq = rdiag[q];
-      for (int e = threadIdx.x; e < (q + 1) * nr; e += kOcThreads) {
-        const int l = e % (q + 1), t = e / (q + 1);
-        const int p = own[t];
-        double* col = colp(pos2col[p]);
+    for (int t = warp; t < nr; t += kOcWarps) {
+      const int p = own[t];
+      double* col = colp(pos2col[p]);
+      for (int q = k - 1; q >= 0; q--) {
         const double bq = col[q];
-        if (l == q) {
-          T[q + static_cast<long long>(p - k) * k] = bq != 0.0 ? bq / dq : bq;
-        } else if (bq != 0.0) {
-          col[l] -= (bq / dq) * rq[l];
+        __syncwarp();
+        const double xq = bq != 0.0 ? bq / rdiag[q] : bq;
+        if (lane == 0) T[q + static_cast<long long>(p - k) * k] = xq;
+        if (bq != 0.0) {
+          const double* rq = colp(pos2col[q]);
+          for (int l = lane; l < q; l += 32) col[l] -= xq * rq[l];
         }
+        __syncwarp();
       }
-      __syncthreads();
     }
+    __syncthreads();
   }
   if constexpr (G > 1) cg::this_cluster().sync();
 }

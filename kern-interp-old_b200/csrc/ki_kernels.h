@@ -203,6 +203,7 @@ struct SweepParams {
   int red_pos_map;      // nonzero: redundant dofs index rows of x via red_pos
   const int* red_pos;
   int cap;              // per-box staging: max over tasks of k + r
+  int ldd = 1;          // dof stride of x: entry (dof, rhs c) is x[dof ldd + c ldx]
 };
 
 // x[red] -= T^T x[skel]; then x[skel] -= L x[red]   (or U^T when use_u)
@@ -222,6 +223,9 @@ cudaError_t launch_diag_solve_t(const SweepParams& p, cudaStream_t s);
 // out[i] = x[idx[i]] (gather) / x[idx[i]] = in[i] (scatter), nrhs columns.
 cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int nrhs,
                           double* out, int ldo, cudaStream_t s);
+// out[i + ldo c] = x[idx[i] ldd + c]: rows of a dof-major matrix
+cudaError_t launch_gather_rows(const double* x, int ldd, const int* idx, int n, int nrhs,
+                               double* out, int ldo, cudaStream_t s);
 cudaError_t launch_scatter(double* x, int ldx, const int* idx, int n, int nrhs,
                            const double* in, int ldi, cudaStream_t s);
 // C = alpha * op(A) * op(B) + beta * C, small dense FP64 (column-major).
@@ -240,10 +244,12 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
                                 const double* targets, const double* mu, int nh,
                                 const double* holes, const double* alpha, double* out,
                                 cudaStream_t s);
-// Hole border of a multiply-connected domain: U (dofs x nb), Psi (nb x
-// dofs) and PsiT = Psi^T (initialize_U_mat / initialize_Psi_mat).
+// Hole border of a multiply-connected domain (initialize_U_mat /
+// initialize_Psi_mat): U (dofs x nb, column-major), Urow the same U stored
+// dof-major (entry (i, b) at i nb + b), Psi (nb x dofs, column-major, which
+// is Psi^T stored dof-major).
 cudaError_t launch_border_fill(int pde, const Node* nodes, int np, const double* holes, int nh,
-                               double* U, double* Psi, double* PsiT, cudaStream_t s);
+                               double* U, double* Psi, double* Urow, cudaStream_t s);
 // Dense kernel block K(tgt, src), column-major nt x ns.
 cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
                                 const int* src, int ns, double* out, cudaStream_t s);

@@ -354,8 +354,8 @@ int Solver::factor() {
     const size_t cnt = static_cast<size_t>(n_dofs_) * nb_;
     KI_ALLOC(d_U_, double, cnt);
     KI_ALLOC(d_Psi_, double, cnt);
-    KI_ALLOC(d_PsiT_, double, cnt);
-    KI_CUDA(launch_border_fill(opt_.pde, d_nodes_, n_points_, d_holes_, nh, d_U_, d_Psi_, d_PsiT_,
+    KI_ALLOC(d_Urow_, double, cnt);
+    KI_CUDA(launch_border_fill(opt_.pde, d_nodes_, n_points_, d_holes_, nh, d_U_, d_Psi_, d_Urow_,
                                stream_));
   }
 
@@ -936,8 +936,11 @@ int Solver::factor_border() {
   double *modU, *modP;
   KI_ALLOC(modU, double, static_cast<size_t>(N) * nb);
   KI_ALLOC(modP, double, static_cast<size_t>(N) * nb);
-  KI_CUDA(cudaMemcpyAsync(modU, d_U_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice, stream_));
-  KI_CUDA(cudaMemcpyAsync(modP, d_PsiT_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
+  // U and Psi^T dof-major (a dof's nb entries contiguous: the sweeps gather
+  // whole rows); Psi's own column-major nb x N layout is Psi^T dof-major
+  KI_CUDA(cudaMemcpyAsync(modU, d_Urow_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
+                          stream_));
+  KI_CUDA(cudaMemcpyAsync(modP, d_Psi_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
                           stream_));
   const int L = static_cast<int>(levels_.size());
   cudaEvent_t b0 = nullptr;
@@ -945,7 +948,7 @@ int Solver::factor_border() {
   for (int l = L - 1; l >= 0; l--) {
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
-    SweepParams sp{lf.d_tasks, lf.ntasks, modU, N, nb, 0, nullptr, lf.cap};
+    SweepParams sp{lf.d_tasks, lf.ntasks, modU, 1, nb, 0, nullptr, lf.cap, nb};
     KI_CUDA(launch_sweep_up(sp, false, stream_));
     sp.x = modP;
     KI_CUDA(launch_sweep_up(sp, true, stream_));
@@ -958,11 +961,11 @@ int Solver::factor_border() {
   KI_ALLOC(us, double, static_cast<size_t>(ns) * nb);
   KI_ALLOC(ps, double, static_cast<size_t>(ns) * nb);
   KI_ALLOC(corr, double, static_cast<size_t>(nb) * nb);
-  KI_CUDA(launch_gather(modU, N, d_allred_, nr, nb, d_Ured_, nr, stream_));
-  KI_CUDA(launch_gather(modP, N, d_allred_, nr, nb, d_Pred_, nr, stream_));
-  KI_CUDA(launch_gather(modU, N, d_allred_, nr, nb, dinv, nr, stream_));
-  KI_CUDA(launch_gather(modU, N, d_allskel_, ns, nb, us, ns, stream_));
-  KI_CUDA(launch_gather(modP, N, d_allskel_, ns, nb, ps, ns, stream_));
+  KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, d_Ured_, nr, stream_));
+  KI_CUDA(launch_gather_rows(modP, nb, d_allred_, nr, nb, d_Pred_, nr, stream_));
+  KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, dinv, nr, stream_));
+  KI_CUDA(launch_gather_rows(modU, nb, d_allskel_, ns, nb, us, ns, stream_));
+  KI_CUDA(launch_gather_rows(modP, nb, d_allskel_, ns, nb, ps, ns, stream_));
   SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dinv, nr, nb, 1, d_red_pos_,
                  all_compressed_.cap};
   KI_CUDA(launch_diag_solve(dp, stream_));

@@ -247,7 +247,7 @@ class Solver {
   int* d_red_pos_ = nullptr;
   double* d_U_ = nullptr;     // N x nb
   double* d_Psi_ = nullptr;   // nb x N
-  double* d_PsiT_ = nullptr;  // Psi^T (N x nb)
+  double* d_Urow_ = nullptr;  // U dof-major (N x nb, row i contiguous)
   double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
   double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
   double* d_tmp_ = nullptr;   // solve scratch

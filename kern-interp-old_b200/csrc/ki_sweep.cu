@@ -64,11 +64,11 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
     double* xr = sm + k * nc;
     for (int t = threadIdx.x; t < k * nc; t += kSweepThreads) {
       const int i = t / nc, c = t - i * nc;
-      xs[t] = P.x[S[i] + static_cast<long long>(P.ldx) * (c0 + c)];
+      xs[t] = P.x[static_cast<long long>(S[i]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
     for (int t = threadIdx.x; t < r * nc; t += kSweepThreads) {
       const int j = t / nc, c = t - j * nc;
-      xr[t] = P.x[R[j] + static_cast<long long>(P.ldx) * (c0 + c)];
+      xr[t] = P.x[static_cast<long long>(R[j]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
     __syncthreads();
     if (MODE <= 1) {
@@ -98,11 +98,11 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
     __syncthreads();
     for (int t = threadIdx.x; t < k * nc; t += kSweepThreads) {
       const int i = t / nc, c = t - i * nc;
-      P.x[S[i] + static_cast<long long>(P.ldx) * (c0 + c)] = xs[t];
+      P.x[static_cast<long long>(S[i]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)] = xs[t];
     }
     for (int t = threadIdx.x; t < r * nc; t += kSweepThreads) {
       const int j = t / nc, c = t - j * nc;
-      P.x[R[j] + static_cast<long long>(P.ldx) * (c0 + c)] = xr[t];
+      P.x[static_cast<long long>(R[j]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)] = xr[t];
     }
     __syncthreads();
   }
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
     double* ys = sm + static_cast<long long>(r) * nc;
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int j = t / nc, c = t - j * nc;
-      xs[t] = P.x[row_of(P, R[j]) + static_cast<long long>(P.ldx) * (c0 + c)];
+      xs[t] = P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
     __syncthreads();
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
     __syncthreads();
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int j = t / nc, c = t - j * nc;
-      P.x[row_of(P, R[j]) + static_cast<long long>(P.ldx) * (c0 + c)] = ys[t];
+      P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)] = ys[t];
     }
     __syncthreads();
   }
