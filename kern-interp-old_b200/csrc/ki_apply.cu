@@ -49,29 +49,6 @@ __global__ void apply_kernel(int pde, const Node* __restrict__ nodes, int n,
   }
 }
 
-// Border columns for one target point (initialize_U_mat, linear_solve.cpp:18-64).
-__device__ void border_u(int pde, double tx, double ty, const double* hole, int comp,
-                         double* out) {
-  const double rx = tx - hole[0], ry = ty - hole[1];
-  const double rn = sqrt(rx * rx + ry * ry);
-  if (pde == kLaplace) {
-    out[0] = log(rn);
-    return;
-  }
-  const double scale = 1.0 / (4 * 3.14159265358979323846);
-  const double inv2 = 1.0 / (rn * rn);
-  const double lg = log(1 / rn);
-  if (comp == 0) {
-    out[0] = scale * (lg + inv2 * rx * rx);
-    out[1] = scale * (inv2 * rx * ry);
-    out[2] = ry * (scale * inv2);
-  } else {
-    out[0] = scale * (inv2 * ry * rx);
-    out[1] = scale * (lg + inv2 * ry * ry);
-    out[2] = -rx * (scale * inv2);
-  }
-}
-
 // The hole border of a multiply-connected domain (initialize_U_mat and
 // initialize_Psi_mat, linear_solve.cpp:18-110), one thread per node: U
 // (dofs x nb, column-major) holds each hole's log / Stokeslet + rotlet

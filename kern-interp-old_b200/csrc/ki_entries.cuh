@@ -160,6 +160,45 @@ __device__ __forceinline__ double forward_entry(int pde, const Node* __restrict_
   return mul(mul(pot, tgt_comp ? r1 : r0), sc ? r1 : r0);
 }
 
+// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
+// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
+// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
+// relative error, so the result is accurate to FP64 rounding.  x = 0 or
+// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
+// only pass far-away padding (whose numerators are zero) beyond it.
+__device__ __forceinline__ double nr_rcp(double x) {
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
+  double y = static_cast<double>(yf);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// Border columns for one target point (initialize_U_mat, linear_solve.cpp:18-64).
+__device__ __forceinline__ void border_u(int pde, double tx, double ty, const double* hole, int comp,
+                         double* out) {
+  const double rx = tx - hole[0], ry = ty - hole[1];
+  const double rn = sqrt(rx * rx + ry * ry);
+  if (pde == kLaplace) {
+    out[0] = log(rn);
+    return;
+  }
+  const double scale = 1.0 / (4 * 3.14159265358979323846);
+  const double inv2 = 1.0 / (rn * rn);
+  const double lg = log(1 / rn);
+  if (comp == 0) {
+    out[0] = scale * (lg + inv2 * rx * rx);
+    out[1] = scale * (inv2 * rx * ry);
+    out[2] = ry * (scale * inv2);
+  } else {
+    out[0] = scale * (inv2 * ry * rx);
+    out[1] = scale * (lg + inv2 * ry * ry);
+    out[2] = -rx * (scale * inv2);
+  }
+}
+
 }  // namespace kib
 
 #endif  // KI_ENTRIES_CUH_

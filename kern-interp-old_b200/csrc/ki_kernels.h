@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <vector>
 
 #include "ki_entries.cuh"
@@ -244,6 +246,22 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
                                 const double* targets, const double* mu, int nh,
                                 const double* holes, const double* alpha, double* out,
                                 cudaStream_t s);
+// Solution on domain points with the domain mask (boundary_integral_solve,
+// linear_solve.cpp:142-180).  kind: kDomainAll (no mask), kDomainNodes
+// (CubicBoundary::is_in_domain on the node curves), kDomainDisk (the
+// Circle / Annulus / Donut test with disk = {cx, cy, R}).  mask: 1 inside,
+// 0 outside.  launch_domain_eval zeroes outside points when mask is given;
+// `part` holds splits x rows doubles when splits > 1 (domain_splits).
+enum DomainKind : int { kDomainAll = 0, kDomainNodes = 1, kDomainDisk = 2 };
+int domain_splits(int nt, int np, int num_sms);
+cudaError_t launch_domain_mask(int kind, const Node* nodes, int np, const double* holes, int nh,
+                               const double* disk, int nt, const double* targets,
+                               unsigned char* mask, cudaStream_t s);
+cudaError_t launch_domain_eval(int pde, const Node* nodes, int np, int nt,
+                               const double* targets, const double* mu, int nh,
+                               const double* holes, const double* alpha,
+                               const unsigned char* mask, int splits, double* part,
+                               double* out, cudaStream_t s);
 // Hole border of a multiply-connected domain (initialize_U_mat /
 // initialize_Psi_mat): U (dofs x nb, column-major), Urow the same U stored
 // dof-major (entry (i, b) at i nb + b), Psi (nb x dofs, column-major, which

@@ -25,22 +25,6 @@ namespace {
 
 constexpr int kMvThreads = 256;
 
-// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
-// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
-// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
-// relative error, so the result is accurate to FP64 rounding.  x = 0 or
-// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
-// only pass far-away padding (whose numerators are zero) beyond it.
-__device__ __forceinline__ double nr_rcp(double x) {
-  float yf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
-  double y = static_cast<double>(yf);
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
-}
-
 // Per-source values staged in shared memory.
 //   Laplace:          a = -(w / 2 pi) x (n_x, n_y)
 //   Laplace-Neumann:  a = (w / 2 pi) x (1, 1)      (target normal applied later)

@@ -11,6 +11,10 @@ namespace kib {
 
 namespace {
 
+// set while a thread runs pool work: a parallel_for issued from inside a job
+// runs inline instead of waiting for the (busy) pool
+thread_local bool t_in_job = false;
+
 class Pool {
  public:
   Pool() {
@@ -49,11 +53,13 @@ class Pool {
 
  private:
   void work() {
+    t_in_job = true;
     for (;;) {
       const int b = next_.fetch_add(grain_);
       if (b >= n_) break;
       (*fn_)(b, std::min(n_, b + grain_));
     }
+    t_in_job = false;
   }
   void loop() {
     long long seen = 0;
@@ -94,7 +100,7 @@ int pool_threads() { return pool().size(); }
 void parallel_for(int n, int grain, const std::function<void(int, int)>& fn, int serial_below) {
   if (n <= 0) return;
   grain = std::max(1, grain);
-  if (n < serial_below || n <= grain || pool().size() == 1) {
+  if (n < serial_below || n <= grain || t_in_job || pool().size() == 1) {
     fn(0, n);
     return;
   }

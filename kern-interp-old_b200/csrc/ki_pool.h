@@ -3,7 +3,8 @@
 // chunks of `grain` indices claimed through an atomic counter; the calling
 // thread works too, and the call returns when every chunk is done.  Jobs
 // below `serial_below` indices run on the caller alone (thread hand-off
-// costs more than small levels take).
+// costs more than small levels take), and so does a parallel_for issued
+// from inside another one.
 #ifndef KI_POOL_H_
 #define KI_POOL_H_
 

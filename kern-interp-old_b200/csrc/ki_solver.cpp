@@ -16,6 +16,7 @@
 #include "ki_pool.h"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -189,9 +190,16 @@ Solver::~Solver() {
   cudaStreamSynchronize(stream_);
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   if (dstream_) cudaStreamSynchronize(dstream_);
+  for (int i = 0; i < kIdStreams; i++)
+    if (id_streams_[i]) cudaStreamSynchronize(id_streams_[i]);
   if (ev_id_) cudaEventDestroy(ev_id_);
   if (ev_dec_) cudaEventDestroy(ev_dec_);
   if (dstream_) cudaStreamDestroy(dstream_);
+  if (id_fork_) cudaEventDestroy(id_fork_);
+  for (int i = 0; i < kIdStreams; i++) {
+    if (id_join_[i]) cudaEventDestroy(id_join_[i]);
+    if (id_streams_[i]) cudaStreamDestroy(id_streams_[i]);
+  }
 }
 
 int Solver::timer_begin(cudaEvent_t* e0, cudaStream_t s) {
@@ -311,9 +319,30 @@ int Solver::factor() {
     KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
     KI_CUDA(cudaEventCreateWithFlags(&ev_id_, cudaEventDisableTiming));
     KI_CUDA(cudaEventCreateWithFlags(&ev_dec_, cudaEventDisableTiming));
+    KI_CUDA(cudaEventCreateWithFlags(&id_fork_, cudaEventDisableTiming));
+    for (int i = 0; i < kIdStreams; i++) {
+      KI_CUDA(cudaStreamCreateWithFlags(&id_streams_[i], cudaStreamNonBlocking));
+      KI_CUDA(cudaEventCreateWithFlags(&id_join_[i], cudaEventDisableTiming));
+    }
   }
-  for (int G = 1; G <= 16; G *= 2)
-    onchip_ok_[G] = id_cluster_fits(kOnChip + G, 4096, 256, (227 * 1024 - id_smem_bytes(4096, 256)) / 8) != 0;
+  {
+    // which full-shared-memory cluster sizes the device can schedule: asked
+    // once per device and process (the occupancy queries are not free)
+    static std::mutex mu;
+    static std::map<int, std::array<bool, 17>> known;
+    int dev = 0;
+    KI_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = known.find(dev);
+    if (it == known.end()) {
+      std::array<bool, 17> ok{};
+      for (int G = 1; G <= 16; G *= 2)
+        ok[G] = id_cluster_fits(kOnChip + G, 4096, 256,
+                                (227 * 1024 - id_smem_bytes(4096, 256)) / 8) != 0;
+      it = known.emplace(dev, ok).first;
+    }
+    for (int G = 0; G <= 16; G++) onchip_ok_[G] = it->second[G];
+  }
   if (starts_.size() > 1) {
     if (!holes_.empty()) return fail("a forest of problems cannot have holes");
     tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
@@ -531,7 +560,11 @@ int Solver::process_level(int level) {
 
   // one launch per cluster size (split further so that the launch's
   // shared-memory layout, sized by its largest rows / columns / column
-  // storage, still fits)
+  // storage, still fits); the first on stream_, the others forked onto the
+  // ID streams and joined back before the ranks are read
+  KI_CUDA(cudaEventRecord(id_fork_, stream_));
+  int nlaunch = 0;
+  bool used[kIdStreams] = {};
   for (int q0 = 0; q0 < nc;) {
     int q1 = q0;
     int m_cap = 0, n_cap = 0;
@@ -571,14 +604,26 @@ int Solver::process_level(int level) {
     p.m_cap = m_cap;
     p.n_cap = n_cap;
     p.onchip_smem = onchip;
-    cudaEvent_t e0 = nullptr;
-    if (time_phases && timer_begin(&e0)) return -2;
-    KI_CUDA(launch_id(p, cand[q0].g, stream_));
-    if (time_phases) {
-      if (timer_end(e0, {level, 0, cand[q0].g, q1 - q0, m_cap, n_cap, 0.0})) return -2;
+    const int si = nlaunch == 0 ? -1 : (nlaunch - 1) % kIdStreams;
+    cudaStream_t ls = si < 0 ? stream_ : id_streams_[si];
+    if (si >= 0 && !used[si]) {
+      KI_CUDA(cudaStreamWaitEvent(ls, id_fork_, 0));
+      used[si] = true;
     }
+    cudaEvent_t e0 = nullptr;
+    if (time_phases && timer_begin(&e0, ls)) return -2;
+    KI_CUDA(launch_id(p, cand[q0].g, ls));
+    if (time_phases) {
+      if (timer_end(e0, {level, 0, cand[q0].g, q1 - q0, m_cap, n_cap, 0.0}, ls)) return -2;
+    }
+    nlaunch++;
     q0 = q1;
   }
+  for (int i = 0; i < kIdStreams; i++)
+    if (used[i]) {
+      KI_CUDA(cudaEventRecord(id_join_[i], id_streams_[i]));
+      KI_CUDA(cudaStreamWaitEvent(stream_, id_join_[i], 0));
+    }
   std::vector<int> rank(nc), perm(perm_total);
   KI_CUDA(cudaMemcpyAsync(rank.data(), d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
   KI_CUDA(cudaMemcpyAsync(perm.data(), d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,

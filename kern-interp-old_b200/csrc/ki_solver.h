@@ -131,6 +131,14 @@ class Solver {
                        double* d_grad_normals, double* d_grad_weights, double* d_grad_curv);
   // y = A x on device (bordered when there are holes).
   int apply_device(const double* d_x, double* d_y);
+  // boundary_integral_solve's evaluation (linear_solve.cpp:142-180):
+  // d_out = K_domain mu + U_forward alpha at nt points, zero outside the
+  // domain of test `kind` (DomainKind; disk = host {cx, cy, R} for
+  // kDomainDisk).  domain_mask writes the test alone (1 inside).
+  int eval_domain(int nt, const double* d_targets, const double* d_mu, const double* d_alpha,
+                  int kind, const double* disk, double* d_out);
+  int domain_mask(int nt, const double* d_targets, int kind, const double* disk,
+                  unsigned char* d_mask);
 
   int n_dofs() const { return n_dofs_; }
   int n_border() const { return nb_; }
@@ -208,6 +216,11 @@ class Solver {
   // GPU runs, the interpolative decompositions of level l - 1.
   cudaStream_t dstream_ = nullptr;
   cudaEvent_t ev_id_ = nullptr, ev_dec_ = nullptr;
+  // A level's ID launches of different cluster sizes are independent: the
+  // second and later ones run on these streams, concurrently with the first.
+  static constexpr int kIdStreams = 3;
+  cudaStream_t id_streams_[kIdStreams] = {};
+  cudaEvent_t id_fork_ = nullptr, id_join_[kIdStreams] = {};
 
   bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
@@ -255,6 +268,7 @@ class Solver {
   // operator-product and dot-product partials
   Scratch kry_;
   Scratch adj_;  // adjoint contraction partials
+  Scratch dom_;  // domain evaluation: split partials and the mask
   int mv_setup();  // tile table of the operator product (once)
   // The solve as a CUDA graph on fixed buffers (captured at the first call,
   // replayed for every preconditioner application of the refinement):

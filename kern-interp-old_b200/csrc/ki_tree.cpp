@@ -19,95 +19,179 @@ int QuadTreeHost::pick_child(const Box& b, double x, double y) const {
   return y < my ? 3 : 2;
 }
 
-void QuadTreeHost::subdivide(int id) {
-  // quadtree.cpp:203-285: four children appended to the next level in
-  // {BL, TL, TR, BR} order, the parent's dofs handed down point by point,
-  // then any over-full child split depth first.
-  boxes[id].leaf = false;
-  double c[8];
-  std::memcpy(c, boxes[id].corner, sizeof(c));
-  const double mx = ((c[6] - c[0]) / 2.0) + c[0];
-  const double my = ((c[3] - c[1]) / 2.0) + c[1];
-  const int lvl = boxes[id].level + 1;
-  const double half = boxes[id].side / 2.0;
-  if (static_cast<int>(levels.size()) < lvl + 1) levels.emplace_back();
-  int kid[4];
-  for (int q = 0; q < 4; q++) {
-    Box ch;
-    std::memcpy(ch.corner, c, sizeof(c));
-    ch.tree = boxes[id].tree;
-    ch.level = lvl;
-    ch.side = half;
-    ch.parent = id;
-    kid[q] = static_cast<int>(boxes.size());
-    boxes.push_back(ch);
-    levels[lvl].push_back(kid[q]);
-  }
-  // Corner edits per child: {index, value} pairs.
-  const int edit_idx[4][4] = {{3, 4, 5, 6}, {1, 4, 6, 7}, {0, 1, 2, 7}, {0, 2, 3, 5}};
-  const double edit_val[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
+// Children's corners: {index, value} edits of the parent's corners per child
+// {BL, TL, TR, BR} (quadtree.cpp:203-285).
+namespace {
+const int kEditIdx[4][4] = {{3, 4, 5, 6}, {1, 4, 6, 7}, {0, 1, 2, 7}, {0, 2, 3, 5}};
+}  // namespace
+
+void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, double hi) {
+  // The reference inserts points one at a time (quadtree.cpp:164-197) and
+  // splits a leaf as soon as it holds more than max_leaf dofs
+  // (node_subdivide, :203-285), over-full children at once, depth first.
+  // The resulting tree does not depend on the order: a box is split exactly
+  // when all its points together exceed max_leaf, so it is built here top
+  // down, every level's boxes partitioned in parallel.  What the insertion
+  // order does decide is the order in which boxes were created (their ids
+  // and the level lists): a box splits when its (cap+1)-th point, in index
+  // order, arrives (cap = max_leaf / sol_dim points), or when its parent
+  // creates it already over-full; splits at the same moment happen depth
+  // first.  Sorting the splits by (that point index, depth-first position)
+  // and numbering the children in that order reproduces the reference ids.
+  //
+  // Boxes hold contiguous ranges of one point permutation; splitting a box
+  // stably partitions its range into its children's ranges (counting sort by
+  // child), so every range is in point-index order until its own box splits
+  // (its list is copied out then; a leaf's at the end).
+  struct Tmp {
+    int parent = -1, level = 0, child[4] = {-1, -1, -1, -1};
+    int begin = 0, count = 0;
+    double corner[8];
+  };
+  std::vector<Tmp> tb(1);
+  const double c0[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
+  std::memcpy(tb[0].corner, c0, sizeof(c0));
+  tb[0].count = p1 - p0;
+  std::vector<int> perm(p1 - p0), scratch(p1 - p0);
+  for (int q = p0; q < p1; q++) perm[q - p0] = q;
+  std::vector<std::vector<int>> split_pts;  // index-ordered points of split boxes
+  std::vector<int> split_slot(1, -1);
+  const int cap = max_leaf_ / sol_dim_;  // split when a box holds more points
+  std::vector<int> frontier{0};
+  while (!frontier.empty()) {
+    std::vector<int> split;
+    for (int id : frontier)
+      if (tb[id].count > cap) split.push_back(id);
+    if (split.empty()) break;
+    const int base = static_cast<int>(tb.size());
+    tb.resize(base + 4 * split.size());
+    split_slot.resize(tb.size(), -1);
+    const int sbase = static_cast<int>(split_pts.size());
+    split_pts.resize(sbase + split.size());
+    parallel_for(static_cast<int>(split.size()), 4, [&](int a, int e) {
+      for (int s = a; s < e; s++) {
+        Tmp& P = tb[split[s]];
+        int* rp = perm.data() + P.begin;
+        int* rq = scratch.data() + P.begin;
+        split_slot[split[s]] = sbase + s;
+        split_pts[sbase + s].assign(rp, rp + P.count);
+        const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
+        const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
+        int cnt[4] = {0, 0, 0, 0};
+        for (int i = 0; i < P.count; i++) {
+          const int pt = rp[i];
+          const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
+          const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
+          rq[i] = q;
+          cnt[q]++;
+        }
+        int pos[4];
+        pos[0] = 0;
+        for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
+        const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
                                  {mx, my, mx, my}, {mx, mx, my, my}};
-  for (int q = 0; q < 4; q++)
-    for (int e = 0; e < 4; e++) boxes[kid[q]].corner[edit_idx[q][e]] = edit_val[q][e];
-  for (int q = 0; q < 4; q++) boxes[id].child[q] = kid[q];
-  const std::vector<int>& dofs = boxes[id].original;
-  for (int q = 0; q < 4; q++) boxes[kid[q]].original.reserve(dofs.size() / 2);
-  for (size_t t = 0; t < dofs.size(); t += sol_dim_) {
-    const int d = dofs[t];
-    const int p = d / sol_dim_;
-    const int q = pick_child(boxes[id], pts_[2 * p], pts_[2 * p + 1]);
-    for (int s = 0; s < sol_dim_; s++) boxes[kid[q]].original.push_back(d + s);
+        for (int q = 0; q < 4; q++) {
+          Tmp& C = tb[base + 4 * s + q];
+          C.parent = split[s];
+          C.level = P.level + 1;
+          C.begin = P.begin + pos[q];
+          C.count = cnt[q];
+          std::memcpy(C.corner, P.corner, sizeof(C.corner));
+          for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
+          P.child[q] = base + 4 * s + q;
+        }
+        // stable scatter: the copied list holds the old order
+        const std::vector<int>& old = split_pts[sbase + s];
+        for (int i = 0; i < P.count; i++) rp[pos[rq[i]]++] = old[i];
+      }
+    });
+    frontier.clear();
+    for (size_t i = base; i < tb.size(); i++) frontier.push_back(static_cast<int>(i));
   }
-  for (int q = 0; q < 4; q++)
-    if (static_cast<int>(boxes[kid[q]].original.size()) > max_leaf_) subdivide(kid[q]);
-}
-
-void QuadTreeHost::insert(int id, double x, double y, int pt) {
-  // quadtree.cpp:164-197: the point's dofs join every box on its path; the
-  // leaf it reaches splits once it holds more than max_leaf dofs.  Here
-  // only the leaf's list grows; the lists of boxes that were already split
-  // are completed once at the end (fill_internal_lists), which gives the
-  // same lists because points arrive in index order.
-  for (;;) {
-    Box& b = boxes[id];
-    const int ch = b.child[pick_child(b, x, y)];
-    if (ch >= 0) {
-      id = ch;
-      continue;
-    }
-    for (int s = 0; s < sol_dim_; s++) b.original.push_back(sol_dim_ * pt + s);
-    if (b.leaf && static_cast<int>(b.original.size()) > max_leaf_) subdivide(id);
-    return;
-  }
-}
-
-void QuadTreeHost::fill_internal_lists() {
-  // Every internal box holds the dofs of all points in it in insertion
-  // (= index) order: the merge of its children's sorted lists, built from
-  // the deepest level up.
-  std::vector<int> tmp;
-  for (int l = static_cast<int>(levels.size()) - 1; l >= 0; l--) {
-    for (int id : levels[l]) {
-      Box& b = boxes[id];
-      if (b.leaf) continue;
-      const std::vector<int>& c0 = boxes[b.child[0]].original;
-      const std::vector<int>& c1 = boxes[b.child[1]].original;
-      const std::vector<int>& c2 = boxes[b.child[2]].original;
-      const std::vector<int>& c3 = boxes[b.child[3]].original;
-      tmp.resize(c0.size() + c1.size());
-      std::merge(c0.begin(), c0.end(), c1.begin(), c1.end(), tmp.begin());
-      std::vector<int> t2(c2.size() + c3.size());
-      std::merge(c2.begin(), c2.end(), c3.begin(), c3.end(), t2.begin());
-      b.original.resize(tmp.size() + t2.size());
-      std::merge(tmp.begin(), tmp.end(), t2.begin(), t2.end(), b.original.begin());
+  // split moments: s(B) = max(index of B's (cap+1)-th point, s(parent));
+  // depth-first positions from an explicit pre-order walk
+  const int nt = static_cast<int>(tb.size());
+  std::vector<long long> when(nt, -1);
+  std::vector<int> pre(nt, 0);
+  {
+    std::vector<int> stack{0};
+    int counter = 0;
+    while (!stack.empty()) {
+      const int id = stack.back();
+      stack.pop_back();
+      pre[id] = counter++;
+      for (int q = 3; q >= 0; q--)
+        if (tb[id].child[q] >= 0) stack.push_back(tb[id].child[q]);
     }
   }
+  std::vector<int> splits;
+  for (int id = 0; id < nt; id++) {
+    if (tb[id].child[0] < 0) continue;
+    long long t = split_pts[split_slot[id]][cap];
+    if (tb[id].parent >= 0) t = std::max(t, when[tb[id].parent]);
+    when[id] = t;
+    splits.push_back(id);
+  }
+  std::sort(splits.begin(), splits.end(), [&](int a, int b) {
+    return when[a] != when[b] ? when[a] < when[b] : pre[a] < pre[b];
+  });
+  // number the boxes in creation order and lay them out
+  std::vector<int> idmap(nt, -1);
+  idmap[0] = 0;
+  int next = 1;
+  for (int id : splits)
+    for (int q = 0; q < 4; q++) idmap[tb[id].child[q]] = next++;
+  boxes.assign(nt, Box());
+  std::vector<int> order(nt);
+  for (int id = 0; id < nt; id++) order[idmap[id]] = id;
+  int depth = 0;
+  for (int id = 0; id < nt; id++) depth = std::max(depth, tb[id].level);
+  levels.assign(depth + 1, {});
+  for (int i = 0; i < nt; i++) levels[tb[order[i]].level].push_back(i);
+  const double side0 = hi - lo;
+  parallel_for(nt, 64, [&](int a, int e) {
+    for (int id = a; id < e; id++) {
+      const Tmp& t = tb[id];
+      Box& b = boxes[idmap[id]];
+      b.tree = tree_id;
+      b.level = t.level;
+      b.parent = t.parent >= 0 ? idmap[t.parent] : -1;
+      b.leaf = t.child[0] < 0;
+      for (int q = 0; q < 4; q++) b.child[q] = t.child[q] >= 0 ? idmap[t.child[q]] : -1;
+      std::memcpy(b.corner, t.corner, sizeof(b.corner));
+      double sd = side0;
+      for (int l = 0; l < t.level; l++) sd /= 2.0;
+      b.side = sd;
+      b.original.resize(static_cast<size_t>(t.count) * sol_dim_);
+      const int* src = split_slot[id] >= 0 ? split_pts[split_slot[id]].data() : perm.data() + t.begin;
+      for (int i = 0; i < t.count; i++)
+        for (int c = 0; c < sol_dim_; c++)
+          b.original[static_cast<size_t>(i) * sol_dim_ + c] = sol_dim_ * src[i] + c;
+    }
+  });
 }
 
-void QuadTreeHost::descendant_neighbors(int big, int small) {
-  // quadtree.cpp:119-161, including its "y < top && y < bottom" side test.
+void QuadTreeHost::descendant_neighbors(int big, int small, std::vector<int>* found) const {
+  // quadtree.cpp:119-161, including its "y < top && y < bottom" side test:
+  // every descendant of `small` with a corner on an edge of `big`, in
+  // depth-first order.
   const double top = boxes[big].corner[3], bottom = boxes[big].corner[1];
   const double left = boxes[big].corner[0], right = boxes[big].corner[4];
+  // The corners of `small` and of all its descendants lie in small's closed
+  // square; when no point of that square can pass either side test below,
+  // the whole subtree is skipped (a widened 1e-12 band keeps the skip
+  // conservative, so the result is unchanged).
+  {
+    const double sx0 = boxes[small].corner[0], sx1 = boxes[small].corner[4];
+    const double sy0 = boxes[small].corner[1], sy1 = boxes[small].corner[3];
+    const double eps = 1e-12;
+    const bool xin = sx0 < right && sx1 > left;
+    const bool horiz = xin && ((sy0 < top + eps && sy1 > top - eps) ||
+                               (sy0 < bottom + eps && sy1 > bottom - eps));
+    const bool vert = sy0 < bottom && ((sx0 < left + eps && sx1 > left - eps) ||
+                                       (sx0 < right + eps && sx1 > right - eps));
+    if (!horiz && !vert) return;
+  }
   for (int q = 0; q < 8; q += 2) {
     const double x = boxes[small].corner[q], y = boxes[small].corner[q + 1];
     const bool horiz = x > left && x < right &&
@@ -115,44 +199,60 @@ void QuadTreeHost::descendant_neighbors(int big, int small) {
     const bool vert = y < top && y < bottom &&
                       (std::fabs(x - left) < 1e-14 || std::fabs(x - right) < 1e-14);
     if (horiz || vert) {
-      boxes[big].nbr.push_back(small);
-      boxes[small].nbr.push_back(big);
+      found->push_back(small);
       break;
     }
   }
   for (int q = 0; q < 4; q++)
-    if (boxes[small].child[q] >= 0) descendant_neighbors(big, boxes[small].child[q]);
+    if (boxes[small].child[q] >= 0) descendant_neighbors(big, boxes[small].child[q], found);
 }
 
 void QuadTreeHost::neighbor_lists() {
-  // quadtree.cpp:27-69: siblings, same-level cousins whose lower-left corners
-  // lie within side*sqrt(2), then (for leaves) adjacent finer boxes.
+  // quadtree.cpp:27-69, level by level: a box's neighbours are the coarser
+  // leaves that found it (appended while their own level was processed),
+  // then its siblings, its same-level cousins whose lower-left corners lie
+  // within side*sqrt(2), and (for leaves) the adjacent finer boxes, each of
+  // which also records the leaf.  The per-box searches of a level only read
+  // finished lists, so they run in parallel; the appends are made in the
+  // level's box order, as the reference makes them.
   for (size_t l = 0; l < levels.size(); l++) {
-    for (int a : levels[l]) {
-      const int par = boxes[a].parent;
-      if (par >= 0) {
-        for (int q = 0; q < 4; q++)
-          if (boxes[par].child[q] != a) boxes[a].nbr.push_back(boxes[par].child[q]);
-        const std::vector<int>& pn = boxes[par].nbr;  // not modified below
-        for (int o : pn) {
-          for (int q = 0; q < 4; q++) {
-            const int cz = boxes[o].child[q];
-            if (cz < 0 || boxes[cz].level != boxes[a].level) continue;
-            const double dist =
-                std::sqrt(std::pow(boxes[a].corner[0] - boxes[cz].corner[0], 2) +
-                          std::pow(boxes[a].corner[1] - boxes[cz].corner[1], 2));
-            if (dist < boxes[a].side * std::sqrt(2) + 1e-5) boxes[a].nbr.push_back(cz);
+    const std::vector<int>& ids = levels[l];
+    const int n = static_cast<int>(ids.size());
+    std::vector<std::vector<int>> near(n), found(n);
+    parallel_for(n, 8, [&](int b0, int b1) {
+      for (int i = b0; i < b1; i++) {
+        const int a = ids[i];
+        const int par = boxes[a].parent;
+        std::vector<int>& nr = near[i];
+        if (par >= 0) {
+          for (int q = 0; q < 4; q++)
+            if (boxes[par].child[q] != a) nr.push_back(boxes[par].child[q]);
+          for (int o : boxes[par].nbr) {
+            for (int q = 0; q < 4; q++) {
+              const int cz = boxes[o].child[q];
+              if (cz < 0 || boxes[cz].level != boxes[a].level) continue;
+              // (squares by multiplication: the corner distances are 0,
+              // side, sqrt(2) side, ..., far from the 1e-5 margin, so the
+              // outcome is that of the reference's pow form)
+              const double dx = boxes[a].corner[0] - boxes[cz].corner[0];
+              const double dy = boxes[a].corner[1] - boxes[cz].corner[1];
+              const double dist = std::sqrt(dx * dx + dy * dy);
+              if (dist < boxes[a].side * std::sqrt(2) + 1e-5) nr.push_back(cz);
+            }
           }
         }
+        if (boxes[a].leaf)
+          for (int o : nr)  // all of the same level
+            for (int q = 0; q < 4; q++)
+              if (boxes[o].child[q] >= 0) descendant_neighbors(a, boxes[o].child[q], &found[i]);
       }
-      if (boxes[a].leaf) {
-        for (size_t t = 0; t < boxes[a].nbr.size(); t++) {
-          const int o = boxes[a].nbr[t];
-          if (boxes[o].level != boxes[a].level) continue;
-          for (int q = 0; q < 4; q++)
-            if (boxes[o].child[q] >= 0) descendant_neighbors(a, boxes[o].child[q]);
-        }
-      }
+    });
+    for (int i = 0; i < n; i++) {
+      const int a = ids[i];
+      std::vector<int>& nb = boxes[a].nbr;
+      nb.insert(nb.end(), near[i].begin(), near[i].end());
+      nb.insert(nb.end(), found[i].begin(), found[i].end());
+      for (int sm : found[i]) boxes[sm].nbr.push_back(a);
     }
   }
 }
@@ -164,8 +264,7 @@ void QuadTreeHost::build(const double* points, int n, int sol_dim,
 
 void QuadTreeHost::build_one(int p0, int p1, int tree_id) {
   // quadtree.cpp:72-114: root square [min - 0.01, max + 0.01]^2 over all
-  // of the tree's coordinates, its points inserted in order, then the
-  // neighbour lists.
+  // of the tree's coordinates, then the partition and the neighbour lists.
   double lo_v = pts_[2 * static_cast<size_t>(p0)], hi_v = lo_v;
   for (size_t i = 2 * static_cast<size_t>(p0); i < 2 * static_cast<size_t>(p1); i++) {
     if (pts_[i] < lo_v) lo_v = pts_[i];
@@ -173,19 +272,7 @@ void QuadTreeHost::build_one(int p0, int p1, int tree_id) {
   }
   min_ = lo_v;
   max_ = hi_v;
-  const double lo = lo_v - 0.01, hi = hi_v + 0.01;
-  boxes.clear();
-  levels.clear();
-  boxes.reserve(4 * (static_cast<size_t>(p1 - p0) * sol_dim_ / std::max(1, max_leaf_)) + 16);
-  Box root;
-  root.tree = tree_id;
-  const double c[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
-  std::memcpy(root.corner, c, sizeof(c));
-  root.side = hi - lo;
-  boxes.push_back(root);
-  levels.push_back({0});
-  for (int q = p0; q < p1; q++) insert(0, pts_[2 * q], pts_[2 * q + 1], q);
-  fill_internal_lists();
+  build_partition(p0, p1, tree_id, lo_v - 0.01, hi_v + 0.01);
   neighbor_lists();
 }
 

@@ -58,10 +58,8 @@ class QuadTreeHost {
 
  private:
   int pick_child(const Box& b, double x, double y) const;
-  void subdivide(int b);
-  void insert(int b, double x, double y, int pt);
-  void fill_internal_lists();
-  void descendant_neighbors(int big, int small);
+  void build_partition(int p0, int p1, int tree_id, double lo, double hi);
+  void descendant_neighbors(int big, int small, std::vector<int>* found) const;
   void neighbor_lists();
 
   int sol_dim_ = 1;

@@ -43,6 +43,14 @@ def cases():
             pr = G.Problem("%s_%s_1024" % (kind, "laplace" if pde == 0 else "stokes"), pde,
                            pts, nrm, kap, w, holes, f, tg, np.zeros(0), 16, 1e-6)
             out.append((pr.name, pr, 1e-6, 32))
+        # the reference's Laplace-Neumann tests use all-ones data
+        # (kern_interp_test.cpp:109-206, boundary.cpp:56-58); holes get no
+        # border for this kernel (kern_interp_test.cpp:39-40)
+        pts, nrm, kap, w, holes = G.reference_shape(kind, 1024)
+        pr = G.Problem("%s_neumann_1024" % kind, G.LAPLACE_NEUMANN, pts, nrm, kap, w, holes,
+                       np.ones(pts.size // 2), np.array([0.5, 0.52, 0.47, 0.55]), np.zeros(0),
+                       16, 1e-6)
+        out.append((pr.name, pr, 1e-6, 32))
     return out
 
 
