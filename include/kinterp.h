@@ -149,6 +149,39 @@ int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets,
 int ki_eval_targets_device(ki_solver_t s, int n_targets, const double* d_targets,
                            const double* d_mu, const double* d_alpha, double* d_out);
 
+/* boundary_integral_solve's evaluation on domain points
+ * (linear_solve.cpp:142-180): out = K_domain mu + U_forward alpha, set to
+ * zero at every point outside the domain.  The domain test `kind`:
+ *   KI_DOMAIN_ALL    no test (every point kept);
+ *   KI_DOMAIN_NODES  CubicBoundary::is_in_domain (cubic_boundary.cpp:182-230)
+ *                    on the handle's node curves (outer nodes first, then
+ *                    each hole's nodes): outside within 1e-2 of a node, or
+ *                    by the crossing counts of the outer curve and holes;
+ *   KI_DOMAIN_DISK   Circle / Annulus / Donut::is_in_domain (circle.cpp:34-42,
+ *                    annulus.cpp:66-79, donut.cpp:67-80) with disk = host
+ *                    {cx, cy, R}: outside when |x - c| + 1e-2 > R or within
+ *                    1e-2 of a hole's circle or inside it.
+ * Entries are formed on the fly (no |targets| x N matrix); the sums agree
+ * with the exact entries to FP64 rounding.  Points exactly on a node get
+ * no contribution from that node (such points are outside every test).
+ * Device variant: targets (interleaved xy), mu, alpha, out on the device,
+ * stream-ordered; host variant copies in and out and returns when out is
+ * in host memory. */
+enum { KI_DOMAIN_ALL = 0, KI_DOMAIN_NODES = 1, KI_DOMAIN_DISK = 2 };
+int ki_eval_domain_device(ki_solver_t s, int n_targets, const double* d_targets,
+                          const double* d_mu, const double* d_alpha, int kind, const double* disk,
+                          double* d_out);
+int ki_eval_domain(ki_solver_t s, int n_targets, const double* targets, const double* mu,
+                   const double* alpha, int kind, const double* disk, double* out);
+/* The domain test alone: d_mask[t] = 1 inside, 0 outside (kind NODES or DISK). */
+int ki_domain_mask_device(ki_solver_t s, int n_targets, const double* d_targets, int kind,
+                          const double* disk, unsigned char* d_mask);
+/* get_domain_points (linear_solve.cpp:183-193): domain_size^2 points,
+ * x = x_min + i/(domain_size-1) (x_max - x_min) in the outer loop and y
+ * likewise in the inner loop, interleaved xy into points (2 domain_size^2). */
+int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, double y_max,
+                     double* points);
+
 /* Kernel::operator() (kernel/kernel.cpp:99-111): column-major nt x ns block
  * K(tgt, src) evaluated on the GPU. */
 int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src,

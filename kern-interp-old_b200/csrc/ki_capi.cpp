@@ -424,6 +424,88 @@ int ki_eval_targets(ki_solver_t s, int n_targets, const double* targets, const d
   return cuda_err(cudaStreamSynchronize(s->stream), "ki_eval_targets");
 }
 
+static int domain_args(ki_solver_t s, int n_targets, int kind, const double* disk,
+                       const char* who) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || n_targets < 0)
+    return set_err(KI_ERR_ARG, std::string(who) + ": bad args");
+  if (kind != KI_DOMAIN_ALL && kind != KI_DOMAIN_NODES && kind != KI_DOMAIN_DISK)
+    return set_err(KI_ERR_ARG, std::string(who) + ": unknown domain test");
+  if (kind == KI_DOMAIN_DISK && !disk)
+    return set_err(KI_ERR_ARG, std::string(who) + ": the disk test needs {cx, cy, R}");
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, std::string(who) + ": not available for a batch of problems");
+  return KI_OK;
+}
+
+int ki_eval_domain_device(ki_solver_t s, int n_targets, const double* d_targets,
+                          const double* d_mu, const double* d_alpha, int kind, const double* disk,
+                          double* d_out) {
+  KI_TRY(domain_args(s, n_targets, kind, disk, "ki_eval_domain_device"));
+  if (n_targets == 0) return KI_OK;
+  if (!d_targets || !d_mu || !d_out)
+    return set_err(KI_ERR_ARG, "ki_eval_domain_device: bad args");
+  return from_solver(s, s->solver->eval_domain(n_targets, d_targets, d_mu, d_alpha, kind, disk,
+                                               d_out));
+}
+
+int ki_domain_mask_device(ki_solver_t s, int n_targets, const double* d_targets, int kind,
+                          const double* disk, unsigned char* d_mask) {
+  KI_TRY(domain_args(s, n_targets, kind, disk, "ki_domain_mask_device"));
+  if (kind == KI_DOMAIN_ALL)
+    return set_err(KI_ERR_ARG, "ki_domain_mask_device: needs KI_DOMAIN_NODES or KI_DOMAIN_DISK");
+  if (n_targets == 0) return KI_OK;
+  if (!d_targets || !d_mask) return set_err(KI_ERR_ARG, "ki_domain_mask_device: bad args");
+  return from_solver(s, s->solver->domain_mask(n_targets, d_targets, kind, disk, d_mask));
+}
+
+int ki_eval_domain(ki_solver_t s, int n_targets, const double* targets, const double* mu,
+                   const double* alpha, int kind, const double* disk, double* out) {
+  KI_TRY(domain_args(s, n_targets, kind, disk, "ki_eval_domain"));
+  if (n_targets == 0) return KI_OK;
+  if (!targets || !mu || !out) return set_err(KI_ERR_ARG, "ki_eval_domain: bad args");
+  kib::Solver& sv = *s->solver;
+  const int N = sv.n_dofs(), nb = sv.n_border(), sd = sv.sol_dim();
+  const bool use_alpha = nb > 0 && alpha;
+  const size_t need = static_cast<size_t>(N) + nb + 2 * static_cast<size_t>(n_targets) +
+                      static_cast<size_t>(sd) * n_targets;
+  KI_TRY(staging(s, sizeof(double) * need));
+  double* d_mu = s->d_io;
+  double* d_al = d_mu + N;
+  double* d_tg = d_al + nb;
+  double* d_out = d_tg + 2 * static_cast<size_t>(n_targets);
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_mu, mu, sizeof(double) * N, cudaMemcpyHostToDevice, s->stream),
+                  "copy mu"));
+  if (use_alpha)
+    KI_TRY(cuda_err(cudaMemcpyAsync(d_al, alpha, sizeof(double) * nb, cudaMemcpyHostToDevice,
+                                    s->stream),
+                    "copy alpha"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_tg, targets, sizeof(double) * 2 * n_targets,
+                                  cudaMemcpyHostToDevice, s->stream),
+                  "copy targets"));
+  KI_TRY(from_solver(s, sv.eval_domain(n_targets, d_tg, d_mu, use_alpha ? d_al : nullptr, kind,
+                                       disk, d_out)));
+  KI_TRY(cuda_err(cudaMemcpyAsync(out, d_out, sizeof(double) * sd * n_targets,
+                                  cudaMemcpyDeviceToHost, s->stream),
+                  "copy out"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_eval_domain");
+}
+
+int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, double y_max,
+                     double* points) {
+  if (domain_size < 0 || (domain_size > 0 && !points))
+    return set_err(KI_ERR_ARG, "ki_domain_points: bad args");
+  size_t k = 0;
+  for (int i = 0; i < domain_size; i++) {
+    const double x = x_min + ((i + 0.0) / (domain_size - 1)) * (x_max - x_min);
+    for (int j = 0; j < domain_size; j++) {
+      points[k++] = x;
+      points[k++] = y_min + ((j + 0.0) / (domain_size - 1)) * (y_max - y_min);
+    }
+  }
+  return KI_OK;
+}
+
 int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src, double* out) {
   if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
   if (!s || !s->solver || nt < 0 || ns < 0 || (nt * ns > 0 && (!tgt || !src || !out)))

@@ -2,16 +2,32 @@
 // linear_solve.cpp:142-180): the split choice, the scratch for the split
 // partials and the mask, and the launches of ki_domain.cu.
 #include <algorithm>
+#include <vector>
 
 #include "ki_solver.h"
 
 namespace kib {
+
+namespace {
+// The node-curve test walks the outer nodes and then each hole's nodes:
+// the hole node counts must be non-negative and fit in the node array.
+bool curves_fit(const std::vector<double>& holes, int n_points) {
+  double used = 0;
+  for (size_t h = 0; h + 3 < holes.size(); h += 4) {
+    if (!(holes[h + 3] >= 0)) return false;
+    used += holes[h + 3];
+  }
+  return used <= n_points;
+}
+}  // namespace
 
 int Solver::domain_mask(int nt, const double* d_targets, int kind, const double* disk,
                         unsigned char* d_mask) {
   if (kind != kDomainNodes && kind != kDomainDisk) return fail("domain_mask: unknown test");
   if (kind == kDomainDisk && !disk) return fail("domain_mask: the disk test needs {cx, cy, R}");
   if (n_trees() > 1) return fail("domain_mask: not available for a batch of problems");
+  if (kind == kDomainNodes && !curves_fit(holes_, n_points_))
+    return fail("domain_mask: hole node counts exceed the number of nodes");
   KI_CUDA(launch_domain_mask(kind, d_nodes_, n_points_, d_holes_, n_holes(), disk, nt, d_targets,
                              d_mask, stream_));
   return 0;
@@ -23,6 +39,8 @@ int Solver::eval_domain(int nt, const double* d_targets, const double* d_mu,
     return fail("eval_domain: unknown domain test");
   if (kind == kDomainDisk && !disk) return fail("eval_domain: the disk test needs {cx, cy, R}");
   if (n_trees() > 1) return fail("eval_domain: not available for a batch of problems");
+  if (kind == kDomainNodes && !curves_fit(holes_, n_points_))
+    return fail("eval_domain: hole node counts exceed the number of nodes");
   if (nt == 0) return 0;
   if (!num_sms_) {
     int dev = 0;

@@ -74,6 +74,13 @@ def load():
     lib.ki_solve_refined_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_double, C.c_int, _ip, _dp]
     lib.ki_eval_targets.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
+    lib.ki_eval_domain.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, _dp, _dp]
+    lib.ki_eval_domain_device.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
+                                          [C.c_int, _dp, C.c_void_p])
+    lib.ki_domain_mask_device.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, _dp,
+                                          C.c_void_p]
+    lib.ki_domain_points.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                     _dp]
     lib.ki_kernel_block.argtypes = [C.c_void_p, C.c_int, _ip, C.c_int, _ip, _dp]
     lib.ki_box_info.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _dp]
     lib.ki_box_lists.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _ip, _ip]
@@ -105,6 +112,28 @@ def _f64(a):
 def _check(rc, what):
     if rc != 0:
         raise KiError("%s failed (%d): %s" % (what, rc, load().ki_last_error().decode()))
+
+
+DOMAIN_KINDS = {"all": 0, "nodes": 1, "disk": 2}
+
+
+def _domain(kind, disk):
+    k = DOMAIN_KINDS[kind]
+    dk = None
+    if k == 2:
+        if disk is None:
+            raise ValueError("the disk test needs disk=(cx, cy, R)")
+        dk = np.ascontiguousarray(disk, dtype=np.float64)
+    return k, dk
+
+
+def domain_points(domain_size, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0):
+    """get_domain_points (linear_solve.cpp:183-193): a domain_size^2 grid,
+    x in the outer loop, interleaved xy."""
+    out = np.zeros(2 * domain_size * domain_size)
+    _check(load().ki_domain_points(domain_size, x_min, x_max, y_min, y_max, _d(out)),
+           "ki_domain_points")
+    return out
 
 
 class _Tree:
@@ -264,6 +293,35 @@ class Solver(_Tree):
                                         _d(out)), "ki_eval_targets")
         return out
 
+    def eval_domain(self, targets, mu, alpha=None, domain="nodes", disk=None):
+        """boundary_integral_solve's evaluation (linear_solve.cpp:142-180):
+        the solution at the points, zero outside the domain.  domain:
+        "nodes" (CubicBoundary::is_in_domain on the node curves), "disk"
+        (Circle / Annulus / Donut::is_in_domain with disk = (cx, cy, R)) or
+        "all" (no test)."""
+        k, dk = _domain(domain, disk)
+        targets = _f64(targets)
+        nt = targets.size // 2
+        out = np.zeros(nt * self.problem.sol_dim)
+        al = _f64(alpha) if alpha is not None and len(alpha) else None
+        _check(self.lib.ki_eval_domain(self.h, nt, _d(targets), _d(_f64(mu)), _d(al), k, _d(dk),
+                                       _d(out)), "ki_eval_domain")
+        return out
+
+    def eval_domain_device(self, n_targets, tg_ptr, mu_ptr, alpha_ptr, out_ptr, domain="nodes",
+                           disk=None):
+        k, dk = _domain(domain, disk)
+        _check(self.lib.ki_eval_domain_device(self.h, n_targets, C.c_void_p(tg_ptr),
+                                              C.c_void_p(mu_ptr),
+                                              C.c_void_p(alpha_ptr) if alpha_ptr else None, k,
+                                              _d(dk), C.c_void_p(out_ptr)),
+               "ki_eval_domain_device")
+
+    def domain_mask_device(self, n_targets, tg_ptr, mask_ptr, domain="nodes", disk=None):
+        k, dk = _domain(domain, disk)
+        _check(self.lib.ki_domain_mask_device(self.h, n_targets, C.c_void_p(tg_ptr), k, _d(dk),
+                                              C.c_void_p(mask_ptr)), "ki_domain_mask_device")
+
     def kernel_block(self, tgt, src):
         tgt = np.ascontiguousarray(tgt, dtype=np.int32)
         src = np.ascontiguousarray(src, dtype=np.int32)
@@ -382,3 +440,17 @@ class BatchSolver(_Tree):
 
     def stats(self):
         return Solver.stats(self)
+
+
+def boundary_integral_solve(problem, domain_pts, id_tol=None, max_leaf_dofs=None,
+                            domain="nodes", disk=None):
+    """boundary_integral_solve (linear_solve.cpp:142-180): factor the
+    problem's boundary operator, solve for mu (and alpha with holes) with the
+    problem's boundary data, and return the solution at domain_pts
+    (interleaved xy), zero outside the domain (see Solver.eval_domain)."""
+    s = Solver(problem, id_tol=id_tol, max_leaf_dofs=max_leaf_dofs)
+    try:
+        mu, alpha = s.solve(problem.f)
+        return s.eval_domain(domain_pts, mu, alpha if s.n_border else None, domain, disk)
+    finally:
+        s.close()

@@ -154,6 +154,14 @@ def ref_available():
     return os.path.exists(REF_SO)
 
 
+def ref_lib():
+    """The reference library (loaded once)."""
+    global _ref_lib
+    if _ref_lib is None:
+        _ref_lib = C.CDLL(REF_SO)
+    return _ref_lib
+
+
 class RefSolver(_Common):
     """The reference solver (oracle/_ref/libkiref.so)."""
 

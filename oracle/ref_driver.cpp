@@ -11,7 +11,10 @@
 #include <memory>
 #include <vector>
 
+#include "kern_interp/boundaries/annulus.h"
 #include "kern_interp/boundaries/boundary.h"
+#include "kern_interp/boundaries/circle.h"
+#include "kern_interp/boundaries/donut.h"
 #include "kern_interp/kernel/kernel.h"
 #include "kern_interp/linear_solve.h"
 #include "kern_interp/quadtree/quadtree.h"
@@ -29,6 +32,18 @@ class ArrayBoundary : public Boundary {
   bool is_in_domain(const Vec2&) const override { return true; }
   std::unique_ptr<Boundary> clone() const override {
     return std::make_unique<ArrayBoundary>(*this);
+  }
+};
+
+// A CubicBoundary whose node arrays are given by the caller, so the
+// reference's own CubicBoundary::is_in_domain (cubic_boundary.cpp:182-230)
+// runs on them.
+class ArrayCubic : public CubicBoundary {
+ public:
+  void initialize(int, BoundaryCondition) override {}
+  void get_spline_points(std::vector<double>*, std::vector<double>*) override {}
+  std::unique_ptr<Boundary> clone() const override {
+    return std::make_unique<ArrayCubic>(*this);
   }
 };
 
@@ -214,5 +229,40 @@ int kiref_allskel(void* hp, int* out) {
   auto& v = h->tree.root->dof_lists.active_box;
   if (out && !v.empty()) std::memcpy(out, v.data(), sizeof(int) * v.size());
   return static_cast<int>(v.size());
+}
+
+// Boundary::is_in_domain of the reference's classes for nt points
+// (interleaved xy): kind 0 CubicBoundary on the given nodes (outer nodes
+// first, then the holes' nodes), 1 Circle, 2 Annulus, 3 Donut (their
+// analytic tests with the given holes).  out[t] = 1 inside, 0 outside.
+void kiref_in_domain(int kind, int n_points, const double* points, int n_holes,
+                     const double* holes, int nt, const double* targets,
+                     unsigned char* out) {
+  std::unique_ptr<Boundary> b;
+  if (kind == 1) b.reset(new Circle());
+  else if (kind == 2) b.reset(new Annulus());
+  else if (kind == 3) b.reset(new Donut());
+  else b.reset(new ArrayCubic());
+  b->points.assign(points, points + 2 * n_points);
+  int outer = n_points;
+  for (int i = 0; i < n_holes; i++) {
+    Hole hole;
+    hole.center = Vec2(holes[4 * i], holes[4 * i + 1]);
+    hole.radius = holes[4 * i + 2];
+    hole.num_nodes = static_cast<int>(holes[4 * i + 3]);
+    outer -= hole.num_nodes;
+    b->holes.push_back(hole);
+  }
+  b->num_outer_nodes = outer;
+  for (int t = 0; t < nt; t++)
+    out[t] = b->is_in_domain(Vec2(targets[2 * t], targets[2 * t + 1])) ? 1 : 0;
+}
+
+// get_domain_points (linear_solve.cpp:183-193) into points (2 size^2).
+void kiref_domain_points(int domain_size, double x_min, double x_max, double y_min,
+                         double y_max, double* points) {
+  std::vector<double> v;
+  get_domain_points(domain_size, &v, x_min, x_max, y_min, y_max);
+  if (!v.empty()) std::memcpy(points, v.data(), sizeof(double) * v.size());
 }
 }
