@@ -237,6 +237,33 @@ int ki_factor_ex(int pde, int n_points, const double* points, const double* norm
                  const double* holes, int max_leaf_dofs, double id_tol, int mode, int timed,
                  void* stream, ki_solver_t* out);
 
+/* QuadTree::perturb (quadtree/quadtree.cpp:359-560) followed by
+ * SkelFactorization::skeletonize (skel_factorization.cpp:94-243), as the
+ * reference's boundary-update loops run them (kern_interp_test.cpp:491-530,
+ * experiment_two.cpp:55-60): the handle follows its boundary to new node
+ * arrays (any number of points; holes as in ki_factor).  Points are matched
+ * to the old ones by exact coordinates.  Leaves that gain or lose points,
+ * their neighbours, their ancestors and the ancestors' neighbours are
+ * factored again, over-full leaves are split and sparse subtrees merged;
+ * every other compressed box keeps its factors (its dofs renumbered).
+ * n_reused (may be NULL) receives the number of boxes kept.  One problem
+ * per handle (not a batch).  On failure the handle is unusable. */
+int ki_update(ki_solver_t s, int n_points, const double* points, const double* normals,
+              const double* curvatures, const double* weights, int n_holes, const double* holes,
+              int* n_reused);
+
+/* The partition half of QuadTree::perturb on a ki_partition handle (no
+ * GPU): the tree follows its points to new ones exactly as ki_update's does. */
+int ki_partition_update(ki_solver_t s, int n_points, const double* points);
+
+/* QuadTree::copy_into (quadtree/quadtree.cpp:584-641) followed by
+ * skeletonize, as kern_interp_test.cpp:533-567 runs them: a new handle on
+ * `stream` (NULL: its own) with a copy of the tree and of every compressed
+ * box's factors; only the boxes without compression and the top level are
+ * factored again, so its solves equal this handle's.  The two handles are
+ * independent afterwards (ki_update on one leaves the other as it is). */
+int ki_copy(ki_solver_t s, void* stream, ki_solver_t* out);
+
 /* Many independent problems factored together (no reference counterpart:
  * the reference factors one boundary per QuadTree).  Problem p has
  * n_points[p] nodes; the geometry arrays are the problems' arrays laid end

@@ -188,4 +188,18 @@ cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int 
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void copy_segments_kernel(const CopySeg* __restrict__ segs) {
+  const CopySeg sg = segs[blockIdx.x];
+  for (long long i = threadIdx.x; i < sg.words; i += blockDim.x) sg.dst[i] = sg.src[i];
+}
+}  // namespace
+
+cudaError_t launch_copy_segments(const CopySeg* segs, int n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  count_launches(1);
+  copy_segments_kernel<<<n, 256, 0, s>>>(segs);
+  return cudaGetLastError();
+}
+
 }  // namespace kib

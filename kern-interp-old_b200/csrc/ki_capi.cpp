@@ -208,6 +208,17 @@ int ki_partition(int n_points, const double* points, int sol_dim, int max_leaf_d
   return KI_OK;
 }
 
+int ki_partition_update(ki_solver_t s, int n_points, const double* points) {
+  if (!s || !s->solver || !s->tree_only)
+    return set_err(KI_ERR_ARG, "ki_partition_update: needs a ki_partition handle");
+  if (n_points <= 0 || !points)
+    return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, "ki_partition_update: not available for a batch of problems");
+  s->solver->perturb_tree_only(n_points, points);
+  return KI_OK;
+}
+
 int ki_partition_batch(int n_problems, const int* n_points, const double* points, int sol_dim,
                        int max_leaf_dofs, ki_solver_t* out) {
   if (!out) return set_err(KI_ERR_ARG, "ki_partition_batch: out is NULL");
@@ -238,6 +249,44 @@ int ki_partition_batch(int n_problems, const int* n_points, const double* points
   h->solver->set_forest(starts);
   h->solver->build_tree_only();
   h->tree_only = true;
+  *out = h.release();
+  return KI_OK;
+}
+
+int ki_update(ki_solver_t s, int n_points, const double* points, const double* normals,
+              const double* curvatures, const double* weights, int n_holes, const double* holes,
+              int* n_reused) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver) return set_err(KI_ERR_ARG, "ki_update: bad handle");
+  if (n_points <= 0 || !points || !normals || !curvatures || !weights)
+    return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
+  if (n_holes < 0 || (n_holes > 0 && !holes)) return set_err(KI_ERR_ARG, "ki_update: bad holes");
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, "ki_update: not available for a batch of problems");
+  return from_solver(s, s->solver->update(n_points, points, normals, curvatures, weights,
+                                          n_holes, holes, n_reused));
+}
+
+int ki_copy(ki_solver_t s, void* stream, ki_solver_t* out) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_copy: out is NULL");
+  *out = nullptr;
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver) return set_err(KI_ERR_ARG, "ki_copy: bad handle");
+  if (s->solver->n_trees() > 1)
+    return set_err(KI_ERR_ARG, "ki_copy: not available for a batch of problems");
+  std::unique_ptr<ki_solver_s> h(new (std::nothrow) ki_solver_s());
+  if (!h) return set_err(KI_ERR_ARG, "out of host memory");
+  if (stream) {
+    h->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    KI_TRY(cuda_err(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking),
+                    "cudaStreamCreate"));
+    h->own_stream = true;
+  }
+  int rc = 0;
+  kib::Solver* c = s->solver->copy(h->stream, &rc);
+  if (!c) return set_err(rc == -2 ? KI_ERR_CUDA : KI_ERR_NUMERIC, s->solver->error);
+  h->solver.reset(c);
   *out = h.release();
   return KI_OK;
 }

@@ -262,6 +262,14 @@ cudaError_t launch_domain_eval(int pde, const Node* nodes, int np, int nt,
                                const double* holes, const double* alpha,
                                const unsigned char* mask, int splits, double* part,
                                double* out, cudaStream_t s);
+// Batched device-to-device copy: segment i moves words[i] 32-bit words from
+// src to dst (one CTA per segment).
+struct CopySeg {
+  const unsigned* src;
+  unsigned* dst;
+  long long words;
+};
+cudaError_t launch_copy_segments(const CopySeg* segs, int n, cudaStream_t s);
 // Hole border of a multiply-connected domain (initialize_U_mat /
 // initialize_Psi_mat): U (dofs x nb, column-major), Urow the same U stored
 // dof-major (entry (i, b) at i nb + b), Psi (nb x dofs, column-major, which

@@ -303,13 +303,28 @@ void Solver::build_tree_only() {
     allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
 }
 
-int Solver::factor() {
-  cudaEvent_t ev0, ev1;
-  KI_CUDA(cudaEventCreate(&ev0));
-  KI_CUDA(cudaEventCreate(&ev1));
-  KI_CUDA(cudaEventRecord(ev0, stream_));
+void Solver::perturb_tree_only(int n_points, const double* points) {
+  const std::vector<double> old = pts_;
+  const int n_old = n_points_;
+  n_points_ = n_points;
+  n_dofs_ = n_points * sd_;
+  pts_.assign(points, points + 2 * static_cast<size_t>(n_points));
+  nrm_.assign(2 * static_cast<size_t>(n_points), 0.0);
+  curv_.assign(n_points, 0.0);
+  wts_.assign(n_points, 0.0);
+  tree.perturb(old.data(), n_old, pts_.data(), n_points_);
+  for (int level = static_cast<int>(tree.levels.size()) - 1; level >= 0; level--)
+    tree.refresh_level(level, nullptr);
+  allskel.clear();
+  for (int r : tree.roots)
+    allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
+}
+
+int Solver::begin_factor(cudaEvent_t* ev0) {
+  KI_CUDA(cudaEventCreate(ev0));
+  KI_CUDA(cudaEventRecord(*ev0, stream_));
   host_start_ = now_ms();
-  ev_start_ = ev0;
+  ev_start_ = *ev0;
   host_marks.clear();
   t_id_ms = t_decouple_ms = t_top_ms = 0;
   id_launches = 0;
@@ -343,6 +358,13 @@ int Solver::factor() {
     }
     for (int G = 0; G <= 16; G++) onchip_ok_[G] = it->second[G];
   }
+  return 0;
+}
+
+int Solver::factor() {
+  cudaEvent_t ev0;
+  const int rc = begin_factor(&ev0);
+  if (rc) return rc;
   if (starts_.size() > 1) {
     if (!holes_.empty()) return fail("a forest of problems cannot have holes");
     tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
@@ -350,6 +372,12 @@ int Solver::factor() {
     tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
   }
   boxdev_.assign(tree.boxes.size(), BoxDev{});
+  return finish_factor(ev0);
+}
+
+int Solver::finish_factor(cudaEvent_t ev0) {
+  cudaEvent_t ev1;
+  KI_CUDA(cudaEventCreate(&ev1));
   levels_.assign(tree.levels.size(), LevelFactors{});
   mark(0, 0);
 
@@ -430,7 +458,7 @@ int Solver::factor() {
   return 0;
 }
 
-int Solver::process_level(int level) {
+int Solver::compress_level(int level, std::vector<int>* fresh) {
   const double h0 = now_ms();
   const std::vector<int>& ids = tree.levels[level];
   const int nids = static_cast<int>(ids.size());
@@ -506,8 +534,6 @@ int Solver::process_level(int level) {
   std::vector<Cand> cand;
   for (int q = 0; q < nids; q++)
     if (keep[q]) cand.push_back(std::move(all[q]));
-  LevelFactors& lf = levels_[level];
-  lf.level = level;
   if (cand.empty()) return 0;
   std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.g < b.g; });
 
@@ -788,37 +814,204 @@ int Solver::process_level(int level) {
                 dstream_))
     return -2;
 
-  // ---- sweep descriptors of the level
+  for (int t = 0; t < ncomp; t++) fresh->push_back(cand[comp[t]].box);
+  return 0;
+}
+
+int Solver::process_level(int level) {
+  // boxes compressed before this factorization (kept by an update or a
+  // copy) are skipped by the IDs and join the level's sweeps as they are
+  std::vector<int> boxes;
+  for (int id : tree.levels[level])
+    if (tree.boxes[id].compressed) boxes.push_back(id);
+  const int rc = compress_level(level, &boxes);
+  if (rc) return rc;
+  return level_sweeps(level, boxes, dstream_);
+}
+
+int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s) {
+  // sweep descriptors of the level's compressed boxes
+  LevelFactors& lf = levels_[level];
+  lf.level = level;
+  const int ncomp = static_cast<int>(boxes.size());
+  if (ncomp == 0) return 0;
   std::vector<int> sk, rd;
   std::vector<SweepTask> st(ncomp);
   std::vector<int> sk_off(ncomp), rd_off(ncomp);
   int cap = 0;
   for (int t = 0; t < ncomp; t++) {
-    const Box& b = tree.boxes[cand[comp[t]].box];
+    const Box& b = tree.boxes[boxes[t]];
     sk_off[t] = static_cast<int>(sk.size());
     rd_off[t] = static_cast<int>(rd.size());
     sk.insert(sk.end(), b.skel.begin(), b.skel.end());
     rd.insert(rd.end(), b.redundant.begin(), b.redundant.end());
     cap = std::max(cap, static_cast<int>(b.skel.size() + b.redundant.size()));
-    lf.boxes.push_back(cand[comp[t]].box);
+    lf.boxes.push_back(boxes[t]);
   }
   KI_ALLOC(lf.d_skel, int, sk.size());
   KI_ALLOC(lf.d_red, int, rd.size());
   KI_ALLOC(lf.d_tasks, SweepTask, ncomp);
   for (int t = 0; t < ncomp; t++) {
-    const int box = cand[comp[t]].box;
-    const Box& b = tree.boxes[box];
-    const BoxDev& bd = boxdev_[box];
+    const Box& b = tree.boxes[boxes[t]];
+    const BoxDev& bd = boxdev_[boxes[t]];
     st[t] = SweepTask{b.rank, static_cast<int>(b.redundant.size()), lf.d_skel + sk_off[t],
                       lf.d_red + rd_off[t], bd.T, bd.L, bd.U, bd.X, bd.piv};
   }
-  KI_UPLOAD(lf.d_skel, sk, dstream_);
-  KI_UPLOAD(lf.d_red, rd, dstream_);
-  KI_UPLOAD(lf.d_tasks, st, dstream_);
+  KI_UPLOAD(lf.d_skel, sk, s);
+  KI_UPLOAD(lf.d_red, rd, s);
+  KI_UPLOAD(lf.d_tasks, st, s);
   lf.h_tasks = st;
   lf.ntasks = ncomp;
   lf.cap = cap;
   return 0;
+}
+
+void Solver::drop_device_state() {
+  // everything in the arena except the box factors, which the caller
+  // re-points; lazily built buffers are rebuilt on first use
+  if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+  solve_exec_ = nullptr;
+  g_x_ = nullptr;
+  d_mv_tiles_ = nullptr;
+  n_mv_tiles_ = mv_splits_ = 0;
+  d_seg_ = nullptr;
+  seg_.clear();
+  d_nodes_ = nullptr;
+  d_proxy_dir_ = nullptr;
+  d_holes_ = nullptr;
+  d_status_ = nullptr;
+  d_forest_ = nullptr;
+  d_top_ = nullptr;
+  d_top_piv_ = nullptr;
+  d_allskel_ = d_allred_ = d_red_pos_ = nullptr;
+  d_U_ = d_Psi_ = d_Urow_ = d_Ured_ = d_Pred_ = d_tmp_ = nullptr;
+  all_compressed_ = LevelFactors{};
+  levels_.clear();
+}
+
+int Solver::adopt_factors(const std::vector<int>& boxes, const std::vector<BoxDevView>& src) {
+  std::vector<CopySeg> segs;
+  auto seg = [&](const void* from, void* to, size_t bytes) {
+    if (bytes) segs.push_back(CopySeg{static_cast<const unsigned*>(from),
+                                      static_cast<unsigned*>(to),
+                                      static_cast<long long>(bytes / 4)});
+  };
+  for (size_t i = 0; i < boxes.size(); i++) {
+    const BoxDevView& v = src[i];
+    const size_t k = v.k, r = v.r;
+    BoxDev& bd = boxdev_[boxes[i]];
+    double* fac;
+    KI_ALLOC(fac, double, 3 * k * r + r * r + k * k);
+    KI_ALLOC(bd.piv, int, r);
+    bd.T = fac;
+    bd.L = bd.T + k * r;
+    bd.U = bd.L + k * r;
+    bd.X = bd.U + k * r;
+    bd.acc = bd.X + r * r;
+    seg(v.T, bd.T, sizeof(double) * k * r);
+    seg(v.L, bd.L, sizeof(double) * k * r);
+    seg(v.U, bd.U, sizeof(double) * k * r);
+    seg(v.X, bd.X, sizeof(double) * r * r);
+    seg(v.acc, bd.acc, sizeof(double) * k * k);
+    seg(v.piv, bd.piv, sizeof(int) * r);
+  }
+  if (segs.empty()) return 0;
+  CopySeg* d_segs;
+  KI_ALLOC(d_segs, CopySeg, segs.size());
+  KI_UPLOAD(d_segs, segs, stream_);
+  KI_CUDA(launch_copy_segments(d_segs, static_cast<int>(segs.size()), stream_));
+  return 0;
+}
+
+int Solver::update(int n_points, const double* points, const double* normals,
+                   const double* curvatures, const double* weights, int n_holes,
+                   const double* holes, int* n_reused) {
+  if (n_trees() > 1) return fail("update: not available for a batch of problems");
+  if (tree.boxes.empty()) return fail("update: factor the boundary first");
+  if (n_points <= 0) return fail("number of boundary points to init tree cannot be 0");
+  // nothing queued may still read the memory that is about to be replaced
+  KI_CUDA(cudaStreamSynchronize(stream_));
+  if (dstream_) KI_CUDA(cudaStreamSynchronize(dstream_));
+  cudaEvent_t ev0;
+  int rc = begin_factor(&ev0);
+  if (rc) return rc;
+  const std::vector<double> old_pts = pts_;
+  const int n_old = n_points_;
+  n_points_ = n_points;
+  n_dofs_ = n_points * sd_;
+  pts_.assign(points, points + 2 * static_cast<size_t>(n_points));
+  nrm_.assign(normals, normals + 2 * static_cast<size_t>(n_points));
+  curv_.assign(curvatures, curvatures + n_points);
+  wts_.assign(weights, weights + n_points);
+  holes_.clear();
+  if (n_holes > 0) holes_.assign(holes, holes + 4 * static_cast<size_t>(n_holes));
+  tree.perturb(old_pts.data(), n_old, pts_.data(), n_points_);
+
+  // the boxes that stay compressed keep their factors: copied out of the
+  // old arena into a fresh one, after which the old arena is released
+  std::vector<int> kept;
+  std::vector<BoxDevView> views;
+  for (const std::vector<int>& lv : tree.levels)
+    for (int id : lv)
+      if (tree.boxes[id].compressed) {
+        const BoxDev& bd = boxdev_[id];
+        const Box& b = tree.boxes[id];
+        kept.push_back(id);
+        views.push_back(BoxDevView{bd.T, bd.L, bd.U, bd.X, bd.acc, bd.piv, b.rank,
+                                   static_cast<int>(b.redundant.size())});
+      }
+  Arena old;
+  old.swap(arena_);
+  drop_device_state();
+  std::vector<BoxDev> old_dev;
+  old_dev.swap(boxdev_);
+  boxdev_.assign(tree.boxes.size(), BoxDev{});
+  rc = adopt_factors(kept, views);
+  if (rc) return rc;
+  KI_CUDA(cudaStreamSynchronize(stream_));
+  if (n_reused) *n_reused = static_cast<int>(kept.size());
+  return finish_factor(ev0);
+}
+
+Solver* Solver::copy(cudaStream_t stream, int* rc) {
+  *rc = 0;
+  if (n_trees() > 1 || tree.boxes.empty()) {
+    *rc = fail("copy: needs a factored single problem");
+    return nullptr;
+  }
+  Solver* c = new Solver(opt_, n_points_, pts_.data(), nrm_.data(), curv_.data(), wts_.data(),
+                         n_holes(), holes_.empty() ? nullptr : holes_.data(), stream);
+  c->time_phases = time_phases;
+  cudaEvent_t ev0;
+  int r = c->begin_factor(&ev0);
+  if (!r) {
+    // this solver's queued work must finish before its factors are read
+    // on the other stream
+    r = c->cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  }
+  if (!r) {
+    c->tree = tree;
+    c->boxdev_.assign(tree.boxes.size(), BoxDev{});
+    std::vector<int> kept;
+    std::vector<BoxDevView> views;
+    for (const std::vector<int>& lv : tree.levels)
+      for (int id : lv)
+        if (tree.boxes[id].compressed) {
+          const BoxDev& bd = boxdev_[id];
+          kept.push_back(id);
+          views.push_back(BoxDevView{bd.T, bd.L, bd.U, bd.X, bd.acc, bd.piv, tree.boxes[id].rank,
+                                     static_cast<int>(tree.boxes[id].redundant.size())});
+        }
+    r = c->adopt_factors(kept, views);
+  }
+  if (!r) r = c->finish_factor(ev0);
+  if (r) {
+    error = c->error;
+    *rc = r;
+    delete c;
+    return nullptr;
+  }
+  return c;
 }
 
 int Solver::build_all_compressed() {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "ki_kernels.h"
@@ -40,6 +41,13 @@ class Arena {
   template <class T>
   T* get(size_t count) { return static_cast<T*>(alloc(sizeof(T) * (count ? count : 1))); }
   size_t reserved() const { return reserved_; }
+  void swap(Arena& o) {
+    std::swap(pinned_, o.pinned_);
+    chunks_.swap(o.chunks_);
+    std::swap(cur_, o.cur_);
+    std::swap(left_, o.left_);
+    std::swap(reserved_, o.reserved_);
+  }
 
  private:
   bool pinned_;
@@ -67,6 +75,13 @@ struct SolverOptions {
   // reference, same accuracy class); for factorizations used with the
   // refinement, never for reference-identical results.
   bool sketch_id = false;
+};
+
+// Device factors of one compressed box, for copying between solvers.
+struct BoxDevView {
+  const double *T, *L, *U, *X, *acc;
+  const int* piv;
+  int k, r;
 };
 
 struct LevelFactors {
@@ -102,8 +117,22 @@ class Solver {
 
   // QuadTree::initialize_tree + SkelFactorization::skeletonize.
   int factor();
+  // QuadTree::perturb (quadtree.cpp:359-560) to a new boundary, then
+  // skeletonize: compressed boxes whose points and neighbourhoods did not
+  // change keep their factors (renumbered); the others, and the top level,
+  // are factored again.  One problem; n_reused reports the kept boxes.
+  int update(int n_points, const double* points, const double* normals,
+             const double* curvatures, const double* weights, int n_holes, const double* holes,
+             int* n_reused);
+  // QuadTree::copy_into (quadtree.cpp:584-641) followed by skeletonize:
+  // a factorization of the same boundary in a new solver on `stream`, its
+  // tree a copy of this one and every compressed box's factors copied on
+  // the device; only the uncompressed boxes and the top level are factored.
+  Solver* copy(cudaStream_t stream, int* rc);
   // QuadTree::initialize_tree only, active lists as before compression.
   void build_tree_only();
+  // The partition half of QuadTree::perturb on a tree-only solver.
+  void perturb_tree_only(int n_points, const double* points);
   // linear_solve on device buffers: d_mu (dofs), d_alpha (border, may be
   // null when there are no holes).  d_b and d_mu may be the same buffer.
   // d_g (nb values, may be null = zero) is the right-hand side of the
@@ -200,6 +229,14 @@ class Solver {
   int fail(const std::string& msg);
   int cuda_check(cudaError_t e, const char* what);
   int process_level(int level);
+  int compress_level(int level, std::vector<int>* fresh);
+  int level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s);
+  int begin_factor(cudaEvent_t* ev0);
+  int finish_factor(cudaEvent_t ev0);
+  // Copies the factors of `boxes` (T, L, U, X^-1, update, pivots) from
+  // `src` into this solver's arena, one batched copy on stream_.
+  int adopt_factors(const std::vector<int>& boxes, const std::vector<BoxDevView>& src);
+  void drop_device_state();
   int build_all_compressed();
   int factor_top();
   int factor_top_forest();

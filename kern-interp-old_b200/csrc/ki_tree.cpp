@@ -7,7 +7,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
+#include <unordered_map>
+#include <utility>
 
 namespace kib {
 
@@ -364,6 +367,191 @@ void QuadTreeHost::refresh_level(int level, std::vector<std::vector<int>>* near)
       nr.insert(nr.end(), src.begin(), src.end());
     }
   }
+}
+
+
+// ---------------------------------------------------------------- perturb
+
+void QuadTreeHost::unmark(int id) {
+  Box& b = boxes[id];
+  b.compressed = false;
+  b.active.clear();
+  b.skel.clear();
+  b.redundant.clear();
+  b.perm.clear();
+  b.rank = 0;
+}
+
+void QuadTreeHost::mark_up(int id) {
+  for (int b = id; b >= 0; b = boxes[b].parent) {
+    unmark(b);
+    for (int o : boxes[b].nbr) unmark(o);
+  }
+}
+
+void QuadTreeHost::subdivide(int id) {
+  boxes[id].leaf = false;
+  const double mx = ((boxes[id].corner[6] - boxes[id].corner[0]) / 2.0) + boxes[id].corner[0];
+  const double my = ((boxes[id].corner[3] - boxes[id].corner[1]) / 2.0) + boxes[id].corner[1];
+  const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my}, {mx, my, mx, my}, {mx, mx, my, my}};
+  const int lvl = boxes[id].level + 1;
+  if (static_cast<int>(levels.size()) < lvl + 1) levels.resize(lvl + 1);
+  int kids[4];
+  for (int q = 0; q < 4; q++) {
+    Box c;
+    c.tree = boxes[id].tree;
+    c.level = lvl;
+    c.parent = id;
+    c.side = boxes[id].side / 2.0;
+    std::memcpy(c.corner, boxes[id].corner, sizeof(c.corner));
+    for (int e = 0; e < 4; e++) c.corner[kEditIdx[q][e]] = ev[q][e];
+    kids[q] = static_cast<int>(boxes.size());
+    boxes.push_back(std::move(c));
+    boxes[id].child[q] = kids[q];
+    levels[lvl].push_back(kids[q]);
+  }
+  // the box keeps its own list; its dofs go down point by point in list order
+  const std::vector<int>& orig = boxes[id].original;
+  for (size_t i = 0; i < orig.size(); i += sol_dim_) {
+    const int dof = orig[i];
+    const int pt = dof / sol_dim_;
+    const int q = pick_child(boxes[id], pts_[2 * static_cast<size_t>(pt)],
+                             pts_[2 * static_cast<size_t>(pt) + 1]);
+    for (int c = 0; c < sol_dim_; c++) boxes[kids[q]].original.push_back(dof + c);
+  }
+  for (int q = 0; q < 4; q++)
+    if (static_cast<int>(boxes[kids[q]].original.size()) > max_leaf_) subdivide(kids[q]);
+}
+
+void QuadTreeHost::consolidate(int id) {
+  // breadth-first over the subtree: the leaves' lists in that order
+  std::vector<int> queue{id};
+  std::vector<int> orig;
+  for (size_t i = 0; i < queue.size(); i++) {
+    const Box& c = boxes[queue[i]];
+    if (c.leaf) {
+      if (queue[i] != id) orig.insert(orig.end(), c.original.begin(), c.original.end());
+    } else {
+      for (int q = 0; q < 4; q++) queue.push_back(c.child[q]);
+    }
+  }
+  boxes[id].original.swap(orig);
+  for (size_t i = 1; i < queue.size(); i++) {
+    std::vector<int>& lv = levels[boxes[queue[i]].level];
+    auto it = std::find(lv.begin(), lv.end(), queue[i]);
+    if (it != lv.end()) lv.erase(it);
+    boxes[queue[i]].dead = true;
+  }
+  for (int q = 0; q < 4; q++) boxes[id].child[q] = -1;
+  boxes[id].leaf = true;
+}
+
+namespace {
+// Exact-coordinate key of a point (the reference hashes the pair of doubles,
+// quadtree.cpp:369); -0.0 and 0.0 compare equal, so both hash as 0.0.
+struct PointHash {
+  size_t operator()(const std::pair<double, double>& p) const {
+    auto bits = [](double v) {
+      if (v == 0.0) v = 0.0;
+      uint64_t u;
+      std::memcpy(&u, &v, sizeof(u));
+      return u;
+    };
+    const uint64_t a = bits(p.first), b = bits(p.second);
+    return static_cast<size_t>(a * 0x9E3779B97F4A7C15ULL ^ (b + 0x632BE59BD9B4E019ULL + (a << 6)));
+  }
+};
+}  // namespace
+
+void QuadTreeHost::perturb(const double* old_pts, int n_old, const double* new_pts, int n_new) {
+  const int sd = sol_dim_;
+  // old point -> new point by exact coordinates (a repeated new point maps
+  // to its last index); unmatched old points are deletions, unmatched new
+  // points additions (quadtree.cpp:361-396)
+  std::unordered_map<std::pair<double, double>, int, PointHash> to_new;
+  to_new.reserve(2 * static_cast<size_t>(n_new) + 1);
+  for (int i = 0; i < n_new; i++) to_new[{new_pts[2 * i], new_pts[2 * i + 1]}] = i;
+  std::vector<int> old_to_new(n_old, -1), deletions, additions;
+  std::vector<char> found(n_new, 0);
+  for (int i = 0; i < n_old; i++) {
+    auto it = to_new.find({old_pts[2 * i], old_pts[2 * i + 1]});
+    if (it != to_new.end()) {
+      old_to_new[i] = it->second;
+      found[it->second] = 1;
+    } else {
+      deletions.push_back(i);
+    }
+  }
+  for (int j = 0; j < n_new; j++)
+    if (!found[j]) additions.push_back(j);
+
+  // renumber the lists; a leaf's original list too (quadtree.cpp:402-458)
+  auto remap = [&](std::vector<int>& v) {
+    size_t w = 0;
+    for (size_t r = 0; r < v.size(); r++) {
+      const int nn = old_to_new[v[r] / sd];
+      if (nn >= 0) v[w++] = sd * nn + v[r] % sd;
+    }
+    v.resize(w);
+  };
+  for (const std::vector<int>& lv : levels)
+    for (int id : lv) {
+      Box& b = boxes[id];
+      if (b.leaf) remap(b.original);
+      remap(b.active);
+      remap(b.skel);
+      remap(b.redundant);
+    }
+
+  const int root = roots.empty() ? 0 : roots[0];
+  // additions: into their leaves (new coordinates), which lose their
+  // compression with their neighbourhoods (quadtree.cpp:460-486)
+  std::vector<int> bursting;
+  for (int a : additions) {
+    const double x = new_pts[2 * static_cast<size_t>(a)], y = new_pts[2 * static_cast<size_t>(a) + 1];
+    int c = root;
+    while (!boxes[c].leaf) c = boxes[c].child[pick_child(boxes[c], x, y)];
+    for (int k = 0; k < sd; k++) boxes[c].original.push_back(sd * a + k);
+    bursting.push_back(c);
+    mark_up(c);
+  }
+  // dofs below every box after the additions (quadtree.cpp:488-502)
+  std::vector<long long> below(boxes.size(), 0);
+  for (const std::vector<int>& lv : levels)
+    for (int id : lv) below[id] = boxes[id].leaf ? static_cast<long long>(boxes[id].original.size()) : 0;
+  for (int l = static_cast<int>(levels.size()) - 1; l >= 1; l--)
+    for (int id : levels[l]) below[boxes[id].parent] += below[id];
+  // deletions: the first box under max_leaf dofs on the point's path (old
+  // coordinates) is merged later; its leaf loses its compression
+  // (quadtree.cpp:504-533)
+  std::vector<int> sparse;
+  std::vector<char> is_sparse(boxes.size(), 0);
+  for (int d : deletions) {
+    const double x = old_pts[2 * static_cast<size_t>(d)], y = old_pts[2 * static_cast<size_t>(d) + 1];
+    int c = root;
+    bool path_marked = false;
+    while (!boxes[c].leaf) {
+      if (below[c] < max_leaf_ && !path_marked) {
+        path_marked = true;
+        if (!is_sparse[c]) {
+          is_sparse[c] = 1;
+          sparse.push_back(c);
+        }
+      }
+      c = boxes[c].child[pick_child(boxes[c], x, y)];
+    }
+    mark_up(c);
+  }
+  // split over-full leaves, merge sparse subtrees (their subtrees are
+  // disjoint, so the order is immaterial), rebuild the neighbour lists
+  // (quadtree.cpp:535-559)
+  pts_ = new_pts;
+  for (int b : bursting)
+    if (boxes[b].leaf && static_cast<int>(boxes[b].original.size()) > max_leaf_) subdivide(b);
+  for (int b : sparse) consolidate(b);
+  for (Box& b : boxes) b.nbr.clear();
+  neighbor_lists();
+  pts_ = nullptr;
 }
 
 }  // namespace kib

@@ -29,6 +29,7 @@ struct Box {
   std::vector<int> skel, redundant;
   std::vector<int> perm;      // ID pivots (local active indices)
   int rank = 0;
+  bool dead = false;  // removed from the levels by a consolidation (perturb)
 };
 
 class QuadTreeHost {
@@ -51,6 +52,19 @@ class QuadTreeHost {
   std::vector<Box> boxes;
   std::vector<std::vector<int>> levels;
 
+  // QuadTree::perturb (quadtree.cpp:359-560): the tree of old_points
+  // (n_old points) follows the boundary to new_points (n_new).  Points are
+  // matched by exact coordinates; matched dofs are renumbered in every
+  // list, unmatched new points are added to their leaves, unmatched old
+  // points are deleted.  The leaf of every added or deleted point, its
+  // neighbours, its ancestors and their neighbours lose their compression
+  // (mark_neighbors_and_parents, :288-313); over-full leaves are split
+  // (node_subdivide) and the highest box below max_leaf dofs on a deleted
+  // point's path is merged into one leaf (consolidate_node, :316-356); the
+  // neighbour lists are rebuilt.  Boxes still `compressed` afterwards keep
+  // their factors.  new_points must stay valid during the call.  One tree.
+  void perturb(const double* old_points, int n_old, const double* new_points, int n_new);
+
   // active(b) for every not-yet-compressed box of `level`, then near(b) for
   // every box of the level (quadtree.cpp:664-691).
   void refresh_level(int level, std::vector<std::vector<int>>* near);
@@ -61,6 +75,10 @@ class QuadTreeHost {
   void build_partition(int p0, int p1, int tree_id, double lo, double hi);
   void descendant_neighbors(int big, int small, std::vector<int>* found) const;
   void neighbor_lists();
+  void subdivide(int id);    // node_subdivide (quadtree.cpp:203-285)
+  void consolidate(int id);  // consolidate_node (quadtree.cpp:316-356)
+  void mark_up(int id);      // mark_neighbors_and_parents (quadtree.cpp:288-313)
+  void unmark(int id);
 
   int sol_dim_ = 1;
   int max_leaf_ = 32;

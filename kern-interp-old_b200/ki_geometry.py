@@ -194,6 +194,49 @@ def star_case(n=16384, seed=2, leaf_points=64, id_tol=1e-10, n_targets=256):
                    leaf_points, id_tol, {"sources": src, "strengths": q})
 
 
+def bumped_star_case(n=2048, center=2.0, amp=0.05, width=0.12, extra=0, seed=2,
+                     leaf_points=64, id_tol=1e-10, n_targets=64):
+    """star_case's boundary with the nodes of one arc (|t - center| < 3 width)
+    replaced: r gets a Gaussian bump amp exp(-((t - center) / width)^2) there,
+    and the arc holds `extra` more (or fewer) nodes, evenly spaced in t
+    between the arc's first and last parameter.  Every node outside the arc
+    is bit-identical to star_case(n)'s, so a boundary update matches it.
+    Boundary data and targets are star_case(n)'s sources and targets."""
+    base = star_case(n=n, seed=seed, leaf_points=leaf_points, id_tol=id_tol,
+                     n_targets=n_targets)
+    r0, dr0, ddr0 = _star_r(0.3, 5)
+    t = 2.0 * np.pi * np.arange(n) / n
+    arc = np.nonzero(np.abs(t - center) < 3.0 * width)[0]
+    a0, a1 = int(arc[0]), int(arc[-1])
+    m = arc.size + extra
+    tn = np.linspace(t[a0], t[a1], m)
+
+    def bump(tt):
+        u = (tt - center) / width
+        g = amp * np.exp(-u * u)
+        return g, g * (-2.0 * u / width), g * (4.0 * u * u - 2.0) / (width * width)
+
+    b0, b1, b2 = bump(tn)
+    rt, drt, ddrt = r0(tn) + b0, dr0(tn) + b1, ddr0(tn) + b2
+    c, s_ = np.cos(tn), np.sin(tn)
+    xp = drt * c - rt * s_
+    yp = drt * s_ + rt * c
+    xpp = ddrt * c - 2.0 * drt * s_ - rt * c
+    ypp = ddrt * s_ + 2.0 * drt * c - rt * s_
+    speed = np.sqrt(xp * xp + yp * yp)
+    new = (rt * c, rt * s_, yp / speed, -xp / speed, (xp * ypp - yp * xpp) / speed**3,
+           speed * ((t[a1] - t[a0]) / (m - 1)))
+    old = (base.points[0::2], base.points[1::2], base.normals[0::2], base.normals[1::2],
+           base.curvatures, base.weights)
+    parts = [tuple(np.concatenate([o[:a0], nw, o[a1 + 1:]]) for o, nw in zip(old, new))]
+    pts, nrm, kap, w = _pack(parts)
+    src, q = base.extra["sources"], base.extra["strengths"]
+    return Problem("bumped_star_n%d_e%d" % (n, extra), LAPLACE, pts, nrm, kap, w,
+                   np.zeros((0, 4)), laplace_potential(pts, src, q), base.targets,
+                   laplace_potential(base.targets, src, q), leaf_points, id_tol,
+                   {"sources": src, "strengths": q, "arc": (a0, a1)})
+
+
 def _place_holes(rng, k, rmin, rmax, outer=1.0, gap=0.05):
     holes = []
     while len(holes) < k:

@@ -74,6 +74,9 @@ def load():
     lib.ki_solve_refined_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_double, C.c_int, _ip, _dp]
     lib.ki_eval_targets.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
+    lib.ki_partition_update.argtypes = [C.c_void_p, C.c_int, _dp]
+    lib.ki_update.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, C.c_int, _dp, _ip]
+    lib.ki_copy.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]
     lib.ki_eval_domain.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_int, _dp, _dp]
     lib.ki_eval_domain_device.argtypes = ([C.c_void_p, C.c_int] + [C.c_void_p] * 3 +
                                           [C.c_int, _dp, C.c_void_p])
@@ -185,6 +188,12 @@ class Partition(_Tree):
                                      C.byref(h)), "ki_partition")
         self.h = h
 
+    def update(self, points):
+        """The partition half of QuadTree::perturb (ki_partition_update)."""
+        pts = _f64(points)
+        _check(self.lib.ki_partition_update(self.h, pts.size // 2, _d(pts)),
+               "ki_partition_update")
+
 
 class Solver(_Tree):
     """A factorization on the GPU (QuadTree + SkelFactorization)."""
@@ -210,6 +219,33 @@ class Solver(_Tree):
         self.h = h
         self.n_dofs = self.lib.ki_num_dofs(h)
         self.n_border = self.lib.ki_num_border(h)
+
+    def update(self, problem):
+        """QuadTree::perturb + skeletonize (ki_update): follow the boundary to
+        `problem`'s geometry, keeping the factors of untouched boxes.
+        Returns the number of boxes kept."""
+        pr = problem
+        self.problem = pr
+        self._keep = [_f64(pr.points), _f64(pr.normals), _f64(pr.curvatures),
+                      _f64(pr.weights), _f64(pr.holes).reshape(-1)]
+        pts, nrm, kap, w, holes = self._keep
+        kept = np.zeros(1, dtype=np.int32)
+        _check(self.lib.ki_update(self.h, pr.n_points, _d(pts), _d(nrm), _d(kap), _d(w),
+                                  pr.holes.shape[0], _d(holes) if holes.size else None,
+                                  _i(kept)), "ki_update")
+        self.n_dofs = self.lib.ki_num_dofs(self.h)
+        self.n_border = self.lib.ki_num_border(self.h)
+        return int(kept[0])
+
+    def copy(self, stream=None):
+        """QuadTree::copy_into + skeletonize (ki_copy): an independent handle."""
+        h = C.c_void_p()
+        _check(self.lib.ki_copy(self.h, C.c_void_p(stream) if stream else None, C.byref(h)),
+               "ki_copy")
+        c = Solver.__new__(Solver)
+        c.lib, c.problem, c._keep, c.h = self.lib, self.problem, list(self._keep), h
+        c.n_dofs, c.n_border = self.n_dofs, self.n_border
+        return c
 
     def solve(self, f):
         f = _f64(f)

@@ -175,6 +175,39 @@ class RefSolver(_Common):
                          else max_leaf_dofs, threads)
 
 
+def _ref_update(self, problem):
+    """kiref_update: QuadTree::perturb + skeletonize on the reference."""
+    pr = problem
+    self.problem = pr
+    self._keep = [_f64(pr.points), _f64(pr.normals), _f64(pr.curvatures),
+                  _f64(pr.weights), _f64(pr.holes).reshape(-1)]
+    pts, nrm, kap, w, holes = self._keep
+    tf = C.c_double(0.0)
+    fn = self.lib.kiref_update
+    fn.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp]
+    fn(C.c_void_p(self.h), pr.n_points, _d(pts), _d(nrm), _d(kap), _d(w), pr.holes.shape[0],
+       _d(holes) if holes.size else None, C.byref(tf))
+    self.t_factor = tf.value
+    self.n_dofs = pr.n_dofs
+
+
+def _ref_copy(self):
+    """kiref_copy: QuadTree::copy_into + skeletonize on the reference."""
+    fn = self.lib.kiref_copy
+    fn.restype = C.c_void_p
+    fn.argtypes = [C.c_void_p]
+    c = RefSolver.__new__(RefSolver)
+    c.lib, c.p, c.problem, c._keep = self.lib, self.p, self.problem, list(self._keep)
+    c.h = fn(C.c_void_p(self.h))
+    c.t_factor = 0.0
+    c.n_dofs = self.n_dofs
+    return c
+
+
+RefSolver.update = _ref_update
+RefSolver.copy = _ref_copy
+
+
 class PortSolver(_Common):
     """The CPU restatement (oracle/libkioracle.so)."""
 

@@ -265,4 +265,52 @@ void kiref_domain_points(int domain_size, double x_min, double x_max, double y_m
   get_domain_points(domain_size, &v, x_min, x_max, y_min, y_max);
   if (!v.empty()) std::memcpy(points, v.data(), sizeof(double) * v.size());
 }
+
+// QuadTree::perturb (quadtree.cpp:359-560) to new node arrays, then the
+// reference's own update of the kernel, the hole border and skeletonize, as
+// the boundary-update test runs them (kern_interp_test.cpp:509-517).
+// Factor time in *t_factor (seconds, skeletonize only).
+void kiref_update(void* hp, int n_points, const double* points, const double* normals,
+                  const double* curvatures, const double* weights, int n_holes,
+                  const double* holes, double* t_factor) {
+  Handle* h = static_cast<Handle*>(hp);
+  Boundary& b = h->boundary;
+  b.points.assign(points, points + 2 * n_points);
+  b.normals.assign(normals, normals + 2 * n_points);
+  b.curvatures.assign(curvatures, curvatures + n_points);
+  b.weights.assign(weights, weights + n_points);
+  b.holes.clear();
+  for (int i = 0; i < n_holes; i++) {
+    Hole hole;
+    hole.center = Vec2(holes[4 * i], holes[4 * i + 1]);
+    hole.radius = holes[4 * i + 2];
+    hole.num_nodes = static_cast<int>(holes[4 * i + 3]);
+    b.holes.push_back(hole);
+  }
+  h->tree.perturb(b);
+  h->kernel.update_boundary(&b);
+  if (h->holes) {
+    h->tree.U = initialize_U_mat(h->kernel.pde, b.holes, b.points);
+    h->tree.Psi = initialize_Psi_mat(h->kernel.pde, b.holes, b);
+  }
+  double t0 = now_s();
+  h->fact.skeletonize(h->kernel, &h->tree);
+  if (t_factor) *t_factor = now_s() - t0;
+}
+
+// QuadTree::copy_into (quadtree.cpp:584-641) into a new handle, which is
+// then skeletonized again (kern_interp_test.cpp:555-563).
+void* kiref_copy(void* hp) {
+  Handle* h = static_cast<Handle*>(hp);
+  Handle* c = new Handle();
+  c->sol_dim = h->sol_dim;
+  c->holes = h->holes;
+  c->boundary = h->boundary;
+  c->kernel = h->kernel;
+  c->kernel.update_boundary(&c->boundary);
+  c->fact = h->fact;
+  h->tree.copy_into(&c->tree);
+  c->fact.skeletonize(c->kernel, &c->tree);
+  return c;
+}
 }

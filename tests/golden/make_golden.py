@@ -2,7 +2,8 @@
 solver (compiled from its own sources into oracle/_ref/libkiref.so by
 ``make -C oracle ref``) on seeded geometries.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py           # every fixture
+    python tests/golden/make_golden.py update    # the boundary-update ones only
 
 Each fixture stores, for one problem: the solver settings, the quadtree
 partition (per level and box: corner, side, parent, leaf flag, original dofs),
@@ -54,6 +55,17 @@ def cases():
     return out
 
 
+def update_cases():
+    """(name, base problem, boundary frames, id_tol, max_leaf_dofs) of the
+    boundary-update fixtures: the reference factors the base boundary, then
+    follows it through the frames (QuadTree::perturb + skeletonize each);
+    the fixture holds the state after the last frame."""
+    base = G.star_case(n=2048, n_targets=64)
+    frames = [G.bumped_star_case(n=2048, center=2.0, amp=0.05, width=0.12, extra=60),
+              G.bumped_star_case(n=2048, center=3.5, amp=0.03, width=0.2, extra=-150)]
+    return [("star_update_2048", base, frames, 1e-10, 64)]
+
+
 def geometry_hash(pr):
     h = hashlib.sha256()
     for a in (pr.points, pr.normals, pr.curvatures, pr.weights, pr.holes, pr.f, pr.targets):
@@ -98,6 +110,16 @@ def main():
     import kioracle as K
     if not K.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
+    for name, base, frames, tol, leaf in update_cases():
+        s = K.RefSolver(base, id_tol=tol, max_leaf_dofs=leaf, threads=1)
+        for fr in frames:
+            s.update(fr)
+        rec = dump(s, frames[-1], tol, leaf)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **rec)
+        print("wrote %s (%d bytes)" % (path, os.path.getsize(path)))
+    if len(sys.argv) > 1 and sys.argv[1] == "update":
+        return
     for name, pr, tol, leaf in cases():
         s = K.RefSolver(pr, id_tol=tol, max_leaf_dofs=leaf, threads=1)
         rec = dump(s, pr, tol, leaf)
