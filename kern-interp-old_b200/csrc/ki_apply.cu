@@ -7,6 +7,10 @@
 //   * explicit kernel blocks K(tgt, src) (Kernel::operator(), kernel.cpp:99-111).
 // One thread per output row; the source nodes are read in the same order by
 // all lanes of a warp, so each load is a broadcast.
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "ki_kernels.h"
 
 namespace kib {
@@ -200,6 +204,21 @@ cudaError_t launch_copy_segments(const CopySeg* segs, int n, cudaStream_t s) {
   count_launches(1);
   copy_segments_kernel<<<n, 256, 0, s>>>(segs);
   return cudaGetLastError();
+}
+
+cudaError_t raise_func_attr(const void* func, cudaFuncAttribute attr, int value) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int>, int> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_tuple(dev, func, static_cast<int>(attr));
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= value) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, attr, value);
+  if (e == cudaSuccess) done[key] = value;
+  return e;
 }
 
 }  // namespace kib

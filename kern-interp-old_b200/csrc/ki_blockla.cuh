@@ -157,11 +157,15 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
           v = red[w];
           p = redi[w];
         }
+      // no comparable entry (a NaN column): keep the row, report failure
+      redi[30] = p < j || p >= n;
+      if (redi[30]) p = j;
       ipiv[j] = p;
       redi[31] = p;
     }
     __syncthreads();
     const int p = redi[31];
+    if (redi[30]) info = 1;
     const double piv = a[p + static_cast<long long>(ld) * j];
     if (piv != 0.0) {
       if (p != j) {
@@ -239,11 +243,15 @@ __device__ inline int cta_gj_invert(double* a, int n, int ld, int* ipiv, double*
           v = red[w];
           p = redi[w];
         }
+      // no comparable entry (a NaN column): keep the row, report failure
+      redi[30] = p < j || p >= n;
+      if (redi[30]) p = j;
       ipiv[j] = p;
       redi[31] = p;
     }
     __syncthreads();
     const int p = redi[31];
+    if (redi[30]) info = 1;
     if (p != j)
       for (int c = threadIdx.x; c < n; c += blockDim.x) {
         double* x = a + static_cast<long long>(ld) * c;

@@ -187,8 +187,9 @@ size_t decouple_smem_bytes(int n_max) {
 cudaError_t launch_decouple(const DecParams& p, int n_max, cudaStream_t s) {
   if (p.ntasks == 0) return cudaSuccess;
   const size_t smem = decouple_smem_bytes(n_max);
-  cudaError_t e = cudaFuncSetAttribute(decouple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&decouple_kernel),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   count_launches(1);
   decouple_kernel<<<p.ntasks, kDecThreads, smem, s>>>(p);

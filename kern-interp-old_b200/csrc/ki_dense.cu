@@ -68,6 +68,10 @@ __global__ void __launch_bounds__(1024) panel_lu_kernel(double* a, int n, int ld
           v = red[q];
           p = redi[q];
         }
+      if (p < j || p >= n) {  // no comparable entry (NaN column)
+        p = j;
+        atomicExch(status, 1);
+      }
       sp = p;
       ipiv[j] = p;
     }
@@ -100,6 +104,268 @@ __global__ void __launch_bounds__(1024) panel_lu_kernel(double* a, int n, int ld
       }
     }
     __syncthreads();
+  }
+}
+
+// Panel factorization with the panel in registers: 512 threads, thread t
+// holding rows t + 512 r (r < R) of the W-column panel; the column loop is
+// unrolled, so every register index is a constant.  Per column: the pivot
+// search over the owned rows and a warp reduction, one barrier, a second
+// reduction over the 16 warp maxima (every warp does it), the owners of the
+// pivot row and of row jj publish them in shared memory, a second barrier,
+// then every thread exchanges (if it owns one of the two rows), forms its
+// multipliers and applies the rank-one update in registers.  Rows are
+// exchanged whole, as LAPACK's getf2 does; the pivot is the largest
+// magnitude, the first such row on ties.
+constexpr int kRegThreads = 512;
+template <int R, int W>
+__global__ void __launch_bounds__(kRegThreads) panel_lu_reg_kernel(double* a, int n, int ld,
+                                                                    int j0, int w, int* ipiv,
+                                                                    int* status) {
+  __shared__ double rowP[W], rowJ[W];
+  __shared__ double red[kRegThreads / 32];
+  __shared__ int redi[kRegThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rows = n - j0;
+  double x[R][W];
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = threadIdx.x + kRegThreads * r;
+#pragma unroll
+    for (int c = 0; c < W; c++)
+      x[r][c] = (i < rows && c < w) ? a[j0 + i + static_cast<long long>(ld) * (j0 + c)] : 0.0;
+  }
+#pragma unroll
+  for (int jj = 0; jj < W; jj++) {
+    if (jj >= w) break;
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = threadIdx.x + kRegThreads * r;
+      const double v = fabs(x[r][jj]);
+      if (i >= jj && i < rows && v > bv) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    double v = lane < kRegThreads / 32 ? red[lane] : -1.0;
+    int p = lane < kRegThreads / 32 ? redi[lane] : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+      const int op = __shfl_xor_sync(0xffffffffu, p, o);
+      if (ov > v || (ov == v && op < p)) {
+        v = ov;
+        p = op;
+      }
+    }
+    // no comparable entry (NaN column): keep the row, flag the factorization
+    const bool bad = p < jj || p >= rows;
+    if (bad) p = jj;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = threadIdx.x + kRegThreads * r;
+      if (i == p) {
+#pragma unroll
+        for (int c = 0; c < W; c++) rowP[c] = x[r][c];
+      }
+      if (i == jj) {
+#pragma unroll
+        for (int c = 0; c < W; c++) rowJ[c] = x[r][c];
+      }
+    }
+    __syncthreads();
+    const double piv = rowP[jj];
+    if (threadIdx.x == 0) {
+      ipiv[j0 + jj] = j0 + p;
+      if (piv == 0.0 || bad) atomicExch(status, 1);
+    }
+    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int i = threadIdx.x + kRegThreads * r;
+      if (i == jj) {
+#pragma unroll
+        for (int c = 0; c < W; c++) x[r][c] = rowP[c];
+      } else if (i == p) {
+#pragma unroll
+        for (int c = 0; c < W; c++) x[r][c] = rowJ[c];
+      }
+      if (i > jj && i < rows) {
+        const double li = x[r][jj] * inv;
+#pragma unroll
+        for (int c = jj + 1; c < W; c++) x[r][c] -= li * rowP[c];
+        x[r][jj] = li;
+      }
+    }
+    // the next step overwrites rowP / rowJ / red only after its first
+    // barrier, which every thread reaches after this step's reads
+  }
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    const int i = threadIdx.x + kRegThreads * r;
+#pragma unroll
+    for (int c = 0; c < W; c++)
+      if (i < rows && c < w) a[j0 + i + static_cast<long long>(ld) * (j0 + c)] = x[r][c];
+  }
+}
+
+// Panel factorization for panels of up to kFastRows rows, staged in shared
+// memory, 512 threads and two barriers per column: after the pivot search
+// (every thread then reads the 16 warp maxima and agrees on the pivot), and
+// after the update.  Warp c % 16 owns panel column c; for step jj each lane
+// forms the multipliers l_i of its rows from the unswapped column jj
+// (l_i = x_i / pivot with rows jj and p exchanged), and the owners apply
+// the row exchange and the rank-one update to their columns > jj and the
+// row exchange to the finished columns < jj.  Column jj itself is exchanged
+// and scaled by its owner during step jj + 1, when nobody reads it any more.  Pivot choice as in LAPACK: the largest
+// magnitude, the first such row on ties.
+constexpr int kFastThreads = 512;
+constexpr int kFastQ = 26;  // rows per lane
+constexpr int kFastRows = 32 * kFastQ;
+__global__ void __launch_bounds__(kFastThreads) panel_lu_fast_kernel(double* a, int n, int ld,
+                                                                     int j0, int w, int* ipiv,
+                                                                     int* status) {
+  extern __shared__ double P[];
+  __shared__ double red[kFastThreads / 32];
+  __shared__ int redi[kFastThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int nw = kFastThreads / 32;
+  const int rows = n - j0, ldp = rows | 1;
+  for (int e = threadIdx.x; e < rows * w; e += kFastThreads) {
+    const int i = e % rows, c = e / rows;
+    P[i + ldp * c] = a[j0 + i + static_cast<long long>(ld) * (j0 + c)];
+  }
+  __syncthreads();
+  int prev_p = 0;
+  double prev_inv = 0.0;
+  for (int jj = 0; jj < w; jj++) {
+    double* col = P + ldp * jj;
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int i = jj + threadIdx.x; i < rows; i += kFastThreads) {
+      const double v = fabs(col[i]);
+      if (v > bv) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    double v = red[0];
+    int p = redi[0];
+#pragma unroll
+    for (int q = 1; q < nw; q++) {
+      const double ov = red[q];
+      const int op = redi[q];
+      if (ov > v || (ov == v && op < p)) {
+        v = ov;
+        p = op;
+      }
+    }
+    const bool bad = p < jj || p >= rows;  // no comparable entry (NaN column)
+    if (bad) p = jj;
+    const double piv = col[p];
+    if (threadIdx.x == 0) {
+      ipiv[j0 + jj] = j0 + p;
+      if (piv == 0.0 || bad) atomicExch(status, 1);
+    }
+    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+    // finished columns < jj (nobody reads them in this step): the previous
+    // column's own exchange and scaling, then this step's row exchange
+    for (int c = warp; c < jj; c += nw) {
+      double* pc = P + ldp * c;
+      if (c == jj - 1) {
+        const double top = pc[jj - 1], other = pc[prev_p];
+        __syncwarp();
+        if (lane == 0 && prev_p != jj - 1) {
+          pc[jj - 1] = other;
+          pc[prev_p] = top;
+        }
+        __syncwarp();
+        for (int i = jj + lane; i < rows; i += 32) pc[i] *= prev_inv;
+        __syncwarp();
+      }
+      if (lane == 0 && p != jj) {
+        const double t = pc[jj];
+        pc[jj] = pc[p];
+        pc[p] = t;
+      }
+      __syncwarp();
+    }
+    // multipliers of this lane's rows
+    double l[kFastQ];
+#pragma unroll
+    for (int q = 0; q < kFastQ; q++) {
+      const int i = lane + 32 * q;
+      l[q] = 0.0;
+      if (32 * q < rows && i > jj && i < rows) l[q] = (i == p ? col[jj] : col[i]) * inv;
+    }
+    for (int c = jj + 1; c < w; c++) {
+      if (c % nw != warp) continue;
+      double* pc = P + ldp * c;
+      const double xj = pc[jj], xp = pc[p];
+      __syncwarp();
+      if (lane == 0) pc[jj] = xp;
+      const double u = xp;
+#pragma unroll
+      for (int q = 0; q < kFastQ; q++) {
+        if (32 * q >= rows) break;
+        const int i = lane + 32 * q;
+        if (i > jj && i < rows) {
+          const double xi = i == p ? xj : pc[i];
+          pc[i] = xi - l[q] * u;
+        }
+      }
+      __syncwarp();
+    }
+    prev_p = p;
+    prev_inv = inv;
+    __syncthreads();
+  }
+  // the last column's exchange and scaling
+  if (w > 0 && warp == (w - 1) % nw) {
+    double* pc = P + ldp * (w - 1);
+    const double top = pc[w - 1], other = pc[prev_p];
+    __syncwarp();
+    if (lane == 0 && prev_p != w - 1) {
+      pc[w - 1] = other;
+      pc[prev_p] = top;
+    }
+    __syncwarp();
+    for (int i = w + lane; i < rows; i += 32) pc[i] *= prev_inv;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < rows * w; e += kFastThreads) {
+    const int i = e % rows, c = e / rows;
+    a[j0 + i + static_cast<long long>(ld) * (j0 + c)] = P[i + ldp * c];
   }
 }
 
@@ -158,6 +424,10 @@ __global__ void __launch_bounds__(1024) panel_lu_smem_kernel(double* a, int n, i
         }
       }
       if (lane == 0) {
+        if (q < jj || q >= rows) {  // no comparable entry (NaN column)
+          q = jj;
+          atomicExch(status, 1);
+        }
         sp = q;
         ipiv[j0 + jj] = j0 + q;
       }
@@ -204,7 +474,7 @@ __global__ void swap_kernel(double* a, int n, int ld, int j0, int w, const int* 
   double* x = a + static_cast<long long>(ld) * c;
   for (int jj = 0; jj < w; jj++) {
     const int j = j0 + jj, p = ipiv[j];
-    if (p != j) {
+    if (p != j && p > j && p < n) {
       const double t = x[j];
       x[j] = x[p];
       x[p] = t;
@@ -212,8 +482,15 @@ __global__ void swap_kernel(double* a, int n, int ld, int j0, int w, const int* 
   }
 }
 
-// A12 <- L11^{-1} A12 (unit lower), one thread per column right of the panel.
+// A12 <- L11^{-1} A12 (unit lower), one thread per column right of the
+// panel, L11 staged in shared memory.
 __global__ void trsm_row_kernel(double* a, int n, int ld, int j0, int w) {
+  __shared__ double l11[kNb][kNb + 1];
+  for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+    const int i = e % w, kk = e / w;
+    l11[i][kk] = a[j0 + i + static_cast<long long>(ld) * (j0 + kk)];
+  }
+  __syncthreads();
   const int c = j0 + w + blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   double* x = a + static_cast<long long>(ld) * c;
@@ -226,11 +503,80 @@ __global__ void trsm_row_kernel(double* a, int n, int ld, int j0, int w) {
     const double v = b[kk];
 #pragma unroll
     for (int i = kk + 1; i < kNb; i++)
-      if (i < w) b[i] -= v * a[j0 + i + static_cast<long long>(ld) * (j0 + kk)];
+      if (i < w) b[i] -= v * l11[i][kk];
   }
 #pragma unroll
   for (int i = 0; i < kNb; i++)
     if (i < w) x[j0 + i] = b[i];
+}
+
+// The panel's row interchanges applied to every column outside the panel,
+// fused with A12 <- L11^{-1} A12 for the columns right of it.  Each block
+// first turns the interchange sequence into a list of (destination, source)
+// rows (at most 2w entries; the rows below j0 are untouched), so a column's
+// moved entries are all loaded before any is stored: independent loads
+// instead of a chain of w dependent exchanges.  One thread per column;
+// dynamic shared memory: n - j0 ints.
+constexpr int kSwapThreads = 128;
+__global__ void __launch_bounds__(kSwapThreads) swap_trsm_kernel(double* a, int n, int ld, int j0,
+                                                                 int w, const int* ipiv) {
+  extern __shared__ int perm[];
+  __shared__ double l11[kNb][kNb + 1];
+  __shared__ int dst[2 * kNb], src[2 * kNb], piv[kNb];
+  __shared__ int cnt;
+  const int rows = n - j0;
+  for (int i = threadIdx.x; i < rows; i += kSwapThreads) perm[i] = i;
+  for (int e = threadIdx.x; e < w * w; e += kSwapThreads) {
+    const int i = e % w, kk = e / w;
+    l11[i][kk] = a[j0 + i + static_cast<long long>(ld) * (j0 + kk)];
+  }
+  if (threadIdx.x < w) piv[threadIdx.x] = ipiv[j0 + threadIdx.x] - j0;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int jj = 0; jj < w; jj++) {
+      const int p = piv[jj];
+      if (p < jj || p >= rows) continue;
+      const int t = perm[jj];
+      perm[jj] = perm[p];
+      perm[p] = t;
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < rows; i += kSwapThreads)
+    if (perm[i] != i) {
+      const int k = atomicAdd(&cnt, 1);
+      dst[k] = i;
+      src[k] = perm[i];
+    }
+  __syncthreads();
+  const int m = cnt;
+  const int q = blockIdx.x * kSwapThreads + threadIdx.x;
+  if (q >= n - w) return;
+  const int c = q < j0 ? q : q + w;
+  double* x = a + static_cast<long long>(ld) * c + j0;
+  // this thread's column alone: every moved entry loaded, then stored
+  double v[2 * kNb];
+#pragma unroll
+  for (int k = 0; k < 2 * kNb; k++)
+    if (k < m) v[k] = x[src[k]];
+#pragma unroll
+  for (int k = 0; k < 2 * kNb; k++)
+    if (k < m) x[dst[k]] = v[k];
+  if (c < j0) return;
+  double b[kNb];
+#pragma unroll
+  for (int i = 0; i < kNb; i++) b[i] = i < w ? x[i] : 0.0;
+#pragma unroll
+  for (int kk = 0; kk < kNb; kk++) {
+    if (kk >= w) break;
+    const double bk = b[kk];
+#pragma unroll
+    for (int i = kk + 1; i < kNb; i++)
+      if (i < w) b[i] -= bk * l11[i][kk];
+  }
+#pragma unroll
+  for (int i = 0; i < kNb; i++)
+    if (i < w) x[i] = b[i];
 }
 
 // A22 -= A21 A12 for the trailing block, 64 x 64 tiles, inner dimension w.
@@ -411,25 +757,49 @@ constexpr size_t kSolveSmemMax = 200 * 1024;
 }  // namespace
 
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s) {
-  for (int j0 = 0; j0 < n; j0 += kNb) {
-    const int w = min(kNb, n - j0);
-    count_launches(n - j0 - w > 0 ? 4 : 2);
+  for (int j0 = 0; j0 < n;) {
+    // register-resident panels: 32 columns while a thread holds one row,
+    // 16 columns for two rows
+    const int rows = n - j0;
+    const int wmax = rows <= kRegThreads ? kNb : rows <= 2 * kRegThreads ? kNb / 2 : kNb;
+    const int w = min(wmax, n - j0);
+    count_launches(n - j0 - w > 0 ? 3 : 2);
     const size_t psmem = sizeof(double) * static_cast<size_t>((n - j0) | 1) * w;
-    if (psmem <= kPanelSmemMax) {
-      const cudaError_t e = cudaFuncSetAttribute(
-          panel_lu_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax);
+    if (rows <= kRegThreads) {
+      panel_lu_reg_kernel<1, kNb><<<1, kRegThreads, 0, s>>>(a, n, ld, j0, w, ipiv, status);
+    } else if (rows <= 2 * kRegThreads) {
+      panel_lu_reg_kernel<2, kNb / 2><<<1, kRegThreads, 0, s>>>(a, n, ld, j0, w, ipiv, status);
+    } else if (psmem <= kPanelSmemMax && n - j0 <= kFastRows) {
+      const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&panel_lu_fast_kernel),
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            kPanelSmemMax);
+      if (e != cudaSuccess) return e;
+      panel_lu_fast_kernel<<<1, kFastThreads, psmem, s>>>(a, n, ld, j0, w, ipiv, status);
+    } else if (psmem <= kPanelSmemMax) {
+      const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&panel_lu_smem_kernel),
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            kPanelSmemMax);
       if (e != cudaSuccess) return e;
       panel_lu_smem_kernel<<<1, 1024, psmem, s>>>(a, n, ld, j0, w, ipiv, status);
     } else {
       panel_lu_kernel<<<1, 1024, 0, s>>>(a, n, ld, j0, w, ipiv, status);
     }
-    swap_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w, ipiv);
     const int right = n - j0 - w;
+    if (n - w > 0) {
+      const size_t ssmem = sizeof(int) * static_cast<size_t>(n - j0);
+      if (ssmem <= 48 * 1024) {
+        swap_trsm_kernel<<<(n - w + kSwapThreads - 1) / kSwapThreads, kSwapThreads, ssmem, s>>>(
+            a, n, ld, j0, w, ipiv);
+      } else {
+        swap_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w, ipiv);
+        if (right > 0) trsm_row_kernel<<<(right + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w);
+      }
+    }
     if (right > 0) {
-      trsm_row_kernel<<<(right + 127) / 128, 128, 0, s>>>(a, n, ld, j0, w);
       const int tiles = (right + 63) / 64;
       trailing_kernel<<<dim3(tiles, tiles), 256, 0, s>>>(a, n, ld, j0, w);
     }
+    j0 += w;
   }
   return cudaGetLastError();
 }
@@ -440,8 +810,9 @@ cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, dou
   count_launches(1);
   const size_t smem = sizeof(double) * static_cast<size_t>(n);
   if (n >= 64 && smem <= kSolveSmemMax) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        lu_solve_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmemMax);
+    const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_solve_cta_kernel),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSolveSmemMax);
     if (e != cudaSuccess) return e;
     lu_solve_cta_kernel<<<nrhs, kSolveThreads, smem, s>>>(lu, n, ld, ipiv, b, ldb);
     return cudaGetLastError();

@@ -109,67 +109,129 @@ __global__ void __launch_bounds__(kDomThreads)
   }
 }
 
-// CubicBoundary::is_in_domain for every target, one thread per target, the
-// nodes staged in shared memory with the height of the next node of their
-// curve and a code marking the last node of the outer curve (1) or of a
-// hole (2).  mask[t] = 1 inside, 0 outside.
-__global__ void __launch_bounds__(kDomThreads)
-    domain_mask_nodes_kernel(const Node* __restrict__ nodes, int np,
-                             const double* __restrict__ holes, int nh, int nt,
-                             const double* __restrict__ tg, unsigned char* __restrict__ mask) {
-  __shared__ double sx[kDomThreads], sy[kDomThreads], syn[kDomThreads];
-  __shared__ int scode[kDomThreads];
-  const int t = blockIdx.x * kDomThreads + threadIdx.x;
-  const bool live = t < nt;
-  const double tx = live ? tg[2 * t] : 0.0, ty = live ? tg[2 * t + 1] : 0.0;
+// CubicBoundary::is_in_domain, in two steps.
+//
+// curve_prep_kernel, one thread per node: the node's position, the height of
+// the next node of its curve, and a code marking the last node of the outer
+// curve (1) or of a hole (2), as structure-of-arrays; and per tile of 32
+// consecutive nodes (one warp) the bounds a point must meet for the tile to
+// matter: the nodes' box, the lowest and highest edge end, whether a curve
+// ends in it.
+//
+// domain_mask_nodes_kernel, one warp per 32 targets, no block barriers: the
+// warp walks the tiles in order; a tile that no target of the warp can be
+// within 1e-2 of (box distance) and that no target lies strictly between
+// the tile's edge ends and left of its rightmost node contributes nothing
+// and is skipped, unless it ends a curve.  Other tiles are staged in the
+// warp's shared-memory slice and every lane runs the reference's tests on
+// the 32 nodes.  mask[t] = 1 inside, 0 outside.
+struct CurveTile {
+  double bx0, bx1, by0, by1, ey0, ey1;
+  int code, pad;
+};
+
+__global__ void curve_prep_kernel(const Node* __restrict__ nodes, int np,
+                                  const double* __restrict__ holes, int nh,
+                                  double* __restrict__ cx, double* __restrict__ cy,
+                                  double* __restrict__ cyn, int* __restrict__ ccode,
+                                  CurveTile* __restrict__ tiles) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
   int n_outer = np;
   for (int h = 0; h < nh; h++) n_outer -= static_cast<int>(holes[4 * h + 3]);
+  double bx0 = NAN, bx1 = NAN, by0 = NAN, by1 = NAN, ey0 = NAN, ey1 = NAN;
+  int code = 0;
+  if (j < np) {
+    int start = 0, end = n_outer;
+    code = 1;
+    if (j >= n_outer) {
+      start = n_outer;
+      code = 2;
+      for (int h = 0; h < nh; h++) {
+        end = start + static_cast<int>(holes[4 * h + 3]);
+        if (j < end) break;
+        start = end;
+      }
+    }
+    const Node s = nodes[j];
+    const double yn = nodes[j + 1 < end ? j + 1 : start].y;
+    code = j == end - 1 ? code : 0;
+    cx[j] = s.x;
+    cy[j] = s.y;
+    cyn[j] = yn;
+    ccode[j] = code;
+    bx0 = bx1 = s.x;
+    by0 = by1 = s.y;
+    ey0 = fmin(s.y, yn);
+    ey1 = fmax(s.y, yn);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    bx0 = fmin(bx0, __shfl_xor_sync(0xffffffffu, bx0, o));
+    bx1 = fmax(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
+    by0 = fmin(by0, __shfl_xor_sync(0xffffffffu, by0, o));
+    by1 = fmax(by1, __shfl_xor_sync(0xffffffffu, by1, o));
+    ey0 = fmin(ey0, __shfl_xor_sync(0xffffffffu, ey0, o));
+    ey1 = fmax(ey1, __shfl_xor_sync(0xffffffffu, ey1, o));
+    code |= __shfl_xor_sync(0xffffffffu, code, o);
+  }
+  if (lane == 0 && j < np) tiles[j >> 5] = CurveTile{bx0, bx1, by0, by1, ey0, ey1, code, 0};
+}
+
+constexpr int kMaskWarps = 8;
+__global__ void __launch_bounds__(32 * kMaskWarps)
+    domain_mask_nodes_kernel(const double* __restrict__ cx, const double* __restrict__ cy,
+                             const double* __restrict__ cyn, const int* __restrict__ ccode,
+                             const CurveTile* __restrict__ tiles, int np, int nt,
+                             const double* __restrict__ tg, unsigned char* __restrict__ mask) {
+  __shared__ double sx[kMaskWarps][32], sy[kMaskWarps][32], syn[kMaskWarps][32];
+  __shared__ int scode[kMaskWarps][32];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int t = (blockIdx.x * kMaskWarps + wl) * 32 + lane;
+  const bool live = t < nt;
+  const double tx = live ? tg[2 * t] : 0.0, ty = live ? tg[2 * t + 1] : 0.0;
   int wind = 0;
   bool out = false;
-  for (int base = 0; base < np; base += kDomThreads) {
-    const int j = base + threadIdx.x;
-    __syncthreads();
+  const int ntiles = (np + 31) >> 5;
+  for (int k = 0; k < ntiles; k++) {
+    const CurveTile tl = tiles[k];
+    const double dx = fmax(fmax(tl.bx0 - tx, tx - tl.bx1), 0.0);
+    const double dy = fmax(fmax(tl.by0 - ty, ty - tl.by1), 0.0);
+    const bool near_box = dx * dx + dy * dy < 1.0004e-4;
+    const bool cross = ty > tl.ey0 && ty < tl.ey1 && tx < tl.bx1;
+    if (!__any_sync(0xffffffffu, live && (near_box || cross)) && tl.code == 0) continue;
+    const int j = (k << 5) + lane;
+    __syncwarp();
     if (j < np) {
-      int start = 0, end = n_outer, code = 1;
-      if (j >= n_outer) {
-        start = n_outer;
-        code = 2;
-        for (int h = 0; h < nh; h++) {
-          end = start + static_cast<int>(holes[4 * h + 3]);
-          if (j < end) break;
-          start = end;
-        }
-      }
-      const Node s = nodes[j];
-      sx[threadIdx.x] = s.x;
-      sy[threadIdx.x] = s.y;
-      syn[threadIdx.x] = nodes[j + 1 < end ? j + 1 : start].y;
-      scode[threadIdx.x] = j == end - 1 ? code : 0;
+      sx[wl][lane] = cx[j];
+      sy[wl][lane] = cy[j];
+      syn[wl][lane] = cyn[j];
+      scode[wl][lane] = ccode[j];
     } else {
       // padding: left of every point (no crossing), infinitely far
-      sx[threadIdx.x] = -INFINITY;
-      sy[threadIdx.x] = 0.0;
-      syn[threadIdx.x] = 0.0;
-      scode[threadIdx.x] = 0;
+      sx[wl][lane] = -INFINITY;
+      sy[wl][lane] = 0.0;
+      syn[wl][lane] = 0.0;
+      scode[wl][lane] = 0;
     }
-    __syncthreads();
-    for (int q = 0; q < kDomThreads; q++) {
-      const double px = sx[q], py = sy[q];
-      const double dx = subd(tx, px), dy = subd(ty, py);
-      const double d2 = add(mul(dx, dx), mul(dy, dy));
+    __syncwarp();
+    for (int q = 0; q < 32; q++) {
+      const double px = sx[wl][q], py = sy[wl][q];
+      const double ddx = subd(tx, px), ddy = subd(ty, py);
+      const double d2 = add(mul(ddx, ddx), mul(ddy, ddy));
       // sqrt(d2) < eps needs d2 < eps^2 (1 + 2^-50); test the root exactly
       if (d2 < 1.0001e-4 && __dsqrt_rn(d2) < kDomainEps) out = true;
       if (px > tx) {
-        const double pyn = syn[q];
+        const double pyn = syn[wl][q];
         if (py < ty && pyn > ty) {
           wind++;
         } else if (py > ty && pyn < ty) {
           wind--;
         }
       }
-      const int code = scode[q];
-      if (code) {
-        if (code == 1 ? wind % 2 == 0 : wind % 2 == 1) out = true;
+      const int cq = scode[wl][q];
+      if (cq) {
+        if (cq == 1 ? wind % 2 == 0 : wind % 2 == 1) out = true;
         wind = 0;
       }
     }
@@ -233,16 +295,33 @@ int domain_splits(int nt, int np, int num_sms) {
   return std::max(1, std::min(want, (np + 1023) / 1024));
 }
 
+size_t domain_mask_scratch_bytes(int np) {
+  const size_t tiles = (static_cast<size_t>(np) + 31) / 32;
+  return 3 * sizeof(double) * np + sizeof(int) * np + sizeof(CurveTile) * tiles + 256;
+}
+
 cudaError_t launch_domain_mask(int kind, const Node* nodes, int np, const double* holes, int nh,
                                const double* disk, int nt, const double* targets,
-                               unsigned char* mask, cudaStream_t s) {
+                               unsigned char* mask, void* scratch, cudaStream_t s) {
   if (nt == 0) return cudaSuccess;
-  const int grid = (nt + kDomThreads - 1) / kDomThreads;
-  count_launches(1);
   if (kind == kDomainNodes) {
-    domain_mask_nodes_kernel<<<grid, kDomThreads, 0, s>>>(nodes, np, holes, nh, nt, targets,
-                                                         mask);
+    // scratch: x, y, next y (np doubles each), tiles (16-byte aligned), codes
+    double* cx = static_cast<double*>(scratch);
+    double* cy = cx + np;
+    double* cyn = cy + np;
+    CurveTile* tiles = reinterpret_cast<CurveTile*>(cyn + np + (np & 1));
+    int* ccode = reinterpret_cast<int*>(tiles + (np + 31) / 32);
+    count_launches(2);
+    curve_prep_kernel<<<(np + 255) / 256, 256, 0, s>>>(nodes, np, holes, nh, cx, cy, cyn, ccode,
+                                                       tiles);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int per_block = 32 * kMaskWarps;
+    domain_mask_nodes_kernel<<<(nt + per_block - 1) / per_block, per_block, 0, s>>>(
+        cx, cy, cyn, ccode, tiles, np, nt, targets, mask);
   } else {
+    count_launches(1);
+    const int grid = (nt + kDomThreads - 1) / kDomThreads;
     domain_mask_disk_kernel<<<grid, kDomThreads, 0, s>>>(disk[0], disk[1], disk[2], holes, nh,
                                                         nt, targets, mask);
   }

@@ -28,8 +28,9 @@ int Solver::domain_mask(int nt, const double* d_targets, int kind, const double*
   if (n_trees() > 1) return fail("domain_mask: not available for a batch of problems");
   if (kind == kDomainNodes && !curves_fit(holes_, n_points_))
     return fail("domain_mask: hole node counts exceed the number of nodes");
+  KI_CUDA(dom_.reserve(domain_mask_scratch_bytes(n_points_), stream_));
   KI_CUDA(launch_domain_mask(kind, d_nodes_, n_points_, d_holes_, n_holes(), disk, nt, d_targets,
-                             d_mask, stream_));
+                             d_mask, dom_.p, stream_));
   return 0;
 }
 
@@ -49,14 +50,18 @@ int Solver::eval_domain(int nt, const double* d_targets, const double* d_mu,
   }
   const int splits = domain_splits(nt, n_points_, num_sms_);
   const size_t rows = static_cast<size_t>(nt) * sd_;
-  const size_t part_bytes = splits > 1 ? sizeof(double) * rows * splits : 0;
+  // scratch: [split partials][node-curve test][mask], 256-byte aligned parts
+  auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+  const size_t part_bytes = up(splits > 1 ? sizeof(double) * rows * splits : 0);
+  const size_t curve_bytes = up(kind == kDomainNodes ? domain_mask_scratch_bytes(n_points_) : 0);
   const size_t mask_bytes = kind != kDomainAll ? static_cast<size_t>(nt) : 0;
-  KI_CUDA(dom_.reserve(part_bytes + mask_bytes + 16, stream_));
-  double* part = static_cast<double*>(dom_.p);
+  KI_CUDA(dom_.reserve(part_bytes + curve_bytes + mask_bytes + 16, stream_));
+  char* base = static_cast<char*>(dom_.p);
+  double* part = reinterpret_cast<double*>(base);
   unsigned char* mask =
-      mask_bytes ? static_cast<unsigned char*>(dom_.p) + part_bytes : nullptr;
+      mask_bytes ? reinterpret_cast<unsigned char*>(base + part_bytes + curve_bytes) : nullptr;
   if (mask) KI_CUDA(launch_domain_mask(kind, d_nodes_, n_points_, d_holes_, n_holes(), disk, nt,
-                                       d_targets, mask, stream_));
+                                       d_targets, mask, base + part_bytes, stream_));
   const bool use_alpha = nb_ > 0 && d_alpha;
   KI_CUDA(launch_domain_eval(opt_.pde, d_nodes_, n_points_, nt, d_targets, d_mu, n_holes(),
                              d_holes_, use_alpha ? d_alpha : nullptr, mask, splits, part, d_out,

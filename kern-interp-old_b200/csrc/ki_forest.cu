@@ -65,8 +65,8 @@ cudaError_t launch_forest_top_solve(const TopTask* tasks, int ntasks, int n_max,
   if (ntasks == 0 || n_max == 0) return cudaSuccess;
   const size_t smem = sizeof(double) * static_cast<size_t>(n_max);
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  const cudaError_t e = cudaFuncSetAttribute(
-      forest_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&forest_solve_kernel),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e != cudaSuccess) return e;
   count_launches(1);
   forest_solve_kernel<<<ntasks, kForestThreads, smem, s>>>(tasks, x);

@@ -845,13 +845,13 @@ template <int G>
 cudaError_t launch_onchip(const IdParams& p, cudaStream_t s) {
   const size_t smem = static_cast<size_t>(p.onchip_smem);
   if (smem == 0 || smem > 227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(id_onchip_kernel<G>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<G>),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   if (G > 8) {
-    e = cudaFuncSetAttribute(id_onchip_kernel<G>, cudaFuncAttributeNonPortableClusterSizeAllowed,
-                             1);
+    e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<G>),
+                        cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e != cudaSuccess) return e;
   }
   cudaLaunchConfig_t cfg = {};
@@ -876,9 +876,9 @@ cudaError_t launch_onchip(const IdParams& p, cudaStream_t s) {
 template <int G>
 cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
   const size_t smem = id_smem_bytes(p.m_cap, p.n_cap);
-  cudaError_t e = cudaFuncSetAttribute(id_kernel<G>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&id_kernel<G>),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G * p.ntasks);
@@ -1054,14 +1054,14 @@ int id_cluster_fits(int group, int m_cap, int n_cap, size_t col_cap) {
   int clusters = 0;
   cudaError_t e;
   switch (G) {
-    case 2: e = cudaFuncSetAttribute(id_onchip_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    case 2: e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<2>), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<2>, &cfg); break;
-    case 4: e = cudaFuncSetAttribute(id_onchip_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    case 4: e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<4>), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<4>, &cfg); break;
-    case 8: e = cudaFuncSetAttribute(id_onchip_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    case 8: e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<8>), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
       if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<8>, &cfg); break;
-    case 16: e = cudaFuncSetAttribute(id_onchip_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-      if (e == cudaSuccess) e = cudaFuncSetAttribute(id_onchip_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    case 16: e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<16>), cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+      if (e == cudaSuccess) e = raise_func_attr(reinterpret_cast<const void*>(&id_onchip_kernel<16>), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&clusters, id_onchip_kernel<16>, &cfg); break;
     default: return 0;
   }

@@ -254,14 +254,22 @@ cudaError_t launch_eval_targets(int pde, const Node* nodes, int n_dofs, int nt,
 // `part` holds splits x rows doubles when splits > 1 (domain_splits).
 enum DomainKind : int { kDomainAll = 0, kDomainNodes = 1, kDomainDisk = 2 };
 int domain_splits(int nt, int np, int num_sms);
+// The node-curve test needs domain_mask_scratch_bytes(np) of device scratch.
+size_t domain_mask_scratch_bytes(int np);
 cudaError_t launch_domain_mask(int kind, const Node* nodes, int np, const double* holes, int nh,
                                const double* disk, int nt, const double* targets,
-                               unsigned char* mask, cudaStream_t s);
+                               unsigned char* mask, void* scratch, cudaStream_t s);
 cudaError_t launch_domain_eval(int pde, const Node* nodes, int np, int nt,
                                const double* targets, const double* mu, int nh,
                                const double* holes, const double* alpha,
                                const unsigned char* mask, int splits, double* part,
                                double* out, cudaStream_t s);
+// cudaFuncSetAttribute(func, attr, value) unless this process already
+// raised the attribute to at least `value` on the current device: the call
+// costs microseconds of host time, which level loops with many short
+// launches otherwise pay on every launch.
+cudaError_t raise_func_attr(const void* func, cudaFuncAttribute attr, int value);
+
 // Batched device-to-device copy: segment i moves words[i] 32-bit words from
 // src to dst (one CTA per segment).
 struct CopySeg {

@@ -51,6 +51,44 @@ __device__ __forceinline__ void apply_sub(double* out, const double* in, int row
   }
 }
 
+// The same for several right-hand sides: a thread owns one output row and a
+// group of up to kGrp right-hand sides, so each matrix entry is loaded once
+// for the whole group (the lanes of a warp hold consecutive rows of one
+// group and read the same staged vector entry).
+constexpr int kGrp = 8;
+__device__ __forceinline__ void apply_sub_multi(double* out, const double* in, int rows, int inner,
+                                                int nc, const double* A, long long si,
+                                                long long sl) {
+  const int ng = (nc + kGrp - 1) / kGrp;
+  for (int t = threadIdx.x; t < rows * ng; t += kSweepThreads) {
+    const int i = t % rows, g = t / rows;
+    const int c0 = g * kGrp, m = min(kGrp, nc - c0);
+    const double* a = A + si * i;
+    double acc[kGrp];
+#pragma unroll
+    for (int c = 0; c < kGrp; c++) acc[c] = 0.0;
+    for (int l = 0; l < inner; l++) {
+      const double av = a[sl * l];
+      const double* x = in + l * nc + c0;
+#pragma unroll
+      for (int c = 0; c < kGrp; c++)
+        if (c < m) acc[c] += av * x[c];
+    }
+#pragma unroll
+    for (int c = 0; c < kGrp; c++)
+      if (c < m) out[i * nc + c0 + c] -= acc[c];
+  }
+}
+
+__device__ __forceinline__ void apply_any(double* out, const double* in, int rows, int inner,
+                                          int nc, const double* A, long long si, long long sl) {
+  if (nc == 1) {
+    apply_sub(out, in, rows, inner, nc, A, si, sl);
+  } else {
+    apply_sub_multi(out, in, rows, inner, nc, A, si, sl);
+  }
+}
+
 template <int MODE>  // 0 up (L), 1 up (U^T), 2 down, 3 transposed up (L^T, T)
 __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int chunk) {
   extern __shared__ double sm[];
@@ -73,27 +111,27 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
     __syncthreads();
     if (MODE <= 1) {
       // xr -= T^T xs : (T^T)(j, l) = T[l + k j]
-      apply_sub(xr, xs, r, k, nc, tk.T, k, 1);
+      apply_any(xr, xs, r, k, nc, tk.T, k, 1);
       __syncthreads();
       if (MODE == 0) {
         // xs -= L xr : L(i, j) = L[i + k j]
-        apply_sub(xs, xr, k, r, nc, tk.L, 1, k);
+        apply_any(xs, xr, k, r, nc, tk.L, 1, k);
       } else {
         // xs -= U^T xr : (U^T)(i, j) = U[j + r i]
-        apply_sub(xs, xr, k, r, nc, tk.U, r, 1);
+        apply_any(xs, xr, k, r, nc, tk.U, r, 1);
       }
     } else if (MODE == 2) {
       // xr -= U xs : U(j, l) = U[j + r l]
-      apply_sub(xr, xs, r, k, nc, tk.U, 1, r);
+      apply_any(xr, xs, r, k, nc, tk.U, 1, r);
       __syncthreads();
       // xs -= T xr : T(i, j) = T[i + k j]
-      apply_sub(xs, xr, k, r, nc, tk.T, 1, k);
+      apply_any(xs, xr, k, r, nc, tk.T, 1, k);
     } else {
       // xr -= L^T xs : (L^T)(j, l) = L[l + k j]
-      apply_sub(xr, xs, r, k, nc, tk.L, k, 1);
+      apply_any(xr, xs, r, k, nc, tk.L, k, 1);
       __syncthreads();
       // xs -= T xr
-      apply_sub(xs, xr, k, r, nc, tk.T, 1, k);
+      apply_any(xs, xr, k, r, nc, tk.T, 1, k);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < k * nc; t += kSweepThreads) {
@@ -129,6 +167,28 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
       xs[t] = P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
     __syncthreads();
+    if (nc > 1) {
+      // a row and a group of right-hand sides per thread: each X^{-1}
+      // entry is loaded once for the group
+      const int ng = (nc + kGrp - 1) / kGrp;
+      for (int t = threadIdx.x; t < r * ng; t += kDiagThreads) {
+        const int i = t % r, g = t / r;
+        const int cg = g * kGrp, m = min(kGrp, nc - cg);
+        double acc[kGrp];
+#pragma unroll
+        for (int c = 0; c < kGrp; c++) acc[c] = 0.0;
+        for (int j = 0; j < r; j++) {
+          const double a = TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
+          const double* x = xs + j * nc + cg;
+#pragma unroll
+          for (int c = 0; c < kGrp; c++)
+            if (c < m) acc[c] += a * x[c];
+        }
+#pragma unroll
+        for (int c = 0; c < kGrp; c++)
+          if (c < m) ys[i * nc + cg + c] = acc[c];
+      }
+    } else
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int i = t % r, c = t / r;  // consecutive threads: consecutive rows i
       double s0 = 0.0, s1 = 0.0;
@@ -158,9 +218,9 @@ template <int MODE>
 cudaError_t launch_mode(const SweepParams& p, cudaStream_t s) {
   const int nc = rhs_chunk(p.nrhs, p.cap);
   const size_t smem = sizeof(double) * static_cast<size_t>(p.cap) * nc;
-  cudaError_t e = cudaFuncSetAttribute(sweep_kernel<MODE>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&sweep_kernel<MODE>),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   sweep_kernel<MODE><<<p.ntasks, kSweepThreads, smem, s>>>(p, nc);
   return cudaGetLastError();
@@ -192,9 +252,9 @@ cudaError_t launch_diag(const SweepParams& p, cudaStream_t s) {
   if (p.ntasks == 0 || p.nrhs == 0) return cudaSuccess;
   const int nc = rhs_chunk(p.nrhs, 2 * (p.cap > 0 ? p.cap : 1));
   const size_t smem = 2 * sizeof(double) * static_cast<size_t>(p.cap > 0 ? p.cap : 1) * nc;
-  cudaError_t e = cudaFuncSetAttribute(diag_inv_kernel<TRANS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem));
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&diag_inv_kernel<TRANS>),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   count_launches(1);
   diag_inv_kernel<TRANS><<<p.ntasks, kDiagThreads, smem, s>>>(p, nc);
