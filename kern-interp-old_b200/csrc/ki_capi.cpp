@@ -63,6 +63,7 @@ int cuda_err(cudaError_t e, const char* what) {
 
 bool box_ref(ki_solver_t s, int level, int idx, const kib::Box** out, int* parent_idx) {
   if (!s || !s->solver) return false;
+  s->solver->tree.materialize_originals();
   const auto& lv = s->solver->tree.levels;
   if (level < 0 || level >= static_cast<int>(lv.size())) return false;
   if (idx < 0 || idx >= static_cast<int>(lv[level].size())) return false;

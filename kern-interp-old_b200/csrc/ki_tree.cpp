@@ -42,10 +42,12 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   // first.  Sorting the splits by (that point index, depth-first position)
   // and numbering the children in that order reproduces the reference ids.
   //
-  // Boxes hold contiguous ranges of one point permutation; splitting a box
-  // stably partitions its range into its children's ranges (counting sort by
-  // child), so every range is in point-index order until its own box splits
-  // (its list is copied out then; a leaf's at the end).
+  // Boxes hold contiguous ranges of one point permutation, the coordinates
+  // permuted along with the indices; splitting a box stably partitions its
+  // range into its children's ranges (counting sort by child), so every
+  // range is in point-index order until its own box splits.  Leaves take
+  // their lists from their ranges; the lists of split boxes are merged from
+  // their children's only when asked for (materialize_originals).
   struct Tmp {
     int parent = -1, level = 0, child[4] = {-1, -1, -1, -1};
     int begin = 0, count = 0;
@@ -54,11 +56,17 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   std::vector<Tmp> tb(1);
   const double c0[8] = {lo, lo, lo, hi, hi, hi, hi, lo};
   std::memcpy(tb[0].corner, c0, sizeof(c0));
-  tb[0].count = p1 - p0;
-  std::vector<int> perm(p1 - p0), scratch(p1 - p0);
-  for (int q = p0; q < p1; q++) perm[q - p0] = q;
-  std::vector<std::vector<int>> split_pts;  // index-ordered points of split boxes
-  std::vector<int> split_slot(1, -1);
+  const int np = p1 - p0;
+  tb[0].count = np;
+  std::vector<int> perm(np), tmpi(np);
+  std::vector<double> pxy(2 * static_cast<size_t>(np)), tmpxy(2 * static_cast<size_t>(np));
+  std::vector<unsigned char> quad(np);
+  for (int q = 0; q < np; q++) {
+    perm[q] = p0 + q;
+    pxy[2 * q] = pts_[2 * static_cast<size_t>(p0 + q)];
+    pxy[2 * q + 1] = pts_[2 * static_cast<size_t>(p0 + q) + 1];
+  }
+  std::vector<long long> moment(1, -1);  // index of a split box's (cap+1)-th point
   const int cap = max_leaf_ / sol_dim_;  // split when a box holds more points
   std::vector<int> frontier{0};
   while (!frontier.empty()) {
@@ -68,26 +76,26 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
     if (split.empty()) break;
     const int base = static_cast<int>(tb.size());
     tb.resize(base + 4 * split.size());
-    split_slot.resize(tb.size(), -1);
-    const int sbase = static_cast<int>(split_pts.size());
-    split_pts.resize(sbase + split.size());
+    moment.resize(tb.size(), -1);
     parallel_for(static_cast<int>(split.size()), 4, [&](int a, int e) {
       for (int s = a; s < e; s++) {
         Tmp& P = tb[split[s]];
-        int* rp = perm.data() + P.begin;
-        int* rq = scratch.data() + P.begin;
-        split_slot[split[s]] = sbase + s;
-        split_pts[sbase + s].assign(rp, rp + P.count);
+        const int b0 = P.begin;
+        int* rp = perm.data() + b0;
+        double* rxy = pxy.data() + 2 * static_cast<size_t>(b0);
+        moment[split[s]] = rp[cap];  // the range is still in index order
         const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
         const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
         int cnt[4] = {0, 0, 0, 0};
         for (int i = 0; i < P.count; i++) {
-          const int pt = rp[i];
-          const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
+          const double x = rxy[2 * i], y = rxy[2 * i + 1];
           const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
-          rq[i] = q;
+          quad[b0 + i] = static_cast<unsigned char>(q);
           cnt[q]++;
         }
+        std::memcpy(tmpi.data() + b0, rp, sizeof(int) * P.count);
+        std::memcpy(tmpxy.data() + 2 * static_cast<size_t>(b0), rxy,
+                    2 * sizeof(double) * P.count);
         int pos[4];
         pos[0] = 0;
         for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
@@ -97,15 +105,21 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
           Tmp& C = tb[base + 4 * s + q];
           C.parent = split[s];
           C.level = P.level + 1;
-          C.begin = P.begin + pos[q];
+          C.begin = b0 + pos[q];
           C.count = cnt[q];
           std::memcpy(C.corner, P.corner, sizeof(C.corner));
           for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
           P.child[q] = base + 4 * s + q;
         }
-        // stable scatter: the copied list holds the old order
-        const std::vector<int>& old = split_pts[sbase + s];
-        for (int i = 0; i < P.count; i++) rp[pos[rq[i]]++] = old[i];
+        // stable scatter from the copy
+        const int* oi = tmpi.data() + b0;
+        const double* oxy = tmpxy.data() + 2 * static_cast<size_t>(b0);
+        for (int i = 0; i < P.count; i++) {
+          const int d = pos[quad[b0 + i]]++;
+          rp[d] = oi[i];
+          rxy[2 * d] = oxy[2 * i];
+          rxy[2 * d + 1] = oxy[2 * i + 1];
+        }
       }
     });
     frontier.clear();
@@ -130,7 +144,7 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   std::vector<int> splits;
   for (int id = 0; id < nt; id++) {
     if (tb[id].child[0] < 0) continue;
-    long long t = split_pts[split_slot[id]][cap];
+    long long t = moment[id];
     if (tb[id].parent >= 0) t = std::max(t, when[tb[id].parent]);
     when[id] = t;
     splits.push_back(id);
@@ -165,13 +179,36 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
       double sd = side0;
       for (int l = 0; l < t.level; l++) sd /= 2.0;
       b.side = sd;
+      if (!b.leaf) continue;
       b.original.resize(static_cast<size_t>(t.count) * sol_dim_);
-      const int* src = split_slot[id] >= 0 ? split_pts[split_slot[id]].data() : perm.data() + t.begin;
+      const int* src = perm.data() + t.begin;
       for (int i = 0; i < t.count; i++)
         for (int c = 0; c < sol_dim_; c++)
           b.original[static_cast<size_t>(i) * sol_dim_ + c] = sol_dim_ * src[i] + c;
     }
   });
+  orig_pending_ = true;
+}
+
+void QuadTreeHost::materialize_originals() {
+  // a split box's list is its points in index order (the reference pushes
+  // every inserted dof into each box on the point's path): the merge of its
+  // children's sorted lists, deepest level first
+  if (!orig_pending_) return;
+  for (int l = static_cast<int>(levels.size()) - 2; l >= 0; l--)
+    for (int id : levels[l]) {
+      Box& b = boxes[id];
+      if (b.leaf) continue;
+      std::vector<int> out;
+      for (int q = 0; q < 4; q++) {
+        const std::vector<int>& c = boxes[b.child[q]].original;
+        std::vector<int> m(out.size() + c.size());
+        std::merge(out.begin(), out.end(), c.begin(), c.end(), m.begin());
+        out.swap(m);
+      }
+      b.original.swap(out);
+    }
+  orig_pending_ = false;
 }
 
 void QuadTreeHost::descendant_neighbors(int big, int small, std::vector<int>* found) const {
@@ -331,6 +368,7 @@ void QuadTreeHost::build_forest(const double* points, int n, int sol_dim, int ma
       if (l < part[p].levels.size())
         for (int id : part[p].levels[l]) levels[l].push_back(id + off[p]);
   for (int p = 0; p < P; p++) roots.push_back(off[p]);
+  orig_pending_ = true;
   min_ = part[0].min_;
   max_ = part[0].max_;
   pts_ = nullptr;
@@ -464,6 +502,9 @@ struct PointHash {
 }  // namespace
 
 void QuadTreeHost::perturb(const double* old_pts, int n_old, const double* new_pts, int n_new) {
+  // split boxes' lists as built, left stale afterwards as the reference
+  // leaves them
+  materialize_originals();
   const int sd = sol_dim_;
   // old point -> new point by exact coordinates (a repeated new point maps
   // to its last index); unmatched old points are deletions, unmatched new

@@ -52,6 +52,10 @@ class QuadTreeHost {
   std::vector<Box> boxes;
   std::vector<std::vector<int>> levels;
 
+  // Fills the `original` lists of split boxes, which the build leaves empty
+  // (only leaves' lists are used by the factorization).  Idempotent.
+  void materialize_originals();
+
   // QuadTree::perturb (quadtree.cpp:359-560): the tree of old_points
   // (n_old points) follows the boundary to new_points (n_new).  Points are
   // matched by exact coordinates; matched dofs are renumbered in every
@@ -82,6 +86,7 @@ class QuadTreeHost {
 
   int sol_dim_ = 1;
   int max_leaf_ = 32;
+  bool orig_pending_ = false;  // split boxes' original lists not made yet
   double min_ = 0, max_ = 0;
   const double* pts_ = nullptr;  // caller's points, valid during the build
   void build_one(int p0, int p1, int tree_id);  // one tree into boxes/levels
