@@ -211,6 +211,9 @@ struct SweepParams {
 // x[red] -= T^T x[skel]; then x[skel] -= L x[red]   (or U^T when use_u)
 cudaError_t launch_sweep_up(const SweepParams& p, bool use_u, cudaStream_t s);
 // x[red] -= U x[skel]; then x[skel] -= T x[red]
+// Both border up sweeps of a level at once: pu (MODE L) and pp (MODE U^T),
+// same tasks, rhs count and capacity, different vectors.
+cudaError_t launch_sweep_up_pair(const SweepParams& pu, const SweepParams& pp, cudaStream_t s);
 cudaError_t launch_sweep_down(const SweepParams& p, cudaStream_t s);
 // x[red] = X_rr^{-1} x[red]
 cudaError_t launch_diag_solve(const SweepParams& p, cudaStream_t s);

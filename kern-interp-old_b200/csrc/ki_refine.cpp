@@ -57,6 +57,10 @@ int Solver::solve_graph(const double* d_b, double* d_mu, double* d_alpha, const 
     return !(e && e[0] == '0');
   }();
   if (!use_graph) return solve_device(d_b, d_mu, d_alpha, d_g);
+  // capturing and instantiating costs more host time than a few solves
+  // save: the graph is made once a factorization has served a few
+  // preconditioner applications, i.e. when it is being reused
+  if (!solve_exec_ && ++graph_uses_ < kGraphAfter) return solve_device(d_b, d_mu, d_alpha, d_g);
   if (!solve_exec_) {
     KI_ALLOC(g_x_, double, static_cast<size_t>(N) + 2 * nb);
     double* ga = g_x_ + N;

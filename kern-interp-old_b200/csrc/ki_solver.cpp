@@ -539,35 +539,44 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
 
   const int nc = static_cast<int>(cand.size());
   std::vector<IdTask> tasks(nc);
-  std::vector<int> act, rows;
   long long a_total = 0, t_total = 0;
   int perm_total = 0;
-  for (int q = 0; q < nc; q++) {
+  size_t act_total = 0, rows_total = 0;
+  for (int q = 0; q < nc; q++) {  // offsets
     const Cand& c = cand[q];
-    const Box& b = tree.boxes[c.box];
     IdTask& t = tasks[q];
-    t.n = c.n;
-    t.m = c.m;
-    t.n_row = c.I;
-    t.proxy = c.m - 2 * c.I;
-    t.act_off = static_cast<int>(act.size());
-    t.row_off = static_cast<int>(rows.size());
     t.lda = c.sk ? onchip_lda(c.sk) : c.g >= kOnChip ? onchip_lda(c.m) : (c.m + 3) & ~3;
-    t.sk = c.sk;
-    t.pad = 0;
+    t.act_off = static_cast<int>(act_total);
+    t.row_off = static_cast<int>(rows_total);
     t.perm_off = perm_total;
     t.a_off = a_total;
     t.t_off = t_total;
-    t.cx = b.corner[0] + b.side / 2.0;
-    t.cy = b.corner[1] + b.side / 2.0;
-    t.rad = b.side * kRadiusRatio;
-    t.pw = 2.0 * M_PI * t.rad / kNumProxy;
-    act.insert(act.end(), b.active.begin(), b.active.end());
-    rows.insert(rows.end(), c.rows.begin(), c.rows.end());
+    act_total += c.n;
+    rows_total += c.rows.size();
     if (c.g < kOnChip) a_total += static_cast<long long>(t.lda) * c.n;  // on-chip: none
     t_total += static_cast<long long>(c.n) * c.n / 4 + 1;
     perm_total += c.n;
   }
+  std::vector<int> act(act_total), rows(rows_total);
+  parallel_for(nc, 16, [&](int a, int e) {  // descriptors and lists
+    for (int q = a; q < e; q++) {
+      const Cand& c = cand[q];
+      const Box& b = tree.boxes[c.box];
+      IdTask& t = tasks[q];
+      t.n = c.n;
+      t.m = c.m;
+      t.n_row = c.I;
+      t.proxy = c.m - 2 * c.I;
+      t.sk = c.sk;
+      t.pad = 0;
+      t.cx = b.corner[0] + b.side / 2.0;
+      t.cy = b.corner[1] + b.side / 2.0;
+      t.rad = b.side * kRadiusRatio;
+      t.pw = 2.0 * M_PI * t.rad / kNumProxy;
+      std::copy(b.active.begin(), b.active.end(), act.begin() + t.act_off);
+      std::copy(c.rows.begin(), c.rows.end(), rows.begin() + t.row_off);
+    }
+  });
   t_host_prep_ms += now_ms() - h0;
   mark(1, level);
   int *d_act, *d_rows, *d_perm, *d_rank;
@@ -665,49 +674,73 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   const double h1 = now_ms();
   mark(2, level);
   std::vector<int> comp;  // candidate indices that compressed
-  for (int q = 0; q < nc; q++) {
-    const Cand& c = cand[q];
-    const IdTask& t = tasks[q];
-    const int k = rank[q];
-    // Algorithmic work of the ID, counted from the actual sizes and rank:
-    // FP64 flops = entry generation (20 per entry) + the Householder steps
-    // actually taken (column dots + rank-one updates over the shrinking
-    // trailing block) + the triangular solve for T; HBM bytes = the dof
-    // lists and node records read, perm and T written, plus, for the
-    // streamed launches, the working matrix written once and read once.
-    // (a sketched box: generation + kSketchBlocks signed adds per entry, the
-    // QR on the sk rows of the sketch)
-    const double n = c.n, m = c.sk ? c.sk : c.m;
-    const int steps = k > 0 ? k : std::min(static_cast<int>(m), c.n);
-    double qr = 20.0 * c.m * n + 1.0 * k * k * (n - k);
-    if (c.sk) qr += 1.0 * kSketchBlocks * c.m * n;
-    for (int j = 0; j < steps; j++) qr += 4.0 * (m - j) * (n - j - 1) + 3.0 * (m - j);
-    const double sd = sd_;  // dofs per node record
-    double bytes = 4.0 * (c.I + 2 * n) + 64.0 * (c.I + c.n) / sd + 8.0 * k * (n - k);
-    if (c.g < kOnChip) bytes += 16.0 * c.m * n;
-    id_flops += qr;
-    id_bytes += bytes;
-    if (c.g >= kOnChip) id_onchip_flops += qr;
-    if (k == 0) continue;
-    Box& b = tree.boxes[c.box];
-    b.compressed = true;
-    b.rank = k;
-    b.perm.assign(perm.begin() + t.perm_off, perm.begin() + t.perm_off + c.n);
-    b.skel.clear();
-    b.redundant.clear();
-    for (int i = 0; i < k; i++) b.skel.push_back(b.active[b.perm[i]]);
-    for (int i = k; i < c.n; i++) b.redundant.push_back(b.active[b.perm[i]]);
-    boxdev_[c.box].T = d_T + t.t_off;
-    comp.push_back(q);
+  {
+    // per candidate, independent: work counts, skeleton / redundant lists
+    std::vector<double> qr_v(nc), bytes_v(nc);
+    parallel_for(nc, 16, [&](int a, int e) {
+      for (int q = a; q < e; q++) {
+        const Cand& c = cand[q];
+        const IdTask& t = tasks[q];
+        const int k = rank[q];
+        // Algorithmic work of the ID, counted from the actual sizes and
+        // rank: FP64 flops = entry generation (20 per entry) + the
+        // Householder steps actually taken (column dots + rank-one updates
+        // over the shrinking trailing block) + the triangular solve for T;
+        // HBM bytes = the dof lists and node records read, perm and T
+        // written, plus, for the streamed launches, the working matrix
+        // written once and read once.  (a sketched box: generation +
+        // kSketchBlocks signed adds per entry, the QR on the sk rows)
+        const double n = c.n, m = c.sk ? c.sk : c.m;
+        const int steps = k > 0 ? k : std::min(static_cast<int>(m), c.n);
+        double qr = 20.0 * c.m * n + 1.0 * k * k * (n - k);
+        if (c.sk) qr += 1.0 * kSketchBlocks * c.m * n;
+        for (int j = 0; j < steps; j++) qr += 4.0 * (m - j) * (n - j - 1) + 3.0 * (m - j);
+        const double sd = sd_;  // dofs per node record
+        double bytes = 4.0 * (c.I + 2 * n) + 64.0 * (c.I + c.n) / sd + 8.0 * k * (n - k);
+        if (c.g < kOnChip) bytes += 16.0 * c.m * n;
+        qr_v[q] = qr;
+        bytes_v[q] = bytes;
+        if (k == 0) continue;
+        Box& b = tree.boxes[c.box];
+        b.compressed = true;
+        b.rank = k;
+        b.perm.assign(perm.begin() + t.perm_off, perm.begin() + t.perm_off + c.n);
+        b.skel.resize(k);
+        b.redundant.resize(c.n - k);
+        for (int i = 0; i < k; i++) b.skel[i] = b.active[b.perm[i]];
+        for (int i = k; i < c.n; i++) b.redundant[i - k] = b.active[b.perm[i]];
+        boxdev_[c.box].T = d_T + t.t_off;
+      }
+    });
+    for (int q = 0; q < nc; q++) {
+      id_flops += qr_v[q];
+      id_bytes += bytes_v[q];
+      if (cand[q].g >= kOnChip) id_onchip_flops += qr_v[q];
+      if (rank[q] > 0) comp.push_back(q);
+    }
   }
   if (comp.empty()) return 0;
 
   // ---- decouple every compressed box of the level
   const int ncomp = static_cast<int>(comp.size());
   std::vector<DecTask> dt(ncomp);
-  std::vector<int> bid, bpos;
-  std::vector<UpdBlock> tab;
-  std::vector<long long> bid_off(ncomp), tab_off(ncomp);
+  // block maps (per position of the box's dof list: which descendant
+  // update, and where in it), made per box in parallel at precomputed offsets
+  std::vector<std::vector<BoxBlock>> blk(ncomp);
+  parallel_for(ncomp, 16, [&](int a, int e) {
+    for (int t = a; t < e; t++) {
+      const Box& b = tree.boxes[cand[comp[t]].box];
+      if (b.leaf) continue;
+      int off = 0;
+      for (int q = 0; q < 4; q++) {
+        const int ch = b.child[q];
+        for (const BoxBlock& x : blocks_of(ch)) blk[t].push_back(BoxBlock{x.acc, x.size, x.pos + off});
+        const Box& cb = tree.boxes[ch];
+        off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
+      }
+    }
+  });
+  std::vector<long long> bid_off(ncomp + 1, 0), tab_off(ncomp + 1, 0);
   long long scratch_total = 0;
   std::vector<long long> k_off(ncomp);
   int n_max = 0;
@@ -716,19 +749,8 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
     const Cand& c = cand[comp[t]];
     const Box& b = tree.boxes[c.box];
     const int n = c.n, k = b.rank, r = n - k;
-    bid_off[t] = static_cast<long long>(bid.size());
-    tab_off[t] = static_cast<long long>(tab.size());
-    std::vector<BoxBlock> blocks;
-    if (!b.leaf) {
-      int off = 0;
-      for (int q = 0; q < 4; q++) {
-        const int ch = b.child[q];
-        for (const BoxBlock& x : blocks_of(ch)) blocks.push_back(BoxBlock{x.acc, x.size, x.pos + off});
-        const Box& cb = tree.boxes[ch];
-        off += static_cast<int>(cb.compressed ? cb.skel.size() : cb.active.size());
-      }
-    }
-    build_block_map(blocks, n, &bid, &bpos, &tab);
+    bid_off[t + 1] = bid_off[t] + n;
+    tab_off[t + 1] = tab_off[t] + static_cast<long long>(blk[t].size());
     k_off[t] = scratch_total;
     if (n > kDecoupleSmemN) {
       scratch_total += static_cast<long long>(n) * n;
@@ -739,6 +761,22 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
                  static_cast<size_t>(k) * k;
     piv_total += r;
   }
+  std::vector<int> bid(bid_off[ncomp], -1), bpos(bid_off[ncomp], 0);
+  std::vector<UpdBlock> tab(tab_off[ncomp]);
+  parallel_for(ncomp, 16, [&](int a, int e) {
+    for (int t = a; t < e; t++) {
+      const std::vector<BoxBlock>& bl = blk[t];
+      int* bi = bid.data() + bid_off[t];
+      int* bp = bpos.data() + bid_off[t];
+      for (size_t q = 0; q < bl.size(); q++) {
+        tab[tab_off[t] + q] = UpdBlock{bl[q].acc, bl[q].size, 0};
+        for (int u = 0; u < bl[q].size; u++) {
+          bi[bl[q].pos + u] = static_cast<int>(q);
+          bp[bl[q].pos + u] = u;
+        }
+      }
+    }
+  });
   int *d_bid, *d_bpos, *d_piv;
   UpdBlock* d_tab;
   double* d_fac;
@@ -871,6 +909,7 @@ void Solver::drop_device_state() {
   // re-points; lazily built buffers are rebuilt on first use
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
   solve_exec_ = nullptr;
+  graph_uses_ = 0;
   g_x_ = nullptr;
   d_mv_tiles_ = nullptr;
   n_mv_tiles_ = mv_splits_ = 0;
@@ -1187,9 +1226,9 @@ int Solver::factor_border() {
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
     SweepParams sp{lf.d_tasks, lf.ntasks, modU, 1, nb, 0, nullptr, lf.cap, nb};
-    KI_CUDA(launch_sweep_up(sp, false, stream_));
-    sp.x = modP;
-    KI_CUDA(launch_sweep_up(sp, true, stream_));
+    SweepParams spp = sp;
+    spp.x = modP;
+    KI_CUDA(launch_sweep_up_pair(sp, spp, stream_));
   }
   if (time_phases && timer_end(b0, {0, 3, 1, nb, 0, N, 0.0})) return -2;
   double *dinv, *us, *ps, *corr;

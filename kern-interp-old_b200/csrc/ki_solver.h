@@ -307,11 +307,13 @@ class Solver {
   Scratch adj_;  // adjoint contraction partials
   Scratch dom_;  // domain evaluation: split partials and the mask
   int mv_setup();  // tile table of the operator product (once)
-  // The solve as a CUDA graph on fixed buffers (captured at the first call,
-  // replayed for every preconditioner application of the refinement):
-  // copies in, one graph launch, copies out.
+  // The solve as a CUDA graph on fixed buffers (captured once the
+  // factorization has served a few preconditioner applications, replayed
+  // for every later one): copies in, one graph launch, copies out.
   int solve_graph(const double* d_b, double* d_mu, double* d_alpha, const double* d_g);
   cudaGraphExec_t solve_exec_ = nullptr;
+  static constexpr int kGraphAfter = 6;  // preconditioner applications before capture
+  int graph_uses_ = 0;
   double* g_x_ = nullptr;  // graph buffers: dofs, then border alpha, then border g
   MvTile* d_mv_tiles_ = nullptr;
   int n_mv_tiles_ = 0, mv_splits_ = 0;

@@ -40,14 +40,19 @@ __device__ __forceinline__ void apply_sub(double* out, const double* in, int row
   for (int t = threadIdx.x; t < rows * nc; t += kSweepThreads) {
     const int i = t / nc, c = t - i * nc;
     const double* a = A + si * i;
-    double s0 = 0.0, s1 = 0.0;
+    // four independent loads in flight per thread
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     int l = 0;
-    for (; l + 1 < inner; l += 2) {
-      s0 += a[sl * l] * in[l * nc + c];
-      s1 += a[sl * (l + 1)] * in[(l + 1) * nc + c];
+    for (; l + 3 < inner; l += 4) {
+      const double a0 = a[sl * l], a1 = a[sl * (l + 1)], a2 = a[sl * (l + 2)],
+                   a3 = a[sl * (l + 3)];
+      s0 += a0 * in[l * nc + c];
+      s1 += a1 * in[(l + 1) * nc + c];
+      s2 += a2 * in[(l + 2) * nc + c];
+      s3 += a3 * in[(l + 3) * nc + c];
     }
-    if (l < inner) s0 += a[sl * l] * in[l * nc + c];
-    out[i * nc + c] -= s0 + s1;
+    for (; l < inner; l++) s0 += a[sl * l] * in[l * nc + c];
+    out[i * nc + c] -= (s0 + s1) + (s2 + s3);
   }
 }
 
@@ -67,7 +72,17 @@ __device__ __forceinline__ void apply_sub_multi(double* out, const double* in, i
     double acc[kGrp];
 #pragma unroll
     for (int c = 0; c < kGrp; c++) acc[c] = 0.0;
-    for (int l = 0; l < inner; l++) {
+    int l = 0;
+    for (; l + 3 < inner; l += 4) {
+      const double av0 = a[sl * l], av1 = a[sl * (l + 1)], av2 = a[sl * (l + 2)],
+                   av3 = a[sl * (l + 3)];
+      const double* x = in + l * nc + c0;
+#pragma unroll
+      for (int c = 0; c < kGrp; c++)
+        if (c < m)
+          acc[c] += av0 * x[c] + av1 * x[nc + c] + av2 * x[2 * nc + c] + av3 * x[3 * nc + c];
+    }
+    for (; l < inner; l++) {
       const double av = a[sl * l];
       const double* x = in + l * nc + c0;
 #pragma unroll
@@ -90,8 +105,7 @@ __device__ __forceinline__ void apply_any(double* out, const double* in, int row
 }
 
 template <int MODE>  // 0 up (L), 1 up (U^T), 2 down, 3 transposed up (L^T, T)
-__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int chunk) {
-  extern __shared__ double sm[];
+__device__ __forceinline__ void sweep_body(const SweepParams& P, int chunk, double* sm) {
   const SweepTask tk = P.tasks[blockIdx.x];
   const int k = tk.k, r = tk.r;
   const int* S = tk.skel;
@@ -146,6 +160,24 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
   }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int chunk) {
+  extern __shared__ double sm[];
+  sweep_body<MODE>(P, chunk, sm);
+}
+
+// The two up sweeps of the hole border (U with L, Psi^T with U^T) of one
+// level in one launch: blockIdx.y picks the sweep.
+__global__ void __launch_bounds__(kSweepThreads) sweep_pair_kernel(SweepParams pu, SweepParams pp,
+                                                                   int chunk) {
+  extern __shared__ double sm[];
+  if (blockIdx.y == 0) {
+    sweep_body<0>(pu, chunk, sm);
+  } else {
+    sweep_body<1>(pp, chunk, sm);
+  }
+}
+
 // x_r <- X_rr^{-1} x_r (TRANS: X_rr^{-T} x_r) on every box's redundant entries,
 // one CTA per box, up to `chunk` right-hand sides per pass staged dof-major
 // in shared memory; the decoupling stored X_rr^{-1} itself, so this is a
@@ -177,8 +209,20 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
         double acc[kGrp];
 #pragma unroll
         for (int c = 0; c < kGrp; c++) acc[c] = 0.0;
-        for (int j = 0; j < r; j++) {
-          const double a = TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
+        auto xa = [&](int j) {
+          return TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
+        };
+        int j = 0;
+        for (; j + 3 < r; j += 4) {
+          const double a0 = xa(j), a1 = xa(j + 1), a2 = xa(j + 2), a3 = xa(j + 3);
+          const double* x = xs + j * nc + cg;
+#pragma unroll
+          for (int c = 0; c < kGrp; c++)
+            if (c < m)
+              acc[c] += a0 * x[c] + a1 * x[nc + c] + a2 * x[2 * nc + c] + a3 * x[3 * nc + c];
+        }
+        for (; j < r; j++) {
+          const double a = xa(j);
           const double* x = xs + j * nc + cg;
 #pragma unroll
           for (int c = 0; c < kGrp; c++)
@@ -191,19 +235,20 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
     } else
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
       const int i = t % r, c = t / r;  // consecutive threads: consecutive rows i
-      double s0 = 0.0, s1 = 0.0;
+      auto xa = [&](int j) {
+        return TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
+      };
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
       int j = 0;
-      for (; j + 1 < r; j += 2) {
-        const double a0 = TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j];
-        const double a1 = TRANS ? Xi[j + 1 + static_cast<long long>(r) * i]
-                                : Xi[i + static_cast<long long>(r) * (j + 1)];
+      for (; j + 3 < r; j += 4) {
+        const double a0 = xa(j), a1 = xa(j + 1), a2 = xa(j + 2), a3 = xa(j + 3);
         s0 += a0 * xs[j * nc + c];
         s1 += a1 * xs[(j + 1) * nc + c];
+        s2 += a2 * xs[(j + 2) * nc + c];
+        s3 += a3 * xs[(j + 3) * nc + c];
       }
-      if (j < r)
-        s0 += (TRANS ? Xi[j + static_cast<long long>(r) * i] : Xi[i + static_cast<long long>(r) * j]) *
-              xs[j * nc + c];
-      ys[i * nc + c] = s0 + s1;
+      for (; j < r; j++) s0 += xa(j) * xs[j * nc + c];
+      ys[i * nc + c] = (s0 + s1) + (s2 + s3);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < r * nc; t += kDiagThreads) {
@@ -232,6 +277,19 @@ cudaError_t launch_sweep_up(const SweepParams& p, bool use_u, cudaStream_t s) {
   if (p.ntasks == 0 || p.nrhs == 0) return cudaSuccess;
   count_launches(1);
   return use_u ? launch_mode<1>(p, s) : launch_mode<0>(p, s);
+}
+
+cudaError_t launch_sweep_up_pair(const SweepParams& pu, const SweepParams& pp, cudaStream_t s) {
+  if (pu.ntasks == 0 || pu.nrhs == 0) return cudaSuccess;
+  const int nc = rhs_chunk(pu.nrhs, pu.cap);
+  const size_t smem = sizeof(double) * static_cast<size_t>(pu.cap) * nc;
+  cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&sweep_pair_kernel),
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem));
+  if (e != cudaSuccess) return e;
+  count_launches(1);
+  sweep_pair_kernel<<<dim3(pu.ntasks, 2), kSweepThreads, smem, s>>>(pu, pp, nc);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_down(const SweepParams& p, cudaStream_t s) {
