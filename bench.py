@@ -11,7 +11,7 @@ skel_factorization.cpp:94-403) to 1e-10 relative error.  The metric is
 unknowns / (factor + solve time), for two methods on the same GPU:
 
   * mixed + refine (`value`): the factorization at ID tolerance 3e-7
-    (1e-6 for stokes65k) in
+    (3e-8 for stokes65k) in
     preconditioner mode (tall ID matrices reduced by a sparse row sketch)
     used by FP64 refinement / GMRES on the operator with on-the-fly FP64
     entries, stopped at true relative residual 1e-12 (ki_factor_ex +
@@ -59,9 +59,9 @@ import ki_geometry as G  # noqa: E402
 METRIC = "factor+solve unknowns/s at 1e-10 rel err"
 MIXED_TOL = 3e-7      # ID tolerance of the preconditioning factorization (default)
 # per workload: the tolerance with the smallest factor + refinement time at
-# the residual bar, measured on a B200 (Stokes: 1e-6 and three products;
-# 3e-7 needs three products as well and a dearer factorization)
-MIXED_TOLS = {"stokes65k": 1e-6}
+# the residual bar, measured on a B200 (Stokes: 3e-8 reaches it in two
+# refinement products, looser tolerances need three)
+MIXED_TOLS = {"stokes65k": 3e-8}
 MIXED_MODE = 1        # KI_MODE_PRECONDITIONER: sketched IDs for tall boxes
 REFINE_TOL = 1e-12    # true relative residual at which the refinement stops
 FP64_TOL = 1e-10

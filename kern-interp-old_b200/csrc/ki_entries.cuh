@@ -37,30 +37,71 @@ __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, 
 __device__ __forceinline__ double subd(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double divd(double a, double b) { return __ddiv_rn(a, b); }
 
+// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
+// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
+// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
+// relative error, so the result is accurate to FP64 rounding.  x = 0 or
+// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
+// only pass far-away padding (whose numerators are zero) beyond it.
+__device__ __forceinline__ double nr_rcp(double x) {
+  float yf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
+  double y = static_cast<double>(yf);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// The arithmetic of the entry formulas.  Exact: every product, sum and
+// quotient a round-to-nearest intrinsic in the reference's evaluation order
+// (no contraction), so entries equal the reference's bits.  Fast: plain
+// expressions (contracted to FMA) and reciprocals by nr_rcp, accurate to a
+// few FP64 ulps: for the sketched IDs of the preconditioner mode, whose
+// skeletons differ from the reference's anyway.
+template <bool FAST>
+struct EM {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <>
+struct EM<true> {
+  static __device__ __forceinline__ double mul(double a, double b) { return a * b; }
+  static __device__ __forceinline__ double add(double a, double b) { return a + b; }
+  static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+  static __device__ __forceinline__ double div(double a, double b) { return a * nr_rcp(b); }
+};
+
 // Kernel::laplace for r = t - s (not the forward/target variant).
+template <bool FAST = false>
 __device__ __forceinline__ double laplace_entry(int pde, double r1, double r2,
                                                 double sw, double sc,
                                                 double sn1, double sn2,
                                                 double tn1, double tn2) {
-  const double rr = add(mul(r1, r1), mul(r2, r2));
+  using M = EM<FAST>;
+  const double rr = M::add(M::mul(r1, r1), M::mul(r2, r2));
   if (pde == kLaplace) {
-    if (r1 == 0. && r2 == 0.) return add(0.5, mul(mul(mul(0.5, sc), sw), KI_INV_2PI));
-    return divd(mul(mul(-sw, KI_INV_2PI), add(mul(r1, sn1), mul(r2, sn2))), rr);
+    if (r1 == 0. && r2 == 0.) return M::add(0.5, M::mul(M::mul(M::mul(0.5, sc), sw), KI_INV_2PI));
+    return M::div(M::mul(M::mul(-sw, KI_INV_2PI), M::add(M::mul(r1, sn1), M::mul(r2, sn2))), rr);
   }
   if (r1 == 0. && r2 == 0.)
-    return add(subd(sw, 0.5), mul(mul(mul(0.5, sc), sw), KI_INV_2PI));
-  return add(sw, divd(mul(mul(sw, KI_INV_2PI), add(mul(r1, tn1), mul(r2, tn2))), rr));
+    return M::add(M::sub(sw, 0.5), M::mul(M::mul(M::mul(0.5, sc), sw), KI_INV_2PI));
+  return M::add(sw, M::div(M::mul(M::mul(sw, KI_INV_2PI), M::add(M::mul(r1, tn1), M::mul(r2, tn2))), rr));
 }
 
 // Boundary operator entry (tgt dof, src dof).  For Stokes a dof is
 // 2*node + component.
+template <bool FAST = false>
 __device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict__ nodes,
                                                  int tgt, int src) {
+  using M = EM<FAST>;
   if (pde != kStokes) {
     const Node s = nodes[src];
     const Node t = nodes[tgt];
-    return laplace_entry(pde, subd(t.x, s.x), subd(t.y, s.y), s.w, s.k, s.nx, s.ny,
-                         t.nx, t.ny);
+    return laplace_entry<FAST>(pde, M::sub(t.x, s.x), M::sub(t.y, s.y), s.w, s.k, s.nx, s.ny,
+                               t.nx, t.ny);
   }
   const Node s = nodes[src >> 1];
   const Node t = nodes[tgt >> 1];
@@ -72,36 +113,46 @@ __device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict
     const int parity = (tgt + src + 1) & 1;
     const double snA = tc ? s.nx : s.ny;  // sn[(tgt + 1) % 2]
     const double snB = sc ? s.nx : s.ny;  // sn[(src + 1) % 2]
-    const double a = mul(-0.5, static_cast<double>(parity));
-    const double b = mul(mul(mul(mul(mul(static_cast<double>(1 - 2 * parity), 0.5), s.k), s.w),
-                             KI_INV_PI), snA);
-    return add(add(a, mul(b, snB)), mul(mul(s.w, tn_t), sn_s));
+    const double a = M::mul(-0.5, static_cast<double>(parity));
+    const double b = M::mul(M::mul(M::mul(M::mul(M::mul(static_cast<double>(1 - 2 * parity), 0.5), s.k), s.w),
+                                   KI_INV_PI), snA);
+    return M::add(M::add(a, M::mul(b, snB)), M::mul(M::mul(s.w, tn_t), sn_s));
   }
-  const double r0 = subd(t.x, s.x), r1 = subd(t.y, s.y);
-  const double rr = add(mul(r0, r0), mul(r1, r1));
-  const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
-                          mul(rr, rr));
+  const double r0 = M::sub(t.x, s.x), r1 = M::sub(t.y, s.y);
+  const double rr = M::add(M::mul(r0, r0), M::mul(r1, r1));
+  double pot;
+  if (FAST) {
+    const double inv = nr_rcp(rr);  // rr (not rr^2) stays in the estimate's range
+    pot = (s.w * KI_INV_PI) * (r0 * s.nx + r1 * s.ny) * (inv * inv);
+  } else {
+    pot = M::div(M::mul(M::mul(s.w, KI_INV_PI), M::add(M::mul(r0, s.nx), M::mul(r1, s.ny))),
+                 M::mul(rr, rr));
+  }
   const double rt = tc ? r1 : r0, rs = sc ? r1 : r0;
-  return add(mul(mul(pot, rt), rs), mul(mul(s.w, tn_t), sn_s));
+  return M::add(M::mul(M::mul(pot, rt), rs), M::mul(M::mul(s.w, tn_t), sn_s));
 }
 
 // Proxy-block row `row` (0 <= row < 2*128 for Laplace, 4*128 for Stokes) for
 // box column dof `src` (kernel.cpp:268-334); circle centre (cx, cy), radius r.
+template <bool FAST = false>
 __device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ nodes,
                                               const double* __restrict__ dir,
                                               int row, int src, double cx, double cy,
                                               double r, double pw) {
+  using M = EM<FAST>;
   const double* c_proxy_cos = dir;
   const double* c_proxy_sin = dir + kNumProxy;
   if (pde != kStokes) {
     const Node b = nodes[src];
     const int q = row & (kNumProxy - 1);
-    const double px = add(cx, mul(r, c_proxy_cos[q]));
-    const double py = add(cy, mul(r, c_proxy_sin[q]));
-    const double r0 = subd(px, b.x), r1 = subd(py, b.y);
+    const double px = M::add(cx, M::mul(r, c_proxy_cos[q]));
+    const double py = M::add(cy, M::mul(r, c_proxy_sin[q]));
+    const double r0 = M::sub(px, b.x), r1 = M::sub(py, b.y);
     if (row < kNumProxy)
-      return laplace_entry(pde, r0, r1, b.w, 0.0, b.nx, b.ny, c_proxy_cos[q], c_proxy_sin[q]);
-    return laplace_entry(pde, -r0, -r1, pw, 0.0, c_proxy_cos[q], c_proxy_sin[q], b.nx, b.ny);
+      return laplace_entry<FAST>(pde, r0, r1, b.w, 0.0, b.nx, b.ny, c_proxy_cos[q],
+                                 c_proxy_sin[q]);
+    return laplace_entry<FAST>(pde, -r0, -r1, pw, 0.0, c_proxy_cos[q], c_proxy_sin[q], b.nx,
+                               b.ny);
   }
   const Node s = nodes[src >> 1];
   const int scomp = src & 1;
@@ -109,22 +160,22 @@ __device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ 
   const int rr_ = second ? row - 2 * kNumProxy : row;
   const int q = rr_ >> 1, comp = rr_ & 1;
   const double tn0 = c_proxy_cos[q], tn1 = c_proxy_sin[q];
-  const double px = add(cx, mul(r, tn0));
-  const double py = add(cy, mul(r, tn1));
-  const double r0 = subd(px, s.x), r1 = subd(py, s.y);
-  const double rr = add(mul(r0, r0), mul(r1, r1));
+  const double px = M::add(cx, M::mul(r, tn0));
+  const double py = M::add(cy, M::mul(r, tn1));
+  const double r0 = M::sub(px, s.x), r1 = M::sub(py, s.y);
+  const double rr = M::add(M::mul(r0, r0), M::mul(r1, r1));
   const double rs = scomp ? r1 : r0;
   const double rc = comp ? r1 : r0;
   const double sns = scomp ? s.ny : s.nx;
   const double tnc = comp ? tn1 : tn0;
   if (!second) {
-    const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
-                            mul(rr, rr));
-    return add(mul(mul(pot, rc), rs), mul(mul(s.w, tnc), sns));
+    const double pot = M::div(M::mul(M::mul(s.w, KI_INV_PI), M::add(M::mul(r0, s.nx), M::mul(r1, s.ny))),
+                              M::mul(rr, rr));
+    return M::add(M::mul(M::mul(pot, rc), rs), M::mul(M::mul(s.w, tnc), sns));
   }
-  const double pot = divd(mul(mul(-pw, KI_INV_PI), add(mul(r0, tn0), mul(r1, tn1))),
-                          mul(rr, rr));
-  return add(mul(mul(pot, rc), rs), mul(mul(pw, sns), tnc));
+  const double pot = M::div(M::mul(M::mul(-pw, KI_INV_PI), M::add(M::mul(r0, tn0), M::mul(r1, tn1))),
+                            M::mul(rr, rr));
+  return M::add(M::mul(M::mul(pot, rc), rs), M::mul(M::mul(pw, sns), tnc));
 }
 
 // Forward (target-point) entry of Kernel::forward (kernel.cpp:337-357) with
@@ -158,22 +209,6 @@ __device__ __forceinline__ double forward_entry(int pde, const Node* __restrict_
   const double pot = divd(mul(mul(s.w, KI_INV_PI), add(mul(r0, s.nx), mul(r1, s.ny))),
                           mul(rr, rr));
   return mul(mul(pot, tgt_comp ? r1 : r0), sc ? r1 : r0);
-}
-
-// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
-// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
-// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
-// relative error, so the result is accurate to FP64 rounding.  x = 0 or
-// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
-// only pass far-away padding (whose numerators are zero) beyond it.
-__device__ __forceinline__ double nr_rcp(double x) {
-  float yf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
-  double y = static_cast<double>(yf);
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
 }
 
 // Border columns for one target point (initialize_U_mat, linear_solve.cpp:18-64).

@@ -496,7 +496,7 @@ constexpr int kOcWarps = kOcThreads / 32;
 // CTA has independent work to hide shared-memory and FP64 latency.
 
 template <int G>
-__global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
+__global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int task = blockIdx.x / G;
   int g = 0;
@@ -523,6 +523,7 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
   int* pos2col = reinterpret_cast<int*>(slot + 2);       // n
   int* own = pos2col + n;                                // n
   int* si = own + n;                                     // [0] own count, [1] pivot
+  int* hs = si + 8;  // sketch: hashed target row of each (tile row, block), ~row if subtracted
 
   auto colp = [&](int j) -> double* {
     double* base = cols + static_cast<long long>(j / G) * lda;
@@ -584,6 +585,13 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
     if (r < 2 * I) return boundary_entry(pde, nodes, cd, rowd[r - I]);
     return proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
   };
+  // sketched boxes (preconditioner mode only): fast entries
+  auto entry_fast = [&](int r, int cd) -> double {
+    if (r < I) return boundary_entry<true>(pde, nodes, rowd[r], cd);
+    if (r < 2 * I) return boundary_entry<true>(pde, nodes, cd, rowd[r - I]);
+    return proxy_entry<true>(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad,
+                             tk.pw);
+  };
   if (sketch) {
     // Y = S A for this CTA's columns, accumulated kSketchTile rows of A at a
     // time: the rows are generated into `tile`, then work item (column,
@@ -599,7 +607,14 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
       __syncthreads();
       for (int e = threadIdx.x; e < rows * nloc; e += kOcThreads) {
         const int rr = e % rows, t = e / rows;
-        tile[rr + (kSketchTile + 1) * t] = entry_at(r0 + rr, act[g + G * t]);
+        tile[rr + (kSketchTile + 1) * t] = entry_fast(r0 + rr, act[g + G * t]);
+      }
+      // the row hashes depend on (row, block) only: once per tile, not per
+      // column
+      for (int e = threadIdx.x; e < rows * kSketchBlocks; e += kOcThreads) {
+        const unsigned h = sketch_hash(static_cast<unsigned>(r0) * kSketchBlocks + e);
+        const int idx = static_cast<int>(h % blk);
+        hs[e] = (h & 0x80000000u) ? ~idx : idx;
       }
       __syncthreads();
       for (int it = threadIdx.x; it < nloc * kSketchBlocks; it += kOcThreads) {
@@ -607,9 +622,13 @@ __global__ void __launch_bounds__(kOcThreads, 1) id_onchip_kernel(IdParams P) {
         double* ycol = cols + static_cast<long long>(lda) * t + b * blk;
         const double* tcol = tile + (kSketchTile + 1) * t;
         for (int rr = 0; rr < rows; rr++) {
-          const unsigned h = sketch_hash(static_cast<unsigned>(r0 + rr) * kSketchBlocks + b);
+          const int code = hs[rr * kSketchBlocks + b];
           const double a = tcol[rr];
-          ycol[h % blk] += (h & 0x80000000u) ? -a : a;
+          if (code < 0) {
+            ycol[~code] += -a;
+          } else {
+            ycol[code] += a;
+          }
         }
       }
     }
@@ -904,7 +923,8 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 size_t id_sketch_smem_bytes(int sk, int n, int G) {
   const size_t nloc = static_cast<size_t>((n + G - 1) / G);
   return id_smem_bytes(sk, n) +
-         sizeof(double) * (nloc * onchip_lda(sk) + static_cast<size_t>(kSketchTile + 1) * nloc);
+         sizeof(double) * (nloc * onchip_lda(sk) + static_cast<size_t>(kSketchTile + 1) * nloc) +
+         sizeof(int) * kSketchTile * kSketchBlocks;
 }
 
 size_t id_onchip_smem_bytes(int m, int n, int G) {

@@ -518,15 +518,19 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
       if (c.m == 0) continue;
       c.g = pick_group(c.m, c.n, onchip_ok_);
       if (opt_.sketch_id) {
-        // the smallest cluster whose shared memory holds the sketch
+        // the smallest cluster whose CTAs' shares of the sketch leave room
+        // for two CTAs per SM (a single CTA per SM leaves the SM idle at
+        // every barrier of the pivoted QR), else the smallest that fits
         const int l = sketch_rows(c.n);
         if (c.m > l + 64)
-          for (int G = 1; G <= 16; G *= 2)
-            if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= 227 * 1024) {
-              c.sk = l;
-              c.g = kOnChip + G;
-              break;
-            }
+          for (const size_t cap : {size_t{113} * 1024, size_t{227} * 1024}) {
+            for (int G = 1; G <= 16 && !c.sk; G *= 2)
+              if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) {
+                c.sk = l;
+                c.g = kOnChip + G;
+              }
+            if (c.sk) break;
+          }
       }
       keep[q] = 1;
     }
