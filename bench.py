@@ -127,14 +127,44 @@ def fp64_peak_tflops(dev):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: NVML
+    polled every 2 ms from a background thread (the timed region of a short
+    run lasts well under nvidia-smi's sampling interval); `nvidia-smi -lms
+    200` if NVML is unavailable.  Read-only queries."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, dev):
+        import threading
         self.proc = None
+        self.samples = []
+        self.stop_ev = threading.Event()
+        self.thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(dev)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def poll():
+                while not self.stop_ev.is_set():
+                    try:
+                        self.samples.append(
+                            (float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                             int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        pass
+                    self.stop_ev.wait(0.002)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(dev), "--query-gpu=" + self.Q,
@@ -144,6 +174,19 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_ev.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = set()
+            for _, bits in self.samples:
+                for name, bit in self.REASONS:
+                    if bits & bit:
+                        reasons.add(name)
+            return {"sm_mhz": float(np.median([c for c, _ in self.samples])),
+                    "sm_max_mhz": self.max_mhz, "reasons": sorted(reasons),
+                    "samples": len(self.samples), "source": "nvml"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -169,7 +212,7 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 # ------------------------------------------------------------------ CPU arms
