@@ -19,8 +19,8 @@ struct ki_solver_s {
   size_t io_bytes = 0;
   bool tree_only = false;  // ki_partition handle: no factors on the device
   ~ki_solver_s() {
-    solver.reset();
-    if (d_io) cudaFree(d_io);
+    solver.reset();  // synchronises the stream: nothing queued uses d_io
+    if (d_io) kib::chunk_pool::put(d_io, io_bytes, false);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 };
@@ -40,13 +40,21 @@ int from_solver(ki_solver_t s, int rc) {
 }
 
 int staging(ki_solver_t s, size_t bytes) {
+  // device staging of the host-buffer calls, from the process-wide chunk
+  // cache (a fresh handle per solve then costs no cudaMalloc / cudaFree)
   if (bytes <= s->io_bytes) return KI_OK;
-  if (s->d_io) cudaFree(s->d_io);
+  if (s->d_io) {
+    const cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return set_err(KI_ERR_CUDA, cudaGetErrorString(e));
+    kib::chunk_pool::put(s->d_io, s->io_bytes, false);
+  }
   s->d_io = nullptr;
   s->io_bytes = 0;
-  cudaError_t e = cudaMalloc(&s->d_io, bytes);
-  if (e != cudaSuccess) return set_err(KI_ERR_CUDA, cudaGetErrorString(e));
-  s->io_bytes = bytes;
+  size_t got = 0;
+  void* p = kib::chunk_pool::get(bytes, false, &got);
+  if (!p) return set_err(KI_ERR_CUDA, "device staging allocation failed");
+  s->d_io = static_cast<double*>(p);
+  s->io_bytes = got;
   return KI_OK;
 }
 

@@ -185,6 +185,24 @@ Solver::Solver(const SolverOptions& opt, int n_points, const double* points,
   if (n_holes > 0) holes_.assign(holes, holes + 4 * static_cast<size_t>(n_holes));
 }
 
+namespace {
+// Side streams and their events, kept for reuse by later solvers on the
+// same device (creating and destroying them costs more host time than a
+// small factorization's level loop).
+struct AuxSet {
+  int dev = -1;
+  cudaStream_t d = nullptr;
+  cudaEvent_t ev_id = nullptr, ev_dec = nullptr, fork = nullptr;
+  cudaStream_t id[3] = {};
+  cudaEvent_t join[3] = {};
+};
+std::mutex g_aux_mu;
+std::vector<AuxSet>& aux_free() {
+  static std::vector<AuxSet> v;
+  return v;
+}
+}  // namespace
+
 Solver::~Solver() {
   // chunks go back to the pool only once no queued work can touch them
   cudaStreamSynchronize(stream_);
@@ -192,13 +210,20 @@ Solver::~Solver() {
   if (dstream_) cudaStreamSynchronize(dstream_);
   for (int i = 0; i < kIdStreams; i++)
     if (id_streams_[i]) cudaStreamSynchronize(id_streams_[i]);
-  if (ev_id_) cudaEventDestroy(ev_id_);
-  if (ev_dec_) cudaEventDestroy(ev_dec_);
-  if (dstream_) cudaStreamDestroy(dstream_);
-  if (id_fork_) cudaEventDestroy(id_fork_);
-  for (int i = 0; i < kIdStreams; i++) {
-    if (id_join_[i]) cudaEventDestroy(id_join_[i]);
-    if (id_streams_[i]) cudaStreamDestroy(id_streams_[i]);
+  if (dstream_) {
+    static_assert(kIdStreams == 3, "AuxSet holds three ID streams");
+    AuxSet a;
+    cudaGetDevice(&a.dev);
+    a.d = dstream_;
+    a.ev_id = ev_id_;
+    a.ev_dec = ev_dec_;
+    a.fork = id_fork_;
+    for (int i = 0; i < kIdStreams; i++) {
+      a.id[i] = id_streams_[i];
+      a.join[i] = id_join_[i];
+    }
+    std::lock_guard<std::mutex> lk(g_aux_mu);
+    aux_free().push_back(a);
   }
 }
 
@@ -331,13 +356,36 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
   id_flops = id_bytes = id_onchip_flops = 0;
 
   if (!dstream_) {
-    KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
-    KI_CUDA(cudaEventCreateWithFlags(&ev_id_, cudaEventDisableTiming));
-    KI_CUDA(cudaEventCreateWithFlags(&ev_dec_, cudaEventDisableTiming));
-    KI_CUDA(cudaEventCreateWithFlags(&id_fork_, cudaEventDisableTiming));
-    for (int i = 0; i < kIdStreams; i++) {
-      KI_CUDA(cudaStreamCreateWithFlags(&id_streams_[i], cudaStreamNonBlocking));
-      KI_CUDA(cudaEventCreateWithFlags(&id_join_[i], cudaEventDisableTiming));
+    int dev = 0;
+    KI_CUDA(cudaGetDevice(&dev));
+    {
+      // a cached set of this device, if a finished solver left one
+      std::lock_guard<std::mutex> lk(g_aux_mu);
+      auto& fl = aux_free();
+      for (size_t i = 0; i < fl.size(); i++)
+        if (fl[i].dev == dev) {
+          const AuxSet a = fl[i];
+          fl.erase(fl.begin() + static_cast<long>(i));
+          dstream_ = a.d;
+          ev_id_ = a.ev_id;
+          ev_dec_ = a.ev_dec;
+          id_fork_ = a.fork;
+          for (int k = 0; k < kIdStreams; k++) {
+            id_streams_[k] = a.id[k];
+            id_join_[k] = a.join[k];
+          }
+          break;
+        }
+    }
+    if (!dstream_) {
+      KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_id_, cudaEventDisableTiming));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_dec_, cudaEventDisableTiming));
+      KI_CUDA(cudaEventCreateWithFlags(&id_fork_, cudaEventDisableTiming));
+      for (int i = 0; i < kIdStreams; i++) {
+        KI_CUDA(cudaStreamCreateWithFlags(&id_streams_[i], cudaStreamNonBlocking));
+        KI_CUDA(cudaEventCreateWithFlags(&id_join_[i], cudaEventDisableTiming));
+      }
     }
   }
   {
