@@ -195,6 +195,8 @@ struct AuxSet {
   cudaEvent_t ev_id = nullptr, ev_dec = nullptr, fork = nullptr;
   cudaStream_t id[3] = {};
   cudaEvent_t join[3] = {};
+  cudaStream_t dl[3] = {};
+  cudaEvent_t dl_fork = nullptr, dl_join[3] = {};
 };
 std::mutex g_aux_mu;
 std::vector<AuxSet>& aux_free() {
@@ -210,8 +212,10 @@ Solver::~Solver() {
   if (dstream_) cudaStreamSynchronize(dstream_);
   for (int i = 0; i < kIdStreams; i++)
     if (id_streams_[i]) cudaStreamSynchronize(id_streams_[i]);
+  for (int i = 0; i < kDecStreams; i++)
+    if (dl_streams_[i]) cudaStreamSynchronize(dl_streams_[i]);
   if (dstream_) {
-    static_assert(kIdStreams == 3, "AuxSet holds three ID streams");
+    static_assert(kIdStreams == 3 && kDecStreams == 3, "AuxSet holds three of each");
     AuxSet a;
     cudaGetDevice(&a.dev);
     a.d = dstream_;
@@ -221,6 +225,11 @@ Solver::~Solver() {
     for (int i = 0; i < kIdStreams; i++) {
       a.id[i] = id_streams_[i];
       a.join[i] = id_join_[i];
+    }
+    a.dl_fork = dl_fork_;
+    for (int i = 0; i < kDecStreams; i++) {
+      a.dl[i] = dl_streams_[i];
+      a.dl_join[i] = dl_join_[i];
     }
     std::lock_guard<std::mutex> lk(g_aux_mu);
     aux_free().push_back(a);
@@ -374,6 +383,11 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
             id_streams_[k] = a.id[k];
             id_join_[k] = a.join[k];
           }
+          dl_fork_ = a.dl_fork;
+          for (int k = 0; k < kDecStreams; k++) {
+            dl_streams_[k] = a.dl[k];
+            dl_join_[k] = a.dl_join[k];
+          }
           break;
         }
     }
@@ -385,6 +399,11 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
       for (int i = 0; i < kIdStreams; i++) {
         KI_CUDA(cudaStreamCreateWithFlags(&id_streams_[i], cudaStreamNonBlocking));
         KI_CUDA(cudaEventCreateWithFlags(&id_join_[i], cudaEventDisableTiming));
+      }
+      KI_CUDA(cudaEventCreateWithFlags(&dl_fork_, cudaEventDisableTiming));
+      for (int i = 0; i < kDecStreams; i++) {
+        KI_CUDA(cudaStreamCreateWithFlags(&dl_streams_[i], cudaStreamNonBlocking));
+        KI_CUDA(cudaEventCreateWithFlags(&dl_join_[i], cudaEventDisableTiming));
       }
     }
   }
@@ -895,9 +914,25 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   if (time_phases && timer_begin(&d0, dstream_)) return -2;
   KI_CUDA(launch_decouple(dp, n_max, dstream_));
   int n_large = 0;
-  for (const DecTask& d : large) {
-    KI_CUDA(decouple_large(d, opt_.pde, d_nodes_, d_status_, dstream_));
-    n_large = std::max(n_large, d.n);
+  if (!large.empty()) {
+    // the large boxes side by side on their own streams, after the level's
+    // uploads, joined back into dstream_
+    KI_CUDA(cudaEventRecord(dl_fork_, dstream_));
+    bool used[kDecStreams] = {};
+    for (size_t t = 0; t < large.size(); t++) {
+      const int si = static_cast<int>(t % kDecStreams);
+      if (!used[si]) {
+        KI_CUDA(cudaStreamWaitEvent(dl_streams_[si], dl_fork_, 0));
+        used[si] = true;
+      }
+      KI_CUDA(decouple_large(large[t], opt_.pde, d_nodes_, d_status_, dl_streams_[si]));
+      n_large = std::max(n_large, large[t].n);
+    }
+    for (int i = 0; i < kDecStreams; i++)
+      if (used[i]) {
+        KI_CUDA(cudaEventRecord(dl_join_[i], dl_streams_[i]));
+        KI_CUDA(cudaStreamWaitEvent(dstream_, dl_join_[i], 0));
+      }
   }
   if (time_phases &&
       timer_end(d0, {level, 1, static_cast<int>(large.size()), ncomp, n_large, n_max, 0.0},

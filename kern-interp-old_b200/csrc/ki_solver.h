@@ -258,6 +258,11 @@ class Solver {
   static constexpr int kIdStreams = 3;
   cudaStream_t id_streams_[kIdStreams] = {};
   cudaEvent_t id_fork_ = nullptr, id_join_[kIdStreams] = {};
+  // The few boxes too big for the batched decouple (one multi-kernel
+  // sequence each) run on these, concurrently with each other.
+  static constexpr int kDecStreams = 3;
+  cudaStream_t dl_streams_[kDecStreams] = {};
+  cudaEvent_t dl_fork_ = nullptr, dl_join_[kDecStreams] = {};
 
   bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
