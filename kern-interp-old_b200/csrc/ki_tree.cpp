@@ -6,6 +6,7 @@
 #include "ki_pool.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -77,50 +78,91 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
     const int base = static_cast<int>(tb.size());
     tb.resize(base + 4 * split.size());
     moment.resize(tb.size(), -1);
-    parallel_for(static_cast<int>(split.size()), 4, [&](int a, int e) {
-      for (int s = a; s < e; s++) {
-        Tmp& P = tb[split[s]];
-        const int b0 = P.begin;
-        int* rp = perm.data() + b0;
-        double* rxy = pxy.data() + 2 * static_cast<size_t>(b0);
-        moment[split[s]] = rp[cap];  // the range is still in index order
-        const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
-        const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
-        int cnt[4] = {0, 0, 0, 0};
-        for (int i = 0; i < P.count; i++) {
-          const double x = rxy[2 * i], y = rxy[2 * i + 1];
-          const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
-          quad[b0 + i] = static_cast<unsigned char>(q);
-          cnt[q]++;
+    // one box: classify its points by child, then a stable scatter from a
+    // copy of the range; a big box (the first levels) is cut into chunks
+    // classified and scattered in parallel at per-chunk offsets (chunks in
+    // order, sequential inside: still stable)
+    auto split_box = [&](int s, bool inner_parallel) {
+      Tmp& P = tb[split[s]];
+      const int b0 = P.begin, cnt_all = P.count;
+      int* rp = perm.data() + b0;
+      double* rxy = pxy.data() + 2 * static_cast<size_t>(b0);
+      moment[split[s]] = rp[cap];  // the range is still in index order
+      const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
+      const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
+      const int kChunk = 4096;
+      const int nch = inner_parallel ? (cnt_all + kChunk - 1) / kChunk : 1;
+      const int csz = inner_parallel ? kChunk : cnt_all;
+      std::vector<std::array<int, 4>> ccnt(nch, std::array<int, 4>{0, 0, 0, 0});
+      auto classify = [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+          const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
+          for (int i = i0; i < i1; i++) {
+            const double x = rxy[2 * i], y = rxy[2 * i + 1];
+            const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
+            quad[b0 + i] = static_cast<unsigned char>(q);
+            ccnt[c][q]++;
+          }
+          std::memcpy(tmpi.data() + b0 + i0, rp + i0, sizeof(int) * (i1 - i0));
+          std::memcpy(tmpxy.data() + 2 * static_cast<size_t>(b0 + i0), rxy + 2 * i0,
+                      2 * sizeof(double) * (i1 - i0));
         }
-        std::memcpy(tmpi.data() + b0, rp, sizeof(int) * P.count);
-        std::memcpy(tmpxy.data() + 2 * static_cast<size_t>(b0), rxy,
-                    2 * sizeof(double) * P.count);
-        int pos[4];
-        pos[0] = 0;
-        for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
-        const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
-                                 {mx, my, mx, my}, {mx, mx, my, my}};
-        for (int q = 0; q < 4; q++) {
-          Tmp& C = tb[base + 4 * s + q];
-          C.parent = split[s];
-          C.level = P.level + 1;
-          C.begin = b0 + pos[q];
-          C.count = cnt[q];
-          std::memcpy(C.corner, P.corner, sizeof(C.corner));
-          for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
-          P.child[q] = base + 4 * s + q;
-        }
-        // stable scatter from the copy
-        const int* oi = tmpi.data() + b0;
-        const double* oxy = tmpxy.data() + 2 * static_cast<size_t>(b0);
-        for (int i = 0; i < P.count; i++) {
-          const int d = pos[quad[b0 + i]]++;
-          rp[d] = oi[i];
-          rxy[2 * d] = oxy[2 * i];
-          rxy[2 * d + 1] = oxy[2 * i + 1];
-        }
+      };
+      if (inner_parallel) parallel_for(nch, 1, classify, 2); else classify(0, 1);
+      int cnt[4] = {0, 0, 0, 0};
+      for (int c = 0; c < nch; c++)
+        for (int q = 0; q < 4; q++) cnt[q] += ccnt[c][q];
+      int pos[4];
+      pos[0] = 0;
+      for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
+      // each chunk's first destination per child
+      std::vector<std::array<int, 4>> cpos(nch);
+      {
+        int run[4] = {pos[0], pos[1], pos[2], pos[3]};
+        for (int c = 0; c < nch; c++)
+          for (int q = 0; q < 4; q++) {
+            cpos[c][q] = run[q];
+            run[q] += ccnt[c][q];
+          }
       }
+      const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
+                               {mx, my, mx, my}, {mx, mx, my, my}};
+      for (int q = 0; q < 4; q++) {
+        Tmp& C = tb[base + 4 * s + q];
+        C.parent = split[s];
+        C.level = P.level + 1;
+        C.begin = b0 + pos[q];
+        C.count = cnt[q];
+        std::memcpy(C.corner, P.corner, sizeof(C.corner));
+        for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
+        P.child[q] = base + 4 * s + q;
+      }
+      const int* oi = tmpi.data() + b0;
+      const double* oxy = tmpxy.data() + 2 * static_cast<size_t>(b0);
+      auto scatter = [&](int c0, int c1) {
+        for (int c = c0; c < c1; c++) {
+          int at[4] = {cpos[c][0], cpos[c][1], cpos[c][2], cpos[c][3]};
+          const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
+          for (int i = i0; i < i1; i++) {
+            const int d = at[quad[b0 + i]]++;
+            rp[d] = oi[i];
+            rxy[2 * d] = oxy[2 * i];
+            rxy[2 * d + 1] = oxy[2 * i + 1];
+          }
+        }
+      };
+      if (inner_parallel) parallel_for(nch, 1, scatter, 2); else scatter(0, 1);
+    };
+    std::vector<int> small_ones;
+    for (int s = 0; s < static_cast<int>(split.size()); s++) {
+      if (tb[split[s]].count >= 16384) {
+        split_box(s, true);
+      } else {
+        small_ones.push_back(s);
+      }
+    }
+    parallel_for(static_cast<int>(small_ones.size()), 4, [&](int a, int e) {
+      for (int q = a; q < e; q++) split_box(small_ones[q], false);
     });
     frontier.clear();
     for (size_t i = base; i < tb.size(); i++) frontier.push_back(static_cast<int>(i));
