@@ -59,9 +59,27 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   std::memcpy(tb[0].corner, c0, sizeof(c0));
   const int np = p1 - p0;
   tb[0].count = np;
-  std::vector<int> perm(np), tmpi(np);
-  std::vector<double> pxy(2 * static_cast<size_t>(np)), tmpxy(2 * static_cast<size_t>(np));
-  std::vector<unsigned char> quad(np);
+  // work arrays kept per thread between builds (no zero fill, no fresh
+  // pages: a build is otherwise dominated by first-touch page faults)
+  struct Work {
+    std::vector<int> perm, tmpi;
+    std::vector<double> pxy, tmpxy;
+    std::vector<unsigned char> quad;
+  };
+  thread_local Work wk;
+  auto grow = [](auto& v, size_t n) {
+    if (v.size() < n) v.resize(n);
+  };
+  grow(wk.perm, np);
+  grow(wk.tmpi, np);
+  grow(wk.pxy, 2 * static_cast<size_t>(np));
+  grow(wk.tmpxy, 2 * static_cast<size_t>(np));
+  grow(wk.quad, np);
+  std::vector<int>& perm = wk.perm;
+  std::vector<int>& tmpi = wk.tmpi;
+  std::vector<double>& pxy = wk.pxy;
+  std::vector<double>& tmpxy = wk.tmpxy;
+  std::vector<unsigned char>& quad = wk.quad;
   for (int q = 0; q < np; q++) {
     perm[q] = p0 + q;
     pxy[2 * q] = pts_[2 * static_cast<size_t>(p0 + q)];
@@ -161,9 +179,10 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
         small_ones.push_back(s);
       }
     }
-    parallel_for(static_cast<int>(small_ones.size()), 4, [&](int a, int e) {
+    // every box is real work: spread even a handful of them
+    parallel_for(static_cast<int>(small_ones.size()), 1, [&](int a, int e) {
       for (int q = a; q < e; q++) split_box(small_ones[q], false);
-    });
+    }, 2);
     frontier.clear();
     for (size_t i = base; i < tb.size(); i++) frontier.push_back(static_cast<int>(i));
   }
