@@ -37,16 +37,14 @@ __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, 
 __device__ __forceinline__ double subd(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ double divd(double a, double b) { return __ddiv_rn(a, b); }
 
-// 1 / x for x > 0 in the FP32 normal range: a single-precision hardware
-// estimate (PTX rcp.approx.ftz.f32, about 2^-22 relative error) refined by
-// two Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
-// relative error, so the result is accurate to FP64 rounding.  x = 0 or
-// beyond FP32 range gives 0 or inf estimates; callers exclude x = 0 and
-// only pass far-away padding (whose numerators are zero) beyond it.
+// 1 / x for normal x > 0: the hardware's approximate FP64 reciprocal (PTX
+// rcp.approx.ftz.f64, an estimate good to roughly 20 bits) refined by two
+// Newton-Raphson steps y <- y + y (1 - x y) in FP64, each squaring the
+// relative error, so the result is accurate to FP64 rounding.  x = 0 gives
+// an infinite estimate: callers exclude it.
 __device__ __forceinline__ double nr_rcp(double x) {
-  float yf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(static_cast<float>(x)));
-  double y = static_cast<double>(yf);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
   double e = fma(-x, y, 1.0);
   y = fma(y, e, y);
   e = fma(-x, y, 1.0);
