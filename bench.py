@@ -215,6 +215,17 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
+def max_over_ranks(times, dist, device):
+    """Every rank's timings replaced by their maximum over the ranks (the
+    job's time is its slowest replica's); unchanged without a process group."""
+    if not dist:
+        return list(times)
+    import torch
+    t = torch.tensor(list(times), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 # ------------------------------------------------------------------ CPU arms
 def _ref_solver():
     import kioracle as K
@@ -466,12 +477,7 @@ def main():
 
     t_e2e = timed_loop(e2e_step)
 
-    t_max = [t_mixed, t_fp64, t_e2e]
-    if dist:
-        t = torch.tensor(t_max, device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = [float(x) for x in t]
-    t_mixed, t_fp64, t_e2e = t_max
+    t_mixed, t_fp64, t_e2e = max_over_ranks([t_mixed, t_fp64, t_e2e], dist, dev)
 
     if rank == 0:
         # accuracy against the FP64 oracle (at the reference's 1e-10 and,
