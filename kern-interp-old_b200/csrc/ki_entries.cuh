@@ -89,20 +89,16 @@ __device__ __forceinline__ double laplace_entry(int pde, double r1, double r2,
   return M::add(sw, M::div(M::mul(M::mul(sw, KI_INV_2PI), M::add(M::mul(r1, tn1), M::mul(r2, tn2))), rr));
 }
 
-// Boundary operator entry (tgt dof, src dof).  For Stokes a dof is
-// 2*node + component.
+// Boundary operator entry for target dof `tgt` at node t and source dof
+// `src` at node s (the dofs give the Stokes components; for Stokes a dof is
+// 2*node + component).
 template <bool FAST = false>
-__device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict__ nodes,
-                                                 int tgt, int src) {
+__device__ __forceinline__ double pair_entry(int pde, const Node& t, int tgt, const Node& s,
+                                             int src) {
   using M = EM<FAST>;
-  if (pde != kStokes) {
-    const Node s = nodes[src];
-    const Node t = nodes[tgt];
+  if (pde != kStokes)
     return laplace_entry<FAST>(pde, M::sub(t.x, s.x), M::sub(t.y, s.y), s.w, s.k, s.nx, s.ny,
                                t.nx, t.ny);
-  }
-  const Node s = nodes[src >> 1];
-  const Node t = nodes[tgt >> 1];
   const int tc = tgt & 1, sc = src & 1;
   const double sn_s = sc ? s.ny : s.nx;   // sn[src % 2]
   const double tn_t = tc ? t.ny : t.nx;   // tn[tgt % 2]
@@ -130,18 +126,26 @@ __device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict
   return M::add(M::mul(M::mul(pot, rt), rs), M::mul(M::mul(s.w, tn_t), sn_s));
 }
 
+// Boundary operator entry (tgt dof, src dof) from the node array.
+template <bool FAST = false>
+__device__ __forceinline__ double boundary_entry(int pde, const Node* __restrict__ nodes,
+                                                 int tgt, int src) {
+  const int sh = pde == kStokes ? 1 : 0;
+  return pair_entry<FAST>(pde, nodes[tgt >> sh], tgt, nodes[src >> sh], src);
+}
+
 // Proxy-block row `row` (0 <= row < 2*128 for Laplace, 4*128 for Stokes) for
 // box column dof `src` (kernel.cpp:268-334); circle centre (cx, cy), radius r.
 template <bool FAST = false>
-__device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ nodes,
-                                              const double* __restrict__ dir,
-                                              int row, int src, double cx, double cy,
-                                              double r, double pw) {
+__device__ __forceinline__ double proxy_entry_node(int pde, const Node& nd,
+                                                   const double* __restrict__ dir, int row,
+                                                   int src, double cx, double cy, double r,
+                                                   double pw) {
   using M = EM<FAST>;
   const double* c_proxy_cos = dir;
   const double* c_proxy_sin = dir + kNumProxy;
   if (pde != kStokes) {
-    const Node b = nodes[src];
+    const Node& b = nd;
     const int q = row & (kNumProxy - 1);
     const double px = M::add(cx, M::mul(r, c_proxy_cos[q]));
     const double py = M::add(cy, M::mul(r, c_proxy_sin[q]));
@@ -152,7 +156,7 @@ __device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ 
     return laplace_entry<FAST>(pde, -r0, -r1, pw, 0.0, c_proxy_cos[q], c_proxy_sin[q], b.nx,
                                b.ny);
   }
-  const Node s = nodes[src >> 1];
+  const Node& s = nd;
   const int scomp = src & 1;
   const bool second = row >= 2 * kNumProxy;
   const int rr_ = second ? row - 2 * kNumProxy : row;
@@ -174,6 +178,16 @@ __device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ 
   const double pot = M::div(M::mul(M::mul(-pw, KI_INV_PI), M::add(M::mul(r0, tn0), M::mul(r1, tn1))),
                             M::mul(rr, rr));
   return M::add(M::mul(M::mul(pot, rc), rs), M::mul(M::mul(pw, sns), tnc));
+}
+
+// The same with the box dof's node taken from the node array.
+template <bool FAST = false>
+__device__ __forceinline__ double proxy_entry(int pde, const Node* __restrict__ nodes,
+                                              const double* __restrict__ dir,
+                                              int row, int src, double cx, double cy,
+                                              double r, double pw) {
+  return proxy_entry_node<FAST>(pde, nodes[pde == kStokes ? src >> 1 : src], dir, row, src, cx,
+                                cy, r, pw);
 }
 
 // Forward (target-point) entry of Kernel::forward (kernel.cpp:337-357) with

@@ -28,6 +28,7 @@
 #include <cooperative_groups.h>
 
 #include <cmath>
+#include <cstdint>
 #include <mutex>
 
 #include "ki_kernels.h"
@@ -585,13 +586,6 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     if (r < 2 * I) return boundary_entry(pde, nodes, cd, rowd[r - I]);
     return proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
   };
-  // sketched boxes (preconditioner mode only): fast entries
-  auto entry_fast = [&](int r, int cd) -> double {
-    if (r < I) return boundary_entry<true>(pde, nodes, rowd[r], cd);
-    if (r < 2 * I) return boundary_entry<true>(pde, nodes, cd, rowd[r - I]);
-    return proxy_entry<true>(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad,
-                             tk.pw);
-  };
   if (sketch) {
     // Y = S A for this CTA's columns, accumulated kSketchTile rows of A at a
     // time: the rows are generated into `tile`, then work item (column,
@@ -600,14 +594,31 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     // deterministic.  Columns never mix, so the CTAs of a cluster need no
     // exchange here.
     const int mA = tk.m, blk = m / kSketchBlocks;
+    // node records staged in shared memory (entries then read no global
+    // memory): this CTA's columns once, each tile's rows per tile
+    const int sh = pde == kStokes ? 1 : 0;
+    Node* cn = reinterpret_cast<Node*>(
+        (reinterpret_cast<uintptr_t>(hs + kSketchTile * kSketchBlocks) + 15) & ~uintptr_t{15});
+    Node* rn = cn + nloc;
+    int* cdof = reinterpret_cast<int*>(rn + kSketchTile);
+    int* rdof = cdof + nloc;
+    for (int t = threadIdx.x; t < nloc; t += kOcThreads) {
+      const int cd = act[g + G * t];
+      cdof[t] = cd;
+      cn[t] = nodes[cd >> sh];
+    }
     for (long long e = threadIdx.x; e < static_cast<long long>(lda) * nloc; e += kOcThreads)
       cols[e] = 0.0;
     for (int r0 = 0; r0 < mA; r0 += kSketchTile) {
       const int rows = min(kSketchTile, mA - r0);
       __syncthreads();
-      for (int e = threadIdx.x; e < rows * nloc; e += kOcThreads) {
-        const int rr = e % rows, t = e / rows;
-        tile[rr + (kSketchTile + 1) * t] = entry_fast(r0 + rr, act[g + G * t]);
+      for (int rr = threadIdx.x; rr < rows; rr += kOcThreads) {
+        const int r = r0 + rr;
+        if (r < 2 * I) {
+          const int d = rowd[r < I ? r : r - I];
+          rdof[rr] = d;
+          rn[rr] = nodes[d >> sh];
+        }
       }
       // the row hashes depend on (row, block) only: once per tile, not per
       // column
@@ -615,6 +626,21 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
         const unsigned h = sketch_hash(static_cast<unsigned>(r0) * kSketchBlocks + e);
         const int idx = static_cast<int>(h % blk);
         hs[e] = (h & 0x80000000u) ? ~idx : idx;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < rows * nloc; e += kOcThreads) {
+        const int rr = e % rows, t = e / rows;
+        const int r = r0 + rr;
+        double val;
+        if (r < I) {
+          val = pair_entry<true>(pde, rn[rr], rdof[rr], cn[t], cdof[t]);
+        } else if (r < 2 * I) {
+          val = pair_entry<true>(pde, cn[t], cdof[t], rn[rr], rdof[rr]);
+        } else {
+          val = proxy_entry_node<true>(pde, cn[t], P.proxy_dir, r - 2 * I, cdof[t], tk.cx, tk.cy,
+                                       tk.rad, tk.pw);
+        }
+        tile[rr + (kSketchTile + 1) * t] = val;
       }
       __syncthreads();
       for (int it = threadIdx.x; it < nloc * kSketchBlocks; it += kOcThreads) {
@@ -922,9 +948,12 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 
 size_t id_sketch_smem_bytes(int sk, int n, int G) {
   const size_t nloc = static_cast<size_t>((n + G - 1) / G);
+  // matrix share, row tile, row hashes, staged node records and dofs of the
+  // columns and of one row tile (+ alignment)
   return id_smem_bytes(sk, n) +
          sizeof(double) * (nloc * onchip_lda(sk) + static_cast<size_t>(kSketchTile + 1) * nloc) +
-         sizeof(int) * kSketchTile * kSketchBlocks;
+         sizeof(int) * kSketchTile * kSketchBlocks +
+         (sizeof(Node) + sizeof(int)) * (nloc + kSketchTile) + 16;
 }
 
 size_t id_onchip_smem_bytes(int m, int n, int G) {
