@@ -39,7 +39,8 @@ enum { KI_LAPLACE = 0, KI_LAPLACE_NEUMANN = 1, KI_STOKES = 2 };
  * (same partition, ranks and skeletons).  KI_MODE_PRECONDITIONER: for a
  * factorization used by ki_solve_refined: boxes whose ID matrix is much
  * taller than wide are decomposed through a sparse random row sketch
- * (cheaper, different skeletons, same accuracy class). */
+ * whose proxy circle has 64 of the reference's 128 points (cheaper,
+ * different skeletons, same accuracy class). */
 enum { KI_MODE_REFERENCE = 0, KI_MODE_PRECONDITIONER = 1 };
 
 /* Message of the last failing call on this thread ("" if none). */

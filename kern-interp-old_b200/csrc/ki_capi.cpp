@@ -119,6 +119,7 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
   opt.max_leaf_dofs = max_leaf_dofs;
   opt.id_tol = id_tol;
   opt.sketch_id = mode == KI_MODE_PRECONDITIONER;
+  opt.proxy_shift = opt.sketch_id ? 1 : 0;  // 64 proxy points for sketched boxes
   h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, n_holes,
                                   holes, h->stream));
   h->solver->time_phases = timed;

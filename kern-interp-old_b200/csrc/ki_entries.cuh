@@ -140,17 +140,18 @@ template <bool FAST = false>
 __device__ __forceinline__ double proxy_entry_node(int pde, const Node& nd,
                                                    const double* __restrict__ dir, int row,
                                                    int src, double cx, double cy, double r,
-                                                   double pw) {
+                                                   double pw, int ps = 0) {
   using M = EM<FAST>;
   const double* c_proxy_cos = dir;
   const double* c_proxy_sin = dir + kNumProxy;
+  const int np = kNumProxy >> ps;  // every 2^ps-th point of the table
   if (pde != kStokes) {
     const Node& b = nd;
-    const int q = row & (kNumProxy - 1);
+    const int q = (row & (np - 1)) << ps;
     const double px = M::add(cx, M::mul(r, c_proxy_cos[q]));
     const double py = M::add(cy, M::mul(r, c_proxy_sin[q]));
     const double r0 = M::sub(px, b.x), r1 = M::sub(py, b.y);
-    if (row < kNumProxy)
+    if (row < np)
       return laplace_entry<FAST>(pde, r0, r1, b.w, 0.0, b.nx, b.ny, c_proxy_cos[q],
                                  c_proxy_sin[q]);
     return laplace_entry<FAST>(pde, -r0, -r1, pw, 0.0, c_proxy_cos[q], c_proxy_sin[q], b.nx,
@@ -158,9 +159,9 @@ __device__ __forceinline__ double proxy_entry_node(int pde, const Node& nd,
   }
   const Node& s = nd;
   const int scomp = src & 1;
-  const bool second = row >= 2 * kNumProxy;
-  const int rr_ = second ? row - 2 * kNumProxy : row;
-  const int q = rr_ >> 1, comp = rr_ & 1;
+  const bool second = row >= 2 * np;
+  const int rr_ = second ? row - 2 * np : row;
+  const int q = (rr_ >> 1) << ps, comp = rr_ & 1;
   const double tn0 = c_proxy_cos[q], tn1 = c_proxy_sin[q];
   const double px = M::add(cx, M::mul(r, tn0));
   const double py = M::add(cy, M::mul(r, tn1));

@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
           val = pair_entry<true>(pde, cn[t], cdof[t], rn[rr], rdof[rr]);
         } else {
           val = proxy_entry_node<true>(pde, cn[t], P.proxy_dir, r - 2 * I, cdof[t], tk.cx, tk.cy,
-                                       tk.rad, tk.pw);
+                                       tk.rad, tk.pw, tk.pshift);
         }
         tile[rr + (kSketchTile + 1) * t] = val;
       }

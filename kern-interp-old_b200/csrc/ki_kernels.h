@@ -36,7 +36,7 @@ struct IdTask {
   long long t_off;  // T output (doubles), capacity n*n/4 + 1
   double cx, cy, rad, pw;  // proxy circle centre, radius, weight
   int sk;         // > 0: on-chip CTA factors the sk x n row sketch S A instead of A
-  int pad;
+  int pshift;     // sketched tasks: proxy circle of kNumProxy >> pshift points
 };
 
 // Row sketch of an ID matrix (on-chip, one CTA): S has kSketchBlocks blocks

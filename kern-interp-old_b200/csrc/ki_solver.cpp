@@ -598,6 +598,7 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
               }
             if (c.sk) break;
           }
+        if (c.sk && level > 2) c.m = 2 * c.I + (P >> opt_.proxy_shift);
       }
       keep[q] = 1;
     }
@@ -639,11 +640,11 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
       t.n_row = c.I;
       t.proxy = c.m - 2 * c.I;
       t.sk = c.sk;
-      t.pad = 0;
+      t.pshift = c.sk && level > 2 ? opt_.proxy_shift : 0;
       t.cx = b.corner[0] + b.side / 2.0;
       t.cy = b.corner[1] + b.side / 2.0;
       t.rad = b.side * kRadiusRatio;
-      t.pw = 2.0 * M_PI * t.rad / kNumProxy;
+      t.pw = 2.0 * M_PI * t.rad / (kNumProxy >> t.pshift);
       std::copy(b.active.begin(), b.active.end(), act.begin() + t.act_off);
       std::copy(c.rows.begin(), c.rows.end(), rows.begin() + t.row_off);
     }

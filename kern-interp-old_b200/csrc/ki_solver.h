@@ -75,6 +75,11 @@ struct SolverOptions {
   // reference, same accuracy class); for factorizations used with the
   // refinement, never for reference-identical results.
   bool sketch_id = false;
+  // Sketched boxes sample the proxy circle at every 2^proxy_shift-th of the
+  // reference's kNumProxy points: the circle's representation error decays
+  // like (box radius / circle radius)^points, far below a preconditioner's
+  // tolerance at 64 points.
+  int proxy_shift = 0;
 };
 
 // Device factors of one compressed box, for copying between solvers.
