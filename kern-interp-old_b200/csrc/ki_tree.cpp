@@ -314,47 +314,79 @@ void QuadTreeHost::neighbor_lists() {
   // then its siblings, its same-level cousins whose lower-left corners lie
   // within side*sqrt(2), and (for leaves) the adjacent finer boxes, each of
   // which also records the leaf.  The per-box searches of a level only read
-  // finished lists, so they run in parallel; the appends are made in the
-  // level's box order, as the reference makes them.
+  // finished lists and append to their own box's list, so they run in
+  // parallel; the finer boxes' records of the leaves that found them are
+  // appended afterwards in the level's box order, as the reference makes
+  // them.
+  // per finer box: how many leaves of the level found it, where its
+  // records start in `by`, how many are placed (reset after each level)
+  std::vector<int> cnt(boxes.size(), 0), start(boxes.size(), 0), fill(boxes.size(), 0);
+  std::vector<int> touched, by;
   for (size_t l = 0; l < levels.size(); l++) {
     const std::vector<int>& ids = levels[l];
     const int n = static_cast<int>(ids.size());
-    std::vector<std::vector<int>> near(n), found(n);
+    std::vector<std::vector<int>> found(n);
     parallel_for(n, 8, [&](int b0, int b1) {
       for (int i = b0; i < b1; i++) {
         const int a = ids[i];
-        const int par = boxes[a].parent;
-        std::vector<int>& nr = near[i];
+        Box& box = boxes[a];
+        const int par = box.parent;
+        std::vector<int>& nb = box.nbr;
+        const size_t own0 = nb.size();
         if (par >= 0) {
+          const Box& pb = boxes[par];
+          nb.reserve(own0 + 8);
           for (int q = 0; q < 4; q++)
-            if (boxes[par].child[q] != a) nr.push_back(boxes[par].child[q]);
-          for (int o : boxes[par].nbr) {
+            if (pb.child[q] != a) nb.push_back(pb.child[q]);
+          for (int o : pb.nbr) {
             for (int q = 0; q < 4; q++) {
               const int cz = boxes[o].child[q];
-              if (cz < 0 || boxes[cz].level != boxes[a].level) continue;
+              if (cz < 0 || boxes[cz].level != box.level) continue;
               // (squares by multiplication: the corner distances are 0,
               // side, sqrt(2) side, ..., far from the 1e-5 margin, so the
               // outcome is that of the reference's pow form)
-              const double dx = boxes[a].corner[0] - boxes[cz].corner[0];
-              const double dy = boxes[a].corner[1] - boxes[cz].corner[1];
+              const double dx = box.corner[0] - boxes[cz].corner[0];
+              const double dy = box.corner[1] - boxes[cz].corner[1];
               const double dist = std::sqrt(dx * dx + dy * dy);
-              if (dist < boxes[a].side * std::sqrt(2) + 1e-5) nr.push_back(cz);
+              if (dist < box.side * std::sqrt(2) + 1e-5) nb.push_back(cz);
             }
           }
         }
-        if (boxes[a].leaf)
-          for (int o : nr)  // all of the same level
+        if (box.leaf) {
+          std::vector<int>& fd = found[i];
+          const size_t own1 = nb.size();
+          for (size_t u = own0; u < own1; u++) {  // all of the same level
+            const int o = nb[u];
             for (int q = 0; q < 4; q++)
-              if (boxes[o].child[q] >= 0) descendant_neighbors(a, boxes[o].child[q], &found[i]);
+              if (boxes[o].child[q] >= 0) descendant_neighbors(a, boxes[o].child[q], &fd);
+          }
+          nb.insert(nb.end(), fd.begin(), fd.end());
+        }
       }
     });
-    for (int i = 0; i < n; i++) {
-      const int a = ids[i];
-      std::vector<int>& nb = boxes[a].nbr;
-      nb.insert(nb.end(), near[i].begin(), near[i].end());
-      nb.insert(nb.end(), found[i].begin(), found[i].end());
-      for (int sm : found[i]) boxes[sm].nbr.push_back(a);
+    // the records grouped by finer box, each group in the level's box order,
+    // then appended box by box in parallel
+    touched.clear();
+    for (int i = 0; i < n; i++)
+      for (int sm : found[i])
+        if (cnt[sm]++ == 0) touched.push_back(sm);
+    int total = 0;
+    for (int sm : touched) {
+      start[sm] = total;
+      total += cnt[sm];
     }
+    by.resize(total);
+    for (int i = 0; i < n; i++)
+      for (int sm : found[i]) by[start[sm] + fill[sm]++] = ids[i];
+    parallel_for(static_cast<int>(touched.size()), 32, [&](int b0, int b1) {
+      for (int u = b0; u < b1; u++) {
+        const int sm = touched[u];
+        std::vector<int>& nb = boxes[sm].nbr;
+        nb.insert(nb.end(), by.begin() + start[sm], by.begin() + start[sm] + cnt[sm]);
+        cnt[sm] = 0;
+        fill[sm] = 0;
+      }
+    });
   }
 }
 
