@@ -163,7 +163,7 @@ cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* s
     return e;
   if ((e = cudaMemcpyAsync(Ksnr, tk.L, sizeof(double) * r * k, cudaMemcpyDeviceToDevice, s)))
     return e;
-  if ((e = dense_lu(tk.X, r, r, tk.piv, status, s))) return e;
+  if ((e = dense_lu(tk.X, r, r, tk.piv, status, s, reinterpret_cast<int*>(tk.K + nn)))) return e;
   count_launches(1);
   identity_kernel<<<(r * r + 255) / 256, 256, 0, s>>>(Y, r);
   if ((e = cudaGetLastError())) return e;

@@ -754,9 +754,258 @@ cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv
 namespace {
 constexpr size_t kPanelSmemMax = 200 * 1024;
 constexpr size_t kSolveSmemMax = 200 * 1024;
+
+// ---- single-launch LU for matrices of up to kLuFusedMaxN rows
+//
+// CTA b of the cooperative grid owns columns [32 b, 32 b + 32) in shared
+// memory for the whole factorization.  For every panel k < b it waits for
+// panel k's flag, then applies that step to its own columns exactly as the
+// panel-by-panel path does (row interchanges, U12 = L11^{-1} A12, A22 -=
+// L21 U12, same operation order, hence the same bits wherever that path
+// takes 32-column panels, i.e. up to 512 rows); then it factors its own
+// panel (the pivot search over its rows, one row interchange, the rank-one
+// update: two barriers per column), publishes the block and its pivots and
+// raises flag b.  The next panel's owner starts as soon as it has applied
+// step b, while the others are still updating: the dependent chain is
+// panel, one step's update on one CTA, panel, ...  Finished blocks apply
+// the later steps' interchanges to their L rows and write them back at the
+// end.  Every read of another CTA's data bypasses L1 (the lines may hold
+// values from before the step).  Every wait is bounded: on a timeout (or
+// another CTA's) the CTA sets *status = 2 and returns.
+constexpr int kFusedThreads = 512;
+constexpr unsigned long long kFusedWaitNs = 200ull * 1000 * 1000;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Thread 0 waits (bounded) for flag k; false for every thread on an abort.
+__device__ bool fused_wait(int* sync, int k, int G, int* status, int* s_ok) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned long long t0 = global_ns();
+    while (ld_acquire_gpu(sync + k) == 0) {
+      if (ld_acquire_gpu(sync + G) != 0 || global_ns() - t0 > kFusedWaitNs) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!ok) {
+      atomicExch(sync + G, 1);
+      atomicExch(status, 2);
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// Row interchanges of one step on this CTA's columns (rows >= j0; one lane
+// per column, in pivot order).
+__device__ __forceinline__ void fused_swaps(double* blk, int np, int n, int j0, int wk, int wb,
+                                            const int* pv) {
+  if (threadIdx.x < wb) {
+    const int c = threadIdx.x;
+    for (int jj = 0; jj < wk; jj++) {
+      const int p = pv[jj], r = j0 + jj;
+      if (p > r && p < n) {
+        const double t = blk[r + np * c];
+        blk[r + np * c] = blk[p + np * c];
+        blk[p + np * c] = t;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1)
+    lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync) {
+  extern __shared__ double blk[];  // np x kNb, column-major
+  __shared__ double l11[kNb][kNb + 1];
+  __shared__ double red[kFusedThreads / 32];
+  __shared__ int redi[kFusedThreads / 32];
+  __shared__ int pv[kNb];
+  __shared__ int s_ok;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int np = n | 1;
+  const int c0 = kNb * b, wb = min(kNb, n - c0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c = 0; c < wb; c++) {  // one column per pass: loads in flight
+#pragma unroll 2
+    for (int i = tid; i < n; i += kFusedThreads)
+      blk[i + np * c] = a[i + static_cast<long long>(ld) * (c0 + c)];
+  }
+  __syncthreads();
+
+  // the steps of the panels to the left
+  for (int k = 0; k < b; k++) {
+    if (!fused_wait(sync, k, G, status, &s_ok)) return;
+    const int j0 = kNb * k, wk = min(kNb, n - j0);
+    for (int e = tid; e < wk * wk; e += kFusedThreads) {
+      const int i = e % wk, kk = e / wk;
+      l11[i][kk] = __ldcg(a + j0 + i + static_cast<long long>(ld) * (j0 + kk));
+    }
+    if (tid < wk) pv[tid] = __ldcg(ipiv + j0 + tid);
+    __syncthreads();
+    fused_swaps(blk, np, n, j0, wk, wb, pv);
+    __syncthreads();
+    // U12 = L11^{-1} A12, one warp per column, in the kk order of the
+    // panel-by-panel path
+    for (int c = warp; c < wb; c += kFusedThreads / 32) {
+      double x = lane < wk ? blk[j0 + lane + np * c] : 0.0;
+      for (int kk = 0; kk < wk; kk++) {
+        const double xk = __shfl_sync(0xffffffffu, x, kk);
+        if (lane > kk && lane < wk) x -= xk * l11[lane][kk];
+      }
+      if (lane < wk) blk[j0 + lane + np * c] = x;
+    }
+    __syncthreads();
+    // A22 -= L21 U12 (the sum over kk first, then subtracted)
+    for (int i = j0 + wk + tid; i < n; i += kFusedThreads) {
+      double acc[kNb];
+#pragma unroll
+      for (int c = 0; c < kNb; c++) acc[c] = 0.0;
+      // L21's row in groups of 8 loads in flight (kk order kept)
+      for (int kk0 = 0; kk0 < wk; kk0 += 8) {
+        double l[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+          l[q] = kk0 + q < wk ? __ldcg(a + i + static_cast<long long>(ld) * (j0 + kk0 + q)) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          if (kk0 + q >= wk) break;
+          const double* u = blk + j0 + kk0 + q;
+#pragma unroll
+          for (int c = 0; c < kNb; c++) acc[c] += l[q] * u[np * c];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < kNb; c++)
+        if (c < wb) blk[i + np * c] -= acc[c];
+    }
+    __syncthreads();
+  }
+
+  // this CTA's panel: rows c0.., thread t owning rows t + 512 q
+  for (int jj = 0; jj < wb; jj++) {
+    const int col = c0 + jj;
+    double bv = -1.0;
+    int bp = 0x7fffffff;
+    for (int i = tid; i < n; i += kFusedThreads) {
+      if (i < col) continue;
+      const double v = fabs(blk[i + np * jj]);
+      if (v > bv) {
+        bv = v;
+        bp = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) {
+      red[warp] = bv;
+      redi[warp] = bp;
+    }
+    __syncthreads();
+    double v = lane < kFusedThreads / 32 ? red[lane] : -1.0;
+    int p = lane < kFusedThreads / 32 ? redi[lane] : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+      const int op = __shfl_xor_sync(0xffffffffu, p, o);
+      if (ov > v || (ov == v && op < p)) {
+        v = ov;
+        p = op;
+      }
+    }
+    // no comparable entry (NaN column): keep the row, flag the factorization
+    const bool bad = p < col || p >= n;
+    if (bad) p = col;
+    if (tid < wb && p != col) {
+      const double t = blk[col + np * tid];
+      blk[col + np * tid] = blk[p + np * tid];
+      blk[p + np * tid] = t;
+    }
+    __syncthreads();
+    const double piv = blk[col + np * jj];
+    if (tid == 0) {
+      ipiv[col] = p;
+      if (piv == 0.0 || bad) atomicExch(status, 1);
+    }
+    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+    for (int i = tid; i < n; i += kFusedThreads) {
+      if (i <= col) continue;
+      const double li = blk[i + np * jj] * inv;
+      for (int c = jj + 1; c < wb; c++) blk[i + np * c] -= li * blk[col + np * c];
+      blk[i + np * jj] = li;
+    }
+    // the next column's barrier orders these updates before its
+    // interchange; the pivot row is not updated
+  }
+  __syncthreads();
+  for (int e = tid; e < n * wb; e += kFusedThreads) {
+    const int i = e % n, c = e / n;
+    __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    st_release_gpu(sync + b, 1);
+  }
+  if (b + 1 == G) return;
+
+  // the later steps' interchanges on this block's L rows, then those rows
+  // written again (every CTA that reads this panel has done so before the
+  // last flag is raised)
+  for (int k = b + 1; k < G; k++) {
+    if (!fused_wait(sync, k, G, status, &s_ok)) return;
+    const int j0 = kNb * k, wk = min(kNb, n - j0);
+    if (tid < wk) pv[tid] = __ldcg(ipiv + j0 + tid);
+    __syncthreads();
+    fused_swaps(blk, np, n, j0, wk, wb, pv);
+    __syncthreads();
+  }
+  const int r1 = c0 + kNb;
+  for (int e = tid; e < (n - r1) * wb; e += kFusedThreads) {
+    const int i = r1 + e % (n - r1), c = e / (n - r1);
+    __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
+  }
+}
 }  // namespace
 
-cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s) {
+cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s,
+                     int* sync) {
+  if (sync && n > 0 && n <= kLuFusedMaxN) {
+    int G = (n + kNb - 1) / kNb;
+    const size_t smem = sizeof(double) * static_cast<size_t>(n | 1) * kNb;
+    cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_fused_kernel),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(sync, 0, sizeof(int) * (G + 1), s)) != cudaSuccess) return e;
+    void* args[] = {&a, &n, &ld, &ipiv, &status, &sync};
+    count_launches(1);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&lu_fused_kernel),
+                                       dim3(G), dim3(kFusedThreads), args, smem, s);
+  }
   for (int j0 = 0; j0 < n;) {
     // register-resident panels: 32 columns while a thread holds one row,
     // 16 columns for two rows

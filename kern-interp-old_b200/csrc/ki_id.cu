@@ -510,11 +510,10 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
 
   // layout of this task (every CTA of the cluster has the same task)
   double* cols = reinterpret_cast<double*>(smem_raw);   // owned columns
-  double* tile = cols + static_cast<long long>((n + G - 1) / G) * lda;  // sketch: rows of A
   const int nloc = (n - g + G - 1) / G;  // columns j = g + G t owned by this CTA
   // (the layout must be the same in every CTA of the cluster, whose peers
-  // read `slot` at the local offset: size the tile for the largest share)
-  double* v = tile + (sketch ? static_cast<long long>(kSketchTile + 1) * ((n + G - 1) / G) : 0);  // m
+  // read `slot` at the local offset: sized for the largest share)
+  double* v = cols + static_cast<long long>((n + G - 1) / G) * lda;  // m
   double* rdiag = v + m;                                 // n
   double* vn1 = rdiag + n;                               // n
   double* vn2 = vn1 + n;                                 // n
@@ -524,7 +523,6 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
   int* pos2col = reinterpret_cast<int*>(slot + 2);       // n
   int* own = pos2col + n;                                // n
   int* si = own + n;                                     // [0] own count, [1] pivot
-  int* hs = si + 8;  // sketch: hashed target row of each (tile row, block), ~row if subtracted
 
   auto colp = [&](int j) -> double* {
     double* base = cols + static_cast<long long>(j / G) * lda;
@@ -587,21 +585,20 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     return proxy_entry(pde, nodes, P.proxy_dir, r - 2 * I, cd, tk.cx, tk.cy, tk.rad, tk.pw);
   };
   if (sketch) {
-    // Y = S A for this CTA's columns, accumulated kSketchTile rows of A at a
-    // time: the rows are generated into `tile`, then work item (column,
-    // block b) adds each row, signed, into its hashed row of block b; items
-    // own disjoint entries of Y and add the rows in order, so the result is
-    // deterministic.  Columns never mix, so the CTAs of a cluster need no
-    // exchange here.
+    // Y = S A for this CTA's columns.  Warp w owns columns t = w, w + 16, ...
+    // and walks the rows of A 32 at a time, lane l generating row r0 + l in
+    // registers; per block, the lanes whose rows hash to the same row of Y
+    // (found with match.any) are summed in lane order through shuffles and
+    // the group's first lane adds the sum.  A column is only touched by its
+    // warp, pass after pass in row order, so the result is deterministic,
+    // and no barrier is needed.  Columns never mix, so the CTAs of a cluster
+    // need no exchange here.
     const int mA = tk.m, blk = m / kSketchBlocks;
-    // node records staged in shared memory (entries then read no global
-    // memory): this CTA's columns once, each tile's rows per tile
     const int sh = pde == kStokes ? 1 : 0;
+    // this CTA's column node records and dofs, staged once
     Node* cn = reinterpret_cast<Node*>(
-        (reinterpret_cast<uintptr_t>(hs + kSketchTile * kSketchBlocks) + 15) & ~uintptr_t{15});
-    Node* rn = cn + nloc;
-    int* cdof = reinterpret_cast<int*>(rn + kSketchTile);
-    int* rdof = cdof + nloc;
+        (reinterpret_cast<uintptr_t>(si + 8) + 15) & ~uintptr_t{15});
+    int* cdof = reinterpret_cast<int*>(cn + nloc);
     for (int t = threadIdx.x; t < nloc; t += kOcThreads) {
       const int cd = act[g + G * t];
       cdof[t] = cd;
@@ -609,51 +606,59 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     }
     for (long long e = threadIdx.x; e < static_cast<long long>(lda) * nloc; e += kOcThreads)
       cols[e] = 0.0;
-    for (int r0 = 0; r0 < mA; r0 += kSketchTile) {
-      const int rows = min(kSketchTile, mA - r0);
-      __syncthreads();
-      for (int rr = threadIdx.x; rr < rows; rr += kOcThreads) {
-        const int r = r0 + rr;
-        if (r < 2 * I) {
-          const int d = rowd[r < I ? r : r - I];
-          rdof[rr] = d;
-          rn[rr] = nodes[d >> sh];
+    __syncthreads();
+    if (warp < nloc) {
+      for (int r0 = 0; r0 < mA; r0 += 32) {
+        const int r = r0 + lane;
+        const bool valid = r < mA;
+        Node rnode = {};
+        int rdof = 0;
+        if (valid && r < 2 * I) {
+          rdof = rowd[r < I ? r : r - I];
+          rnode = nodes[rdof >> sh];
         }
-      }
-      // the row hashes depend on (row, block) only: once per tile, not per
-      // column
-      for (int e = threadIdx.x; e < rows * kSketchBlocks; e += kOcThreads) {
-        const unsigned h = sketch_hash(static_cast<unsigned>(r0) * kSketchBlocks + e);
-        const int idx = static_cast<int>(h % blk);
-        hs[e] = (h & 0x80000000u) ? ~idx : idx;
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < rows * nloc; e += kOcThreads) {
-        const int rr = e % rows, t = e / rows;
-        const int r = r0 + rr;
-        double val;
-        if (r < I) {
-          val = pair_entry<true>(pde, rn[rr], rdof[rr], cn[t], cdof[t]);
-        } else if (r < 2 * I) {
-          val = pair_entry<true>(pde, cn[t], cdof[t], rn[rr], rdof[rr]);
-        } else {
-          val = proxy_entry_node<true>(pde, cn[t], P.proxy_dir, r - 2 * I, cdof[t], tk.cx, tk.cy,
-                                       tk.rad, tk.pw, tk.pshift);
+        // this row's hashed row of Y in each block (sign from the top bit)
+        // and the lanes sharing it; an idle lane is a group of its own
+        int idx[kSketchBlocks];
+        bool neg[kSketchBlocks];
+        unsigned grp[kSketchBlocks];
+        int gmax = 0;
+#pragma unroll
+        for (int b = 0; b < kSketchBlocks; b++) {
+          const unsigned h = sketch_hash(static_cast<unsigned>(r) * kSketchBlocks + b);
+          idx[b] = static_cast<int>(h % blk);
+          neg[b] = (h & 0x80000000u) != 0;
+          grp[b] = __match_any_sync(0xffffffffu, valid ? idx[b] : -1 - lane);
+          gmax = max(gmax, __popc(grp[b]));
         }
-        tile[rr + (kSketchTile + 1) * t] = val;
-      }
-      __syncthreads();
-      for (int it = threadIdx.x; it < nloc * kSketchBlocks; it += kOcThreads) {
-        const int t = it % nloc, b = it / nloc;
-        double* ycol = cols + static_cast<long long>(lda) * t + b * blk;
-        const double* tcol = tile + (kSketchTile + 1) * t;
-        for (int rr = 0; rr < rows; rr++) {
-          const int code = hs[rr * kSketchBlocks + b];
-          const double a = tcol[rr];
-          if (code < 0) {
-            ycol[~code] += -a;
-          } else {
-            ycol[code] += a;
+        gmax = __reduce_max_sync(0xffffffffu, gmax);
+        for (int t = warp; t < nloc; t += kOcWarps) {
+          double val = 0.0;
+          if (valid) {
+            if (r < I) {
+              val = pair_entry<true>(pde, rnode, rdof, cn[t], cdof[t]);
+            } else if (r < 2 * I) {
+              val = pair_entry<true>(pde, cn[t], cdof[t], rnode, rdof);
+            } else {
+              val = proxy_entry_node<true>(pde, cn[t], P.proxy_dir, r - 2 * I, cdof[t], tk.cx,
+                                           tk.cy, tk.rad, tk.pw, tk.pshift);
+            }
+          }
+          double* ycol = cols + static_cast<long long>(lda) * t;
+#pragma unroll
+          for (int b = 0; b < kSketchBlocks; b++) {
+            const double sv = neg[b] ? -val : val;
+            unsigned rest = grp[b];
+            double sum = 0.0;
+            for (int q = 0; q < gmax; q++) {
+              const int src = rest ? __ffs(rest) - 1 : lane;
+              const double o = __shfl_sync(0xffffffffu, sv, src);
+              if (rest) {
+                sum += o;
+                rest &= rest - 1;
+              }
+            }
+            if (valid && (grp[b] & ((1u << lane) - 1u)) == 0) ycol[b * blk + idx[b]] += sum;
           }
         }
       }
@@ -948,12 +953,9 @@ cudaError_t launch_g(const IdParams& p, cudaStream_t s) {
 
 size_t id_sketch_smem_bytes(int sk, int n, int G) {
   const size_t nloc = static_cast<size_t>((n + G - 1) / G);
-  // matrix share, row tile, row hashes, staged node records and dofs of the
-  // columns and of one row tile (+ alignment)
-  return id_smem_bytes(sk, n) +
-         sizeof(double) * (nloc * onchip_lda(sk) + static_cast<size_t>(kSketchTile + 1) * nloc) +
-         sizeof(int) * kSketchTile * kSketchBlocks +
-         (sizeof(Node) + sizeof(int)) * (nloc + kSketchTile) + 16;
+  // matrix share, staged node records and dofs of the columns (+ alignment)
+  return id_smem_bytes(sk, n) + sizeof(double) * nloc * onchip_lda(sk) +
+         (sizeof(Node) + sizeof(int)) * nloc + 16;
 }
 
 size_t id_onchip_smem_bytes(int m, int n, int G) {

@@ -43,7 +43,6 @@ struct IdTask {
 // of sk / kSketchBlocks rows, and every row of A is added with a hashed sign
 // into one hashed row of each block (a sparse sign embedding).
 constexpr int kSketchBlocks = 2;
-constexpr int kSketchTile = 32;  // rows of A generated per pass
 // Sketch rows for an m x n matrix: n + 16 rounded up to the block count.
 inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlocks * kSketchBlocks; }
 
@@ -113,7 +112,7 @@ struct DecTask {
   const int* bpos;       // per active position: row inside that block
   const UpdBlock* blocks;
   const double* T;       // k x r, ld k (from the ID)
-  double* K;             // scratch n x n (boxes too large for shared memory)
+  double* K;             // scratch n x n + kLuSyncInts (boxes too large for shared memory)
   double* L;             // k x r, ld k
   double* U;             // r x k, ld r
   double* X;             // X_rr^{-1}, r x r, ld r (written by the decoupling)
@@ -166,8 +165,16 @@ cudaError_t launch_forest_top_solve(const TopTask* tasks, int ntasks, int n_max,
 
 // ---------------------------------------------------------------- dense LU
 // In-place LU with partial pivoting of an n x n matrix (ld), pivots 0-based
-// row indices as LAPACK's (ipiv[j] = row swapped with j).
-cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s);
+// row indices as LAPACK's (ipiv[j] = row swapped with j).  With `sync`
+// (kLuSyncInts ints of device scratch, used by this call alone until it
+// completes) a matrix of up to kLuFusedMaxN rows is factored by one
+// cooperative launch; otherwise, or when larger, panel by panel (the same
+// bits up to 512 rows).  *status: 1 zero pivot, 2 a bounded wait between the
+// cooperative launch's thread blocks ran out.
+constexpr int kLuFusedMaxN = 768;
+constexpr int kLuSyncInts = kLuFusedMaxN / 32 + 8;
+cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s,
+                     int* sync = nullptr);
 // Multi-CTA tiled C = C0 - op(A) op(B) (64 x 64 tiles); C0 may be null.
 cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, const double* A,
                             int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,

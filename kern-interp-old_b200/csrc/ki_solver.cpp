@@ -6,7 +6,10 @@
 // device work descriptor per box, then one launch runs every box's
 // interpolative decomposition and one launch decouples every compressed box.
 // The ranks and pivots come back to the host (a few KB per level) because
-// the next level's active lists are made of this level's skeletons.  The top
+// the next level's active lists are made of this level's skeletons; the
+// next level's IDs are launched before this level's decoupling is prepared,
+// so that host bookkeeping overlaps GPU work.  With holes, the border
+// columns are swept up each level as soon as it is decoupled.  The top
 // skeleton matrix (or, with holes, the bordered system S of
 // skel_factorization.cpp:130-242) is assembled and LU-factored on the GPU.
 // solve_device() runs the level sweeps of SkelFactorization::solve and
@@ -21,6 +24,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 
 namespace kib {
@@ -102,13 +106,18 @@ void* Arena::alloc(size_t bytes) {
 
 Scratch::~Scratch() {
   if (p) chunk_pool::put(p, bytes, false);
+  for (const auto& r : retired) chunk_pool::put(r.first, r.second, false);
 }
 
-cudaError_t Scratch::reserve(size_t want, cudaStream_t s) {
+cudaError_t Scratch::reserve(size_t want, cudaStream_t s, bool retire) {
   if (want <= bytes) return cudaSuccess;
-  cudaError_t e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return e;
-  if (p) chunk_pool::put(p, bytes, false);
+  if (retire) {
+    if (p) retired.emplace_back(p, bytes);
+  } else {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    if (p) chunk_pool::put(p, bytes, false);
+  }
   p = nullptr;
   bytes = 0;
   size_t got = 0;
@@ -192,7 +201,7 @@ namespace {
 struct AuxSet {
   int dev = -1;
   cudaStream_t d = nullptr;
-  cudaEvent_t ev_id = nullptr, ev_dec = nullptr, fork = nullptr;
+  cudaEvent_t ev_id[2] = {}, ev_dec = nullptr, fork = nullptr;
   cudaStream_t id[3] = {};
   cudaEvent_t join[3] = {};
   cudaStream_t dl[3] = {};
@@ -219,7 +228,8 @@ Solver::~Solver() {
     AuxSet a;
     cudaGetDevice(&a.dev);
     a.d = dstream_;
-    a.ev_id = ev_id_;
+    a.ev_id[0] = ev_id_[0];
+    a.ev_id[1] = ev_id_[1];
     a.ev_dec = ev_dec_;
     a.fork = id_fork_;
     for (int i = 0; i < kIdStreams; i++) {
@@ -376,7 +386,8 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
           const AuxSet a = fl[i];
           fl.erase(fl.begin() + static_cast<long>(i));
           dstream_ = a.d;
-          ev_id_ = a.ev_id;
+          ev_id_[0] = a.ev_id[0];
+          ev_id_[1] = a.ev_id[1];
           ev_dec_ = a.ev_dec;
           id_fork_ = a.fork;
           for (int k = 0; k < kIdStreams; k++) {
@@ -393,7 +404,8 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
     }
     if (!dstream_) {
       KI_CUDA(cudaStreamCreateWithFlags(&dstream_, cudaStreamNonBlocking));
-      KI_CUDA(cudaEventCreateWithFlags(&ev_id_, cudaEventDisableTiming));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_id_[0], cudaEventDisableTiming));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_id_[1], cudaEventDisableTiming));
       KI_CUDA(cudaEventCreateWithFlags(&ev_dec_, cudaEventDisableTiming));
       KI_CUDA(cudaEventCreateWithFlags(&id_fork_, cudaEventDisableTiming));
       for (int i = 0; i < kIdStreams; i++) {
@@ -481,14 +493,39 @@ int Solver::finish_factor(cudaEvent_t ev0) {
     KI_ALLOC(d_Urow_, double, cnt);
     KI_CUDA(launch_border_fill(opt_.pde, d_nodes_, n_points_, d_holes_, nh, d_U_, d_Psi_, d_Urow_,
                                stream_));
+    // the border columns swept up through each level as soon as the level
+    // is decoupled (U and Psi^T dof-major: a dof's nb entries contiguous, the
+    // sweeps gather whole rows; Psi's own column-major nb x N layout is
+    // Psi^T dof-major)
+    KI_ALLOC(d_modU_, double, cnt);
+    KI_ALLOC(d_modP_, double, cnt);
+    KI_CUDA(cudaMemcpyAsync(d_modU_, d_Urow_, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
+                            stream_));
+    KI_CUDA(cudaMemcpyAsync(d_modP_, d_Psi_, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
+                            stream_));
   }
 
   const int L = static_cast<int>(tree.levels.size());
   launch_log.clear();
   t_wait_ms = t_host_prep_ms = t_host_post_ms = t_upload_ms = t_host_top_ms = 0;
   g_upload_ms = 0;
-  for (int level = L - 1; level > 0; level--) {
-    const int rc = process_level(level);
+  // dstream_ (decoupling, border sweeps) after everything queued so far on
+  // stream_: adopted factors, border columns
+  KI_CUDA(cudaEventRecord(ev_id_[0], stream_));
+  KI_CUDA(cudaStreamWaitEvent(dstream_, ev_id_[0], 0));
+  if (L > 1) {
+    // level l's IDs, then per level: the IDs of l - 1 launched, l's
+    // decoupling prepared and launched while they run, l - 1's ranks read
+    auto cur = std::make_unique<PendingLevel>();
+    int rc = id_launch(L - 1, cur.get());
+    if (!rc) rc = id_finish(cur.get());
+    for (int level = L - 1; level > 0 && !rc; level--) {
+      auto next = std::make_unique<PendingLevel>();
+      if (level > 1) rc = id_launch(level - 1, next.get());
+      if (!rc) rc = decouple_level(cur.get());
+      if (!rc && level > 1) rc = id_finish(next.get());
+      cur = std::move(next);
+    }
     if (rc) return rc;
   }
   for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
@@ -521,12 +558,18 @@ int Solver::finish_factor(cudaEvent_t ev0) {
   cudaEventDestroy(ev1);
   if (trc) return -2;
   t_upload_ms = g_upload_ms;
+  if (status == 2) return fail("an LU factorization stopped: a bounded wait timed out");
   if (status) return fail("zero pivot in an LU factorization (singular block)");
   return 0;
 }
 
-int Solver::compress_level(int level, std::vector<int>* fresh) {
+int Solver::id_launch(int level, PendingLevel* pl) {
   const double h0 = now_ms();
+  pl->level = level;
+  // boxes compressed before this factorization (kept by an update or a
+  // copy) are skipped by the IDs and join the level's sweeps as they are
+  for (int id : tree.levels[level])
+    if (tree.boxes[id].compressed) pl->boxes.push_back(id);
   const std::vector<int>& ids = tree.levels[level];
   const int nids = static_cast<int>(ids.size());
   // active lists of the level (quadtree.cpp:694-720), independent per box
@@ -536,10 +579,7 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   });
   const int P = sd_ == 2 ? 4 * kNumProxy : 2 * kNumProxy;
 
-  struct Cand {
-    int box = -1, n = 0, m = 0, I = 0, g = 0, sk = 0;
-    std::vector<int> rows;
-  };
+  using Cand = IdCand;
   std::vector<Cand> all(nids);
   std::vector<char> keep(nids, 0);
   parallel_for(nids, 8, [&](int a, int e) {
@@ -603,16 +643,17 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
       keep[q] = 1;
     }
   });
-  std::vector<Cand> cand;
+  std::vector<Cand>& cand = pl->cand;
   for (int q = 0; q < nids; q++)
     if (keep[q]) cand.push_back(std::move(all[q]));
   if (cand.empty()) return 0;
   std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.g < b.g; });
 
   const int nc = static_cast<int>(cand.size());
-  std::vector<IdTask> tasks(nc);
+  std::vector<IdTask>& tasks = pl->tasks;
+  tasks.assign(nc, IdTask{});
   long long a_total = 0, t_total = 0;
-  int perm_total = 0;
+  int& perm_total = pl->perm_total;
   size_t act_total = 0, rows_total = 0;
   for (int q = 0; q < nc; q++) {  // offsets
     const Cand& c = cand[q];
@@ -731,10 +772,34 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
       KI_CUDA(cudaEventRecord(id_join_[i], id_streams_[i]));
       KI_CUDA(cudaStreamWaitEvent(stream_, id_join_[i], 0));
     }
-  std::vector<int> rank(nc), perm(perm_total);
-  KI_CUDA(cudaMemcpyAsync(rank.data(), d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
-  KI_CUDA(cudaMemcpyAsync(perm.data(), d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,
+  // the level's decoupling (on dstream_) waits for its IDs and nothing
+  // later (the next level's IDs are queued on stream_ before it)
+  KI_CUDA(cudaEventRecord(ev_id_[level & 1], stream_));
+  pl->ids_queued = true;
+  // ranks and pivots into pinned memory: the copies queue behind the IDs
+  // without blocking the host (a copy to pageable memory would wait for them)
+  pl->rank = static_cast<int*>(stage_.alloc(sizeof(int) * nc));
+  pl->perm = static_cast<int*>(stage_.alloc(sizeof(int) * (perm_total + 1)));
+  if (!pl->rank || !pl->perm) return fail("pinned staging allocation failed");
+  KI_CUDA(cudaMemcpyAsync(pl->rank, d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
+  KI_CUDA(cudaMemcpyAsync(pl->perm, d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,
                           stream_));
+  pl->d_act = d_act;
+  pl->d_perm = d_perm;
+  pl->d_T = d_T;
+  return 0;
+}
+
+int Solver::id_finish(PendingLevel* pl) {
+  const int level = pl->level;
+  const int nc = static_cast<int>(pl->cand.size());
+  if (nc == 0) return 0;
+  using Cand = IdCand;
+  const std::vector<Cand>& cand = pl->cand;
+  const std::vector<IdTask>& tasks = pl->tasks;
+  const int* rank = pl->rank;
+  const int* perm = pl->perm;
+  double* d_T = pl->d_T;
   {
     const auto w0 = std::chrono::steady_clock::now();
     KI_CUDA(cudaStreamSynchronize(stream_));
@@ -745,7 +810,7 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   // skeleton / redundant sets (InteractionLists::set_rs_ranges, quadtree.h:23-35)
   const double h1 = now_ms();
   mark(2, level);
-  std::vector<int> comp;  // candidate indices that compressed
+  std::vector<int>& comp = pl->comp;  // candidate indices that compressed
   {
     // per candidate, independent: work counts, skeleton / redundant lists
     std::vector<double> qr_v(nc), bytes_v(nc);
@@ -776,7 +841,7 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
         Box& b = tree.boxes[c.box];
         b.compressed = true;
         b.rank = k;
-        b.perm.assign(perm.begin() + t.perm_off, perm.begin() + t.perm_off + c.n);
+        b.perm.assign(perm + t.perm_off, perm + t.perm_off + c.n);
         b.skel.resize(k);
         b.redundant.resize(c.n - k);
         for (int i = 0; i < k; i++) b.skel[i] = b.active[b.perm[i]];
@@ -791,9 +856,39 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
       if (rank[q] > 0) comp.push_back(q);
     }
   }
-  if (comp.empty()) return 0;
+  t_host_post_ms += now_ms() - h1;
+  return 0;
+}
 
+int Solver::decouple_level(PendingLevel* pl) {
+  if (pl->ids_queued) KI_CUDA(cudaStreamWaitEvent(dstream_, ev_id_[pl->level & 1], 0));
+  if (!pl->comp.empty()) {
+    const int rc = decouple_boxes(pl);
+    if (rc) return rc;
+  }
+  const int rc = level_sweeps(pl->level, pl->boxes, dstream_);
+  if (rc) return rc;
+  const LevelFactors& lf = levels_[pl->level];
+  if (nb_ > 0 && lf.ntasks) {
+    // skel_factorization.cpp:146-160 for this level: U and Psi^T swept up
+    SweepParams sp{lf.d_tasks, lf.ntasks, d_modU_, 1, nb_, 0, nullptr, lf.cap, nb_};
+    SweepParams spp = sp;
+    spp.x = d_modP_;
+    KI_CUDA(launch_sweep_up_pair(sp, spp, dstream_));
+  }
+  return 0;
+}
+
+int Solver::decouple_boxes(PendingLevel* pl) {
   // ---- decouple every compressed box of the level
+  const double h1 = now_ms();
+  const int level = pl->level;
+  using Cand = IdCand;
+  const std::vector<Cand>& cand = pl->cand;
+  const std::vector<IdTask>& tasks = pl->tasks;
+  const std::vector<int>& comp = pl->comp;
+  int* d_act = pl->d_act;
+  int* d_perm = pl->d_perm;
   const int ncomp = static_cast<int>(comp.size());
   std::vector<DecTask> dt(ncomp);
   // block maps (per position of the box's dof list: which descendant
@@ -825,7 +920,8 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
     tab_off[t + 1] = tab_off[t] + static_cast<long long>(blk[t].size());
     k_off[t] = scratch_total;
     if (n > kDecoupleSmemN) {
-      scratch_total += static_cast<long long>(n) * n;
+      // n x n, then the LU's flags (kLuSyncInts ints)
+      scratch_total += static_cast<long long>(n) * n + kLuSyncInts;
     } else {
       n_max = std::max(n_max, n);
     }
@@ -859,7 +955,9 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   KI_ALLOC(d_fac, double, fac_total);
   KI_ALLOC(d_piv, int, piv_total);
   KI_ALLOC(d_dt, DecTask, ncomp);
-  KI_CUDA(scratch2_.reserve(sizeof(double) * (scratch_total + 1), dstream_));
+  // (earlier levels' decouplings may still be queued on dstream_ with the
+  // old buffer: it is retired, not waited for)
+  KI_CUDA(scratch2_.reserve(sizeof(double) * (scratch_total + 1), dstream_, true));
   double* scr = static_cast<double*>(scratch2_.p);
   size_t fo = 0, po = 0;
   for (int t = 0; t < ncomp; t++) {
@@ -897,8 +995,6 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
   // small boxes first in one batched launch, then each large box
   std::vector<DecTask> small, large;
   for (const DecTask& d : dt) (d.n > kDecoupleSmemN ? large : small).push_back(d);
-  KI_CUDA(cudaEventRecord(ev_id_, stream_));
-  KI_CUDA(cudaStreamWaitEvent(dstream_, ev_id_, 0));
   KI_UPLOAD(d_bid, bid, dstream_);
   KI_UPLOAD(d_bpos, bpos, dstream_);
   KI_UPLOAD(d_tab, tab, dstream_);
@@ -940,19 +1036,8 @@ int Solver::compress_level(int level, std::vector<int>* fresh) {
                 dstream_))
     return -2;
 
-  for (int t = 0; t < ncomp; t++) fresh->push_back(cand[comp[t]].box);
+  for (int t = 0; t < ncomp; t++) pl->boxes.push_back(cand[comp[t]].box);
   return 0;
-}
-
-int Solver::process_level(int level) {
-  // boxes compressed before this factorization (kept by an update or a
-  // copy) are skipped by the IDs and join the level's sweeps as they are
-  std::vector<int> boxes;
-  for (int id : tree.levels[level])
-    if (tree.boxes[id].compressed) boxes.push_back(id);
-  const int rc = compress_level(level, &boxes);
-  if (rc) return rc;
-  return level_sweeps(level, boxes, dstream_);
 }
 
 int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s) {
@@ -1012,6 +1097,7 @@ void Solver::drop_device_state() {
   d_top_piv_ = nullptr;
   d_allskel_ = d_allred_ = d_red_pos_ = nullptr;
   d_U_ = d_Psi_ = d_Urow_ = d_Ured_ = d_Pred_ = d_tmp_ = nullptr;
+  d_modU_ = d_modP_ = nullptr;
   all_compressed_ = LevelFactors{};
   levels_.clear();
 }
@@ -1269,7 +1355,9 @@ int Solver::factor_top() {
   }
   cudaEvent_t l0 = nullptr;
   if (time_phases && timer_begin(&l0)) return -2;
-  if (ntop > 0) KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_));
+  int* lu_sync;
+  KI_ALLOC(lu_sync, int, kLuSyncInts);
+  if (ntop > 0) KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_, lu_sync));
   if (time_phases && timer_end(l0, {0, 4, 1, 1, 0, ntop, 0.0})) return -2;
   return 0;
 }
@@ -1298,27 +1386,11 @@ int Solver::factor_border() {
   KI_UPLOAD(d_allred_, allred, stream_);
   KI_UPLOAD(d_red_pos_, red_pos, stream_);
 
-  double *modU, *modP;
-  KI_ALLOC(modU, double, static_cast<size_t>(N) * nb);
-  KI_ALLOC(modP, double, static_cast<size_t>(N) * nb);
-  // U and Psi^T dof-major (a dof's nb entries contiguous: the sweeps gather
-  // whole rows); Psi's own column-major nb x N layout is Psi^T dof-major
-  KI_CUDA(cudaMemcpyAsync(modU, d_Urow_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
-                          stream_));
-  KI_CUDA(cudaMemcpyAsync(modP, d_Psi_, sizeof(double) * N * nb, cudaMemcpyDeviceToDevice,
-                          stream_));
-  const int L = static_cast<int>(levels_.size());
+  // U and Psi^T were swept up level by level with the decoupling
+  double* modU = d_modU_;
+  double* modP = d_modP_;
   cudaEvent_t b0 = nullptr;
   if (time_phases && timer_begin(&b0)) return -2;
-  for (int l = L - 1; l >= 0; l--) {
-    const LevelFactors& lf = levels_[l];
-    if (!lf.ntasks) continue;
-    SweepParams sp{lf.d_tasks, lf.ntasks, modU, 1, nb, 0, nullptr, lf.cap, nb};
-    SweepParams spp = sp;
-    spp.x = modP;
-    KI_CUDA(launch_sweep_up_pair(sp, spp, stream_));
-  }
-  if (time_phases && timer_end(b0, {0, 3, 1, nb, 0, N, 0.0})) return -2;
   double *dinv, *us, *ps, *corr;
   KI_ALLOC(d_Ured_, double, static_cast<size_t>(nr) * nb);
   KI_ALLOC(d_Pred_, double, static_cast<size_t>(nr) * nb);
@@ -1336,6 +1408,7 @@ int Solver::factor_border() {
   KI_CUDA(launch_diag_solve(dp, stream_));
   KI_CUDA(small_gemm(true, false, nb, nb, nr, 1.0, d_Pred_, nr, dinv, nr, 0.0, corr, nb, stream_));
   KI_CUDA(launch_fill_border(d_top_, ns + nb, ns, nb, us, ps, corr, stream_));
+  if (time_phases && timer_end(b0, {0, 3, 1, nb, 0, N, 0.0})) return -2;
   return 0;
 }
 

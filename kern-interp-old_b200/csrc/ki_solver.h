@@ -61,8 +61,13 @@ class Arena {
 struct Scratch {
   void* p = nullptr;
   size_t bytes = 0;
+  // buffers outgrown without waiting for the stream (returned to the pool
+  // when the scratch is destroyed, after its owner synchronized)
+  std::vector<std::pair<void*, size_t>> retired;
   ~Scratch();
-  cudaError_t reserve(size_t want, cudaStream_t s);
+  // Grows to at least `want` bytes; the old buffer is released after `s`
+  // has drained (a synchronization), or, with retire, kept until the end.
+  cudaError_t reserve(size_t want, cudaStream_t s, bool retire = false);
 };
 
 struct SolverOptions {
@@ -233,8 +238,30 @@ class Solver {
   int timers_resolve();
   int fail(const std::string& msg);
   int cuda_check(cudaError_t e, const char* what);
-  int process_level(int level);
-  int compress_level(int level, std::vector<int>* fresh);
+  // One level's IDs between their launch and its decoupling: the next
+  // level's IDs are launched before this level's decouple bookkeeping.
+  struct IdCand {
+    int box = -1, n = 0, m = 0, I = 0, g = 0, sk = 0;
+    std::vector<int> rows;
+  };
+  struct PendingLevel {
+    int level = 0;
+    std::vector<int> boxes;  // compressed boxes of the level (earlier ones first)
+    std::vector<IdCand> cand;
+    std::vector<IdTask> tasks;
+    std::vector<int> comp;  // candidates that compressed
+    int* rank = nullptr;  // pinned device-to-host targets
+    int* perm = nullptr;
+    int* d_act = nullptr;
+    int* d_perm = nullptr;
+    double* d_T = nullptr;
+    int perm_total = 0;
+    bool ids_queued = false;  // ev_id_[level & 1] marks the end of its IDs
+  };
+  int id_launch(int level, PendingLevel* pl);
+  int id_finish(PendingLevel* pl);
+  int decouple_level(PendingLevel* pl);
+  int decouple_boxes(PendingLevel* pl);
   int level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s);
   int begin_factor(cudaEvent_t* ev0);
   int finish_factor(cudaEvent_t ev0);
@@ -257,7 +284,7 @@ class Solver {
   // Decoupling of level l runs on dstream_ while the host prepares, and the
   // GPU runs, the interpolative decompositions of level l - 1.
   cudaStream_t dstream_ = nullptr;
-  cudaEvent_t ev_id_ = nullptr, ev_dec_ = nullptr;
+  cudaEvent_t ev_id_[2] = {}, ev_dec_ = nullptr;  // ev_id_: per level parity
   // A level's ID launches of different cluster sizes are independent: the
   // second and later ones run on these streams, concurrently with the first.
   static constexpr int kIdStreams = 3;
@@ -308,6 +335,8 @@ class Solver {
   double* d_U_ = nullptr;     // N x nb
   double* d_Psi_ = nullptr;   // nb x N
   double* d_Urow_ = nullptr;  // U dof-major (N x nb, row i contiguous)
+  double* d_modU_ = nullptr;  // U and Psi^T dof-major, swept up level by level
+  double* d_modP_ = nullptr;
   double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
   double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
   double* d_tmp_ = nullptr;   // solve scratch
