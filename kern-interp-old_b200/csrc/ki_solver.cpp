@@ -246,14 +246,39 @@ Solver::~Solver() {
   }
 }
 
+namespace {
+// Timing events, reused across timed factorizations (creating two events per
+// launch cost more host time than the launches of a small level).
+std::mutex g_ev_mu;
+std::vector<cudaEvent_t>& ev_free() {
+  static std::vector<cudaEvent_t> v;
+  return v;
+}
+cudaError_t ev_get(cudaEvent_t* e) {
+  {
+    std::lock_guard<std::mutex> lk(g_ev_mu);
+    if (!ev_free().empty()) {
+      *e = ev_free().back();
+      ev_free().pop_back();
+      return cudaSuccess;
+    }
+  }
+  return cudaEventCreate(e);
+}
+void ev_put(cudaEvent_t e) {
+  std::lock_guard<std::mutex> lk(g_ev_mu);
+  ev_free().push_back(e);
+}
+}  // namespace
+
 int Solver::timer_begin(cudaEvent_t* e0, cudaStream_t s) {
-  if (cuda_check(cudaEventCreate(e0), "cudaEventCreate")) return -2;
+  if (cuda_check(ev_get(e0), "cudaEventCreate")) return -2;
   return cuda_check(cudaEventRecord(*e0, s ? s : stream_), "cudaEventRecord");
 }
 
 int Solver::timer_end(cudaEvent_t e0, const LaunchRecord& rec, cudaStream_t s) {
   cudaEvent_t e1;
-  if (cuda_check(cudaEventCreate(&e1), "cudaEventCreate")) return -2;
+  if (cuda_check(ev_get(&e1), "cudaEventCreate")) return -2;
   if (cuda_check(cudaEventRecord(e1, s ? s : stream_), "cudaEventRecord")) return -2;
   pending_.push_back({e0, e1, rec});
   return 0;
@@ -284,8 +309,8 @@ int Solver::timers_resolve() {
       t_top_ms += ms;
     }
     launch_log.push_back(r);
-    cudaEventDestroy(p.e0);
-    cudaEventDestroy(p.e1);
+    ev_put(p.e0);
+    ev_put(p.e1);
   }
   pending_.clear();
   return 0;
@@ -365,7 +390,7 @@ void Solver::perturb_tree_only(int n_points, const double* points) {
 }
 
 int Solver::begin_factor(cudaEvent_t* ev0) {
-  KI_CUDA(cudaEventCreate(ev0));
+  KI_CUDA(ev_get(ev0));
   KI_CUDA(cudaEventRecord(*ev0, stream_));
   host_start_ = now_ms();
   ev_start_ = *ev0;
@@ -456,7 +481,7 @@ int Solver::factor() {
 
 int Solver::finish_factor(cudaEvent_t ev0) {
   cudaEvent_t ev1;
-  KI_CUDA(cudaEventCreate(&ev1));
+  KI_CUDA(ev_get(&ev1));
   levels_.assign(tree.levels.size(), LevelFactors{});
   mark(0, 0);
 
@@ -554,8 +579,8 @@ int Solver::finish_factor(cudaEvent_t ev0) {
   t_factor_ms = ms;
   const int trc = timers_resolve();
   ev_start_ = nullptr;
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
+  ev_put(ev0);
+  ev_put(ev1);
   if (trc) return -2;
   t_upload_ms = g_upload_ms;
   if (status == 2) return fail("an LU factorization stopped: a bounded wait timed out");
