@@ -791,6 +791,22 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Warp argmax of non-negative doubles (first index on ties) with three
+// integer reductions instead of shuffle rounds: a non-negative double's bit
+// pattern orders like the value, so the maximum is found on its high word,
+// then its low word, then the smallest index holding it.  A lane with no
+// candidate passes key 0 and index INT_MAX.
+__device__ __forceinline__ void warp_argmax_bits(unsigned long long key, int idx,
+                                                 unsigned long long* kmax, int* imin) {
+  const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  *imin = static_cast<int>(__reduce_min_sync(0xffffffffu, top ? static_cast<unsigned>(idx)
+                                                              : 0x7fffffffu));
+  *kmax = (static_cast<unsigned long long>(mhi) << 32) | mlo;
+}
+
 // Thread 0 waits (bounded) for flag k; false for every thread on an abort.
 __device__ bool fused_wait(int* sync, int k, int G, int* status, int* s_ok) {
   if (threadIdx.x == 0) {
@@ -834,7 +850,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync) {
   extern __shared__ double blk[];  // np x kNb, column-major
   __shared__ double l11[kNb][kNb + 1];
-  __shared__ double red[kFusedThreads / 32];
+  __shared__ unsigned long long redk[kFusedThreads / 32];
   __shared__ int redi[kFusedThreads / 32];
   __shared__ int pv[kNb];
   __shared__ int s_ok;
@@ -901,40 +917,34 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // this CTA's panel: rows c0.., thread t owning rows t + 512 q
   for (int jj = 0; jj < wb; jj++) {
     const int col = c0 + jj;
-    double bv = -1.0;
-    int bp = 0x7fffffff;
+    // candidates: |a_ij| for rows i >= col (a NaN is no candidate); the
+    // largest, the first such row on ties
+    unsigned long long key = 0;
+    int idx = 0x7fffffff;
     for (int i = tid; i < n; i += kFusedThreads) {
       if (i < col) continue;
       const double v = fabs(blk[i + np * jj]);
-      if (v > bv) {
-        bv = v;
-        bp = i;
+      if (v == v) {
+        const unsigned long long kv = static_cast<unsigned long long>(__double_as_longlong(v));
+        if (idx == 0x7fffffff || kv > key) {
+          key = kv;
+          idx = i;
+        }
       }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
-      if (ov > bv || (ov == bv && op < bp)) {
-        bv = ov;
-        bp = op;
-      }
-    }
+    unsigned long long wk2;
+    int wi;
+    warp_argmax_bits(key, idx, &wk2, &wi);
     if (lane == 0) {
-      red[warp] = bv;
-      redi[warp] = bp;
+      redk[warp] = wk2;
+      redi[warp] = wi;
     }
     __syncthreads();
-    double v = lane < kFusedThreads / 32 ? red[lane] : -1.0;
-    int p = lane < kFusedThreads / 32 ? redi[lane] : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-      const int op = __shfl_xor_sync(0xffffffffu, p, o);
-      if (ov > v || (ov == v && op < p)) {
-        v = ov;
-        p = op;
-      }
+    int p;
+    {
+      unsigned long long k2;
+      warp_argmax_bits(lane < kFusedThreads / 32 ? redk[lane] : 0ull,
+                       lane < kFusedThreads / 32 ? redi[lane] : 0x7fffffff, &k2, &p);
     }
     // no comparable entry (NaN column): keep the row, flag the factorization
     const bool bad = p < col || p >= n;
@@ -953,9 +963,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
     for (int i = tid; i < n; i += kFusedThreads) {
       if (i <= col) continue;
-      const double li = blk[i + np * jj] * inv;
-      for (int c = jj + 1; c < wb; c++) blk[i + np * c] -= li * blk[col + np * c];
-      blk[i + np * jj] = li;
+      // the pivot row and this row never alias (i > col): loads may run ahead
+      const double* __restrict__ prow = blk + col;
+      double* __restrict__ row = blk + i;
+      const double li = row[np * jj] * inv;
+#pragma unroll 4
+      for (int c = jj + 1; c < wb; c++) row[np * c] -= li * prow[np * c];
+      row[np * jj] = li;
     }
     // the next column's barrier orders these updates before its
     // interchange; the pivot row is not updated
