@@ -311,7 +311,10 @@ constexpr int kMaxKrylov = 64;  // vectors per multi-dot
 struct MvTile {
   int t0, t1, s0, s1, split, rank1_slot, first, pad;
 };
-int matvec_splits(int n_nodes, int num_sms);
+// Source splits for nseg segments of about n_nodes nodes each: the count
+// whose tiles fill whole waves of the resident CTAs best (a last, partly
+// filled wave costs as much time as a full one).
+int matvec_splits(int pde, int n_nodes, int nseg, int num_sms);
 // seg: node offsets of the segments (size nseg + 1); one segment = one
 // problem, so a forest's operator is block diagonal.
 void matvec_tiles(const std::vector<int>& seg, int splits, std::vector<MvTile>* tiles);

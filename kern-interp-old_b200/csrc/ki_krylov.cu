@@ -276,11 +276,31 @@ __global__ void segment_sumsq_kernel(const double* __restrict__ v, const int* __
 
 }  // namespace
 
-int matvec_splits(int n_nodes, int num_sms) {
-  const int tblocks = (n_nodes + kMvThreads - 1) / kMvThreads;
-  const int want = (4 * num_sms + tblocks - 1) / tblocks;  // about 4 CTAs per SM
-  const int max_split = (n_nodes + kMvThreads - 1) / kMvThreads;  // >= 256 sources each
-  return std::max(1, std::min(want, std::min(max_split, kMaxMatvecSplits)));
+int matvec_splits(int pde, int n_nodes, int nseg, int num_sms) {
+  // resident CTAs of the product kernel on the whole GPU
+  int per_sm = 0;
+  const void* fn = pde == kLaplace ? reinterpret_cast<const void*>(&mv_partial_kernel<kLaplace>)
+                   : pde == kLaplaceNeumann
+                       ? reinterpret_cast<const void*>(&mv_partial_kernel<kLaplaceNeumann>)
+                       : reinterpret_cast<const void*>(&mv_partial_kernel<kStokes>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kMvThreads, 0) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const long long slots = static_cast<long long>(per_sm) * std::max(1, num_sms);
+  const int per_seg = (n_nodes + kMvThreads - 1) / kMvThreads;  // target tiles
+  const long long tblocks = static_cast<long long>(per_seg) * std::max(1, nseg);
+  const int max_split = std::max(1, std::min(per_seg, kMaxMatvecSplits));  // >= 256 sources each
+  // time ~ waves x (sources per split): minimise ceil(tblocks S / slots) / S
+  int best = 1;
+  double best_t = 1e300;
+  for (int S = 1; S <= max_split; S++) {
+    const double t = static_cast<double>((tblocks * S + slots - 1) / slots) / S;
+    if (t < best_t * (1.0 - 1e-9)) {
+      best_t = t;
+      best = S;
+    }
+  }
+  return best;
 }
 
 void matvec_tiles(const std::vector<int>& seg, int splits, std::vector<MvTile>* tiles) {

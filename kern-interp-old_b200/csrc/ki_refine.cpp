@@ -34,10 +34,8 @@ int Solver::mv_setup() {
   }
   seg_ = starts_.size() > 1 ? starts_ : std::vector<int>{0, n_points_};
   const int nseg = static_cast<int>(seg_.size()) - 1;
-  // splits sized for the average problem: about 4 CTAs per SM over the job
-  mv_splits_ = matvec_splits(std::max(1, n_points_ / nseg), num_sms_);
-  mv_splits_ = std::max(1, std::min(mv_splits_, (4 * num_sms_ * 256 + n_points_ - 1) /
-                                                   std::max(1, n_points_)));
+  // splits sized for the average problem, filling whole waves of the GPU
+  mv_splits_ = matvec_splits(opt_.pde, std::max(1, n_points_ / nseg), nseg, num_sms_);
   std::vector<MvTile> tiles;
   matvec_tiles(seg_, mv_splits_, &tiles);
   n_mv_tiles_ = static_cast<int>(tiles.size());
