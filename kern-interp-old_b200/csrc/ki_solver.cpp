@@ -672,7 +672,12 @@ int Solver::id_launch(int level, PendingLevel* pl) {
   for (int q = 0; q < nids; q++)
     if (keep[q]) cand.push_back(std::move(all[q]));
   if (cand.empty()) return 0;
-  std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.g < b.g; });
+  // by cluster size, then the largest ID matrices first: CTAs start in
+  // index order, so the long tasks do not end up in a launch's last wave
+  std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) {
+    if (a.g != b.g) return a.g < b.g;
+    return static_cast<long long>(a.m) * a.n > static_cast<long long>(b.m) * b.n;
+  });
 
   const int nc = static_cast<int>(cand.size());
   std::vector<IdTask>& tasks = pl->tasks;
@@ -1020,6 +1025,9 @@ int Solver::decouple_boxes(PendingLevel* pl) {
   // small boxes first in one batched launch, then each large box
   std::vector<DecTask> small, large;
   for (const DecTask& d : dt) (d.n > kDecoupleSmemN ? large : small).push_back(d);
+  // the largest boxes first (CTAs start in index order: no long last wave)
+  std::stable_sort(small.begin(), small.end(),
+                   [](const DecTask& a, const DecTask& b) { return a.n > b.n; });
   KI_UPLOAD(d_bid, bid, dstream_);
   KI_UPLOAD(d_bpos, bpos, dstream_);
   KI_UPLOAD(d_tab, tab, dstream_);
