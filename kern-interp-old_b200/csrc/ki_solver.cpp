@@ -634,14 +634,26 @@ int Solver::id_launch(int level, PendingLevel* pl) {
         // their original dofs, others their active ones, quadtree.cpp:
         // 664-691) that lie inside the proxy circle (kernel.cpp:209-218)
         const double cx = b.corner[0] + b.side / 2.0, cy = b.corner[1] + b.side / 2.0;
+        const double R = kRadiusRatio * b.side;
+        // squared distances decide all but a thin band around the circle,
+        // where the reference's own expression decides
+        const double lo2 = R * R * (1.0 - 1e-9), hi2 = R * R * (1.0 + 1e-9);
         for (int o : b.nbr) {
           const Box& ob = tree.boxes[o];
           if (ob.level > b.level) continue;
+          int last_pt = -1;
+          bool last_in = false;
           for (int dof : ob.leaf ? ob.original : ob.active) {
             const int pt = dof / sd_;
-            const double x = pts_[2 * pt], y = pts_[2 * pt + 1];
-            const double dist = std::sqrt(std::pow(cx - x, 2) + std::pow(cy - y, 2));
-            if (dist < kRadiusRatio * b.side) c.rows.push_back(dof);
+            if (pt != last_pt) {  // a Stokes node's two dofs are adjacent
+              const double dx = cx - pts_[2 * pt], dy = cy - pts_[2 * pt + 1];
+              const double d2 = dx * dx + dy * dy;
+              last_in = d2 < lo2 ? true
+                        : d2 > hi2 ? false
+                                   : std::sqrt(std::pow(dx, 2) + std::pow(dy, 2)) < R;
+              last_pt = pt;
+            }
+            if (last_in) c.rows.push_back(dof);
           }
         }
         c.I = static_cast<int>(c.rows.size());
