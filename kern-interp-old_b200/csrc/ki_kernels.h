@@ -42,7 +42,7 @@ struct IdTask {
 // Row sketch of an ID matrix (on-chip, one CTA): S has kSketchBlocks blocks
 // of sk / kSketchBlocks rows, and every row of A is added with a hashed sign
 // into one hashed row of each block (a sparse sign embedding).
-constexpr int kSketchBlocks = 2;
+constexpr int kSketchBlocks = 1;
 // Sketch rows for an m x n matrix: n + 16 rounded up to the block count.
 inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlocks * kSketchBlocks; }
 
