@@ -393,6 +393,7 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
   KI_CUDA(ev_get(ev0));
   KI_CUDA(cudaEventRecord(*ev0, stream_));
   host_start_ = now_ms();
+  geom_ready_ = false;
   ev_start_ = *ev0;
   host_marks.clear();
   t_id_ms = t_decouple_ms = t_top_ms = 0;
@@ -465,34 +466,23 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
   return 0;
 }
 
-int Solver::factor() {
-  cudaEvent_t ev0;
-  const int rc = begin_factor(&ev0);
-  if (rc) return rc;
-  if (starts_.size() > 1) {
-    if (!holes_.empty()) return fail("a forest of problems cannot have holes");
-    tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
-  } else {
-    tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
-  }
-  boxdev_.assign(tree.boxes.size(), BoxDev{});
-  return finish_factor(ev0);
-}
-
-int Solver::finish_factor(cudaEvent_t ev0) {
-  cudaEvent_t ev1;
-  KI_CUDA(ev_get(&ev1));
-  levels_.assign(tree.levels.size(), LevelFactors{});
-  mark(0, 0);
-
+// Device geometry, proxy directions, holes, status flag and the border
+// columns: none depends on the quadtree, so factor() queues them before
+// building it (the copies and the border kernels run during the build).
+int Solver::setup_geometry() {
   // geometry, proxy directions, holes, status flag
   {
-    std::vector<Node> nodes(n_points_);
-    for (int i = 0; i < n_points_; i++)
-      nodes[i] = Node{pts_[2 * i], pts_[2 * i + 1], nrm_[2 * i], nrm_[2 * i + 1], wts_[i],
-                      curv_[i], 0.0, 0.0};
+    // node records formed straight into pinned staging, in parallel
+    Node* st = static_cast<Node*>(stage_.alloc(sizeof(Node) * n_points_));
+    if (!st) return fail("pinned staging allocation failed");
+    parallel_for(n_points_, 4096, [&](int a, int e) {
+      for (int i = a; i < e; i++)
+        st[i] = Node{pts_[2 * i], pts_[2 * i + 1], nrm_[2 * i], nrm_[2 * i + 1], wts_[i],
+                     curv_[i], 0.0, 0.0};
+    });
     KI_ALLOC(d_nodes_, Node, n_points_);
-    KI_UPLOAD(d_nodes_, nodes, stream_);
+    KI_CUDA(cudaMemcpyAsync(d_nodes_, st, sizeof(Node) * n_points_, cudaMemcpyHostToDevice,
+                            stream_));
     std::vector<double> dir(2 * kNumProxy);
     for (int i = 0; i < kNumProxy; i++) {
       const double ang = 2 * M_PI * i * (1.0 / kNumProxy);
@@ -528,6 +518,37 @@ int Solver::finish_factor(cudaEvent_t ev0) {
                             stream_));
     KI_CUDA(cudaMemcpyAsync(d_modP_, d_Psi_, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
                             stream_));
+  }
+
+  geom_ready_ = true;
+  return 0;
+}
+
+int Solver::factor() {
+  cudaEvent_t ev0;
+  const int rc = begin_factor(&ev0);
+  if (rc) return rc;
+  if (starts_.size() > 1 && !holes_.empty()) return fail("a forest of problems cannot have holes");
+  const int grc = setup_geometry();
+  if (grc) return grc;
+  if (starts_.size() > 1) {
+    tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
+  } else {
+    tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
+  }
+  boxdev_.assign(tree.boxes.size(), BoxDev{});
+  return finish_factor(ev0);
+}
+
+int Solver::finish_factor(cudaEvent_t ev0) {
+  cudaEvent_t ev1;
+  KI_CUDA(ev_get(&ev1));
+  levels_.assign(tree.levels.size(), LevelFactors{});
+  mark(0, 0);
+
+  if (!geom_ready_) {
+    const int rc = setup_geometry();
+    if (rc) return rc;
   }
 
   const int L = static_cast<int>(tree.levels.size());

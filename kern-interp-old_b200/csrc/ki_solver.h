@@ -264,6 +264,8 @@ class Solver {
   int decouple_boxes(PendingLevel* pl);
   int level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s);
   int begin_factor(cudaEvent_t* ev0);
+  int setup_geometry();
+  bool geom_ready_ = false;  // setup_geometry done for this factorization
   int finish_factor(cudaEvent_t ev0);
   // Copies the factors of `boxes` (T, L, U, X^-1, update, pivots) from
   // `src` into this solver's arena, one batched copy on stream_.
