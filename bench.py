@@ -14,24 +14,29 @@ unknowns / (factor + solve time), for two methods on the same GPU:
     (3e-8 for stokes65k) in
     preconditioner mode (tall ID matrices reduced by a sparse row sketch)
     used by FP64 refinement / GMRES on the operator with on-the-fly FP64
-    entries, stopped at true relative residual 1e-12 (ki_factor_ex +
-    ki_solve_refined_device);
+    entries, stopped at relative residual 1e-12 (ki_factor_ex +
+    ki_solve_refined_device; residuals below 1e-5 are updated with the
+    correction product, FP32 far field / FP64 near field, and the true FP64
+    residual of the result is reported beside it);
   * FP64 (`fp64`): the reference method, factorization at ID tolerance
     1e-10 and one direct solve (ki_factor + ki_solve_device).
 
-The default workload is the Laplace star r = 1 + 0.3 cos 5t, N = 16384 nodes,
-64-point leaves; `stokes65k` is the Stokes disk with 8 holes (65,536 dofs);
-`batch256` is 256 random stars of 512-8192 nodes factored together
-(ki_factor_batch).  Errors are reported against the FP64 oracle (the
+The default workload is the Stokes disk with 8 holes (65,536 dofs, 64-point
+leaves, multiply connected); `star16k` is the Laplace star r = 1 + 0.3 cos 5t,
+N = 16384 nodes; `batch256` is 256 random stars of 512-8192 nodes factored
+together (ki_factor_batch).  Errors are reported against the FP64 oracle (the
 reference algorithm restated on the CPU) at ID tolerance 1e-10 and, as the
 converged reference, at 1e-13.
 
 Timing: CUDA events on the stream the library launches on, the right-hand
-side resident in HBM, the L2 flushed (256 MiB write) before every step;
-`e2e` is the mixed method through the host-buffer API (pinned geometry and
-data in, solution out) in the same way.  With N > 1 GPUs (torchrun) every
+side resident in HBM, geometry in pinned host memory, the L2 flushed (256
+MiB write) before every step, no per-launch instrumentation inside the timed
+steps (the per-kernel figures come from one instrumented factorization and
+the refinement's parts timed alone afterwards); `e2e` is the mixed method
+through the host-buffer API (pinned geometry and data in, solution out) in
+the same way.  With N > 1 GPUs (torchrun) every
 rank solves its own replica (one problem does not shard): weak scaling, time
-= max over ranks.  Unless --no-adjoint, the default workload also times the
+= max over ranks.  Unless --no-adjoint, a single-problem workload also times the
 adjoint of the target-potential objective on the 8192-node Fourier star
 (forward solve + targets, backward transposed solve + kernel-derivative
 contractions).  `--impl reference` times the reference solver compiled from
@@ -325,13 +330,51 @@ def rel(a, b):
 
 
 # ------------------------------------------------------------------ GPU arm
+# algorithmic FP64 flops per (target node, source node) pair of the operator
+# product: Laplace r (2), |r|^2 (3), reciprocal (1), r.n (3), scaled sum (2);
+# Stokes the same pair terms plus the 2x2 tensor block (r.n, r.d, two
+# outputs): 20
+PAIR_FLOPS = {G.LAPLACE: 11.0, G.LAPLACE_NEUMANN: 11.0, G.STOKES: 20.0}
+
+
+def pin_problem(p):
+    """A copy of the problem whose geometry and data arrays are in pinned
+    host memory (the arrays the factorization reads)."""
+    import copy
+    import torch
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
+    q = copy.copy(p)
+    q.points, q.normals = pin(p.points), pin(p.normals)
+    q.curvatures, q.weights = pin(p.curvatures), pin(p.weights)
+    q.f = pin(p.f)
+    return q
+
+
+def event_ms(stream, fn, reps=5, flush=None):
+    """Median CUDA-event time of fn() on `stream` (L2 flushed before each)."""
+    import torch
+    out = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.median(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="star16k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="stokes65k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
@@ -366,35 +409,42 @@ def main():
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    # geometry and data in pinned host memory for every arm
+    pp = [pin_problem(p) for p in probs]
     f_host = np.concatenate([p.f for p in probs])
     f_dev = torch.tensor(f_host, device=dev, dtype=torch.float64)
     mu_dev = torch.empty_like(f_dev)
-    pr0 = probs[0]
+    pr0 = pp[0]
     nb = 0 if batch else (3 * pr0.holes.shape[0] if pr0.pde == G.STOKES else pr0.holes.shape[0])
     al_dev = torch.empty(max(nb, 1), device=dev, dtype=torch.float64)
 
     def factor(tol, timed=False, mode=0):
         if batch:
-            return kinterp.BatchSolver(probs, id_tol=tol, stream=sh, mode=mode)
+            return kinterp.BatchSolver(pp, id_tol=tol, stream=sh, mode=mode)
         return kinterp.Solver(pr0, id_tol=tol, stream=sh, timed=timed, mode=mode)
 
-    def mixed_step(timed):
-        s = factor(MIXED_TOL, timed, MIXED_MODE)
+    def refine(s):
         if batch:
-            it, rr = s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
-                                            rel_tol=REFINE_TOL, max_iters=20)
-        else:
-            it, rr = s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
-                                            al_dev.data_ptr() if nb else None,
-                                            rel_tol=REFINE_TOL, max_iters=20)
-        return s, it, rr
+            return s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
+                                          rel_tol=REFINE_TOL, max_iters=20)
+        return s.solve_refined_device(f_dev.data_ptr(), mu_dev.data_ptr(),
+                                      al_dev.data_ptr() if nb else None,
+                                      rel_tol=REFINE_TOL, max_iters=20)
 
-    def fp64_step(timed):
-        s = factor(FP64_TOL, timed)
+    def direct(s):
         if batch:
             s.solve_device(f_dev.data_ptr(), mu_dev.data_ptr())
         else:
             s.solve_device(f_dev.data_ptr(), mu_dev.data_ptr(), al_dev.data_ptr() if nb else None)
+
+    def mixed_step(timed=False):
+        s = factor(MIXED_TOL, timed, MIXED_MODE)
+        it, rr = refine(s)
+        return s, it, rr
+
+    def fp64_step(timed=False):
+        s = factor(FP64_TOL, timed)
+        direct(s)
         return s
 
     def timed_loop(step_fn):
@@ -415,25 +465,19 @@ def main():
 
     # warm-up of both methods
     for _ in range(args.warmup):
-        mixed_step(False)[0].close()
-        fp64_step(False).close()
+        mixed_step()[0].close()
+        fp64_step().close()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
 
-    # ---- mixed + refine (the value)
+    # ---- mixed + refine (the value): no per-launch timing instrumentation
     clocks = Clocks(local)
     launches0 = kinterp.kernel_launches()
-    keys = ("id_ms", "id_flops", "id_bytes", "id_launches", "factor_ms", "decouple_ms", "top_ms")
-    st_acc = {k: 0.0 for k in keys}
     iters, rres = [], []
 
     def mixed_timed():
-        s, it, rr = mixed_step(not batch)
-        if not batch:
-            st = s.stats()
-            for k in keys:
-                st_acc[k] += st[k]
+        s, it, rr = mixed_step()
         iters.append(it)
         rres.append(rr)
         s.close()
@@ -441,37 +485,23 @@ def main():
     t_mixed = timed_loop(mixed_timed)
     launches = kinterp.kernel_launches() - launches0
     clk = clocks.stop()
+    torch.cuda.synchronize()
     mu_mixed = mu_dev.cpu().numpy()
     al_mixed = al_dev.cpu().numpy()[:nb]
 
     # ---- FP64 direct (the reference method on the GPU)
-    f64_factor = []
-
-    def fp64_timed():
-        s = fp64_step(not batch)
-        if not batch:
-            f64_factor.append(s.stats()["factor_ms"])
-        s.close()
-
-    t_fp64 = timed_loop(fp64_timed)
+    t_fp64 = timed_loop(lambda: fp64_step().close())
+    torch.cuda.synchronize()
     mu_fp64 = mu_dev.cpu().numpy()
 
     # ---- e2e: public host-buffer API, pinned inputs, solution read back
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
-    import copy
-    pp = []
-    for p in probs:
-        q = copy.copy(p)
-        q.points, q.normals = pin(p.points), pin(p.normals)
-        q.curvatures, q.weights = pin(p.curvatures), pin(p.weights)
-        pp.append(q)
-    f_pin = pin(f_host)
+    f_pin = torch.from_numpy(f_host).pin_memory().numpy()
 
     def e2e_step():
         if batch:
             s = kinterp.BatchSolver(pp, id_tol=MIXED_TOL, stream=sh, mode=MIXED_MODE)
         else:
-            s = kinterp.Solver(pp[0], id_tol=MIXED_TOL, stream=sh, mode=MIXED_MODE)
+            s = kinterp.Solver(pr0, id_tol=MIXED_TOL, stream=sh, mode=MIXED_MODE)
         s.solve_refined(f_pin, rel_tol=REFINE_TOL, max_iters=20)
         s.close()
 
@@ -480,6 +510,38 @@ def main():
     t_mixed, t_fp64, t_e2e = max_over_ranks([t_mixed, t_fp64, t_e2e], dist, dev)
 
     if rank == 0:
+        # ---- per-kernel figures from separate, untimed passes: one
+        # instrumented factorization of each method (launch durations by
+        # CUDA events on the launching streams), then the refinement's parts
+        # (one preconditioner application, one FP64 operator product, one
+        # correction product) timed alone on the factorization it uses
+        st, st64 = {}, {}
+        parts = {}
+        if not batch:
+            s = factor(MIXED_TOL, True, MIXED_MODE)
+            st = s.stats()
+            n = s.n_dofs + s.n_border
+            xv = torch.randn(n, device=dev, dtype=torch.float64)
+            yv = torch.empty_like(xv)
+            parts["solve_ms"] = event_ms(stream, lambda: direct(s), flush=flush)
+            parts["matvec_ms"] = event_ms(
+                stream, lambda: s.matvec_device(xv.data_ptr(), yv.data_ptr()), flush=flush)
+            parts["corr_matvec_ms"] = event_ms(
+                stream, lambda: s.matvec_correction_device(xv.data_ptr(), yv.data_ptr(), 1.0),
+                flush=flush)
+            parts["refine_ms"] = event_ms(stream, lambda: refine(s), flush=flush)
+            # true FP64 residual of the timed run's solution
+            xs = torch.tensor(np.concatenate([mu_mixed, al_mixed]), device=dev,
+                              dtype=torch.float64)
+            s.matvec_device(xs.data_ptr(), yv.data_ptr())
+            torch.cuda.synchronize()
+            bvec = np.concatenate([f_host, np.zeros(nb)])
+            parts["true_rel_residual"] = float(np.linalg.norm(bvec - yv.cpu().numpy()) /
+                                               np.linalg.norm(f_host))
+            s.close()
+            s = factor(FP64_TOL, True)
+            st64 = s.stats()
+            s.close()
         # accuracy against the FP64 oracle (at the reference's 1e-10 and,
         # as the converged solution, at 1e-13)
         idx = [0, 100, 200] if batch else [0]
@@ -494,13 +556,55 @@ def main():
             s.close()
         peak64 = fp64_peak_tflops(dev)
         hbm_peak, hbm_kind = peaks()
-        id_ms = st_acc["id_ms"]
-        achieved = (st_acc["id_flops"] / (id_ms * 1e-3)) / 1e12 if id_ms > 0 else None
-        nlaunch = max(st_acc["id_launches"], 1)
         h2d = sum(8 * (6 * p.n_points) for p in probs) + 8 * units
         d2h = 8 * (units + nb)
         value = world * units * args.steps / (t_mixed * 1e-3)
         fp64_value = world * units * args.steps / (t_fp64 * 1e-3)
+        rooflines = {}
+        if st:
+            def fp64_line(kernel, flops, ms, launches=None):
+                a = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
+                return {"kernel": kernel, "bound": "fp64", "achieved": a, "peak": peak64,
+                        "unit": "TFLOP/s", "frac": a / peak64 if a else None,
+                        "flops_per_step": flops, "ms_per_step": ms, "launches": launches}
+            rooflines["id"] = fp64_line(
+                "id_onchip_kernel / id_kernel (entry generation, pivoted QR, T)",
+                st["id_flops"], st["id_ms"], st["id_launches"])
+            rooflines["id"]["algorithmic_hbm_bytes"] = st["id_bytes"]
+            rooflines["id"]["traffic_per_launch"] = traffic_from_profile(args.workload)
+            rooflines["decouple"] = fp64_line(
+                "decouple_kernel + large-box sequences (K_BN, T products, X_rr^-1, L, U, update)",
+                st["dec_flops"], st["decouple_ms"])
+            rooflines["top"] = fp64_line("assemble_top + lu_fused_kernel (top-level LU)",
+                                         st["top_flops"], st["top_ms"])
+            pairs = float(sum(p.n_points ** 2 for p in probs))
+            rooflines["operator_product"] = fp64_line(
+                "mv_partial_kernel + mv_finish_kernel (FP64 refinement residual)",
+                PAIR_FLOPS[pr0.pde] * pairs, parts["matvec_ms"])
+            sb = st["solve_bytes"]
+            rooflines["solve_sweeps"] = {
+                "kernel": "sweep_kernel / diag_inv_kernel / top LU solve (one preconditioner "
+                          "application)", "bound": "hbm",
+                "achieved": sb / (parts["solve_ms"] * 1e-3) / 1e9, "peak": hbm_peak,
+                "unit": "GB/s", "frac": sb / (parts["solve_ms"] * 1e-3) / 1e9 / hbm_peak,
+                "bytes": sb, "ms": parts["solve_ms"], "peak_source": hbm_kind}
+        # the dominant kernel family of the mixed step
+        dom = None
+        if rooflines:
+            shares = {"id": st["id_ms"], "decouple": st["decouple_ms"], "top": st["top_ms"],
+                      "operator_product": parts["matvec_ms"],
+                      "solve_sweeps": parts["solve_ms"] * max(1.0, float(np.mean(iters)))}
+            dom = max(shares, key=shares.get)
+        roof = None
+        if dom:
+            r = rooflines[dom]
+            roof = {"kernel": r["kernel"], "family": dom, "bound": r["bound"],
+                    "achieved": r["achieved"], "peak": r["peak"], "unit": r["unit"],
+                    "frac": r["frac"],
+                    "peak_source": ("measured live on this GPU: cuBLAS DGEMM 4096^3 (no FP64 "
+                                    "figure in MEASURED_PEAKS.json)" if r["bound"] == "fp64"
+                                    else "MEASURED_PEAKS.json hbm_gbs (%s)" % hbm_kind),
+                    "traffic": traffic_from_profile(args.workload) if dom == "id" else None}
         line = {
             "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed / args.steps,
@@ -509,47 +613,44 @@ def main():
             "config": {"workload": WORKLOADS[args.workload][1], "n_dofs": units,
                        "method": "mixed+refine: factor at id_tol %g in preconditioner mode "
                                  "(sketched IDs), FP64 refinement/GMRES with on-the-fly FP64 "
-                                 "operator to true rel. residual %g" % (MIXED_TOL, REFINE_TOL),
+                                 "operator (small residuals updated with FP32 far-field "
+                                 "correction products) to rel. residual %g"
+                                 % (MIXED_TOL, REFINE_TOL),
                        "leaf_dofs": pr0.max_leaf_dofs,
                        "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "flushed between steps (256 MiB device write)"},
-            "gmres_iters": float(np.mean(iters)), "true_rel_residual": float(max(rres)),
+                       "l2": "flushed between steps (256 MiB device write)",
+                       "inputs": "geometry and data in pinned host memory; f resident in HBM "
+                                 "for value, copied in and mu copied out for e2e"},
+            "gmres_iters": float(np.mean(iters)), "rel_residual": float(max(rres)),
+            "true_rel_residual": parts.get("true_rel_residual"),
             "rel_err_vs_fp64_oracle": err(mu_mixed, o10),
             "rel_err_vs_converged_oracle": err(mu_mixed, o13),
             "fp64_oracle_own_err": max(rel(a, b) for a, b in zip(o10, o13)),
             "analytic_rel_err": analytic,
-            "factor_ms": None if batch else st_acc["factor_ms"] / args.steps,
-            "phase_ms_per_step": None if batch else {
-                "id": id_ms / args.steps, "decouple": st_acc["decouple_ms"] / args.steps,
-                "top": st_acc["top_ms"] / args.steps},
+            "phase_ms": None if batch else {
+                "factor": st["factor_ms"], "id": st["id_ms"], "decouple": st["decouple_ms"],
+                "top": st["top_ms"], "host_wait_on_ranks": st["wait_ms"],
+                "refine": parts["refine_ms"], "one_solve": parts["solve_ms"],
+                "fp64_operator_product": parts["matvec_ms"],
+                "correction_product": parts["corr_matvec_ms"],
+                "note": "one instrumented factorization and the refinement's parts timed "
+                        "alone, outside the timed steps; launch durations overlap "
+                        "(IDs of level l-1 run beside the decoupling of level l)"},
             "fp64": {"value": fp64_value, "ms_per_step": t_fp64 / args.steps,
-                     "factor_ms": float(np.mean(f64_factor)) if f64_factor else None,
+                     "factor_ms": st64.get("factor_ms"),
                      "id_tol": FP64_TOL,
                      "rel_err_vs_fp64_oracle": err(mu_fp64, o10),
                      "rel_err_vs_converged_oracle": err(mu_fp64, o13)},
             "speedup_mixed_vs_fp64": value / fp64_value,
-            "roofline": None if not id_ms else {
-                "kernel": "ID kernels (id_onchip_kernel / id_kernel: entry generation, "
-                          "pivoted QR, T) of the mixed factorization",
-                "bound": "tensor", "pipe": "fp64 (no tcgen05 FP64 kind; FP64 FMA)",
-                "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                "frac": (achieved / peak64) if achieved else None,
-                "peak_source": "measured live on this GPU: cuBLAS DGEMM 4096^3 "
-                               "(no FP64 figure in MEASURED_PEAKS.json)",
-                "flops_per_launch": st_acc["id_flops"] / nlaunch,
-                "algorithmic_hbm_bytes_per_launch": st_acc["id_bytes"] / nlaunch,
-                "hbm_frac_of_measured": (st_acc["id_bytes"] / (id_ms * 1e-3)) / 1e9 / hbm_peak,
-                "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_kind,
-                "launches_per_step": st_acc["id_launches"] / args.steps,
-                "ms_per_step": id_ms / args.steps,
-                "traffic": traffic_from_profile(args.workload)},
+            "roofline": roof,
+            "rooflines": rooflines or None,
             "e2e": {"value": world * units * args.steps / (t_e2e * 1e-3),
                     "unit": "unknowns/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "clocks": clk,
         }
-        if args.workload == "star16k" and not args.no_adjoint:
+        if not args.no_adjoint and not batch:
             line["adjoint"] = adjoint_bench(dev, stream)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args.workload, probs)

@@ -120,6 +120,12 @@ int ki_solve_refined(ki_solver_t s, const double* f, double* mu, double* alpha, 
 /* The refinement's operator product: same y as ki_apply_device up to FP64
  * rounding (fused and reassociated, not bit-identical to the entries). */
 int ki_matvec_device(ki_solver_t s, const double* d_x, double* d_y);
+/* The refinement's product for a small correction d (no reference
+ * counterpart): source blocks far from a target tile summed in FP32 (d
+ * scaled by dscale > 0 on the way, to keep it in FP32's normal range), near
+ * ones in FP64; relative error ~1e-6 of |A| |d|.  ki_solve_refined uses it
+ * to update small residuals. */
+int ki_matvec_correction_device(ki_solver_t s, const double* d_x, double* d_y, double dscale);
 
 /* x = A^-T b with the factorization (no reference counterpart: the
  * reference solves only with A, skel_factorization.cpp:341-403).  Simply
@@ -183,6 +189,19 @@ int ki_domain_mask_device(ki_solver_t s, int n_targets, const double* d_targets,
 int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, double y_max,
                      double* points);
 
+/* A handle holding device copies of the boundary arrays only, without a
+ * quadtree or factors: the Kernel object of the reference (kernel.h:15-41,
+ * its boundary copies) for dense entry blocks (ki_kernel_block,
+ * ki_forward_block); every other call refuses it.  Free with ki_destroy. */
+int ki_geometry(int pde, int n_points, const double* points, const double* normals,
+                const double* curvatures, const double* weights, void* stream,
+                ki_solver_t* out);
+/* Kernel::operator() with forward = true (kernel.cpp:114-150, 337-357): the
+ * column-major nt x ns block of forward entries, row i the domain dof tgt[i]
+ * (point tgt[i] / sol_dim of the n_targets interleaved xy targets, velocity
+ * component tgt[i] % sol_dim), column j the boundary dof src[j]. */
+int ki_forward_block(ki_solver_t s, int n_targets, const double* targets, int nt, const int* tgt,
+                     int ns, const int* src, double* out);
 /* Kernel::operator() (kernel/kernel.cpp:99-111): column-major nt x ns block
  * K(tgt, src) evaluated on the GPU. */
 int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src,
@@ -197,6 +216,11 @@ int ki_num_boxes(ki_solver_t s, int level);
 int ki_box_info(ki_solver_t s, int level, int idx, int* info, double* geom);
 int ki_box_lists(ki_solver_t s, int level, int idx, int* original, int* active,
                  int* skel, int* redundant);
+/* Neighbour list of a box (QuadTreeNode::neighbors, computed by
+ * compute_neighbor_lists, quadtree.cpp:27-69), in the reference's order:
+ * neighbour q is box nbr_idx[q] of level nbr_level[q].  Returns the count
+ * (negative on error); either output may be NULL. */
+int ki_box_neighbors(ki_solver_t s, int level, int idx, int* nbr_level, int* nbr_idx);
 /* Top-level skeleton (root active box); returns its size, fills out if given. */
 int ki_allskel(ki_solver_t s, int* out);
 
@@ -207,9 +231,13 @@ int ki_allskel(ki_solver_t s, int* out);
  * [5] decouple ms, [6] top-level LU ms, [7] host ms blocked on rank
  * downloads, host ms spent on [8] level lists before the ID launches,
  * [9] skeleton/decouple bookkeeping, [10] uploads, [11] the top level,
- * [12] the part of [3] done by on-chip launches (timed factorizations only for
- * [1], [5], [6]).  Returns the number of values written (at most n, at
- * most 13). */
+ * [12] the part of [3] done by on-chip launches, [13] pinned staging bytes
+ * the handle has used since it was made or last updated, [14] decoupling
+ * algorithmic FP64 flops (K_BN entries, the products with T, X_rr^-1, L,
+ * U and the accumulated update), [15] top-level flops (assembly + 2/3 n^3
+ * LU), [16] factor bytes one solve reads (T twice, L, U, X_rr^-1, top LU,
+ * 8 vector passes) (timed factorizations only for [1], [5], [6]).
+ * Returns the number of values written (at most n, at most 17). */
 int ki_stats(ki_solver_t s, double* out, int n);
 /* Launch log of a ki_factor_timed factorization: rows of 7 doubles
  * (level, kind 0 ID / 1 decouple / 2 top LU, cluster size, boxes, max rows,
@@ -297,7 +325,8 @@ int ki_box_tree(ki_solver_t s, int level, int idx);
  * the n_rows near dofs.  The ID matrix is [K(rows, active); K(active,
  * rows)^T], followed, when proxy is nonzero, by the 128-point proxy-circle
  * rows of centre (cx, cy) and the given radius (256 rows for Laplace, 512
- * for Stokes).  Device outputs: *d_rank (0: not compressible), d_perm
+ * for Stokes).  Every dof in d_active and d_rows must be below n_points
+ * (Laplace) or 2 n_points (Stokes): the device does not check them.  Device outputs: *d_rank (0: not compressible), d_perm
  * (n_active pivots, active positions), d_T (k x (n_active - k), ld k;
  * capacity n_active^2 / 4 + 1 doubles).
  * The m x n working matrix lives in one static 8 MiB device array: calls

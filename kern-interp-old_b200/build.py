@@ -77,9 +77,35 @@ def build(force=False, verbose=False):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    build_facade(force)
     if verbose:
-        print("built", LIB)
+        print("built", LIB, "and", FACADE_LIB)
     return LIB
+
+
+FACADE = os.path.join(HERE, "facade")
+FACADE_LIB = os.path.join(HERE, "libkern_interp.so")
+
+
+def build_facade(force=False):
+    """libkern_interp.so: the C++ drop-in API (include/kern_interp/*.h),
+    host code over the C ABI of libkinterp.so (found next to it at run
+    time through its rpath)."""
+    srcs = sorted(os.path.join(FACADE, f) for f in os.listdir(FACADE) if f.endswith(".cpp"))
+    hdrs = []
+    for d, _, fs in os.walk(os.path.join(INCLUDE, "kern_interp")):
+        hdrs += [os.path.join(d, f) for f in fs if f.endswith(".h")]
+    hdrs.append(os.path.join(INCLUDE, "kinterp.h"))
+    newest = max(os.path.getmtime(x) for x in srcs + hdrs + [LIB])
+    if not force and os.path.exists(FACADE_LIB) and os.path.getmtime(FACADE_LIB) >= newest:
+        return FACADE_LIB
+    cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + INCLUDE, "-o", FACADE_LIB] + srcs + \
+          ["-L" + HERE, "-l:libkinterp.so", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("facade build failed:\n%s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+    return FACADE_LIB
 
 
 if __name__ == "__main__":

@@ -147,7 +147,32 @@ __global__ void block_kernel(int pde, const Node* __restrict__ nodes, const int*
   out[e] = boundary_entry(pde, nodes, tgt[i], src[j]);
 }
 
+// Forward entries (Kernel::forward, kernel.cpp:337-357): row i is domain
+// dof tgt[i] (the point tgt[i] / sd, velocity component tgt[i] % sd),
+// column j boundary dof src[j]; column-major nt x ns.
+__global__ void forward_block_kernel(int pde, const Node* __restrict__ nodes,
+                                     const double* __restrict__ tp, const int* tgt, int nt,
+                                     const int* src, int ns, double* out) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(nt) * ns) return;
+  const int i = static_cast<int>(e % nt), j = static_cast<int>(e / nt);
+  const int sd = pde == kStokes ? 2 : 1;
+  const int pt = tgt[i] / sd, comp = tgt[i] % sd;
+  out[e] = forward_entry(pde, nodes, tp[2 * pt], tp[2 * pt + 1], comp, src[j]);
+}
+
 }  // namespace
+
+cudaError_t launch_forward_block(int pde, const Node* nodes, const double* targets,
+                                 const int* tgt, int nt, const int* src, int ns, double* out,
+                                 cudaStream_t s) {
+  const long long tot = static_cast<long long>(nt) * ns;
+  if (tot == 0) return cudaSuccess;
+  count_launches(1);
+  forward_block_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(pde, nodes, targets,
+                                                                           tgt, nt, src, ns, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_apply_operator(int pde, const Node* nodes, int n_dofs, const int* seg,
                                   int nseg, const double* x, double* y, int nb, const double* U,

@@ -18,6 +18,7 @@ struct ki_solver_s {
   double* d_io = nullptr;  // staging for host-buffer calls
   size_t io_bytes = 0;
   bool tree_only = false;  // ki_partition handle: no factors on the device
+  bool geom_only = false;  // ki_geometry handle: device boundary arrays only
   ~ki_solver_s() {
     solver.reset();  // synchronises the stream: nothing queued uses d_io
     if (d_io) kib::chunk_pool::put(d_io, io_bytes, false);
@@ -387,6 +388,13 @@ int ki_matvec_device(ki_solver_t s, const double* d_x, double* d_y) {
   return from_solver(s, s->solver->matvec_device(d_x, d_y));
 }
 
+int ki_matvec_correction_device(ki_solver_t s, const double* d_x, double* d_y, double dscale) {
+  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || !d_x || !d_y || !(dscale > 0.0))
+    return set_err(KI_ERR_ARG, "ki_matvec_correction_device: bad args");
+  return from_solver(s, s->solver->corr_matvec_device(d_x, d_y, dscale));
+}
+
 int ki_solve_transpose_device(ki_solver_t s, const double* d_b, double* d_x) {
   if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
   if (!s || !s->solver || !d_b || !d_x) return set_err(KI_ERR_ARG, "ki_solve_transpose_device: bad args");
@@ -565,8 +573,77 @@ int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, 
   return KI_OK;
 }
 
+int ki_geometry(int pde, int n_points, const double* points, const double* normals,
+                const double* curvatures, const double* weights, void* stream,
+                ki_solver_t* out) {
+  if (!out) return set_err(KI_ERR_ARG, "ki_geometry: out is NULL");
+  *out = nullptr;
+  if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_geometry: bad pde");
+  if (n_points <= 0 || !points || !normals || !curvatures || !weights)
+    return set_err(KI_ERR_ARG, "ki_geometry: no boundary points");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+    return set_err(KI_ERR_CUDA, "no CUDA device available");
+  std::unique_ptr<ki_solver_s> h(new (std::nothrow) ki_solver_s());
+  if (!h) return set_err(KI_ERR_ARG, "out of host memory");
+  if (stream) {
+    h->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    KI_TRY(cuda_err(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking),
+                    "cudaStreamCreate"));
+    h->own_stream = true;
+  }
+  kib::SolverOptions opt;
+  opt.pde = pde;
+  h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, 0,
+                                  nullptr, h->stream));
+  const int rc = h->solver->prepare_geometry();
+  if (rc) return from_solver(h.get(), rc);
+  h->tree_only = true;
+  h->geom_only = true;
+  *out = h.release();
+  return KI_OK;
+}
+
+int ki_forward_block(ki_solver_t s, int n_targets, const double* targets, int nt, const int* tgt,
+                     int ns, const int* src, double* out) {
+  if (s && s->tree_only && !s->geom_only)
+    return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (!s || !s->solver || n_targets < 0 || nt < 0 || ns < 0 ||
+      (nt * ns > 0 && (!tgt || !src || !out || !targets)))
+    return set_err(KI_ERR_ARG, "ki_forward_block: bad args");
+  if (nt == 0 || ns == 0) return KI_OK;
+  const int N = s->solver->n_dofs();
+  const int sd = s->solver->pde() == KI_STOKES ? 2 : 1;
+  for (int i = 0; i < nt; i++)
+    if (tgt[i] < 0 || tgt[i] >= sd * n_targets)
+      return set_err(KI_ERR_ARG, "ki_forward_block: tgt out of range");
+  for (int j = 0; j < ns; j++)
+    if (src[j] < 0 || src[j] >= N) return set_err(KI_ERR_ARG, "ki_forward_block: src out of range");
+  const size_t ints = static_cast<size_t>(nt) + ns;
+  const size_t need = sizeof(double) * (static_cast<size_t>(nt) * ns + 2 * n_targets) +
+                      sizeof(int) * ints + 64;
+  KI_TRY(staging(s, need));
+  double* d_out = s->d_io;
+  double* d_tp = d_out + static_cast<size_t>(nt) * ns;
+  int* d_t = reinterpret_cast<int*>(d_tp + 2 * static_cast<size_t>(n_targets));
+  int* d_s = d_t + nt;
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_tp, targets, sizeof(double) * 2 * n_targets,
+                                  cudaMemcpyHostToDevice, s->stream), "copy"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_t, tgt, sizeof(int) * nt, cudaMemcpyHostToDevice, s->stream), "copy"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(d_s, src, sizeof(int) * ns, cudaMemcpyHostToDevice, s->stream), "copy"));
+  KI_TRY(cuda_err(kib::launch_forward_block(s->solver->pde(), s->solver->d_nodes(), d_tp, d_t,
+                                            nt, d_s, ns, d_out, s->stream),
+                  "forward block"));
+  KI_TRY(cuda_err(cudaMemcpyAsync(out, d_out, sizeof(double) * nt * ns, cudaMemcpyDeviceToHost,
+                                  s->stream),
+                  "copy out"));
+  return cuda_err(cudaStreamSynchronize(s->stream), "ki_forward_block");
+}
+
 int ki_kernel_block(ki_solver_t s, int nt, const int* tgt, int ns, const int* src, double* out) {
-  if (s && s->tree_only) return set_err(KI_ERR_STATE, "handle holds a partition only");
+  if (s && s->tree_only && !s->geom_only)
+    return set_err(KI_ERR_STATE, "handle holds a partition only");
   if (!s || !s->solver || nt < 0 || ns < 0 || (nt * ns > 0 && (!tgt || !src || !out)))
     return set_err(KI_ERR_ARG, "ki_kernel_block: bad args");
   if (nt == 0 || ns == 0) return KI_OK;
@@ -639,6 +716,25 @@ int ki_box_lists(ki_solver_t s, int level, int idx, int* original, int* active, 
   return KI_OK;
 }
 
+int ki_box_neighbors(ki_solver_t s, int level, int idx, int* nbr_level, int* nbr_idx) {
+  const kib::Box* b;
+  int par;
+  if (!box_ref(s, level, idx, &b, &par)) return -set_err(KI_ERR_ARG, "ki_box_neighbors: bad box");
+  const auto& lv = s->solver->tree.levels;
+  const auto& boxes = s->solver->tree.boxes;
+  int q = 0;
+  for (int o : b->nbr) {
+    const int ol = boxes[o].level;
+    int pos = -1;
+    for (size_t i = 0; i < lv[ol].size() && pos < 0; i++)
+      if (lv[ol][i] == o) pos = static_cast<int>(i);
+    if (nbr_level) nbr_level[q] = ol;
+    if (nbr_idx) nbr_idx[q] = pos;
+    q++;
+  }
+  return q;
+}
+
 int ki_allskel(ki_solver_t s, int* out) {
   if (!s || !s->solver) return -KI_ERR_ARG;
   const auto& v = s->solver->allskel;
@@ -688,8 +784,9 @@ int ki_stats(ki_solver_t s, double* out, int n) {
                          v.id_flops,       v.id_bytes,       v.t_decouple_ms,
                          v.t_top_ms,       v.t_wait_ms,      v.t_host_prep_ms,
                          v.t_host_post_ms, v.t_upload_ms,    v.t_host_top_ms,
-                         v.id_onchip_flops};
-  const int cnt = n < 13 ? n : 13;
+                         v.id_onchip_flops, static_cast<double>(v.staging_bytes()),
+                         v.dec_flops,      v.top_flops,      v.solve_bytes};
+  const int cnt = n < 17 ? n : 17;
   for (int i = 0; i < cnt; i++) out[i] = vals[i];
   return cnt;
 }

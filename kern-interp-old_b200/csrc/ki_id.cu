@@ -1004,6 +1004,8 @@ static __device__ __align__(256) double g_noalloc_dir[2 * kNumProxy];
 
 namespace {
 
+__global__ void noalloc_set_task_kernel(IdTask tk) { g_noalloc_task[0] = tk; }
+
 struct NoAllocSlot {
   bool ready = false;
   double* scratch = nullptr;
@@ -1065,7 +1067,11 @@ cudaError_t launch_id_noalloc(int pde, const Node* nodes, const int* act, int n,
   tk.cy = cy;
   tk.rad = radius;
   tk.pw = 2.0 * M_PI * radius / kNumProxy;
-  e = cudaMemcpyToSymbolAsync(g_noalloc_task, &tk, sizeof(IdTask), 0, cudaMemcpyHostToDevice, s);
+  // the descriptor travels as a kernel argument (copied at launch, so the
+  // host's copy may go out of scope at once) and is stored by one thread
+  count_launches(1);
+  noalloc_set_task_kernel<<<1, 1, 0, s>>>(tk);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   IdParams p{};
   p.tasks = sl->task;

@@ -294,6 +294,11 @@ cudaError_t launch_copy_segments(const CopySeg* segs, int n, cudaStream_t s);
 // is Psi^T stored dof-major).
 cudaError_t launch_border_fill(int pde, const Node* nodes, int np, const double* holes, int nh,
                                double* U, double* Psi, double* Urow, cudaStream_t s);
+// Forward block: domain dofs tgt (point tgt / sd of `targets`, component
+// tgt % sd) against boundary dofs src, column-major nt x ns.
+cudaError_t launch_forward_block(int pde, const Node* nodes, const double* targets,
+                                 const int* tgt, int nt, const int* src, int ns, double* out,
+                                 cudaStream_t s);
 // Dense kernel block K(tgt, src), column-major nt x ns.
 cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int nt,
                                 const int* src, int ns, double* out, cudaStream_t s);
@@ -323,6 +328,14 @@ cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, 
                                const int* seg, int nseg, int n_dofs, int splits, const double* x,
                                double* y, int nb, const double* U, const double* Psi,
                                double* part, cudaStream_t s);
+// The same product for a small correction d (see ki_krylov.cu): source
+// blocks whose bounding box comes within near_gap of the target tile's in
+// FP64, the others in FP32 with the densities scaled by dscale (> 0).
+cudaError_t launch_corr_matvec(int pde, const Node* nodes, const MvTile* tiles, int ntiles,
+                               const int* seg, int nseg, int n_dofs, int splits, const double* x,
+                               double dscale, double near_gap, double* y, int nb,
+                               const double* U, const double* Psi, double* part,
+                               cudaStream_t s);
 // out[j] = V_j . w for j < k (V column j at V + ldv j); part needs
 // k * multi_dot_blocks(n) doubles.  Fixed reduction order.
 int multi_dot_blocks(int n);

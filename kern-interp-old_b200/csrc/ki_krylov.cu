@@ -126,6 +126,193 @@ __global__ void __launch_bounds__(kMvThreads)
   }
 }
 
+// Operator product of a refinement correction, y = A d, where d is small
+// next to the iterate (|d| ~ the preconditioner's accuracy times |x|), so a
+// relative error eps in A d moves the updated residual r - A d by eps |d|
+// only.  The pair sums run in FP32 (twice the FP64 pipe's rate, one MUFU
+// reciprocal per pair) on coordinates taken relative to the target tile's
+// first node, with the densities scaled by `dscale` (~1/|d|) to keep them
+// in FP32's normal range; each 256-source block's FP32 sums are added to
+// FP64 accumulators.  A source block whose bounding box comes within
+// sqrt(near2) of the target tile's is summed in FP64 exactly as in
+// mv_partial_kernel: for nearby nodes of one curve r.n_s is a small
+// difference of O(|r|) terms (it behaves like kappa |r|^2 / 2), which FP32
+// coordinates cannot resolve.  With gap g, the FP32 pairs' entries err by
+// about u32 (|s - o| + |t - o|) w / (pi r^2); summed along a curve of node
+// spacing h beyond the gap this is ~ u32 diam w / (h g) per unit density,
+// 1e-6 for g = 0.01 on the workloads here.  Partials, rank-one slots and the
+// finish are those of the FP64 product.
+template <int PDE>
+__global__ void __launch_bounds__(kMvThreads)
+    mv_corr_partial_kernel(const Node* __restrict__ nodes, const MvTile* __restrict__ tiles,
+                           long long part_stride, const double* __restrict__ x, double dscale,
+                           float near2, double* __restrict__ part,
+                           double* __restrict__ part_rank1) {
+  __shared__ double sx[kMvThreads], sy[kMvThreads], sa0[kMvThreads], sa1[kMvThreads];
+  __shared__ double sd0[kMvThreads], sd1[kMvThreads];
+  __shared__ float fx[kMvThreads], fy[kMvThreads], fa0[kMvThreads], fa1[kMvThreads];
+  __shared__ float fd0[kMvThreads], fd1[kMvThreads];
+  __shared__ float wbox[2][4][kMvThreads / 32];  // per-warp box: [target|source][x0,y0,-x1,-y1]
+  __shared__ double red[kMvThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const MvTile tile = tiles[blockIdx.x];
+  const int t = tile.t0 + threadIdx.x;
+  const int s0 = tile.s0, s1 = tile.s1;
+  const bool live = t < tile.t1;
+  const Node org = nodes[tile.t0];
+  const double ox = org.x, oy = org.y;
+  const double inv_scale = 1.0 / dscale;
+  double tx = 0, ty = 0, tnx = 0, tny = 0;
+  if (live) {
+    const Node nt = nodes[t];
+    tx = nt.x;
+    ty = nt.y;
+    tnx = nt.nx;
+    tny = nt.ny;
+  }
+  const float ftx = static_cast<float>(tx - ox), fty = static_cast<float>(ty - oy);
+  const float ftnx = static_cast<float>(tnx), ftny = static_cast<float>(tny);
+  // bounding box of a point per thread over the CTA: warp min/max here, the
+  // per-warp results combined by every thread after the next barrier
+  auto warp_box = [&](int which, bool valid, float px, float py) {
+    float b0 = valid ? px : 3e38f, b1 = valid ? py : 3e38f;
+    float b2 = valid ? -px : 3e38f, b3 = valid ? -py : 3e38f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      b0 = fminf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
+      b1 = fminf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+      b2 = fminf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+      b3 = fminf(b3, __shfl_xor_sync(0xffffffffu, b3, o));
+    }
+    if (lane == 0) {
+      wbox[which][0][warp] = b0;
+      wbox[which][1][warp] = b1;
+      wbox[which][2][warp] = b2;
+      wbox[which][3][warp] = b3;
+    }
+  };
+  auto cta_box = [&](int which, int c) {
+    float b = 3e38f;
+#pragma unroll
+    for (int w = 0; w < kMvThreads / 32; w++) b = fminf(b, wbox[which][c][w]);
+    return b;
+  };
+  warp_box(0, live, ftx, fty);
+  double y0 = 0.0, y1 = 0.0, r1 = 0.0;
+  for (int base = s0; base < s1; base += kMvThreads) {
+    const int j = base + threadIdx.x;
+    __syncthreads();
+    const bool valid = j < s1;
+    float fsx = 0.f, fsy = 0.f;
+    if (valid) {
+      const Node s = nodes[j];
+      sx[threadIdx.x] = s.x;
+      sy[threadIdx.x] = s.y;
+      fsx = static_cast<float>(s.x - ox);
+      fsy = static_cast<float>(s.y - oy);
+      if (PDE == kLaplace) {
+        const double c = -s.w * KI_INV_2PI * x[j];
+        sa0[threadIdx.x] = c * s.nx;
+        sa1[threadIdx.x] = c * s.ny;
+        fa0[threadIdx.x] = static_cast<float>(c * dscale * s.nx);
+        fa1[threadIdx.x] = static_cast<float>(c * dscale * s.ny);
+      } else if (PDE == kLaplaceNeumann) {
+        sa0[threadIdx.x] = s.w * KI_INV_2PI * x[j];
+        fa0[threadIdx.x] = static_cast<float>(s.w * KI_INV_2PI * (x[j] * dscale));
+        if (tile.first) r1 += s.w * x[j];
+      } else {
+        const double c = s.w * KI_INV_PI;
+        sa0[threadIdx.x] = c * s.nx;
+        sa1[threadIdx.x] = c * s.ny;
+        fa0[threadIdx.x] = static_cast<float>(c * s.nx);
+        fa1[threadIdx.x] = static_cast<float>(c * s.ny);
+        const double d0 = x[2 * j], d1 = x[2 * j + 1];
+        sd0[threadIdx.x] = d0;
+        sd1[threadIdx.x] = d1;
+        fd0[threadIdx.x] = static_cast<float>(d0 * dscale);
+        fd1[threadIdx.x] = static_cast<float>(d1 * dscale);
+        if (tile.first) r1 += s.w * (s.nx * d0 + s.ny * d1);
+      }
+    } else {
+      // padding: a far source of zero strength
+      sx[threadIdx.x] = 1e15;
+      sy[threadIdx.x] = 1e15;
+      sa0[threadIdx.x] = sa1[threadIdx.x] = 0.0;
+      sd0[threadIdx.x] = sd1[threadIdx.x] = 0.0;
+      fsx = fsy = 1e15f;
+      fa0[threadIdx.x] = fa1[threadIdx.x] = 0.f;
+      fd0[threadIdx.x] = fd1[threadIdx.x] = 0.f;
+    }
+    fx[threadIdx.x] = fsx;
+    fy[threadIdx.x] = fsy;
+    warp_box(1, valid, fsx, fsy);
+    __syncthreads();
+    // gap between the boxes (0 when they overlap)
+    const float gx = fmaxf(0.f, fmaxf(cta_box(1, 0) + cta_box(0, 2), cta_box(0, 0) + cta_box(1, 2)));
+    const float gy = fmaxf(0.f, fmaxf(cta_box(1, 1) + cta_box(0, 3), cta_box(0, 1) + cta_box(1, 3)));
+    if (gx * gx + gy * gy < near2) {
+#pragma unroll 4
+      for (int q = 0; q < kMvThreads; q++) {
+        const double r0 = tx - sx[q], rr1 = ty - sy[q];
+        const double rr = r0 * r0 + rr1 * rr1;
+        const double inv = rr > 0.0 ? nr_rcp(rr) : 0.0;
+        if (PDE == kLaplace) {
+          y0 += (r0 * sa0[q] + rr1 * sa1[q]) * inv;
+        } else if (PDE == kLaplaceNeumann) {
+          y0 += ((r0 * tnx + rr1 * tny) * sa0[q]) * inv;
+        } else {
+          const double rn = r0 * sa0[q] + rr1 * sa1[q];
+          const double rx = r0 * sd0[q] + rr1 * sd1[q];
+          const double pq = (rn * rx) * (inv * inv);
+          y0 += pq * r0;
+          y1 += pq * rr1;
+        }
+      }
+    } else {
+      float f0 = 0.f, f1 = 0.f;
+#pragma unroll 8
+      for (int q = 0; q < kMvThreads; q++) {
+        const float r0 = ftx - fx[q], rr1 = fty - fy[q];
+        const float rr = fmaf(r0, r0, rr1 * rr1);
+        float inv;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(rr));
+        if (PDE == kLaplace) {
+          f0 = fmaf(fmaf(r0, fa0[q], rr1 * fa1[q]), inv, f0);
+        } else if (PDE == kLaplaceNeumann) {
+          f0 = fmaf(fmaf(r0, ftnx, rr1 * ftny) * fa0[q], inv, f0);
+        } else {
+          const float rn = fmaf(r0, fa0[q], rr1 * fa1[q]);
+          const float rx = fmaf(r0, fd0[q], rr1 * fd1[q]);
+          const float pq = (rn * rx) * (inv * inv);
+          f0 = fmaf(pq, r0, f0);
+          f1 = fmaf(pq, rr1, f1);
+        }
+      }
+      y0 += static_cast<double>(f0) * inv_scale;
+      y1 += static_cast<double>(f1) * inv_scale;
+    }
+  }
+  if (live) {
+    if (PDE == kStokes) {
+      part[part_stride * tile.split + 2 * t] = y0;
+      part[part_stride * tile.split + 2 * t + 1] = y1;
+    } else {
+      part[part_stride * tile.split + t] = y0;
+    }
+  }
+  if (PDE != kLaplace && tile.first) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+    if (lane == 0) red[warp] = r1;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double v = 0.0;
+      for (int w = 0; w < kMvThreads / 32; w++) v += red[w];
+      part_rank1[tile.rank1_slot] = v;
+    }
+  }
+}
+
 // y_i = sum of the splits' partials + diagonal correction + rank-one term +
 // U x_border; the border rows are done by mv_border_rows_kernel.
 __device__ __forceinline__ int segment_of(const int* __restrict__ seg, int nseg, int node) {
@@ -336,6 +523,30 @@ cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, 
   else
     mv_partial_kernel<kStokes><<<ntiles, kMvThreads, 0, s>>>(nodes, tiles, n_dofs, x, part,
                                                               part_rank1);
+  mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
+                                                        part_rank1, seg, nseg, x, y, nb, U);
+  if (nb) mv_border_rows_kernel<<<nb, 256, 0, s>>>(n_dofs, nb, Psi, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_corr_matvec(int pde, const Node* nodes, const MvTile* tiles, int ntiles,
+                               const int* seg, int nseg, int n_dofs, int splits, const double* x,
+                               double dscale, double near_gap, double* y, int nb,
+                               const double* U, const double* Psi, double* part,
+                               cudaStream_t s) {
+  if (splits < 1 || splits > kMaxMatvecSplits || !(dscale > 0.0)) return cudaErrorInvalidValue;
+  double* part_rank1 = part + static_cast<long long>(splits) * n_dofs;
+  const float near2 = static_cast<float>(near_gap * near_gap);
+  count_launches(nb ? 3 : 2);
+  if (pde == kLaplace)
+    mv_corr_partial_kernel<kLaplace><<<ntiles, kMvThreads, 0, s>>>(
+        nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
+  else if (pde == kLaplaceNeumann)
+    mv_corr_partial_kernel<kLaplaceNeumann><<<ntiles, kMvThreads, 0, s>>>(
+        nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
+  else
+    mv_corr_partial_kernel<kStokes><<<ntiles, kMvThreads, 0, s>>>(
+        nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
   mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
                                                         part_rank1, seg, nseg, x, y, nb, U);
   if (nb) mv_border_rows_kernel<<<nb, 256, 0, s>>>(n_dofs, nb, Psi, x, y);

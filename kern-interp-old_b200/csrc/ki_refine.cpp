@@ -105,6 +105,17 @@ int Solver::matvec_device(const double* d_x, double* d_y) {
   return 0;
 }
 
+int Solver::corr_matvec_device(const double* d_x, double* d_y, double dscale) {
+  if (mv_setup()) return -2;
+  const int nseg = static_cast<int>(seg_.size()) - 1;
+  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg);
+  if (kry_.bytes < sizeof(double) * need) KI_CUDA(kry_.reserve(sizeof(double) * need, stream_));
+  KI_CUDA(launch_corr_matvec(opt_.pde, d_nodes_, d_mv_tiles_, n_mv_tiles_, d_seg_, nseg, n_dofs_,
+                             mv_splits_, d_x, dscale, kCorrNearGap, d_y, nb_, d_U_, d_Psi_,
+                             static_cast<double*>(kry_.p), stream_));
+  return 0;
+}
+
 int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, double rel_tol,
                           int max_iters, int* iters_out, double* rel_res_out) {
   const int N = n_dofs_, nb = nb_, n = N + nb;
@@ -129,7 +140,7 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
   double* dh = part + dotp;  // [0, k) first pass, [kMax, kMax + k) second, [2 kMax] norm
   double* dseg = dh + 3 * kMaxKrylov;
   if (!h_kry_) {
-    h_kry_ = stage_.get<double>(3 * kMaxKrylov + nseg + 1);
+    h_kry_ = keep_stage_.get<double>(3 * kMaxKrylov + nseg + 1);
     if (!h_kry_) return fail("pinned allocation failed: refinement coefficients");
   }
   double* hh = h_kry_;
@@ -199,16 +210,23 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
   // Stationary refinement first: X = M^-1 B, then X += M^-1 (B - A X) while
   // each step shrinks the residual at least tenfold (one solve and one
   // operator product per step, no inner products).  If it stalls, GMRES
-  // continues from the current X and residual.
+  // continues from the current X and residual.  Once the residual r is
+  // small, a step's correction D = M^-1 r is small too and the residual is
+  // updated as r -= A D with the correction product: its relative error
+  // (~1e-6, see launch_corr_matvec) applies to |D| ~ |r|, not to |X|.
+  static const double corr_rel = [] {
+    const char* e = std::getenv("KI_CORR_REL");
+    return e ? std::atof(e) : kCorrRel;
+  }();
   double beta = 0.0;
   bool done = false;
   {
     if (solve_graph(B, X, nb ? X + N : nullptr, nb ? B + N : nullptr)) return -2;
     iters++;
+    if (matvec_device(X, W)) return -2;
+    KI_CUDA(launch_sub(V, B, W, n, stream_));
     double prev = 1.0;
     for (;;) {
-      if (matvec_device(X, W)) return -2;
-      KI_CUDA(launch_sub(V, B, W, n, stream_));
       if (residual(&beta, &rel)) return -2;
       if (rel <= rel_tol || iters >= max_iters || beta == 0.0) {
         done = true;
@@ -219,6 +237,14 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
       if (solve_graph(V, W, nb ? W + N : nullptr, nb ? V + N : nullptr)) return -2;
       KI_CUDA(launch_add(X, W, n, stream_));
       iters++;
+      if (rel <= corr_rel) {
+        // Z (unused until GMRES) receives A D
+        if (corr_matvec_device(W, Z, 1.0 / beta)) return -2;
+        KI_CUDA(launch_sub(V, V, Z, n, stream_));
+      } else {
+        if (matvec_device(X, W)) return -2;
+        KI_CUDA(launch_sub(V, B, W, n, stream_));
+      }
     }
   }
   bool have_r = true;  // V holds B - A X with norm beta

@@ -101,6 +101,7 @@ void* Arena::alloc(size_t bytes) {
   void* r = cur_;
   cur_ += bytes;
   left_ -= bytes;
+  used_ += bytes;
   return r;
 }
 
@@ -399,6 +400,7 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
   t_id_ms = t_decouple_ms = t_top_ms = 0;
   id_launches = 0;
   id_flops = id_bytes = id_onchip_flops = 0;
+  dec_flops = top_flops = solve_bytes = 0;
 
   if (!dstream_) {
     int dev = 0;
@@ -991,6 +993,13 @@ int Solver::decouple_boxes(PendingLevel* pl) {
     fac_total += static_cast<size_t>(k) * r * 2 + static_cast<size_t>(r) * r +
                  static_cast<size_t>(k) * k;
     piv_total += r;
+    {
+      const double dk = k, dr = r, dn = n;
+      // K_BN entries (~20 flops each), T^T K_ss, T^T K_sr, K_r_sn T, K_ss T,
+      // X_rr^-1 (Gauss-Jordan), U = X^-1 K_r_sn, L = K_sn_r X^-1, L K_r_sn
+      dec_flops += 20.0 * dn * dn + 2.0 * dr * dr * dr + 8.0 * dr * dr * dk + 6.0 * dr * dk * dk;
+      solve_bytes += 8.0 * (4.0 * dk * dr + dr * dr);
+    }
   }
   std::vector<int> bid(bid_off[ncomp], -1), bpos(bid_off[ncomp], 0);
   std::vector<UpdBlock> tab(tab_off[ncomp]);
@@ -1211,6 +1220,12 @@ int Solver::update(int n_points, const double* points, const double* normals,
   // nothing queued may still read the memory that is about to be replaced
   KI_CUDA(cudaStreamSynchronize(stream_));
   if (dstream_) KI_CUDA(cudaStreamSynchronize(dstream_));
+  {
+    // no queued copy reads the staging any more: its chunks go back to the
+    // pool and the refactorization stages into a fresh arena
+    Arena fresh(true);
+    fresh.swap(stage_);
+  }
   cudaEvent_t ev0;
   int rc = begin_factor(&ev0);
   if (rc) return rc;
@@ -1410,6 +1425,8 @@ int Solver::factor_top() {
   KI_UPLOAD(d_bpos, bpos, stream_);
   KI_UPLOAD(d_tab, tab, stream_);
   const int ntop = ns_ + nb_;
+  top_flops += 20.0 * ns_ * ns_ + 2.0 / 3.0 * static_cast<double>(ntop) * ntop * ntop;
+  solve_bytes += 8.0 * ntop * ntop + 8.0 * 8.0 * n_dofs_;
   KI_ALLOC(d_top_, double, static_cast<size_t>(ntop) * ntop);
   KI_ALLOC(d_top_piv_, int, ntop);
   KI_ALLOC(d_tmp_, double, 4 * static_cast<size_t>(n_dofs_ + ntop) + 64);

@@ -41,12 +41,14 @@ class Arena {
   template <class T>
   T* get(size_t count) { return static_cast<T*>(alloc(sizeof(T) * (count ? count : 1))); }
   size_t reserved() const { return reserved_; }
+  size_t used() const { return used_; }  // bytes handed out since construction
   void swap(Arena& o) {
     std::swap(pinned_, o.pinned_);
     chunks_.swap(o.chunks_);
     std::swap(cur_, o.cur_);
     std::swap(left_, o.left_);
     std::swap(reserved_, o.reserved_);
+    std::swap(used_, o.used_);
   }
 
  private:
@@ -55,6 +57,7 @@ class Arena {
   char* cur_ = nullptr;
   size_t left_ = 0;
   size_t reserved_ = 0;
+  size_t used_ = 0;
 };
 
 // Reusable device scratch that only grows.
@@ -123,6 +126,7 @@ class Solver {
   // previous problems'.  Call before factor(); no holes.
   void set_forest(const std::vector<int>& starts) { starts_ = starts; }
   int n_trees() const { return starts_.size() > 1 ? static_cast<int>(starts_.size()) - 1 : 1; }
+  size_t staging_bytes() const { return stage_.used() + keep_stage_.used(); }
   const std::vector<int>& starts() const { return starts_; }
 
   // QuadTree::initialize_tree + SkelFactorization::skeletonize.
@@ -141,6 +145,12 @@ class Solver {
   Solver* copy(cudaStream_t stream, int* rc);
   // QuadTree::initialize_tree only, active lists as before compression.
   void build_tree_only();
+  // Device copies of the boundary arrays only (no quadtree, no factors),
+  // for dense entry blocks; returns after the copies are done.
+  int prepare_geometry() {
+    const int rc = setup_geometry();
+    return rc ? rc : cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  }
   // The partition half of QuadTree::perturb on a tree-only solver.
   void perturb_tree_only(int n_points, const double* points);
   // linear_solve on device buffers: d_mu (dofs), d_alpha (border, may be
@@ -149,15 +159,27 @@ class Solver {
   // border rows [Psi -I][mu; alpha] = g; the reference always has g = 0.
   int solve_device(const double* d_b, double* d_mu, double* d_alpha,
                    const double* d_g = nullptr);
-  // FP64 GMRES on the (bordered) boundary operator, right-preconditioned by
-  // this factorization, entries of A formed on the fly: stops when
-  // ||[f; 0] - A [mu; alpha]|| <= rel_tol ||f|| (true residual) or after
-  // max_iters preconditioned products.  iters / rel_res report the work and
-  // the final true residual.
+  // FP64 refinement / GMRES on the (bordered) boundary operator,
+  // preconditioned by this factorization, entries of A formed on the fly:
+  // stops when ||[f; 0] - A [mu; alpha]|| <= rel_tol ||f|| or after
+  // max_iters preconditioned products.  The first residual is formed with
+  // the FP64 product; once the residual is below kCorrRel ||f||, a
+  // stationary step updates it as r -= A d with the correction product of
+  // its small correction d (corr_matvec_device), whose error is a tiny
+  // fraction of |d|.  iters / rel_res report the work and the final
+  // residual.
   int solve_refined(const double* d_f, double* d_mu, double* d_alpha, double rel_tol,
                     int max_iters, int* iters, double* rel_res);
   // Fast FP64 product y = A x (bordered), the refinement's residual operator.
   int matvec_device(const double* d_x, double* d_y);
+  // y = A d for a small correction d: far source blocks summed in FP32 with
+  // d scaled by dscale, near blocks in FP64 (launch_corr_matvec).
+  int corr_matvec_device(const double* d_x, double* d_y, double dscale);
+  // Residuals below this fraction of ||f|| are updated with the correction
+  // product (KI_CORR_REL overrides; 0 disables it).
+  static constexpr double kCorrRel = 1e-5;
+  // Bounding-box gap below which a source block is summed in FP64.
+  static constexpr double kCorrNearGap = 0.01;
   // x = A^-T b with the same factorization (simply connected domains):
   // the sweeps of solve_device transposed and run in reverse order.
   int solve_transpose_device(const double* d_b, double* d_x);
@@ -198,6 +220,11 @@ class Solver {
   int id_launches = 0;
   double id_flops = 0, id_bytes = 0;  // algorithmic FP64 flops / HBM bytes of all ID launches
   double id_onchip_flops = 0;         // the part of id_flops done by on-chip launches
+  // algorithmic FP64 flops of the decoupling launches (entries of K_BN, the
+  // products with T, X_rr^-1, L, U and the accumulated update) and of the
+  // top level (assembly + LU); FP64 factor bytes one solve reads (T twice,
+  // L, U, X_rr^-1, the top LU) plus its vector passes
+  double dec_flops = 0, top_flops = 0, solve_bytes = 0;
   bool time_phases = false;
   // Per-launch record of the timed factorization: kind 0 ID, 1 decouple,
   // 2 top-level assembly + LU; ms from CUDA events on the solver stream.
@@ -300,7 +327,11 @@ class Solver {
 
   bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
-  Arena stage_{true};  // pinned staging of every host-to-device upload
+  // pinned staging of every host-to-device upload and of the per-level rank
+  // readbacks; replaced by a fresh arena at each update() (after the
+  // streams are synchronised), so a long sequence of updates keeps it bounded
+  Arena stage_{true};
+  Arena keep_stage_{true};  // long-lived pinned buffers (refinement coefficients)
   template <class T>
   int upload(T* dst, const std::vector<T>& src, cudaStream_t s);
   Scratch work_, scratch2_;

@@ -70,6 +70,7 @@ def load():
                                        C.c_void_p]
     lib.ki_adjoint_backward.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8
     lib.ki_matvec_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ki_matvec_correction_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]
     lib.ki_solve_refined.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_int, _ip, _dp]
     lib.ki_solve_refined_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                             C.c_double, C.c_int, _ip, _dp]
@@ -88,6 +89,7 @@ def load():
     lib.ki_box_info.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _dp]
     lib.ki_box_lists.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _ip, _ip]
     lib.ki_allskel.argtypes = [C.c_void_p, _ip]
+    lib.ki_box_neighbors.argtypes = [C.c_void_p, C.c_int, C.c_int, _ip, _ip]
     lib.ki_stats.argtypes = [C.c_void_p, _dp, C.c_int]
     lib.ki_launch_log.argtypes = [C.c_void_p, _dp, C.c_int]
     lib.ki_timeline.argtypes = [C.c_void_p, _dp, C.c_int]
@@ -160,6 +162,17 @@ class _Tree:
                 "corner": (geom[0], geom[1]), "side": geom[2],
                 "original": lists[0], "active": lists[1], "skel": lists[2],
                 "redundant": lists[3], "tree": int(self.lib.ki_box_tree(self.h, level, idx))}
+
+    def neighbors(self, level, idx):
+        """(level, index) of each neighbour of box idx of `level`, in the
+        reference's neighbour-list order."""
+        n = self.lib.ki_box_neighbors(self.h, level, idx, None, None)
+        if n < 0:
+            _check(-n, "ki_box_neighbors")
+        lv = np.zeros(max(n, 1), dtype=np.int32)
+        ix = np.zeros(max(n, 1), dtype=np.int32)
+        self.lib.ki_box_neighbors(self.h, level, idx, _i(lv), _i(ix))
+        return list(zip(lv[:n].tolist(), ix[:n].tolist()))
 
     def all_nodes(self):
         return [[self.node(l, i) for i in range(self.nodes(l))]
@@ -298,6 +311,10 @@ class Solver(_Tree):
         _check(self.lib.ki_matvec_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)),
                "ki_matvec_device")
 
+    def matvec_correction_device(self, x_ptr, y_ptr, dscale=1.0):
+        _check(self.lib.ki_matvec_correction_device(self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                                    dscale), "ki_matvec_correction_device")
+
     def solve_refined(self, f, rel_tol=1e-12, max_iters=20):
         """FP64 GMRES refinement preconditioned by this factorization.
         Returns (mu, alpha, iterations, final true relative residual)."""
@@ -373,15 +390,17 @@ class Solver(_Tree):
         return out
 
     def stats(self):
-        out = np.zeros(13)
-        self.lib.ki_stats(self.h, _d(out), 13)
+        out = np.zeros(17)
+        self.lib.ki_stats(self.h, _d(out), 17)
         return {"factor_ms": float(out[0]), "id_ms": float(out[1]),
                 "id_launches": int(out[2]), "id_flops": float(out[3]),
                 "id_bytes": float(out[4]), "decouple_ms": float(out[5]),
                 "top_ms": float(out[6]), "wait_ms": float(out[7]),
                 "host_prep_ms": float(out[8]), "host_post_ms": float(out[9]),
                 "upload_ms": float(out[10]), "host_top_ms": float(out[11]),
-                "id_onchip_flops": float(out[12])}
+                "id_onchip_flops": float(out[12]), "staging_bytes": float(out[13]),
+                "dec_flops": float(out[14]), "top_flops": float(out[15]),
+                "solve_bytes": float(out[16])}
 
     def timeline(self):
         n = self.lib.ki_timeline(self.h, None, 0)

@@ -51,6 +51,31 @@ def test_fast_matvec_matches_entry_exact_product(name):
     assert np.linalg.norm(a - b) / np.linalg.norm(a) < 1e-13
 
 
+@pytest.mark.parametrize("name", list(_problems()) + ["star_laplace_16384", "stokes_holes_65536"])
+def test_correction_product_error(name):
+    """The FP32 far-field / FP64 near-field product of a correction: within
+    2e-6 of the FP64 product relative to |y|, for any scaling of the
+    density (the FP32 stage sees d * dscale), on vectors of magnitude 1e-9
+    like the late corrections of a refinement."""
+    import torch
+    pr = {"star_laplace_16384": lambda: G.star_case(),
+          "stokes_holes_65536": lambda: G.stokes_holes_case()}.get(name, lambda: _problems()[name])()
+    s = kinterp.Solver(pr, id_tol=1e-6, mode=1)
+    rng = np.random.default_rng(11)
+    x = _dev(1e-9 * rng.standard_normal(s.n_dofs + s.n_border))
+    y0 = torch.empty_like(x)
+    y1 = torch.empty_like(x)
+    s.matvec_device(x.data_ptr(), y0.data_ptr())
+    errs = []
+    for scale in (1e9, 1e7):
+        s.matvec_correction_device(x.data_ptr(), y1.data_ptr(), scale)
+        torch.cuda.synchronize()
+        a, b = y0.cpu().numpy(), y1.cpu().numpy()
+        errs.append(np.linalg.norm(a - b) / np.linalg.norm(a))
+    assert max(errs) < 2e-6, errs
+    s.close()
+
+
 def test_fast_matvec_laplace_neumann():
     import torch
     pr = G.ellipse_case(n=1024)
@@ -109,6 +134,31 @@ def test_refined_loose_factor_reaches_fp64(name, mode):
         assert np.abs(alpha - at).max() < 1e-10 * max(1.0, np.abs(mt).max())
     own = H.rel(mo, mt)
     assert H.rel(mu, mo) < max(1e-10, 2.0 * own)
+
+
+@pytest.mark.parametrize("name,tol", [("star_laplace_16384", 3e-7),
+                                      ("stokes_holes_65536", 3e-8),
+                                      ("stokes_holes_4096", 1e-6)])
+def test_refined_true_residual(name, tol):
+    """The refinement updates small residuals with the correction product:
+    the residual it reports must agree with the true FP64 residual
+    ||[f; 0] - A [mu; alpha]|| / ||f|| of the solution it returns, which must
+    meet the 1e-12 bar."""
+    import torch
+    pr = {"star_laplace_16384": lambda: G.star_case(),
+          "stokes_holes_65536": lambda: G.stokes_holes_case()}.get(name, lambda: _problems()[name])()
+    s = kinterp.Solver(pr, id_tol=tol, mode=1)
+    mu, alpha, it, rr = s.solve_refined(pr.f, rel_tol=1e-12, max_iters=30)
+    assert rr <= 1e-12, (it, rr)
+    x = _dev(np.concatenate([mu, alpha]))
+    y = torch.empty_like(x)
+    s.matvec_device(x.data_ptr(), y.data_ptr())
+    torch.cuda.synchronize()
+    b = np.concatenate([pr.f, np.zeros(len(alpha))])
+    true = np.linalg.norm(b - y.cpu().numpy()) / np.linalg.norm(pr.f)
+    assert true <= 1.5e-12, (true, rr, it)
+    assert abs(true - rr) <= 0.5e-12 + 0.5 * rr, (true, rr)
+    s.close()
 
 
 def test_refined_matches_dense_solve():

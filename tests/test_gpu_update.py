@@ -152,3 +152,20 @@ def test_copy_of_an_updated_handle():
     c = s.copy()
     assert H.compare_solvers(s, c)["rank"] == 0
     assert np.linalg.norm(c.solve(new.f)[0] - s.solve(new.f)[0]) <= 1e-15
+
+
+def test_many_updates_keep_pinned_staging_bounded():
+    """A shape-optimisation loop calls ki_update many times: the pinned
+    staging a handle uses must not grow with the number of updates (each
+    update stages only its own refactorization)."""
+    base = G.star_case(n=8192, n_targets=16)
+    s = kinterp.Solver(base, id_tol=1e-8)
+    held = []
+    for k in range(16):
+        fr = G.bumped_star_case(n=8192, n_targets=16, center=0.5 + 0.3 * k, amp=0.03,
+                                width=0.1, extra=(-1) ** k * 20)
+        s.update(fr)
+        s.solve_refined(fr.f, rel_tol=1e-12)
+        held.append(s.stats()["staging_bytes"])
+    assert max(held) <= 1.5 * min(held), held
+    s.close()

@@ -31,17 +31,19 @@ def _nodes(pr):
     return rec.ravel()
 
 
-def _call(lib, pr, d_nodes, act, rows, tol, torch):
+def _call(lib, pr, d_nodes, act, rows, tol, torch, circle=None):
     d_act = torch.tensor(act, dtype=torch.int32, device="cuda")
     d_rows = torch.tensor(rows, dtype=torch.int32, device="cuda")
     n = len(act)
     d_rank = torch.full((1,), -1, dtype=torch.int32, device="cuda")
     d_perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
     d_T = torch.zeros(n * n // 4 + 1, dtype=torch.float64, device="cuda")
+    cx, cy, rad = circle if circle is not None else (0.0, 0.0, 0.0)
     torch.cuda.synchronize()
     rc = lib.ki_id_noalloc(pr.pde, C.c_void_p(d_nodes.data_ptr()), pr.n_points,
                            C.c_void_p(d_act.data_ptr()), n, C.c_void_p(d_rows.data_ptr()),
-                           len(rows), 0, C.c_double(0.0), C.c_double(0.0), C.c_double(0.0),
+                           len(rows), 1 if circle is not None else 0, C.c_double(cx),
+                           C.c_double(cy), C.c_double(rad),
                            C.c_double(tol), C.c_void_p(d_rank.data_ptr()),
                            C.c_void_p(d_perm.data_ptr()), C.c_void_p(d_T.data_ptr()), None)
     assert rc == 0, lib.ki_last_error()
@@ -79,6 +81,67 @@ def test_noalloc_id_matches_factor_on_two_calls():
         calls += 1
         if calls == 2:
             break
+    assert calls == 2
+
+
+def _proxy_rows(s, pr, level, idx, box):
+    """The ID rows ki_factor uses for a box of level >= 3 (kernel.cpp:209-218):
+    the dofs of its neighbours at this level or coarser (a leaf's original
+    dofs, otherwise its active dofs) whose node lies inside the proxy circle
+    of radius 1.5 side about the box centre, in neighbour-list order; and the
+    circle (centre x, centre y, radius)."""
+    side = box["side"]
+    cx, cy = box["corner"][0] + side / 2.0, box["corner"][1] + side / 2.0
+    R = 1.5 * side
+    rows = []
+    for ol, oi in s.neighbors(level, idx):
+        if ol > level:
+            continue
+        o = s.node(ol, oi)
+        for dof in (o["original"] if o["is_leaf"] else o["active"]):
+            pt = dof // pr.sol_dim
+            dx, dy = cx - pr.points[2 * pt], cy - pr.points[2 * pt + 1]
+            if np.sqrt(dx * dx + dy * dy) < R:
+                rows.append(dof)
+    return np.array(rows, dtype=np.int32), (cx, cy, R)
+
+
+@pytest.mark.parametrize("kind", ["laplace", "stokes"])
+def test_noalloc_id_with_proxy_rows_matches_factor(kind):
+    """Boxes of level >= 3 take the proxy-circle rows (256 for Laplace, 512
+    for Stokes) besides their near rows: two such calls in a row must give
+    ki_factor's rank and skeleton for the box, and a T that reproduces the
+    redundant columns of the near-row block."""
+    import torch
+    lib = kinterp.load()
+    lib.ki_id_noalloc.restype = C.c_int
+    if kind == "laplace":
+        pr = G.star_case(n=4096, n_targets=16)
+    else:
+        pr = G.stokes_holes_case(n_total=4096, n_targets=16)
+    s = kinterp.Solver(pr)
+    d_nodes = torch.tensor(_nodes(pr), device="cuda", dtype=torch.float64)
+    calls = 0
+    for level in range(3, s.levels()):
+        for idx in range(s.nodes(level)):
+            box = s.node(level, idx)
+            if not box["compressed"] or len(box["active"]) < 24:
+                continue
+            act = box["active"]
+            rows, circle = _proxy_rows(s, pr, level, idx, box)
+            if len(rows) == 0:
+                continue
+            k, perm, Tflat = _call(lib, pr, d_nodes, act, rows, pr.id_tol, torch, circle)
+            assert k == len(box["skel"]), (level, idx)
+            assert np.array_equal(np.sort(act[perm[:k]]), np.sort(box["skel"])), (level, idx)
+            assert np.array_equal(np.sort(act[perm[k:]]), np.sort(box["redundant"]))
+            A = np.vstack([s.kernel_block(rows, act), s.kernel_block(act, rows).T])
+            T = Tflat[:k * (len(act) - k)].reshape(len(act) - k, k).T
+            resid = A[:, perm[k:]] - A[:, perm[:k]] @ T
+            assert np.linalg.norm(resid) <= 1e3 * pr.id_tol * np.linalg.norm(A)
+            calls += 1
+            if calls == 2:
+                return
     assert calls == 2
 
 
