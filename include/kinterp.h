@@ -57,7 +57,7 @@ void ki_release_cache(void);
 
 /* Builds the quadtree and skeletonizes the boundary operator.
  * Replaces QuadTree::initialize_tree (quadtree/quadtree.h:85-86), the U/Psi
- * set-up of boundary_integral_solve (linear_solve.cpp:194-203) and
+ * set-up of boundary_integral_solve (linear_solve.cpp:155-163) and
  * SkelFactorization(id_tol, threads).skeletonize (skel_factorization/
  * skel_factorization.h:25,40).  max_leaf_dofs is the reference's
  * MAX_LEAF_DOFS (quadtree.h:10; 32 there). */
@@ -189,6 +189,16 @@ int ki_domain_mask_device(ki_solver_t s, int n_targets, const double* d_targets,
 int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, double y_max,
                      double* points);
 
+/* Test hook for the failure path (no reference counterpart; the reference
+ * has no bounded waits).  KI_INJECT_LU_ABORT: the next top-level LU done
+ * by the cooperative launch (33 to 768 rows) starts with its abort word
+ * raised; KI_INJECT_LU_STALL: its first block
+ * keeps its flag down, so the other blocks' bounded waits (200 ms) run out.
+ * Either way that factorization returns KI_ERR_NUMERIC ("a bounded wait
+ * timed out") and the device stays usable.  One-shot, process-wide;
+ * KI_INJECT_NONE clears it. */
+enum { KI_INJECT_NONE = 0, KI_INJECT_LU_ABORT = 1, KI_INJECT_LU_STALL = 2 };
+int ki_test_inject_fault(int what);
 /* A handle holding device copies of the boundary arrays only, without a
  * quadtree or factors: the Kernel object of the reference (kernel.h:15-41,
  * its boundary copies) for dense entry blocks (ki_kernel_block,

@@ -118,7 +118,8 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
 
 // In-place LU with partial pivoting (dgetf2) of an n x n matrix over the
 // CTA.  ipiv[j] = row exchanged with row j.  `red` needs 2 * 32 doubles.
-// Returns nonzero if an exactly zero pivot was met (LAPACK's info > 0).
+// Returns nonzero if an exactly zero or infinite pivot was met, or a column
+// held no comparable entry (NaN).
 __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nw = blockDim.x >> 5;
@@ -180,6 +181,7 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
       const double inv = 1.0 / piv;
       for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x)
         a[i + static_cast<long long>(ld) * j] *= inv;
+      if (isinf(piv)) info = 1;
     } else {
       info = 1;
     }
@@ -261,7 +263,7 @@ __device__ inline int cta_gj_invert(double* a, int n, int ld, int* ipiv, double*
       }
     __syncthreads();
     const double piv = a[j + static_cast<long long>(ld) * j];
-    if (piv == 0.0) {
+    if (piv == 0.0 || isinf(piv)) {
       info = 1;
       continue;
     }
@@ -311,7 +313,8 @@ __device__ inline void warp_lu_solve(const double* lu, int n, int ld, const int*
   if (lane == 0)
     for (int i = 0; i < n; i++) {
       const int p = ipiv[i];
-      if (p != i) {
+      // (a pivot out of range, left by an LU that stopped early, is skipped)
+      if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
         const double t = b[static_cast<long long>(inc) * i];
         b[static_cast<long long>(inc) * i] = b[static_cast<long long>(inc) * p];
         b[static_cast<long long>(inc) * p] = t;
@@ -364,7 +367,8 @@ __device__ inline void warp_lu_solve_t(const double* lu, int n, int ld, const in
   if (lane == 0)
     for (int i = n - 1; i >= 0; i--) {
       const int p = ipiv[i];
-      if (p != i) {
+      // (a pivot out of range, left by an LU that stopped early, is skipped)
+      if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
         const double t = b[static_cast<long long>(inc) * i];
         b[static_cast<long long>(inc) * i] = b[static_cast<long long>(inc) * p];
         b[static_cast<long long>(inc) * p] = t;
@@ -384,7 +388,8 @@ __device__ inline void cta_lu_solve(const double* __restrict__ lu, int n, int ld
   if (threadIdx.x == 0)
     for (int i = 0; i < n; i++) {
       const int p = ipiv[i];
-      if (p != i) {
+      // (a pivot out of range, left by an LU that stopped early, is skipped)
+      if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
         const double t = x[i];
         x[i] = x[p];
         x[p] = t;

@@ -2,6 +2,7 @@
 // include/kinterp.h).
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -88,6 +89,21 @@ bool box_ref(ki_solver_t s, int level, int idx, const kib::Box** out, int* paren
   return true;
 }
 
+// Every value finite (NaN and infinities fail): boundary data with a
+// non-finite value would only surface as NaN factors.
+bool all_finite(const double* a, size_t n) {
+  bool ok = true;
+  for (size_t i = 0; i < n; i++) ok &= std::isfinite(a[i]);
+  return ok;
+}
+
+bool geometry_finite(int n_points, const double* points, const double* normals,
+                     const double* curvatures, const double* weights) {
+  const size_t n = static_cast<size_t>(n_points);
+  return all_finite(points, 2 * n) && all_finite(normals, 2 * n) && all_finite(curvatures, n) &&
+         all_finite(weights, n);
+}
+
 int factor_impl(int pde, int n_points, const double* points, const double* normals,
                 const double* curvatures, const double* weights, int n_holes,
                 const double* holes, int max_leaf_dofs, double id_tol, void* stream,
@@ -100,6 +116,9 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
     return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
   if (n_holes < 0 || (n_holes > 0 && !holes)) return set_err(KI_ERR_ARG, "ki_factor: bad holes");
   if (max_leaf_dofs < 1) return set_err(KI_ERR_ARG, "ki_factor: max_leaf_dofs must be >= 1");
+  if (!geometry_finite(n_points, points, normals, curvatures, weights) ||
+      (n_holes > 0 && !all_finite(holes, 4 * static_cast<size_t>(n_holes))))
+    return set_err(KI_ERR_ARG, "ki_factor: non-finite boundary data (NaN or infinity)");
   if (!(id_tol > 0)) return set_err(KI_ERR_ARG, "id_tol must be greater than 0");
   if (mode != KI_MODE_REFERENCE && mode != KI_MODE_PRECONDITIONER)
     return set_err(KI_ERR_ARG, "ki_factor: bad mode");
@@ -272,6 +291,9 @@ int ki_update(ki_solver_t s, int n_points, const double* points, const double* n
   if (n_points <= 0 || !points || !normals || !curvatures || !weights)
     return set_err(KI_ERR_ARG, "number of boundary points to init tree cannot be 0");
   if (n_holes < 0 || (n_holes > 0 && !holes)) return set_err(KI_ERR_ARG, "ki_update: bad holes");
+  if (!geometry_finite(n_points, points, normals, curvatures, weights) ||
+      (n_holes > 0 && !all_finite(holes, 4 * static_cast<size_t>(n_holes))))
+    return set_err(KI_ERR_ARG, "ki_update: non-finite boundary data (NaN or infinity)");
   if (s->solver->n_trees() > 1)
     return set_err(KI_ERR_ARG, "ki_update: not available for a batch of problems");
   return from_solver(s, s->solver->update(n_points, points, normals, curvatures, weights,
@@ -573,6 +595,13 @@ int ki_domain_points(int domain_size, double x_min, double x_max, double y_min, 
   return KI_OK;
 }
 
+int ki_test_inject_fault(int what) {
+  if (what < KI_INJECT_NONE || what > KI_INJECT_LU_STALL)
+    return set_err(KI_ERR_ARG, "ki_test_inject_fault: unknown fault");
+  kib::inject_lu_fault(what);
+  return KI_OK;
+}
+
 int ki_geometry(int pde, int n_points, const double* points, const double* normals,
                 const double* curvatures, const double* weights, void* stream,
                 ki_solver_t* out) {
@@ -581,6 +610,8 @@ int ki_geometry(int pde, int n_points, const double* points, const double* norma
   if (pde < KI_LAPLACE || pde > KI_STOKES) return set_err(KI_ERR_ARG, "ki_geometry: bad pde");
   if (n_points <= 0 || !points || !normals || !curvatures || !weights)
     return set_err(KI_ERR_ARG, "ki_geometry: no boundary points");
+  if (!geometry_finite(n_points, points, normals, curvatures, weights))
+    return set_err(KI_ERR_ARG, "ki_geometry: non-finite boundary data (NaN or infinity)");
   int dev_count = 0;
   if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
     return set_err(KI_ERR_CUDA, "no CUDA device available");

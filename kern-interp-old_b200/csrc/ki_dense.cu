@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(1024) panel_lu_kernel(double* a, int n, int ld
     __syncthreads();
     const int p = sp;
     const double piv = a[p + static_cast<long long>(ld) * j];
-    if (piv != 0.0) {
+    if (piv != 0.0 && !isinf(piv)) {
       if (p != j && threadIdx.x < w) {
         double* x = a + static_cast<long long>(ld) * (j0 + threadIdx.x);
         const double t = x[j];
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kRegThreads) panel_lu_reg_kernel(double* a, in
     const double piv = rowP[jj];
     if (threadIdx.x == 0) {
       ipiv[j0 + jj] = j0 + p;
-      if (piv == 0.0 || bad) atomicExch(status, 1);
+      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
     }
     const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
 #pragma unroll
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kFastThreads) panel_lu_fast_kernel(double* a, 
     const double piv = col[p];
     if (threadIdx.x == 0) {
       ipiv[j0 + jj] = j0 + p;
-      if (piv == 0.0 || bad) atomicExch(status, 1);
+      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
     }
     const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
     // finished columns < jj (nobody reads them in this step): the previous
@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(1024) panel_lu_smem_kernel(double* a, int n, i
     }
     __syncthreads();
     const double piv = col[jj];
-    if (piv == 0.0) {
+    if (piv == 0.0 || isinf(piv)) {
       if (threadIdx.x == 0) atomicExch(status, 1);
     } else {
       const double inv = 1.0 / piv;
@@ -846,8 +846,10 @@ __device__ __forceinline__ void fused_swaps(double* blk, int np, int n, int j0, 
   }
 }
 
+// hold (a test hook, normally 0): thread block 0 keeps its flag down, so the
+// other blocks' bounded waits run out and the launch ends with status 2.
 __global__ void __launch_bounds__(kFusedThreads, 1)
-    lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync) {
+    lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync, int hold) {
   extern __shared__ double blk[];  // np x kNb, column-major
   __shared__ double l11[kNb][kNb + 1];
   __shared__ unsigned long long redk[kFusedThreads / 32];
@@ -958,7 +960,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     const double piv = blk[col + np * jj];
     if (tid == 0) {
       ipiv[col] = p;
-      if (piv == 0.0 || bad) atomicExch(status, 1);
+      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
     }
     const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
     for (int i = tid; i < n; i += kFusedThreads) {
@@ -980,7 +982,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
   }
   __syncthreads();
-  if (tid == 0) {
+  if (tid == 0 && !(hold && b == 0)) {
     __threadfence();
     st_release_gpu(sync + b, 1);
   }
@@ -1005,8 +1007,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 }
 }  // namespace
 
+namespace {
+std::atomic<int> g_lu_inject{0};
+}  // namespace
+
+void inject_lu_fault(int mode) { g_lu_inject.store(mode); }
+
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s,
-                     int* sync) {
+                     int* sync, bool top_level) {
   if (sync && n > 0 && n <= kLuFusedMaxN) {
     int G = (n + kNb - 1) / kNb;
     const size_t smem = sizeof(double) * static_cast<size_t>(n | 1) * kNb;
@@ -1015,7 +1023,16 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
                                     static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(sync, 0, sizeof(int) * (G + 1), s)) != cudaSuccess) return e;
-    void* args[] = {&a, &n, &ld, &ipiv, &status, &sync};
+    // test hook (inject_lu_fault): the abort word raised before the start,
+    // or block 0's flag held down; one top-level launch of more than one block
+    int hold = 0;
+    if (top_level && G > 1 && g_lu_inject.load() != 0) {
+      const int mode = g_lu_inject.exchange(0);
+      if (mode == 1 && (e = cudaMemsetAsync(sync + G, 0x7f, sizeof(int), s)) != cudaSuccess)
+        return e;
+      hold = mode == 2 ? 1 : 0;
+    }
+    void* args[] = {&a, &n, &ld, &ipiv, &status, &sync, &hold};
     count_launches(1);
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&lu_fused_kernel),
                                        dim3(G), dim3(kFusedThreads), args, smem, s);

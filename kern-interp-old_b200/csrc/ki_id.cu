@@ -273,7 +273,9 @@ __global__ void __launch_bounds__(kIdThreads, 1) id_kernel(IdParams P) {
       bp = wbest[lane].pos;
     }
     warp_best(bv, bp);
-    const int pvt = bp;
+    // no comparable candidate (every remaining norm NaN, from non-finite
+    // entries): keep column i in place rather than index past the columns
+    const int pvt = bp >= i && bp < n ? bp : i;
     const int ci = pos2col[i];
     const int cp = pos2col[pvt];
     __syncwarp();
@@ -556,7 +558,9 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
       bp = wbest[lane].pos;
     }
     warp_best(bv, bp);
-    const int pvt = bp;
+    // no comparable candidate (every remaining norm NaN, from non-finite
+    // entries): keep column i in place rather than index past the columns
+    const int pvt = bp >= i && bp < n ? bp : i;
     const int ci = pos2col[i];
     const int cp = pos2col[pvt];
     __syncwarp();

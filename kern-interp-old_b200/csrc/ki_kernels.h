@@ -174,7 +174,13 @@ cudaError_t launch_forest_top_solve(const TopTask* tasks, int ntasks, int n_max,
 constexpr int kLuFusedMaxN = 768;
 constexpr int kLuSyncInts = kLuFusedMaxN / 32 + 8;
 cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStream_t s,
-                     int* sync = nullptr);
+                     int* sync = nullptr, bool top_level = false);
+// Test hook for the failure path of the cooperative LU: the next top-level
+// launch (dense_lu with top_level) of more than one thread block starts with
+// its abort word raised (mode 1) or with block 0's flag held down so that
+// the other blocks' bounded waits run out (mode 2); either way it ends with
+// *status = 2.  0 clears it.
+void inject_lu_fault(int mode);
 // Multi-CTA tiled C = C0 - op(A) op(B) (64 x 64 tiles); C0 may be null.
 cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, const double* A,
                             int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,

@@ -1440,7 +1440,8 @@ int Solver::factor_top() {
   if (time_phases && timer_begin(&l0)) return -2;
   int* lu_sync;
   KI_ALLOC(lu_sync, int, kLuSyncInts);
-  if (ntop > 0) KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_, lu_sync));
+  if (ntop > 0)
+    KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_, lu_sync, true));
   if (time_phases && timer_end(l0, {0, 4, 1, 1, 0, ntop, 0.0})) return -2;
   return 0;
 }

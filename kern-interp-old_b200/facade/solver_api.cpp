@@ -314,6 +314,11 @@ void SkelFactorization::skeletonize(const Kernel& K, QuadTree* tree) {
   const bool border = tree->U.width() > 0 && K.pde != Kernel::LAPLACE_NEUMANN;
   const std::vector<double> holes = border ? holes_array(st.holes) : std::vector<double>();
   const int nh = static_cast<int>(holes.size() / 4);
+  if (st.factored && !st.perturbed) {
+    // every box is compressed already: the reference's skeletonize skips
+    // compressed boxes and redoes only the top level, which is the same
+    return;
+  }
   if (st.factored && st.perturbed) {
     int kept = 0;
     check(ki_update(st.h, n, K.boundary_points.data(), K.boundary_normals.data(),
