@@ -34,12 +34,26 @@ __device__ inline void cta_gemm_sub(double* C, int ldc, const double* C0, int ld
   }
 }
 
-// Tiled CTA GEMM: C (m x n) = C0 + alpha op(A) op(B) (alpha = -1 unless
-// given), op(A) m x kk, op(B) kk x n, 64 x 64 output tiles with a 4 x 4 block
-// per thread (256 threads), inner dimension staged 16 at a time in `tile`
-// (2 * 16 * 65 doubles).  C0 may be null (taken as zero) or alias C; C must
-// not alias A or B.  Operands may live in shared or global memory.  Ends
-// with a barrier.
+// One FP64 tensor-core step (DMMA, mma.sync m8n8k4 .f64): the warp's 8 x 8
+// block C += A (8 x 4) B (4 x 8).  Fragments: lane l holds A(l / 4, l % 4),
+// B(l % 4, l / 4) and C(l / 4, 2 (l % 4) + v), v = 0, 1.
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
+               : "=d"(c0), "=d"(c1)
+               : "d"(a), "d"(b), "d"(c0), "d"(c1));
+}
+
+// Tiled CTA GEMM on the FP64 tensor cores: C (m x n) = C0 + alpha op(A)
+// op(B) (alpha = -1 unless given), op(A) m x kk, op(B) kk x n, 64 x 64
+// output tiles, the inner dimension staged 16 at a time in `tile` (2 * 16 *
+// 65 doubles, zero-padded past the matrix edges).  The 8 warps of the
+// (256-thread) CTA are laid out 2 x 4 over a tile: each warp owns a 32 x 16
+// block, i.e. 4 x 2 DMMA blocks of 8 x 8 with their accumulators in
+// registers, and takes 6 fragment loads from shared memory per 8 DMMAs
+// (2048 FMAs), where a 4 x 4 register tile per thread needs a load per two
+// FMAs, more than shared memory delivers at the FP64 rate.  C0 may be null
+// (taken as zero) or alias C; C must not alias A or B.  Operands may live in
+// shared or global memory.  Ends with a barrier.
 constexpr int kGemmTileDoubles = 2 * 16 * 65;
 
 __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int ldc0,
@@ -48,14 +62,16 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
                                       double alpha = -1.0) {
   double* sa = tile;            // [16][65]: sa[l * 65 + i] = op(A)(i0 + i, l0 + l)
   double* sb = tile + 16 * 65;  // [16][65]: sb[l * 65 + j] = op(B)(l0 + l, j0 + j)
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;  // this warp's block in the tile
+  const int fr = lane >> 2, fk = lane & 3;                 // fragment row / inner index
   for (int i0 = 0; i0 < m; i0 += 64) {
     for (int j0 = 0; j0 < n; j0 += 64) {
-      double acc[4][4];
+      double acc[4][2][2];
 #pragma unroll
       for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+        for (int b = 0; b < 2; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
       for (int l0 = 0; l0 < kk; l0 += 16) {
         for (int e = threadIdx.x; e < 16 * 64; e += 256) {
           // A: element (row i0 + q, inner l0 + l); B: (inner l0 + l, col j0 + q)
@@ -88,29 +104,32 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
         }
         __syncthreads();
 #pragma unroll
-        for (int l = 0; l < 16; l++) {
-          double av[4], bv[4];
+        for (int ks = 0; ks < 4; ks++) {
+          const int lrow = (ks * 4 + fk) * 65;
+          double af[4], bf[2];
 #pragma unroll
-          for (int a = 0; a < 4; a++) av[a] = sa[l * 65 + tx + 16 * a];
+          for (int a = 0; a < 4; a++) af[a] = sa[lrow + wm + 8 * a + fr];
 #pragma unroll
-          for (int b = 0; b < 4; b++) bv[b] = sb[l * 65 + ty + 16 * b];
+          for (int b = 0; b < 2; b++) bf[b] = sb[lrow + wn + 8 * b + fr];
 #pragma unroll
           for (int a = 0; a < 4; a++)
 #pragma unroll
-            for (int b = 0; b < 4; b++) acc[a][b] += av[a] * bv[b];
+            for (int b = 0; b < 2; b++) dmma_8x8x4(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
         }
         __syncthreads();
       }
 #pragma unroll
       for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int gi = i0 + tx + 16 * a, gj = j0 + ty + 16 * b;
-          if (gi < m && gj < n) {
-            const double c0 = C0 ? C0[gi + static_cast<long long>(ldc0) * gj] : 0.0;
-            C[gi + static_cast<long long>(ldc) * gj] = c0 + alpha * acc[a][b];
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            const int gi = i0 + wm + 8 * a + fr, gj = j0 + wn + 8 * b + 2 * fk + v;
+            if (gi < m && gj < n) {
+              const double c0 = C0 ? C0[gi + static_cast<long long>(ldc0) * gj] : 0.0;
+              C[gi + static_cast<long long>(ldc) * gj] = c0 + alpha * acc[a][b][v];
+            }
           }
-        }
     }
   }
   __syncthreads();

@@ -170,8 +170,12 @@ cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* s
   if ((e = dense_lu_solve(tk.X, r, r, tk.piv, Y, r, r, s))) return e;
   if ((e = cudaMemcpyAsync(tk.X, Y, sizeof(double) * r * r, cudaMemcpyDeviceToDevice, s))) return e;
   // U = X^{-1} K_r_sn, L = K_sn_r X^{-1}, acc = update + L K_r_sn
-  if ((e = small_gemm(false, false, r, k, r, 1.0, tk.X, r, Krsn, r, 0.0, tk.U, r, s))) return e;
-  if ((e = small_gemm(false, false, k, r, r, 1.0, Ksnr, k, tk.X, r, 0.0, tk.L, k, s))) return e;
+  if ((e = launch_gemm_tiled(tk.U, r, nullptr, 0, tk.X, r, false, Krsn, r, false, r, k, r, 1.0,
+                             s)))
+    return e;
+  if ((e = launch_gemm_tiled(tk.L, k, nullptr, 0, Ksnr, k, false, tk.X, r, false, k, r, r, 1.0,
+                             s)))
+    return e;
   if ((e = launch_gemm_sub(tk.acc, k, nullptr, 0, tk.L, k, false, Krsn, r, false, k, k, r, s)))
     return e;
   acc_finish_kernel<<<(k * k + 255) / 256, 256, 0, s>>>(tk.acc, k, tk.perm, tk.bid, tk.bpos,

@@ -579,7 +579,9 @@ __global__ void __launch_bounds__(kSwapThreads) swap_trsm_kernel(double* a, int 
     if (i < w) x[i] = b[i];
 }
 
-// A22 -= A21 A12 for the trailing block, 64 x 64 tiles, inner dimension w.
+// A22 -= A21 A12 for the trailing block, 64 x 64 tiles, inner dimension w,
+// on the FP64 tensor cores: 8 warps laid out 2 x 4, a warp's 32 x 16 block
+// as 4 x 2 DMMA blocks (dmma_8x8x4 fragment layout).
 __global__ void __launch_bounds__(256) trailing_kernel(double* a, int n, int ld, int j0, int w) {
   __shared__ double sa[kNb][64 + 1];
   __shared__ double sb[kNb][64 + 1];
@@ -592,28 +594,32 @@ __global__ void __launch_bounds__(256) trailing_kernel(double* a, int n, int ld,
     sb[l][i] = (gc < n && l < w) ? a[j0 + l + static_cast<long long>(ld) * gc] : 0.0;
   }
   __syncthreads();
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4] = {};
-#pragma unroll 4
-  for (int l = 0; l < kNb; l++) {
-    double av[4], bv[4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const int fr = lane >> 2, fk = lane & 3;
+  double acc[4][2][2] = {};
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      av[q] = sa[l][tx + 16 * q];
-      bv[q] = sb[l][ty + 16 * q];
-    }
+  for (int ks = 0; ks < kNb / 4; ks++) {
+    if (4 * ks >= w) break;
+    double af[4], bf[2];
+#pragma unroll
+    for (int q = 0; q < 4; q++) af[q] = sa[4 * ks + fk][wm + 8 * q + fr];
+#pragma unroll
+    for (int t = 0; t < 2; t++) bf[t] = sb[4 * ks + fk][wn + 8 * t + fr];
 #pragma unroll
     for (int q = 0; q < 4; q++)
 #pragma unroll
-      for (int t = 0; t < 4; t++) acc[q][t] += av[q] * bv[t];
+      for (int t = 0; t < 2; t++) dmma_8x8x4(acc[q][t][0], acc[q][t][1], af[q], bf[t]);
   }
 #pragma unroll
   for (int q = 0; q < 4; q++)
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
-      const int gi = r0 + tx + 16 * q, gc = c0 + ty + 16 * t;
-      if (gi < n && gc < n) a[gi + static_cast<long long>(ld) * gc] -= acc[q][t];
-    }
+    for (int t = 0; t < 2; t++)
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        const int gi = r0 + wm + 8 * q + fr, gc = c0 + wn + 8 * t + 2 * fk + v;
+        if (gi < n && gc < n) a[gi + static_cast<long long>(ld) * gc] -= acc[q][t][v];
+      }
 }
 
 // B <- A^{-1} B, one CTA per right-hand side, the vector in shared memory.
@@ -707,11 +713,12 @@ __global__ void __launch_bounds__(256) gemm_tn_long_kernel(int m, int k, double 
   }
 }
 
-// One 64 x 64 tile of C = C0 - op(A) op(B) per CTA.
+// One 64 x 64 tile of C = C0 + alpha op(A) op(B) per CTA (FP64 tensor cores).
 __global__ void __launch_bounds__(256) gemm_sub_kernel(double* C, int ldc, const double* C0,
                                                        int ldc0, const double* A, int lda,
                                                        bool ta, const double* B, int ldb,
-                                                       bool tb, int m, int n, int kk) {
+                                                       bool tb, int m, int n, int kk,
+                                                       double alpha) {
   __shared__ double tile[kGemmTileDoubles];
   const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
   const int mt = min(64, m - i0), nt = min(64, n - j0);
@@ -719,7 +726,7 @@ __global__ void __launch_bounds__(256) gemm_sub_kernel(double* C, int ldc, const
   const double* Bb = tb ? B + j0 : B + static_cast<long long>(ldb) * j0;
   cta_gemm_tiled(C + i0 + static_cast<long long>(ldc) * j0, ldc,
                  C0 ? C0 + i0 + static_cast<long long>(ldc0) * j0 : nullptr, ldc0, Ab, lda, ta, Bb,
-                 ldb, tb, mt, nt, kk, tile);
+                 ldb, tb, mt, nt, kk, tile, alpha);
 }
 
 // Rows of B (nrows rows, row stride 1, column stride ldb) <- rows of B A^{-1},
@@ -739,7 +746,17 @@ cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, cons
   if (m <= 0 || n <= 0) return cudaSuccess;
   count_launches(1);
   gemm_sub_kernel<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(C, ldc, C0, ldc0, A, lda, ta,
-                                                                      B, ldb, tb, m, n, k);
+                                                                      B, ldb, tb, m, n, k, -1.0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_tiled(double* C, int ldc, const double* C0, int ldc0, const double* A,
+                              int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,
+                              int k, double alpha, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return cudaSuccess;
+  count_launches(1);
+  gemm_sub_kernel<<<dim3((m + 63) / 64, (n + 63) / 64), 256, 0, s>>>(C, ldc, C0, ldc0, A, lda, ta,
+                                                                      B, ldb, tb, m, n, k, alpha);
   return cudaGetLastError();
 }
 

@@ -739,9 +739,54 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
   const double tol3z = sqrt(0.5 * 2.220446049250313e-16);
   int rank = 0;
   double thresh = 0.0;
+  // Sketched boxes (rows sk = n + 16): warp 0 forms step i's Householder
+  // vector right after choosing its pivot, so a step costs two CTA barriers
+  // (after the trailing update, after warp 0) instead of four.
+  double* hh = red + 16;  // [0] tau, [1] |tol R_00|; si[2]: the rank once found
+  auto householder_w0 = [&](int i) {
+    const double* colc = colp(si[1]);
+    double part = 0.0;
+    for (int r = i + 1 + lane; r < m; r += 32) {
+      const double a0 = colc[r];
+      v[r] = a0;
+      part += a0 * a0;
+    }
+    const double xnorm = sqrt(warp_sum(part));
+    const double alpha = colc[i];
+    double beta = alpha, tau = 0.0, scal = 0.0;
+    if (i < m - 1 && xnorm != 0.0) {
+      beta = -copysign(lapy2(alpha, xnorm), alpha);
+      tau = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+    for (int r = i + 1 + lane; r < m; r += 32) v[r] *= scal;
+    if (lane == 0) {
+      if (i == 0) hh[1] = fabs(P.tol * beta);
+      if (i >= 1 && fabs(beta) < hh[1]) si[2] = i;
+      rdiag[i] = beta;
+      v[i] = 1.0;
+      hh[0] = tau;
+    }
+  };
+  if (sketch) {
+    if (warp == 0) {
+      if (lane == 0) si[2] = 0;
+      __syncwarp();
+      if (mn > 0) householder_w0(0);
+    }
+    __syncthreads();
+  }
   for (int i = 0; i < mn; i++) {
     const int c = si[1];
     const double* colc = colp(c);
+    double tau = 0.0;
+    if (sketch) {
+      if (si[2] != 0) {
+        rank = si[2];
+        break;
+      }
+      tau = hh[0];
+    } else {
     double part = 0.0;
     for (int r = i + 1 + threadIdx.x; r < m; r += kOcThreads) {
       const double a0 = colc[r];
@@ -756,7 +801,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     for (int w = 0; w < kOcWarps; w++) xs += red[w];
     const double xnorm = sqrt(xs);
     const double alpha = colc[i];
-    double beta = alpha, tau = 0.0, scal = 0.0;
+    double beta = alpha, scal = 0.0;
     if (i < m - 1 && xnorm != 0.0) {
       beta = -copysign(lapy2(alpha, xnorm), alpha);
       tau = (beta - alpha) / beta;
@@ -773,6 +818,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     }
     for (int r = i + 1 + threadIdx.x; r < m; r += kOcThreads) v[r] *= scal;
     __syncthreads();
+    }
     const int nown = si[0];
     // lanes per column for this step: spread the trailing columns over all
     // warps (L = 1 .. 32, a power of two); lane s of a group walks rows
@@ -845,7 +891,13 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
         }
         cg::this_cluster().sync();
       }
-      if (warp == 0) select_pivot(i + 1, G > 1);
+      if (warp == 0) {
+        select_pivot(i + 1, G > 1);
+        if (sketch) {
+          __syncwarp();
+          householder_w0(i + 1);
+        }
+      }
       __syncthreads();
     }
   }

@@ -181,6 +181,11 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
 // the other blocks' bounded waits run out (mode 2); either way it ends with
 // *status = 2.  0 clears it.
 void inject_lu_fault(int mode);
+// Multi-CTA tiled C = C0 + alpha op(A) op(B) (64 x 64 tiles, FP64 tensor
+// cores); C0 may be null.
+cudaError_t launch_gemm_tiled(double* C, int ldc, const double* C0, int ldc0, const double* A,
+                              int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,
+                              int k, double alpha, cudaStream_t s);
 // Multi-CTA tiled C = C0 - op(A) op(B) (64 x 64 tiles); C0 may be null.
 cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, const double* A,
                             int lda, bool ta, const double* B, int ldb, bool tb, int m, int n,
