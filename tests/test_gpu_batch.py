@@ -82,3 +82,31 @@ def test_batch_exact_operator_is_block_diagonal():
         torch.cuda.synchronize()
         assert np.array_equal(yp.cpu().numpy(), ys[p])
         s.close()
+
+
+def test_full_batch256_config_against_the_oracle():
+    """The benchmark's batch configuration itself: 256 random stars of
+    512-8192 nodes (seed 4) in one batched factorization.  FP64 at id_tol
+    1e-10: 16 problems spread over the batch (every 16th) are within 1e-10
+    of the FP64 oracle's solution of the same problem; mixed+refine: every
+    problem's residual meets 1e-12 and the same 16 are within 1e-10 of the
+    converged oracle (id_tol 1e-13)."""
+    probs = G.random_star_cases(256, seed=4)
+    pick = list(range(0, 256, 16))
+    bs = kinterp.BatchSolver(probs, id_tol=1e-10)
+    parts = bs.split(bs.solve())
+    bs.close()
+    bm = kinterp.BatchSolver(probs, id_tol=3e-7, mode=1)
+    mu, it, rr = bm.solve_refined(rel_tol=1e-12, max_iters=20)
+    mixed = bm.split(mu)
+    bm.close()
+    assert rr <= 1e-12, (it, rr)
+    for p in pick:
+        o = K.PortSolver(probs[p], id_tol=1e-10, threads=8)
+        mo, _ = o.solve(probs[p].f)
+        o.close()
+        assert H.rel(parts[p], mo) < 1e-10, p
+        o = K.PortSolver(probs[p], id_tol=1e-13, threads=8)
+        mt, _ = o.solve(probs[p].f)
+        o.close()
+        assert H.rel(mixed[p], mt) < 1e-10, p
