@@ -15,7 +15,7 @@ unknowns / (factor + solve time), for two methods on the same GPU:
     preconditioner mode (tall ID matrices reduced by a sparse row sketch)
     used by FP64 refinement / GMRES on the operator with on-the-fly FP64
     entries, stopped at relative residual 1e-12 (ki_factor_ex +
-    ki_solve_refined_device; residuals below 1e-5 are updated with the
+    ki_solve_refined_device; residuals below 5e-8 are updated with the
     correction product, FP32 far field / FP64 near field, and the true FP64
     residual of the result is reported beside it);
   * FP64 (`fp64`): the reference method, factorization at ID tolerance

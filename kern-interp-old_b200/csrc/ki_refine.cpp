@@ -213,10 +213,12 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
   // continues from the current X and residual.  Once the residual r is
   // small, a step's correction D = M^-1 r is small too and the residual is
   // updated as r -= A D with the correction product: its relative error
-  // (~1e-6, see launch_corr_matvec) applies to |D| ~ |r|, not to |X|.
-  static const double corr_rel = [] {
-    const char* e = std::getenv("KI_CORR_REL");
-    return e ? std::atof(e) : kCorrRel;
+  // (kCorrErr, see launch_corr_matvec) applies to |A D| ~ |r|, not to |X|,
+  // so the updated residual stays within kCorrErr |r| of the true one; the
+  // product is used only while that is below a tenth of the tolerance.
+  static const bool corr_on = [] {
+    const char* e = std::getenv("KI_CORR");
+    return !(e && e[0] == '0');
   }();
   double beta = 0.0;
   bool done = false;
@@ -237,7 +239,7 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
       if (solve_graph(V, W, nb ? W + N : nullptr, nb ? V + N : nullptr)) return -2;
       KI_CUDA(launch_add(X, W, n, stream_));
       iters++;
-      if (rel <= corr_rel) {
+      if (corr_on && kCorrErr * rel <= 0.1 * rel_tol) {
         // Z (unused until GMRES) receives A D
         if (corr_matvec_device(W, Z, 1.0 / beta)) return -2;
         KI_CUDA(launch_sub(V, V, Z, n, stream_));

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -542,7 +543,41 @@ int Solver::factor() {
   return finish_factor(ev0);
 }
 
+int Solver::check_coincident() {
+  // Two nodes at the same position make two columns of the operator equal
+  // (the reference takes r = 0 as the diagonal, kernel.cpp:23-36, 80-85),
+  // an exactly singular system that no pivot would reveal.  Coincident
+  // nodes fall in the same leaf: each leaf's points are sorted and
+  // neighbours compared.
+  std::vector<int> leaves;
+  for (size_t i = 0; i < tree.boxes.size(); i++)
+    if (tree.boxes[i].leaf && !tree.boxes[i].dead) leaves.push_back(static_cast<int>(i));
+  std::atomic<long long> hit{-1};
+  parallel_for(static_cast<int>(leaves.size()), 16, [&](int a, int e) {
+    std::vector<int> pt;
+    for (int q = a; q < e; q++) {
+      pt.clear();
+      for (int dof : tree.boxes[leaves[q]].original)
+        if (dof % sd_ == 0) pt.push_back(dof / sd_);
+      std::sort(pt.begin(), pt.end(), [&](int u, int v) {
+        return pts_[2 * u] < pts_[2 * v] ||
+               (pts_[2 * u] == pts_[2 * v] && pts_[2 * u + 1] < pts_[2 * v + 1]);
+      });
+      for (size_t i = 1; i < pt.size(); i++)
+        if (pts_[2 * pt[i]] == pts_[2 * pt[i - 1]] &&
+            pts_[2 * pt[i] + 1] == pts_[2 * pt[i - 1] + 1])
+          hit.store(static_cast<long long>(std::min(pt[i], pt[i - 1])) << 32 |
+                    std::max(pt[i], pt[i - 1]));
+    }
+  });
+  const long long h = hit.load();
+  if (h < 0) return 0;
+  return fail("coincident boundary nodes " + std::to_string(h >> 32) + " and " +
+              std::to_string(h & 0xffffffffLL) + " (the operator is singular)");
+}
+
 int Solver::finish_factor(cudaEvent_t ev0) {
+  if (const int crc = check_coincident()) return crc;
   cudaEvent_t ev1;
   KI_CUDA(ev_get(&ev1));
   levels_.assign(tree.levels.size(), LevelFactors{});

@@ -163,11 +163,11 @@ class Solver {
   // preconditioned by this factorization, entries of A formed on the fly:
   // stops when ||[f; 0] - A [mu; alpha]|| <= rel_tol ||f|| or after
   // max_iters preconditioned products.  The first residual is formed with
-  // the FP64 product; once the residual is below kCorrRel ||f||, a
-  // stationary step updates it as r -= A d with the correction product of
-  // its small correction d (corr_matvec_device), whose error is a tiny
-  // fraction of |d|.  iters / rel_res report the work and the final
-  // residual.
+  // the FP64 product; once the residual r is small enough that the
+  // correction product's error (kCorrErr |r|) stays below a tenth of
+  // rel_tol ||f||, a stationary step updates it as r -= A d with the
+  // correction product of its correction d (corr_matvec_device).  iters /
+  // rel_res report the work and the final residual.
   int solve_refined(const double* d_f, double* d_mu, double* d_alpha, double rel_tol,
                     int max_iters, int* iters, double* rel_res);
   // Fast FP64 product y = A x (bordered), the refinement's residual operator.
@@ -175,9 +175,9 @@ class Solver {
   // y = A d for a small correction d: far source blocks summed in FP32 with
   // d scaled by dscale, near blocks in FP64 (launch_corr_matvec).
   int corr_matvec_device(const double* d_x, double* d_y, double dscale);
-  // Residuals below this fraction of ||f|| are updated with the correction
-  // product (KI_CORR_REL overrides; 0 disables it).
-  static constexpr double kCorrRel = 1e-5;
+  // Relative error bound of the correction product (measured below 2e-6 of
+  // |A d| on every test geometry); KI_CORR=0 turns the product off.
+  static constexpr double kCorrErr = 2e-6;
   // Bounding-box gap below which a source block is summed in FP64.
   static constexpr double kCorrNearGap = 0.01;
   // x = A^-T b with the same factorization (simply connected domains):
@@ -292,6 +292,7 @@ class Solver {
   int level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s);
   int begin_factor(cudaEvent_t* ev0);
   int setup_geometry();
+  int check_coincident();  // refuse nodes at the same position
   bool geom_ready_ = false;  // setup_geometry done for this factorization
   int finish_factor(cudaEvent_t ev0);
   // Copies the factors of `boxes` (T, L, U, X^-1, update, pivots) from

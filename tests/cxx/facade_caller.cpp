@@ -142,13 +142,19 @@ int main() {
     expect_le("left_multiply_inverse", (X * U - K).frob_norm() / K.frob_norm(), 1e-13);
     expect_le("right_multiply_inverse", (L * X - K.transpose()).frob_norm() / K.frob_norm(),
               1e-13);
-    ki_Mat A(60, 30);  // rank 8
+    // rank 8: a product of 60 x 8 and 8 x 30 factors with pseudo-random
+    // entries in [-1, 1)
+    unsigned long long seed = 12345;
+    auto rnd = [&seed]() {
+      seed = seed * 6364136223846793005ull + 1442695040888963407ull;
+      return static_cast<double>(seed >> 11) / 9007199254740992.0 * 2.0 - 1.0;
+    };
+    ki_Mat F(60, 8), Gm(8, 30);
+    for (int j = 0; j < 8; j++)
+      for (int i = 0; i < 60; i++) F.set(i, j, rnd());
     for (int j = 0; j < 30; j++)
-      for (int i = 0; i < 60; i++) {
-        double v = 0;
-        for (int r = 0; r < 8; r++) v += std::cos(0.1 * i * (r + 1)) * std::sin(0.3 * j + r);
-        A.set(i, j, v);
-      }
+      for (int i = 0; i < 8; i++) Gm.set(i, j, rnd());
+    ki_Mat A = F * Gm;
     std::vector<int> p;
     ki_Mat Z;
     const int k = A.id(&p, &Z, 1e-10);

@@ -3,9 +3,10 @@ cooperative LU's bounded waits (200 ms, %globaltimer) end a factorization
 with KI_ERR_NUMERIC instead of hanging, both when its abort word is raised
 before it starts and when one thread block withholds its flag so that the
 others' waits run out; the device stays usable and the next factorization
-is exact.  Coincident boundary nodes (a 0/0 kernel entry between them, as
-in the reference's formula) end the factorization with KI_ERR_NUMERIC
-instead of returning NaN factors.  The reference exits or asserts in these
+is exact.  Coincident boundary nodes make two columns of the operator equal
+(the reference's entry formula takes r = 0 as the diagonal), an exactly
+singular system no pivot reveals in floating point: the factorization
+refuses them with KI_ERR_NUMERIC instead of returning meaningless factors.  The reference exits or asserts in these
 cases (skel_factorization.cpp:151-154)."""
 import ctypes as C
 import time
@@ -55,7 +56,8 @@ def test_coincident_nodes_fail_with_numeric_error():
     pts[2 * 700:2 * 701] = pts[2 * 701:2 * 702]  # node 700 on top of node 701
     bad = G.Problem(pr.name + "_dup", pr.pde, pts, pr.normals, pr.curvatures, pr.weights,
                     pr.holes, pr.f, pr.targets, pr.exact, pr.leaf_points, pr.id_tol, pr.extra)
-    _expect_numeric_failure(bad)
+    msg = _expect_numeric_failure(bad)
+    assert "coincident" in msg
     # and the device is still usable
     s = kinterp.Solver(pr)
     mu, _ = s.solve(pr.f)
