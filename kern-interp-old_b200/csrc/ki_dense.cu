@@ -629,6 +629,16 @@ __global__ void __launch_bounds__(kSolveThreads)
                         double* b, int ldb) {
   extern __shared__ double x[];
   double* bc = b + static_cast<long long>(ldb) * blockIdx.x;
+  // the whole LU into L2 up front (one prefetch per 128-byte line): the
+  // blocked substitutions then wait on L2, not HBM, at every block step
+  {
+    const int lines = (n * 8 + 127) / 128;  // per column, upper bound
+    for (int e = threadIdx.x; e < n * lines; e += blockDim.x) {
+      const int c = e / lines, q = e % lines;
+      const double* a = lu + static_cast<long long>(ld) * c + 16 * q;
+      if (16 * q < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+    }
+  }
   for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[i];
   __syncthreads();
   cta_lu_solve(lu, n, ld, ipiv, x);

@@ -102,6 +102,64 @@ __device__ __forceinline__ void warp_best(double& v, int& p) {
   }
 }
 
+// Stokes entries of one ID-matrix row for both dofs (components 0, 1) of a
+// column node, with the arithmetic of the fast single-entry path
+// (pair_entry<true> / proxy_entry_node<true>) and the pair's shared part (r,
+// |r|^2, its reciprocal, r.n) formed once.  kind 0: row = target dof rdof
+// of node rn, the column node the source; kind 1: the transposed block
+// (the column node the target, rn/rdof the source); kind 2: proxy row pr.
+__device__ __forceinline__ void stokes_entries2(int kind, const Node& rn, int rdof, const Node& cn,
+                                                int cdof0, int pr, const double* dir, double cx,
+                                                double cy, double rad, double pw, int ps,
+                                                double* e0, double* e1) {
+  if (kind == 2) {
+    const int np = kNumProxy >> ps;
+    const bool second = pr >= 2 * np;
+    const int rr_ = second ? pr - 2 * np : pr;
+    const int q = (rr_ >> 1) << ps, comp = rr_ & 1;
+    const double tn0 = dir[q], tn1 = dir[kNumProxy + q];
+    const double r0 = (cx + rad * tn0) - cn.x, r1 = (cy + rad * tn1) - cn.y;
+    const double rr = r0 * r0 + r1 * r1;
+    const double rc = comp ? r1 : r0, tnc = comp ? tn1 : tn0;
+    if (!second) {
+      const double pot = ((cn.w * KI_INV_PI) * (r0 * cn.nx + r1 * cn.ny)) * nr_rcp(rr * rr);
+      *e0 = (pot * rc) * r0 + (cn.w * tnc) * cn.nx;
+      *e1 = (pot * rc) * r1 + (cn.w * tnc) * cn.ny;
+    } else {
+      const double pot = ((-pw * KI_INV_PI) * (r0 * tn0 + r1 * tn1)) * nr_rcp(rr * rr);
+      *e0 = (pot * rc) * r0 + (pw * cn.nx) * tnc;
+      *e1 = (pot * rc) * r1 + (pw * cn.ny) * tnc;
+    }
+    return;
+  }
+  if (rn.x == cn.x && rn.y == cn.y) {  // a node with itself: the diagonal formula
+    if (kind == 0) {
+      *e0 = pair_entry<true>(kStokes, rn, rdof, cn, cdof0);
+      *e1 = pair_entry<true>(kStokes, rn, rdof, cn, cdof0 + 1);
+    } else {
+      *e0 = pair_entry<true>(kStokes, cn, cdof0, rn, rdof);
+      *e1 = pair_entry<true>(kStokes, cn, cdof0 + 1, rn, rdof);
+    }
+    return;
+  }
+  const Node& t = kind == 0 ? rn : cn;  // target node
+  const Node& s = kind == 0 ? cn : rn;  // source node
+  const double r0 = t.x - s.x, r1 = t.y - s.y;
+  const double inv = nr_rcp(r0 * r0 + r1 * r1);
+  const double pot = (s.w * KI_INV_PI) * (r0 * s.nx + r1 * s.ny) * (inv * inv);
+  if (kind == 0) {  // the row's component fixed, the source component varies
+    const int tc = rdof & 1;
+    const double rt = tc ? r1 : r0, tn = tc ? t.ny : t.nx;
+    *e0 = (pot * rt) * r0 + (s.w * tn) * s.nx;
+    *e1 = (pot * rt) * r1 + (s.w * tn) * s.ny;
+  } else {  // the row's (source) component fixed, the target component varies
+    const int sc = rdof & 1;
+    const double rs = sc ? r1 : r0, sn = sc ? s.ny : s.nx;
+    *e0 = (pot * r0) * rs + (s.w * t.nx) * sn;
+    *e1 = (pot * r1) * rs + (s.w * t.ny) * sn;
+  }
+}
+
 __device__ __forceinline__ double lapy2(double x, double y) {
   const double xa = fabs(x), ya = fabs(y);
   const double w = fmax(xa, ya), z = fmin(xa, ya);
@@ -591,18 +649,22 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
   if (sketch) {
     // Y = S A for this CTA's columns.  Warp w owns columns t = w, w + 16, ...
     // and walks the rows of A 32 at a time, lane l generating row r0 + l in
-    // registers; per block, the lanes whose rows hash to the same row of Y
-    // (found with match.any) are summed in lane order through shuffles and
-    // the group's first lane adds the sum.  A column is only touched by its
-    // warp, pass after pass in row order, so the result is deterministic,
-    // and no barrier is needed.  Columns never mix, so the CTAs of a cluster
-    // need no exchange here.
-    const int mA = tk.m, blk = m / kSketchBlocks;
+    // registers and adding it, with its row's hashed sign, into row
+    // (h(block) + l) mod sk of Y: a sparse sign embedding whose buckets are
+    // runs of 32 from a hashed start, so the lanes of a block never hit the
+    // same row (sk >= 32) and each adds its entry directly.  A column is only
+    // touched by its warp, pass after pass in row order, so the result is
+    // deterministic, and no barrier is needed.  Columns never mix, so the
+    // CTAs of a cluster need no exchange here.
+    const int mA = tk.m;
     const int sh = pde == kStokes ? 1 : 0;
     // this CTA's column node records and dofs, staged once
     Node* cn = reinterpret_cast<Node*>(
         (reinterpret_cast<uintptr_t>(si + 8) + 15) & ~uintptr_t{15});
     int* cdof = reinterpret_cast<int*>(cn + nloc);
+    // work units: a column, or (Stokes, G = 1) the two dofs of one node in
+    // consecutive columns, whose entries share r, |r|^2 and r.n
+    int* unit = cdof + nloc;  // 2 t + (pair ? 1 : 0)
     for (int t = threadIdx.x; t < nloc; t += kOcThreads) {
       const int cd = act[g + G * t];
       cdof[t] = cd;
@@ -611,7 +673,26 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     for (long long e = threadIdx.x; e < static_cast<long long>(lda) * nloc; e += kOcThreads)
       cols[e] = 0.0;
     __syncthreads();
-    if (warp < nloc) {
+    const bool pairs = G == 1 && pde == kStokes;
+    if (warp == 0) {
+      int cnt = 0;
+      for (int base = 0; base < nloc; base += 32) {
+        const int t = base + lane;
+        bool start = t < nloc, two = false;
+        if (start && pairs) {
+          const int cd = cdof[t];
+          start = !((cd & 1) && t > 0 && cdof[t - 1] == cd - 1);
+          two = !(cd & 1) && t + 1 < nloc && cdof[t + 1] == cd + 1;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, start);
+        if (start) unit[cnt + __popc(bal & ((1u << lane) - 1u))] = 2 * t + (two ? 1 : 0);
+        cnt += __popc(bal);
+      }
+      if (lane == 0) si[3] = cnt;
+    }
+    __syncthreads();
+    const int nunits = si[3];
+    if (warp < nunits) {
       for (int r0 = 0; r0 < mA; r0 += 32) {
         const int r = r0 + lane;
         const bool valid = r < mA;
@@ -621,22 +702,26 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
           rdof = rowd[r < I ? r : r - I];
           rnode = nodes[rdof >> sh];
         }
-        // this row's hashed row of Y in each block (sign from the top bit)
-        // and the lanes sharing it; an idle lane is a group of its own
-        int idx[kSketchBlocks];
-        bool neg[kSketchBlocks];
-        unsigned grp[kSketchBlocks];
-        int gmax = 0;
-#pragma unroll
-        for (int b = 0; b < kSketchBlocks; b++) {
-          const unsigned h = sketch_hash(static_cast<unsigned>(r) * kSketchBlocks + b);
-          idx[b] = static_cast<int>(h % blk);
-          neg[b] = (h & 0x80000000u) != 0;
-          grp[b] = __match_any_sync(0xffffffffu, valid ? idx[b] : -1 - lane);
-          gmax = max(gmax, __popc(grp[b]));
-        }
-        gmax = __reduce_max_sync(0xffffffffu, gmax);
-        for (int t = warp; t < nloc; t += kOcWarps) {
+        // the block of 32 rows lands on 32 consecutive rows of Y (mod sk)
+        // from a hashed start, so the lanes of a block never collide; the
+        // sign comes from the row's own hash
+        int idx = static_cast<int>(sketch_hash(static_cast<unsigned>(r0 >> 5) ^ 0x9e3779b9u) %
+                                   static_cast<unsigned>(m)) + lane;
+        if (idx >= m) idx -= m;
+        const bool neg = (sketch_hash(static_cast<unsigned>(r)) & 0x80000000u) != 0;
+        for (int u = warp; u < nunits; u += kOcWarps) {
+          const int t = unit[u] >> 1;
+          if (unit[u] & 1) {
+            if (valid) {
+              double e0, e1;
+              stokes_entries2(r < I ? 0 : r < 2 * I ? 1 : 2, rnode, rdof, cn[t], cdof[t],
+                              r - 2 * I, P.proxy_dir, tk.cx, tk.cy, tk.rad, tk.pw, tk.pshift,
+                              &e0, &e1);
+              cols[static_cast<long long>(lda) * t + idx] += neg ? -e0 : e0;
+              cols[static_cast<long long>(lda) * (t + 1) + idx] += neg ? -e1 : e1;
+            }
+            continue;
+          }
           double val = 0.0;
           if (valid) {
             if (r < I) {
@@ -648,22 +733,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
                                            tk.cy, tk.rad, tk.pw, tk.pshift);
             }
           }
-          double* ycol = cols + static_cast<long long>(lda) * t;
-#pragma unroll
-          for (int b = 0; b < kSketchBlocks; b++) {
-            const double sv = neg[b] ? -val : val;
-            unsigned rest = grp[b];
-            double sum = 0.0;
-            for (int q = 0; q < gmax; q++) {
-              const int src = rest ? __ffs(rest) - 1 : lane;
-              const double o = __shfl_sync(0xffffffffu, sv, src);
-              if (rest) {
-                sum += o;
-                rest &= rest - 1;
-              }
-            }
-            if (valid && (grp[b] & ((1u << lane) - 1u)) == 0) ycol[b * blk + idx[b]] += sum;
-          }
+          if (valid) cols[static_cast<long long>(lda) * t + idx] += neg ? -val : val;
         }
       }
     }
@@ -755,9 +825,10 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     const double alpha = colc[i];
     double beta = alpha, tau = 0.0, scal = 0.0;
     if (i < m - 1 && xnorm != 0.0) {
+      // (sketched boxes only: reciprocals by Newton-refined estimates)
       beta = -copysign(lapy2(alpha, xnorm), alpha);
-      tau = (beta - alpha) / beta;
-      scal = 1.0 / (alpha - beta);
+      tau = (beta - alpha) * nr_rcp(beta);
+      scal = nr_rcp(alpha - beta);
     }
     for (int r = i + 1 + lane; r < m; r += 32) v[r] *= scal;
     if (lane == 0) {
@@ -849,9 +920,11 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
         nv1 = vn1[j];
         const double nv2 = vn2[j];
         if (nv1 != 0.0) {
-          double temp = fabs(aij) / nv1;
+          // sketched boxes need not follow dlaqp2's rounding: reciprocal
+          // estimates instead of divisions on this per-step chain
+          double temp = sketch ? fabs(aij) * nr_rcp(nv1) : fabs(aij) / nv1;
           temp = fmax(1.0 - temp * temp, 0.0);
-          const double qq = nv1 / nv2;
+          const double qq = sketch ? nv1 * nr_rcp(nv2) : nv1 / nv2;
           const double temp2 = temp * (qq * qq);
           if (temp2 <= tol3z) {
             recompute = true;
@@ -923,6 +996,9 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
       }
       if (lane == 0) si[0] = cnt;
     }
+    // reciprocals of R's diagonal, off the substitutions' dependent chains
+    // (vn2 is free once the factorization has stopped)
+    for (int q = threadIdx.x; q < k; q += kOcThreads) vn2[q] = 1.0 / rdiag[q];
     __syncthreads();
     // one warp per redundant column: the column's back substitution runs
     // in its warp with no CTA barrier (columns are independent)
@@ -933,7 +1009,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
       for (int q = k - 1; q >= 0; q--) {
         const double bq = col[q];
         __syncwarp();
-        const double xq = bq != 0.0 ? bq / rdiag[q] : bq;
+        const double xq = bq * vn2[q];
         if (lane == 0) T[q + static_cast<long long>(p - k) * k] = xq;
         if (bq != 0.0) {
           const double* rq = colp(pos2col[q]);
@@ -1011,7 +1087,7 @@ size_t id_sketch_smem_bytes(int sk, int n, int G) {
   const size_t nloc = static_cast<size_t>((n + G - 1) / G);
   // matrix share, staged node records and dofs of the columns (+ alignment)
   return id_smem_bytes(sk, n) + sizeof(double) * nloc * onchip_lda(sk) +
-         (sizeof(Node) + sizeof(int)) * nloc + 16;
+         (sizeof(Node) + 2 * sizeof(int)) * nloc + 16;
 }
 
 size_t id_onchip_smem_bytes(int m, int n, int G) {

@@ -39,9 +39,10 @@ struct IdTask {
   int pshift;     // sketched tasks: proxy circle of kNumProxy >> pshift points
 };
 
-// Row sketch of an ID matrix (on-chip, one CTA): S has kSketchBlocks blocks
-// of sk / kSketchBlocks rows, and every row of A is added with a hashed sign
-// into one hashed row of each block (a sparse sign embedding).
+// Row sketch of an ID matrix (on-chip): every row of A is added with a
+// hashed sign into one row of the sk-row sketch, the rows of each 32-row
+// block of A into a run of 32 consecutive sketch rows (mod sk) from a hashed
+// start (a sparse sign embedding; sk >= 32).
 constexpr int kSketchBlocks = 1;
 // Sketch rows for an m x n matrix: n + 16 rounded up to the block count.
 inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlocks * kSketchBlocks; }
@@ -317,7 +318,7 @@ cudaError_t launch_kernel_block(int pde, const Node* nodes, const int* tgt, int 
 // ---------------------------------------------------------------- Krylov
 // Fast FP64 operator product y = A x (fused, reassociated: accurate to FP64
 // rounding, not bit-identical to the entry kernels), bordered by U / Psi
-// when nb > 0.  `part` needs fast_matvec_scratch_doubles(n_dofs, splits).
+// when nb > 0.  `part` needs fast_matvec_scratch_doubles(n_dofs, splits, nseg, nb).
 constexpr int kMaxMatvecSplits = 64;
 constexpr int kMaxKrylov = 64;  // vectors per multi-dot
 // One CTA of the operator product: targets [t0, t1) (nodes) against sources
@@ -334,7 +335,7 @@ int matvec_splits(int pde, int n_nodes, int nseg, int num_sms);
 // seg: node offsets of the segments (size nseg + 1); one segment = one
 // problem, so a forest's operator is block diagonal.
 void matvec_tiles(const std::vector<int>& seg, int splits, std::vector<MvTile>* tiles);
-size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg);
+size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg, int nb);
 cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, int ntiles,
                                const int* seg, int nseg, int n_dofs, int splits, const double* x,
                                double* y, int nb, const double* U, const double* Psi,
@@ -376,6 +377,8 @@ cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int 
 cudaError_t launch_add(double* x, const double* y, int n, cudaStream_t s);
 // r = b - ax
 cudaError_t launch_sub(double* r, const double* b, const double* ax, int n, cudaStream_t s);
+// y = g - y (g null: y = -y)
+cudaError_t launch_rsub(double* y, const double* g, int n, cudaStream_t s);
 
 }  // namespace kib
 

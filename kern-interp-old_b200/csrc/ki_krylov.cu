@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kMvThreads)
 }
 
 // y_i = sum of the splits' partials + diagonal correction + rank-one term +
-// U x_border; the border rows are done by mv_border_rows_kernel.
+// U x_border; the border rows are done by mv_border_partial_kernel.
 __device__ __forceinline__ int segment_of(const int* __restrict__ seg, int nseg, int node) {
   int lo = 0, hi = nseg - 1;  // seg[lo] <= node < seg[hi + 1]
   while (lo < hi) {
@@ -358,23 +358,56 @@ __global__ void mv_finish_kernel(int pde, const Node* __restrict__ nodes, int n_
   y[i] = s;
 }
 
-// Border rows: y_{N+h} = Psi(h, :) x(0:N) - x_{N+h}, one CTA per row.
-__global__ void mv_border_rows_kernel(int n_dofs, int nb, const double* __restrict__ Psi,
-                                      const double* __restrict__ x, double* __restrict__ y) {
-  __shared__ double red[32];
-  const int h = blockIdx.x;
-  double s = 0.0;
-  for (int j = threadIdx.x; j < n_dofs; j += blockDim.x)
-    s += Psi[h + static_cast<long long>(nb) * j] * x[j];
+// Border rows y_{N+h} = Psi(h, :) x(0:N) - x_{N+h} in one pass over Psi:
+// Psi is nb x N column-major, so a dof's nb entries are contiguous; each
+// thread walks dofs, accumulating up to 32 rows at a time in registers, and
+// each CTA writes its partial sums (kBorderBlocks x nb), added in a fixed
+// order by mv_border_finish_kernel.
+constexpr int kBorderBlocks = 64;
+__global__ void __launch_bounds__(256)
+    mv_border_partial_kernel(int n_dofs, int nb, const double* __restrict__ Psi,
+                             const double* __restrict__ x, double* __restrict__ part) {
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int per = (n_dofs + gridDim.x - 1) / gridDim.x;
+  const int j0 = blockIdx.x * per, j1 = min(n_dofs, j0 + per);
+  for (int h0 = 0; h0 < nb; h0 += 32) {
+    const int hn = min(32, nb - h0);
+    double acc[32];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double v = 0.0;
-    for (int w = 0; w < static_cast<int>(blockDim.x >> 5); w++) v += red[w];
-    y[n_dofs + h] = v - x[n_dofs + h];
+    for (int h = 0; h < 32; h++) acc[h] = 0.0;
+    for (int j = j0 + threadIdx.x; j < j1; j += 256) {
+      const double xj = x[j];
+      const double* pc = Psi + static_cast<long long>(nb) * j + h0;
+#pragma unroll
+      for (int h = 0; h < 32; h++)
+        if (h < hn) acc[h] += pc[h] * xj;
+    }
+#pragma unroll
+    for (int h = 0; h < 32; h++) {
+      double v = acc[h];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][h] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < hn) {
+      double v = 0.0;
+      for (int w = 0; w < 8; w++) v += red[w][threadIdx.x];
+      part[static_cast<long long>(blockIdx.x) * nb + h0 + threadIdx.x] = v;
+    }
+    __syncthreads();
   }
+}
+
+__global__ void mv_border_finish_kernel(int n_dofs, int nb, int nblk,
+                                        const double* __restrict__ part,
+                                        const double* __restrict__ x, double* __restrict__ y) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= nb) return;
+  double v = 0.0;
+  for (int b = 0; b < nblk; b++) v += part[static_cast<long long>(b) * nb + h];
+  y[n_dofs + h] = v - x[n_dofs + h];
 }
 
 // ---- vector kernels (n up to a few million; k <= kMaxKrylov vectors)
@@ -433,6 +466,11 @@ __global__ void scale_copy_kernel(double* __restrict__ dst, const double* __rest
 __global__ void add_kernel(double* __restrict__ x, const double* __restrict__ y, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] += y[i];
+}
+
+__global__ void rsub_kernel(double* __restrict__ y, const double* __restrict__ g, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = (g ? g[i] : 0.0) - y[i];
 }
 
 __global__ void sub_kernel(double* __restrict__ r, const double* __restrict__ b,
@@ -525,7 +563,12 @@ cudaError_t launch_fast_matvec(int pde, const Node* nodes, const MvTile* tiles, 
                                                               part_rank1);
   mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
                                                         part_rank1, seg, nseg, x, y, nb, U);
-  if (nb) mv_border_rows_kernel<<<nb, 256, 0, s>>>(n_dofs, nb, Psi, x, y);
+  if (nb) {
+    double* bpart = part_rank1 + static_cast<long long>(splits) * nseg;
+    count_launches(1);
+    mv_border_partial_kernel<<<kBorderBlocks, 256, 0, s>>>(n_dofs, nb, Psi, x, bpart);
+    mv_border_finish_kernel<<<(nb + 63) / 64, 64, 0, s>>>(n_dofs, nb, kBorderBlocks, bpart, x, y);
+  }
   return cudaGetLastError();
 }
 
@@ -549,12 +592,18 @@ cudaError_t launch_corr_matvec(int pde, const Node* nodes, const MvTile* tiles, 
         nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
   mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
                                                         part_rank1, seg, nseg, x, y, nb, U);
-  if (nb) mv_border_rows_kernel<<<nb, 256, 0, s>>>(n_dofs, nb, Psi, x, y);
+  if (nb) {
+    double* bpart = part_rank1 + static_cast<long long>(splits) * nseg;
+    count_launches(1);
+    mv_border_partial_kernel<<<kBorderBlocks, 256, 0, s>>>(n_dofs, nb, Psi, x, bpart);
+    mv_border_finish_kernel<<<(nb + 63) / 64, 64, 0, s>>>(n_dofs, nb, kBorderBlocks, bpart, x, y);
+  }
   return cudaGetLastError();
 }
 
-size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg) {
-  return static_cast<size_t>(splits) * n_dofs + static_cast<size_t>(splits) * nseg;
+size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg, int nb) {
+  return static_cast<size_t>(splits) * n_dofs + static_cast<size_t>(splits) * nseg +
+         static_cast<size_t>(kBorderBlocks) * nb;
 }
 
 int multi_dot_blocks(int n) { return std::max(1, std::min(296, (n + 1023) / 1024)); }
@@ -593,6 +642,13 @@ cudaError_t launch_segment_sumsq(const double* v, const int* seg, int nseg, int 
 cudaError_t launch_add(double* x, const double* y, int n, cudaStream_t s) {
   count_launches(1);
   add_kernel<<<(n + 255) / 256, 256, 0, s>>>(x, y, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rsub(double* y, const double* g, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launches(1);
+  rsub_kernel<<<(n + 255) / 256, 256, 0, s>>>(y, g, n);
   return cudaGetLastError();
 }
 

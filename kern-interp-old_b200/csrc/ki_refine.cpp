@@ -95,7 +95,7 @@ int Solver::solve_graph(const double* d_b, double* d_mu, double* d_alpha, const 
 int Solver::matvec_device(const double* d_x, double* d_y) {
   if (mv_setup()) return -2;
   const int nseg = static_cast<int>(seg_.size()) - 1;
-  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg);
+  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg, nb_);
   // the product's partials live at the start of kry_; solve_refined places
   // its vectors after them
   if (kry_.bytes < sizeof(double) * need) KI_CUDA(kry_.reserve(sizeof(double) * need, stream_));
@@ -108,7 +108,7 @@ int Solver::matvec_device(const double* d_x, double* d_y) {
 int Solver::corr_matvec_device(const double* d_x, double* d_y, double dscale) {
   if (mv_setup()) return -2;
   const int nseg = static_cast<int>(seg_.size()) - 1;
-  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg);
+  const size_t need = fast_matvec_scratch_doubles(n_dofs_, mv_splits_, nseg, nb_);
   if (kry_.bytes < sizeof(double) * need) KI_CUDA(kry_.reserve(sizeof(double) * need, stream_));
   KI_CUDA(launch_corr_matvec(opt_.pde, d_nodes_, d_mv_tiles_, n_mv_tiles_, d_seg_, nseg, n_dofs_,
                              mv_splits_, d_x, dscale, kCorrNearGap, d_y, nb_, d_U_, d_Psi_,
@@ -122,7 +122,7 @@ int Solver::solve_refined(const double* d_f, double* d_mu, double* d_alpha, doub
   const int m = std::max(1, std::min(max_iters, kMaxKrylov - 2));  // restart length
   if (mv_setup()) return -2;
   const int nseg = static_cast<int>(seg_.size()) - 1;
-  const size_t mv = (fast_matvec_scratch_doubles(N, mv_splits_, nseg) + 31) / 32 * 32;
+  const size_t mv = (fast_matvec_scratch_doubles(N, mv_splits_, nseg, nb) + 31) / 32 * 32;
   const size_t ldv = (static_cast<size_t>(n) + 31) / 32 * 32;
   const size_t dotp = static_cast<size_t>(kMaxKrylov) * multi_dot_blocks(n);
   // [mv partials][V: (m+1) ldv][Z: m ldv][B][X][W][dot partials][h: 3 kMaxKrylov]

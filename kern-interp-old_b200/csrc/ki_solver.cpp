@@ -724,7 +724,7 @@ int Solver::id_launch(int level, PendingLevel* pl) {
         // for two CTAs per SM (a single CTA per SM leaves the SM idle at
         // every barrier of the pivoted QR), else the smallest that fits
         const int l = sketch_rows(c.n);
-        if (c.m > l + 64)
+        if (c.m > l + 64 && l >= 32)  // (the buckets of a 32-row block must differ)
           for (const size_t cap : {size_t{113} * 1024, size_t{227} * 1024}) {
             for (int G = 1; G <= 16 && !c.sk; G *= 2)
               if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) {
@@ -1569,11 +1569,18 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dw, nr, 1, 1, d_red_pos_,
                    all_compressed_.cap};
     KI_CUDA(launch_diag_solve(dp, stream_));
-    // border rows of the reduced system: g - Psi~_r D^-1 w_r
-    if (d_g)
-      KI_CUDA(cudaMemcpyAsync(M + ns, d_g, sizeof(double) * nb, cudaMemcpyDeviceToDevice, stream_));
-    KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, d_g ? 1.0 : 0.0, M + ns,
-                       nb, stream_));
+    // border rows of the reduced system: g - Psi~_r D^-1 w_r (the nb dot
+    // products in one pass over the rows, partials behind M)
+    if (nb <= kMaxKrylov) {
+      KI_CUDA(launch_multi_dot(d_Pred_, nr, nb, dw, nr, M + ns + nb, M + ns, stream_));
+      KI_CUDA(launch_rsub(M + ns, d_g, nb, stream_));
+    } else {
+      if (d_g)
+        KI_CUDA(cudaMemcpyAsync(M + ns, d_g, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
+                                stream_));
+      KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, d_g ? 1.0 : 0.0,
+                         M + ns, nb, stream_));
+    }
     KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_));
     if (d_alpha)
       KI_CUDA(cudaMemcpyAsync(d_alpha, M + ns, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
