@@ -377,6 +377,8 @@ def main():
     ap.add_argument("--workload", default="stokes65k", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--mixed-tol", type=float, default=None,
+                    help="ID tolerance of the preconditioning factorization (default: per workload)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -384,7 +386,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     global MIXED_TOL
-    MIXED_TOL = MIXED_TOLS.get(args.workload, MIXED_TOL)
+    MIXED_TOL = args.mixed_tol or MIXED_TOLS.get(args.workload, MIXED_TOL)
     built = WORKLOADS[args.workload][0]()
     batch = args.workload == "batch256"
     probs = built if batch else [built]

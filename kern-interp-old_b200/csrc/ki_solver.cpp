@@ -742,10 +742,21 @@ int Solver::id_launch(int level, PendingLevel* pl) {
   for (int q = 0; q < nids; q++)
     if (keep[q]) cand.push_back(std::move(all[q]));
   if (cand.empty()) return 0;
-  // by cluster size, then the largest ID matrices first: CTAs start in
-  // index order, so the long tasks do not end up in a launch's last wave
-  std::stable_sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) {
-    if (a.g != b.g) return a.g < b.g;
+  // grouped by cluster size, the group holding the widest ID matrix first
+  // (its launch then takes SMs before the many-box launch fills them: the
+  // few big boxes are each level's longest tasks), and inside a group the
+  // largest first (CTAs start in index order, so the long tasks do not end
+  // up in a launch's last wave)
+  std::map<int, long long> group_max;  // widest task (its steps and sketch rows grow with n)
+  for (const Cand& c : cand) {
+    long long& v = group_max[c.g];
+    v = std::max(v, static_cast<long long>(c.n) * 100000 + std::min(c.m, 99999));
+  }
+  std::stable_sort(cand.begin(), cand.end(), [&](const Cand& a, const Cand& b) {
+    if (a.g != b.g) {
+      const long long ma = group_max[a.g], mb = group_max[b.g];
+      return ma != mb ? ma > mb : a.g > b.g;
+    }
     return static_cast<long long>(a.m) * a.n > static_cast<long long>(b.m) * b.n;
   });
 
