@@ -628,6 +628,12 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
       si[1] = cp;
     }
     __syncwarp();
+    if constexpr (G == 1) {
+      // a single CTA owns every column: the positions > i, in order (the
+      // trailing update takes p = i + 1 + q without the list)
+      if (lane == 0) si[0] = n - i - 1;
+      return;
+    }
     int cnt = 0;
     for (int base = i + 1; base < n; base += 32) {
       const int p = base + lane;
@@ -904,7 +910,7 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     for (int q0 = 0; q0 < nown; q0 += ngroups) {
       const int q = q0 + gi;
       const bool active = q < nown;
-      const int p = active ? own[q] : 0;
+      const int p = active ? (G == 1 ? i + 1 + q : own[q]) : 0;
       const int j = active ? pos2col[p] : g;
       double* col = colp(j);
       double w = 0.0;
@@ -975,6 +981,9 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     }
   }
   if constexpr (G > 1) cg::this_cluster().sync();
+  // a sketch shorter than n + 16 rows certifies a rank only well below its
+  // row count; otherwise the box is reported (-1) for the full sketch
+  if (sketch && m < n + 16 && (rank == 0 || rank > m - 16)) rank = -1;
 
   if (g == 0) {
     if (threadIdx.x == 0) P.rank[task] = rank;

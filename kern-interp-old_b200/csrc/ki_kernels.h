@@ -46,6 +46,16 @@ struct IdTask {
 constexpr int kSketchBlocks = 1;
 // Sketch rows for an m x n matrix: n + 16 rounded up to the block count.
 inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlocks * kSketchBlocks; }
+// Sketch rows when the box's rank is expected near rank_hint (the largest
+// rank of the level below; 0 when unknown): rank_hint + 40, at least 64 and
+// at most n + 16, a multiple of 8.  A rank found above rows - 16, or none,
+// is not trusted (the kernel reports -1 and the box is decomposed again
+// with n + 16 rows).
+inline int sketch_rows_hint(int n, int rank_hint) {
+  const int want = ((rank_hint > 24 ? rank_hint : 24) + 40 + 7) / 8 * 8;
+  const int full = sketch_rows(n);
+  return want < full ? want : full;
+}
 
 struct IdParams {
   const IdTask* tasks;

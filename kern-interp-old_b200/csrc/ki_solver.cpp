@@ -401,6 +401,7 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
   t_id_ms = t_decouple_ms = t_top_ms = 0;
   id_launches = 0;
   id_flops = id_bytes = id_onchip_flops = 0;
+  rank_hint_ = -1;
   dec_flops = top_flops = solve_bytes = 0;
 
   if (!dstream_) {
@@ -723,16 +724,24 @@ int Solver::id_launch(int level, PendingLevel* pl) {
         // the smallest cluster whose CTAs' shares of the sketch leave room
         // for two CTAs per SM (a single CTA per SM leaves the SM idle at
         // every barrier of the pivoted QR), else the smallest that fits
+        auto fit = [&](int l) {  // cluster size for an l-row sketch, 0: none
+          for (const size_t cap : {size_t{113} * 1024, size_t{227} * 1024})
+            for (int G = 1; G <= 16; G *= 2)
+              if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) return G;
+          return 0;
+        };
+        // the full sketch (n + 16 rows) must be possible; the box is then
+        // sketched with rows sized by the level below's ranks, and decomposed
+        // again with the full sketch if those do not certify its rank
         const int l = sketch_rows(c.n);
-        if (c.m > l + 64 && l >= 32)  // (the buckets of a 32-row block must differ)
-          for (const size_t cap : {size_t{113} * 1024, size_t{227} * 1024}) {
-            for (int G = 1; G <= 16 && !c.sk; G *= 2)
-              if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) {
-                c.sk = l;
-                c.g = kOnChip + G;
-              }
-            if (c.sk) break;
-          }
+        const int G_full = c.m > l + 64 && l >= 32 ? fit(l) : 0;  // (bucket runs need l >= 32)
+        if (G_full) {
+          const int ls = sketch_rows_hint(c.n, rank_hint_);
+          const int G_short = ls < l ? fit(ls) : 0;
+          c.sk = G_short ? ls : l;
+          c.g = kOnChip + (G_short ? G_short : G_full);
+          c.g_full = G_short ? kOnChip + G_full : 0;
+        }
         if (c.sk && level > 2) c.m = 2 * c.I + (P >> opt_.proxy_shift);
       }
       keep[q] = 1;
@@ -896,8 +905,73 @@ int Solver::id_launch(int level, PendingLevel* pl) {
   KI_CUDA(cudaMemcpyAsync(pl->perm, d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,
                           stream_));
   pl->d_act = d_act;
+  pl->d_rows = d_rows;
   pl->d_perm = d_perm;
   pl->d_T = d_T;
+  return 0;
+}
+
+int Solver::id_rerun_full(PendingLevel* pl) {
+  const int nc = static_cast<int>(pl->cand.size());
+  std::vector<int> qs;
+  for (int q = 0; q < nc; q++)
+    if (pl->rank[q] < 0) qs.push_back(q);
+  // the same boxes with n + 16 sketch rows, grouped by cluster size
+  std::stable_sort(qs.begin(), qs.end(), [&](int a, int b) {
+    return pl->cand[a].g_full > pl->cand[b].g_full;
+  });
+  std::vector<IdTask> t2(qs.size());
+  for (size_t u = 0; u < qs.size(); u++) {
+    IdCand& c = pl->cand[qs[u]];
+    if (!c.g_full) return fail("interpolative decomposition: sketch too short for a box");
+    t2[u] = pl->tasks[qs[u]];
+    t2[u].sk = sketch_rows(c.n);
+    t2[u].lda = onchip_lda(t2[u].sk);
+    c.sk = t2[u].sk;
+    c.g = c.g_full;
+  }
+  IdTask* d_t2;
+  int* d_r2;
+  KI_ALLOC(d_t2, IdTask, t2.size());
+  KI_ALLOC(d_r2, int, t2.size());
+  KI_UPLOAD(d_t2, t2, stream_);
+  for (size_t q0 = 0; q0 < qs.size();) {
+    size_t q1 = q0;
+    const int g = pl->cand[qs[q0]].g;
+    long long smem = 0;
+    int n_cap = 0;
+    while (q1 < qs.size() && pl->cand[qs[q1]].g == g) {
+      const IdCand& c = pl->cand[qs[q1]];
+      smem = std::max<long long>(smem, id_sketch_smem_bytes(c.sk, c.n, g - kOnChip));
+      n_cap = std::max(n_cap, c.n);
+      q1++;
+    }
+    IdParams p{};
+    p.tasks = d_t2 + q0;
+    p.ntasks = static_cast<int>(q1 - q0);
+    p.pde = opt_.pde;
+    p.nodes = d_nodes_;
+    p.act = pl->d_act;
+    p.rowdofs = pl->d_rows;
+    p.work = static_cast<double*>(work_.p);
+    p.tout = pl->d_T;
+    p.perm = pl->d_perm;
+    p.rank = d_r2 + q0;
+    p.proxy_dir = d_proxy_dir_;
+    p.tol = opt_.id_tol;
+    p.m_cap = 0;
+    p.n_cap = n_cap;
+    p.onchip_smem = smem;
+    KI_CUDA(launch_id(p, g, stream_));
+    q0 = q1;
+  }
+  int* r2 = static_cast<int*>(stage_.alloc(sizeof(int) * qs.size()));
+  if (!r2) return fail("pinned staging allocation failed");
+  KI_CUDA(cudaMemcpyAsync(r2, d_r2, sizeof(int) * qs.size(), cudaMemcpyDeviceToHost, stream_));
+  KI_CUDA(cudaMemcpyAsync(pl->perm, pl->d_perm, sizeof(int) * pl->perm_total,
+                          cudaMemcpyDeviceToHost, stream_));
+  KI_CUDA(cudaStreamSynchronize(stream_));
+  for (size_t u = 0; u < qs.size(); u++) pl->rank[qs[u]] = std::max(r2[u], 0);
   return 0;
 }
 
@@ -917,6 +991,12 @@ int Solver::id_finish(PendingLevel* pl) {
     t_wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0)
                      .count();
   }
+  for (int q = 0; q < nc; q++)
+    if (rank[q] < 0) {
+      const int rc = id_rerun_full(pl);
+      if (rc) return rc;
+      break;
+    }
 
   // skeleton / redundant sets (InteractionLists::set_rs_ranges, quadtree.h:23-35)
   const double h1 = now_ms();
@@ -965,6 +1045,7 @@ int Solver::id_finish(PendingLevel* pl) {
       id_bytes += bytes_v[q];
       if (cand[q].g >= kOnChip) id_onchip_flops += qr_v[q];
       if (rank[q] > 0) comp.push_back(q);
+      rank_hint_ = std::max(rank_hint_, rank[q]);
     }
   }
   t_host_post_ms += now_ms() - h1;

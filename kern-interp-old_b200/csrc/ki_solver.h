@@ -269,6 +269,7 @@ class Solver {
   // level's IDs are launched before this level's decouple bookkeeping.
   struct IdCand {
     int box = -1, n = 0, m = 0, I = 0, g = 0, sk = 0;
+    int g_full = 0;  // sketched with fewer than n + 16 rows: the cluster for n + 16
     std::vector<int> rows;
   };
   struct PendingLevel {
@@ -280,6 +281,7 @@ class Solver {
     int* rank = nullptr;  // pinned device-to-host targets
     int* perm = nullptr;
     int* d_act = nullptr;
+    int* d_rows = nullptr;
     int* d_perm = nullptr;
     double* d_T = nullptr;
     int perm_total = 0;
@@ -287,6 +289,12 @@ class Solver {
   };
   int id_launch(int level, PendingLevel* pl);
   int id_finish(PendingLevel* pl);
+  // Boxes whose short sketch could not certify their rank (rank -1 from
+  // the kernel) decomposed again with the full n + 16 rows.
+  int id_rerun_full(PendingLevel* pl);
+  // Largest rank of the previous (deeper) level of this factorization
+  // (-1 before the first level): sizes the next level's sketches.
+  int rank_hint_ = -1;
   int decouple_level(PendingLevel* pl);
   int decouple_boxes(PendingLevel* pl);
   int level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t s);
