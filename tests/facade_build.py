@@ -41,6 +41,6 @@ def build_reference_tests():
     if not os.path.isdir(os.path.join(REF_DIR, "kern_interp")):
         return REF_TESTS_BIN if os.path.exists(REF_TESTS_BIN) else None
     facade_lib()
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "facade", "REF=" + REF_DIR],
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "facade", "KI_REFERENCE_DIR=" + REF_DIR],
                    check=True, capture_output=True)
     return REF_TESTS_BIN
