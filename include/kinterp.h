@@ -256,9 +256,10 @@ int ki_launch_log(ki_solver_t s, double* out, int cap);
 /* Timeline of a ki_factor_timed factorization: rows of 4 doubles
  * (what, level, start ms, end ms) after the factorization began: `what` <
  * 100 is a launch kind of ki_launch_log timed on the GPU clock; `what` =
- * 100 + code is a host mark (0 tree built, 1 level lists ready and ID
- * launched, 2 ranks received, 3 decouple launched, 4 top level started,
- * 5 top level launched, 6 synchronised) on the host clock.  Returns the row
+ * 100 + code is a host mark (7 geometry queued, 8 partition built, 0 tree
+ * checked, 1 level lists ready and ID launched, 2 ranks received, 3 decouple
+ * launched, 4 top level started, 5 top level launched, 6 synchronised) on
+ * the host clock.  Returns the row
  * count; writes at most cap rows. */
 int ki_timeline(ki_solver_t s, double* out, int cap);
 

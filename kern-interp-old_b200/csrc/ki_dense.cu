@@ -787,11 +787,12 @@ constexpr size_t kSolveSmemMax = 200 * 1024;
 // CTA b of the cooperative grid owns columns [32 b, 32 b + 32) in shared
 // memory for the whole factorization.  For every panel k < b it waits for
 // panel k's flag, then applies that step to its own columns exactly as the
-// panel-by-panel path does (row interchanges, U12 = L11^{-1} A12, A22 -=
-// L21 U12, same operation order, hence the same bits wherever that path
-// takes 32-column panels, i.e. up to 512 rows); then it factors its own
+// panel-by-panel path does (row interchanges, U12 = L11^{-1} A12 in the
+// same order, A22 -= L21 U12 on the FP64 tensor cores: the same values up
+// to the order of the sums over the panel's 32 columns); then it factors its own
 // panel (the pivot search over its rows, one row interchange, the rank-one
-// update: two barriers per column), publishes the block and its pivots and
+// update: one barrier per column with the rows in registers up to 512 rows,
+// two in shared memory beyond), publishes the block and its pivots and
 // raises flag b.  The next panel's owner starts as soon as it has applied
 // step b, while the others are still updating: the dependent chain is
 // panel, one step's update on one CTA, panel, ...  Finished blocks apply
@@ -873,8 +874,105 @@ __device__ __forceinline__ void fused_swaps(double* blk, int np, int n, int j0, 
   }
 }
 
+// This CTA's panel when every row has its own thread (n <= kFusedThreads):
+// thread t holds row t's block columns in registers, and each column costs
+// one barrier.  Before it, every warp publishes its best candidate (key,
+// row) and that row whole, and the owner of row `col` publishes row col;
+// after it, every thread agrees on the pivot p from the 16 warp maxima and
+// reads the pivot row from its warp's slot, rows col and p trade values, and
+// the rows below apply the rank-one update in registers.  The slots are
+// double-buffered by column parity: column jj + 2 writes a slot only after
+// the barrier of column jj + 1, which every thread reaches after its reads
+// of column jj.  Same pivots and the same arithmetic (l = x * (1 / piv),
+// x_c -= l * prow_c) as the shared-memory panel.
+struct __align__(16) PanelSlots {
+  double cand[2][kFusedThreads / 32][kNb];
+  double crow[2][kNb];
+  unsigned long long key[2][kFusedThreads / 32];
+  int idx[2][kFusedThreads / 32];
+};
+
+__device__ __forceinline__ void fused_panel_regs(double* blk, int np, int n, int c0, int wb,
+                                                 int* ipiv, int* status, PanelSlots& S) {
+  const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
+  double x[kNb];
+#pragma unroll
+  for (int c = 0; c < kNb; c++) x[c] = i < n && c < wb ? blk[i + np * c] : 0.0;
+#pragma unroll
+  for (int jj = 0; jj < kNb; jj++) {
+    if (jj >= wb) break;
+    const int col = c0 + jj, buf = jj & 1;
+    // candidates: |x| of rows >= col (a NaN is no candidate), the largest,
+    // the first such row on ties
+    const double v = fabs(x[jj]);
+    const bool is_cand = i >= col && i < n && v == v;
+    unsigned long long wkey;
+    int widx;
+    warp_argmax_bits(is_cand ? static_cast<unsigned long long>(__double_as_longlong(v)) : 0ull,
+                     is_cand ? i : 0x7fffffff, &wkey, &widx);
+    if (lane == 0) {
+      S.key[buf][warp] = wkey;
+      S.idx[buf][warp] = widx;
+    }
+    // (rows moved as pairs of doubles: half the shared-memory instructions)
+    if (i == widx) {
+      double2* d = reinterpret_cast<double2*>(S.cand[buf][warp]);
+#pragma unroll
+      for (int q = 0; q < kNb / 2; q++) d[q] = make_double2(x[2 * q], x[2 * q + 1]);
+    }
+    if (i == col) {
+      double2* d = reinterpret_cast<double2*>(S.crow[buf]);
+#pragma unroll
+      for (int q = 0; q < kNb / 2; q++) d[q] = make_double2(x[2 * q], x[2 * q + 1]);
+    }
+    __syncthreads();
+    unsigned long long gkey;
+    int p;
+    warp_argmax_bits(lane < kFusedThreads / 32 ? S.key[buf][lane] : 0ull,
+                     lane < kFusedThreads / 32 ? S.idx[buf][lane] : 0x7fffffff, &gkey, &p);
+    // no comparable entry (NaN column): keep the row, flag the factorization
+    const bool bad = p < col || p >= n;
+    const double* prow = bad ? S.crow[buf] : S.cand[buf][p >> 5];
+    if (bad) p = col;
+    const double piv = prow[jj];
+    if (i == 0) {
+      ipiv[col] = p;
+      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
+    }
+    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+    const double2* prow2 = reinterpret_cast<const double2*>(prow);
+    if (i == col || i == p) {
+      const double2* src = i == col ? prow2 : reinterpret_cast<const double2*>(S.crow[buf]);
+#pragma unroll
+      for (int q = 0; q < kNb / 2; q++) {
+        const double2 t = src[q];
+        x[2 * q] = t.x;
+        x[2 * q + 1] = t.y;
+      }
+    }
+    if (i > col && i < n) {
+      const double li = x[jj] * inv;
+#pragma unroll
+      for (int q = (jj + 1) / 2; q < kNb / 2; q++) {
+        const double2 t = prow2[q];
+        if (2 * q > jj) x[2 * q] -= li * t.x;
+        x[2 * q + 1] -= li * t.y;
+      }
+      x[jj] = li;
+    }
+  }
+  if (i >= c0 && i < n) {
+#pragma unroll
+    for (int c = 0; c < kNb; c++)
+      if (c < wb) blk[i + np * c] = x[c];
+  }
+}
+
 // hold (a test hook, normally 0): thread block 0 keeps its flag down, so the
 // other blocks' bounded waits run out and the launch ends with status 2.
+// kRegPanel: n <= kFusedThreads, the panel in registers (one instantiation
+// per panel form keeps each one's registers to itself).
+template <bool kRegPanel>
 __global__ void __launch_bounds__(kFusedThreads, 1)
     lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync, int hold) {
   extern __shared__ double blk[];  // np x kNb, column-major
@@ -883,14 +981,20 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   __shared__ int redi[kFusedThreads / 32];
   __shared__ int pv[kNb];
   __shared__ int s_ok;
+  __shared__ PanelSlots slots;
   const int G = gridDim.x, b = blockIdx.x;
   const int np = n | 1;
   const int c0 = kNb * b, wb = min(kNb, n - c0);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int c = 0; c < wb; c++) {  // one column per pass: loads in flight
-#pragma unroll 2
-    for (int i = tid; i < n; i += kFusedThreads)
-      blk[i + np * c] = a[i + static_cast<long long>(ld) * (c0 + c)];
+  for (int i0 = 0; i0 < n; i0 += kFusedThreads) {  // a row's 32 loads in flight at once
+    const int i = i0 + tid;
+    double v[kNb];
+#pragma unroll
+    for (int c = 0; c < kNb; c++)
+      v[c] = i < n && c < wb ? a[i + static_cast<long long>(ld) * (c0 + c)] : 0.0;
+#pragma unroll
+    for (int c = 0; c < kNb; c++)
+      if (i < n && c < wb) blk[i + np * c] = v[c];
   }
   __syncthreads();
 
@@ -906,45 +1010,92 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     __syncthreads();
     fused_swaps(blk, np, n, j0, wk, wb, pv);
     __syncthreads();
-    // U12 = L11^{-1} A12, one warp per column, in the kk order of the
-    // panel-by-panel path
-    for (int c = warp; c < wb; c += kFusedThreads / 32) {
-      double x = lane < wk ? blk[j0 + lane + np * c] : 0.0;
+    // U12 = L11^{-1} A12, one warp per two columns (interleaved), in the kk
+    // order of the panel-by-panel path
+    static_assert(kNb == 2 * (kFusedThreads / 32), "two columns per warp");
+    {
+      const int ca = warp, cb = warp + kFusedThreads / 32;
+      double xa = lane < wk && ca < wb ? blk[j0 + lane + np * ca] : 0.0;
+      double xb = lane < wk && cb < wb ? blk[j0 + lane + np * cb] : 0.0;
+#pragma unroll 8
       for (int kk = 0; kk < wk; kk++) {
-        const double xk = __shfl_sync(0xffffffffu, x, kk);
-        if (lane > kk && lane < wk) x -= xk * l11[lane][kk];
-      }
-      if (lane < wk) blk[j0 + lane + np * c] = x;
-    }
-    __syncthreads();
-    // A22 -= L21 U12 (the sum over kk first, then subtracted)
-    for (int i = j0 + wk + tid; i < n; i += kFusedThreads) {
-      double acc[kNb];
-#pragma unroll
-      for (int c = 0; c < kNb; c++) acc[c] = 0.0;
-      // L21's row in groups of 8 loads in flight (kk order kept)
-      for (int kk0 = 0; kk0 < wk; kk0 += 8) {
-        double l[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++)
-          l[q] = kk0 + q < wk ? __ldcg(a + i + static_cast<long long>(ld) * (j0 + kk0 + q)) : 0.0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-          if (kk0 + q >= wk) break;
-          const double* u = blk + j0 + kk0 + q;
-#pragma unroll
-          for (int c = 0; c < kNb; c++) acc[c] += l[q] * u[np * c];
+        const double ya = __shfl_sync(0xffffffffu, xa, kk);
+        const double yb = __shfl_sync(0xffffffffu, xb, kk);
+        if (lane > kk && lane < wk) {
+          const double l = l11[lane][kk];
+          xa -= ya * l;
+          xb -= yb * l;
         }
       }
+      if (lane < wk && ca < wb) blk[j0 + lane + np * ca] = xa;
+      if (lane < wk && cb < wb) blk[j0 + lane + np * cb] = xb;
+    }
+    __syncthreads();
+    // A22 -= L21 U12 on the FP64 tensor cores (m8n8k4): warp w takes the
+    // 8-row tiles w, w + 16, w + 32, w + 48 below the panel against the
+    // block's 8-column tiles, L21 fragments from global memory (L2), U12
+    // fragments from the block; the sum over kk first, then subtracted
+    {
+      const int r0 = j0 + wk, nr = n - r0;
+      const int fr = lane >> 2, fk = lane & 3;
+      constexpr int nw = kFusedThreads / 32;
+      for (int t0 = warp; 8 * t0 < nr; t0 += 4 * nw) {
+        // every L21 fragment of the warp's rows requested at once (one L2
+        // round trip), then the block's columns in two halves of 16
+        double af[kNb / 4][4];
 #pragma unroll
-      for (int c = 0; c < kNb; c++)
-        if (c < wb) blk[i + np * c] -= acc[c];
+        for (int ks = 0; ks < kNb / 4; ks++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int row = r0 + 8 * (t0 + nw * q) + fr, kk = 4 * ks + fk;
+            af[ks][q] = row < n && kk < wk
+                            ? __ldcg(a + row + static_cast<long long>(ld) * (j0 + kk))
+                            : 0.0;
+          }
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+          double acc[4][2][2];
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int t = 0; t < 2; t++) acc[q][t][0] = acc[q][t][1] = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < kNb / 4; ks++) {
+            const int kk = 4 * ks + fk;
+            double bf[2];
+#pragma unroll
+            for (int t = 0; t < 2; t++) {
+              const int col = 16 * h + 8 * t + fr;
+              bf[t] = kk < wk && col < wb ? blk[j0 + kk + np * col] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+#pragma unroll
+              for (int t = 0; t < 2; t++)
+                dmma_8x8x4(acc[q][t][0], acc[q][t][1], af[ks][q], bf[t]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int row = r0 + 8 * (t0 + nw * q) + fr;
+            if (row >= n) continue;
+#pragma unroll
+            for (int t = 0; t < 2; t++)
+#pragma unroll
+              for (int v = 0; v < 2; v++) {
+                const int col = 16 * h + 8 * t + 2 * fk + v;
+                if (col < wb) blk[row + np * col] -= acc[q][t][v];
+              }
+          }
+        }
+      }
     }
     __syncthreads();
   }
 
-  // this CTA's panel: rows c0.., thread t owning rows t + 512 q
-  for (int jj = 0; jj < wb; jj++) {
+  // this CTA's panel: in registers when every row has a thread, else in
+  // shared memory (thread t owning rows t + 512 q, two barriers a column)
+  if (kRegPanel) fused_panel_regs(blk, np, n, c0, wb, ipiv, status, slots);
+  for (int jj = 0; jj < wb && !kRegPanel; jj++) {
     const int col = c0 + jj;
     // candidates: |a_ij| for rows i >= col (a NaN is no candidate); the
     // largest, the first such row on ties
@@ -1045,7 +1196,9 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
   if (sync && n > 0 && n <= kLuFusedMaxN) {
     int G = (n + kNb - 1) / kNb;
     const size_t smem = sizeof(double) * static_cast<size_t>(n | 1) * kNb;
-    cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_fused_kernel),
+    const void* fn = n <= kFusedThreads ? reinterpret_cast<const void*>(&lu_fused_kernel<true>)
+                                        : reinterpret_cast<const void*>(&lu_fused_kernel<false>);
+    cudaError_t e = raise_func_attr(fn,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1061,8 +1214,7 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
     }
     void* args[] = {&a, &n, &ld, &ipiv, &status, &sync, &hold};
     count_launches(1);
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&lu_fused_kernel),
-                                       dim3(G), dim3(kFusedThreads), args, smem, s);
+    return cudaLaunchCooperativeKernel(fn, dim3(G), dim3(kFusedThreads), args, smem, s);
   }
   for (int j0 = 0; j0 < n;) {
     // register-resident panels: 32 columns while a thread holds one row,

@@ -51,6 +51,8 @@ inline int sketch_rows(int n) { return (n + 16 + kSketchBlocks - 1) / kSketchBlo
 // at most n + 16, a multiple of 8.  A rank found above rows - 16, or none,
 // is not trusted (the kernel reports -1 and the box is decomposed again
 // with n + 16 rows).
+// Levels of at most this many boxes take the full sketch directly.
+constexpr int kShortSketchMinBoxes = 32;
 inline int sketch_rows_hint(int n, int rank_hint) {
   const int want = ((rank_hint > 24 ? rank_hint : 24) + 40 + 7) / 8 * 8;
   const int full = sketch_rows(n);
@@ -180,7 +182,7 @@ cudaError_t launch_forest_top_solve(const TopTask* tasks, int ntasks, int n_max,
 // (kLuSyncInts ints of device scratch, used by this call alone until it
 // completes) a matrix of up to kLuFusedMaxN rows is factored by one
 // cooperative launch; otherwise, or when larger, panel by panel (the same
-// bits up to 512 rows).  *status: 1 zero pivot, 2 a bounded wait between the
+// pivot rule and values, the trailing sums in another order).  *status: 1 zero pivot, 2 a bounded wait between the
 // cooperative launch's thread blocks ran out.
 constexpr int kLuFusedMaxN = 768;
 constexpr int kLuSyncInts = kLuFusedMaxN / 32 + 8;

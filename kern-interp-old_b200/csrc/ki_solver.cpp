@@ -208,6 +208,8 @@ struct AuxSet {
   cudaEvent_t join[3] = {};
   cudaStream_t dl[3] = {};
   cudaEvent_t dl_fork = nullptr, dl_join[3] = {};
+  cudaStream_t b = nullptr;
+  cudaEvent_t ev_lvl = nullptr, ev_bdr = nullptr;
 };
 std::mutex g_aux_mu;
 std::vector<AuxSet>& aux_free() {
@@ -225,6 +227,7 @@ Solver::~Solver() {
     if (id_streams_[i]) cudaStreamSynchronize(id_streams_[i]);
   for (int i = 0; i < kDecStreams; i++)
     if (dl_streams_[i]) cudaStreamSynchronize(dl_streams_[i]);
+  if (bstream_) cudaStreamSynchronize(bstream_);
   if (dstream_) {
     static_assert(kIdStreams == 3 && kDecStreams == 3, "AuxSet holds three of each");
     AuxSet a;
@@ -243,6 +246,9 @@ Solver::~Solver() {
       a.dl[i] = dl_streams_[i];
       a.dl_join[i] = dl_join_[i];
     }
+    a.b = bstream_;
+    a.ev_lvl = ev_lvl_;
+    a.ev_bdr = ev_bdr_;
     std::lock_guard<std::mutex> lk(g_aux_mu);
     aux_free().push_back(a);
   }
@@ -429,6 +435,9 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
             dl_streams_[k] = a.dl[k];
             dl_join_[k] = a.dl_join[k];
           }
+          bstream_ = a.b;
+          ev_lvl_ = a.ev_lvl;
+          ev_bdr_ = a.ev_bdr;
           break;
         }
     }
@@ -447,6 +456,9 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
         KI_CUDA(cudaStreamCreateWithFlags(&dl_streams_[i], cudaStreamNonBlocking));
         KI_CUDA(cudaEventCreateWithFlags(&dl_join_[i], cudaEventDisableTiming));
       }
+      KI_CUDA(cudaStreamCreateWithFlags(&bstream_, cudaStreamNonBlocking));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_lvl_, cudaEventDisableTiming));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_bdr_, cudaEventDisableTiming));
     }
   }
   {
@@ -535,11 +547,13 @@ int Solver::factor() {
   if (starts_.size() > 1 && !holes_.empty()) return fail("a forest of problems cannot have holes");
   const int grc = setup_geometry();
   if (grc) return grc;
+  mark(7, 0);
   if (starts_.size() > 1) {
     tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
   } else {
     tree.build(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs);
   }
+  mark(8, 0);
   boxdev_.assign(tree.boxes.size(), BoxDev{});
   return finish_factor(ev0);
 }
@@ -618,6 +632,8 @@ int Solver::finish_factor(cudaEvent_t ev0) {
     allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
   KI_CUDA(cudaEventRecord(ev_dec_, dstream_));
   KI_CUDA(cudaStreamWaitEvent(stream_, ev_dec_, 0));
+  KI_CUDA(cudaEventRecord(ev_bdr_, bstream_));
+  KI_CUDA(cudaStreamWaitEvent(stream_, ev_bdr_, 0));
   cudaEvent_t t0 = nullptr;
   if (time_phases && timer_begin(&t0)) return -2;
   const double ht = now_ms();
@@ -730,13 +746,17 @@ int Solver::id_launch(int level, PendingLevel* pl) {
               if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) return G;
           return 0;
         };
-        // the full sketch (n + 16 rows) must be possible; the box is then
-        // sketched with rows sized by the level below's ranks, and decomposed
-        // again with the full sketch if those do not certify its rank
+        // the full sketch (n + 16 rows) must be possible; on a level of many
+        // boxes the box is then sketched with rows sized by the level below's
+        // ranks, and decomposed again with the full sketch if those do not
+        // certify its rank (a level of a few boxes, whose launches are short
+        // of work anyway, takes the full sketch: a second pass would put a
+        // whole launch and rank read-back on the factorization's critical
+        // path)
         const int l = sketch_rows(c.n);
         const int G_full = c.m > l + 64 && l >= 32 ? fit(l) : 0;  // (bucket runs need l >= 32)
         if (G_full) {
-          const int ls = sketch_rows_hint(c.n, rank_hint_);
+          const int ls = nids > kShortSketchMinBoxes ? sketch_rows_hint(c.n, rank_hint_) : l;
           const int G_short = ls < l ? fit(ls) : 0;
           c.sk = G_short ? ls : l;
           c.g = kOnChip + (G_short ? G_short : G_full);
@@ -1062,11 +1082,16 @@ int Solver::decouple_level(PendingLevel* pl) {
   if (rc) return rc;
   const LevelFactors& lf = levels_[pl->level];
   if (nb_ > 0 && lf.ntasks) {
-    // skel_factorization.cpp:146-160 for this level: U and Psi^T swept up
+    // skel_factorization.cpp:146-160 for this level: U and Psi^T swept up,
+    // on their own stream after the level's decoupling (in level order
+    // there), off the chain of decouplings: the next level's does not read
+    // them; the top level's border system waits for them
     SweepParams sp{lf.d_tasks, lf.ntasks, d_modU_, 1, nb_, 0, nullptr, lf.cap, nb_};
     SweepParams spp = sp;
     spp.x = d_modP_;
-    KI_CUDA(launch_sweep_up_pair(sp, spp, dstream_));
+    KI_CUDA(cudaEventRecord(ev_lvl_, dstream_));
+    KI_CUDA(cudaStreamWaitEvent(bstream_, ev_lvl_, 0));
+    KI_CUDA(launch_sweep_up_pair(sp, spp, bstream_));
   }
   return 0;
 }
@@ -1211,28 +1236,48 @@ int Solver::decouple_boxes(PendingLevel* pl) {
   t_host_post_ms += now_ms() - h1;
   mark(3, level);
   if (time_phases && timer_begin(&d0, dstream_)) return -2;
-  KI_CUDA(launch_decouple(dp, n_max, dstream_));
-  int n_large = 0;
-  if (!large.empty()) {
-    // the large boxes side by side on their own streams, after the level's
-    // uploads, joined back into dstream_
-    KI_CUDA(cudaEventRecord(dl_fork_, dstream_));
-    bool used[kDecStreams] = {};
-    for (size_t t = 0; t < large.size(); t++) {
-      const int si = static_cast<int>(t % kDecStreams);
-      if (!used[si]) {
-        KI_CUDA(cudaStreamWaitEvent(dl_streams_[si], dl_fork_, 0));
-        used[si] = true;
-      }
-      KI_CUDA(decouple_large(large[t], opt_.pde, d_nodes_, d_status_, dl_streams_[si]));
-      n_large = std::max(n_large, large[t].n);
+  // The batched boxes in size classes, one launch each: a launch's shared
+  // memory is sized by its largest box, so the small boxes of a level get
+  // three CTAs per SM (n <= 86), the middle ones two (n <= 110), and only
+  // the largest one (72 registers x 256 threads leave room for three); the widest class on dstream_, the others and the large
+  // boxes (one multi-kernel sequence each) side by side on their own
+  // streams after the level's uploads, joined back into dstream_.
+  KI_CUDA(cudaEventRecord(dl_fork_, dstream_));
+  bool used[kDecStreams] = {};
+  int next_side = 0;
+  auto side_stream = [&](cudaStream_t* out) -> int {
+    const int si = next_side++ % kDecStreams;
+    if (!used[si]) {
+      KI_CUDA(cudaStreamWaitEvent(dl_streams_[si], dl_fork_, 0));
+      used[si] = true;
     }
-    for (int i = 0; i < kDecStreams; i++)
-      if (used[i]) {
-        KI_CUDA(cudaEventRecord(dl_join_[i], dl_streams_[i]));
-        KI_CUDA(cudaStreamWaitEvent(dstream_, dl_join_[i], 0));
-      }
+    *out = dl_streams_[si];
+    return 0;
+  };
+  auto size_class = [](int n) { return n > 110 ? 0 : n > 86 ? 1 : 2; };
+  for (size_t a = 0; a < small.size();) {
+    size_t b = a;
+    while (b < small.size() && size_class(small[b].n) == size_class(small[a].n)) b++;
+    DecParams dpc = dp;
+    dpc.tasks = d_dt + a;
+    dpc.ntasks = static_cast<int>(b - a);
+    cudaStream_t cs = dstream_;
+    if (a > 0 && side_stream(&cs)) return -2;
+    KI_CUDA(launch_decouple(dpc, small[a].n, cs));  // (sorted: the class's largest first)
+    a = b;
   }
+  int n_large = 0;
+  for (size_t t = 0; t < large.size(); t++) {
+    cudaStream_t cs;
+    if (side_stream(&cs)) return -2;
+    KI_CUDA(decouple_large(large[t], opt_.pde, d_nodes_, d_status_, cs));
+    n_large = std::max(n_large, large[t].n);
+  }
+  for (int i = 0; i < kDecStreams; i++)
+    if (used[i]) {
+      KI_CUDA(cudaEventRecord(dl_join_[i], dl_streams_[i]));
+      KI_CUDA(cudaStreamWaitEvent(dstream_, dl_join_[i], 0));
+    }
   if (time_phases &&
       timer_end(d0, {level, 1, static_cast<int>(large.size()), ncomp, n_large, n_max, 0.0},
                 dstream_))

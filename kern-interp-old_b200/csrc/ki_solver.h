@@ -234,9 +234,10 @@ class Solver {
     double t0 = 0, t1 = 0;  // start / end, ms after the factorization began (GPU clock)
   };
   std::vector<LaunchRecord> launch_log;
-  // Host side of the timed factorization: code (0 tree built, 1 level lists
-  // ready / ID launched, 2 ranks received, 3 decouple launched, 4 top level
-  // started, 5 top level launched, 6 factorization synchronised), level,
+  // Host side of the timed factorization: code (7 geometry queued, 8
+  // partition built, 0 tree checked, 1 level lists ready / ID launched, 2
+  // ranks received, 3 decouple launched, 4 top level started, 5 top level
+  // launched, 6 factorization synchronised), level,
   // ms after the factorization began (host clock).
   struct HostMark {
     int code, level;
@@ -333,6 +334,9 @@ class Solver {
   static constexpr int kDecStreams = 3;
   cudaStream_t dl_streams_[kDecStreams] = {};
   cudaEvent_t dl_fork_ = nullptr, dl_join_[kDecStreams] = {};
+  // the border columns' level sweeps (U, Psi^T), beside the decouplings
+  cudaStream_t bstream_ = nullptr;
+  cudaEvent_t ev_lvl_ = nullptr, ev_bdr_ = nullptr;
 
   bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
