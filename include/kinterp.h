@@ -257,7 +257,8 @@ int ki_launch_log(ki_solver_t s, double* out, int cap);
  * (what, level, start ms, end ms) after the factorization began: `what` <
  * 100 is a launch kind of ki_launch_log timed on the GPU clock; `what` =
  * 100 + code is a host mark (7 geometry queued, 8 partition built, 0 tree
- * checked, 1 level lists ready and ID launched, 2 ranks received, 3 decouple
+ * checked, 9 a level's active lists, 10 its ID rows, 11 its ID groups
+ * ordered, 1 level lists ready and ID launched, 2 ranks received, 3 decouple
  * launched, 4 top level started, 5 top level launched, 6 synchronised) on
  * the host clock.  Returns the row
  * count; writes at most cap rows. */

@@ -46,7 +46,9 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 // Tiled CTA GEMM on the FP64 tensor cores: C (m x n) = C0 + alpha op(A)
 // op(B) (alpha = -1 unless given), op(A) m x kk, op(B) kk x n, 64 x 64
 // output tiles, the inner dimension staged 16 at a time in `tile` (2 * 16 *
-// 65 doubles, zero-padded past the matrix edges).  The 8 warps of the
+// kTileLd doubles, zero-padded past the matrix edges; kTileLd = 68, 4 mod
+// 16 doubles: a half-warp's fragment loads, rows 4 fk apart and columns fr
+// apart, then land on 16 distinct banks).  The 8 warps of the
 // (256-thread) CTA are laid out 2 x 4 over a tile: each warp owns a 32 x 16
 // block, i.e. 4 x 2 DMMA blocks of 8 x 8 with their accumulators in
 // registers, and takes 6 fragment loads from shared memory per 8 DMMAs
@@ -54,14 +56,15 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
 // FMAs, more than shared memory delivers at the FP64 rate.  C0 may be null
 // (taken as zero) or alias C; C must not alias A or B.  Operands may live in
 // shared or global memory.  Ends with a barrier.
-constexpr int kGemmTileDoubles = 2 * 16 * 65;
+constexpr int kTileLd = 68;
+constexpr int kGemmTileDoubles = 2 * 16 * kTileLd;
 
 __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int ldc0,
                                       const double* A, int lda, bool ta, const double* B,
                                       int ldb, bool tb, int m, int n, int kk, double* tile,
                                       double alpha = -1.0) {
-  double* sa = tile;            // [16][65]: sa[l * 65 + i] = op(A)(i0 + i, l0 + l)
-  double* sb = tile + 16 * 65;  // [16][65]: sb[l * 65 + j] = op(B)(l0 + l, j0 + j)
+  double* sa = tile;                 // [16][kTileLd]: sa[l kTileLd + i] = op(A)(i0 + i, l0 + l)
+  double* sb = tile + 16 * kTileLd;  // [16][kTileLd]: sb[l kTileLd + j] = op(B)(l0 + l, j0 + j)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;  // this warp's block in the tile
   const int fr = lane >> 2, fk = lane & 3;                 // fragment row / inner index
@@ -87,7 +90,7 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
           double va = 0.0;
           if (gi < m && gl < kk)
             va = ta ? A[gl + static_cast<long long>(lda) * gi] : A[gi + static_cast<long long>(lda) * gl];
-          sa[l * 65 + q] = va;
+          sa[l * kTileLd + q] = va;
           int qb, lb;
           if (tb) {  // op(B)(l, j) = B[j + ldb l]: output index fastest
             qb = e & 63;
@@ -100,12 +103,12 @@ __device__ inline void cta_gemm_tiled(double* C, int ldc, const double* C0, int 
           double vb = 0.0;
           if (gj < n && glb < kk)
             vb = tb ? B[gj + static_cast<long long>(ldb) * glb] : B[glb + static_cast<long long>(ldb) * gj];
-          sb[lb * 65 + qb] = vb;
+          sb[lb * kTileLd + qb] = vb;
         }
         __syncthreads();
 #pragma unroll
         for (int ks = 0; ks < 4; ks++) {
-          const int lrow = (ks * 4 + fk) * 65;
+          const int lrow = (ks * 4 + fk) * kTileLd;
           double af[4], bf[2];
 #pragma unroll
           for (int a = 0; a < 4; a++) af[a] = sa[lrow + wm + 8 * a + fr];
@@ -401,67 +404,108 @@ __device__ inline void warp_lu_solve_t(const double* lu, int n, int ld, const in
 // L) and backward (U) substitution in 32-row blocks; warp 0 solves each
 // diagonal block from registers, then every thread updates its rows with
 // the block's 32 values.  Ends with a barrier.
+// x (length n, in shared memory) <- A^{-1} x for the LU above, by the whole
+// CTA, in 32-row blocks.  ipiv: the row interchanges, applied first in
+// order (nullptr: x is already permuted); piv_smem (optional, n ints of
+// shared memory) stages ipiv so that the sequential interchanges wait on
+// shared memory, not on a global load each.  Per block: the diagonal
+// triangle by warp 0 in registers (loaded one block ahead, during the
+// previous block's update), then the update of the remaining rows, a
+// thread per row with the block's 32 entries requested at once.
 __device__ inline void cta_lu_solve(const double* __restrict__ lu, int n, int ld,
-                                    const int* __restrict__ ipiv, double* x) {
+                                    const int* __restrict__ ipiv, double* x,
+                                    int* piv_smem = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0)
-    for (int i = 0; i < n; i++) {
-      const int p = ipiv[i];
-      // (a pivot out of range, left by an LU that stopped early, is skipped)
-      if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
-        const double t = x[i];
-        x[i] = x[p];
-        x[p] = t;
-      }
+  if (ipiv) {
+    const int* pv = ipiv;
+    if (piv_smem) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) piv_smem[i] = ipiv[i];
+      __syncthreads();
+      pv = piv_smem;
     }
+    if (threadIdx.x == 0)
+      for (int i = 0; i < n; i++) {
+        const int p = pv[i];
+        // (a pivot out of range, left by an LU that stopped early, is skipped)
+        if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
+          const double t = x[i];
+          x[i] = x[p];
+          x[p] = t;
+        }
+      }
+  }
   __syncthreads();
+  auto lower_block = [&](int kb, double* Lr) {  // warp 0: rows kb.., strictly lower
+    const int nbk = min(32, n - kb);
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      Lr[k] = (lane < nbk && k < lane) ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)]
+                                       : 0.0;
+  };
+  double Dr[32];
+  if (warp == 0) lower_block(0, Dr);
   for (int kb = 0; kb < n; kb += 32) {  // L y = P b
     const int nbk = min(32, n - kb);
     if (warp == 0) {
-      double Lr[32];
-#pragma unroll
-      for (int k = 0; k < 32; k++)
-        Lr[k] = (lane < nbk && k < lane) ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)] : 0.0;
       double xv = lane < nbk ? x[kb + lane] : 0.0;
 #pragma unroll
       for (int k = 0; k < 32; k++) {
         const double xk = __shfl_sync(0xffffffffu, xv, k);
-        xv -= Lr[k] * xk;  // Lr[k] = 0 unless k < lane
+        xv -= Dr[k] * xk;  // Dr[k] = 0 unless k < lane
       }
       if (lane < nbk) x[kb + lane] = xv;
     }
     __syncthreads();
+    if (warp == 0 && kb + 32 < n) lower_block(kb + 32, Dr);
     for (int i = kb + nbk + threadIdx.x; i < n; i += blockDim.x) {
+      double l[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+        l[k] = k < nbk ? lu[i + static_cast<long long>(ld) * (kb + k)] : 0.0;
       double s = 0.0;
-      for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(ld) * (kb + k)] * x[kb + k];
+#pragma unroll
+      for (int k = 0; k < 32; k++) s += l[k] * x[kb + (k < nbk ? k : 0)];
       x[i] -= s;
     }
     __syncthreads();
   }
-  for (int kb = ((n - 1) / 32) * 32; kb >= 0; kb -= 32) {  // U x = y
+  auto upper_block = [&](int kb, double* Ur, double* rd) {  // warp 0
+    const int nbk = min(32, n - kb);
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+      Ur[k] = (lane < nbk && k < nbk && k > lane)
+                  ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)]
+                  : 0.0;
+    // the diagonal's reciprocal, formed off the substitution's chain
+    *rd = lane < nbk ? 1.0 / lu[kb + lane + static_cast<long long>(ld) * (kb + lane)] : 0.0;
+  };
+  const int kb_last = ((n - 1) / 32) * 32;
+  double rd = 0.0;
+  if (warp == 0 && n > 0) upper_block(kb_last, Dr, &rd);
+  for (int kb = kb_last; kb >= 0; kb -= 32) {  // U x = y
     const int nbk = min(32, n - kb);
     if (warp == 0) {
-      double Ur[32];
-#pragma unroll
-      for (int k = 0; k < 32; k++)
-        Ur[k] = (lane < nbk && k < nbk && k >= lane)
-                    ? lu[kb + lane + static_cast<long long>(ld) * (kb + k)]
-                    : 0.0;
       double xv = lane < nbk ? x[kb + lane] : 0.0;
 #pragma unroll
       for (int k = 31; k >= 0; k--) {
         if (k < nbk) {
-          if (lane == k) xv /= Ur[k];
+          if (lane == k) xv *= rd;
           const double xk = __shfl_sync(0xffffffffu, xv, k);
-          if (lane < k) xv -= Ur[k] * xk;
+          xv -= Dr[k] * xk;  // Dr[k] = 0 unless lane < k
         }
       }
       if (lane < nbk) x[kb + lane] = xv;
     }
     __syncthreads();
+    if (warp == 0 && kb > 0) upper_block(kb - 32, Dr, &rd);
     for (int i = threadIdx.x; i < kb; i += blockDim.x) {
+      double u[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++)
+        u[k] = k < nbk ? lu[i + static_cast<long long>(ld) * (kb + k)] : 0.0;
       double s = 0.0;
-      for (int k = 0; k < nbk; k++) s += lu[i + static_cast<long long>(ld) * (kb + k)] * x[kb + k];
+#pragma unroll
+      for (int k = 0; k < 32; k++) s += u[k] * x[kb + (k < nbk ? k : 0)];
       x[i] -= s;
     }
     __syncthreads();

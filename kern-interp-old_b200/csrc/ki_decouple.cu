@@ -74,23 +74,26 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   // X = (K_rr - T^T K_sr) - K_r_sn T
   cta_gemm_tiled(X, r, Krr, n, T, k, true, Ksr, n, false, r, r, k, tile);
   cta_gemm_tiled(X, r, X, r, U, r, false, T, k, false, r, r, k, tile);
-  // K is done with: stage X, K_r_sn and K_sn_r in its place (r^2 + 2 k r
-  // <= n^2) and invert X there (Gauss-Jordan, partial pivoting)
+  // K is done with: stage X, K_r_sn and K_sn_r in its place (r ldx + 2 k r
+  // <= n^2) and invert X there (Gauss-Jordan, partial pivoting).  X's
+  // leading dimension is odd where that fits (r <= k^2): the elimination's
+  // row operations, a thread per column, then hit distinct banks
+  const int ldx = (r | 1) * r + 2 * k * r <= n * n ? (r | 1) : r;
   double* Xw = kbuf;
-  double* Krsn = Xw + r * r;    // r x k
+  double* Krsn = Xw + ldx * r;  // r x k
   double* Ksnr = Krsn + r * k;  // k x r
-  for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e] = X[e];
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e % r + ldx * (e / r)] = X[e];
   for (int e = threadIdx.x; e < r * k; e += kDecThreads) {
     Krsn[e] = U[e];
     Ksnr[e] = L[e];
   }
   __syncthreads();
-  const int info = cta_gj_invert(Xw, r, r, piv, tile, red);
+  const int info = cta_gj_invert(Xw, r, ldx, piv, tile, red);
   if (info && threadIdx.x == 0) atomicExch(P.status, 1);
-  for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e];
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e % r + ldx * (e / r)];
   // U = X^{-1} K_r_sn,  L = K_sn_r X^{-1}
-  cta_gemm_tiled(U, r, nullptr, 0, Xw, r, false, Krsn, r, false, r, k, r, tile, 1.0);
-  cta_gemm_tiled(L, k, nullptr, 0, Ksnr, k, false, Xw, r, false, k, r, r, tile, 1.0);
+  cta_gemm_tiled(U, r, nullptr, 0, Xw, ldx, false, Krsn, r, false, r, k, r, tile, 1.0);
+  cta_gemm_tiled(L, k, nullptr, 0, Ksnr, k, false, Xw, ldx, false, k, r, r, tile, 1.0);
   // acc = update(s, s) + L K_r_sn
   cta_gemm_tiled(acc, k, nullptr, 0, L, k, false, Krsn, r, false, k, k, r, tile, 1.0);
   for (int e = threadIdx.x; e < k * k; e += kDecThreads) {

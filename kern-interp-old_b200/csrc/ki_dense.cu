@@ -622,12 +622,15 @@ __global__ void __launch_bounds__(256) trailing_kernel(double* a, int n, int ld,
       }
 }
 
-// B <- A^{-1} B, one CTA per right-hand side, the vector in shared memory.
+// B <- A^{-1} B, one CTA per right-hand side, the vector in shared memory
+// (then n ints staging the pivots).  perm (optional): the interchanges
+// composed into one permutation (pivots_to_perm), applied as a gather.
 constexpr int kSolveThreads = 512;
 __global__ void __launch_bounds__(kSolveThreads)
     lu_solve_cta_kernel(const double* __restrict__ lu, int n, int ld, const int* __restrict__ ipiv,
-                        double* b, int ldb) {
+                        const int* __restrict__ perm, double* b, int ldb) {
   extern __shared__ double x[];
+  int* pv = reinterpret_cast<int*>(x + n);
   double* bc = b + static_cast<long long>(ldb) * blockIdx.x;
   // the whole LU into L2 up front (one prefetch per 128-byte line): the
   // blocked substitutions then wait on L2, not HBM, at every block step
@@ -639,9 +642,13 @@ __global__ void __launch_bounds__(kSolveThreads)
       if (16 * q < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
     }
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[i];
+  if (perm) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[perm[i]];
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[i];
+  }
   __syncthreads();
-  cta_lu_solve(lu, n, ld, ipiv, x);
+  cta_lu_solve(lu, n, ld, perm ? nullptr : ipiv, x, pv);
   for (int i = threadIdx.x; i < n; i += blockDim.x) bc[i] = x[i];
 }
 
@@ -1263,17 +1270,56 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
   return cudaGetLastError();
 }
 
+// The row interchanges of an LU composed into one permutation: (P b)[i] =
+// b[perm[i]].  One thread walks the interchanges in order over shared
+// memory (the pivots staged there first).
+__global__ void pivots_to_perm_kernel(const int* __restrict__ ipiv, int n, int* perm) {
+  extern __shared__ int sh[];
+  int* pv = sh;
+  int* idx = sh + n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    pv[i] = ipiv[i];
+    idx[i] = i;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int i = 0; i < n; i++) {
+      const int p = pv[i];
+      if (p != i && static_cast<unsigned>(p) < static_cast<unsigned>(n)) {
+        const int t = idx[i];
+        idx[i] = idx[p];
+        idx[p] = t;
+      }
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = idx[i];
+}
+
+cudaError_t launch_pivots_to_perm(const int* ipiv, int n, int* perm, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const size_t smem = 2 * sizeof(int) * static_cast<size_t>(n);
+  if (smem > 48 * 1024) {
+    const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&pivots_to_perm_kernel),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+  }
+  count_launches(1);
+  pivots_to_perm_kernel<<<1, 256, smem, s>>>(ipiv, n, perm);
+  return cudaGetLastError();
+}
+
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
-                           int nrhs, int ldb, cudaStream_t s) {
+                           int nrhs, int ldb, cudaStream_t s, const int* perm) {
   if (n == 0 || nrhs == 0) return cudaSuccess;
   count_launches(1);
-  const size_t smem = sizeof(double) * static_cast<size_t>(n);
+  const size_t smem = (sizeof(double) + sizeof(int)) * static_cast<size_t>(n);
   if (n >= 64 && smem <= kSolveSmemMax) {
     const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_solve_cta_kernel),
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kSolveSmemMax);
     if (e != cudaSuccess) return e;
-    lu_solve_cta_kernel<<<nrhs, kSolveThreads, smem, s>>>(lu, n, ld, ipiv, b, ldb);
+    lu_solve_cta_kernel<<<nrhs, kSolveThreads, smem, s>>>(lu, n, ld, ipiv, perm, b, ldb);
     return cudaGetLastError();
   }
   const int per = 4;

@@ -145,6 +145,8 @@ struct DecParams {
 // Boxes with n > kDecoupleSmemN must go through decouple_large instead.
 constexpr int kDecoupleSmemN = 160;
 cudaError_t launch_decouple(const DecParams& p, int n_max, cudaStream_t s);
+// Dynamic shared memory of a decouple launch whose largest box has n_max dofs.
+size_t decouple_smem_bytes(int n_max);
 // The same decoupling for one large box as a sequence of GPU-wide kernels
 // (tk is the host copy of the box's descriptor; tk.K must hold n x n).
 cudaError_t decouple_large(const DecTask& tk, int pde, const Node* nodes, int* status,
@@ -206,9 +208,13 @@ cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, cons
 // Each of the nrows rows of B (column stride ldb) <- row * A^{-1}.
 cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv, double* b,
                                 int nrows, int ldb, cudaStream_t s);
-// B <- A^{-1} B (n x nrhs, ldb) for the LU above.
+// B <- A^{-1} B (n x nrhs, ldb) for the LU above; perm (optional, from
+// launch_pivots_to_perm) replaces the sequential interchanges by a gather.
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
-                           int nrhs, int ldb, cudaStream_t s);
+                           int nrhs, int ldb, cudaStream_t s, const int* perm = nullptr);
+// The interchanges ipiv[0..n) of an LU composed into one permutation:
+// (P b)[i] = b[perm[i]].
+cudaError_t launch_pivots_to_perm(const int* ipiv, int n, int* perm, cudaStream_t s);
 
 // Border blocks of the bordered top-level system S (ld >= ns + nb).
 cudaError_t launch_fill_border(double* S, int ld, int ns, int nb, const double* us,

@@ -479,6 +479,17 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
     }
     for (int G = 0; G <= 16; G++) onchip_ok_[G] = it->second[G];
   }
+  if (!num_sms_) {
+    int dev = 0;
+    KI_CUDA(cudaGetDevice(&dev));
+    KI_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+  }
+  if (!smem_per_sm_) {
+    int dev = 0;
+    KI_CUDA(cudaGetDevice(&dev));
+    KI_CUDA(cudaDeviceGetAttribute(&smem_per_sm_, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                   dev));
+  }
   return 0;
 }
 
@@ -677,6 +688,7 @@ int Solver::id_launch(int level, PendingLevel* pl) {
     for (int q = a; q < e; q++)
       if (!tree.boxes[ids[q]].compressed) tree.refresh_box(ids[q]);
   });
+  mark(9, level);
   const int P = sd_ == 2 ? 4 * kNumProxy : 2 * kNumProxy;
 
   using Cand = IdCand;
@@ -737,10 +749,19 @@ int Solver::id_launch(int level, PendingLevel* pl) {
       if (c.m == 0) continue;
       c.g = pick_group(c.m, c.n, onchip_ok_);
       if (opt_.sketch_id) {
-        // the smallest cluster whose CTAs' shares of the sketch leave room
-        // for two CTAs per SM (a single CTA per SM leaves the SM idle at
-        // every barrier of the pivoted QR), else the smallest that fits
+        // A level whose boxes, each spread over the widest cluster that
+        // still leaves a CTA 12 columns, fit one wave at two CTAs per SM
+        // takes that width: the pivoted QR's steps shrink with the columns
+        // a CTA owns (measured on a B200, the Stokes workload's level-2
+        // IDs: 0.96 -> 0.72 ms).  Otherwise the smallest cluster whose
+        // CTAs' shares of the sketch leave room for two CTAs per SM (a
+        // single CTA per SM leaves the SM idle at every barrier of the
+        // pivoted QR), else the smallest that fits.
         auto fit = [&](int l) {  // cluster size for an l-row sketch, 0: none
+          for (int G = 16; G >= 2; G /= 2)
+            if (onchip_ok_[G] && c.n >= 12 * G && nids * G <= 2 * num_sms_ &&
+                id_sketch_smem_bytes(l, c.n, G) <= size_t{113} * 1024)
+              return G;
           for (const size_t cap : {size_t{113} * 1024, size_t{227} * 1024})
             for (int G = 1; G <= 16; G *= 2)
               if (onchip_ok_[G] && id_sketch_smem_bytes(l, c.n, G) <= cap) return G;
@@ -767,6 +788,7 @@ int Solver::id_launch(int level, PendingLevel* pl) {
       keep[q] = 1;
     }
   });
+  mark(10, level);
   std::vector<Cand>& cand = pl->cand;
   for (int q = 0; q < nids; q++)
     if (keep[q]) cand.push_back(std::move(all[q]));
@@ -789,6 +811,7 @@ int Solver::id_launch(int level, PendingLevel* pl) {
     return static_cast<long long>(a.m) * a.n > static_cast<long long>(b.m) * b.n;
   });
 
+  mark(11, level);
   const int nc = static_cast<int>(cand.size());
   std::vector<IdTask>& tasks = pl->tasks;
   tasks.assign(nc, IdTask{});
@@ -1237,11 +1260,12 @@ int Solver::decouple_boxes(PendingLevel* pl) {
   mark(3, level);
   if (time_phases && timer_begin(&d0, dstream_)) return -2;
   // The batched boxes in size classes, one launch each: a launch's shared
-  // memory is sized by its largest box, so the small boxes of a level get
-  // three CTAs per SM (n <= 86), the middle ones two (n <= 110), and only
-  // the largest one (72 registers x 256 threads leave room for three); the widest class on dstream_, the others and the large
-  // boxes (one multi-kernel sequence each) side by side on their own
-  // streams after the level's uploads, joined back into dstream_.
+  // memory is sized by its largest box, so the boxes of a level are grouped
+  // by how many CTAs of theirs an SM holds (three at most: 72 registers x
+  // 256 threads; on a B200 n <= 85 gives three, n <= 110 two); the widest
+  // class on dstream_, the others and the large boxes (one multi-kernel
+  // sequence each) side by side on their own streams after the level's
+  // uploads, joined back into dstream_.
   KI_CUDA(cudaEventRecord(dl_fork_, dstream_));
   bool used[kDecStreams] = {};
   int next_side = 0;
@@ -1254,7 +1278,10 @@ int Solver::decouple_boxes(PendingLevel* pl) {
     *out = dl_streams_[si];
     return 0;
   };
-  auto size_class = [](int n) { return n > 110 ? 0 : n > 86 ? 1 : 2; };
+  auto size_class = [&](int n) {
+    // (1 KB of each CTA's shared memory is reserved by the system)
+    return std::min<size_t>(3, static_cast<size_t>(smem_per_sm_) / (decouple_smem_bytes(n) + 1024));
+  };
   for (size_t a = 0; a < small.size();) {
     size_t b = a;
     while (b < small.size() && size_class(small[b].n) == size_class(small[a].n)) b++;
@@ -1342,6 +1369,7 @@ void Solver::drop_device_state() {
   d_forest_ = nullptr;
   d_top_ = nullptr;
   d_top_piv_ = nullptr;
+  d_top_perm_ = nullptr;
   d_allskel_ = d_allred_ = d_red_pos_ = nullptr;
   d_U_ = d_Psi_ = d_Urow_ = d_Ured_ = d_Pred_ = d_tmp_ = nullptr;
   d_modU_ = d_modP_ = nullptr;
@@ -1601,6 +1629,7 @@ int Solver::factor_top() {
   solve_bytes += 8.0 * ntop * ntop + 8.0 * 8.0 * n_dofs_;
   KI_ALLOC(d_top_, double, static_cast<size_t>(ntop) * ntop);
   KI_ALLOC(d_top_piv_, int, ntop);
+  KI_ALLOC(d_top_perm_, int, ntop);
   KI_ALLOC(d_tmp_, double, 4 * static_cast<size_t>(n_dofs_ + ntop) + 64);
   KI_CUDA(launch_assemble_top(opt_.pde, d_nodes_, d_allskel_, ns_, d_bid, d_bpos, d_tab, d_top_,
                               ntop, stream_));
@@ -1614,6 +1643,8 @@ int Solver::factor_top() {
   KI_ALLOC(lu_sync, int, kLuSyncInts);
   if (ntop > 0)
     KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_, lu_sync, true));
+  // the interchanges composed once, so each solve gathers instead
+  if (ntop > 0) KI_CUDA(launch_pivots_to_perm(d_top_piv_, ntop, d_top_perm_, stream_));
   if (time_phases && timer_end(l0, {0, 4, 1, 1, 0, ntop, 0.0})) return -2;
   return 0;
 }
@@ -1692,7 +1723,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     KI_CUDA(launch_diag_solve(dp, stream_));
     if (ns > 0) {
       KI_CUDA(launch_gather(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
-      KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_));
+      KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_, d_top_perm_));
       KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
     }
   } else {
@@ -1718,7 +1749,8 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
       KI_CUDA(small_gemm(true, false, nb, 1, nr, -1.0, d_Pred_, nr, dw, nr, d_g ? 1.0 : 0.0,
                          M + ns, nb, stream_));
     }
-    KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_));
+    KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_,
+                           d_top_perm_));
     if (d_alpha)
       KI_CUDA(cudaMemcpyAsync(d_alpha, M + ns, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
                               stream_));

@@ -235,7 +235,8 @@ class Solver {
   };
   std::vector<LaunchRecord> launch_log;
   // Host side of the timed factorization: code (7 geometry queued, 8
-  // partition built, 0 tree checked, 1 level lists ready / ID launched, 2
+  // partition built, 0 tree checked, 9 a level's active lists, 10 its ID
+  // rows, 11 its ID groups ordered, 1 level lists ready / ID launched, 2
   // ranks received, 3 decouple launched, 4 top level started, 5 top level
   // launched, 6 factorization synchronised), level,
   // ms after the factorization began (host clock).
@@ -375,6 +376,7 @@ class Solver {
   int ns_ = 0;
   double* d_top_ = nullptr;  // LU of allskel_mat, or of S with holes
   int* d_top_piv_ = nullptr;
+  int* d_top_perm_ = nullptr;  // the top LU's interchanges as one permutation
   int* d_allskel_ = nullptr;
   int* d_allred_ = nullptr;
   int* d_red_pos_ = nullptr;
@@ -406,6 +408,7 @@ class Solver {
   std::vector<int> seg_;
   double* h_kry_ = nullptr;  // pinned host copy of the Arnoldi coefficients
   int num_sms_ = 0;
+  int smem_per_sm_ = 0;  // shared memory of an SM, bytes
 };
 
 }  // namespace kib

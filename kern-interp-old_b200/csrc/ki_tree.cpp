@@ -52,6 +52,7 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   struct Tmp {
     int parent = -1, level = 0, child[4] = {-1, -1, -1, -1};
     int begin = 0, count = 0;
+    long long moment = -1;  // a split box's (cap+1)-th point, in index order
     double corner[8];
   };
   std::vector<Tmp> tb(1);
@@ -85,106 +86,167 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
     pxy[2 * q] = pts_[2 * static_cast<size_t>(p0 + q)];
     pxy[2 * q + 1] = pts_[2 * static_cast<size_t>(p0 + q) + 1];
   }
-  std::vector<long long> moment(1, -1);  // index of a split box's (cap+1)-th point
   const int cap = max_leaf_ / sol_dim_;  // split when a box holds more points
+  // Box P's range into its four children ch[0..3] (ranges, corners, level;
+  // the caller links them): classify the points by child, then a stable
+  // scatter from a copy of the range.  A big box (the first levels) is cut
+  // into chunks classified and scattered in parallel at per-chunk offsets
+  // (chunks in order, sequential inside: still stable).
+  auto split_one = [&](Tmp& P, Tmp* ch, bool inner_parallel) {
+    const int b0 = P.begin, cnt_all = P.count;
+    int* rp = perm.data() + b0;
+    double* rxy = pxy.data() + 2 * static_cast<size_t>(b0);
+    P.moment = rp[cap];  // the range is still in index order
+    const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
+    const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
+    const int kChunk = 4096;
+    const int nch = inner_parallel ? (cnt_all + kChunk - 1) / kChunk : 1;
+    const int csz = inner_parallel ? kChunk : cnt_all;
+    std::array<int, 4> ccnt1{0, 0, 0, 0}, cpos1{};
+    std::vector<std::array<int, 4>> ccntv, cposv;
+    if (nch > 1) {
+      ccntv.assign(nch, std::array<int, 4>{0, 0, 0, 0});
+      cposv.resize(nch);
+    }
+    std::array<int, 4>* ccnt = nch > 1 ? ccntv.data() : &ccnt1;
+    std::array<int, 4>* cpos = nch > 1 ? cposv.data() : &cpos1;
+    auto classify = [&](int c0, int c1) {
+      for (int c = c0; c < c1; c++) {
+        const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
+        for (int i = i0; i < i1; i++) {
+          const double x = rxy[2 * i], y = rxy[2 * i + 1];
+          const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
+          quad[b0 + i] = static_cast<unsigned char>(q);
+          ccnt[c][q]++;
+        }
+        std::memcpy(tmpi.data() + b0 + i0, rp + i0, sizeof(int) * (i1 - i0));
+        std::memcpy(tmpxy.data() + 2 * static_cast<size_t>(b0 + i0), rxy + 2 * i0,
+                    2 * sizeof(double) * (i1 - i0));
+      }
+    };
+    if (nch > 1) parallel_for(nch, 1, classify, 2); else classify(0, 1);
+    int cnt[4] = {0, 0, 0, 0};
+    for (int c = 0; c < nch; c++)
+      for (int q = 0; q < 4; q++) cnt[q] += ccnt[c][q];
+    int pos[4];
+    pos[0] = 0;
+    for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
+    {
+      // each chunk's first destination per child
+      int run[4] = {pos[0], pos[1], pos[2], pos[3]};
+      for (int c = 0; c < nch; c++)
+        for (int q = 0; q < 4; q++) {
+          cpos[c][q] = run[q];
+          run[q] += ccnt[c][q];
+        }
+    }
+    const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
+                             {mx, my, mx, my}, {mx, mx, my, my}};
+    for (int q = 0; q < 4; q++) {
+      Tmp& C = ch[q];
+      C.level = P.level + 1;
+      C.begin = b0 + pos[q];
+      C.count = cnt[q];
+      std::memcpy(C.corner, P.corner, sizeof(C.corner));
+      for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
+    }
+    const int* oi = tmpi.data() + b0;
+    const double* oxy = tmpxy.data() + 2 * static_cast<size_t>(b0);
+    auto scatter = [&](int c0, int c1) {
+      for (int c = c0; c < c1; c++) {
+        int at[4] = {cpos[c][0], cpos[c][1], cpos[c][2], cpos[c][3]};
+        const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
+        for (int i = i0; i < i1; i++) {
+          const int d = at[quad[b0 + i]]++;
+          rp[d] = oi[i];
+          rxy[2 * d] = oxy[2 * i];
+          rxy[2 * d + 1] = oxy[2 * i + 1];
+        }
+      }
+    };
+    if (nch > 1) parallel_for(nch, 1, scatter, 2); else scatter(0, 1);
+  };
+  // The first levels level by level (a few big boxes: each split in
+  // parallel chunks, or side by side), until the frontier holds enough
+  // boxes to keep every thread busy; then each frontier box's subtree by
+  // one thread, breadth first into its own list, appended after the
+  // others (parents keep smaller indices than their children, all that the
+  // numbering below relies on).
+  const int seeds = 4 * pool_threads();
   std::vector<int> frontier{0};
-  while (!frontier.empty()) {
+  while (!frontier.empty() && static_cast<int>(frontier.size()) < seeds) {
     std::vector<int> split;
     for (int id : frontier)
       if (tb[id].count > cap) split.push_back(id);
-    if (split.empty()) break;
+    if (split.empty()) {
+      frontier.clear();
+      break;
+    }
     const int base = static_cast<int>(tb.size());
     tb.resize(base + 4 * split.size());
-    moment.resize(tb.size(), -1);
-    // one box: classify its points by child, then a stable scatter from a
-    // copy of the range; a big box (the first levels) is cut into chunks
-    // classified and scattered in parallel at per-chunk offsets (chunks in
-    // order, sequential inside: still stable)
-    auto split_box = [&](int s, bool inner_parallel) {
-      Tmp& P = tb[split[s]];
-      const int b0 = P.begin, cnt_all = P.count;
-      int* rp = perm.data() + b0;
-      double* rxy = pxy.data() + 2 * static_cast<size_t>(b0);
-      moment[split[s]] = rp[cap];  // the range is still in index order
-      const double mx = ((P.corner[6] - P.corner[0]) / 2.0) + P.corner[0];
-      const double my = ((P.corner[3] - P.corner[1]) / 2.0) + P.corner[1];
-      const int kChunk = 4096;
-      const int nch = inner_parallel ? (cnt_all + kChunk - 1) / kChunk : 1;
-      const int csz = inner_parallel ? kChunk : cnt_all;
-      std::vector<std::array<int, 4>> ccnt(nch, std::array<int, 4>{0, 0, 0, 0});
-      auto classify = [&](int c0, int c1) {
-        for (int c = c0; c < c1; c++) {
-          const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
-          for (int i = i0; i < i1; i++) {
-            const double x = rxy[2 * i], y = rxy[2 * i + 1];
-            const int q = x < mx ? (y < my ? 0 : 1) : (y < my ? 3 : 2);  // quadtree.cpp:171-185
-            quad[b0 + i] = static_cast<unsigned char>(q);
-            ccnt[c][q]++;
-          }
-          std::memcpy(tmpi.data() + b0 + i0, rp + i0, sizeof(int) * (i1 - i0));
-          std::memcpy(tmpxy.data() + 2 * static_cast<size_t>(b0 + i0), rxy + 2 * i0,
-                      2 * sizeof(double) * (i1 - i0));
-        }
-      };
-      if (inner_parallel) parallel_for(nch, 1, classify, 2); else classify(0, 1);
-      int cnt[4] = {0, 0, 0, 0};
-      for (int c = 0; c < nch; c++)
-        for (int q = 0; q < 4; q++) cnt[q] += ccnt[c][q];
-      int pos[4];
-      pos[0] = 0;
-      for (int q = 1; q < 4; q++) pos[q] = pos[q - 1] + cnt[q - 1];
-      // each chunk's first destination per child
-      std::vector<std::array<int, 4>> cpos(nch);
-      {
-        int run[4] = {pos[0], pos[1], pos[2], pos[3]};
-        for (int c = 0; c < nch; c++)
-          for (int q = 0; q < 4; q++) {
-            cpos[c][q] = run[q];
-            run[q] += ccnt[c][q];
-          }
-      }
-      const double ev[4][4] = {{my, mx, my, mx}, {my, mx, mx, my},
-                               {mx, my, mx, my}, {mx, mx, my, my}};
+    auto link = [&](int s) {
       for (int q = 0; q < 4; q++) {
-        Tmp& C = tb[base + 4 * s + q];
-        C.parent = split[s];
-        C.level = P.level + 1;
-        C.begin = b0 + pos[q];
-        C.count = cnt[q];
-        std::memcpy(C.corner, P.corner, sizeof(C.corner));
-        for (int e2 = 0; e2 < 4; e2++) C.corner[kEditIdx[q][e2]] = ev[q][e2];
-        P.child[q] = base + 4 * s + q;
+        tb[base + 4 * s + q].parent = split[s];
+        tb[split[s]].child[q] = base + 4 * s + q;
       }
-      const int* oi = tmpi.data() + b0;
-      const double* oxy = tmpxy.data() + 2 * static_cast<size_t>(b0);
-      auto scatter = [&](int c0, int c1) {
-        for (int c = c0; c < c1; c++) {
-          int at[4] = {cpos[c][0], cpos[c][1], cpos[c][2], cpos[c][3]};
-          const int i0 = c * csz, i1 = std::min(cnt_all, i0 + csz);
-          for (int i = i0; i < i1; i++) {
-            const int d = at[quad[b0 + i]]++;
-            rp[d] = oi[i];
-            rxy[2 * d] = oxy[2 * i];
-            rxy[2 * d + 1] = oxy[2 * i + 1];
-          }
-        }
-      };
-      if (inner_parallel) parallel_for(nch, 1, scatter, 2); else scatter(0, 1);
     };
     std::vector<int> small_ones;
     for (int s = 0; s < static_cast<int>(split.size()); s++) {
       if (tb[split[s]].count >= 16384) {
-        split_box(s, true);
+        split_one(tb[split[s]], &tb[base + 4 * s], true);
+        link(s);
       } else {
         small_ones.push_back(s);
       }
     }
     // every box is real work: spread even a handful of them
     parallel_for(static_cast<int>(small_ones.size()), 1, [&](int a, int e) {
-      for (int q = a; q < e; q++) split_box(small_ones[q], false);
+      for (int q = a; q < e; q++) {
+        split_one(tb[split[small_ones[q]]], &tb[base + 4 * small_ones[q]], false);
+        link(small_ones[q]);
+      }
     }, 2);
     frontier.clear();
     for (size_t i = base; i < tb.size(); i++) frontier.push_back(static_cast<int>(i));
+  }
+  if (!frontier.empty()) {
+    const int nf = static_cast<int>(frontier.size());
+    std::vector<std::vector<Tmp>> sub(nf);
+    parallel_for(nf, 1, [&](int a, int e) {
+      for (int f = a; f < e; f++) {
+        std::vector<Tmp>& loc = sub[f];
+        loc.push_back(tb[frontier[f]]);  // [0]: the seed
+        for (size_t q = 0; q < loc.size(); q++) {
+          if (loc[q].count <= cap) continue;
+          const size_t base = loc.size();
+          loc.resize(base + 4);
+          split_one(loc[q], &loc[base], false);
+          for (int c = 0; c < 4; c++) {
+            loc[base + c].parent = static_cast<int>(q);
+            loc[q].child[c] = static_cast<int>(base + c);
+          }
+        }
+      }
+    }, 2);
+    // seed f keeps its index; its local box j >= 1 becomes off[f] + j - 1
+    std::vector<int> off(nf + 1);
+    off[0] = static_cast<int>(tb.size());
+    for (int f = 0; f < nf; f++) off[f + 1] = off[f] + static_cast<int>(sub[f].size()) - 1;
+    tb.resize(off[nf]);
+    parallel_for(nf, 4, [&](int a, int e) {
+      for (int f = a; f < e; f++) {
+        const std::vector<Tmp>& loc = sub[f];
+        auto gid = [&](int j) { return j == 0 ? frontier[f] : off[f] + j - 1; };
+        for (size_t j = 0; j < loc.size(); j++) {
+          Tmp& t = tb[gid(static_cast<int>(j))];
+          const int parent = t.parent;
+          t = loc[j];
+          t.parent = j == 0 ? parent : gid(loc[j].parent);
+          for (int q = 0; q < 4; q++)
+            if (loc[j].child[q] >= 0) t.child[q] = gid(loc[j].child[q]);
+        }
+      }
+    });
   }
   // split moments: s(B) = max(index of B's (cap+1)-th point, s(parent));
   // depth-first positions from an explicit pre-order walk
@@ -205,7 +267,7 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   std::vector<int> splits;
   for (int id = 0; id < nt; id++) {
     if (tb[id].child[0] < 0) continue;
-    long long t = moment[id];
+    long long t = tb[id].moment;
     if (tb[id].parent >= 0) t = std::max(t, when[tb[id].parent]);
     when[id] = t;
     splits.push_back(id);
