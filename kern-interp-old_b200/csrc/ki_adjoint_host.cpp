@@ -25,11 +25,12 @@ int Solver::solve_transpose_device(const double* d_b, double* d_x) {
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
     SweepParams sp{lf.d_tasks, lf.ntasks, d_x, N, 1, 0, nullptr, lf.cap};
+    sp.kr = lf.kr;
     KI_CUDA(launch_sweep_up(sp, true, stream_));
   }
   SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, d_x, N, 1, 0, nullptr,
                  all_compressed_.cap};
-  KI_CUDA(launch_diag_solve_t(dp, stream_));
+  if (diag_all(dp, true)) return -2;
   const int ns = ns_;
   if (ns > 0) {
     KI_CUDA(launch_gather(d_x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
@@ -40,6 +41,7 @@ int Solver::solve_transpose_device(const double* d_b, double* d_x) {
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
     SweepParams sp{lf.d_tasks, lf.ntasks, d_x, N, 1, 0, nullptr, lf.cap};
+    sp.kr = lf.kr;
     KI_CUDA(launch_transposed_up(sp, stream_));
   }
   return 0;

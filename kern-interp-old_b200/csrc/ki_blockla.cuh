@@ -222,111 +222,96 @@ __device__ inline int cta_lu(double* a, int n, int ld, int* ipiv, double* red) {
   return info;
 }
 
-// In-place inverse of the n x n matrix a (leading dimension ld) by
-// Gauss-Jordan elimination with partial pivoting over the CTA: at step j the
-// first-maximum |a(i, j)|, i >= j, is swapped into row j (ipiv[j] records
-// it), row j is scaled by the pivot's reciprocal and column j eliminated
-// from every other row; the row interchanges are undone as column
-// interchanges in reverse order at the end.  `col` needs n doubles, `red`
-// 64.  Returns nonzero if an exactly zero pivot was met.
-__device__ inline int cta_gj_invert(double* a, int n, int ld, int* ipiv, double* col,
-                                    double* red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  int* redi = reinterpret_cast<int*>(red + 32);
+// Warp argmax of non-negative doubles (first index on ties) with three
+// integer reductions instead of shuffle rounds: a non-negative double's bit
+// pattern orders like the value, so the maximum is found on its high word,
+// then its low word, then the smallest index holding it.  A lane with no
+// candidate passes key 0 and index INT_MAX.
+__device__ __forceinline__ void warp_argmax_bits(unsigned long long key, int idx,
+                                                 unsigned long long* kmax, int* imin) {
+  const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  *imin = static_cast<int>(__reduce_min_sync(0xffffffffu, top ? static_cast<unsigned>(idx)
+                                                              : 0x7fffffffu));
+  *kmax = (static_cast<unsigned long long>(mhi) << 32) | mlo;
+}
+
+// Gauss-Jordan inversion of the n x n matrix a (column-major, ld; n <=
+// blockDim.x, a thread per row) in place, partial pivoting, one barrier per
+// pivot step.  Rows are never exchanged: step j eliminates column j with
+// the row p_j (the largest |a(i, j)| among the rows not yet pivots, the
+// first on ties; a NaN counts as 0), every other row i updating itself as
+// a(i, :) -= (a(i, j) / a(p_j, j)) a(p_j, :) with a(i, j) <- -a(i, j) /
+// a(p_j, j) (the in-place trick), while row p_j waits until the next
+// step's barrier, when nobody reads it any more, to scale itself by the
+// reciprocal it kept.  Before the barrier each warp publishes its best
+// candidate (key, row) in a slot double-buffered by step parity; after it
+// every thread reduces the slots to the same p_j.  On return the result B
+// holds A^{-1}(j, q) = B(p_j, p^{-1}(q)); pivot_row[j] = p_j.  Returns
+// nonzero when a pivot was 0, infinite or NaN.  Slots: 2 x 32 keys and rows.
+__device__ inline int cta_gj_invert_inplace(double* a, int n, int ld, int* pivot_row,
+                                            unsigned long long* slot_key, int* slot_row) {
+  const int i = threadIdx.x, lane = i & 31, warp = i >> 5, nw = blockDim.x >> 5;
+  bool used = false, pending = false;
+  int jprev = 0;
+  double own_inv = 0.0;
   int info = 0;
   for (int j = 0; j < n; j++) {
-    double bv = -1.0;
-    int bp = 0x7fffffff;
-    for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
-      const double v = fabs(a[i + static_cast<long long>(ld) * j]);
-      if (v > bv || (v == bv && i < bp)) {
-        bv = v;
-        bp = i;
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int op = __shfl_xor_sync(0xffffffffu, bp, o);
-      if (ov > bv || (ov == bv && op < bp)) {
-        bv = ov;
-        bp = op;
-      }
-    }
+    const int buf = j & 1;
+    const bool cand = i < n && !used;
+    double v = cand ? fabs(a[i + static_cast<long long>(ld) * j]) : 0.0;
+    if (v != v) v = 0.0;
+    unsigned long long wk;
+    int wi;
+    warp_argmax_bits(cand ? static_cast<unsigned long long>(__double_as_longlong(v)) : 0ull,
+                     cand ? i : 0x7fffffff, &wk, &wi);
     if (lane == 0) {
-      red[warp] = bv;
-      redi[warp] = bp;
+      slot_key[32 * buf + warp] = wk;
+      slot_row[32 * buf + warp] = wi;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double v = red[0];
-      int p = redi[0];
-      for (int w = 1; w < nw; w++)
-        if (red[w] > v || (red[w] == v && redi[w] < p)) {
-          v = red[w];
-          p = redi[w];
-        }
-      // no comparable entry (a NaN column): keep the row, report failure
-      redi[30] = p < j || p >= n;
-      if (redi[30]) p = j;
-      ipiv[j] = p;
-      redi[31] = p;
+    unsigned long long gk;
+    int p;
+    warp_argmax_bits(lane < nw ? slot_key[32 * buf + lane] : 0ull,
+                     lane < nw ? slot_row[32 * buf + lane] : 0x7fffffff, &gk, &p);
+    if (pending) {  // the previous step's pivot row, scaled now
+      double* ar = a + i;
+#pragma unroll 4
+      for (int c = 0; c < n; c++) ar[static_cast<long long>(ld) * c] *= own_inv;
+      ar[static_cast<long long>(ld) * jprev] = own_inv;
+      pending = false;
     }
-    __syncthreads();
-    const int p = redi[31];
-    if (redi[30]) info = 1;
-    if (p != j)
-      for (int c = threadIdx.x; c < n; c += blockDim.x) {
-        double* x = a + static_cast<long long>(ld) * c;
-        const double t = x[j];
-        x[j] = x[p];
-        x[p] = t;
-      }
-    __syncthreads();
-    const double piv = a[j + static_cast<long long>(ld) * j];
-    if (piv == 0.0 || isinf(piv)) {
-      info = 1;
-      continue;
-    }
+    const double* ap = a + p;
+    const double piv = ap[static_cast<long long>(ld) * j];
+    if (!(fabs(piv) > 0.0) || isinf(piv)) info = 1;  // (0, NaN or infinite)
     const double inv = 1.0 / piv;
-    // keep column j (the multipliers), scale row j
-    for (int i = threadIdx.x; i < n; i += blockDim.x) col[i] = a[i + static_cast<long long>(ld) * j];
-    __syncthreads();
-    for (int c = threadIdx.x; c < n; c += blockDim.x)
-      a[j + static_cast<long long>(ld) * c] = c == j ? inv : a[j + static_cast<long long>(ld) * c] * inv;
-    __syncthreads();
-    // eliminate column j from the other rows: warps take columns, lanes
-    // walk the rows (no index division in the inner loop)
-    for (int c = warp; c < n; c += nw) {
-      double* ac = a + static_cast<long long>(ld) * c;
-      if (c == j) {
-        for (int i = lane; i < n; i += 32)
-          if (i != j) ac[i] = -col[i] * inv;
-      } else {
-        const double rj = ac[j];
-        if (rj != 0.0)
-          for (int i = lane; i < n; i += 32)
-            if (i != j) ac[i] -= col[i] * rj;
-      }
+    if (i == 0) pivot_row[j] = p;
+    if (i == p) {
+      used = true;
+      pending = true;
+      own_inv = inv;
+      jprev = j;
+    } else if (i < n) {
+      double* ar = a + i;
+      const double f = ar[static_cast<long long>(ld) * j] * inv;
+#pragma unroll 4
+      for (int c = 0; c < n; c++)
+        ar[static_cast<long long>(ld) * c] -= f * ap[static_cast<long long>(ld) * c];
+      ar[static_cast<long long>(ld) * j] = -f;
     }
-    __syncthreads();
   }
-  // undo the row interchanges as column interchanges, last first
-  for (int j = n - 1; j >= 0; j--) {
-    const int p = ipiv[j];
-    if (p != j)
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double* cj = a + static_cast<long long>(ld) * j;
-        double* cp = a + static_cast<long long>(ld) * p;
-        const double t = cj[i];
-        cj[i] = cp[i];
-        cp[i] = t;
-      }
-    __syncthreads();
+  __syncthreads();  // (every read of the last pivot row done)
+  if (pending) {
+    double* ar = a + i;
+    for (int c = 0; c < n; c++) ar[static_cast<long long>(ld) * c] *= own_inv;
+    ar[static_cast<long long>(ld) * jprev] = own_inv;
   }
+  __syncthreads();
   return info;
 }
+
 
 // b (length n, stride inc) <- A^{-1} b for the LU above, by one warp.
 __device__ inline void warp_lu_solve(const double* lu, int n, int ld, const int* ipiv,

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/kinterp.h"
+#include "ki_kernels.h"
 #include "ki_solver.h"
 
 struct ki_solver_s {
@@ -140,6 +141,7 @@ int factor_impl(int pde, int n_points, const double* points, const double* norma
   opt.id_tol = id_tol;
   opt.sketch_id = mode == KI_MODE_PRECONDITIONER;
   opt.proxy_shift = opt.sketch_id ? 1 : 0;  // 64 proxy points for sketched boxes
+  opt.top_keep_max = opt.sketch_id ? kib::kLuFusedMaxN : 0;
   h->solver.reset(new kib::Solver(opt, n_points, points, normals, curvatures, weights, n_holes,
                                   holes, h->stream));
   h->solver->time_phases = timed;

@@ -88,9 +88,27 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
     Ksnr[e] = L[e];
   }
   __syncthreads();
-  const int info = cta_gj_invert(Xw, r, ldx, piv, tile, red);
+  // Gauss-Jordan with the pivot rows left in place (one barrier per step);
+  // the result B gives X^{-1}(j, q) = B(p_j, p^{-1}(q)), gathered into X
+  // in global memory and read back into shared memory for the products
+  int* prow = reinterpret_cast<int*>(tile);  // the tile is free until U, L
+  int* pinv = prow + kSmemN;
+  unsigned long long* slot_key = reinterpret_cast<unsigned long long*>(pinv + kSmemN);
+  int* slot_row = reinterpret_cast<int*>(slot_key + 64);
+  const int info = cta_gj_invert_inplace(Xw, r, ldx, prow, slot_key, slot_row);
   if (info && threadIdx.x == 0) atomicExch(P.status, 1);
-  for (int e = threadIdx.x; e < r * r; e += kDecThreads) X[e] = Xw[e % r + ldx * (e / r)];
+  for (int j = threadIdx.x; j < r; j += kDecThreads) {
+    pinv[prow[j]] = j;
+    piv[j] = prow[j];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) {
+    const int j = e % r, q = e / r;
+    X[e] = Xw[prow[j] + ldx * pinv[q]];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < r * r; e += kDecThreads) Xw[e % r + ldx * (e / r)] = X[e];
+  __syncthreads();
   // U = X^{-1} K_r_sn,  L = K_sn_r X^{-1}
   cta_gemm_tiled(U, r, nullptr, 0, Xw, ldx, false, Krsn, r, false, r, k, r, tile, 1.0);
   cta_gemm_tiled(L, k, nullptr, 0, Ksnr, k, false, Xw, ldx, false, k, r, r, tile, 1.0);

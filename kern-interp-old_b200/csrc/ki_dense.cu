@@ -826,22 +826,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Warp argmax of non-negative doubles (first index on ties) with three
-// integer reductions instead of shuffle rounds: a non-negative double's bit
-// pattern orders like the value, so the maximum is found on its high word,
-// then its low word, then the smallest index holding it.  A lane with no
-// candidate passes key 0 and index INT_MAX.
-__device__ __forceinline__ void warp_argmax_bits(unsigned long long key, int idx,
-                                                 unsigned long long* kmax, int* imin) {
-  const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
-  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
-  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
-  const bool top = hi == mhi && lo == mlo;
-  *imin = static_cast<int>(__reduce_min_sync(0xffffffffu, top ? static_cast<unsigned>(idx)
-                                                              : 0x7fffffffu));
-  *kmax = (static_cast<unsigned long long>(mhi) << 32) | mlo;
-}
-
 // Thread 0 waits (bounded) for flag k; false for every thread on an abort.
 __device__ bool fused_wait(int* sync, int k, int G, int* status, int* s_ok) {
   if (threadIdx.x == 0) {
@@ -975,11 +959,198 @@ __device__ __forceinline__ void fused_panel_regs(double* blk, int np, int n, int
   }
 }
 
+// The panel for 512 < n <= 2 * kFusedThreads: each thread holds rows t and
+// t + 512, the block's 32 columns factored as two halves of 16 (the
+// registers of two 32-column rows would not fit), as a recursive LU does:
+// the left half in registers (pivot search, interchanges and rank-one
+// updates inside its 16 columns, one barrier per column as above), its
+// interchanges then applied to the right half, U12 = L11^{-1} A12 and
+// A22 -= L21 U12 (FP64 tensor cores) on the right half, the right half
+// factored the same way, and its interchanges applied to the left half.
+// The pivots are those of the 32-column panel; the sums run in another order.
+constexpr int kHalf = kNb / 2;
+
+// Factors block columns cb .. cb + wh - 1 (absolute c0 + cb + jj) over
+// rows >= c0 + cb in registers, interchanges restricted to those columns;
+// the pivots also go to hp[0 .. wh).
+__device__ __forceinline__ void fused_half_regs2(double* blk, int np, int n, int c0, int cb,
+                                                 int wh, int* ipiv, int* status, PanelSlots& S,
+                                                 int* hp) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int i0 = t, i1 = t + kFusedThreads;  // this thread's rows
+  double x0[kHalf], x1[kHalf];
+#pragma unroll
+  for (int c = 0; c < kHalf; c++) {
+    x0[c] = i0 < n && c < wh ? blk[i0 + np * (cb + c)] : 0.0;
+    x1[c] = i1 < n && c < wh ? blk[i1 + np * (cb + c)] : 0.0;
+  }
+#pragma unroll
+  for (int jj = 0; jj < kHalf; jj++) {
+    if (jj >= wh) break;
+    const int col = c0 + cb + jj, buf = jj & 1;
+    // this thread's candidate: the larger of its two rows (the first on ties)
+    const double v0 = fabs(x0[jj]), v1 = fabs(x1[jj]);
+    const bool c0ok = i0 >= col && i0 < n && v0 == v0;
+    const bool c1ok = i1 >= col && i1 < n && v1 == v1;
+    const unsigned long long k0 = c0ok ? static_cast<unsigned long long>(__double_as_longlong(v0)) : 0ull;
+    const unsigned long long k1 = c1ok ? static_cast<unsigned long long>(__double_as_longlong(v1)) : 0ull;
+    const bool take1 = c1ok && (!c0ok || k1 > k0);
+    unsigned long long wkey;
+    int widx;
+    warp_argmax_bits(take1 ? k1 : k0, take1 ? i1 : (c0ok ? i0 : 0x7fffffff), &wkey, &widx);
+    if (lane == 0) {
+      S.key[buf][warp] = wkey;
+      S.idx[buf][warp] = widx;
+    }
+    if (widx == i0 || widx == i1) {
+      const bool w1 = widx == i1;
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) S.cand[buf][warp][c] = w1 ? x1[c] : x0[c];
+    }
+    if (col == i0 || col == i1) {
+      const bool w1 = col == i1;
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) S.crow[buf][c] = w1 ? x1[c] : x0[c];
+    }
+    __syncthreads();
+    unsigned long long gkey;
+    int p;
+    warp_argmax_bits(lane < kFusedThreads / 32 ? S.key[buf][lane] : 0ull,
+                     lane < kFusedThreads / 32 ? S.idx[buf][lane] : 0x7fffffff, &gkey, &p);
+    const bool bad = p < col || p >= n;
+    // the winning row sits in the slot of the warp holding it (row p is
+    // thread p mod 512's)
+    const double* prow = bad ? S.crow[buf] : S.cand[buf][(p % kFusedThreads) >> 5];
+    if (bad) p = col;
+    const double piv = prow[jj];
+    if (t == 0) {
+      ipiv[col] = p;
+      hp[jj] = p;
+      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
+    }
+    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
+    // interchange (rows col and p trade their 16 values), then the update
+    if (i0 == col) {
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) x0[c] = prow[c];
+    } else if (i0 == p) {
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) x0[c] = S.crow[buf][c];
+    }
+    if (i1 == col) {
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) x1[c] = prow[c];
+    } else if (i1 == p) {
+#pragma unroll
+      for (int c = 0; c < kHalf; c++) x1[c] = S.crow[buf][c];
+    }
+    if (i0 > col && i0 < n) {
+      const double li = x0[jj] * inv;
+#pragma unroll
+      for (int c = jj + 1; c < kHalf; c++) x0[c] -= li * prow[c];
+      x0[jj] = li;
+    }
+    if (i1 > col && i1 < n) {
+      const double li = x1[jj] * inv;
+#pragma unroll
+      for (int c = jj + 1; c < kHalf; c++) x1[c] -= li * prow[c];
+      x1[jj] = li;
+    }
+  }
+  const int rmin = c0 + cb;
+#pragma unroll
+  for (int c = 0; c < kHalf; c++) {
+    if (c < wh) {
+      if (i0 >= rmin && i0 < n) blk[i0 + np * (cb + c)] = x0[c];
+      if (i1 >= rmin && i1 < n) blk[i1 + np * (cb + c)] = x1[c];
+    }
+  }
+}
+
+// The row interchanges hp[0 .. cnt) of rows r0 + jj, on block columns
+// [cfrom, cto): a thread per column, in pivot order.
+__device__ __forceinline__ void half_swaps(double* blk, int np, int n, int r0, int cnt,
+                                           const int* hp, int cfrom, int cto) {
+  const int c = cfrom + static_cast<int>(threadIdx.x);
+  if (c < cto) {
+    for (int jj = 0; jj < cnt; jj++) {
+      const int p = hp[jj], r = r0 + jj;
+      if (p > r && p < n) {
+        const double tmp = blk[r + np * c];
+        blk[r + np * c] = blk[p + np * c];
+        blk[p + np * c] = tmp;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void fused_panel_split(double* blk, int np, int n, int c0, int wb,
+                                                  int* ipiv, int* status, PanelSlots& S,
+                                                  int* hp) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wl = min(kHalf, wb), wr = wb - wl;
+  fused_half_regs2(blk, np, n, c0, 0, wl, ipiv, status, S, hp);
+  __syncthreads();
+  if (wr <= 0) return;
+  // the left half's interchanges on the right half
+  half_swaps(blk, np, n, c0, wl, hp, kHalf, kHalf + wr);
+  __syncthreads();
+  // U12 = L11^{-1} A12: a warp per right-half column
+  if (warp < wr) {
+    const int c = kHalf + warp;
+    double xv = lane < wl ? blk[c0 + lane + np * c] : 0.0;
+#pragma unroll
+    for (int kk = 0; kk < kHalf; kk++) {
+      const double xk = __shfl_sync(0xffffffffu, xv, kk);
+      if (kk < wl && lane > kk && lane < wl) xv -= xk * blk[c0 + lane + np * kk];
+    }
+    if (lane < wl) blk[c0 + lane + np * c] = xv;
+  }
+  __syncthreads();
+  // A22 -= L21 U12 on the FP64 tensor cores: rows c0 + 16 .., 8-row tiles
+  // over the warps, both 8-column tiles of the right half, k = 16
+  {
+    const int r0 = c0 + wl, nr = n - r0;
+    const int fr = lane >> 2, fk = lane & 3;
+    for (int tr = warp; 8 * tr < nr; tr += kFusedThreads / 32) {
+      const int row = r0 + 8 * tr + fr;
+      double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+      for (int ks = 0; ks < kHalf / 4; ks++) {
+        const int kk = 4 * ks + fk;
+        const double af = row < n && kk < wl ? blk[row + np * kk] : 0.0;
+#pragma unroll
+        for (int tc = 0; tc < 2; tc++) {
+          const int cc = kHalf + 8 * tc + fr;
+          const double bf = kk < wl && cc < kHalf + wr ? blk[c0 + kk + np * cc] : 0.0;
+          dmma_8x8x4(acc[tc][0], acc[tc][1], af, bf);
+        }
+      }
+      const int rowc = r0 + 8 * tr + fr;
+      if (rowc < n) {
+#pragma unroll
+        for (int tc = 0; tc < 2; tc++)
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            const int cc = kHalf + 8 * tc + 2 * fk + v;
+            if (cc < kHalf + wr) blk[rowc + np * cc] -= acc[tc][v];
+          }
+      }
+    }
+  }
+  __syncthreads();
+  fused_half_regs2(blk, np, n, c0, kHalf, wr, ipiv, status, S, hp + kHalf);
+  __syncthreads();
+  // the right half's interchanges on the left half
+  half_swaps(blk, np, n, c0 + kHalf, wr, hp + kHalf, 0, wl);
+}
+
 // hold (a test hook, normally 0): thread block 0 keeps its flag down, so the
 // other blocks' bounded waits run out and the launch ends with status 2.
-// kRegPanel: n <= kFusedThreads, the panel in registers (one instantiation
-// per panel form keeps each one's registers to itself).
-template <bool kRegPanel>
+// kPanel: 1 (n <= kFusedThreads) the panel in registers; 2 (n <= 2
+// kFusedThreads) in registers as two halves; 0 in shared memory (one
+// instantiation per panel form keeps each one's registers to itself).
+template <int kPanel>
 __global__ void __launch_bounds__(kFusedThreads, 1)
     lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync, int hold) {
   extern __shared__ double blk[];  // np x kNb, column-major
@@ -989,6 +1160,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   __shared__ int pv[kNb];
   __shared__ int s_ok;
   __shared__ PanelSlots slots;
+  __shared__ int half_piv[kNb];
   const int G = gridDim.x, b = blockIdx.x;
   const int np = n | 1;
   const int c0 = kNb * b, wb = min(kNb, n - c0);
@@ -1101,8 +1273,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
 
   // this CTA's panel: in registers when every row has a thread, else in
   // shared memory (thread t owning rows t + 512 q, two barriers a column)
-  if (kRegPanel) fused_panel_regs(blk, np, n, c0, wb, ipiv, status, slots);
-  for (int jj = 0; jj < wb && !kRegPanel; jj++) {
+  if (kPanel == 1) fused_panel_regs(blk, np, n, c0, wb, ipiv, status, slots);
+  if (kPanel == 2) fused_panel_split(blk, np, n, c0, wb, ipiv, status, slots, half_piv);
+  for (int jj = 0; jj < wb && kPanel == 0; jj++) {
     const int col = c0 + jj;
     // candidates: |a_ij| for rows i >= col (a NaN is no candidate); the
     // largest, the first such row on ties
@@ -1203,8 +1376,9 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
   if (sync && n > 0 && n <= kLuFusedMaxN) {
     int G = (n + kNb - 1) / kNb;
     const size_t smem = sizeof(double) * static_cast<size_t>(n | 1) * kNb;
-    const void* fn = n <= kFusedThreads ? reinterpret_cast<const void*>(&lu_fused_kernel<true>)
-                                        : reinterpret_cast<const void*>(&lu_fused_kernel<false>);
+    const void* fn = n <= kFusedThreads       ? reinterpret_cast<const void*>(&lu_fused_kernel<1>)
+                     : n <= 2 * kFusedThreads ? reinterpret_cast<const void*>(&lu_fused_kernel<2>)
+                                              : reinterpret_cast<const void*>(&lu_fused_kernel<0>);
     cudaError_t e = raise_func_attr(fn,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem));

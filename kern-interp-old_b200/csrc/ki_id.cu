@@ -241,6 +241,7 @@ __device__ __forceinline__ void strided_axpy(double* col, const double* v, int r
 // and the result held in registers (k <= 32 kTRegs); colq(q) is column q of
 // R in pivot order.  Returns false when k is too large for the registers.
 constexpr int kTRegs = 8;
+constexpr int kTRegsOc = 4;  // the on-chip kernel's register T solve: ranks <= 128
 template <class ColFn>
 __device__ __forceinline__ bool warp_tsolve(const double* bcol, int k, const double* rdiag,
                                             ColFn colq, double* out) {
@@ -1010,16 +1011,54 @@ __global__ void __launch_bounds__(kOcThreads, 2) id_onchip_kernel(IdParams P) {
     for (int q = threadIdx.x; q < k; q += kOcThreads) vn2[q] = 1.0 / rdiag[q];
     __syncthreads();
     // one warp per redundant column: the column's back substitution runs
-    // in its warp with no CTA barrier (columns are independent)
+    // in its warp with no CTA barrier (columns are independent).  Up to
+    // 32 kTRegsOc rows (a budget that leaves the 64-register launch bound
+    // without local memory) the column lives in registers (lane l holding rows l,
+    // l + 32, ...): per step one shuffle on the dependent chain, T written
+    // once at the end
     const int nr = si[0];
     for (int t = warp; t < nr; t += kOcWarps) {
       const int p = own[t];
       double* col = colp(pos2col[p]);
+      double* Tp = T + static_cast<long long>(p - k) * k;
+      if (k <= 32 * kTRegsOc) {
+        double b[kTRegsOc];
+#pragma unroll
+        for (int u = 0; u < kTRegsOc; u++) {
+          const int l = lane + 32 * u;
+          b[u] = l < k ? col[l] : 0.0;
+        }
+        // rows q in [32 u, 32 u + 32) sit in slot u: the slot loop outside
+        // (unrolled), so every register index is a constant
+#pragma unroll
+        for (int u = kTRegsOc - 1; u >= 0; u--) {
+          for (int q = min(k, 32 * u + 32) - 1; q >= 32 * u; q--) {
+            const double* rq = colp(pos2col[q]);
+            const double bq = __shfl_sync(0xffffffffu, b[u], q & 31);
+            const double xq = bq * vn2[q];
+#pragma unroll
+            for (int v = 0; v <= u; v++) {
+              const int l = lane + 32 * v;
+              if (l == q) {
+                b[v] = xq;
+              } else if (l < q && bq != 0.0) {
+                b[v] -= xq * rq[l];
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kTRegsOc; u++) {
+          const int l = lane + 32 * u;
+          if (l < k) Tp[l] = b[u];
+        }
+        continue;
+      }
       for (int q = k - 1; q >= 0; q--) {
         const double bq = col[q];
         __syncwarp();
         const double xq = bq * vn2[q];
-        if (lane == 0) T[q + static_cast<long long>(p - k) * k] = xq;
+        if (lane == 0) Tp[q] = xq;
         if (bq != 0.0) {
           const double* rq = colp(pos2col[q]);
           for (int l = lane; l < q; l += 32) col[l] -= xq * rq[l];

@@ -219,6 +219,12 @@ std::vector<AuxSet>& aux_free() {
 }  // namespace
 
 Solver::~Solver() {
+  // the host quadtree (thousands of small lists) is freed on a background
+  // thread: nothing waits for that memory
+  {
+    auto* t = new QuadTreeHost(std::move(tree));
+    release_later([t] { delete t; });
+  }
   // chunks go back to the pool only once no queued work can touch them
   cudaStreamSynchronize(stream_);
   if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
@@ -569,6 +575,19 @@ int Solver::factor() {
   return finish_factor(ev0);
 }
 
+bool Solver::level1_stays() {
+  // (level 2's ranks are in: level 1's active lists are its children's
+  // skeletons)
+  if (opt_.top_keep_max <= 0 || tree.roots.size() != 1 || tree.levels.size() < 3) return false;
+  long long total = nb_;
+  for (int id : tree.levels[1]) {
+    if (tree.boxes[id].compressed) return false;  // kept by an update: compressed as before
+    tree.refresh_box(id);
+    total += static_cast<long long>(tree.boxes[id].active.size());
+  }
+  return total <= opt_.top_keep_max;
+}
+
 int Solver::check_coincident() {
   // Two nodes at the same position make two columns of the operator equal
   // (the reference takes r = 0 as the diagonal, kernel.cpp:23-36, 80-85),
@@ -630,9 +649,11 @@ int Solver::finish_factor(cudaEvent_t ev0) {
     if (!rc) rc = id_finish(cur.get());
     for (int level = L - 1; level > 0 && !rc; level--) {
       auto next = std::make_unique<PendingLevel>();
-      if (level > 1) rc = id_launch(level - 1, next.get());
+      const bool more = level > 1 && !(level == 2 && level1_stays());
+      if (more) rc = id_launch(level - 1, next.get());
       if (!rc) rc = decouple_level(cur.get());
-      if (!rc && level > 1) rc = id_finish(next.get());
+      if (!rc && more) rc = id_finish(next.get());
+      if (!more) break;
       cur = std::move(next);
     }
     if (rc) return rc;
@@ -1323,7 +1344,7 @@ int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t 
   std::vector<int> sk, rd;
   std::vector<SweepTask> st(ncomp);
   std::vector<int> sk_off(ncomp), rd_off(ncomp);
-  int cap = 0;
+  int cap = 0, kr = 0;
   for (int t = 0; t < ncomp; t++) {
     const Box& b = tree.boxes[boxes[t]];
     sk_off[t] = static_cast<int>(sk.size());
@@ -1331,6 +1352,7 @@ int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t 
     sk.insert(sk.end(), b.skel.begin(), b.skel.end());
     rd.insert(rd.end(), b.redundant.begin(), b.redundant.end());
     cap = std::max(cap, static_cast<int>(b.skel.size() + b.redundant.size()));
+    kr = std::max(kr, static_cast<int>(b.skel.size() * b.redundant.size()));
     lf.boxes.push_back(boxes[t]);
   }
   KI_ALLOC(lf.d_skel, int, sk.size());
@@ -1348,6 +1370,7 @@ int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t 
   lf.h_tasks = st;
   lf.ntasks = ncomp;
   lf.cap = cap;
+  lf.kr = kr;
   return 0;
 }
 
@@ -1517,10 +1540,46 @@ int Solver::build_all_compressed() {
     all.insert(all.end(), lf.h_tasks.begin(), lf.h_tasks.end());
     cap = std::max(cap, lf.cap);
   }
+  // the boxes (disjoint redundant dofs, any order) by descending r: the
+  // large ones first, then those whose X^{-1} a single-right-hand-side
+  // diagonal solve stages in shared memory (a launch of their own)
+  std::stable_sort(all.begin(), all.end(),
+                   [](const SweepTask& a, const SweepTask& b) { return a.r > b.r; });
+  int nbig = 0, kr = 0;
+  for (const SweepTask& t : all) {
+    if (static_cast<long long>(t.r) * t.r > kDiagStageMaxR * kDiagStageMaxR) {
+      nbig++;
+    } else {
+      kr = std::max(kr, t.r * t.r);
+    }
+  }
   all_compressed_.ntasks = static_cast<int>(all.size());
   all_compressed_.cap = cap;
+  all_compressed_.nbig = nbig;
+  all_compressed_.kr = kr;
   KI_ALLOC(all_compressed_.d_tasks, SweepTask, all.size());
   KI_UPLOAD(all_compressed_.d_tasks, all, stream_);
+  return 0;
+}
+
+int Solver::diag_all(SweepParams dp, bool trans) {
+  // every compressed box's x_r <- X_rr^{-1} x_r: the boxes too large to
+  // stage X^{-1}, then (one right-hand side) the others with it staged
+  const LevelFactors& ac = all_compressed_;
+  auto run = [&](const SweepParams& p) {
+    return trans ? launch_diag_solve_t(p, stream_) : launch_diag_solve(p, stream_);
+  };
+  if (dp.nrhs != 1 || ac.nbig == ac.ntasks || ac.kr == 0) {
+    KI_CUDA(run(dp));
+    return 0;
+  }
+  SweepParams big = dp, small = dp;
+  big.ntasks = ac.nbig;
+  small.tasks = dp.tasks + ac.nbig;
+  small.ntasks = ac.ntasks - ac.nbig;
+  small.kr = ac.kr;
+  if (big.ntasks) KI_CUDA(run(big));
+  KI_CUDA(run(small));
   return 0;
 }
 
@@ -1709,18 +1768,19 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
     SweepParams sp{lf.d_tasks, lf.ntasks, x, N, 1, 0, nullptr, lf.cap};
+    sp.kr = lf.kr;
     KI_CUDA(launch_sweep_up(sp, false, stream_));
   }
   const int ns = ns_, nb = nb_;
   if (d_forest_) {
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, x, N, 1, 0, nullptr,
                    all_compressed_.cap};
-    KI_CUDA(launch_diag_solve(dp, stream_));
+    if (diag_all(dp, false)) return -2;
     KI_CUDA(launch_forest_top_solve(d_forest_, n_trees(), forest_nmax_, x, stream_));
   } else if (nb == 0) {
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, x, N, 1, 0, nullptr,
                    all_compressed_.cap};
-    KI_CUDA(launch_diag_solve(dp, stream_));
+    if (diag_all(dp, false)) return -2;
     if (ns > 0) {
       KI_CUDA(launch_gather(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
       KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_, d_top_perm_));
@@ -1736,7 +1796,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     KI_CUDA(cudaMemcpyAsync(dw, w, sizeof(double) * nr, cudaMemcpyDeviceToDevice, stream_));
     SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dw, nr, 1, 1, d_red_pos_,
                    all_compressed_.cap};
-    KI_CUDA(launch_diag_solve(dp, stream_));
+    if (diag_all(dp, false)) return -2;
     // border rows of the reduced system: g - Psi~_r D^-1 w_r (the nb dot
     // products in one pass over the rows, partials behind M)
     if (nb <= kMaxKrylov) {
@@ -1756,7 +1816,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
                               stream_));
     KI_CUDA(small_gemm(false, false, nr, 1, nb, -1.0, d_Ured_, nr, M + ns, nb, 1.0, w, nr, stream_));
     dp.x = w;
-    KI_CUDA(launch_diag_solve(dp, stream_));
+    if (diag_all(dp, false)) return -2;
     KI_CUDA(launch_scatter(x, N, d_allred_, nr, 1, w, nr, stream_));
     KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, M, ns, stream_));
   }
@@ -1764,6 +1824,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     const LevelFactors& lf = levels_[l];
     if (!lf.ntasks) continue;
     SweepParams sp{lf.d_tasks, lf.ntasks, x, N, 1, 0, nullptr, lf.cap};
+    sp.kr = lf.kr;
     KI_CUDA(launch_sweep_down(sp, stream_));
   }
   return 0;

@@ -88,6 +88,13 @@ struct SolverOptions {
   // like (box radius / circle radius)^points, far below a preconditioner's
   // tolerance at 64 points.
   int proxy_shift = 0;
+  // Preconditioner mode, one tree: level 1 is left uncompressed when its
+  // active dofs (with the hole border) are at most this many (0: never).
+  // The top-level matrix grows from level 1's skeletons to its active dofs,
+  // which the single-launch LU factors in less time than the level-1 IDs
+  // and decouplings take (their pivoted QRs are the factorization's longest
+  // dependent chains); the factorization only gets more accurate.
+  int top_keep_max = 0;
 };
 
 // Device factors of one compressed box, for copying between solvers.
@@ -101,6 +108,8 @@ struct LevelFactors {
   int level = 0;
   int ntasks = 0;
   int cap = 0;
+  int kr = 0;  // max over the level's boxes of k r (rank x redundant); all_compressed_: max r^2 of the staged boxes
+  int nbig = 0;  // all_compressed_: the first nbig tasks (largest r) stage nothing
   SweepTask* d_tasks = nullptr;
   std::vector<SweepTask> h_tasks;  // host copy of d_tasks
   int* d_skel = nullptr;
@@ -310,6 +319,8 @@ class Solver {
   int adopt_factors(const std::vector<int>& boxes, const std::vector<BoxDevView>& src);
   void drop_device_state();
   int build_all_compressed();
+  bool level1_stays();
+  int diag_all(SweepParams dp, bool trans);
   int factor_top();
   int factor_top_forest();
   int factor_border();

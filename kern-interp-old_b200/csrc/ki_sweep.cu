@@ -30,6 +30,19 @@ inline int rhs_chunk(int nrhs, int cap) {
   return std::max(1, std::min(std::min(nrhs, kRhsChunkMax), fit));
 }
 
+// Asynchronous 8-byte copies global -> shared (cp.async; waited for with
+// cp_async_wait_all before a barrier).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ void stage_async(double* dst, const double* src, int cnt) {
+  for (int e = threadIdx.x; e < cnt; e += blockDim.x) cp_async8(dst + e, src + e);
+}
+
 __device__ __forceinline__ int row_of(const SweepParams& P, int dof) {
   return P.red_pos_map ? P.red_pos[dof] : dof;
 }
@@ -37,7 +50,7 @@ __device__ __forceinline__ int row_of(const SweepParams& P, int dof) {
 // out[i, c] -= sum_l M(i, l) * in[l, c] with M(i, l) = A[i * si + l * sl].
 __device__ __forceinline__ void apply_sub(double* out, const double* in, int rows, int inner,
                                           int nc, const double* A, long long si, long long sl) {
-  for (int t = threadIdx.x; t < rows * nc; t += kSweepThreads) {
+  for (int t = threadIdx.x; t < rows * nc; t += blockDim.x) {
     const int i = t / nc, c = t - i * nc;
     const double* a = A + si * i;
     // four independent loads in flight per thread
@@ -65,7 +78,7 @@ __device__ __forceinline__ void apply_sub_multi(double* out, const double* in, i
                                                 int nc, const double* A, long long si,
                                                 long long sl) {
   const int ng = (nc + kGrp - 1) / kGrp;
-  for (int t = threadIdx.x; t < rows * ng; t += kSweepThreads) {
+  for (int t = threadIdx.x; t < rows * ng; t += blockDim.x) {
     const int i = t % rows, g = t / rows;
     const int c0 = g * kGrp, m = min(kGrp, nc - c0);
     const double* a = A + si * i;
@@ -95,9 +108,75 @@ __device__ __forceinline__ void apply_sub_multi(double* out, const double* in, i
   }
 }
 
+// One right-hand side on a wide CTA (a level of a few large boxes, the
+// factors read from global memory): where the inner index is contiguous
+// (sl = 1) a warp per output row, lanes over the inner index (coalesced,
+// eight loads in flight per lane per pass); otherwise threads over the
+// contiguous rows with the inner index cut into segments, partial sums
+// through shared memory (part: segments x rows doubles) added in segment
+// order.  Ends with a barrier.
+constexpr int kWideThreads = 512;
+__device__ __forceinline__ void apply_sub_wide(double* out, const double* in, int rows, int inner,
+                                               const double* A, long long si, long long sl,
+                                               double* part) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (sl == 1) {
+    for (int i = warp; i < rows; i += nw) {
+      const double* a = A + si * i;
+      double acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) acc[u] = 0.0;
+      for (int l0 = 0; l0 < inner; l0 += 256) {
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int l = l0 + 32 * u + lane;
+          if (l < inner) acc[u] += a[l] * in[l];
+        }
+      }
+      double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) out[i] -= s;
+    }
+    __syncthreads();
+    return;
+  }
+  const int rows32 = (rows + 31) & ~31;
+  const int nseg = max(1, min(static_cast<int>(blockDim.x) / max(rows32, 1), 16));
+  const int seg_len = (inner + nseg - 1) / nseg;
+  for (int t = threadIdx.x; t < rows32 * nseg; t += blockDim.x) {
+    const int i = t % rows32, g = t / rows32;
+    double s = 0.0;
+    if (i < rows) {
+      const double* a = A + si * i;
+      const int l1 = min(inner, (g + 1) * seg_len);
+      double acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) acc[u] = 0.0;
+      for (int l0 = g * seg_len; l0 < l1; l0 += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+          if (l0 + u < l1) acc[u] += a[sl * (l0 + u)] * in[l0 + u];
+      }
+      s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    }
+    part[g * rows32 + i] = s;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < rows; i += blockDim.x) {
+    double s = 0.0;
+    for (int g = 0; g < nseg; g++) s += part[g * rows32 + i];
+    out[i] -= s;
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ void apply_any(double* out, const double* in, int rows, int inner,
-                                          int nc, const double* A, long long si, long long sl) {
-  if (nc == 1) {
+                                          int nc, const double* A, long long si, long long sl,
+                                          double* part = nullptr) {
+  if (part) {
+    apply_sub_wide(out, in, rows, inner, A, si, sl, part);
+  } else if (nc == 1) {
     apply_sub(out, in, rows, inner, nc, A, si, sl);
   } else {
     apply_sub_multi(out, in, rows, inner, nc, A, si, sl);
@@ -105,54 +184,69 @@ __device__ __forceinline__ void apply_any(double* out, const double* in, int row
 }
 
 template <int MODE>  // 0 up (L), 1 up (U^T), 2 down, 3 transposed up (L^T, T)
-__device__ __forceinline__ void sweep_body(const SweepParams& P, int chunk, double* sm) {
+__device__ __forceinline__ void sweep_body(const SweepParams& P, int chunk, double* sm,
+                                           bool wide = false) {
   const SweepTask tk = P.tasks[blockIdx.x];
   const int k = tk.k, r = tk.r;
   const int* S = tk.skel;
   const int* R = tk.red;
+  // the two factor matrices of this mode (each k r entries, contiguous)
+  const double* F1 = MODE == 2 ? tk.U : MODE == 3 ? tk.L : tk.T;
+  const double* F2 = MODE == 0 ? tk.L : MODE == 1 ? tk.U : tk.T;
+  const bool staged = P.kr > 0 && chunk == 1;  // (uniform over the launch)
+  if (staged) {
+    double* f1 = sm + P.cap;
+    stage_async(f1, F1, k * r);
+    stage_async(f1 + P.kr, F2, k * r);
+    F1 = f1;
+    F2 = f1 + P.kr;
+  }
+  // wide CTA, one right-hand side: partial-sum scratch after the vector
+  double* part = wide && chunk == 1 ? sm + P.cap : nullptr;
   for (int c0 = 0; c0 < P.nrhs; c0 += chunk) {
     const int nc = min(chunk, P.nrhs - c0);
     double* xs = sm;
     double* xr = sm + k * nc;
-    for (int t = threadIdx.x; t < k * nc; t += kSweepThreads) {
+    for (int t = threadIdx.x; t < k * nc; t += blockDim.x) {
       const int i = t / nc, c = t - i * nc;
       xs[t] = P.x[static_cast<long long>(S[i]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
-    for (int t = threadIdx.x; t < r * nc; t += kSweepThreads) {
+    for (int t = threadIdx.x; t < r * nc; t += blockDim.x) {
       const int j = t / nc, c = t - j * nc;
       xr[t] = P.x[static_cast<long long>(R[j]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
+    if (staged) cp_async_wait_all();
     __syncthreads();
     if (MODE <= 1) {
       // xr -= T^T xs : (T^T)(j, l) = T[l + k j]
-      apply_any(xr, xs, r, k, nc, tk.T, k, 1);
+      apply_any(xr, xs, r, k, nc, F1, k, 1, part);
       __syncthreads();
       if (MODE == 0) {
         // xs -= L xr : L(i, j) = L[i + k j]
-        apply_any(xs, xr, k, r, nc, tk.L, 1, k);
+        apply_any(xs, xr, k, r, nc, F2, 1, k, part);
       } else {
         // xs -= U^T xr : (U^T)(i, j) = U[j + r i]
-        apply_any(xs, xr, k, r, nc, tk.U, r, 1);
+        apply_any(xs, xr, k, r, nc, F2, r, 1, part);
       }
     } else if (MODE == 2) {
       // xr -= U xs : U(j, l) = U[j + r l]
-      apply_any(xr, xs, r, k, nc, tk.U, 1, r);
+      apply_any(xr, xs, r, k, nc, F1, 1, r, part);
       __syncthreads();
       // xs -= T xr : T(i, j) = T[i + k j]
-      apply_any(xs, xr, k, r, nc, tk.T, 1, k);
+      apply_any(xs, xr, k, r, nc, F2, 1, k, part);
     } else {
       // xr -= L^T xs : (L^T)(j, l) = L[l + k j]
-      apply_any(xr, xs, r, k, nc, tk.L, k, 1);
+      apply_any(xr, xs, r, k, nc, F1, k, 1, part);
       __syncthreads();
       // xs -= T xr
-      apply_any(xs, xr, k, r, nc, tk.T, 1, k);
+      apply_any(xs, xr, k, r, nc, F2, 1, k, part);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < k * nc; t += kSweepThreads) {
+    for (int t = threadIdx.x; t < k * nc; t += blockDim.x) {
       const int i = t / nc, c = t - i * nc;
       P.x[static_cast<long long>(S[i]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)] = xs[t];
     }
-    for (int t = threadIdx.x; t < r * nc; t += kSweepThreads) {
+    for (int t = threadIdx.x; t < r * nc; t += blockDim.x) {
       const int j = t / nc, c = t - j * nc;
       P.x[static_cast<long long>(R[j]) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)] = xr[t];
     }
@@ -164,6 +258,14 @@ template <int MODE>
 __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int chunk) {
   extern __shared__ double sm[];
   sweep_body<MODE>(P, chunk, sm);
+}
+
+// A level of a few large boxes, one right-hand side, factors not staged:
+// 512 threads per box (see apply_sub_wide).
+template <int MODE>
+__global__ void __launch_bounds__(kWideThreads) sweep_wide_kernel(SweepParams P) {
+  extern __shared__ double sm[];
+  sweep_body<MODE>(P, 1, sm, true);
 }
 
 // The two up sweeps of the hole border (U with L, Psi^T with U^T) of one
@@ -190,6 +292,13 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
   const int r = tk.r;
   const double* Xi = tk.X;
   const int* R = tk.red;
+  // one right-hand side: X^{-1} staged in shared memory (P.kr = max r^2)
+  const bool staged = P.kr > 0 && chunk == 1;
+  if (staged) {
+    double* xi = sm + 2 * P.cap;
+    stage_async(xi, Xi, r * r);
+    Xi = xi;
+  }
   for (int c0 = 0; c0 < P.nrhs; c0 += chunk) {
     const int nc = min(chunk, P.nrhs - c0);
     double* xs = sm;
@@ -198,6 +307,7 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
       const int j = t / nc, c = t - j * nc;
       xs[t] = P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd + static_cast<long long>(P.ldx) * (c0 + c)];
     }
+    if (staged) cp_async_wait_all();
     __syncthreads();
     if (nc > 1) {
       // a row and a group of right-hand sides per thread: each X^{-1}
@@ -259,10 +369,34 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, i
   }
 }
 
+// A single right-hand side stages the factors when both fit next to the
+// vector in this much shared memory.
+constexpr size_t kStageSmemMax = 100 * 1024;
+// Levels of at most this many boxes whose factors are not staged sweep a
+// single right-hand side with wide CTAs.
+constexpr int kWideMaxBoxes = 64;
+
 template <int MODE>
-cudaError_t launch_mode(const SweepParams& p, cudaStream_t s) {
+cudaError_t launch_mode(const SweepParams& p0, cudaStream_t s) {
+  SweepParams p = p0;
   const int nc = rhs_chunk(p.nrhs, p.cap);
-  const size_t smem = sizeof(double) * static_cast<size_t>(p.cap) * nc;
+  size_t smem = sizeof(double) * static_cast<size_t>(p.cap) * nc;
+  if (nc == 1 && p.kr > 0 && smem + 2 * sizeof(double) * static_cast<size_t>(p.kr) <= kStageSmemMax)
+    smem += 2 * sizeof(double) * static_cast<size_t>(p.kr);
+  else
+    p.kr = 0;
+  if (nc == 1 && p.kr == 0 && p.ntasks <= kWideMaxBoxes) {
+    // the partial sums: segments x rows rounded to 32, at most the larger
+    // of kWideThreads and the rows rounded up (a single segment)
+    const size_t wsmem =
+        smem + sizeof(double) * (std::max(kWideThreads, (p.cap + 31) & ~31) + 64);
+    cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&sweep_wide_kernel<MODE>),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(wsmem));
+    if (e != cudaSuccess) return e;
+    sweep_wide_kernel<MODE><<<p.ntasks, kWideThreads, wsmem, s>>>(p);
+    return cudaGetLastError();
+  }
   cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&sweep_kernel<MODE>),
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem));
@@ -305,11 +439,53 @@ cudaError_t launch_transposed_up(const SweepParams& p, cudaStream_t s) {
 }
 
 namespace {
+// The diagonal step of a few large boxes, one right-hand side: 512 threads
+// per box, x_r <- X^{-1} x_r through apply_sub_wide (ys = 0 - X^{-1} xs,
+// stored negated).
 template <bool TRANS>
-cudaError_t launch_diag(const SweepParams& p, cudaStream_t s) {
-  if (p.ntasks == 0 || p.nrhs == 0) return cudaSuccess;
+__global__ void __launch_bounds__(kWideThreads) diag_wide_kernel(SweepParams P) {
+  extern __shared__ double sm[];
+  const SweepTask tk = P.tasks[blockIdx.x];
+  const int r = tk.r;
+  const int* R = tk.red;
+  double* xs = sm;
+  double* ys = sm + P.cap;
+  double* part = ys + P.cap;
+  for (int j = threadIdx.x; j < r; j += blockDim.x) {
+    xs[j] = P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd];
+    ys[j] = 0.0;
+  }
+  __syncthreads();
+  if (TRANS) {
+    apply_sub_wide(ys, xs, r, r, tk.X, r, 1, part);  // X^{-T}(i, j) = X[j + r i]
+  } else {
+    apply_sub_wide(ys, xs, r, r, tk.X, 1, r, part);  // X^{-1}(i, j) = X[i + r j]
+  }
+  for (int j = threadIdx.x; j < r; j += blockDim.x)
+    P.x[static_cast<long long>(row_of(P, R[j])) * P.ldd] = -ys[j];
+}
+
+template <bool TRANS>
+cudaError_t launch_diag(const SweepParams& p0, cudaStream_t s) {
+  if (p0.ntasks == 0 || p0.nrhs == 0) return cudaSuccess;
+  SweepParams p = p0;
   const int nc = rhs_chunk(p.nrhs, 2 * (p.cap > 0 ? p.cap : 1));
-  const size_t smem = 2 * sizeof(double) * static_cast<size_t>(p.cap > 0 ? p.cap : 1) * nc;
+  size_t smem = 2 * sizeof(double) * static_cast<size_t>(p.cap > 0 ? p.cap : 1) * nc;
+  if (nc == 1 && p.kr > 0 && smem + sizeof(double) * static_cast<size_t>(p.kr) <= kStageSmemMax)
+    smem += sizeof(double) * static_cast<size_t>(p.kr);
+  else
+    p.kr = 0;
+  if (nc == 1 && p.kr == 0 && p.ntasks <= kWideMaxBoxes) {
+    const size_t wsmem = sizeof(double) * (2 * static_cast<size_t>(p.cap) +
+                                           std::max(kWideThreads, (p.cap + 31) & ~31) + 64);
+    cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&diag_wide_kernel<TRANS>),
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(wsmem));
+    if (e != cudaSuccess) return e;
+    count_launches(1);
+    diag_wide_kernel<TRANS><<<p.ntasks, kWideThreads, wsmem, s>>>(p);
+    return cudaGetLastError();
+  }
   cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&diag_inv_kernel<TRANS>),
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem));

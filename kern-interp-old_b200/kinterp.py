@@ -497,6 +497,34 @@ class BatchSolver(_Tree):
         return Solver.stats(self)
 
 
+def tune_id_tol(problem, candidates=(1e-6, 3e-7, 1e-7, 3e-8, 1e-8), rel_tol=1e-12,
+                max_iters=20, reps=3, stream=None):
+    """Autotuner for the mixed method: the preconditioner's ID tolerance
+    trades factorization time (tighter: higher ranks) against refinement
+    steps (looser: more of them).  Times factor + refinement for each
+    candidate (host wall clock around the public calls, which synchronise:
+    the best of `reps` after one untimed run) and returns (best_tol, table),
+    table = [(tol, seconds, iterations, residual)].  Candidates whose
+    refinement does not reach rel_tol are skipped."""
+    import time
+    table = []
+    for tol in candidates:
+        best, it, rr = None, None, None
+        for rep in range(reps + 1):
+            t0 = time.perf_counter()
+            s = Solver(problem, id_tol=tol, stream=stream, mode=1)
+            _, _, it, rr = s.solve_refined(problem.f, rel_tol=rel_tol, max_iters=max_iters)
+            dt = time.perf_counter() - t0
+            s.close()
+            if rep > 0 and (best is None or dt < best):
+                best = dt
+        if rr <= rel_tol:
+            table.append((tol, best, it, rr))
+    if not table:
+        raise KiError("tune_id_tol: no candidate tolerance reached the refinement target")
+    return min(table, key=lambda row: row[1])[0], table
+
+
 def boundary_integral_solve(problem, domain_pts, id_tol=None, max_leaf_dofs=None,
                             domain="nodes", disk=None):
     """boundary_integral_solve (linear_solve.cpp:142-180): factor the

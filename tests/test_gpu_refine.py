@@ -199,3 +199,13 @@ def test_sketched_ids_in_clusters_reach_fp64():
     mt, at = o.solve(pr.f)
     o.close()
     assert H.rel(mu, mt) < 1e-10
+
+
+def test_tune_id_tol_returns_the_fastest_converging_candidate():
+    """The autotuner times factor + refinement per candidate tolerance and
+    returns the fastest one among those whose refinement reaches the target."""
+    pr = _problems()["stokes_holes_4096"]
+    tol, table = kinterp.tune_id_tol(pr, candidates=(1e-5, 1e-8), reps=1)
+    assert [row[0] for row in table] == [1e-5, 1e-8]
+    assert all(row[3] <= 1e-12 and row[2] >= 1 for row in table)
+    assert tol == min(table, key=lambda row: row[1])[0]
