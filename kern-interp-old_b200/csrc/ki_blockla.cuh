@@ -239,29 +239,46 @@ __device__ __forceinline__ void warp_argmax_bits(unsigned long long key, int idx
 }
 
 // Gauss-Jordan inversion of the n x n matrix a (column-major, ld; n <=
-// blockDim.x, a thread per row) in place, partial pivoting, one barrier per
-// pivot step.  Rows are never exchanged: step j eliminates column j with
-// the row p_j (the largest |a(i, j)| among the rows not yet pivots, the
-// first on ties; a NaN counts as 0), every other row i updating itself as
-// a(i, :) -= (a(i, j) / a(p_j, j)) a(p_j, :) with a(i, j) <- -a(i, j) /
-// a(p_j, j) (the in-place trick), while row p_j waits until the next
-// step's barrier, when nobody reads it any more, to scale itself by the
-// reciprocal it kept.  Before the barrier each warp publishes its best
-// candidate (key, row) in a slot double-buffered by step parity; after it
-// every thread reduces the slots to the same p_j.  On return the result B
-// holds A^{-1}(j, q) = B(p_j, p^{-1}(q)); pivot_row[j] = p_j.  Returns
-// nonzero when a pivot was 0, infinite or NaN.  Slots: 2 x 32 keys and rows.
+// blockDim.x) in place, partial pivoting, one barrier per pivot step.  Row
+// i is updated by S = blockDim.x / n threads (at most 8), thread (i, s)
+// owning the columns of segment s.  Rows are never exchanged: step j
+// eliminates column j with row p_j (the largest |a(i, j)| among the rows
+// not yet pivots, the first on ties; a NaN counts as 0).  Before the step's
+// barrier the owner of a(i, j) keeps it in colj (double-buffered by step
+// parity) and each warp publishes its best candidate (key, row) in a slot;
+// after it every thread reduces the slots to the same p_j and updates its
+// segment with the arithmetic of the row-swapping form: a(i, c) -= a(i, j)
+// (a(p, c) / piv) via the reciprocal, a(i, j) <- -a(i, j) / piv, while row
+// p_j waits until the next step's barrier, when nobody reads it any more,
+// to scale itself (a(p, c) / piv, a(p, j) <- 1 / piv).  On return the
+// result B holds A^{-1}(j, q) = B(p_j, p^{-1}(q)); pivot_row[j] = p_j.
+// Returns nonzero when a pivot was 0, infinite or NaN.  Slots: 2 x 32 keys
+// and rows; colj: 2 n doubles.
 __device__ inline int cta_gj_invert_inplace(double* a, int n, int ld, int* pivot_row,
-                                            unsigned long long* slot_key, int* slot_row) {
-  const int i = threadIdx.x, lane = i & 31, warp = i >> 5, nw = blockDim.x >> 5;
+                                            unsigned long long* slot_key, int* slot_row,
+                                            double* colj) {
+  if (n <= 0) return 0;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = blockDim.x >> 5;
+  const int S = max(1, min(static_cast<int>(blockDim.x) / n, 8));
+  const int i = t % n, sg = t / n;
+  const bool live = sg < S;
+  const int L = (n + S - 1) / S, cb = sg * L, ce = min(n, cb + L);
+  double* ar = a + i;
   bool used = false, pending = false;
   int jprev = 0;
   double own_inv = 0.0;
   int info = 0;
   for (int j = 0; j < n; j++) {
     const int buf = j & 1;
-    const bool cand = i < n && !used;
-    double v = cand ? fabs(a[i + static_cast<long long>(ld) * j]) : 0.0;
+    const bool owner = live && j >= cb && j < ce;
+    double aij = 0.0;
+    if (owner) {
+      aij = ar[static_cast<long long>(ld) * j];
+      if (pending) aij *= own_inv;  // (the row scales itself after the barrier)
+      colj[buf * n + i] = aij;
+    }
+    const bool cand = owner && !used;
+    double v = cand ? fabs(aij) : 0.0;
     if (v != v) v = 0.0;
     unsigned long long wk;
     int wi;
@@ -277,36 +294,39 @@ __device__ inline int cta_gj_invert_inplace(double* a, int n, int ld, int* pivot
     warp_argmax_bits(lane < nw ? slot_key[32 * buf + lane] : 0ull,
                      lane < nw ? slot_row[32 * buf + lane] : 0x7fffffff, &gk, &p);
     if (pending) {  // the previous step's pivot row, scaled now
-      double* ar = a + i;
-#pragma unroll 4
-      for (int c = 0; c < n; c++) ar[static_cast<long long>(ld) * c] *= own_inv;
-      ar[static_cast<long long>(ld) * jprev] = own_inv;
+      for (int c = cb; c < ce; c++) {
+        double* e = ar + static_cast<long long>(ld) * c;
+        *e = c == jprev ? own_inv : *e * own_inv;
+      }
       pending = false;
     }
     const double* ap = a + p;
     const double piv = ap[static_cast<long long>(ld) * j];
     if (!(fabs(piv) > 0.0) || isinf(piv)) info = 1;  // (0, NaN or infinite)
     const double inv = 1.0 / piv;
-    if (i == 0) pivot_row[j] = p;
+    if (t == 0) pivot_row[j] = p;
     if (i == p) {
-      used = true;
-      pending = true;
-      own_inv = inv;
-      jprev = j;
-    } else if (i < n) {
-      double* ar = a + i;
-      const double f = ar[static_cast<long long>(ld) * j] * inv;
+      if (live) {
+        used = true;
+        pending = true;
+        own_inv = inv;
+        jprev = j;
+      }
+    } else if (live) {
+      const double f = colj[buf * n + i];
 #pragma unroll 4
-      for (int c = 0; c < n; c++)
-        ar[static_cast<long long>(ld) * c] -= f * ap[static_cast<long long>(ld) * c];
-      ar[static_cast<long long>(ld) * j] = -f;
+      for (int c = cb; c < ce; c++) {
+        double* e = ar + static_cast<long long>(ld) * c;
+        *e = c == j ? -f * inv : *e - f * (ap[static_cast<long long>(ld) * c] * inv);
+      }
     }
   }
   __syncthreads();  // (every read of the last pivot row done)
   if (pending) {
-    double* ar = a + i;
-    for (int c = 0; c < n; c++) ar[static_cast<long long>(ld) * c] *= own_inv;
-    ar[static_cast<long long>(ld) * jprev] = own_inv;
+    for (int c = cb; c < ce; c++) {
+      double* e = ar + static_cast<long long>(ld) * c;
+      *e = c == jprev ? own_inv : *e * own_inv;
+    }
   }
   __syncthreads();
   return info;

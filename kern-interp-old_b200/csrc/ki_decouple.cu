@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(kDecThreads) decouple_kernel(DecParams P) {
   int* pinv = prow + kSmemN;
   unsigned long long* slot_key = reinterpret_cast<unsigned long long*>(pinv + kSmemN);
   int* slot_row = reinterpret_cast<int*>(slot_key + 64);
-  const int info = cta_gj_invert_inplace(Xw, r, ldx, prow, slot_key, slot_row);
+  double* colj = reinterpret_cast<double*>(slot_row + 64);  // 2 r
+  const int info = cta_gj_invert_inplace(Xw, r, ldx, prow, slot_key, slot_row, colj);
   if (info && threadIdx.x == 0) atomicExch(P.status, 1);
   for (int j = threadIdx.x; j < r; j += kDecThreads) {
     pinv[prow[j]] = j;

@@ -20,9 +20,7 @@ thread_local bool t_in_job = false;
 // Workers spin on the job counter for a while after each job before they
 // sleep on the condition variable: the factorization issues many short
 // jobs back to back (one or two per level and phase), and a sleeping
-// worker takes tens of microseconds to wake.  The window (1 ms) outlasts a
-// level's IDs on the GPU, during which the host only waits for their
-// ranks, so the next level's bookkeeping finds the workers awake.
+// worker takes tens of microseconds to wake.
 class Pool {
  public:
   Pool() {
@@ -86,7 +84,7 @@ class Pool {
           break;
         }
         if ((spin & 255) == 255 &&
-            std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(1000))
+            std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(200))
           break;
       }
       if (!got) {
@@ -120,43 +118,6 @@ Pool& pool() {
 }  // namespace
 
 int pool_threads() { return pool().size(); }
-
-namespace {
-// One background thread draining a queue of release jobs.  Made once and
-// never destroyed (jobs queued at process exit may be dropped: they only
-// free host memory).
-struct Releaser {
-  std::mutex mu;
-  std::condition_variable cv;
-  std::vector<std::function<void()>> jobs;
-  Releaser() {
-    std::thread([this] {
-      for (;;) {
-        std::vector<std::function<void()>> now;
-        {
-          std::unique_lock<std::mutex> lk(mu);
-          cv.wait(lk, [&] { return !jobs.empty(); });
-          now.swap(jobs);
-        }
-        for (auto& f : now) f();
-      }
-    }).detach();
-  }
-};
-Releaser& releaser() {
-  static Releaser* r = new Releaser();
-  return *r;
-}
-}  // namespace
-
-void release_later(std::function<void()> fn) {
-  Releaser& r = releaser();
-  {
-    std::lock_guard<std::mutex> lk(r.mu);
-    r.jobs.push_back(std::move(fn));
-  }
-  r.cv.notify_one();
-}
 
 void parallel_for(int n, int grain, const std::function<void(int, int)>& fn, int serial_below) {
   if (n <= 0) return;

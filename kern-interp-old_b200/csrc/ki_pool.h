@@ -16,9 +16,6 @@ namespace kib {
 void parallel_for(int n, int grain, const std::function<void(int, int)>& fn,
                   int serial_below = 64);
 int pool_threads();
-// Runs fn later on a background thread (host memory that nothing waits
-// for, freed off the caller's path).  Jobs run in order.
-void release_later(std::function<void()> fn);
 
 }  // namespace kib
 

@@ -218,12 +218,22 @@ std::vector<AuxSet>& aux_free() {
 }
 }  // namespace
 
+namespace {
+// One finished solver's host quadtree, kept for the next solver of the
+// process: the next build reuses its boxes' list capacities, so neither the
+// finished solver's close nor the next build frees or allocates the
+// thousands of small lists a tree holds.
+std::mutex g_tree_mu;
+std::unique_ptr<QuadTreeHost>& tree_slot() {
+  static std::unique_ptr<QuadTreeHost> slot;
+  return slot;
+}
+}  // namespace
+
 Solver::~Solver() {
-  // the host quadtree (thousands of small lists) is freed on a background
-  // thread: nothing waits for that memory
   {
-    auto* t = new QuadTreeHost(std::move(tree));
-    release_later([t] { delete t; });
+    std::lock_guard<std::mutex> lk(g_tree_mu);
+    if (!tree_slot()) tree_slot().reset(new QuadTreeHost(std::move(tree)));
   }
   // chunks go back to the pool only once no queued work can touch them
   cudaStreamSynchronize(stream_);
@@ -565,6 +575,13 @@ int Solver::factor() {
   const int grc = setup_geometry();
   if (grc) return grc;
   mark(7, 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tree_mu);
+    if (tree_slot()) {
+      tree = std::move(*tree_slot());
+      tree_slot().reset();
+    }
+  }
   if (starts_.size() > 1) {
     tree.build_forest(pts_.data(), n_points_, sd_, opt_.max_leaf_dofs, starts_);
   } else {

@@ -281,7 +281,9 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
   int next = 1;
   for (int id : splits)
     for (int q = 0; q < 4; q++) idmap[tb[id].child[q]] = next++;
-  boxes.assign(nt, Box());
+  // (a reused tree keeps its boxes' list capacities: every field is reset
+  // below, the lists cleared rather than freed)
+  boxes.resize(nt);
   std::vector<int> order(nt);
   for (int id = 0; id < nt; id++) order[idmap[id]] = id;
   int depth = 0;
@@ -293,6 +295,15 @@ void QuadTreeHost::build_partition(int p0, int p1, int tree_id, double lo, doubl
     for (int id = a; id < e; id++) {
       const Tmp& t = tb[id];
       Box& b = boxes[idmap[id]];
+      b.nbr.clear();
+      b.original.clear();
+      b.active.clear();
+      b.skel.clear();
+      b.redundant.clear();
+      b.perm.clear();
+      b.compressed = false;
+      b.rank = 0;
+      b.dead = false;
       b.tree = tree_id;
       b.level = t.level;
       b.parent = t.parent >= 0 ? idmap[t.parent] : -1;
