@@ -632,16 +632,7 @@ __global__ void __launch_bounds__(kSolveThreads)
   extern __shared__ double x[];
   int* pv = reinterpret_cast<int*>(x + n);
   double* bc = b + static_cast<long long>(ldb) * blockIdx.x;
-  // the whole LU into L2 up front (one prefetch per 128-byte line): the
-  // blocked substitutions then wait on L2, not HBM, at every block step
-  {
-    const int lines = (n * 8 + 127) / 128;  // per column, upper bound
-    for (int e = threadIdx.x; e < n * lines; e += blockDim.x) {
-      const int c = e / lines, q = e % lines;
-      const double* a = lu + static_cast<long long>(ld) * c + 16 * q;
-      if (16 * q < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
-    }
-  }
+  // (the caller brings the LU into L2 beforehand: launch_l2_prefetch)
   if (perm) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = bc[perm[i]];
   } else {
@@ -650,6 +641,15 @@ __global__ void __launch_bounds__(kSolveThreads)
   __syncthreads();
   cta_lu_solve(lu, n, ld, perm ? nullptr : ipiv, x, pv);
   for (int i = threadIdx.x; i < n; i += blockDim.x) bc[i] = x[i];
+}
+
+// Every 128-byte line of [p, p + bytes) into L2 with the evict-last
+// priority, from the whole grid (the prefetches return at once; the lines
+// arrive at HBM bandwidth while later kernels run).
+__global__ void l2_prefetch_kernel(const char* p, long long lines) {
+  for (long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; e < lines;
+       e += static_cast<long long>(gridDim.x) * blockDim.x)
+    asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p + 128 * e));
 }
 
 // B <- A^{-1} B with one warp per right-hand side.
@@ -1480,6 +1480,15 @@ cudaError_t launch_pivots_to_perm(const int* ipiv, int n, int* perm, cudaStream_
   }
   count_launches(1);
   pivots_to_perm_kernel<<<1, 256, smem, s>>>(ipiv, n, perm);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_l2_prefetch(const void* p, size_t bytes, cudaStream_t s) {
+  const long long lines = static_cast<long long>((bytes + 127) / 128);
+  if (lines == 0) return cudaSuccess;
+  const int blocks = static_cast<int>(std::min<long long>(592, (lines + 255) / 256));
+  count_launches(1);
+  l2_prefetch_kernel<<<blocks, 256, 0, s>>>(static_cast<const char*>(p), lines);
   return cudaGetLastError();
 }
 

@@ -217,6 +217,9 @@ cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv
 // launch_pivots_to_perm) replaces the sequential interchanges by a gather.
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
                            int nrhs, int ldb, cudaStream_t s, const int* perm = nullptr);
+// Brings [p, p + bytes) into L2 (evict-last priority) from a whole grid of
+// prefetches; returns as soon as they are issued.
+cudaError_t launch_l2_prefetch(const void* p, size_t bytes, cudaStream_t s);
 // The interchanges ipiv[0..n) of an LU composed into one permutation:
 // (P b)[i] = b[perm[i]].
 cudaError_t launch_pivots_to_perm(const int* ipiv, int n, int* perm, cudaStream_t s);

@@ -415,35 +415,61 @@ __global__ void mv_border_finish_kernel(int n_dofs, int nb, int nblk,
 constexpr int kVecThreads = 256;
 
 // part[j * gridDim.x + b] = sum over this CTA's slice of V_j . w
+// Partial sums of V(:, j) . w over this block's rows for j < k: a thread
+// per row, the columns 16 at a time with their loads in flight together,
+// then a fixed-order reduction over the block.
+constexpr int kDotChunk = 16;
 __global__ void multi_dot_kernel(const double* __restrict__ V, long long ldv, int k,
                                  const double* __restrict__ w, int n, double* __restrict__ part) {
-  __shared__ double red[kVecThreads / 32][kMaxKrylov + 1];
+  __shared__ double red[kVecThreads / 32][kDotChunk];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int per = (n + gridDim.x - 1) / gridDim.x;
   const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
-  for (int j = 0; j < k; j++) {
-    const double* v = V + ldv * j;
-    double s = 0.0;
-    for (int i = i0 + threadIdx.x; i < i1; i += kVecThreads) s += v[i] * w[i];
+  for (int j0 = 0; j0 < k; j0 += kDotChunk) {
+    double s[kDotChunk];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) red[warp][j] = s;
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < k; j += kVecThreads) {
-    double v = 0.0;
-    for (int q = 0; q < kVecThreads / 32; q++) v += red[q][j];
-    part[static_cast<long long>(j) * gridDim.x + blockIdx.x] = v;
+    for (int u = 0; u < kDotChunk; u++) s[u] = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += kVecThreads) {
+      const double wi = w[i];
+#pragma unroll
+      for (int u = 0; u < kDotChunk; u++)
+        if (j0 + u < k) s[u] += V[ldv * (j0 + u) + i] * wi;
+    }
+#pragma unroll
+    for (int u = 0; u < kDotChunk; u++) {
+      double v = s[u];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][u] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDotChunk && j0 + threadIdx.x < k) {
+      double v = 0.0;
+      for (int q = 0; q < kVecThreads / 32; q++) v += red[q][threadIdx.x];
+      part[static_cast<long long>(j0 + threadIdx.x) * gridDim.x + blockIdx.x] = v;
+    }
+    __syncthreads();
   }
 }
 
+// out[j] = the sum of column j's partials: a warp per column (lanes over
+// the blocks, then a shuffle tree: a fixed order).
 __global__ void multi_dot_finish_kernel(const double* __restrict__ part, int nblk, int k,
                                         double* __restrict__ out) {
-  const int j = threadIdx.x;
+  const int j = blockIdx.x, lane = threadIdx.x;
   if (j >= k) return;
-  double v = 0.0;
-  for (int b = 0; b < nblk; b++) v += part[static_cast<long long>(j) * nblk + b];
-  out[j] = v;
+  const double* p = part + static_cast<long long>(j) * nblk;
+  double v0 = 0.0, v1 = 0.0;
+  int b = lane;
+  for (; b + 32 < nblk; b += 64) {
+    v0 += p[b];
+    v1 += p[b + 32];
+  }
+  if (b < nblk) v0 += p[b];
+  double v = v0 + v1;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) out[j] = v;
 }
 
 // w -= V h (h on the device, k entries)
@@ -606,7 +632,7 @@ size_t fast_matvec_scratch_doubles(int n_dofs, int splits, int nseg, int nb) {
          static_cast<size_t>(kBorderBlocks) * nb;
 }
 
-int multi_dot_blocks(int n) { return std::max(1, std::min(296, (n + 1023) / 1024)); }
+int multi_dot_blocks(int n) { return std::max(1, std::min(592, (n + 255) / 256)); }
 
 cudaError_t launch_multi_dot(const double* V, long long ldv, int k, const double* w, int n,
                              double* part, double* out, cudaStream_t s) {
@@ -614,7 +640,7 @@ cudaError_t launch_multi_dot(const double* V, long long ldv, int k, const double
   const int nblk = multi_dot_blocks(n);
   count_launches(2);
   multi_dot_kernel<<<nblk, kVecThreads, 0, s>>>(V, ldv, k, w, n, part);
-  multi_dot_finish_kernel<<<1, 64, 0, s>>>(part, nblk, k, out);
+  multi_dot_finish_kernel<<<k, 32, 0, s>>>(part, nblk, k, out);
   return cudaGetLastError();
 }
 

@@ -1780,6 +1780,11 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
   double* x = d_mu;
   if (d_b != d_mu)
     KI_CUDA(cudaMemcpyAsync(x, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, stream_));
+  // the top-level LU into L2 while the up sweeps run (its substitution is
+  // a chain of dependent blocks, each waiting on its loads)
+  if (d_top_ && !d_forest_)
+    KI_CUDA(launch_l2_prefetch(d_top_, sizeof(double) * static_cast<size_t>(ns_ + nb_) * (ns_ + nb_),
+                               stream_));
   const int L = static_cast<int>(levels_.size());
   for (int l = L - 1; l >= 0; l--) {
     const LevelFactors& lf = levels_[l];
