@@ -219,10 +219,11 @@ std::vector<AuxSet>& aux_free() {
 }  // namespace
 
 namespace {
-// One finished solver's host quadtree, kept for the next solver of the
-// process: the next build reuses its boxes' list capacities, so neither the
-// finished solver's close nor the next build frees or allocates the
-// thousands of small lists a tree holds.
+// One finished single-tree solver's host quadtree, kept for the next
+// single-tree solver of the process: the next build reuses its boxes' list
+// capacities, so neither the finished solver's close nor the next build
+// frees or allocates the thousands of small lists a tree holds.  (A forest
+// is laid out from per-problem trees and would only free the kept one.)
 std::mutex g_tree_mu;
 std::unique_ptr<QuadTreeHost>& tree_slot() {
   static std::unique_ptr<QuadTreeHost> slot;
@@ -233,7 +234,7 @@ std::unique_ptr<QuadTreeHost>& tree_slot() {
 Solver::~Solver() {
   {
     std::lock_guard<std::mutex> lk(g_tree_mu);
-    if (!tree_slot()) tree_slot().reset(new QuadTreeHost(std::move(tree)));
+    if (!tree_slot() && starts_.size() <= 2) tree_slot().reset(new QuadTreeHost(std::move(tree)));
   }
   // chunks go back to the pool only once no queued work can touch them
   cudaStreamSynchronize(stream_);
@@ -577,7 +578,7 @@ int Solver::factor() {
   mark(7, 0);
   {
     std::lock_guard<std::mutex> lk(g_tree_mu);
-    if (tree_slot()) {
+    if (tree_slot() && starts_.size() <= 2) {
       tree = std::move(*tree_slot());
       tree_slot().reset();
     }
