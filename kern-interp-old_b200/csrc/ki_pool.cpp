@@ -20,7 +20,10 @@ thread_local bool t_in_job = false;
 // Workers spin on the job counter for a while after each job before they
 // sleep on the condition variable: the factorization issues many short
 // jobs back to back (one or two per level and phase), and a sleeping
-// worker takes tens of microseconds to wake.
+// worker takes tens of microseconds to wake.  The window (1 ms) outlasts
+// most of a level's GPU work, during which the host only waits, so the next
+// level's bookkeeping finds the workers awake (measured on a B200 host: the
+// 256-problem batch factorization 65 -> 61 ms against a 200 us window).
 class Pool {
  public:
   Pool() {
@@ -84,7 +87,7 @@ class Pool {
           break;
         }
         if ((spin & 255) == 255 &&
-            std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(200))
+            std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(1000))
           break;
       }
       if (!got) {
