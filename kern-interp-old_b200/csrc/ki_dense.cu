@@ -643,6 +643,153 @@ __global__ void __launch_bounds__(kSolveThreads)
   for (int i = threadIdx.x; i < n; i += blockDim.x) bc[i] = x[i];
 }
 
+// The inverses of the 16 x 16 diagonal blocks of an LU's factors, a warp
+// per block, lane j forming column j: L_kk^{-1} by forward substitution on
+// e_j (unit diagonal), U_kk^{-1} by back substitution (the divisions by
+// u_ii in full precision).  A last block of fewer rows is completed with
+// the identity.  dinv: block k's L^{-1} then U^{-1}, each column-major,
+// 2 * 256 doubles a block.
+constexpr int kInvBlk = 16;
+__global__ void lu_block_inv_kernel(const double* __restrict__ lu, int n, int ld,
+                                    double* __restrict__ dinv) {
+  const int blk = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int j = threadIdx.x & 31;
+  if (blk >= (n + kInvBlk - 1) / kInvBlk || j >= kInvBlk) return;
+  const int kb = blk * kInvBlk, nbk = min(kInvBlk, n - kb);
+  auto A = [&](int i, int k) -> double {
+    return i < nbk && k < nbk ? lu[kb + i + static_cast<long long>(ld) * (kb + k)]
+                              : (i == k ? 1.0 : 0.0);
+  };
+  double* out = dinv + static_cast<long long>(blk) * 2 * kInvBlk * kInvBlk;
+  double y[kInvBlk];
+#pragma unroll
+  for (int i = 0; i < kInvBlk; i++) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; k++) s += A(i, k) * y[k];
+    y[i] = i < j ? 0.0 : (i == j ? 1.0 : -s);
+  }
+#pragma unroll
+  for (int i = 0; i < kInvBlk; i++) out[j * kInvBlk + i] = y[i];
+#pragma unroll
+  for (int i = kInvBlk - 1; i >= 0; i--) {
+    double s = i == j ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = i + 1; k < kInvBlk; k++) s -= A(i, k) * y[k];
+    y[i] = i > j ? 0.0 : s / A(i, i);
+  }
+#pragma unroll
+  for (int i = 0; i < kInvBlk; i++) out[kInvBlk * kInvBlk + j * kInvBlk + i] = y[i];
+}
+
+// b <- A^{-1} b for the LU above, one CTA per right-hand side, a thread per
+// row (n <= kInvSolveThreads), 16-row blocks: warp 0 applies the block's
+// inverse L_kk^{-1} (forward) or U_kk^{-1} (backward) to the block's values,
+// then every row still to be solved subtracts its 16 entries of the block
+// column times them.  Each thread requests its row's entries of the next
+// block column while the current block is applied, so the loads overlap the
+// barrier and the block product.  The block inverses (lu_block_inv_kernel)
+// are staged in shared memory at the start, behind them the vector.  perm:
+// the interchanges composed into one permutation, applied as a gather.
+constexpr int kInvSolveThreads = kLuBlockInvMaxN;
+__global__ void __launch_bounds__(kInvSolveThreads, 1)
+    lu_solve_inv_kernel(const double* __restrict__ lu, int n, int ld,
+                        const double* __restrict__ dinv, const int* __restrict__ perm, double* b,
+                        int ldb) {
+  extern __shared__ __align__(16) double sm[];
+  constexpr int NB = kInvBlk, BS = 2 * kInvBlk * kInvBlk;
+  const int nblk = (n + NB - 1) / NB;
+  double* di = sm;              // nblk x BS
+  double* x = sm + nblk * BS;   // nblk x NB, zero past n
+  double* bc = b + static_cast<long long>(ldb) * blockIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int e = 2 * t; e < nblk * BS; e += 2 * kInvSolveThreads) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(di + e));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(dinv + e));
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  for (int i = t; i < nblk * NB; i += kInvSolveThreads) x[i] = i < n ? bc[perm[i]] : 0.0;
+  const bool mine = t < n;
+  double l[NB];
+  // rows below block 0: its column entries (L, unit lower)
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    l[k] = mine && t >= NB && k < n ? lu[t + static_cast<long long>(ld) * k] : 0.0;
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  for (int kb = 0; kb < n; kb += NB) {  // L y = P b
+    if (warp == 0) {
+      const double* Li = di + (kb / NB) * BS;
+      const int r = lane & (NB - 1);
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < NB; k++) acc += Li[k * NB + r] * x[kb + k];
+      __syncwarp();
+      if (lane < NB) x[kb + lane] = acc;
+    }
+    __syncthreads();
+    if (mine && t >= kb + NB) {
+      const double2* xv = reinterpret_cast<const double2*>(x + kb);
+      double s = 0.0;
+#pragma unroll
+      for (int h = 0; h < NB / 2; h++) {
+        const double2 u = xv[h];
+        s += l[2 * h] * u.x;
+        s += l[2 * h + 1] * u.y;
+      }
+      x[t] -= s;
+    }
+    const int kn = kb + NB;
+    if (mine && t >= kn + NB) {
+      const double* q = lu + t + static_cast<long long>(ld) * kn;
+      if (kn + NB <= n) {
+#pragma unroll
+        for (int k = 0; k < NB; k++) l[k] = q[static_cast<long long>(ld) * k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < NB; k++) l[k] = kn + k < n ? q[static_cast<long long>(ld) * k] : 0.0;
+      }
+    }
+    __syncthreads();
+  }
+  const int kb_last = (nblk - 1) * NB;
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    l[k] = t < kb_last && kb_last + k < n ? lu[t + static_cast<long long>(ld) * (kb_last + k)]
+                                          : 0.0;
+  for (int kb = kb_last; kb >= 0; kb -= NB) {  // U x = y
+    if (warp == 0) {
+      const double* Ui = di + (kb / NB) * BS + NB * NB;
+      const int r = lane & (NB - 1);
+      double acc = 0.0;
+#pragma unroll
+      for (int k = 0; k < NB; k++) acc += Ui[k * NB + r] * x[kb + k];
+      __syncwarp();
+      if (lane < NB && kb + lane < n) x[kb + lane] = acc;
+    }
+    __syncthreads();
+    if (t < kb) {
+      const double2* xv = reinterpret_cast<const double2*>(x + kb);
+      double s = 0.0;
+#pragma unroll
+      for (int h = 0; h < NB / 2; h++) {
+        const double2 u = xv[h];
+        s += l[2 * h] * u.x;
+        s += l[2 * h + 1] * u.y;
+      }
+      x[t] -= s;
+    }
+    const int kp = kb - NB;
+    if (kp >= 0 && t < kp) {
+      const double* q = lu + t + static_cast<long long>(ld) * kp;
+#pragma unroll
+      for (int k = 0; k < NB; k++) l[k] = q[static_cast<long long>(ld) * k];
+    }
+    __syncthreads();
+  }
+  if (mine) bc[t] = x[t];
+}
+
 // Every 128-byte line of [p, p + bytes) into L2 with the evict-last
 // priority, from the whole grid (the prefetches return at once; the lines
 // arrive at HBM bandwidth while later kernels run).
@@ -865,17 +1012,12 @@ __device__ __forceinline__ void fused_swaps(double* blk, int np, int n, int j0, 
   }
 }
 
-// This CTA's panel when every row has its own thread (n <= kFusedThreads):
-// thread t holds row t's block columns in registers, and each column costs
-// one barrier.  Before it, every warp publishes its best candidate (key,
-// row) and that row whole, and the owner of row `col` publishes row col;
-// after it, every thread agrees on the pivot p from the 16 warp maxima and
-// reads the pivot row from its warp's slot, rows col and p trade values, and
-// the rows below apply the rank-one update in registers.  The slots are
-// double-buffered by column parity: column jj + 2 writes a slot only after
-// the barrier of column jj + 1, which every thread reaches after its reads
-// of column jj.  Same pivots and the same arithmetic (l = x * (1 / piv),
-// x_c -= l * prow_c) as the shared-memory panel.
+// The slots through which a register panel's column step publishes, before
+// its barrier, each warp's best candidate (key, row) and that row whole, and
+// row `col` (the one the pivot row trades places with).  Double-buffered by
+// column parity: column jj + 2 writes a slot only after the barrier of
+// column jj + 1, which every panel thread reaches after its reads of column
+// jj.
 struct __align__(16) PanelSlots {
   double cand[2][kFusedThreads / 32][kNb];
   double crow[2][kNb];
@@ -883,144 +1025,99 @@ struct __align__(16) PanelSlots {
   int idx[2][kFusedThreads / 32];
 };
 
-__device__ __forceinline__ void fused_panel_regs(double* blk, int np, int n, int c0, int wb,
-                                                 int* ipiv, int* status, PanelSlots& S) {
-  const int i = threadIdx.x, lane = i & 31, warp = i >> 5;
-  double x[kNb];
+// The 32-column panel is factored as two halves of 16 columns, as a
+// recursive LU does: the left half in registers, its interchanges then
+// applied to the right half, U12 = L11^{-1} A12 and A22 -= L21 U12 (FP64
+// tensor cores) on the right half, the right half factored the same way,
+// and its interchanges applied to the left half.  The pivots are those of
+// the 32-column panel; the sums run in another order.
+constexpr int kHalf = kNb / 2;
+
+// The barrier of the panel threads (the first T of the block): the block's
+// own when all take part, else named barrier 1 (the other warps wait at the
+// block barrier that follows the half).
+template <int T>
+__device__ __forceinline__ void panel_sync() {
+  if (T == kFusedThreads) {
+    __syncthreads();
+  } else {
+    asm volatile("bar.sync 1, %0;" ::"n"(T) : "memory");
+  }
+}
+
+// Factors block columns cb .. cb + wh - 1 (absolute c0 + cb + jj) over rows
+// >= c0 + cb in registers, interchanges restricted to those columns; the
+// pivots also go to hp[0 .. wh).  Called by threads t < T only, thread t
+// holding rows t + T q (q < R; T R >= n).  Each column costs one barrier of
+// the T threads: before it every warp publishes its best candidate and that
+// row, and the owner of row col publishes row col; after it every thread
+// agrees on the pivot p from the T / 32 warp maxima, reads the pivot row
+// from the slot of the warp holding it, rows col and p trade values and the
+// rows below apply the rank-one update.  Pivot rule: the largest |a(i, col)|
+// over rows i >= col, the first such row on ties, a NaN no candidate.
+// Arithmetic: l = x * (1 / piv), x_c -= l * prow_c.  Fewer panel threads than
+// the block's 512 (256 with two or three rows each) shorten the column step:
+// half the warps to reduce and to synchronise, the same rank-one work.
+// Not inlined: the two calls share its code, and inside the fused kernel
+// (128 registers a thread) an inlined copy spills in the column loop.
+template <int T, int R>
+__device__ __noinline__ void fused_half_rt(double* blk, int np, int n, int c0, int cb, int wh,
+                                              int* ipiv, int* status, PanelSlots& S, int* hp) {
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  double x[R][kHalf];
 #pragma unroll
-  for (int c = 0; c < kNb; c++) x[c] = i < n && c < wb ? blk[i + np * c] : 0.0;
+  for (int q = 0; q < R; q++)
 #pragma unroll
-  for (int jj = 0; jj < kNb; jj++) {
-    if (jj >= wb) break;
-    const int col = c0 + jj, buf = jj & 1;
-    // candidates: |x| of rows >= col (a NaN is no candidate), the largest,
-    // the first such row on ties
-    const double v = fabs(x[jj]);
-    const bool is_cand = i >= col && i < n && v == v;
+    for (int c = 0; c < kHalf; c++) {
+      const int row = t + T * q;
+      x[q][c] = row < n && c < wh ? blk[row + np * (cb + c)] : 0.0;
+    }
+#pragma unroll
+  for (int jj = 0; jj < kHalf; jj++) {
+    if (jj >= wh) break;
+    const int col = c0 + cb + jj, buf = jj & 1;
+    unsigned long long key = 0;
+    int idx = 0x7fffffff;
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      const int row = t + T * q;
+      const double v = fabs(x[q][jj]);
+      const unsigned long long k = static_cast<unsigned long long>(__double_as_longlong(v));
+      if (row >= col && row < n && v == v && (idx == 0x7fffffff || k > key)) {
+        key = k;
+        idx = row;
+      }
+    }
     unsigned long long wkey;
     int widx;
-    warp_argmax_bits(is_cand ? static_cast<unsigned long long>(__double_as_longlong(v)) : 0ull,
-                     is_cand ? i : 0x7fffffff, &wkey, &widx);
+    warp_argmax_bits(key, idx, &wkey, &widx);
     if (lane == 0) {
       S.key[buf][warp] = wkey;
       S.idx[buf][warp] = widx;
     }
     // (rows moved as pairs of doubles: half the shared-memory instructions)
-    if (i == widx) {
-      double2* d = reinterpret_cast<double2*>(S.cand[buf][warp]);
 #pragma unroll
-      for (int q = 0; q < kNb / 2; q++) d[q] = make_double2(x[2 * q], x[2 * q + 1]);
-    }
-    if (i == col) {
-      double2* d = reinterpret_cast<double2*>(S.crow[buf]);
+    for (int q = 0; q < R; q++) {
+      const int row = t + T * q;
+      if (row == widx) {
+        double2* d = reinterpret_cast<double2*>(S.cand[buf][warp]);
 #pragma unroll
-      for (int q = 0; q < kNb / 2; q++) d[q] = make_double2(x[2 * q], x[2 * q + 1]);
+        for (int h = 0; h < kHalf / 2; h++) d[h] = make_double2(x[q][2 * h], x[q][2 * h + 1]);
+      }
+      if (row == col) {
+        double2* d = reinterpret_cast<double2*>(S.crow[buf]);
+#pragma unroll
+        for (int h = 0; h < kHalf / 2; h++) d[h] = make_double2(x[q][2 * h], x[q][2 * h + 1]);
+      }
     }
-    __syncthreads();
+    panel_sync<T>();
     unsigned long long gkey;
     int p;
-    warp_argmax_bits(lane < kFusedThreads / 32 ? S.key[buf][lane] : 0ull,
-                     lane < kFusedThreads / 32 ? S.idx[buf][lane] : 0x7fffffff, &gkey, &p);
+    warp_argmax_bits(lane < T / 32 ? S.key[buf][lane] : 0ull,
+                     lane < T / 32 ? S.idx[buf][lane] : 0x7fffffff, &gkey, &p);
     // no comparable entry (NaN column): keep the row, flag the factorization
     const bool bad = p < col || p >= n;
-    const double* prow = bad ? S.crow[buf] : S.cand[buf][p >> 5];
-    if (bad) p = col;
-    const double piv = prow[jj];
-    if (i == 0) {
-      ipiv[col] = p;
-      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
-    }
-    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
-    const double2* prow2 = reinterpret_cast<const double2*>(prow);
-    if (i == col || i == p) {
-      const double2* src = i == col ? prow2 : reinterpret_cast<const double2*>(S.crow[buf]);
-#pragma unroll
-      for (int q = 0; q < kNb / 2; q++) {
-        const double2 t = src[q];
-        x[2 * q] = t.x;
-        x[2 * q + 1] = t.y;
-      }
-    }
-    if (i > col && i < n) {
-      const double li = x[jj] * inv;
-#pragma unroll
-      for (int q = (jj + 1) / 2; q < kNb / 2; q++) {
-        const double2 t = prow2[q];
-        if (2 * q > jj) x[2 * q] -= li * t.x;
-        x[2 * q + 1] -= li * t.y;
-      }
-      x[jj] = li;
-    }
-  }
-  if (i >= c0 && i < n) {
-#pragma unroll
-    for (int c = 0; c < kNb; c++)
-      if (c < wb) blk[i + np * c] = x[c];
-  }
-}
-
-// The panel for 512 < n <= 2 * kFusedThreads: each thread holds rows t and
-// t + 512, the block's 32 columns factored as two halves of 16 (the
-// registers of two 32-column rows would not fit), as a recursive LU does:
-// the left half in registers (pivot search, interchanges and rank-one
-// updates inside its 16 columns, one barrier per column as above), its
-// interchanges then applied to the right half, U12 = L11^{-1} A12 and
-// A22 -= L21 U12 (FP64 tensor cores) on the right half, the right half
-// factored the same way, and its interchanges applied to the left half.
-// The pivots are those of the 32-column panel; the sums run in another order.
-constexpr int kHalf = kNb / 2;
-
-// Factors block columns cb .. cb + wh - 1 (absolute c0 + cb + jj) over
-// rows >= c0 + cb in registers, interchanges restricted to those columns;
-// the pivots also go to hp[0 .. wh).
-__device__ __forceinline__ void fused_half_regs2(double* blk, int np, int n, int c0, int cb,
-                                                 int wh, int* ipiv, int* status, PanelSlots& S,
-                                                 int* hp) {
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int i0 = t, i1 = t + kFusedThreads;  // this thread's rows
-  double x0[kHalf], x1[kHalf];
-#pragma unroll
-  for (int c = 0; c < kHalf; c++) {
-    x0[c] = i0 < n && c < wh ? blk[i0 + np * (cb + c)] : 0.0;
-    x1[c] = i1 < n && c < wh ? blk[i1 + np * (cb + c)] : 0.0;
-  }
-#pragma unroll
-  for (int jj = 0; jj < kHalf; jj++) {
-    if (jj >= wh) break;
-    const int col = c0 + cb + jj, buf = jj & 1;
-    // this thread's candidate: the larger of its two rows (the first on ties)
-    const double v0 = fabs(x0[jj]), v1 = fabs(x1[jj]);
-    const bool c0ok = i0 >= col && i0 < n && v0 == v0;
-    const bool c1ok = i1 >= col && i1 < n && v1 == v1;
-    const unsigned long long k0 = c0ok ? static_cast<unsigned long long>(__double_as_longlong(v0)) : 0ull;
-    const unsigned long long k1 = c1ok ? static_cast<unsigned long long>(__double_as_longlong(v1)) : 0ull;
-    const bool take1 = c1ok && (!c0ok || k1 > k0);
-    unsigned long long wkey;
-    int widx;
-    warp_argmax_bits(take1 ? k1 : k0, take1 ? i1 : (c0ok ? i0 : 0x7fffffff), &wkey, &widx);
-    if (lane == 0) {
-      S.key[buf][warp] = wkey;
-      S.idx[buf][warp] = widx;
-    }
-    if (widx == i0 || widx == i1) {
-      const bool w1 = widx == i1;
-#pragma unroll
-      for (int c = 0; c < kHalf; c++) S.cand[buf][warp][c] = w1 ? x1[c] : x0[c];
-    }
-    if (col == i0 || col == i1) {
-      const bool w1 = col == i1;
-#pragma unroll
-      for (int c = 0; c < kHalf; c++) S.crow[buf][c] = w1 ? x1[c] : x0[c];
-    }
-    __syncthreads();
-    unsigned long long gkey;
-    int p;
-    warp_argmax_bits(lane < kFusedThreads / 32 ? S.key[buf][lane] : 0ull,
-                     lane < kFusedThreads / 32 ? S.idx[buf][lane] : 0x7fffffff, &gkey, &p);
-    const bool bad = p < col || p >= n;
-    // the winning row sits in the slot of the warp holding it (row p is
-    // thread p mod 512's)
-    const double* prow = bad ? S.crow[buf] : S.cand[buf][(p % kFusedThreads) >> 5];
+    const double* prow = bad ? S.crow[buf] : S.cand[buf][(p % T) >> 5];
     if (bad) p = col;
     const double piv = prow[jj];
     if (t == 0) {
@@ -1029,42 +1126,44 @@ __device__ __forceinline__ void fused_half_regs2(double* blk, int np, int n, int
       if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
     }
     const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
-    // interchange (rows col and p trade their 16 values), then the update
-    if (i0 == col) {
+    const double2* prow2 = reinterpret_cast<const double2*>(prow);
+    // interchange (rows col and p trade their values), then the update
 #pragma unroll
-      for (int c = 0; c < kHalf; c++) x0[c] = prow[c];
-    } else if (i0 == p) {
+    for (int q = 0; q < R; q++) {
+      const int row = t + T * q;
+      if (row == col || row == p) {
+        const double2* src = row == col ? prow2 : reinterpret_cast<const double2*>(S.crow[buf]);
 #pragma unroll
-      for (int c = 0; c < kHalf; c++) x0[c] = S.crow[buf][c];
+        for (int h = 0; h < kHalf / 2; h++) {
+          const double2 u = src[h];
+          x[q][2 * h] = u.x;
+          x[q][2 * h + 1] = u.y;
+        }
+      }
     }
-    if (i1 == col) {
 #pragma unroll
-      for (int c = 0; c < kHalf; c++) x1[c] = prow[c];
-    } else if (i1 == p) {
+    for (int q = 0; q < R; q++) {
+      const int row = t + T * q;
+      if (row > col && row < n) {
+        const double li = x[q][jj] * inv;
 #pragma unroll
-      for (int c = 0; c < kHalf; c++) x1[c] = S.crow[buf][c];
-    }
-    if (i0 > col && i0 < n) {
-      const double li = x0[jj] * inv;
-#pragma unroll
-      for (int c = jj + 1; c < kHalf; c++) x0[c] -= li * prow[c];
-      x0[jj] = li;
-    }
-    if (i1 > col && i1 < n) {
-      const double li = x1[jj] * inv;
-#pragma unroll
-      for (int c = jj + 1; c < kHalf; c++) x1[c] -= li * prow[c];
-      x1[jj] = li;
+        for (int h = (jj + 1) / 2; h < kHalf / 2; h++) {
+          const double2 u = prow2[h];
+          if (2 * h > jj) x[q][2 * h] -= li * u.x;
+          x[q][2 * h + 1] -= li * u.y;
+        }
+        x[q][jj] = li;
+      }
     }
   }
   const int rmin = c0 + cb;
 #pragma unroll
-  for (int c = 0; c < kHalf; c++) {
-    if (c < wh) {
-      if (i0 >= rmin && i0 < n) blk[i0 + np * (cb + c)] = x0[c];
-      if (i1 >= rmin && i1 < n) blk[i1 + np * (cb + c)] = x1[c];
+  for (int q = 0; q < R; q++)
+#pragma unroll
+    for (int c = 0; c < kHalf; c++) {
+      const int row = t + T * q;
+      if (c < wh && row >= rmin && row < n) blk[row + np * (cb + c)] = x[q][c];
     }
-  }
 }
 
 // The row interchanges hp[0 .. cnt) of rows r0 + jj, on block columns
@@ -1084,12 +1183,13 @@ __device__ __forceinline__ void half_swaps(double* blk, int np, int n, int r0, i
   }
 }
 
+template <int T, int R>
 __device__ __forceinline__ void fused_panel_split(double* blk, int np, int n, int c0, int wb,
                                                   int* ipiv, int* status, PanelSlots& S,
                                                   int* hp) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wl = min(kHalf, wb), wr = wb - wl;
-  fused_half_regs2(blk, np, n, c0, 0, wl, ipiv, status, S, hp);
+  if (threadIdx.x < T) fused_half_rt<T, R>(blk, np, n, c0, 0, wl, ipiv, status, S, hp);
   __syncthreads();
   if (wr <= 0) return;
   // the left half's interchanges on the right half
@@ -1139,7 +1239,7 @@ __device__ __forceinline__ void fused_panel_split(double* blk, int np, int n, in
     }
   }
   __syncthreads();
-  fused_half_regs2(blk, np, n, c0, kHalf, wr, ipiv, status, S, hp + kHalf);
+  if (threadIdx.x < T) fused_half_rt<T, R>(blk, np, n, c0, kHalf, wr, ipiv, status, S, hp + kHalf);
   __syncthreads();
   // the right half's interchanges on the left half
   half_swaps(blk, np, n, c0 + kHalf, wr, hp + kHalf, 0, wl);
@@ -1147,16 +1247,13 @@ __device__ __forceinline__ void fused_panel_split(double* blk, int np, int n, in
 
 // hold (a test hook, normally 0): thread block 0 keeps its flag down, so the
 // other blocks' bounded waits run out and the launch ends with status 2.
-// kPanel: 1 (n <= kFusedThreads) the panel in registers; 2 (n <= 2
-// kFusedThreads) in registers as two halves; 0 in shared memory (one
-// instantiation per panel form keeps each one's registers to itself).
+// kPanel: the rows each of the 256 panel threads holds (2: n <= 512, 3: n
+// <= 768; one instantiation per form keeps each one's registers to itself).
 template <int kPanel>
 __global__ void __launch_bounds__(kFusedThreads, 1)
     lu_fused_kernel(double* a, int n, int ld, int* ipiv, int* status, int* sync, int hold) {
   extern __shared__ double blk[];  // np x kNb, column-major
   __shared__ double l11[kNb][kNb + 1];
-  __shared__ unsigned long long redk[kFusedThreads / 32];
-  __shared__ int redi[kFusedThreads / 32];
   __shared__ int pv[kNb];
   __shared__ int s_ok;
   __shared__ PanelSlots slots;
@@ -1271,69 +1368,8 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     __syncthreads();
   }
 
-  // this CTA's panel: in registers when every row has a thread, else in
-  // shared memory (thread t owning rows t + 512 q, two barriers a column)
-  if (kPanel == 1) fused_panel_regs(blk, np, n, c0, wb, ipiv, status, slots);
-  if (kPanel == 2) fused_panel_split(blk, np, n, c0, wb, ipiv, status, slots, half_piv);
-  for (int jj = 0; jj < wb && kPanel == 0; jj++) {
-    const int col = c0 + jj;
-    // candidates: |a_ij| for rows i >= col (a NaN is no candidate); the
-    // largest, the first such row on ties
-    unsigned long long key = 0;
-    int idx = 0x7fffffff;
-    for (int i = tid; i < n; i += kFusedThreads) {
-      if (i < col) continue;
-      const double v = fabs(blk[i + np * jj]);
-      if (v == v) {
-        const unsigned long long kv = static_cast<unsigned long long>(__double_as_longlong(v));
-        if (idx == 0x7fffffff || kv > key) {
-          key = kv;
-          idx = i;
-        }
-      }
-    }
-    unsigned long long wk2;
-    int wi;
-    warp_argmax_bits(key, idx, &wk2, &wi);
-    if (lane == 0) {
-      redk[warp] = wk2;
-      redi[warp] = wi;
-    }
-    __syncthreads();
-    int p;
-    {
-      unsigned long long k2;
-      warp_argmax_bits(lane < kFusedThreads / 32 ? redk[lane] : 0ull,
-                       lane < kFusedThreads / 32 ? redi[lane] : 0x7fffffff, &k2, &p);
-    }
-    // no comparable entry (NaN column): keep the row, flag the factorization
-    const bool bad = p < col || p >= n;
-    if (bad) p = col;
-    if (tid < wb && p != col) {
-      const double t = blk[col + np * tid];
-      blk[col + np * tid] = blk[p + np * tid];
-      blk[p + np * tid] = t;
-    }
-    __syncthreads();
-    const double piv = blk[col + np * jj];
-    if (tid == 0) {
-      ipiv[col] = p;
-      if (piv == 0.0 || bad || isinf(piv)) atomicExch(status, 1);
-    }
-    const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
-    for (int i = tid; i < n; i += kFusedThreads) {
-      if (i <= col) continue;
-      // the pivot row and this row never alias (i > col): loads may run ahead
-      const double* __restrict__ prow = blk + col;
-      double* __restrict__ row = blk + i;
-      const double li = row[np * jj] * inv;
-#pragma unroll 4
-      for (int c = jj + 1; c < wb; c++) row[np * c] -= li * prow[np * c];
-      row[np * jj] = li;
-    }
-    // the next column's barrier orders these updates before its
-    // interchange; the pivot row is not updated
-  }
+  // this CTA's panel, in registers
+  fused_panel_split<256, kPanel>(blk, np, n, c0, wb, ipiv, status, slots, half_piv);
   __syncthreads();
   for (int e = tid; e < n * wb; e += kFusedThreads) {
     const int i = e % n, c = e / n;
@@ -1376,9 +1412,9 @@ cudaError_t dense_lu(double* a, int n, int ld, int* ipiv, int* status, cudaStrea
   if (sync && n > 0 && n <= kLuFusedMaxN) {
     int G = (n + kNb - 1) / kNb;
     const size_t smem = sizeof(double) * static_cast<size_t>(n | 1) * kNb;
-    const void* fn = n <= kFusedThreads       ? reinterpret_cast<const void*>(&lu_fused_kernel<1>)
-                     : n <= 2 * kFusedThreads ? reinterpret_cast<const void*>(&lu_fused_kernel<2>)
-                                              : reinterpret_cast<const void*>(&lu_fused_kernel<0>);
+    static_assert(kLuFusedMaxN <= 3 * 256, "three rows per panel thread at most");
+    const void* fn = n <= 512 ? reinterpret_cast<const void*>(&lu_fused_kernel<2>)
+                              : reinterpret_cast<const void*>(&lu_fused_kernel<3>);
     cudaError_t e = raise_func_attr(fn,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem));
@@ -1493,9 +1529,20 @@ cudaError_t launch_l2_prefetch(const void* p, size_t bytes, cudaStream_t s) {
 }
 
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
-                           int nrhs, int ldb, cudaStream_t s, const int* perm) {
+                           int nrhs, int ldb, cudaStream_t s, const int* perm,
+                           const double* dinv) {
   if (n == 0 || nrhs == 0) return cudaSuccess;
   count_launches(1);
+  if (dinv && perm && n <= kInvSolveThreads) {
+    const int nblk = (n + kInvBlk - 1) / kInvBlk;
+    const size_t ism = sizeof(double) * static_cast<size_t>(nblk) * (2 * kInvBlk * kInvBlk + kInvBlk);
+    const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_solve_inv_kernel),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(ism));
+    if (e != cudaSuccess) return e;
+    lu_solve_inv_kernel<<<nrhs, kInvSolveThreads, ism, s>>>(lu, n, ld, dinv, perm, b, ldb);
+    return cudaGetLastError();
+  }
   const size_t smem = (sizeof(double) + sizeof(int)) * static_cast<size_t>(n);
   if (n >= 64 && smem <= kSolveSmemMax) {
     const cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&lu_solve_cta_kernel),
@@ -1507,6 +1554,14 @@ cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, dou
   }
   const int per = 4;
   lu_solve_kernel<<<(nrhs + per - 1) / per, 32 * per, 0, s>>>(lu, n, ld, ipiv, b, nrhs, ldb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lu_block_inv(const double* lu, int n, int ld, double* dinv, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launches(1);
+  const int nblk = (n + kInvBlk - 1) / kInvBlk;
+  lu_block_inv_kernel<<<(nblk + 3) / 4, 128, 0, s>>>(lu, n, ld, dinv);
   return cudaGetLastError();
 }
 

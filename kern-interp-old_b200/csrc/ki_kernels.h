@@ -214,9 +214,18 @@ cudaError_t launch_gemm_sub(double* C, int ldc, const double* C0, int ldc0, cons
 cudaError_t dense_lu_solve_rows(const double* lu, int n, int ld, const int* ipiv, double* b,
                                 int nrows, int ldb, cudaStream_t s);
 // B <- A^{-1} B (n x nrhs, ldb) for the LU above; perm (optional, from
-// launch_pivots_to_perm) replaces the sequential interchanges by a gather.
+// launch_pivots_to_perm) replaces the sequential interchanges by a gather;
+// dinv (optional, with perm, n <= kLuBlockInvMaxN: launch_lu_block_inv)
+// the inverted 16 x 16 diagonal blocks, applied as products in place of
+// the in-block substitutions.
 cudaError_t dense_lu_solve(const double* lu, int n, int ld, const int* ipiv, double* b,
-                           int nrhs, int ldb, cudaStream_t s, const int* perm = nullptr);
+                           int nrhs, int ldb, cudaStream_t s, const int* perm = nullptr,
+                           const double* dinv = nullptr);
+// The inverses of the 16 x 16 diagonal blocks of L and U of an n x n LU:
+// lu_block_inv_doubles(n) doubles at dinv.
+constexpr int kLuBlockInvMaxN = 768;
+inline size_t lu_block_inv_doubles(int n) { return static_cast<size_t>((n + 15) / 16) * 512; }
+cudaError_t launch_lu_block_inv(const double* lu, int n, int ld, double* dinv, cudaStream_t s);
 // Brings [p, p + bytes) into L2 (evict-last priority) from a whole grid of
 // prefetches; returns as soon as they are issued.
 cudaError_t launch_l2_prefetch(const void* p, size_t bytes, cudaStream_t s);

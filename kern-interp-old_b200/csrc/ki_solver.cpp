@@ -1411,6 +1411,7 @@ void Solver::drop_device_state() {
   d_top_ = nullptr;
   d_top_piv_ = nullptr;
   d_top_perm_ = nullptr;
+  d_top_dinv_ = nullptr;
   d_allskel_ = d_allred_ = d_red_pos_ = nullptr;
   d_U_ = d_Psi_ = d_Urow_ = d_Ured_ = d_Pred_ = d_tmp_ = nullptr;
   d_modU_ = d_modP_ = nullptr;
@@ -1720,8 +1721,14 @@ int Solver::factor_top() {
   KI_ALLOC(lu_sync, int, kLuSyncInts);
   if (ntop > 0)
     KI_CUDA(dense_lu(d_top_, ntop, ntop, d_top_piv_, d_status_, stream_, lu_sync, true));
-  // the interchanges composed once, so each solve gathers instead
+  // the interchanges composed once, so each solve gathers instead, and the
+  // factors' 16 x 16 diagonal blocks inverted, so each solve multiplies
+  // instead of substituting within a block
   if (ntop > 0) KI_CUDA(launch_pivots_to_perm(d_top_piv_, ntop, d_top_perm_, stream_));
+  if (ntop > 0 && ntop <= kLuBlockInvMaxN) {
+    KI_ALLOC(d_top_dinv_, double, lu_block_inv_doubles(ntop));
+    KI_CUDA(launch_lu_block_inv(d_top_, ntop, ntop, d_top_dinv_, stream_));
+  }
   if (time_phases && timer_end(l0, {0, 4, 1, 1, 0, ntop, 0.0})) return -2;
   return 0;
 }
@@ -1806,7 +1813,8 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
     if (diag_all(dp, false)) return -2;
     if (ns > 0) {
       KI_CUDA(launch_gather(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
-      KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_, d_top_perm_));
+      KI_CUDA(dense_lu_solve(d_top_, ns, ns, d_top_piv_, d_tmp_, 1, ns, stream_, d_top_perm_,
+                             d_top_dinv_));
       KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
     }
   } else {
@@ -1833,7 +1841,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
                          M + ns, nb, stream_));
     }
     KI_CUDA(dense_lu_solve(d_top_, ns + nb, ns + nb, d_top_piv_, M, 1, ns + nb, stream_,
-                           d_top_perm_));
+                           d_top_perm_, d_top_dinv_));
     if (d_alpha)
       KI_CUDA(cudaMemcpyAsync(d_alpha, M + ns, sizeof(double) * nb, cudaMemcpyDeviceToDevice,
                               stream_));

@@ -388,6 +388,7 @@ class Solver {
   double* d_top_ = nullptr;  // LU of allskel_mat, or of S with holes
   int* d_top_piv_ = nullptr;
   int* d_top_perm_ = nullptr;  // the top LU's interchanges as one permutation
+  double* d_top_dinv_ = nullptr;  // its inverted 16 x 16 diagonal blocks (or nullptr)
   int* d_allskel_ = nullptr;
   int* d_allred_ = nullptr;
   int* d_red_pos_ = nullptr;
