@@ -1278,13 +1278,25 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   for (int k = 0; k < b; k++) {
     if (!fused_wait(sync, k, G, status, &s_ok)) return;
     const int j0 = kNb * k, wk = min(kNb, n - j0);
-    for (int e = tid; e < wk * wk; e += kFusedThreads) {
-      const int i = e % wk, kk = e / wk;
-      l11[i][kk] = __ldcg(a + j0 + i + static_cast<long long>(ld) * (j0 + kk));
+    if (warp == 0) {
+      // the step's interchanges on this block (a lane per column, pivots
+      // by shuffle) while the other warps bring L11 in
+      const int pr = lane < wk ? __ldcg(ipiv + j0 + lane) : 0;
+      for (int jj = 0; jj < wk; jj++) {
+        const int p = __shfl_sync(0xffffffffu, pr, jj), r = j0 + jj;
+        if (lane < wb && p > r && p < n) {
+          const double t = blk[r + np * lane];
+          blk[r + np * lane] = blk[p + np * lane];
+          blk[p + np * lane] = t;
+        }
+      }
+    } else {
+      for (int e = tid - 32; e < kNb * kNb; e += kFusedThreads - 32) {
+        const int i = e & (kNb - 1), kk = e / kNb;
+        if (i < wk && kk < wk)
+          l11[i][kk] = __ldcg(a + j0 + i + static_cast<long long>(ld) * (j0 + kk));
+      }
     }
-    if (tid < wk) pv[tid] = __ldcg(ipiv + j0 + tid);
-    __syncthreads();
-    fused_swaps(blk, np, n, j0, wk, wb, pv);
     __syncthreads();
     // U12 = L11^{-1} A12, one warp per two columns (interleaved), in the kk
     // order of the panel-by-panel path
@@ -1371,15 +1383,19 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
   // this CTA's panel, in registers
   fused_panel_split<256, kPanel>(blk, np, n, c0, wb, ipiv, status, slots, half_piv);
   __syncthreads();
-  for (int e = tid; e < n * wb; e += kFusedThreads) {
-    const int i = e % n, c = e / n;
-    __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
-  }
+  // the rows the later blocks read (this panel's L11, L21 and U11) before
+  // the flag, the U12 rows above after it
+  for (int i = c0 + tid; i < n; i += kFusedThreads)
+#pragma unroll 4
+    for (int c = 0; c < wb; c++) __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
   __syncthreads();
   if (tid == 0 && !(hold && b == 0)) {
     __threadfence();
     st_release_gpu(sync + b, 1);
   }
+  for (int i = tid; i < c0; i += kFusedThreads)
+#pragma unroll 4
+    for (int c = 0; c < wb; c++) __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
   if (b + 1 == G) return;
 
   // the later steps' interchanges on this block's L rows, then those rows
@@ -1394,10 +1410,9 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
     __syncthreads();
   }
   const int r1 = c0 + kNb;
-  for (int e = tid; e < (n - r1) * wb; e += kFusedThreads) {
-    const int i = r1 + e % (n - r1), c = e / (n - r1);
-    __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
-  }
+  for (int i = r1 + tid; i < n; i += kFusedThreads)
+#pragma unroll 4
+    for (int c = 0; c < wb; c++) __stcg(a + i + static_cast<long long>(ld) * (c0 + c), blk[i + np * c]);
 }
 }  // namespace
 
