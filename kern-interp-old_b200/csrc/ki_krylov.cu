@@ -142,41 +142,63 @@ __global__ void __launch_bounds__(kMvThreads)
 // spacing h beyond the gap this is ~ u32 diam w / (h g) per unit density,
 // 1e-6 for g = 0.01 on the workloads here.  Partials, rank-one slots and the
 // finish are those of the FP64 product.
+//
+// A thread owns two targets of the 256-target tile, t and t + 128, as the two
+// lanes of Blackwell's packed FP32 instructions (FADD2 / FMUL2 / FFMA2, one
+// issue for both lanes): each source's values sit in shared memory twice,
+// {v, v}, so a 16-byte load yields the packed operands of both lanes.  Every
+// lane rounds exactly as the scalar fmaf, product or sum it stands for, so a
+// target's sums are those of one target per thread; the packing halves the
+// FP32 instructions the issue slots carry (loads, MUFU and FP32 shared them).
+constexpr int kCorrThreads = kMvThreads / 2;
+
 template <int PDE>
-__global__ void __launch_bounds__(kMvThreads)
+__global__ void __launch_bounds__(kCorrThreads)
     mv_corr_partial_kernel(const Node* __restrict__ nodes, const MvTile* __restrict__ tiles,
                            long long part_stride, const double* __restrict__ x, double dscale,
                            float near2, double* __restrict__ part,
                            double* __restrict__ part_rank1) {
   __shared__ double sx[kMvThreads], sy[kMvThreads], sa0[kMvThreads], sa1[kMvThreads];
   __shared__ double sd0[kMvThreads], sd1[kMvThreads];
-  __shared__ float fx[kMvThreads], fy[kMvThreads], fa0[kMvThreads], fa1[kMvThreads];
-  __shared__ float fd0[kMvThreads], fd1[kMvThreads];
-  __shared__ float wbox[2][4][kMvThreads / 32];  // per-warp box: [target|source][x0,y0,-x1,-y1]
-  __shared__ double red[kMvThreads / 32];
+  // FP32 source values relative to the tile origin, each twice:
+  // pos {-x, -x, -y, -y}, amp {a0, a0, a1, a1}, den {d0, d0, d1, d1}
+  __shared__ float4 fpos[kMvThreads], famp[kMvThreads], fden[kMvThreads];
+  __shared__ float wbox[2][4][kCorrThreads / 32];  // per-warp box: [target|source][x0,y0,-x1,-y1]
+  __shared__ double red[kCorrThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const MvTile tile = tiles[blockIdx.x];
-  const int t = tile.t0 + threadIdx.x;
   const int s0 = tile.s0, s1 = tile.s1;
-  const bool live = t < tile.t1;
   const Node org = nodes[tile.t0];
   const double ox = org.x, oy = org.y;
   const double inv_scale = 1.0 / dscale;
-  double tx = 0, ty = 0, tnx = 0, tny = 0;
-  if (live) {
-    const Node nt = nodes[t];
-    tx = nt.x;
-    ty = nt.y;
-    tnx = nt.nx;
-    tny = nt.ny;
+  double tx[2], ty[2], tnx[2], tny[2];
+  bool live[2];
+  float ftx[2], fty[2], ftnx[2], ftny[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int t = tile.t0 + threadIdx.x + h * kCorrThreads;
+    live[h] = t < tile.t1;
+    tx[h] = ty[h] = tnx[h] = tny[h] = 0.0;
+    if (live[h]) {
+      const Node nt = nodes[t];
+      tx[h] = nt.x;
+      ty[h] = nt.y;
+      tnx[h] = nt.nx;
+      tny[h] = nt.ny;
+    }
+    ftx[h] = static_cast<float>(tx[h] - ox);
+    fty[h] = static_cast<float>(ty[h] - oy);
+    ftnx[h] = static_cast<float>(tnx[h]);
+    ftny[h] = static_cast<float>(tny[h]);
   }
-  const float ftx = static_cast<float>(tx - ox), fty = static_cast<float>(ty - oy);
-  const float ftnx = static_cast<float>(tnx), ftny = static_cast<float>(tny);
-  // bounding box of a point per thread over the CTA: warp min/max here, the
-  // per-warp results combined by every thread after the next barrier
-  auto warp_box = [&](int which, bool valid, float px, float py) {
-    float b0 = valid ? px : 3e38f, b1 = valid ? py : 3e38f;
-    float b2 = valid ? -px : 3e38f, b3 = valid ? -py : 3e38f;
+  // bounding box of a thread's two points over the CTA: warp min/max here,
+  // the per-warp results combined by every thread after the next barrier
+  auto warp_box = [&](int which, bool v0, float px0, float py0, bool v1, float px1,
+                      float py1) {
+    float b0 = fminf(v0 ? px0 : 3e38f, v1 ? px1 : 3e38f);
+    float b1 = fminf(v0 ? py0 : 3e38f, v1 ? py1 : 3e38f);
+    float b2 = fminf(v0 ? -px0 : 3e38f, v1 ? -px1 : 3e38f);
+    float b3 = fminf(v0 ? -py0 : 3e38f, v1 ? -py1 : 3e38f);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       b0 = fminf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
@@ -194,110 +216,131 @@ __global__ void __launch_bounds__(kMvThreads)
   auto cta_box = [&](int which, int c) {
     float b = 3e38f;
 #pragma unroll
-    for (int w = 0; w < kMvThreads / 32; w++) b = fminf(b, wbox[which][c][w]);
+    for (int w = 0; w < kCorrThreads / 32; w++) b = fminf(b, wbox[which][c][w]);
     return b;
   };
-  warp_box(0, live, ftx, fty);
-  double y0 = 0.0, y1 = 0.0, r1 = 0.0;
+  warp_box(0, live[0], ftx[0], fty[0], live[1], ftx[1], fty[1]);
+  const float2 tx2 = make_float2(ftx[0], ftx[1]), ty2 = make_float2(fty[0], fty[1]);
+  const float2 tnx2 = make_float2(ftnx[0], ftnx[1]), tny2 = make_float2(ftny[0], ftny[1]);
+  double y0[2] = {0.0, 0.0}, y1[2] = {0.0, 0.0}, r1 = 0.0;
   for (int base = s0; base < s1; base += kMvThreads) {
-    const int j = base + threadIdx.x;
     __syncthreads();
-    const bool valid = j < s1;
-    float fsx = 0.f, fsy = 0.f;
-    if (valid) {
-      const Node s = nodes[j];
-      sx[threadIdx.x] = s.x;
-      sy[threadIdx.x] = s.y;
-      fsx = static_cast<float>(s.x - ox);
-      fsy = static_cast<float>(s.y - oy);
-      if (PDE == kLaplace) {
-        const double c = -s.w * KI_INV_2PI * x[j];
-        sa0[threadIdx.x] = c * s.nx;
-        sa1[threadIdx.x] = c * s.ny;
-        fa0[threadIdx.x] = static_cast<float>(c * dscale * s.nx);
-        fa1[threadIdx.x] = static_cast<float>(c * dscale * s.ny);
-      } else if (PDE == kLaplaceNeumann) {
-        sa0[threadIdx.x] = s.w * KI_INV_2PI * x[j];
-        fa0[threadIdx.x] = static_cast<float>(s.w * KI_INV_2PI * (x[j] * dscale));
-        if (tile.first) r1 += s.w * x[j];
+    bool valid[2];
+    float fsx[2], fsy[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int k = threadIdx.x + h * kCorrThreads;  // staging slot
+      const int j = base + k;
+      valid[h] = j < s1;
+      float fa0 = 0.f, fa1 = 0.f, fd0 = 0.f, fd1 = 0.f;
+      if (valid[h]) {
+        const Node s = nodes[j];
+        sx[k] = s.x;
+        sy[k] = s.y;
+        fsx[h] = static_cast<float>(s.x - ox);
+        fsy[h] = static_cast<float>(s.y - oy);
+        if (PDE == kLaplace) {
+          const double c = -s.w * KI_INV_2PI * x[j];
+          sa0[k] = c * s.nx;
+          sa1[k] = c * s.ny;
+          fa0 = static_cast<float>(c * dscale * s.nx);
+          fa1 = static_cast<float>(c * dscale * s.ny);
+        } else if (PDE == kLaplaceNeumann) {
+          sa0[k] = s.w * KI_INV_2PI * x[j];
+          fa0 = static_cast<float>(s.w * KI_INV_2PI * (x[j] * dscale));
+          if (tile.first) r1 += s.w * x[j];
+        } else {
+          const double c = s.w * KI_INV_PI;
+          sa0[k] = c * s.nx;
+          sa1[k] = c * s.ny;
+          fa0 = static_cast<float>(c * s.nx);
+          fa1 = static_cast<float>(c * s.ny);
+          const double d0 = x[2 * j], d1 = x[2 * j + 1];
+          sd0[k] = d0;
+          sd1[k] = d1;
+          fd0 = static_cast<float>(d0 * dscale);
+          fd1 = static_cast<float>(d1 * dscale);
+          if (tile.first) r1 += s.w * (s.nx * d0 + s.ny * d1);
+        }
       } else {
-        const double c = s.w * KI_INV_PI;
-        sa0[threadIdx.x] = c * s.nx;
-        sa1[threadIdx.x] = c * s.ny;
-        fa0[threadIdx.x] = static_cast<float>(c * s.nx);
-        fa1[threadIdx.x] = static_cast<float>(c * s.ny);
-        const double d0 = x[2 * j], d1 = x[2 * j + 1];
-        sd0[threadIdx.x] = d0;
-        sd1[threadIdx.x] = d1;
-        fd0[threadIdx.x] = static_cast<float>(d0 * dscale);
-        fd1[threadIdx.x] = static_cast<float>(d1 * dscale);
-        if (tile.first) r1 += s.w * (s.nx * d0 + s.ny * d1);
+        // padding: a far source of zero strength
+        sx[k] = 1e15;
+        sy[k] = 1e15;
+        sa0[k] = sa1[k] = 0.0;
+        sd0[k] = sd1[k] = 0.0;
+        fsx[h] = fsy[h] = 1e15f;
       }
-    } else {
-      // padding: a far source of zero strength
-      sx[threadIdx.x] = 1e15;
-      sy[threadIdx.x] = 1e15;
-      sa0[threadIdx.x] = sa1[threadIdx.x] = 0.0;
-      sd0[threadIdx.x] = sd1[threadIdx.x] = 0.0;
-      fsx = fsy = 1e15f;
-      fa0[threadIdx.x] = fa1[threadIdx.x] = 0.f;
-      fd0[threadIdx.x] = fd1[threadIdx.x] = 0.f;
+      fpos[k] = make_float4(-fsx[h], -fsx[h], -fsy[h], -fsy[h]);
+      famp[k] = make_float4(fa0, fa0, fa1, fa1);
+      if (PDE == kStokes) fden[k] = make_float4(fd0, fd0, fd1, fd1);
     }
-    fx[threadIdx.x] = fsx;
-    fy[threadIdx.x] = fsy;
-    warp_box(1, valid, fsx, fsy);
+    warp_box(1, valid[0], fsx[0], fsy[0], valid[1], fsx[1], fsy[1]);
     __syncthreads();
     // gap between the boxes (0 when they overlap)
     const float gx = fmaxf(0.f, fmaxf(cta_box(1, 0) + cta_box(0, 2), cta_box(0, 0) + cta_box(1, 2)));
     const float gy = fmaxf(0.f, fmaxf(cta_box(1, 1) + cta_box(0, 3), cta_box(0, 1) + cta_box(1, 3)));
     if (gx * gx + gy * gy < near2) {
-#pragma unroll 4
+#pragma unroll 2
       for (int q = 0; q < kMvThreads; q++) {
-        const double r0 = tx - sx[q], rr1 = ty - sy[q];
-        const double rr = r0 * r0 + rr1 * rr1;
-        const double inv = rr > 0.0 ? nr_rcp(rr) : 0.0;
-        if (PDE == kLaplace) {
-          y0 += (r0 * sa0[q] + rr1 * sa1[q]) * inv;
-        } else if (PDE == kLaplaceNeumann) {
-          y0 += ((r0 * tnx + rr1 * tny) * sa0[q]) * inv;
-        } else {
-          const double rn = r0 * sa0[q] + rr1 * sa1[q];
-          const double rx = r0 * sd0[q] + rr1 * sd1[q];
-          const double pq = (rn * rx) * (inv * inv);
-          y0 += pq * r0;
-          y1 += pq * rr1;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const double r0 = tx[h] - sx[q], rr1 = ty[h] - sy[q];
+          const double rr = r0 * r0 + rr1 * rr1;
+          const double inv = rr > 0.0 ? nr_rcp(rr) : 0.0;
+          if (PDE == kLaplace) {
+            y0[h] += (r0 * sa0[q] + rr1 * sa1[q]) * inv;
+          } else if (PDE == kLaplaceNeumann) {
+            y0[h] += ((r0 * tnx[h] + rr1 * tny[h]) * sa0[q]) * inv;
+          } else {
+            const double rn = r0 * sa0[q] + rr1 * sa1[q];
+            const double rx = r0 * sd0[q] + rr1 * sd1[q];
+            const double pq = (rn * rx) * (inv * inv);
+            y0[h] += pq * r0;
+            y1[h] += pq * rr1;
+          }
         }
       }
     } else {
-      float f0 = 0.f, f1 = 0.f;
+      float2 f0 = make_float2(0.f, 0.f), f1 = make_float2(0.f, 0.f);
 #pragma unroll 8
       for (int q = 0; q < kMvThreads; q++) {
-        const float r0 = ftx - fx[q], rr1 = fty - fy[q];
-        const float rr = fmaf(r0, r0, rr1 * rr1);
-        float inv;
-        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(rr));
+        const float4 p = fpos[q], a = famp[q];
+        const float2 r0 = __fadd2_rn(tx2, make_float2(p.x, p.y));
+        const float2 rr1 = __fadd2_rn(ty2, make_float2(p.z, p.w));
+        const float2 rr = __ffma2_rn(r0, r0, __fmul2_rn(rr1, rr1));
+        float2 inv;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv.x) : "f"(rr.x));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(inv.y) : "f"(rr.y));
+        const float2 a0 = make_float2(a.x, a.y), a1 = make_float2(a.z, a.w);
         if (PDE == kLaplace) {
-          f0 = fmaf(fmaf(r0, fa0[q], rr1 * fa1[q]), inv, f0);
+          f0 = __ffma2_rn(__ffma2_rn(r0, a0, __fmul2_rn(rr1, a1)), inv, f0);
         } else if (PDE == kLaplaceNeumann) {
-          f0 = fmaf(fmaf(r0, ftnx, rr1 * ftny) * fa0[q], inv, f0);
+          f0 = __ffma2_rn(__fmul2_rn(__ffma2_rn(r0, tnx2, __fmul2_rn(rr1, tny2)), a0), inv, f0);
         } else {
-          const float rn = fmaf(r0, fa0[q], rr1 * fa1[q]);
-          const float rx = fmaf(r0, fd0[q], rr1 * fd1[q]);
-          const float pq = (rn * rx) * (inv * inv);
-          f0 = fmaf(pq, r0, f0);
-          f1 = fmaf(pq, rr1, f1);
+          const float4 d = fden[q];
+          const float2 rn = __ffma2_rn(r0, a0, __fmul2_rn(rr1, a1));
+          const float2 rx = __ffma2_rn(r0, make_float2(d.x, d.y),
+                                       __fmul2_rn(rr1, make_float2(d.z, d.w)));
+          const float2 pq = __fmul2_rn(__fmul2_rn(rn, rx), __fmul2_rn(inv, inv));
+          f0 = __ffma2_rn(pq, r0, f0);
+          f1 = __ffma2_rn(pq, rr1, f1);
         }
       }
-      y0 += static_cast<double>(f0) * inv_scale;
-      y1 += static_cast<double>(f1) * inv_scale;
+      y0[0] += static_cast<double>(f0.x) * inv_scale;
+      y0[1] += static_cast<double>(f0.y) * inv_scale;
+      y1[0] += static_cast<double>(f1.x) * inv_scale;
+      y1[1] += static_cast<double>(f1.y) * inv_scale;
     }
   }
-  if (live) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    if (!live[h]) continue;
+    const int t = tile.t0 + threadIdx.x + h * kCorrThreads;
     if (PDE == kStokes) {
-      part[part_stride * tile.split + 2 * t] = y0;
-      part[part_stride * tile.split + 2 * t + 1] = y1;
+      part[part_stride * tile.split + 2 * t] = y0[h];
+      part[part_stride * tile.split + 2 * t + 1] = y1[h];
     } else {
-      part[part_stride * tile.split + t] = y0;
+      part[part_stride * tile.split + t] = y0[h];
     }
   }
   if (PDE != kLaplace && tile.first) {
@@ -307,7 +350,7 @@ __global__ void __launch_bounds__(kMvThreads)
     __syncthreads();
     if (threadIdx.x == 0) {
       double v = 0.0;
-      for (int w = 0; w < kMvThreads / 32; w++) v += red[w];
+      for (int w = 0; w < kCorrThreads / 32; w++) v += red[w];
       part_rank1[tile.rank1_slot] = v;
     }
   }
@@ -608,13 +651,13 @@ cudaError_t launch_corr_matvec(int pde, const Node* nodes, const MvTile* tiles, 
   const float near2 = static_cast<float>(near_gap * near_gap);
   count_launches(nb ? 3 : 2);
   if (pde == kLaplace)
-    mv_corr_partial_kernel<kLaplace><<<ntiles, kMvThreads, 0, s>>>(
+    mv_corr_partial_kernel<kLaplace><<<ntiles, kCorrThreads, 0, s>>>(
         nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
   else if (pde == kLaplaceNeumann)
-    mv_corr_partial_kernel<kLaplaceNeumann><<<ntiles, kMvThreads, 0, s>>>(
+    mv_corr_partial_kernel<kLaplaceNeumann><<<ntiles, kCorrThreads, 0, s>>>(
         nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
   else
-    mv_corr_partial_kernel<kStokes><<<ntiles, kMvThreads, 0, s>>>(
+    mv_corr_partial_kernel<kStokes><<<ntiles, kCorrThreads, 0, s>>>(
         nodes, tiles, n_dofs, x, dscale, near2, part, part_rank1);
   mv_finish_kernel<<<(n_dofs + 255) / 256, 256, 0, s>>>(pde, nodes, n_dofs, splits, part,
                                                         part_rank1, seg, nseg, x, y, nb, U);

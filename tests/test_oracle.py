@@ -84,15 +84,44 @@ def test_analytic_ellipse():
 
 
 @pytest.mark.skipif(not K.ref_available(), reason="oracle/_ref not built here")
-def test_port_matches_live_reference_star16k():
-    pr = G.star_case()
+@pytest.mark.parametrize("make", [G.star_case, G.stokes_holes_case])
+def test_port_matches_live_reference_full_size(make):
+    """The restatement against the reference build on the two full-size
+    workloads (16,384-dof star; 65,536-dof Stokes disk with 8 holes)."""
+    pr = make()
     a = K.RefSolver(pr, threads=4)
     b = K.PortSolver(pr, threads=4)
     d = H.compare_solvers(a, b)
-    assert d["partition"] == 0 and d["rank"] == 0 and d["skel"] == 0
-    ma, _ = a.solve(pr.f)
-    mb, _ = b.solve(pr.f)
+    assert d["partition"] == 0 and d["rank"] == 0 and d["skel"] == 0, d
+    ma, aa = a.solve(pr.f)
+    mb, ab = b.solve(pr.f)
     assert H.rel(mb, ma) < 1e-10
+    if len(aa):
+        assert np.abs(ab - aa).max() < 1e-10 * max(1.0, np.abs(ma).max())
+
+
+SYMMETRIC_SHAPES = [n for n in CASES if n.split("_")[0] in ("circle", "annulus", "donut")]
+
+
+@pytest.mark.parametrize("name", SYMMETRIC_SHAPES)
+def test_symmetric_shape_ties_are_blas_defined(name):
+    """On the reference's rotation/mirror-symmetric test shapes columns tie
+    exactly in norm, and which tied column dgeqp3 takes first is decided by
+    the last bits of the BLAS's norms and reflector products.  The
+    restatement runs the reference's own steps (dgeqp3's dlaqp2 pivoting,
+    the same rank rule) with plain-loop BLAS; against the fixtures made by
+    the reference build (OpenBLAS) it shows the same kind of differences the
+    GPU tests allow on these shapes: identical partition, ranks off by at
+    most one in a few boxes, skeleton sets that differ where ties were
+    broken the other way."""
+    pr, tol, leaf = CASES[name]
+    gold = H.load_golden(name)
+    s = K.PortSolver(pr, id_tol=tol, max_leaf_dofs=leaf)
+    boxes = H.flatten(s)
+    assert H.compare_partition(boxes, gold) == 0
+    so = gold["skel_off"]
+    diffs = [abs(len(b["skel"]) - (so[q + 1] - so[q])) for q, b in enumerate(boxes)]
+    assert max(diffs) <= 1 and sum(d > 0 for d in diffs) <= max(2, len(boxes) // 20)
 
 
 def test_planted_error_is_caught():
@@ -107,3 +136,22 @@ def test_planted_error_is_caught():
     s = K.PortSolver(bad, id_tol=tol, max_leaf_dofs=leaf)
     mu, _ = s.solve(bad.f)
     assert H.rel(mu, gold["mu"]) > 1e-10
+
+
+def test_restatement_breaks_some_ties_differently():
+    """The evidence behind the bar above: with the same algorithm and plain
+    loops in place of OpenBLAS, the restatement's skeleton sets differ from
+    the reference build's on some boxes of the symmetric shapes (54 of 2,141
+    boxes when written), while matching them exactly on the four asymmetric
+    workload fixtures."""
+    skel_bad = 0
+    for name in SYMMETRIC_SHAPES:
+        pr, tol, leaf = CASES[name]
+        s = K.PortSolver(pr, id_tol=tol, max_leaf_dofs=leaf)
+        skel_bad += H.compare_skeletons(H.flatten(s), H.load_golden(name))[1]
+    assert skel_bad > 0
+    for name in ("ellipse_laplace_1024", "star_laplace_2048", "disk_holes_stokes_2048",
+                 "fourier_star_laplace_1024"):
+        pr, tol, leaf = CASES[name]
+        s = K.PortSolver(pr, id_tol=tol, max_leaf_dofs=leaf)
+        assert H.compare_skeletons(H.flatten(s), H.load_golden(name)) == (0, 0, 0)
