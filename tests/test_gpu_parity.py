@@ -49,8 +49,11 @@ def test_gpu_reference_shapes_backward_error(name):
     (kern_interp_test.cpp:79,92), A applied by the GPU's on-the-fly FP64
     operator, plus an exact partition.  These test shapes are rotation or
     mirror symmetric, so columns tie exactly in norm and the pivot order
-    among tied columns is implementation-defined (LAPACK's and ours may
-    differ); ranks are then allowed to differ by one in a few boxes."""
+    among tied columns is decided by the last bits of the BLAS's sums: the
+    CPU restatement with plain-loop BLAS differs from the reference build on
+    these shapes in the same way (test_oracle.py,
+    test_symmetric_shape_ties_are_blas_defined); ranks are then allowed to
+    differ by one in a few boxes."""
     import torch
     pr, tol, leaf = CASES[name]
     gold = H.load_golden(name)
@@ -104,7 +107,6 @@ def test_gpu_full_size_matches_reference_build(make):
     at its id_tol 1e-10: identical partition, ranks and skeleton sets, and
     the solution within 1e-10."""
     import os
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     pr = make()
     s = kinterp.Solver(pr)
     r = K.RefSolver(pr, threads=max(1, min(16, os.cpu_count() or 1)))
