@@ -1589,6 +1589,37 @@ cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int n
   return cudaGetLastError();
 }
 
+// Redundant-dof index of the bordered system (skel_factorization.cpp:
+// 130-160 splits the dofs into the top level's skeletons and the rest):
+// allred = the dofs outside the ascending, repeat-free skeleton list, in
+// ascending order; red_pos[d] = d's position in allred, -1 for a skeleton.
+// A dof's position is d minus the skeletons below it (binary search), so
+// the lists are made where they are used instead of on the host.
+__global__ void red_index_kernel(const int* __restrict__ skel_sorted, int ns, int n,
+                                 int* __restrict__ allred, int* __restrict__ red_pos) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  int lo = 0, hi = ns;  // the first skeleton >= d
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (skel_sorted[mid] < d) lo = mid + 1; else hi = mid;
+  }
+  if (lo < ns && skel_sorted[lo] == d) {
+    red_pos[d] = -1;
+    return;
+  }
+  red_pos[d] = d - lo;
+  allred[d - lo] = d;
+}
+
+cudaError_t launch_red_index(const int* skel_sorted, int ns, int n, int* allred, int* red_pos,
+                             cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  count_launches(1);
+  red_index_kernel<<<(n + 255) / 256, 256, 0, s>>>(skel_sorted, ns, n, allred, red_pos);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_gather_rows(const double* x, int ldd, const int* idx, int n, int nrhs,
                                double* out, int ldo, cudaStream_t s) {
   const long long tot = static_cast<long long>(n) * nrhs;

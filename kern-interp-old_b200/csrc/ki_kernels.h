@@ -292,6 +292,11 @@ cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int n
 // out[i + ldo c] = x[idx[i] ldd + c]: rows of a dof-major matrix
 cudaError_t launch_gather_rows(const double* x, int ldd, const int* idx, int n, int nrhs,
                                double* out, int ldo, cudaStream_t s);
+// allred (the n - ns dofs outside skel_sorted, ascending) and red_pos (n:
+// position in allred, -1 for a skeleton) from the ascending, repeat-free
+// skeleton dofs skel_sorted[0..ns), all below n
+cudaError_t launch_red_index(const int* skel_sorted, int ns, int n, int* allred, int* red_pos,
+                             cudaStream_t s);
 cudaError_t launch_scatter(double* x, int ldx, const int* idx, int n, int nrhs,
                            const double* in, int ldi, cudaStream_t s);
 // C = alpha * op(A) * op(B) + beta * C, small dense FP64 (column-major).

@@ -210,6 +210,8 @@ struct AuxSet {
   cudaEvent_t dl_fork = nullptr, dl_join[3] = {};
   cudaStream_t b = nullptr;
   cudaEvent_t ev_lvl = nullptr, ev_bdr = nullptr;
+  cudaStream_t u = nullptr;
+  cudaEvent_t ev_up = nullptr;
 };
 std::mutex g_aux_mu;
 std::vector<AuxSet>& aux_free() {
@@ -245,6 +247,7 @@ Solver::~Solver() {
   for (int i = 0; i < kDecStreams; i++)
     if (dl_streams_[i]) cudaStreamSynchronize(dl_streams_[i]);
   if (bstream_) cudaStreamSynchronize(bstream_);
+  if (ustream_) cudaStreamSynchronize(ustream_);
   if (dstream_) {
     static_assert(kIdStreams == 3 && kDecStreams == 3, "AuxSet holds three of each");
     AuxSet a;
@@ -266,6 +269,8 @@ Solver::~Solver() {
     a.b = bstream_;
     a.ev_lvl = ev_lvl_;
     a.ev_bdr = ev_bdr_;
+    a.u = ustream_;
+    a.ev_up = ev_up_;
     std::lock_guard<std::mutex> lk(g_aux_mu);
     aux_free().push_back(a);
   }
@@ -455,6 +460,8 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
           bstream_ = a.b;
           ev_lvl_ = a.ev_lvl;
           ev_bdr_ = a.ev_bdr;
+          ustream_ = a.u;
+          ev_up_ = a.ev_up;
           break;
         }
     }
@@ -476,6 +483,8 @@ int Solver::begin_factor(cudaEvent_t* ev0) {
       KI_CUDA(cudaStreamCreateWithFlags(&bstream_, cudaStreamNonBlocking));
       KI_CUDA(cudaEventCreateWithFlags(&ev_lvl_, cudaEventDisableTiming));
       KI_CUDA(cudaEventCreateWithFlags(&ev_bdr_, cudaEventDisableTiming));
+      KI_CUDA(cudaStreamCreateWithFlags(&ustream_, cudaStreamNonBlocking));
+      KI_CUDA(cudaEventCreateWithFlags(&ev_up_, cudaEventDisableTiming));
     }
   }
   {
@@ -659,16 +668,24 @@ int Solver::finish_factor(cudaEvent_t ev0) {
   // stream_: adopted factors, border columns
   KI_CUDA(cudaEventRecord(ev_id_[0], stream_));
   KI_CUDA(cudaStreamWaitEvent(dstream_, ev_id_[0], 0));
+  // the coarsest level whose active lists id_launch has made (each level's
+  // uncompressed boxes are refreshed there, after their children's ranks;
+  // nothing below changes afterwards): only the levels above it remain
+  int refreshed = L;
   if (L > 1) {
     // level l's IDs, then per level: the IDs of l - 1 launched, l's
     // decoupling prepared and launched while they run, l - 1's ranks read
     auto cur = std::make_unique<PendingLevel>();
     int rc = id_launch(L - 1, cur.get());
+    refreshed = L - 1;
     if (!rc) rc = id_finish(cur.get());
     for (int level = L - 1; level > 0 && !rc; level--) {
       auto next = std::make_unique<PendingLevel>();
       const bool more = level > 1 && !(level == 2 && level1_stays());
-      if (more) rc = id_launch(level - 1, next.get());
+      if (more) {
+        rc = id_launch(level - 1, next.get());
+        refreshed = level - 1;
+      }
       if (!rc) rc = decouple_level(cur.get());
       if (!rc && more) rc = id_finish(next.get());
       if (!more) break;
@@ -676,14 +693,17 @@ int Solver::finish_factor(cudaEvent_t ev0) {
     }
     if (rc) return rc;
   }
-  for (int level = L - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
+  for (int level = refreshed - 1; level >= 0; level--) tree.refresh_level(level, nullptr);
   allskel.clear();
   for (int r : tree.roots)
     allskel.insert(allskel.end(), tree.boxes[r].active.begin(), tree.boxes[r].active.end());
   KI_CUDA(cudaEventRecord(ev_dec_, dstream_));
   KI_CUDA(cudaStreamWaitEvent(stream_, ev_dec_, 0));
   KI_CUDA(cudaEventRecord(ev_bdr_, bstream_));
-  KI_CUDA(cudaStreamWaitEvent(stream_, ev_bdr_, 0));
+  // the top-level assembly needs only the decouplings: a single tree's
+  // border system waits for the border sweeps itself (factor_border), so
+  // the assembly runs beside the last level's sweeps
+  if (tree.roots.size() > 1 || nb_ == 0) KI_CUDA(cudaStreamWaitEvent(stream_, ev_bdr_, 0));
   cudaEvent_t t0 = nullptr;
   if (time_phases && timer_begin(&t0)) return -2;
   const double ht = now_ms();
@@ -1284,10 +1304,12 @@ int Solver::decouple_boxes(PendingLevel* pl) {
   // the largest boxes first (CTAs start in index order: no long last wave)
   std::stable_sort(small.begin(), small.end(),
                    [](const DecTask& a, const DecTask& b) { return a.n > b.n; });
-  KI_UPLOAD(d_bid, bid, dstream_);
-  KI_UPLOAD(d_bpos, bpos, dstream_);
-  KI_UPLOAD(d_tab, tab, dstream_);
-  KI_UPLOAD(d_dt, small, dstream_);
+  KI_UPLOAD(d_bid, bid, ustream_);
+  KI_UPLOAD(d_bpos, bpos, ustream_);
+  KI_UPLOAD(d_tab, tab, ustream_);
+  KI_UPLOAD(d_dt, small, ustream_);
+  KI_CUDA(cudaEventRecord(ev_up_, ustream_));
+  KI_CUDA(cudaStreamWaitEvent(dstream_, ev_up_, 0));
   DecParams dp{};
   dp.tasks = d_dt;
   dp.ntasks = static_cast<int>(small.size());
@@ -1382,9 +1404,11 @@ int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t 
     st[t] = SweepTask{b.rank, static_cast<int>(b.redundant.size()), lf.d_skel + sk_off[t],
                       lf.d_red + rd_off[t], bd.T, bd.L, bd.U, bd.X, bd.piv};
   }
-  KI_UPLOAD(lf.d_skel, sk, s);
-  KI_UPLOAD(lf.d_red, rd, s);
-  KI_UPLOAD(lf.d_tasks, st, s);
+  KI_UPLOAD(lf.d_skel, sk, ustream_);
+  KI_UPLOAD(lf.d_red, rd, ustream_);
+  KI_UPLOAD(lf.d_tasks, st, ustream_);
+  KI_CUDA(cudaEventRecord(ev_up_, ustream_));
+  KI_CUDA(cudaStreamWaitEvent(s, ev_up_, 0));
   lf.h_tasks = st;
   lf.ntasks = ncomp;
   lf.cap = cap;
@@ -1462,6 +1486,7 @@ int Solver::update(int n_points, const double* points, const double* normals,
   // nothing queued may still read the memory that is about to be replaced
   KI_CUDA(cudaStreamSynchronize(stream_));
   if (dstream_) KI_CUDA(cudaStreamSynchronize(dstream_));
+  if (ustream_) KI_CUDA(cudaStreamSynchronize(ustream_));
   {
     // no queued copy reads the staging any more: its chunks go back to the
     // pool and the refactorization stages into a fresh arena
@@ -1737,25 +1762,24 @@ int Solver::factor_border() {
   // skel_factorization.cpp:130-242: sweep U and Psi^T with the factors,
   // D^{-1} on the redundant rows, then the bordered Schur system S.
   const int N = n_dofs_, nb = nb_, ns = ns_;
+  // the redundant dofs (everything outside the top level's skeletons) and
+  // each dof's position among them, listed on the GPU from the sorted
+  // skeletons: no N-long host lists on the way to the top-level LU
   std::vector<int> sorted = allskel;
   std::sort(sorted.begin(), sorted.end());
-  allred.clear();
-  size_t si = 0;
-  for (int i = 0; i < N; i++) {
-    if (si < sorted.size() && i == sorted[si]) {
-      si++;
-    } else {
-      allred.push_back(i);
-    }
-  }
-  if (allred.empty()) return fail("No compression possible");
-  const int nr = static_cast<int>(allred.size());
-  std::vector<int> red_pos(N, -1);
-  for (int i = 0; i < nr; i++) red_pos[allred[i]] = i;
+  for (size_t i = 0; i < sorted.size(); i++)
+    if (sorted[i] < 0 || sorted[i] >= N || (i > 0 && sorted[i] == sorted[i - 1]))
+      return fail("top-level skeleton dofs out of range or repeated");
+  const int nr = N - static_cast<int>(sorted.size());
+  if (nr <= 0) return fail("No compression possible");
+  n_red_ = nr;
+  int* d_sorted;
+  KI_ALLOC(d_sorted, int, sorted.size());
   KI_ALLOC(d_allred_, int, nr);
   KI_ALLOC(d_red_pos_, int, N);
-  KI_UPLOAD(d_allred_, allred, stream_);
-  KI_UPLOAD(d_red_pos_, red_pos, stream_);
+  KI_UPLOAD(d_sorted, sorted, stream_);
+  KI_CUDA(launch_red_index(d_sorted, static_cast<int>(sorted.size()), N, d_allred_, d_red_pos_,
+                           stream_));
 
   // U and Psi^T were swept up level by level with the decoupling
   double* modU = d_modU_;
@@ -1769,6 +1793,7 @@ int Solver::factor_border() {
   KI_ALLOC(us, double, static_cast<size_t>(ns) * nb);
   KI_ALLOC(ps, double, static_cast<size_t>(ns) * nb);
   KI_ALLOC(corr, double, static_cast<size_t>(nb) * nb);
+  KI_CUDA(cudaStreamWaitEvent(stream_, ev_bdr_, 0));  // U, Psi^T swept up
   KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, d_Ured_, nr, stream_));
   KI_CUDA(launch_gather_rows(modP, nb, d_allred_, nr, nb, d_Pred_, nr, stream_));
   KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, dinv, nr, stream_));
@@ -1818,7 +1843,7 @@ int Solver::solve_device(const double* d_b, double* d_mu, double* d_alpha, const
       KI_CUDA(launch_scatter(x, N, d_allskel_, ns, 1, d_tmp_, ns, stream_));
     }
   } else {
-    const int nr = static_cast<int>(allred.size());
+    const int nr = n_red_;
     double* w = d_tmp_;
     double* dw = w + nr;
     double* M = dw + nr;

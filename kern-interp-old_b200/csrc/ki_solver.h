@@ -221,7 +221,7 @@ class Solver {
 
   QuadTreeHost tree;
   std::vector<int> allskel;
-  std::vector<int> allred;
+  int n_red_ = 0;  // dofs outside allskel (the bordered system's redundant rows)
 
   // Phase times of the last factor/solve (ms, CUDA events); id_ms is the
   // summed duration of the ID launches, id_launches their count.
@@ -349,6 +349,13 @@ class Solver {
   // the border columns' level sweeps (U, Psi^T), beside the decouplings
   cudaStream_t bstream_ = nullptr;
   cudaEvent_t ev_lvl_ = nullptr, ev_bdr_ = nullptr;
+  // a level's decoupling uploads (block maps, task lists, sweep
+  // descriptors): queued on their own stream, they copy while the level
+  // below is still decoupling, and the decoupling stream waits on ev_up_
+  // (long complete by then) instead of running the copies between two
+  // levels' decouplings, the factorization's longest chain
+  cudaStream_t ustream_ = nullptr;
+  cudaEvent_t ev_up_ = nullptr;
 
   bool onchip_ok_[17] = {};  // a G-CTA cluster with full shared memory fits
   Arena arena_;
