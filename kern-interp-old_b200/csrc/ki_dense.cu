@@ -1639,6 +1639,144 @@ cudaError_t launch_scatter(double* x, int ldx, const int* idx, int n, int nrhs,
   return cudaGetLastError();
 }
 
+// The bordered system's row gathers in one pass (skel_factorization.cpp:
+// 146-170): U, Psi^T and X_rr^{-1} U (dof-major, nb entries a dof) at the
+// redundant dofs into Ured, Pred and dinv, U and Psi^T at the top-level
+// skeletons into us, ps; all outputs column-major.
+__global__ void border_gather_kernel(const double* __restrict__ modU,
+                                     const double* __restrict__ modP,
+                                     const double* __restrict__ modD, int nb,
+                                     const int* __restrict__ allred, int nr,
+                                     const int* __restrict__ allskel, int ns,
+                                     double* __restrict__ Ured, double* __restrict__ Pred,
+                                     double* __restrict__ dinv, double* __restrict__ us,
+                                     double* __restrict__ ps) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(nr + ns) * nb) return;
+  const int c = static_cast<int>(e % nb), i = static_cast<int>(e / nb);
+  if (i < nr) {
+    const long long src = static_cast<long long>(allred[i]) * nb + c;
+    const long long dst = i + static_cast<long long>(nr) * c;
+    Ured[dst] = modU[src];
+    dinv[dst] = modD[src];
+    Pred[dst] = modP[src];
+  } else {
+    const int j = i - nr;
+    const long long src = static_cast<long long>(allskel[j]) * nb + c;
+    const long long dst = j + static_cast<long long>(ns) * c;
+    us[dst] = modU[src];
+    ps[dst] = modP[src];
+  }
+}
+
+cudaError_t launch_border_gather(const double* modU, const double* modP, const double* modD,
+                                 int nb, const int* allred, int nr, const int* allskel, int ns,
+                                 double* Ured, double* Pred, double* dinv, double* us,
+                                 double* ps, cudaStream_t s) {
+  const long long tot = static_cast<long long>(nr + ns) * nb;
+  if (tot == 0) return cudaSuccess;
+  count_launches(1);
+  border_gather_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(
+      modU, modP, modD, nb, allred, nr, allskel, ns, Ured, Pred, dinv, us, ps);
+  return cudaGetLastError();
+}
+
+// dst rows idx[0..n) <- src rows (dof-major, nb entries a dof)
+__global__ void copy_rows_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                 int nb, const int* __restrict__ idx, int n) {
+  const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (e >= static_cast<long long>(n) * nb) return;
+  const long long o = static_cast<long long>(idx[e / nb]) * nb + e % nb;
+  dst[o] = src[o];
+}
+
+cudaError_t launch_copy_rows(const double* src, double* dst, int nb, const int* idx, int n,
+                             cudaStream_t s) {
+  const long long tot = static_cast<long long>(n) * nb;
+  if (tot == 0) return cudaSuccess;
+  count_launches(1);
+  copy_rows_kernel<<<static_cast<int>((tot + 255) / 256), 256, 0, s>>>(src, dst, nb, idx, n);
+  return cudaGetLastError();
+}
+
+// C = alpha A^T B + beta C for a long inner dimension k and a small C (m, n
+// <= kLongTnMax): split over k, every CTA reading its rows of A and B once
+// (64 at a time through shared memory) and summing all m n entries of its
+// part; the parts are then added in split order (deterministic).  Replaces
+// a CTA per entry of C, which read A and B m n times over through L2.
+constexpr int kLongTnMax = 32;
+constexpr int kLongTnRows = 64;
+constexpr int kLongTnAcc = kLongTnMax * kLongTnMax / 256;  // entries of C a thread owns
+
+__global__ void __launch_bounds__(256) gemm_tn_split_kernel(int m, int n, int k, const double* a,
+                                                            int lda, const double* b, int ldb,
+                                                            int rows_per, double* part) {
+  __shared__ double As[kLongTnRows][kLongTnMax + 1], Bs[kLongTnRows][kLongTnMax + 1];
+  const int l0 = blockIdx.x * rows_per, l1 = min(k, l0 + rows_per);
+  const int mn = m * n;
+  double acc[kLongTnAcc];
+#pragma unroll
+  for (int q = 0; q < kLongTnAcc; q++) acc[q] = 0.0;
+  for (int r0 = l0; r0 < l1; r0 += kLongTnRows) {
+    const int rn = min(kLongTnRows, l1 - r0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kLongTnRows * m; e += blockDim.x) {
+      const int r = e % kLongTnRows, i = e / kLongTnRows;
+      As[r][i] = r < rn ? a[r0 + r + static_cast<long long>(lda) * i] : 0.0;
+    }
+    for (int e = threadIdx.x; e < kLongTnRows * n; e += blockDim.x) {
+      const int r = e % kLongTnRows, j = e / kLongTnRows;
+      Bs[r][j] = r < rn ? b[r0 + r + static_cast<long long>(ldb) * j] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kLongTnAcc; q++) {
+      const int o = threadIdx.x + 256 * q;
+      if (o < mn) {
+        const int i = o % m, j = o / m;
+        double v = acc[q];
+        for (int r = 0; r < kLongTnRows; r++) v += As[r][i] * Bs[r][j];
+        acc[q] = v;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kLongTnAcc; q++) {
+    const int o = threadIdx.x + 256 * q;
+    if (o < mn) part[static_cast<long long>(blockIdx.x) * mn + o] = acc[q];
+  }
+}
+
+__global__ void gemm_tn_split_finish_kernel(int m, int n, int splits, const double* part,
+                                            double alpha, double beta, double* c, int ldc) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mn = m * n;
+  if (o >= mn) return;
+  double v = 0.0;
+  for (int q = 0; q < splits; q++) v += part[static_cast<long long>(q) * mn + o];
+  double* cp = c + (o % m) + static_cast<long long>(ldc) * (o / m);
+  *cp = alpha * v + (beta == 0.0 ? 0.0 : beta * *cp);
+}
+
+int long_gemm_tn_splits(int m, int n, int k) {
+  if (m < 1 || n < 1 || m > kLongTnMax || n > kLongTnMax || k < 1) return 0;
+  return std::max(1, std::min(296, (k + 255) / 256));
+}
+
+cudaError_t long_gemm_tn(int m, int n, int k, double alpha, const double* a, int lda,
+                         const double* b, int ldb, double beta, double* c, int ldc,
+                         double* part, cudaStream_t s) {
+  const int splits = long_gemm_tn_splits(m, n, k);
+  if (splits < 1) return cudaErrorInvalidValue;
+  const int rows_per = (k + splits - 1) / splits;
+  const int used = (k + rows_per - 1) / rows_per;  // (every split gets rows)
+  count_launches(2);
+  gemm_tn_split_kernel<<<used, 256, 0, s>>>(m, n, k, a, lda, b, ldb, rows_per, part);
+  gemm_tn_split_finish_kernel<<<(m * n + 255) / 256, 256, 0, s>>>(m, n, used, part, alpha, beta,
+                                                                 c, ldc);
+  return cudaGetLastError();
+}
+
 cudaError_t small_gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* a,
                        int lda, const double* b, int ldb, double beta, double* c, int ldc,
                        cudaStream_t s) {

@@ -292,6 +292,23 @@ cudaError_t launch_gather(const double* x, int ldx, const int* idx, int n, int n
 // out[i + ldo c] = x[idx[i] ldd + c]: rows of a dof-major matrix
 cudaError_t launch_gather_rows(const double* x, int ldd, const int* idx, int n, int nrhs,
                                double* out, int ldo, cudaStream_t s);
+// Ured, Pred, dinv <- rows allred of U, Psi^T, X^{-1} U (dof-major, nb a
+// dof); us, ps <- rows allskel of U, Psi^T; outputs column-major (ld nr, ns)
+cudaError_t launch_border_gather(const double* modU, const double* modP, const double* modD,
+                                 int nb,
+                                 const int* allred, int nr, const int* allskel, int ns,
+                                 double* Ured, double* Pred, double* dinv, double* us,
+                                 double* ps, cudaStream_t s);
+// dst rows idx[0..n) <- the same rows of src (dof-major, nb entries a dof)
+cudaError_t launch_copy_rows(const double* src, double* dst, int nb, const int* idx, int n,
+                             cudaStream_t s);
+// C (m x n, m, n <= 32) = alpha A^T B + beta C, A k x m, B k x n column-major,
+// split over k; `part` holds long_gemm_tn_splits(m, n, k) * m * n doubles
+// (0: sizes not supported)
+int long_gemm_tn_splits(int m, int n, int k);
+cudaError_t long_gemm_tn(int m, int n, int k, double alpha, const double* a, int lda,
+                         const double* b, int ldb, double beta, double* c, int ldc,
+                         double* part, cudaStream_t s);
 // allred (the n - ns dofs outside skel_sorted, ascending) and red_pos (n:
 // position in allred, -1 for a skeleton) from the ascending, repeat-free
 // skeleton dofs skel_sorted[0..ns), all below n

@@ -567,6 +567,7 @@ int Solver::setup_geometry() {
     // Psi^T dof-major)
     KI_ALLOC(d_modU_, double, cnt);
     KI_ALLOC(d_modP_, double, cnt);
+    KI_ALLOC(d_modD_, double, cnt);
     KI_CUDA(cudaMemcpyAsync(d_modU_, d_Urow_, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
                             stream_));
     KI_CUDA(cudaMemcpyAsync(d_modP_, d_Psi_, sizeof(double) * cnt, cudaMemcpyDeviceToDevice,
@@ -917,16 +918,30 @@ int Solver::id_launch(int level, PendingLevel* pl) {
   int *d_act, *d_rows, *d_perm, *d_rank;
   double* d_T;
   IdTask* d_tasks;
-  KI_ALLOC(d_act, int, act.size());
-  KI_ALLOC(d_rows, int, rows.size());
-  KI_ALLOC(d_perm, int, perm_total);
-  KI_ALLOC(d_rank, int, nc);
+  // the level's three lists in one host-to-device copy and its ranks and
+  // pivots in one copy back: each copy adds its own latency to the chain of
+  // ID levels (a level's lists wait for the ranks of the level below)
+  const size_t b_act = sizeof(int) * act.size(), b_rows = sizeof(int) * rows.size();
+  const size_t o_rows = (b_act + 255) & ~static_cast<size_t>(255);
+  const size_t o_tasks = o_rows + ((b_rows + 255) & ~static_cast<size_t>(255));
+  const size_t b_pack = o_tasks + sizeof(IdTask) * nc;
+  char* d_pack;
+  KI_ALLOC(d_pack, char, b_pack);
+  d_act = reinterpret_cast<int*>(d_pack);
+  d_rows = reinterpret_cast<int*>(d_pack + o_rows);
+  d_tasks = reinterpret_cast<IdTask*>(d_pack + o_tasks);
+  KI_ALLOC(d_rank, int, nc + perm_total);  // [ranks | pivots]
+  d_perm = d_rank + nc;
   KI_ALLOC(d_T, double, t_total);
-  KI_ALLOC(d_tasks, IdTask, nc);
   KI_CUDA(work_.reserve(sizeof(double) * a_total, stream_));
-  KI_UPLOAD(d_act, act, stream_);
-  KI_UPLOAD(d_rows, rows, stream_);
-  KI_UPLOAD(d_tasks, tasks, stream_);
+  {
+    char* st = static_cast<char*>(stage_.alloc(b_pack));
+    if (!st) return fail("pinned staging allocation failed");
+    if (b_act) std::memcpy(st, act.data(), b_act);
+    if (b_rows) std::memcpy(st + o_rows, rows.data(), b_rows);
+    std::memcpy(st + o_tasks, tasks.data(), sizeof(IdTask) * nc);
+    KI_CUDA(cudaMemcpyAsync(d_pack, st, b_pack, cudaMemcpyHostToDevice, stream_));
+  }
 
   // one launch per cluster size (split further so that the launch's
   // shared-memory layout, sized by its largest rows / columns / column
@@ -1000,12 +1015,11 @@ int Solver::id_launch(int level, PendingLevel* pl) {
   pl->ids_queued = true;
   // ranks and pivots into pinned memory: the copies queue behind the IDs
   // without blocking the host (a copy to pageable memory would wait for them)
-  pl->rank = static_cast<int*>(stage_.alloc(sizeof(int) * nc));
-  pl->perm = static_cast<int*>(stage_.alloc(sizeof(int) * (perm_total + 1)));
-  if (!pl->rank || !pl->perm) return fail("pinned staging allocation failed");
-  KI_CUDA(cudaMemcpyAsync(pl->rank, d_rank, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream_));
-  KI_CUDA(cudaMemcpyAsync(pl->perm, d_perm, sizeof(int) * perm_total, cudaMemcpyDeviceToHost,
-                          stream_));
+  pl->rank = static_cast<int*>(stage_.alloc(sizeof(int) * (nc + perm_total + 1)));
+  if (!pl->rank) return fail("pinned staging allocation failed");
+  pl->perm = pl->rank + nc;
+  KI_CUDA(cudaMemcpyAsync(pl->rank, d_rank, sizeof(int) * (nc + perm_total),
+                          cudaMemcpyDeviceToHost, stream_));
   pl->d_act = d_act;
   pl->d_rows = d_rows;
   pl->d_perm = d_perm;
@@ -1174,6 +1188,14 @@ int Solver::decouple_level(PendingLevel* pl) {
     KI_CUDA(cudaEventRecord(ev_lvl_, dstream_));
     KI_CUDA(cudaStreamWaitEvent(bstream_, ev_lvl_, 0));
     KI_CUDA(launch_sweep_up_pair(sp, spp, bstream_));
+    // the level's redundant rows of U are final now (coarser levels' sweeps
+    // touch only their own active dofs): X_rr^{-1} is applied to a copy of
+    // them here, beside the next decouplings, instead of to every box's at
+    // once between the last decoupling and the top-level LU
+    KI_CUDA(launch_copy_rows(d_modU_, d_modD_, nb_, lf.d_red, lf.nred, bstream_));
+    SweepParams sd = sp;
+    sd.x = d_modD_;
+    KI_CUDA(launch_diag_solve(sd, bstream_));
   }
   return 0;
 }
@@ -1411,6 +1433,7 @@ int Solver::level_sweeps(int level, const std::vector<int>& boxes, cudaStream_t 
   KI_CUDA(cudaStreamWaitEvent(s, ev_up_, 0));
   lf.h_tasks = st;
   lf.ntasks = ncomp;
+  lf.nred = static_cast<int>(rd.size());
   lf.cap = cap;
   lf.kr = kr;
   return 0;
@@ -1438,7 +1461,7 @@ void Solver::drop_device_state() {
   d_top_dinv_ = nullptr;
   d_allskel_ = d_allred_ = d_red_pos_ = nullptr;
   d_U_ = d_Psi_ = d_Urow_ = d_Ured_ = d_Pred_ = d_tmp_ = nullptr;
-  d_modU_ = d_modP_ = nullptr;
+  d_modU_ = d_modP_ = d_modD_ = nullptr;
   all_compressed_ = LevelFactors{};
   levels_.clear();
 }
@@ -1794,15 +1817,17 @@ int Solver::factor_border() {
   KI_ALLOC(ps, double, static_cast<size_t>(ns) * nb);
   KI_ALLOC(corr, double, static_cast<size_t>(nb) * nb);
   KI_CUDA(cudaStreamWaitEvent(stream_, ev_bdr_, 0));  // U, Psi^T swept up
-  KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, d_Ured_, nr, stream_));
-  KI_CUDA(launch_gather_rows(modP, nb, d_allred_, nr, nb, d_Pred_, nr, stream_));
-  KI_CUDA(launch_gather_rows(modU, nb, d_allred_, nr, nb, dinv, nr, stream_));
-  KI_CUDA(launch_gather_rows(modU, nb, d_allskel_, ns, nb, us, ns, stream_));
-  KI_CUDA(launch_gather_rows(modP, nb, d_allskel_, ns, nb, ps, ns, stream_));
-  SweepParams dp{all_compressed_.d_tasks, all_compressed_.ntasks, dinv, nr, nb, 1, d_red_pos_,
-                 all_compressed_.cap};
-  KI_CUDA(launch_diag_solve(dp, stream_));
-  KI_CUDA(small_gemm(true, false, nb, nb, nr, 1.0, d_Pred_, nr, dinv, nr, 0.0, corr, nb, stream_));
+  // (dinv: X_rr^{-1} U_r of every compressed box, solved level by level)
+  KI_CUDA(launch_border_gather(modU, modP, d_modD_, nb, d_allred_, nr, d_allskel_, ns, d_Ured_,
+                               d_Pred_, dinv, us, ps, stream_));
+  if (const int splits = long_gemm_tn_splits(nb, nb, nr)) {
+    double* part;
+    KI_ALLOC(part, double, static_cast<size_t>(splits) * nb * nb);
+    KI_CUDA(long_gemm_tn(nb, nb, nr, 1.0, d_Pred_, nr, dinv, nr, 0.0, corr, nb, part, stream_));
+  } else {
+    KI_CUDA(small_gemm(true, false, nb, nb, nr, 1.0, d_Pred_, nr, dinv, nr, 0.0, corr, nb,
+                       stream_));
+  }
   KI_CUDA(launch_fill_border(d_top_, ns + nb, ns, nb, us, ps, corr, stream_));
   if (time_phases && timer_end(b0, {0, 3, 1, nb, 0, N, 0.0})) return -2;
   return 0;

@@ -114,6 +114,7 @@ struct LevelFactors {
   std::vector<SweepTask> h_tasks;  // host copy of d_tasks
   int* d_skel = nullptr;
   int* d_red = nullptr;
+  int nred = 0;  // entries of d_red (the level's redundant dofs)
   std::vector<int> boxes;  // compressed boxes of this level
 };
 
@@ -404,6 +405,9 @@ class Solver {
   double* d_Urow_ = nullptr;  // U dof-major (N x nb, row i contiguous)
   double* d_modU_ = nullptr;  // U and Psi^T dof-major, swept up level by level
   double* d_modP_ = nullptr;
+  // X_rr^{-1} U at every compressed box's redundant rows (dof-major), filled
+  // level by level on the border stream
+  double* d_modD_ = nullptr;
   double* d_Ured_ = nullptr;  // modified U rows of allred (|red| x nb)
   double* d_Pred_ = nullptr;  // modified Psi^T rows of allred (|red| x nb)
   double* d_tmp_ = nullptr;   // solve scratch
