@@ -254,8 +254,36 @@ __device__ __forceinline__ void sweep_body(const SweepParams& P, int chunk, doub
   }
 }
 
+// The solve is a chain of short dependent launches (a few per level, up
+// and down the tree).  They are launched as programmatic dependents of the
+// kernel before them: the launch is processed while that kernel's last
+// blocks drain, and each block first waits (griddepcontrol.wait) until the
+// previous grid has completed and its writes are visible, so no read of x
+// can overtake its producer.  Outside such a launch the wait returns at once.
+__device__ __forceinline__ void wait_prior_grid() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_chained(void (*kernel)(KArgs...), int blocks, int threads, size_t smem,
+                           cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, args...);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int chunk) {
+  wait_prior_grid();
   extern __shared__ double sm[];
   sweep_body<MODE>(P, chunk, sm);
 }
@@ -264,6 +292,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_kernel(SweepParams P, int
 // 512 threads per box (see apply_sub_wide).
 template <int MODE>
 __global__ void __launch_bounds__(kWideThreads) sweep_wide_kernel(SweepParams P) {
+  wait_prior_grid();
   extern __shared__ double sm[];
   sweep_body<MODE>(P, 1, sm, true);
 }
@@ -287,6 +316,7 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_pair_kernel(SweepParams p
 constexpr int kDiagThreads = 256;
 template <bool TRANS>
 __global__ void __launch_bounds__(kDiagThreads) diag_inv_kernel(SweepParams P, int chunk) {
+  wait_prior_grid();
   extern __shared__ double sm[];
   const SweepTask tk = P.tasks[blockIdx.x];
   const int r = tk.r;
@@ -394,15 +424,13 @@ cudaError_t launch_mode(const SweepParams& p0, cudaStream_t s) {
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(wsmem));
     if (e != cudaSuccess) return e;
-    sweep_wide_kernel<MODE><<<p.ntasks, kWideThreads, wsmem, s>>>(p);
-    return cudaGetLastError();
+    return launch_chained(sweep_wide_kernel<MODE>, p.ntasks, kWideThreads, wsmem, s, p);
   }
   cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&sweep_kernel<MODE>),
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem));
   if (e != cudaSuccess) return e;
-  sweep_kernel<MODE><<<p.ntasks, kSweepThreads, smem, s>>>(p, nc);
-  return cudaGetLastError();
+  return launch_chained(sweep_kernel<MODE>, p.ntasks, kSweepThreads, smem, s, p, nc);
 }
 
 }  // namespace
@@ -444,6 +472,7 @@ namespace {
 // stored negated).
 template <bool TRANS>
 __global__ void __launch_bounds__(kWideThreads) diag_wide_kernel(SweepParams P) {
+  wait_prior_grid();
   extern __shared__ double sm[];
   const SweepTask tk = P.tasks[blockIdx.x];
   const int r = tk.r;
@@ -483,16 +512,14 @@ cudaError_t launch_diag(const SweepParams& p0, cudaStream_t s) {
                                     static_cast<int>(wsmem));
     if (e != cudaSuccess) return e;
     count_launches(1);
-    diag_wide_kernel<TRANS><<<p.ntasks, kWideThreads, wsmem, s>>>(p);
-    return cudaGetLastError();
+    return launch_chained(diag_wide_kernel<TRANS>, p.ntasks, kWideThreads, wsmem, s, p);
   }
   cudaError_t e = raise_func_attr(reinterpret_cast<const void*>(&diag_inv_kernel<TRANS>),
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   static_cast<int>(smem));
   if (e != cudaSuccess) return e;
   count_launches(1);
-  diag_inv_kernel<TRANS><<<p.ntasks, kDiagThreads, smem, s>>>(p, nc);
-  return cudaGetLastError();
+  return launch_chained(diag_inv_kernel<TRANS>, p.ntasks, kDiagThreads, smem, s, p, nc);
 }
 }  // namespace
 
