@@ -1706,45 +1706,49 @@ cudaError_t launch_copy_rows(const double* src, double* dst, int nb, const int* 
 // a CTA per entry of C, which read A and B m n times over through L2.
 constexpr int kLongTnMax = 32;
 constexpr int kLongTnRows = 64;
-constexpr int kLongTnAcc = kLongTnMax * kLongTnMax / 256;  // entries of C a thread owns
 
+// A thread owns a 2 x 2 block of C (four independent FMA chains, four
+// shared-memory loads per four FMAs); the tiles' columns past m and n are
+// zero, so an odd m or n needs no test in the loop.
 __global__ void __launch_bounds__(256) gemm_tn_split_kernel(int m, int n, int k, const double* a,
                                                             int lda, const double* b, int ldb,
                                                             int rows_per, double* part) {
-  __shared__ double As[kLongTnRows][kLongTnMax + 1], Bs[kLongTnRows][kLongTnMax + 1];
+  __shared__ double As[kLongTnRows][kLongTnMax + 2], Bs[kLongTnRows][kLongTnMax + 2];
   const int l0 = blockIdx.x * rows_per, l1 = min(k, l0 + rows_per);
-  const int mn = m * n;
-  double acc[kLongTnAcc];
-#pragma unroll
-  for (int q = 0; q < kLongTnAcc; q++) acc[q] = 0.0;
+  const int mb = (m + 1) / 2, nbk = (n + 1) / 2;
+  const bool owner = threadIdx.x < mb * nbk;
+  const int i0 = 2 * (threadIdx.x % mb), j0 = 2 * (threadIdx.x / mb);
+  double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
   for (int r0 = l0; r0 < l1; r0 += kLongTnRows) {
     const int rn = min(kLongTnRows, l1 - r0);
     __syncthreads();
-    for (int e = threadIdx.x; e < kLongTnRows * m; e += blockDim.x) {
+    for (int e = threadIdx.x; e < kLongTnRows * (2 * mb); e += blockDim.x) {
       const int r = e % kLongTnRows, i = e / kLongTnRows;
-      As[r][i] = r < rn ? a[r0 + r + static_cast<long long>(lda) * i] : 0.0;
+      As[r][i] = r < rn && i < m ? a[r0 + r + static_cast<long long>(lda) * i] : 0.0;
     }
-    for (int e = threadIdx.x; e < kLongTnRows * n; e += blockDim.x) {
+    for (int e = threadIdx.x; e < kLongTnRows * (2 * nbk); e += blockDim.x) {
       const int r = e % kLongTnRows, j = e / kLongTnRows;
-      Bs[r][j] = r < rn ? b[r0 + r + static_cast<long long>(ldb) * j] : 0.0;
+      Bs[r][j] = r < rn && j < n ? b[r0 + r + static_cast<long long>(ldb) * j] : 0.0;
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kLongTnAcc; q++) {
-      const int o = threadIdx.x + 256 * q;
-      if (o < mn) {
-        const int i = o % m, j = o / m;
-        double v = acc[q];
-        for (int r = 0; r < kLongTnRows; r++) v += As[r][i] * Bs[r][j];
-        acc[q] = v;
+    if (owner) {
+#pragma unroll 16
+      for (int r = 0; r < kLongTnRows; r++) {
+        const double a0 = As[r][i0], a1 = As[r][i0 + 1];
+        const double b0 = Bs[r][j0], b1 = Bs[r][j0 + 1];
+        c00 += a0 * b0;
+        c01 += a0 * b1;
+        c10 += a1 * b0;
+        c11 += a1 * b1;
       }
     }
   }
-#pragma unroll
-  for (int q = 0; q < kLongTnAcc; q++) {
-    const int o = threadIdx.x + 256 * q;
-    if (o < mn) part[static_cast<long long>(blockIdx.x) * mn + o] = acc[q];
-  }
+  if (!owner) return;
+  double* pp = part + static_cast<long long>(blockIdx.x) * m * n;
+  if (i0 < m && j0 < n) pp[i0 + m * j0] = c00;
+  if (i0 < m && j0 + 1 < n) pp[i0 + m * (j0 + 1)] = c01;
+  if (i0 + 1 < m && j0 < n) pp[i0 + 1 + m * j0] = c10;
+  if (i0 + 1 < m && j0 + 1 < n) pp[i0 + 1 + m * (j0 + 1)] = c11;
 }
 
 __global__ void gemm_tn_split_finish_kernel(int m, int n, int splits, const double* part,
