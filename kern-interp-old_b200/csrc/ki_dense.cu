@@ -1651,9 +1651,11 @@ __global__ void border_gather_kernel(const double* __restrict__ modU,
                                      double* __restrict__ Ured, double* __restrict__ Pred,
                                      double* __restrict__ dinv, double* __restrict__ us,
                                      double* __restrict__ ps) {
+  // the row index runs fastest: the column-major writes coalesce, and a
+  // dof's nb entries, read by nb neighbouring passes, come from cache
   const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
   if (e >= static_cast<long long>(nr + ns) * nb) return;
-  const int c = static_cast<int>(e % nb), i = static_cast<int>(e / nb);
+  const int c = static_cast<int>(e / (nr + ns)), i = static_cast<int>(e % (nr + ns));
   if (i < nr) {
     const long long src = static_cast<long long>(allred[i]) * nb + c;
     const long long dst = i + static_cast<long long>(nr) * c;
@@ -1713,24 +1715,40 @@ constexpr int kLongTnRows = 64;
 __global__ void __launch_bounds__(256) gemm_tn_split_kernel(int m, int n, int k, const double* a,
                                                             int lda, const double* b, int ldb,
                                                             int rows_per, double* part) {
+  // tile loads staged in registers: a tile's loads are all in flight at
+  // once, and the next tile's while this one is summed (one memory round
+  // trip per CTA instead of one per load and tile)
+  constexpr int kLoads = kLongTnRows * (kLongTnMax + 1) / 256 + 1;
   __shared__ double As[kLongTnRows][kLongTnMax + 2], Bs[kLongTnRows][kLongTnMax + 2];
   const int l0 = blockIdx.x * rows_per, l1 = min(k, l0 + rows_per);
   const int mb = (m + 1) / 2, nbk = (n + 1) / 2;
+  const int ea = kLongTnRows * 2 * mb, eb = kLongTnRows * 2 * nbk;  // tile entries
   const bool owner = threadIdx.x < mb * nbk;
   const int i0 = 2 * (threadIdx.x % mb), j0 = 2 * (threadIdx.x / mb);
-  double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
-  for (int r0 = l0; r0 < l1; r0 += kLongTnRows) {
+  double ra[kLoads], rb[kLoads];
+  auto fetch = [&](int r0) {
     const int rn = min(kLongTnRows, l1 - r0);
-    __syncthreads();
-    for (int e = threadIdx.x; e < kLongTnRows * (2 * mb); e += blockDim.x) {
-      const int r = e % kLongTnRows, i = e / kLongTnRows;
-      As[r][i] = r < rn && i < m ? a[r0 + r + static_cast<long long>(lda) * i] : 0.0;
+#pragma unroll
+    for (int q = 0; q < kLoads; q++) {
+      const int e = threadIdx.x + 256 * q;
+      const int r = e % kLongTnRows, c = e / kLongTnRows;
+      ra[q] = e < ea && r < rn && c < m ? a[r0 + r + static_cast<long long>(lda) * c] : 0.0;
+      rb[q] = e < eb && r < rn && c < n ? b[r0 + r + static_cast<long long>(ldb) * c] : 0.0;
     }
-    for (int e = threadIdx.x; e < kLongTnRows * (2 * nbk); e += blockDim.x) {
-      const int r = e % kLongTnRows, j = e / kLongTnRows;
-      Bs[r][j] = r < rn && j < n ? b[r0 + r + static_cast<long long>(ldb) * j] : 0.0;
+  };
+  double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+  if (l0 < l1) fetch(l0);
+  for (int r0 = l0; r0 < l1; r0 += kLongTnRows) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kLoads; q++) {
+      const int e = threadIdx.x + 256 * q;
+      const int r = e % kLongTnRows, c = e / kLongTnRows;
+      if (e < ea) As[r][c] = ra[q];
+      if (e < eb) Bs[r][c] = rb[q];
     }
     __syncthreads();
+    if (r0 + kLongTnRows < l1) fetch(r0 + kLongTnRows);
     if (owner) {
 #pragma unroll 16
       for (int r = 0; r < kLongTnRows; r++) {
